@@ -1,0 +1,192 @@
+/*
+ * amoeba_gpu.h -- C ABI of libamoeba_gpu.so, the sm_100a (B200) AMOEBA
+ * electrostatics library: permanent multipoles (empole), the mutual
+ * induced-dipole solve (induce) and polarization energy/forces (epolar),
+ * each as real-space Ewald pairs (with Thole damping for polarization) plus
+ * a smooth-PME reciprocal part.
+ *
+ * The entry points replace, for a caller of the reference (momokchung/polmdqc):
+ *   - polmdqc::empole<CalcMode>()   src/md/empole.cpp:49-83 (dispatcher) and
+ *     empole_a src/md/empole.cpp:96-357 (the only implemented variant; the
+ *     Ewald variants empole_c/d are stubs at src/md/empole.cpp:53-64,359-368)
+ *   - polmdqc::epolar<CalcMode>()   whose call is commented out at
+ *     src/md/energy.cpp:267 (no induce/epolar code exists in the reference)
+ *   - the electrostatic part of polmdqc::energy<CalcMode>()
+ *     src/md/energy.cpp:31-338
+ * Inputs are exactly the module globals those routines read after mechanic()
+ * (atoms.h, mpole.h, polar.h, polgrp.h, couple.h, polpot.h, mplpot.h,
+ * ewald.h, pme.h, boxes.h, chgpot.h); outputs are the globals they write
+ * (energi.h em/ep, deriv.h dem/dep, analyz.h aem/aep, action.h nem/nep,
+ * inter.h einter, virial.h vir, polar.h uind/uinp).
+ *
+ * Conventions (all follow the reference):
+ *   - coordinates in Angstrom; energies in kcal/mol; gradients are dE/dx in
+ *     kcal/mol/Angstrom (deriv.h "dem"), ADDED to the caller's arrays;
+ *   - multipoles: 13 components per atom [c, dx,dy,dz, qxx,qxy,qxz, qyx,qyy,
+ *     qyz, qzx,qzy,qzz] in the local frame, dipoles in e*Angstrom and
+ *     quadrupoles already divided by 3 (kmpole.cpp:547-550);
+ *   - frame atoms zaxis/xaxis/yaxis are 1-based, 0 = none; yaxis < 0 marks a
+ *     chiral site (mpole.h); polaxe uses the LocalFrame enum (kmulti.h:23-31);
+ *   - 1-n neighbour and polarization-group lists are 0-based (couple.h,
+ *     polgrp.h) and passed as CSR (offsets[n+1], indices);
+ *   - induced dipoles in e*Angstrom (polar.h uind/uinp); convergence eps in
+ *     Debye RMS per polarizable site (polpot.h poleps).
+ *
+ * Every function returns an int status (AMG_OK = 0) and never exits the
+ * process; amg_last_error() gives a message for the last failing call.
+ * One host thread per context; calls are synchronous (stream-ordered and
+ * synchronized before returning).
+ */
+#ifndef AMOEBA_GPU_H
+#define AMOEBA_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AMG_ABI_VERSION 1
+
+/* status codes */
+#define AMG_OK               0
+#define AMG_ERR_BAD_ARG      1
+#define AMG_ERR_UNSUPPORTED  2  /* cell shape / feature not implemented */
+#define AMG_ERR_NO_CONVERGE  3  /* PCG reached politer without meeting poleps */
+#define AMG_ERR_NAN          4  /* non-finite energy or gradient */
+#define AMG_ERR_CUDA         5  /* a CUDA runtime / cuFFT call failed */
+#define AMG_ERR_NO_DEVICE    6  /* no usable sm_100 device */
+#define AMG_ERR_OUT_OF_RANGE 7  /* size limit of the entry point exceeded */
+
+/* local frame types, same numbering as the reference's LocalFrame enum */
+#define AMG_FRAME_NONE       0
+#define AMG_FRAME_ZTHENX     1
+#define AMG_FRAME_ZONLY      2
+#define AMG_FRAME_BISECTOR   3
+#define AMG_FRAME_ZBISECT    4
+#define AMG_FRAME_THREEFOLD  5
+
+/* arithmetic of a context */
+#define AMG_PREC_FP64   0  /* every kernel in double precision */
+#define AMG_PREC_MIXED  1  /* FP32 pair/grid work; FP64 PCG dots, norms,
+                              accumulators and one FP64 correction sweep */
+
+/* polarization models (polpot.h poltyp) */
+#define AMG_POL_NONE    0
+#define AMG_POL_MUTUAL  1
+#define AMG_POL_DIRECT  2
+
+/* CalcMode flags for amg_forward (reference calcMode.h:18-45) */
+#define AMG_DO_ENERGY    1
+#define AMG_DO_ANALYSIS  2  /* per-atom energies, pair counts, einter */
+#define AMG_DO_GRADIENT  4
+#define AMG_DO_VIRIAL    8
+#define AMG_DO_DIPOLES  16  /* copy uind/uinp back */
+
+typedef struct amg_list {
+    const int32_t* offsets;   /* [n+1] */
+    const int32_t* indices;   /* [offsets[n]] 0-based atom numbers */
+} amg_list;
+
+typedef struct amg_params {
+    int32_t n;                       /* atoms (atoms.h n) */
+    const double* pole;              /* [n*13] local-frame multipoles (mpole.h pole) */
+    const int32_t* zaxis;            /* [n] 1-based, 0 = none */
+    const int32_t* xaxis;
+    const int32_t* yaxis;
+    const int32_t* polaxe;           /* [n] AMG_FRAME_* */
+    const int32_t* molcule;          /* [n] molecule id (molcul.h), for einter; may be NULL */
+    const double* polarity;          /* [n] Angstrom^3 (polar.h); NULL if no polarization */
+    const double* thole;             /* [n] */
+    const double* pdamp;             /* [n] polarity^(1/6) */
+    amg_list i12, i13, i14, i15;     /* couple.h */
+    amg_list ip11, ip12, ip13, ip14; /* polgrp.h (ip11 includes the atom itself) */
+    double m_scale[4];               /* m2..m5   (mplpot.h) */
+    double p_scale[4];               /* p2..p5   (polpot.h) */
+    double p_iscale[4];              /* p2i..p5i */
+    double d_scale[4];               /* d1..d4 */
+    double u_scale[4];               /* u1..u4 */
+    int32_t use_ewald;               /* limits.h use_ewald */
+    int32_t use_bounds;              /* bound.h use_bounds (periodic box) */
+    double aewald;                   /* ewald.h aeewald (1/Angstrom) */
+    int32_t nfft[3];                 /* pme.h nefft1..3 */
+    int32_t bsorder;                 /* pme.h bseorder (B-spline order) */
+    double cutoff;                   /* real-space cutoff: ewaldcut with Ewald, mpolecut without */
+    int32_t poltyp;                  /* AMG_POL_* */
+    double poleps;                   /* polpot.h poleps (Debye RMS) */
+    int32_t politer;                 /* polpot.h politer */
+    double electric;                 /* chgpot.h electric (kcal/mol*Angstrom/e^2) */
+    double dielec;                   /* chgpot.h dielec */
+    double debye;                    /* units.h debye (e*Angstrom -> Debye) */
+    int32_t precision;               /* AMG_PREC_* */
+    int32_t pcg_guess;               /* polpcg.h pcgguess: start from direct dipoles */
+    int32_t device;                  /* CUDA device ordinal */
+} amg_params;
+
+typedef struct amg_results {
+    double em;          /* permanent multipole energy */
+    double ep;          /* polarization energy */
+    double einter;      /* intermolecular part of em+ep (AMG_DO_ANALYSIS) */
+    int64_t nem;        /* multipole pairs with nonzero energy (AMG_DO_ANALYSIS) */
+    int64_t nep;        /* polarization sites with nonzero energy (AMG_DO_ANALYSIS) */
+    double vir[9];      /* added to with AMG_DO_VIRIAL (real-space part only) */
+    double* dem;        /* [n*3] gradient of em, ADDED to; may be NULL */
+    double* dep;        /* [n*3] gradient of ep, ADDED to; may be NULL */
+    double* aem;        /* [n] per-atom em (AMG_DO_ANALYSIS), overwritten; may be NULL */
+    double* aep;        /* [n] per-atom ep (AMG_DO_ANALYSIS), overwritten; may be NULL */
+    double* uind;       /* [n*3] mutual induced dipoles (AMG_DO_DIPOLES); may be NULL */
+    double* uinp;       /* [n*3] dipoles in the polarization-energy field; may be NULL */
+    double* rpole;      /* [n*13] global-frame multipoles; may be NULL */
+    int32_t pcg_iters;  /* PCG iterations taken */
+    double pcg_eps;     /* final RMS residual (Debye) */
+} amg_results;
+
+/* Cotangents (upstream adjoints) for amg_backward.  The scalar seed dE on the
+ * total energy em+ep is the usual case; the dipole cotangents make the
+ * backward solve one extra PCG with the same symmetric operator. */
+typedef struct amg_cotangents {
+    double d_energy;          /* dL/d(em+ep) */
+    const double* d_uind;     /* [n*3] dL/duind, or NULL */
+    const double* d_uinp;     /* [n*3] dL/duinp, or NULL */
+} amg_cotangents;
+
+/* Gradients of L with respect to the parameters; any pointer may be NULL. */
+typedef struct amg_param_grads {
+    double* d_pole;       /* [n*13] dL/d(local-frame pole) */
+    double* d_polarity;   /* [n] dL/dpolarity (includes the pdamp = alpha^(1/6) path) */
+    double* d_thole;      /* [n] dL/dthole (through pair thole = min(thole_i, thole_k)) */
+    double* d_xyz;        /* [n*3] dL/dx */
+} amg_param_grads;
+
+typedef struct amg_ctx amg_ctx;
+
+/* Creates a context on params->device: uploads parameters, topology-derived
+ * scaled-pair tables and PME plans.  Arrays in params are copied. */
+int amg_create(const amg_params* params, amg_ctx** out);
+
+/* Sets coordinates [n*3] (Angstrom) and the box: a,b,c (Angstrom) and
+ * alpha,beta,gamma (degrees) as boxes.h xbox,ybox,zbox,alphaA,betaA,gammaA.
+ * Only orthogonal boxes are supported with use_bounds (else UNSUPPORTED). */
+int amg_set_coords(amg_ctx* ctx, const double* xyz, const double box[6]);
+
+/* Evaluates em and ep (and their gradients, analysis data, dipoles) for the
+ * current coordinates.  flags: AMG_DO_* bits. */
+int amg_forward(amg_ctx* ctx, int32_t flags, amg_results* res);
+
+/* Adjoint of the last amg_forward: gradients of L = d_energy*(em+ep)
+ * + <d_uind,uind> + <d_uinp,uinp> with respect to the parameters and
+ * coordinates, recomputing pair intermediates instead of storing them. */
+int amg_backward(amg_ctx* ctx, const amg_cotangents* cot, amg_param_grads* grads);
+
+/* Timing of the last amg_forward on the device (ms) by phase: 0 total,
+ * 1 setup (rotation, sort, lists), 2 permanent field, 3 PCG, 4 forces. */
+int amg_last_timing(amg_ctx* ctx, double ms[5]);
+
+const char* amg_last_error(amg_ctx* ctx);
+int amg_abi_version(void);
+void amg_destroy(amg_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AMOEBA_GPU_H */

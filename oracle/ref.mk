@@ -1,0 +1,67 @@
+# Builds the reference (momokchung/polmdqc) MD library from its own sources into
+# oracle/_ref/, for use as a test-only checker.  Nothing here is shipped: the
+# product library never links these objects.
+#
+#   make -f oracle/ref.mk REF=/root/reference -j8
+#
+# Flags follow the reference's CMakeLists.txt:15 (-O3 -finline-functions
+# -ffast-math -fopenmp).  The upstream CMake build is not used: it hard-codes
+# homebrew compilers and libint2/OpenBLAS/GMP paths.  The alpha-shape / GMP
+# sources and the QM programs are left out (not on the electrostatics path).
+
+REF    ?= /root/reference
+OUT    ?= oracle/_ref
+REFCXX ?= g++
+INC     = -I$(REF)/include -I$(REF)/include/md -I$(REF)/include/oqc -I$(REF)/include/qc
+FLAGS   = -std=c++17 -O3 -finline-functions -ffast-math -fopenmp -fPIC -w
+
+EXCLUDE = delcx sosgmp alfcx alphavol alphamol alphamol1 alphamol2 alfmol alforder \
+          alfboxsize initalf initalf2 initalfatm spacefill tetrahedron vertex edge face \
+          hilbert kalf kdtree multimol
+MD_ALL  = $(basename $(notdir $(wildcard $(REF)/src/md/*.cpp)))
+MD_SRC  = $(filter-out %Exe $(EXCLUDE),$(MD_ALL))
+OBJS    = $(addprefix $(OUT)/obj/md_,$(addsuffix .o,$(MD_SRC))) \
+          $(OUT)/obj/mod.o $(OUT)/obj/promo.o $(OUT)/obj/rootdir.o $(OUT)/obj/finalqm.o
+
+# The library without empole.o / energy.o is what the drop-in shim links against.
+CORE_OBJS = $(filter-out $(OUT)/obj/md_empole.o $(OUT)/obj/md_energy.o,$(OBJS))
+
+all: $(OUT)/libpolmdqc.a $(OUT)/libpolmdqc_core.a $(OUT)/ref_dump $(OUT)/data.stamp
+
+$(OUT)/obj/md_%.o: $(REF)/src/md/%.cpp
+	@mkdir -p $(dir $@)
+	$(REFCXX) $(FLAGS) $(INC) -c $< -o $@
+
+$(OUT)/obj/mod.o: $(REF)/src/mod.cpp
+	@mkdir -p $(dir $@)
+	$(REFCXX) $(FLAGS) $(INC) -c $< -o $@
+$(OUT)/obj/promo.o: $(REF)/src/promo.cpp
+	@mkdir -p $(dir $@)
+	$(REFCXX) $(FLAGS) $(INC) -c $< -o $@
+$(OUT)/obj/rootdir.o: $(REF)/src/rootdir.cpp
+	@mkdir -p $(dir $@)
+	$(REFCXX) $(FLAGS) $(INC) -c $< -o $@
+$(OUT)/obj/finalqm.o: $(REF)/src/qc/finalqm.cpp
+	@mkdir -p $(dir $@)
+	$(REFCXX) $(FLAGS) $(INC) -c $< -o $@
+
+$(OUT)/libpolmdqc.a: $(OBJS)
+	rm -f $@ && ar rcs $@ $^
+
+$(OUT)/libpolmdqc_core.a: $(CORE_OBJS)
+	rm -f $@ && ar rcs $@ $^
+
+# ref_dump: our own driver (oracle/ref_dump.cpp) around the reference library;
+# runs initial/getcart/mechanic/energy and prints the globals as JSON.
+$(OUT)/ref_dump: oracle/ref_dump.cpp $(OUT)/libpolmdqc.a
+	$(REFCXX) $(FLAGS) $(INC) $< $(OUT)/libpolmdqc.a -o $@
+
+# Parameter files and test fixtures the reference's own tests read, copied next
+# to the build so that runs on another machine can find them.
+$(OUT)/data.stamp: $(wildcard $(REF)/params/*.prm)
+	@mkdir -p $(OUT)/params $(OUT)/testFiles
+	cp $(REF)/params/water03.prm $(REF)/params/amoebabio09.prm $(REF)/params/amoebabio18.prm $(OUT)/params/
+	cp -r $(REF)/test/testFiles/amoeba $(REF)/test/testFiles/bounds $(REF)/test/testFiles/rotpole $(OUT)/testFiles/
+	touch $@
+
+.PHONY: all

@@ -1,0 +1,212 @@
+"""Benchmark of the AMOEBA electrostatics path on B200.
+
+Metric: full AMOEBA electrostatic E+F evaluations per second (permanent
+multipoles + mutual induced dipoles to 1e-6 D RMS + polarization, real-space
+Ewald with Thole damping and smooth PME), mixed precision, on the seeded
+4,096-water box (12,288 atoms, 49.7 A, PME grid 54^3, order 5, alpha 0.5446,
+cutoff 7 A).  One step = one E+F evaluation.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Multi-GPU runs are independent replicas (one box per rank, seed = rank):
+value = evaluations of all ranks / max-over-ranks device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WATERS, BOX, GRID = 4096, 49.7, 54
+METRIC = "AMOEBA E+F evaluations/s (mixed precision, mutual polarization to 1e-6 D)"
+UNIT = "evals/s"
+FLUSH_BYTES = 256 << 20          # > 126 MB L2, written before every timed step
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+class Clocks:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(gpu), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait()
+        self.f.flush()
+        rows = [r.split(", ") for r in open(self.f.name).read().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        sm = [float(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]), "reasons": reasons,
+                "samples": len(rows)}
+
+
+def workload_config():
+    return {"workload": f"{WATERS}-water AMOEBA box (water03), {3 * WATERS} atoms, {BOX} A, PME {GRID}^3 order 5, "
+                        "alpha 0.5446, cutoff 7 A, mutual polarization 1e-6 D",
+            "atoms": 3 * WATERS, "pme_grid": [GRID] * 3, "cutoff_A": 7.0, "poleps_D": 1e-6,
+            "precision": "mixed (FP32 pairs/grids, FP64 PCG reductions, accumulators, correction sweep)",
+            "l2": f"flushed before every timed step ({FLUSH_BYTES >> 20} MiB write)"}
+
+
+def cpu_baseline_oracle(seed=0):
+    """FP64 CPU restatement (OpenMP, all host cores) on one full evaluation of
+    the same box: a bounded sample of the workload."""
+    from oracle import oracle
+    from polmdqc_b200 import abi, systems
+    from polmdqc_b200.engine import Settings
+    s = systems.water_box(WATERS, BOX, seed=seed)
+    st = Settings(nfft=(GRID,) * 3, precision=abi.PREC_FP64)
+    oracle.forward(systems.water_box(27, 9.32, seed=1), Settings(nfft=(16,) * 3, cutoff=4.6))  # load + warm
+    t = time.perf_counter()
+    oracle.forward(s, st, flags=abi.DO_ENERGY | abi.DO_GRADIENT)
+    dt = time.perf_counter() - t
+    return {"value": 1.0 / dt, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+            "sample": f"1 full E+F evaluation of the {WATERS}-water box, FP64, OpenMP on {os.cpu_count()} threads "
+                      f"({dt:.2f} s)"}
+
+
+def run_reference(args):
+    """CPU reference arm: the oracle port of the full path (the reference
+    itself implements only non-Ewald multipoles, src/md/empole.cpp:53-64)."""
+    rank = int(os.environ.get("RANK", 0))
+    if rank != 0:
+        return 0
+    steps = max(1, min(args.steps, 2))
+    vals = []
+    base = None
+    for k in range(steps):
+        base = cpu_baseline_oracle(seed=k)
+        vals.append(base["value"])
+    v = statistics.mean(vals)
+    base["value"] = v
+    base["sample"] += f"; {steps} step(s) (steps capped at 2 to bound the run)"
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
+            "warmup": 0, "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded water box)", "config": workload_config(),
+            "cpu_baseline": base, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    from polmdqc_b200 import abi, systems
+    from polmdqc_b200.engine import Engine, Settings
+
+    rank, world = int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    s = systems.water_box(WATERS, BOX, seed=rank)
+    st = Settings(nfft=(GRID,) * 3, precision=abi.PREC_MIXED, device=local)
+    eng = Engine(s, st)
+    flags = abi.DO_ENERGY | abi.DO_GRADIENT
+    eng.bench(max(args.warmup, 3), flags, FLUSH_BYTES)           # warm-up (untimed)
+    barrier()
+    clocks = Clocks(local) if rank == 0 else None
+    ms, launches = eng.bench(args.steps, flags, FLUSH_BYTES)      # timed: device-resident
+    barrier()
+    clk = clocks.stop() if clocks else None
+    dev_s = max_over_ranks(float(np.sum(ms)) / 1000.0)
+    value = world * args.steps / dev_s
+
+    # end to end through the C ABI: host coordinates (pinned) in, gradients out
+    n = s.n
+    xyz = torch.from_numpy(s.xyz.reshape(-1).copy()).pin_memory().numpy()
+    dem = torch.zeros(3 * n, dtype=torch.float64).pin_memory().numpy()
+    dep = torch.zeros(3 * n, dtype=torch.float64).pin_memory().numpy()
+    for _ in range(2):
+        eng.set_coords(xyz)
+        eng.forward_into(flags, dem, dep)
+    barrier()
+    t0 = time.perf_counter()
+    iters = []
+    for _ in range(args.steps):
+        eng.set_coords(xyz)
+        em, ep, it, eps = eng.forward_into(flags, dem, dep)
+        iters.append(it)
+    barrier()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e = {"value": world * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 8 * 3 * n + 8 * 6,
+           "d2h_bytes_per_step": 8 * 2 * 3 * n + 8 * (8 + 8 + 4) + 4 * 2}
+
+    if rank == 0:
+        peaks, src = load_peaks()
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1000.0 * dev_s / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64 (mixed)", "data": "synthetic (seeded water box)",
+                "config": workload_config(), "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+                "pcg_iterations": int(statistics.median(iters)), "em": em, "ep": ep,
+                "ns_per_day": {"dt_1fs": value * 86400 * 1e-6, "dt_2fs": value * 86400 * 2e-6},
+                "peaks_source": src}
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline_oracle(seed=0)
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

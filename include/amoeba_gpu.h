@@ -179,8 +179,23 @@ int amg_forward(amg_ctx* ctx, int32_t flags, amg_results* res);
 int amg_backward(amg_ctx* ctx, const amg_cotangents* cot, amg_param_grads* grads);
 
 /* Timing of the last amg_forward on the device (ms) by phase: 0 total,
- * 1 setup (rotation, sort, lists), 2 permanent field, 3 PCG, 4 forces. */
+ * 1 setup (rotation, sort, lists), 2 permanent field, 3 PCG, 4 forces
+ * (zeros when the evaluation ran as one captured graph). */
 int amg_last_timing(amg_ctx* ctx, double ms[5]);
+
+/* Benchmark support (no counterpart in the reference): runs `steps`
+ * evaluations with the coordinates already on the device and the results
+ * left there, writing `flush_bytes` to a scratch buffer before each one
+ * (L2 eviction, not timed), and returns each evaluation's device time in
+ * ms_steps[steps] (CUDA events on the context's stream) and the number of
+ * this library's kernel launches in *launches.  Runs one untimed
+ * evaluation first. */
+int amg_bench(amg_ctx* ctx, int32_t flags, int32_t steps, int64_t flush_bytes, double* ms_steps,
+              int64_t* launches);
+
+/* Kernel launches of the last amg_forward, whether it ran as one captured
+ * CUDA graph, and the lanes per site of the pair kernels. */
+int amg_last_stats(amg_ctx* ctx, int64_t* launches, int32_t* graphed, int32_t* lanes_per_site);
 
 const char* amg_last_error(amg_ctx* ctx);
 int amg_abi_version(void);

@@ -1,0 +1,1312 @@
+// amg_api.cu -- host side of libamoeba_gpu.so: the C ABI of
+// include/amoeba_gpu.h, device buffers, cuFFT plans and the evaluation
+// pipeline (frames -> lists -> permanent field -> PCG -> energies/forces).
+//
+// One context = one device, one stream.  Everything between amg_set_coords
+// and the result copy stays on the device; the PCG convergence test reads
+// two FP64 scalars per iteration.
+#include "../../include/amoeba_gpu.h"
+#include "kernels_setup.cuh"
+#include "kernels_pme.cuh"
+#include "kernels_pair.cuh"
+#include "kernels_misc.cuh"
+
+#include <cub/device/device_radix_sort.cuh>
+#include <cufft.h>
+
+#include <algorithm>
+#include <initializer_list>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace amg;
+
+namespace {
+
+constexpr int kOrder = 5;  // B-spline order compiled in (pme.h bseorder default)
+constexpr int kThreads = 128;
+
+inline unsigned nblk(size_t n, int t = kThreads) { return (unsigned)((n + t - 1) / t); }
+
+// lanes per site of the bulk pair kernels (runtime choice among compiled 8/16/32)
+#define LPA_DISPATCH(lpa, ...)                      \
+    do {                                            \
+        if ((lpa) == 32) {                          \
+            constexpr int L = 32;                   \
+            __VA_ARGS__                             \
+        } else if ((lpa) == 16) {                   \
+            constexpr int L = 16;                   \
+            __VA_ARGS__                             \
+        } else {                                    \
+            constexpr int L = 8;                    \
+            __VA_ARGS__                             \
+        }                                           \
+    } while (0)
+
+template <class R>
+struct CufftTypes;
+template <>
+struct CufftTypes<float> {
+    static constexpr cufftType r2c = CUFFT_R2C, c2r = CUFFT_C2R;
+    static cufftResult fwd(cufftHandle p, float* i, cufftComplex* o) { return cufftExecR2C(p, i, o); }
+    static cufftResult inv(cufftHandle p, cufftComplex* i, float* o) { return cufftExecC2R(p, i, o); }
+    using C = cufftComplex;
+};
+template <>
+struct CufftTypes<double> {
+    static constexpr cufftType r2c = CUFFT_D2Z, c2r = CUFFT_Z2D;
+    static cufftResult fwd(cufftHandle p, double* i, cufftDoubleComplex* o) { return cufftExecD2Z(p, i, o); }
+    static cufftResult inv(cufftHandle p, cufftDoubleComplex* i, double* o) { return cufftExecZ2D(p, i, o); }
+    using C = cufftDoubleComplex;
+};
+
+template <class R>
+struct Pme {
+    bool ready = false;
+    R* grid = nullptr;                       // [2][K1 K2 K3]
+    typename CufftTypes<R>::C* cgrid = nullptr;  // [2][K1 K2 (K3/2+1)]
+    R* infl = nullptr;                       // [K1 K2 (K3/2+1)]
+    R* theta = nullptr;                      // [n][3][4][P]
+    int* k0 = nullptr;                       // [n][3]
+    cufftHandle f1 = 0, i1 = 0, f2 = 0, i2 = 0;
+    double infl_box[3] = {0, 0, 0};
+    size_t G = 0, Gc = 0;
+};
+
+template <class R>
+struct Atoms {
+    AtomR<R>* at = nullptr;
+    R4<R>* u4 = nullptr;  // [2n]
+};
+
+}  // namespace
+
+struct amg_ctx {
+    // configuration
+    int n = 0, prec = AMG_PREC_MIXED, poltyp = AMG_POL_NONE, politer = 100, guess = 1, device = 0;
+    bool ewald = false, bounds = false, has_pol = false;
+    double aewald = 0, cut = 0, f = 0, debye = 4.80321, poleps = 1e-6;
+    int K[3] = {0, 0, 0}, order = kOrder;
+    std::string err;
+    double box[6] = {0, 0, 0, 90, 90, 90};
+    Box bx{};
+    bool have_coords = false;
+    int nsp = 0;
+    // device, persistent
+    double *pole13 = nullptr, *pol = nullptr, *thole = nullptr, *pdamp = nullptr, *xyz = nullptr, *rp10 = nullptr;
+    int *zax = nullptr, *xax = nullptr, *yax = nullptr, *axe = nullptr, *mol = nullptr;
+    ScaledPair* sp = nullptr;
+    int *xoff = nullptr, *xidx = nullptr;  // scaled partners of each atom (CSR)
+    Atoms<float> af;
+    Atoms<double> ad;
+    // cell list / neighbour list
+    unsigned *keys = nullptr, *skeys = nullptr;
+    int *ids = nullptr, *sids = nullptr, *cstart = nullptr, *cend = nullptr;
+    size_t ncell_alloc = 0;
+    char* cubtmp = nullptr;
+    size_t cubtmp_bytes = 0;
+    int* nbr = nullptr;
+    int* nnb = nullptr;
+    int cap = 0, lpa = 16;
+    int* overflow = nullptr;
+    double4* spos = nullptr;  // coordinates in cell order
+    // vectors
+    double *Ed = nullptr, *Ep = nullptr, *ud = nullptr, *up = nullptr, *rd = nullptr, *rp = nullptr, *zd = nullptr,
+           *zp = nullptr, *pd = nullptr, *pp = nullptr, *Apd = nullptr, *App = nullptr, *Fd = nullptr, *Fp = nullptr,
+           *resd = nullptr;
+    double *scal = nullptr, *eacc = nullptr;
+    unsigned long long* cnt = nullptr;
+    double *grad_m = nullptr, *grad_p = nullptr, *trq_m = nullptr, *trq_p = nullptr, *aem = nullptr,
+           *aep = nullptr;
+    double *phiM = nullptr, *phiU = nullptr, *phiU4 = nullptr;
+    Pme<float> pmf;
+    Pme<double> pmd;
+    cudaStream_t st = nullptr, st2 = nullptr;
+    cudaEvent_t ev[6] = {};
+    CellGrid cg{};
+    double cell_volume = 1.0;
+    int npolar = 0;
+    int *iter = nullptr, *cont = nullptr;
+    // captured evaluation (periodic systems)
+    bool use_graphs = true, graph_dirty = true, graphed_last = false;
+    cudaGraphExec_t gexec = nullptr;
+    int gflags = -1;
+    // kernel launches of this library: counter, and per captured graph the
+    // launches outside the PCG loop and per loop iteration
+    long long kcount = 0, kmain = 0, kbody = 0, klast = 0;
+    char* flushbuf = nullptr;
+    size_t flush_bytes = 0;
+    std::string graph_note;
+    double timing[5] = {0, 0, 0, 0, 0};
+    // last forward state for the adjoint
+    bool have_forward = false;
+};
+
+namespace {
+
+struct Fail {
+    int code;
+};
+
+#define CK(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) {                                                                   \
+            ctx->err = std::string(#call) + ": " + cudaGetErrorString(e_);                         \
+            throw Fail{AMG_ERR_CUDA};                                                              \
+        }                                                                                          \
+    } while (0)
+#define CKFFT(call)                                                                                \
+    do {                                                                                           \
+        cufftResult r_ = (call);                                                                   \
+        if (r_ != CUFFT_SUCCESS) {                                                                 \
+            ctx->err = std::string(#call) + ": cufft error " + std::to_string((int)r_);            \
+            throw Fail{AMG_ERR_CUDA};                                                              \
+        }                                                                                          \
+    } while (0)
+#define KCHECK()                 \
+    do {                         \
+        CK(cudaGetLastError());  \
+        ctx->kcount++;           \
+    } while (0)
+
+template <class T>
+void dalloc(amg_ctx* ctx, T*& p, size_t count) {
+    if (p) cudaFree(p);
+    p = nullptr;
+    if (count == 0) count = 1;
+    CK(cudaMalloc((void**)&p, sizeof(T) * count));
+}
+template <class T>
+void dfree(T*& p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+template <class T>
+void upload(amg_ctx* ctx, T*& d, const T* h, size_t count) {
+    dalloc(ctx, d, count);
+    if (h && count) CK(cudaMemcpy(d, h, sizeof(T) * count, cudaMemcpyHostToDevice));
+}
+
+// ------------------------------------------------------------ scaled pairs
+// The scaled-pair table: m-scales by 1-2..1-5 (applied in order, a later
+// list overwrites, as the reference's exclusion set-up at
+// src/md/empole.cpp:224-235); p-scales by 1-n with the intra-group value for
+// partners in the same polarization group; d- and u-scales by group
+// connectivity ip11..ip14 (polpot.h:18-45 meanings).
+std::vector<ScaledPair> build_scaled(const amg_params* P) {
+    struct S {
+        double m = 1, p = 1, d = 1, u = 1;
+    };
+    std::vector<ScaledPair> out;
+    const amg_list* bonded[4] = {&P->i12, &P->i13, &P->i14, &P->i15};
+    const amg_list* groups[4] = {&P->ip11, &P->ip12, &P->ip13, &P->ip14};
+    std::vector<int> touched;
+    std::vector<S> sc(P->n);
+    std::vector<char> mark(P->n, 0), ingrp(P->n, 0);
+    for (int i = 0; i < P->n; i++) {
+        touched.clear();
+        if (P->ip11.offsets)
+            for (int j = P->ip11.offsets[i]; j < P->ip11.offsets[i + 1]; j++) ingrp[P->ip11.indices[j]] = 1;
+        auto touch = [&](int k) {
+            if (!mark[k]) {
+                mark[k] = 1;
+                touched.push_back(k);
+                sc[k] = S{};
+            }
+        };
+        for (int b = 0; b < 4; b++) {
+            const amg_list& L = *bonded[b];
+            if (!L.offsets) continue;
+            for (int j = L.offsets[i]; j < L.offsets[i + 1]; j++) {
+                int k = L.indices[j];
+                if (k == i) continue;
+                touch(k);
+                sc[k].m = P->m_scale[b];
+                sc[k].p = ingrp[k] ? P->p_iscale[b] : P->p_scale[b];
+            }
+        }
+        if (P->polarity)
+            for (int g = 0; g < 4; g++) {
+                const amg_list& L = *groups[g];
+                if (!L.offsets) continue;
+                for (int j = L.offsets[i]; j < L.offsets[i + 1]; j++) {
+                    int k = L.indices[j];
+                    if (k == i) continue;
+                    touch(k);
+                    sc[k].d = P->d_scale[g];
+                    sc[k].u = P->u_scale[g];
+                }
+            }
+        for (int k : touched) {
+            mark[k] = 0;
+            if (k <= i) continue;
+            const S& s = sc[k];
+            if (s.m != 1 || s.p != 1 || s.d != 1 || s.u != 1) out.push_back(ScaledPair{i, k, s.m, s.p, s.d, s.u});
+        }
+        if (P->ip11.offsets)
+            for (int j = P->ip11.offsets[i]; j < P->ip11.offsets[i + 1]; j++) ingrp[P->ip11.indices[j]] = 0;
+    }
+    return out;
+}
+
+// ------------------------------------------------------------ PME set-up
+void bsmod_axis(int K, int p, std::vector<double>& out) {
+    // |sum_{k=0}^{p-2} M_p(k+1) e^{2 pi i m k / K}|^2, zeros (odd p at the
+    // Nyquist frequency) replaced by the mean of the neighbours
+    std::vector<double> Mp(p + 1, 0.0);
+    {
+        // cardinal B-spline values at integers 1..p-1 by the order recursion
+        std::vector<double> b(p + 1, 0.0), nb(p + 1, 0.0);
+        b[1] = 1.0;  // M_2(1) = 1 (values at x = 0..n)
+        int order = 2;
+        // M_n(x) at integer x: M_n(x) = (x M_{n-1}(x) + (n - x) M_{n-1}(x-1)) / (n-1)
+        while (order < p) {
+            order++;
+            std::fill(nb.begin(), nb.end(), 0.0);
+            for (int x = 1; x < order; x++) nb[x] = (x * b[x] + (order - x) * b[x - 1]) / (order - 1);
+            b = nb;
+        }
+        for (int x = 0; x <= p; x++) Mp[x] = b[x];
+    }
+    out.assign(K, 0.0);
+    for (int m = 0; m < K; m++) {
+        double re = 0, im = 0;
+        for (int k = 0; k <= p - 2; k++) {
+            double ang = 2 * kPi * m * k / K;
+            re += Mp[k + 1] * cos(ang);
+            im += Mp[k + 1] * sin(ang);
+        }
+        out[m] = re * re + im * im;
+    }
+    for (int m = 0; m < K; m++)
+        if (out[m] < 1e-7) out[m] = 0.5 * (out[(m - 1 + K) % K] + out[(m + 1) % K]);
+}
+
+template <class R>
+void pme_prepare(amg_ctx* ctx, Pme<R>& pm) {
+    const int K1 = ctx->K[0], K2 = ctx->K[1], K3 = ctx->K[2];
+    if (!pm.ready) {
+        pm.G = (size_t)K1 * K2 * K3;
+        pm.Gc = (size_t)K1 * K2 * (K3 / 2 + 1);
+        dalloc(ctx, pm.grid, 2 * pm.G);
+        dalloc(ctx, pm.cgrid, 2 * pm.Gc);
+        dalloc(ctx, pm.infl, pm.Gc);
+        dalloc(ctx, pm.theta, (size_t)ctx->n * 3 * 4 * kOrder);
+        dalloc(ctx, pm.k0, (size_t)ctx->n * 3);
+        int dims[3] = {K1, K2, K3};
+        CKFFT(cufftPlanMany(&pm.f1, 3, dims, nullptr, 1, 0, nullptr, 1, 0, CufftTypes<R>::r2c, 1));
+        CKFFT(cufftPlanMany(&pm.i1, 3, dims, nullptr, 1, 0, nullptr, 1, 0, CufftTypes<R>::c2r, 1));
+        CKFFT(cufftPlanMany(&pm.f2, 3, dims, nullptr, 1, 0, nullptr, 1, 0, CufftTypes<R>::r2c, 2));
+        CKFFT(cufftPlanMany(&pm.i2, 3, dims, nullptr, 1, 0, nullptr, 1, 0, CufftTypes<R>::c2r, 2));
+        cufftHandle hs[4] = {pm.f1, pm.i1, pm.f2, pm.i2};
+        for (int k = 0; k < 4; k++) CKFFT(cufftSetStream(hs[k], ctx->st));
+        pm.ready = true;
+    }
+    if (pm.infl_box[0] != ctx->box[0] || pm.infl_box[1] != ctx->box[1] || pm.infl_box[2] != ctx->box[2]) {
+        std::vector<double> b1, b2, b3;
+        bsmod_axis(K1, kOrder, b1);
+        bsmod_axis(K2, kOrder, b2);
+        bsmod_axis(K3, kOrder, b3);
+        const double L1 = ctx->box[0], L2 = ctx->box[1], L3 = ctx->box[2], V = L1 * L2 * L3;
+        const double pref = 1.0 / (kPi * V), a2 = ctx->aewald * ctx->aewald;
+        std::vector<R> h(pm.Gc);
+        const int K3h = K3 / 2 + 1;
+        for (int a = 0; a < K1; a++)
+            for (int b = 0; b < K2; b++)
+                for (int c = 0; c < K3h; c++) {
+                    size_t id = ((size_t)a * K2 + b) * K3h + c;
+                    if (a == 0 && b == 0 && c == 0) { h[id] = 0; continue; }
+                    int ma = a <= K1 / 2 ? a : a - K1, mb = b <= K2 / 2 ? b : b - K2, mc = c;
+                    double hx = ma / L1, hy = mb / L2, hz = mc / L3;
+                    double h2 = hx * hx + hy * hy + hz * hz;
+                    h[id] = (R)(pref * exp(-kPi * kPi * h2 / a2) / h2 / (b1[a] * b2[b] * b3[c]));
+                }
+        CK(cudaMemcpy(pm.infl, h.data(), sizeof(R) * pm.Gc, cudaMemcpyHostToDevice));
+        for (int a = 0; a < 3; a++) pm.infl_box[a] = ctx->box[a];
+    }
+}
+
+template <class R>
+void pme_destroy(Pme<R>& pm) {
+    cufftHandle* hs[4] = {&pm.f1, &pm.i1, &pm.f2, &pm.i2};
+    for (int k = 0; k < 4; k++)
+        if (*hs[k]) { cufftDestroy(*hs[k]); *hs[k] = 0; }
+    dfree(pm.grid); dfree(pm.cgrid); dfree(pm.infl); dfree(pm.theta); dfree(pm.k0);
+    pm.ready = false;
+}
+
+template <class R>
+Atoms<R>& atoms_of(amg_ctx* ctx);
+template <>
+Atoms<float>& atoms_of<float>(amg_ctx* ctx) { return ctx->af; }
+template <>
+Atoms<double>& atoms_of<double>(amg_ctx* ctx) { return ctx->ad; }
+template <class R>
+Pme<R>& pme_of(amg_ctx* ctx);
+template <>
+Pme<float>& pme_of<float>(amg_ctx* ctx) { return ctx->pmf; }
+template <>
+Pme<double>& pme_of<double>(amg_ctx* ctx) { return ctx->pmd; }
+
+// ------------------------------------------------------------ pipeline
+template <class R>
+void rotate_and_pack(amg_ctx* ctx, cudaStream_t s) {
+    Atoms<R>& A = atoms_of<R>(ctx);
+    k_rotate<R><<<nblk(ctx->n), kThreads, 0, s>>>(ctx->n, ctx->xyz, ctx->pole13, ctx->zax, ctx->xax, ctx->yax,
+                                                  ctx->axe, ctx->has_pol ? ctx->pdamp : nullptr,
+                                                  ctx->has_pol ? ctx->thole : nullptr,
+                                                  ctx->has_pol ? ctx->pol : nullptr, ctx->rp10, A.at);
+    KCHECK();
+}
+
+// Cell grid for the current box (periodic) or coordinate bounding box
+// (non-periodic), computed on the host when coordinates are set.
+void cell_grid(amg_ctx* ctx, const double* hxyz) {
+    CellGrid& cg = ctx->cg;
+    cg = CellGrid{};
+    cg.periodic = ctx->bounds;
+    double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    if (!ctx->bounds) {
+        for (int a = 0; a < 3; a++) { lo[a] = 1e300; hi[a] = -1e300; }
+        for (int i = 0; i < ctx->n; i++)
+            for (int a = 0; a < 3; a++) {
+                lo[a] = std::min(lo[a], hxyz[3 * i + a]);
+                hi[a] = std::max(hi[a], hxyz[3 * i + a]);
+            }
+    }
+    double vol = 1.0;
+    for (int a = 0; a < 3; a++) {
+        if (ctx->bounds) {
+            double L = ctx->box[a];
+            cg.nc[a] = std::max(1, (int)std::floor(L / ctx->cut));
+            cg.size[a] = L / cg.nc[a];
+            vol *= L;
+            if (cg.nc[a] >= 3) { cg.off_lo[a] = -1; cg.off_hi[a] = 1; }
+            else if (cg.nc[a] == 2) { cg.off_lo[a] = 0; cg.off_hi[a] = 1; }
+            else { cg.off_lo[a] = 0; cg.off_hi[a] = 0; }
+        } else {
+            double ext = hi[a] - lo[a] + 1e-6;
+            cg.nc[a] = std::max(1, std::min(128, (int)std::floor(ext / ctx->cut)));
+            cg.size[a] = ext / cg.nc[a];
+            cg.origin[a] = lo[a];
+            vol *= std::max(ext, 1.0);
+            cg.off_lo[a] = -1;
+            cg.off_hi[a] = 1;
+        }
+    }
+    ctx->cell_volume = vol;
+}
+
+void ensure_list_buffers(amg_ctx* ctx) {
+    const int n = ctx->n;
+    size_t ncell = (size_t)ctx->cg.nc[0] * ctx->cg.nc[1] * ctx->cg.nc[2];
+    if (ncell > ctx->ncell_alloc) {
+        dalloc(ctx, ctx->cstart, ncell);
+        dalloc(ctx, ctx->cend, ncell);
+        ctx->ncell_alloc = ncell;
+        ctx->graph_dirty = true;
+    }
+    if (!ctx->keys) {
+        dalloc(ctx, ctx->keys, n);
+        dalloc(ctx, ctx->skeys, n);
+        dalloc(ctx, ctx->ids, n);
+        dalloc(ctx, ctx->sids, n);
+        dalloc(ctx, ctx->nnb, n);
+        dalloc(ctx, ctx->overflow, 1);
+        dalloc(ctx, ctx->spos, n);
+        size_t bytes = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, bytes, ctx->keys, ctx->skeys, ctx->ids, ctx->sids, n);
+        dalloc(ctx, ctx->cubtmp, bytes);
+        ctx->cubtmp_bytes = bytes;
+    }
+    if (ctx->cap == 0) {
+        double rho = n / ctx->cell_volume;
+        double est = 4.0 / 3.0 * kPi * ctx->cut * ctx->cut * ctx->cut * rho;
+        int cap = (int)std::min<double>(n - 1, std::ceil(1.4 * est) + 64);
+        ctx->cap = std::max(cap, 1);
+        dalloc(ctx, ctx->nbr, (size_t)ctx->cap * n);
+        ctx->graph_dirty = true;
+    }
+}
+
+// cell binning (CUB radix sort on the cell key) and the exact lists; an
+// overflow of the per-atom capacity is flagged on the device and handled by
+// the caller after the evaluation (grow and evaluate again)
+void enqueue_lists(amg_ctx* ctx, cudaStream_t s) {
+    const int n = ctx->n;
+    const CellGrid& cg = ctx->cg;
+    size_t ncell = (size_t)cg.nc[0] * cg.nc[1] * cg.nc[2];
+    int nbits = 1;
+    while ((1ull << nbits) < ncell) nbits++;
+    k_zero<int><<<nblk(ncell, 256), 256, 0, s>>>(ctx->cstart, ncell);
+    KCHECK();
+    k_zero<int><<<nblk(ncell, 256), 256, 0, s>>>(ctx->cend, ncell);
+    KCHECK();
+    k_cell_index<<<nblk(n), kThreads, 0, s>>>(n, ctx->xyz, cg, ctx->bx, ctx->keys, ctx->ids);
+    KCHECK();
+    size_t bytes = ctx->cubtmp_bytes;
+    CK(cub::DeviceRadixSort::SortPairs(ctx->cubtmp, bytes, ctx->keys, ctx->skeys, ctx->ids, ctx->sids, n, 0, nbits, s));
+    k_cell_bounds<<<nblk(n), kThreads, 0, s>>>(n, ctx->skeys, ctx->sids, ctx->xyz, ctx->cstart, ctx->cend, ctx->spos);
+    KCHECK();
+    k_neighbors<<<nblk((size_t)n * 32), kThreads, 0, s>>>(n, ctx->spos, ctx->skeys, ctx->sids, ctx->cstart, ctx->cend,
+                                                          cg, ctx->bx, ctx->cut * ctx->cut, ctx->cap, ctx->xoff,
+                                                          ctx->xidx, ctx->nbr, ctx->nnb, ctx->overflow);
+    KCHECK();
+}
+
+template <class R>
+void pme_stencils(amg_ctx* ctx, cudaStream_t s) {
+    Pme<R>& pm = pme_of<R>(ctx);
+    k_bspline<R, kOrder><<<nblk(ctx->n), kThreads, 0, s>>>(ctx->n, ctx->xyz, ctx->bx,
+                                                           make_int3(ctx->K[0], ctx->K[1], ctx->K[2]), pm.theta, pm.k0);
+    KCHECK();
+}
+
+// reciprocal potential derivatives of the permanent multipoles -> phiM [n][20]
+template <class R>
+void pme_mpole(amg_ctx* ctx, cudaStream_t s) {
+    Pme<R>& pm = pme_of<R>(ctx);
+    int3 K = make_int3(ctx->K[0], ctx->K[1], ctx->K[2]);
+    double sc[3] = {ctx->K[0] / ctx->box[0], ctx->K[1] / ctx->box[1], ctx->K[2] / ctx->box[2]};
+    k_zero<R><<<nblk(pm.G, 256), 256, 0, s>>>(pm.grid, pm.G);
+    KCHECK();
+    k_spread_mpole<R, kOrder><<<nblk(ctx->n), kThreads, 0, s>>>(ctx->n, ctx->rp10, pm.theta, pm.k0, K, (R)sc[0],
+                                                                (R)sc[1], (R)sc[2], pm.grid);
+    KCHECK();
+    CKFFT(cufftSetStream(pm.f1, s));
+    CKFFT(cufftSetStream(pm.i1, s));
+    CKFFT(CufftTypes<R>::fwd(pm.f1, pm.grid, pm.cgrid));
+    k_convolve<R><<<nblk(pm.Gc, 256), 256, 0, s>>>(pm.Gc, 1, pm.infl, (typename Cplx<R>::type*)pm.cgrid);
+    KCHECK();
+    CKFFT(CufftTypes<R>::inv(pm.i1, pm.cgrid, pm.grid));
+    k_gather<R, kOrder, 20><<<nblk(ctx->n), kThreads, 0, s>>>(ctx->n, pm.grid, pm.theta, pm.k0, K, sc[0], sc[1], sc[2],
+                                                              ctx->phiM);
+    KCHECK();
+}
+
+// reciprocal potentials of two dipole sets -> phi [2][n][NC]
+template <class R, int NC>
+void pme_dipoles(amg_ctx* ctx, cudaStream_t s, const double* vd, const double* vp, double* phi) {
+    Pme<R>& pm = pme_of<R>(ctx);
+    int3 K = make_int3(ctx->K[0], ctx->K[1], ctx->K[2]);
+    double sc[3] = {ctx->K[0] / ctx->box[0], ctx->K[1] / ctx->box[1], ctx->K[2] / ctx->box[2]};
+    k_zero<R><<<nblk(2 * pm.G, 256), 256, 0, s>>>(pm.grid, 2 * pm.G);
+    KCHECK();
+    k_spread_dipoles<R, kOrder><<<nblk(ctx->n), kThreads, 0, s>>>(ctx->n, vd, vp, pm.theta, pm.k0, K, (R)sc[0],
+                                                                  (R)sc[1], (R)sc[2], pm.grid, pm.G);
+    KCHECK();
+    CKFFT(cufftSetStream(pm.f2, s));
+    CKFFT(cufftSetStream(pm.i2, s));
+    CKFFT(CufftTypes<R>::fwd(pm.f2, pm.grid, pm.cgrid));
+    k_convolve<R><<<nblk(pm.Gc, 256), 256, 0, s>>>(pm.Gc, 2, pm.infl, (typename Cplx<R>::type*)pm.cgrid);
+    KCHECK();
+    CKFFT(CufftTypes<R>::inv(pm.i2, pm.cgrid, pm.grid));
+    for (int b = 0; b < 2; b++) {
+        k_gather<R, kOrder, NC><<<nblk(ctx->n), kThreads, 0, s>>>(ctx->n, pm.grid + b * pm.G, pm.theta, pm.k0, K, sc[0],
+                                                                  sc[1], sc[2], phi + (size_t)b * NC * ctx->n);
+        KCHECK();
+    }
+}
+
+double ewald_alpha(const amg_ctx* ctx) { return ctx->ewald ? ctx->aewald : 0.0; }
+
+double self_coef(const amg_ctx* ctx) {
+    double a = ctx->aewald;
+    return ctx->ewald ? 4.0 * a * a * a / (3.0 * kSqrtPi) : 0.0;
+}
+
+// A v for both dipole sets (v/alpha - field of v)
+template <class R>
+void matvec(amg_ctx* ctx, cudaStream_t s, const double* vd, const double* vp, double* Ad, double* Ap) {
+    const int n = ctx->n;
+    Atoms<R>& A = atoms_of<R>(ctx);
+    k_pack_u<R><<<nblk(n), kThreads, 0, s>>>(n, vd, vp, A.u4);
+    KCHECK();
+    LPA_DISPATCH(ctx->lpa, {
+        if (ctx->ewald)
+            k_Tu<R, true, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(n, A.at, A.u4, ctx->bx, (R)ctx->aewald, ctx->nbr,
+                                                                      ctx->cap, ctx->nnb, ctx->Fd, ctx->Fp);
+        else
+            k_Tu<R, false, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(n, A.at, A.u4, ctx->bx, (R)0, ctx->nbr, ctx->cap,
+                                                                       ctx->nnb, ctx->Fd, ctx->Fp);
+    });
+    KCHECK();
+    if (ctx->nsp) {
+        k_scaled_Tu<<<nblk(ctx->nsp), kThreads, 0, s>>>(ctx->nsp, ctx->sp, ctx->xyz, ctx->pdamp, ctx->thole, ctx->bx,
+                                                       ctx->cut * ctx->cut, ewald_alpha(ctx), vd, vp, ctx->Fd, ctx->Fp);
+        KCHECK();
+    }
+    if (ctx->ewald) pme_dipoles<R, 4>(ctx, s, vd, vp, ctx->phiU4);
+    k_matvec_finish<<<nblk(n), kThreads, 0, s>>>(n, vd, vp, ctx->Fd, ctx->Fp, ctx->phiU4, ctx->ewald, self_coef(ctx),
+                                                 ctx->pol, Ad, Ap);
+    KCHECK();
+}
+
+bool iterative(const amg_ctx* ctx) { return ctx->has_pol && ctx->poltyp == AMG_POL_MUTUAL && ctx->npolar > 0; }
+
+double pcg_threshold(const amg_ctx* ctx) {
+    double t = ctx->poleps / ctx->debye;
+    return t * t * ctx->npolar;
+}
+
+// set-up of the solve: r = E - A u0, z = p = alpha r, and the first control
+// decision (continue while rr > threshold and iterations < politer)
+template <class R>
+void enqueue_pcg_init(amg_ctx* ctx, cudaStream_t s, cudaGraphConditionalHandle h, int use_handle) {
+    const int n = ctx->n;
+    if (!ctx->guess) {
+        k_zero<double><<<nblk(3 * n, 256), 256, 0, s>>>(ctx->ud, 3 * (size_t)n);
+        KCHECK();
+        k_zero<double><<<nblk(3 * n, 256), 256, 0, s>>>(ctx->up, 3 * (size_t)n);
+        KCHECK();
+    }
+    k_zero<double><<<1, 32, 0, s>>>(ctx->scal, NSCAL);
+    KCHECK();
+    matvec<R>(ctx, s, ctx->ud, ctx->up, ctx->Apd, ctx->App);
+    k_pcg_init<<<nblk(n), kThreads, 0, s>>>(n, ctx->Ed, ctx->Ep, ctx->Apd, ctx->App, ctx->pol, ctx->rd, ctx->rp, ctx->zd,
+                                            ctx->zp, ctx->pd, ctx->pp, ctx->scal);
+    KCHECK();
+    k_pcg_control<<<1, 1, 0, s>>>(ctx->scal, ctx->iter, pcg_threshold(ctx), ctx->politer, 1, h, use_handle, ctx->cont);
+    KCHECK();
+}
+
+// one PCG iteration (both right-hand sides), ending with the control kernel
+template <class R>
+void enqueue_pcg_iter(amg_ctx* ctx, cudaStream_t s, cudaGraphConditionalHandle h, int use_handle) {
+    const int n = ctx->n, n3 = 3 * n;
+    k_zero<double><<<1, 32, 0, s>>>(ctx->scal + PAP_D, 6);
+    KCHECK();
+    matvec<R>(ctx, s, ctx->pd, ctx->pp, ctx->Apd, ctx->App);
+    k_dot2<<<nblk(n3, 256), 256, 0, s>>>(n3, ctx->pd, ctx->Apd, ctx->pp, ctx->App, ctx->scal + PAP_D, ctx->scal + PAP_P);
+    KCHECK();
+    k_pcg_update<<<nblk(n), kThreads, 0, s>>>(n, ctx->pol, ctx->pd, ctx->pp, ctx->Apd, ctx->App, ctx->ud, ctx->up,
+                                              ctx->rd, ctx->rp, ctx->zd, ctx->zp, ctx->scal);
+    KCHECK();
+    k_pcg_dir<<<nblk(n3, 256), 256, 0, s>>>(n3, ctx->zd, ctx->zp, ctx->pd, ctx->pp, ctx->scal);
+    KCHECK();
+    k_pcg_control<<<1, 1, 0, s>>>(ctx->scal, ctx->iter, pcg_threshold(ctx), ctx->politer, 0, h, use_handle, ctx->cont);
+    KCHECK();
+}
+
+// FP64 correction sweep: the true residual with every term in FP64, one
+// diagonal-preconditioned step u += alpha r, and the residual norms
+void enqueue_sweep(amg_ctx* ctx, cudaStream_t s) {
+    matvec<double>(ctx, s, ctx->ud, ctx->up, ctx->Apd, ctx->App);
+    k_zero<double><<<1, 32, 0, s>>>(ctx->scal + PAP_D, 6);
+    KCHECK();
+    k_correct<<<nblk(ctx->n), kThreads, 0, s>>>(ctx->n, ctx->Ed, ctx->Ep, ctx->Apd, ctx->App, ctx->pol, ctx->ud, ctx->up,
+                                                ctx->resd, ctx->scal);
+    KCHECK();
+}
+
+// everything before the PCG loop: frames, lists, stencils, permanent field,
+// direct dipoles
+template <class R>
+void enqueue_front(amg_ctx* ctx, cudaStream_t s) {
+    const int n = ctx->n;
+    const bool mixed = ctx->prec == AMG_PREC_MIXED;
+    CK(cudaEventRecord(ctx->ev[0], s));
+    rotate_and_pack<R>(ctx, s);
+    if (mixed && iterative(ctx)) rotate_and_pack<double>(ctx, s);
+    enqueue_lists(ctx, s);
+    if (ctx->ewald) {
+        pme_stencils<R>(ctx, s);
+        if (mixed && iterative(ctx)) pme_stencils<double>(ctx, s);
+    }
+    k_zero<double><<<1, 32, 0, s>>>(ctx->eacc, 8);
+    KCHECK();
+    k_zero<unsigned long long><<<1, 32, 0, s>>>(ctx->cnt, 4);
+    KCHECK();
+    CK(cudaEventRecord(ctx->ev[1], s));
+    Atoms<R>& A = atoms_of<R>(ctx);
+    const R aew = (R)ctx->aewald;
+    if (ctx->has_pol) {
+        LPA_DISPATCH(ctx->lpa, {
+            if (ctx->ewald)
+                k_perm_field<R, true, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(n, A.at, ctx->bx, aew, ctx->nbr, ctx->cap,
+                                                                                  ctx->nnb, ctx->Ed, ctx->Ep);
+            else
+                k_perm_field<R, false, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(n, A.at, ctx->bx, aew, ctx->nbr,
+                                                                                   ctx->cap, ctx->nnb, ctx->Ed, ctx->Ep);
+        });
+        KCHECK();
+        if (ctx->nsp) {
+            k_scaled_field<<<nblk(ctx->nsp), kThreads, 0, s>>>(ctx->nsp, ctx->sp, ctx->xyz, ctx->rp10, ctx->pdamp,
+                                                              ctx->thole, ctx->bx, ctx->cut * ctx->cut, ewald_alpha(ctx),
+                                                              ctx->Ed, ctx->Ep);
+            KCHECK();
+        }
+    }
+    if (ctx->ewald) pme_mpole<R>(ctx, s);
+    if (ctx->has_pol) {
+        k_field_finish<<<nblk(n), kThreads, 0, s>>>(n, ctx->phiM, ctx->ewald, ctx->rp10, self_coef(ctx), ctx->pol, ctx->Ed,
+                                                    ctx->Ep, ctx->ud, ctx->up);
+        KCHECK();
+    }
+    CK(cudaEventRecord(ctx->ev[2], s));
+}
+
+// everything after the solve: energies, gradients, torques
+template <class R>
+void enqueue_back(amg_ctx* ctx, cudaStream_t s, int flags) {
+    const int n = ctx->n;
+    const bool grad = flags & AMG_DO_GRADIENT;
+    const bool analysis = flags & AMG_DO_ANALYSIS;
+    const double cut2 = ctx->cut * ctx->cut;
+    Atoms<R>& A = atoms_of<R>(ctx);
+    const R aew = (R)ctx->aewald;
+    CK(cudaEventRecord(ctx->ev[3], s));
+    k_zero<double><<<nblk(3 * n, 256), 256, 0, s>>>(ctx->grad_m, 3 * (size_t)n);
+    KCHECK();
+    k_zero<double><<<nblk(3 * n, 256), 256, 0, s>>>(ctx->trq_m, 3 * (size_t)n);
+    KCHECK();
+    k_zero<double><<<nblk(n, 256), 256, 0, s>>>(ctx->aem, (size_t)n);
+    KCHECK();
+    const int* mol = ctx->mol;
+    LPA_DISPATCH(ctx->lpa, {
+        const size_t nb = nblk((size_t)n * L);
+        if (ctx->ewald) {
+            if (analysis)
+                k_mpole_pair<R, true, true, L><<<nb, kThreads, 0, s>>>(n, A.at, ctx->bx, aew, ctx->nbr, ctx->cap, ctx->nnb,
+                                                                       ctx->f, ctx->grad_m, ctx->trq_m, ctx->eacc,
+                                                                       ctx->aem, mol, ctx->cnt);
+            else
+                k_mpole_pair<R, true, false, L><<<nb, kThreads, 0, s>>>(n, A.at, ctx->bx, aew, ctx->nbr, ctx->cap,
+                                                                        ctx->nnb, ctx->f, ctx->grad_m, ctx->trq_m,
+                                                                        ctx->eacc, nullptr, nullptr, nullptr);
+        } else {
+            if (analysis)
+                k_mpole_pair<R, false, true, L><<<nb, kThreads, 0, s>>>(n, A.at, ctx->bx, aew, ctx->nbr, ctx->cap,
+                                                                        ctx->nnb, ctx->f, ctx->grad_m, ctx->trq_m,
+                                                                        ctx->eacc, ctx->aem, mol, ctx->cnt);
+            else
+                k_mpole_pair<R, false, false, L><<<nb, kThreads, 0, s>>>(n, A.at, ctx->bx, aew, ctx->nbr, ctx->cap,
+                                                                         ctx->nnb, ctx->f, ctx->grad_m, ctx->trq_m,
+                                                                         ctx->eacc, nullptr, nullptr, nullptr);
+        }
+    });
+    KCHECK();
+    if (ctx->nsp) {
+        k_scaled_mpole<<<nblk(ctx->nsp), kThreads, 0, s>>>(ctx->nsp, ctx->sp, ctx->xyz, ctx->rp10, ctx->bx, cut2,
+                                                          ewald_alpha(ctx), ctx->f, ctx->grad_m, ctx->trq_m, ctx->eacc,
+                                                          analysis ? ctx->aem : nullptr, analysis ? mol : nullptr,
+                                                          analysis ? ctx->cnt : nullptr);
+        KCHECK();
+    }
+    if (ctx->ewald) {
+        k_recip_mpole<<<nblk(n), kThreads, 0, s>>>(n, ctx->rp10, ctx->phiM, ctx->f, ctx->aewald, ctx->grad_m, ctx->trq_m,
+                                                   ctx->eacc + 2, analysis ? ctx->aem : nullptr, ctx->eacc + 3);
+        KCHECK();
+    }
+    if (ctx->has_pol) {
+        k_polar_energy<<<nblk(n), kThreads, 0, s>>>(n, ctx->ud, ctx->Ep, ctx->f, ctx->eacc + 4,
+                                                    analysis ? ctx->aep : nullptr, ctx->cnt + 1);
+        KCHECK();
+    }
+    if (grad && ctx->has_pol) {
+        k_zero<double><<<nblk(3 * n, 256), 256, 0, s>>>(ctx->grad_p, 3 * (size_t)n);
+        KCHECK();
+        k_zero<double><<<nblk(3 * n, 256), 256, 0, s>>>(ctx->trq_p, 3 * (size_t)n);
+        KCHECK();
+        int mutual = ctx->poltyp == AMG_POL_MUTUAL;
+        k_pack_u<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->ud, ctx->up, A.u4);
+        KCHECK();
+        LPA_DISPATCH(ctx->lpa, {
+            if (ctx->ewald)
+                k_polar_pair<R, true, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(n, A.at, A.u4, ctx->bx, aew, ctx->nbr,
+                                                                                  ctx->cap, ctx->nnb, mutual, ctx->f,
+                                                                                  ctx->grad_p, ctx->trq_p);
+            else
+                k_polar_pair<R, false, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(n, A.at, A.u4, ctx->bx, aew, ctx->nbr,
+                                                                                   ctx->cap, ctx->nnb, mutual, ctx->f,
+                                                                                   ctx->grad_p, ctx->trq_p);
+        });
+        KCHECK();
+        if (ctx->nsp) {
+            k_scaled_polar<<<nblk(ctx->nsp), kThreads, 0, s>>>(ctx->nsp, ctx->sp, ctx->xyz, ctx->rp10, ctx->pdamp,
+                                                              ctx->thole, ctx->bx, cut2, ewald_alpha(ctx), ctx->ud,
+                                                              ctx->up, mutual, ctx->f, ctx->grad_p, ctx->trq_p);
+            KCHECK();
+        }
+        if (ctx->ewald) {
+            pme_dipoles<R, 20>(ctx, s, ctx->ud, ctx->up, ctx->phiU);
+            k_recip_polar<<<nblk(n), kThreads, 0, s>>>(n, ctx->rp10, ctx->phiM, ctx->phiU, ctx->phiU + 20 * (size_t)n,
+                                                       ctx->ud, ctx->up, mutual, self_coef(ctx), ctx->f, ctx->grad_p,
+                                                       ctx->trq_p);
+            KCHECK();
+        }
+        k_torque<<<nblk(n), kThreads, 0, s>>>(n, ctx->xyz, ctx->zax, ctx->xax, ctx->yax, ctx->axe, ctx->trq_p,
+                                              ctx->grad_p);
+        KCHECK();
+    }
+    if (grad) {
+        k_torque<<<nblk(n), kThreads, 0, s>>>(n, ctx->xyz, ctx->zax, ctx->xax, ctx->yax, ctx->axe, ctx->trq_m,
+                                              ctx->grad_m);
+        KCHECK();
+    }
+    CK(cudaEventRecord(ctx->ev[4], s));
+}
+
+// Captures the whole evaluation as one CUDA graph: the PCG loop is a
+// conditional WHILE node whose body is one iteration; its last kernel sets
+// the condition from the FP64 residual norms on the device.
+template <class R>
+bool capture_graph(amg_ctx* ctx, int flags) {
+    cudaStream_t s = ctx->st;
+    cudaGraph_t graph = nullptr;
+    auto fail = [&](const char* what, cudaError_t e) {
+        ctx->graph_note = std::string(what) + ": " + cudaGetErrorString(e);
+        cudaStreamCaptureStatus st;
+        if (cudaStreamIsCapturing(s, &st) == cudaSuccess && st != cudaStreamCaptureStatusNone) {
+            cudaGraph_t g2;
+            cudaStreamEndCapture(s, &g2);
+            if (g2) cudaGraphDestroy(g2);
+        }
+        cudaGetLastError();
+        return false;
+    };
+    cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return fail("begin capture", e);
+    const long long k0 = ctx->kcount;
+    long long kb = 0;
+    try {
+        enqueue_front<R>(ctx, s);
+        if (iterative(ctx)) {
+            const cudaGraphNode_t* deps = nullptr;
+            size_t ndeps = 0;
+            cudaStreamCaptureStatus cs;
+            e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &graph, &deps, &ndeps);
+            if (e != cudaSuccess) return fail("capture info", e);
+            cudaGraphConditionalHandle h;
+            e = cudaGraphConditionalHandleCreate(&h, graph, 0, 0);
+            if (e != cudaSuccess) return fail("conditional handle", e);
+            enqueue_pcg_init<R>(ctx, s, h, 1);
+            e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &graph, &deps, &ndeps);
+            if (e != cudaSuccess) return fail("capture info", e);
+            cudaGraphNodeParams cp = {};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = h;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            cudaGraphNode_t cnode;
+            e = cudaGraphAddNode(&cnode, graph, deps, ndeps, &cp);
+            if (e != cudaSuccess) return fail("add conditional node", e);
+            cudaGraph_t body = cp.conditional.phGraph_out[0];
+            e = cudaStreamUpdateCaptureDependencies(s, &cnode, 1, cudaStreamSetCaptureDependencies);
+            if (e != cudaSuccess) return fail("update dependencies", e);
+            e = cudaStreamBeginCaptureToGraph(ctx->st2, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+            if (e != cudaSuccess) return fail("body capture", e);
+            const long long kb0 = ctx->kcount;
+            enqueue_pcg_iter<R>(ctx, ctx->st2, h, 1);
+            kb = ctx->kcount - kb0;
+            e = cudaStreamEndCapture(ctx->st2, &body);
+            if (e != cudaSuccess) return fail("end body capture", e);
+            enqueue_sweep(ctx, s);
+        }
+        enqueue_back<R>(ctx, s, flags);
+    } catch (Fail&) {
+        return fail("enqueue", cudaGetLastError());
+    }
+    e = cudaStreamEndCapture(s, &graph);
+    if (e != cudaSuccess) return fail("end capture", e);
+    if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+    ctx->gexec = nullptr;
+    e = cudaGraphInstantiate(&ctx->gexec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        ctx->gexec = nullptr;
+        return fail("instantiate", e);
+    }
+    ctx->gflags = flags;
+    ctx->graph_dirty = false;
+    ctx->kbody = kb;
+    ctx->kmain = ctx->kcount - k0 - kb;
+    ctx->kcount = k0;
+    return true;
+}
+
+template <class R>
+void enqueue_eager(amg_ctx* ctx, int flags) {
+    cudaStream_t s = ctx->st;
+    enqueue_front<R>(ctx, s);
+    if (iterative(ctx)) {
+        enqueue_pcg_init<R>(ctx, s, 0, 0);
+        int cont = 1;
+        while (true) {
+            CK(cudaMemcpyAsync(&cont, ctx->cont, sizeof(int), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            if (!cont) break;
+            enqueue_pcg_iter<R>(ctx, s, 0, 0);
+        }
+        enqueue_sweep(ctx, s);
+    }
+    enqueue_back<R>(ctx, s, flags);
+}
+
+template <class R>
+int forward_impl(amg_ctx* ctx, int flags, amg_results* res) {
+    const int n = ctx->n;
+    const bool grad = flags & AMG_DO_GRADIENT;
+    const bool analysis = flags & AMG_DO_ANALYSIS;
+    cudaStream_t st = ctx->st;
+    for (int attempt = 0; attempt < 2; attempt++) {
+        ensure_list_buffers(ctx);
+        if (ctx->ewald) {
+            pme_prepare<R>(ctx, pme_of<R>(ctx));
+            if (ctx->prec == AMG_PREC_MIXED && iterative(ctx)) pme_prepare<double>(ctx, pme_of<double>(ctx));
+        }
+        bool graphed = false;
+        const long long kstart = ctx->kcount;
+        if (ctx->use_graphs && ctx->bounds) {
+            if (ctx->graph_dirty || !ctx->gexec || ctx->gflags != flags) capture_graph<R>(ctx, flags);
+            if (ctx->gexec) {
+                CK(cudaGraphLaunch(ctx->gexec, st));
+                graphed = true;
+            }
+        }
+        if (!graphed) enqueue_eager<R>(ctx, flags);
+        ctx->klast = graphed ? -1 : ctx->kcount - kstart;  // graph: completed below from the iteration count
+        int over = 0;
+        CK(cudaMemcpyAsync(&over, ctx->overflow, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (over <= ctx->cap) break;
+        if (attempt == 1) {
+            ctx->err = "neighbour list overflow";
+            return AMG_ERR_CUDA;
+        }
+        ctx->cap = ((over * 5 / 4) + 31) / 32 * 32;
+        dalloc(ctx, ctx->nbr, (size_t)ctx->cap * n);
+        ctx->graph_dirty = true;
+    }
+    ctx->graphed_last = ctx->use_graphs && ctx->bounds && ctx->gexec != nullptr;
+    // ---- results
+    double e[8], hs[NSCAL];
+    unsigned long long c[4];
+    int iters = 0;
+    CK(cudaMemcpyAsync(e, ctx->eacc, sizeof(e), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(c, ctx->cnt, sizeof(c), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(hs, ctx->scal, sizeof(hs), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&iters, ctx->iter, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    double eps = 0;
+    int status = AMG_OK;
+    if (ctx->klast < 0) ctx->klast = ctx->kmain + (long long)iters * ctx->kbody;
+    if (iterative(ctx)) {
+        eps = ctx->debye * std::sqrt(std::max(hs[RR_D], hs[RR_P]) / ctx->npolar);
+        if (eps > ctx->poleps) status = AMG_ERR_NO_CONVERGE;
+    } else {
+        iters = 0;
+    }
+    std::vector<double> h;
+    auto fetch_add = [&](double* dst, const double* src, size_t cnt) {
+        if (!dst) return;
+        h.resize(cnt);
+        CK(cudaMemcpyAsync(h.data(), src, sizeof(double) * cnt, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        for (size_t k = 0; k < cnt; k++) dst[k] += h[k];
+    };
+    auto fetch = [&](double* dst, const double* src, size_t cnt) {
+        if (!dst) return;
+        CK(cudaMemcpyAsync(dst, src, sizeof(double) * cnt, cudaMemcpyDeviceToHost, st));
+    };
+    double em = e[0] + e[2];
+    if (ctx->ewald) {
+        double V = ctx->box[0] * ctx->box[1] * ctx->box[2];
+        double qt = e[3];
+        em += -ctx->f * kPi * qt * qt / (2 * V * ctx->aewald * ctx->aewald);
+    }
+    res->em = em;
+    res->ep = ctx->has_pol ? e[4] : 0.0;
+    res->einter = e[1];
+    res->nem = (int64_t)(c[0] / 2);
+    res->nep = (int64_t)c[1];
+    res->pcg_iters = iters;
+    res->pcg_eps = eps;
+    if (grad) {
+        fetch_add(res->dem, ctx->grad_m, 3 * (size_t)n);
+        if (ctx->has_pol) fetch_add(res->dep, ctx->grad_p, 3 * (size_t)n);
+    }
+    if (analysis) {
+        fetch(res->aem, ctx->aem, n);
+        if (ctx->has_pol) fetch(res->aep, ctx->aep, n);
+    }
+    if ((flags & AMG_DO_DIPOLES) && ctx->has_pol) {
+        fetch(res->uind, ctx->ud, 3 * (size_t)n);
+        fetch(res->uinp, ctx->up, 3 * (size_t)n);
+    }
+    if (res->rpole) {
+        std::vector<double> r10(10 * (size_t)n);
+        CK(cudaMemcpyAsync(r10.data(), ctx->rp10, sizeof(double) * 10 * n, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        for (int i = 0; i < n; i++) {
+            const double* m = &r10[10 * (size_t)i];
+            double* o = res->rpole + 13 * (size_t)i;
+            double v[13] = {m[0], m[1], m[2], m[3], m[4], m[5], m[6], m[5], m[7], m[8], m[6], m[8], m[9]};
+            std::memcpy(o, v, sizeof(v));
+        }
+    }
+    CK(cudaStreamSynchronize(st));
+    float ms[4] = {0, 0, 0, 0};
+    for (int k = 0; k < 4; k++)
+        if (cudaEventElapsedTime(&ms[k], ctx->ev[k], ctx->ev[k + 1]) != cudaSuccess) ms[k] = 0;
+    cudaGetLastError();
+    ctx->timing[0] = ms[0] + ms[1] + ms[2] + ms[3];
+    for (int k = 0; k < 4; k++) ctx->timing[k + 1] = ms[k];
+    ctx->have_forward = true;
+    if (!std::isfinite(res->em) || !std::isfinite(res->ep)) {
+        ctx->err = "non-finite energy";
+        return AMG_ERR_NAN;
+    }
+    if (status != AMG_OK) ctx->err = "PCG did not reach poleps within politer iterations";
+    return status;
+}
+
+void release(amg_ctx* ctx) {
+    double** dbl[] = {&ctx->pole13, &ctx->pol, &ctx->thole, &ctx->pdamp, &ctx->xyz, &ctx->rp10, &ctx->Ed, &ctx->Ep,
+                      &ctx->ud, &ctx->up, &ctx->rd, &ctx->rp, &ctx->zd, &ctx->zp, &ctx->pd, &ctx->pp, &ctx->Apd,
+                      &ctx->App, &ctx->Fd, &ctx->Fp, &ctx->resd, &ctx->scal, &ctx->eacc, &ctx->grad_m, &ctx->grad_p,
+                      &ctx->trq_m, &ctx->trq_p, &ctx->aem, &ctx->aep, &ctx->phiM, &ctx->phiU, &ctx->phiU4};
+    for (double** p : dbl) dfree(*p);
+    int** ints[] = {&ctx->zax, &ctx->xax, &ctx->yax, &ctx->axe, &ctx->mol, &ctx->ids, &ctx->sids, &ctx->cstart,
+                    &ctx->cend, &ctx->nbr, &ctx->nnb, &ctx->overflow, &ctx->xoff, &ctx->xidx};
+    for (int** p : ints) dfree(*p);
+    dfree(ctx->keys);
+    dfree(ctx->skeys);
+    dfree(ctx->spos);
+    dfree(ctx->cnt);
+    dfree(ctx->sp);
+    if (ctx->cubtmp) cudaFree(ctx->cubtmp);
+    ctx->cubtmp = nullptr;
+    dfree(ctx->af.at); dfree(ctx->af.u4); dfree(ctx->ad.at); dfree(ctx->ad.u4);
+    pme_destroy(ctx->pmf);
+    pme_destroy(ctx->pmd);
+    for (auto& e : ctx->ev)
+        if (e) { cudaEventDestroy(e); e = nullptr; }
+    if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
+    dfree(ctx->iter);
+    dfree(ctx->cont);
+    dfree(ctx->flushbuf);
+    if (ctx->st) { cudaStreamDestroy(ctx->st); ctx->st = nullptr; }
+    if (ctx->st2) { cudaStreamDestroy(ctx->st2); ctx->st2 = nullptr; }
+}
+
+int create_impl(amg_ctx* ctx, const amg_params* P) {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        ctx->err = "no CUDA device";
+        return AMG_ERR_NO_DEVICE;
+    }
+    if (P->device < 0 || P->device >= ndev) {
+        ctx->err = "device ordinal out of range";
+        return AMG_ERR_BAD_ARG;
+    }
+    CK(cudaSetDevice(P->device));
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, P->device));
+    if (prop.major < 10) {
+        ctx->err = "libamoeba_gpu is built for sm_100a (B200)";
+        return AMG_ERR_NO_DEVICE;
+    }
+    const int n = P->n;
+    ctx->n = n;
+    ctx->device = P->device;
+    ctx->prec = P->precision;
+    ctx->ewald = P->use_ewald;
+    ctx->bounds = P->use_bounds;
+    ctx->aewald = P->aewald;
+    ctx->cut = P->cutoff;
+    ctx->f = P->electric / P->dielec;
+    ctx->debye = P->debye;
+    ctx->poleps = P->poleps;
+    ctx->politer = P->politer;
+    ctx->guess = P->pcg_guess;
+    ctx->has_pol = P->polarity != nullptr && P->poltyp != AMG_POL_NONE;
+    ctx->poltyp = ctx->has_pol ? P->poltyp : AMG_POL_NONE;
+    for (int a = 0; a < 3; a++) ctx->K[a] = P->nfft[a];
+    CK(cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&ctx->st2, cudaStreamNonBlocking));
+    if (const char* g = getenv("AMG_NO_GRAPH")) ctx->use_graphs = !(g[0] == '1');
+    ctx->lpa = n < 50000 ? 16 : 8;
+    if (const char* l = getenv("AMG_LPA")) ctx->lpa = atoi(l);
+    if (ctx->lpa != 8 && ctx->lpa != 16 && ctx->lpa != 32) ctx->lpa = 16;
+    dalloc(ctx, ctx->iter, 1);
+    dalloc(ctx, ctx->cont, 1);
+    CK(cudaMemset(ctx->iter, 0, sizeof(int)));
+    if (ctx->has_pol)
+        for (int i = 0; i < n; i++) ctx->npolar += P->polarity[i] > 0;
+    for (auto& e : ctx->ev) CK(cudaEventCreate(&e));
+    upload(ctx, ctx->pole13, P->pole, 13 * (size_t)n);
+    upload(ctx, ctx->zax, P->zaxis, n);
+    upload(ctx, ctx->xax, P->xaxis, n);
+    upload(ctx, ctx->yax, P->yaxis, n);
+    upload(ctx, ctx->axe, P->polaxe, n);
+    if (P->molcule) upload(ctx, ctx->mol, P->molcule, n);
+    std::vector<double> zeros(n, 0.0);
+    upload(ctx, ctx->pol, ctx->has_pol ? P->polarity : zeros.data(), n);
+    upload(ctx, ctx->thole, ctx->has_pol ? P->thole : zeros.data(), n);
+    upload(ctx, ctx->pdamp, ctx->has_pol ? P->pdamp : zeros.data(), n);
+    std::vector<ScaledPair> sp = build_scaled(P);
+    ctx->nsp = (int)sp.size();
+    upload(ctx, ctx->sp, sp.data(), sp.size());
+    {
+        std::vector<int> off(n + 1, 0), idx(2 * sp.size() + 1);
+        for (const ScaledPair& q : sp) { off[q.i + 1]++; off[q.k + 1]++; }
+        for (int i = 0; i < n; i++) off[i + 1] += off[i];
+        std::vector<int> fill(off.begin(), off.end() - 1);
+        for (const ScaledPair& q : sp) { idx[fill[q.i]++] = q.k; idx[fill[q.k]++] = q.i; }
+        upload(ctx, ctx->xoff, off.data(), off.size());
+        upload(ctx, ctx->xidx, idx.data(), idx.size());
+    }
+    dalloc(ctx, ctx->xyz, 3 * (size_t)n);
+    dalloc(ctx, ctx->rp10, 10 * (size_t)n);
+    dalloc(ctx, ctx->ad.at, n);
+    dalloc(ctx, ctx->ad.u4, 2 * (size_t)n);
+    if (ctx->prec == AMG_PREC_MIXED) {
+        dalloc(ctx, ctx->af.at, n);
+        dalloc(ctx, ctx->af.u4, 2 * (size_t)n);
+    }
+    double** vecs[] = {&ctx->Ed, &ctx->Ep, &ctx->ud, &ctx->up, &ctx->rd, &ctx->rp, &ctx->zd, &ctx->zp, &ctx->pd,
+                       &ctx->pp, &ctx->Apd, &ctx->App, &ctx->Fd, &ctx->Fp, &ctx->resd, &ctx->grad_m, &ctx->grad_p,
+                       &ctx->trq_m, &ctx->trq_p};
+    for (double** p : vecs) {
+        dalloc(ctx, *p, 3 * (size_t)n);
+        CK(cudaMemset(*p, 0, sizeof(double) * 3 * n));
+    }
+    dalloc(ctx, ctx->aem, n);
+    dalloc(ctx, ctx->aep, n);
+    dalloc(ctx, ctx->scal, 16);
+    dalloc(ctx, ctx->eacc, 8);
+    dalloc(ctx, ctx->cnt, 4);
+    dalloc(ctx, ctx->phiM, 20 * (size_t)n);
+    CK(cudaMemset(ctx->phiM, 0, sizeof(double) * 20 * n));
+    if (ctx->has_pol) {
+        dalloc(ctx, ctx->phiU, 40 * (size_t)n);
+        dalloc(ctx, ctx->phiU4, 8 * (size_t)n);
+    }
+    return AMG_OK;
+}
+
+int validate(const amg_params* P, std::string& why) {
+    if (!P || P->n <= 0 || !P->pole || !P->zaxis || !P->xaxis || !P->yaxis || !P->polaxe) {
+        why = "missing required arrays";
+        return AMG_ERR_BAD_ARG;
+    }
+    if (P->precision != AMG_PREC_FP64 && P->precision != AMG_PREC_MIXED) {
+        why = "precision must be AMG_PREC_FP64 or AMG_PREC_MIXED";
+        return AMG_ERR_BAD_ARG;
+    }
+    if (P->cutoff <= 0 || P->electric <= 0 || P->dielec <= 0) {
+        why = "cutoff, electric and dielec must be positive";
+        return AMG_ERR_BAD_ARG;
+    }
+    if (P->use_ewald) {
+        if (!P->use_bounds) { why = "Ewald needs a periodic box"; return AMG_ERR_BAD_ARG; }
+        if (P->bsorder != kOrder) { why = "only B-spline order 5 is compiled"; return AMG_ERR_UNSUPPORTED; }
+        if (P->aewald <= 0 || P->nfft[0] < 8 || P->nfft[1] < 8 || P->nfft[2] < 8) {
+            why = "Ewald alpha and PME grid (>= 8) required";
+            return AMG_ERR_BAD_ARG;
+        }
+    }
+    if (P->polarity && P->poltyp != AMG_POL_NONE && (!P->thole || !P->pdamp)) {
+        why = "polarization needs thole and pdamp";
+        return AMG_ERR_BAD_ARG;
+    }
+    if (P->poltyp != AMG_POL_NONE && P->poltyp != AMG_POL_MUTUAL && P->poltyp != AMG_POL_DIRECT) {
+        why = "unknown polarization model";
+        return AMG_ERR_UNSUPPORTED;
+    }
+    for (int i = 0; i < P->n; i++) {
+        int ft = P->polaxe[i];
+        if (ft < AMG_FRAME_NONE || ft > AMG_FRAME_THREEFOLD) { why = "bad frame type"; return AMG_ERR_BAD_ARG; }
+        if (ft != AMG_FRAME_NONE) {
+            int need[3] = {P->zaxis[i], ft == AMG_FRAME_ZONLY ? 1 : P->xaxis[i],
+                           (ft == AMG_FRAME_ZBISECT || ft == AMG_FRAME_THREEFOLD) ? std::abs(P->yaxis[i]) : 1};
+            for (int v : need)
+                if (v < 1 || v > P->n) { why = "frame atom out of range"; return AMG_ERR_BAD_ARG; }
+        }
+    }
+    return AMG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int amg_abi_version(void) { return AMG_ABI_VERSION; }
+
+int amg_create(const amg_params* params, amg_ctx** out) {
+    if (!out) return AMG_ERR_BAD_ARG;
+    *out = nullptr;
+    std::string why;
+    int rc = validate(params, why);
+    if (rc != AMG_OK) return rc;
+    amg_ctx* ctx = new amg_ctx();
+    try {
+        rc = create_impl(ctx, params);
+    } catch (Fail& f) {
+        rc = f.code;
+    }
+    if (rc != AMG_OK) {
+        release(ctx);
+        delete ctx;
+        return rc;
+    }
+    *out = ctx;
+    return AMG_OK;
+}
+
+int amg_set_coords(amg_ctx* ctx, const double* xyz, const double box[6]) {
+    if (!ctx || !xyz) return AMG_ERR_BAD_ARG;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        if (ctx->bounds) {
+            if (!box || box[0] <= 0 || box[1] <= 0 || box[2] <= 0) {
+                ctx->err = "periodic box lengths must be positive";
+                return AMG_ERR_BAD_ARG;
+            }
+            if (box[3] != 90.0 || box[4] != 90.0 || box[5] != 90.0) {
+                ctx->err = "only orthogonal boxes are supported";
+                return AMG_ERR_UNSUPPORTED;
+            }
+            for (int a = 0; a < 3; a++)
+                if (ctx->cut > 0.5 * box[a] + 1e-12) {
+                    ctx->err = "cutoff exceeds half the box (minimum image)";
+                    return AMG_ERR_BAD_ARG;
+                }
+            for (int a = 0; a < 3; a++)
+                if (ctx->box[a] != box[a]) ctx->graph_dirty = true;
+            for (int a = 0; a < 6; a++) ctx->box[a] = box[a];
+            for (int a = 0; a < 3; a++) { ctx->bx.L[a] = box[a]; ctx->bx.iL[a] = 1.0 / box[a]; }
+        } else {
+            for (int a = 0; a < 3; a++) { ctx->bx.L[a] = 0; ctx->bx.iL[a] = 0; }
+        }
+        for (int i = 0; i < 3 * ctx->n; i++)
+            if (!std::isfinite(xyz[i])) {
+                ctx->err = "non-finite coordinate";
+                return AMG_ERR_NAN;
+            }
+        cell_grid(ctx, xyz);
+        CK(cudaMemcpyAsync(ctx->xyz, xyz, sizeof(double) * 3 * ctx->n, cudaMemcpyHostToDevice, ctx->st));
+        ctx->have_coords = true;
+        ctx->have_forward = false;
+    } catch (Fail& f) {
+        return f.code;
+    }
+    return AMG_OK;
+}
+
+int amg_forward(amg_ctx* ctx, int32_t flags, amg_results* res) {
+    if (!ctx || !res) return AMG_ERR_BAD_ARG;
+    if (!ctx->have_coords) {
+        ctx->err = "amg_set_coords not called";
+        return AMG_ERR_BAD_ARG;
+    }
+    if (flags & AMG_DO_VIRIAL) {
+        ctx->err = "virial not implemented";
+        return AMG_ERR_UNSUPPORTED;
+    }
+    try {
+        CK(cudaSetDevice(ctx->device));
+        if (ctx->prec == AMG_PREC_MIXED) return forward_impl<float>(ctx, flags, res);
+        return forward_impl<double>(ctx, flags, res);
+    } catch (Fail& f) {
+        return f.code;
+    }
+}
+
+int amg_backward(amg_ctx* ctx, const amg_cotangents* cot, amg_param_grads* grads) {
+    if (!ctx || !cot || !grads) return AMG_ERR_BAD_ARG;
+    ctx->err = "backward not implemented yet";
+    return AMG_ERR_UNSUPPORTED;
+}
+
+int amg_bench(amg_ctx* ctx, int32_t flags, int32_t steps, int64_t flush_bytes, double* ms_steps,
+              int64_t* launches) {
+    if (!ctx || steps <= 0 || !ms_steps) return AMG_ERR_BAD_ARG;
+    if (!ctx->have_coords) {
+        ctx->err = "amg_set_coords not called";
+        return AMG_ERR_BAD_ARG;
+    }
+    amg_results res{};
+    int rc = amg_forward(ctx, flags, &res);  // captures the graph and sizes the lists
+    if (rc != AMG_OK) return rc;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        if (flush_bytes > 0 && (size_t)flush_bytes > ctx->flush_bytes) {
+            dalloc(ctx, ctx->flushbuf, (size_t)flush_bytes);
+            ctx->flush_bytes = (size_t)flush_bytes;
+        }
+        cudaEvent_t a, b;
+        CK(cudaEventCreate(&a));
+        CK(cudaEventCreate(&b));
+        long long total = 0;
+        for (int k = 0; k < steps; k++) {
+            if (flush_bytes > 0) CK(cudaMemsetAsync(ctx->flushbuf, k & 0xff, (size_t)flush_bytes, ctx->st));
+            const long long kstart = ctx->kcount;
+            CK(cudaEventRecord(a, ctx->st));
+            bool graphed = false;
+            if (ctx->use_graphs && ctx->bounds && ctx->gexec && !ctx->graph_dirty && ctx->gflags == flags) {
+                CK(cudaGraphLaunch(ctx->gexec, ctx->st));
+                graphed = true;
+            } else if (ctx->prec == AMG_PREC_MIXED) {
+                enqueue_eager<float>(ctx, flags);
+            } else {
+                enqueue_eager<double>(ctx, flags);
+            }
+            CK(cudaEventRecord(b, ctx->st));
+            CK(cudaEventSynchronize(b));
+            float ms = 0;
+            CK(cudaEventElapsedTime(&ms, a, b));
+            ms_steps[k] = ms;
+            if (graphed) {
+                int iters = 0;
+                CK(cudaMemcpy(&iters, ctx->iter, sizeof(int), cudaMemcpyDeviceToHost));
+                total += ctx->kmain + (long long)(iterative(ctx) ? iters : 0) * ctx->kbody;
+            } else {
+                total += ctx->kcount - kstart;
+            }
+        }
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        if (launches) *launches = total;
+        int over = 0;
+        CK(cudaMemcpy(&over, ctx->overflow, sizeof(int), cudaMemcpyDeviceToHost));
+        if (over > ctx->cap) {
+            ctx->err = "neighbour list overflow during the benchmark";
+            return AMG_ERR_CUDA;
+        }
+    } catch (Fail& f) {
+        return f.code;
+    }
+    return AMG_OK;
+}
+
+int amg_last_stats(amg_ctx* ctx, int64_t* launches, int32_t* graphed, int32_t* lanes_per_site) {
+    if (!ctx) return AMG_ERR_BAD_ARG;
+    if (launches) *launches = ctx->klast;
+    if (graphed) *graphed = ctx->graphed_last;
+    if (lanes_per_site) *lanes_per_site = ctx->lpa;
+    return AMG_OK;
+}
+
+int amg_last_timing(amg_ctx* ctx, double ms[5]) {
+    if (!ctx || !ms) return AMG_ERR_BAD_ARG;
+    for (int k = 0; k < 5; k++) ms[k] = ctx->timing[k];
+    return AMG_OK;
+}
+
+const char* amg_last_error(amg_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+void amg_destroy(amg_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    release(ctx);
+    delete ctx;
+}
+
+}  // extern "C"

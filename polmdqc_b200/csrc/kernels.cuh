@@ -1,0 +1,74 @@
+// kernels.cuh -- the sm_100a kernels of the electrostatics path.
+//
+// Data layout in HBM (per atom, original atom order):
+//   AtomR<R> : 4 x R4  = (x,y,z,q) (dx,dy,dz,Qxx) (Qxy,Qxz,Qyy,Qyz)
+//              (Qzz, pdamp, thole, polarity)   -- 64 B per atom in FP32
+//   induced dipoles (and PCG vectors) as double[3n]; R4 copies for the
+//   pair kernels; neighbour list neighbour-major (nbr[slot*n + i]) so that a
+//   warp of consecutive atoms reads one slot coalesced.
+#pragma once
+#include "device_util.cuh"
+#include "pair_math.cuh"
+
+namespace amg {
+
+constexpr double kPi = 3.141592653589793238462643383279502884;
+constexpr double kSqrtPi = 1.772453850905516027298167483341145183;
+
+template <class R>
+struct AtomR {
+    R4<R> a, b, c, e;
+};
+
+struct Box {
+    double L[3];       // box lengths (0: no periodic wrapping on that axis)
+    double iL[3];
+};
+
+template <class R>
+__device__ __forceinline__ Mpole<R> load_mpole(const AtomR<R>& A) {
+    Mpole<R> M;
+    M.q = A.a.w;
+    M.d = v3<R>(A.b.x, A.b.y, A.b.z);
+    M.Q = Sym<R>{A.b.w, A.c.x, A.c.y, A.c.z, A.c.w, A.e.x};
+    return M;
+}
+
+template <class R>
+__device__ __forceinline__ V3<R> min_image(V3<R> d, const Box& bx) {
+    return v3<R>(wrap1<R>(d.x, (R)bx.L[0], (R)bx.iL[0]), wrap1<R>(d.y, (R)bx.L[1], (R)bx.iL[1]),
+                 wrap1<R>(d.z, (R)bx.L[2], (R)bx.iL[2]));
+}
+
+// pair Thole value: the smaller, or the larger when the smaller is zero
+// (src/md/kpolar.cpp:514-517)
+template <class R>
+__device__ __forceinline__ R pair_thole(R ti, R tk) {
+    R a = fmin(ti, tk);
+    return a == R(0) ? fmax(ti, tk) : a;
+}
+
+// Radial hierarchy of the bulk (unscaled) pair: Ewald (or bare) minus the
+// part removed by Thole damping, B_n = ewald_n - (1 - lam_n) bare_n.
+template <class R, bool EWALD, bool THOLE>
+__device__ __forceinline__ void bulk_radial(R r2, R aewald, R damp, R thl, R (&B)[6]) {
+    R rinv = rsqrt_<R>(r2);
+    R r = r2 * rinv;
+    R rinv2 = rinv * rinv;
+    R bare[6];
+    bare_terms<R, 6>(rinv, rinv2, bare);
+    if (EWALD) {
+        ewald_terms<R, 6>(r, rinv2, aewald, B);
+    } else {
+#pragma unroll
+        for (int n = 0; n < 6; n++) B[n] = bare[n];
+    }
+    if (THOLE) {
+        R lam[5];
+        thole_lambda<R>(r, damp, thl, lam);
+#pragma unroll
+        for (int n = 1; n < 5; n++) B[n] -= (R(1) - lam[n]) * bare[n];
+    }
+}
+
+}  // namespace amg

@@ -1,0 +1,386 @@
+// kernels_misc.cuh -- reciprocal/self finishing steps, the PCG vector
+// updates (FP64 vectors, FP64 dot products), energies and torque -> force.
+#pragma once
+#include "kernels.cuh"
+
+namespace amg {
+
+// Fields from the reciprocal potential (E = -grad phi) and the Ewald self
+// field (4 a^3 / (3 sqrt(pi))) d; then the direct dipoles u = alpha E.
+__global__ void k_field_finish(int n, const double* __restrict__ phiM, int ewald, const double* __restrict__ rp10,
+                               double selfc, const double* __restrict__ pol, double* __restrict__ Ed,
+                               double* __restrict__ Ep, double* __restrict__ ud, double* __restrict__ up) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int a = 0; a < 3; a++) {
+        double add = ewald ? -phiM[20 * (size_t)i + 1 + a] + selfc * rp10[10 * i + 1 + a] : 0.0;
+        double ed = Ed[3 * i + a] + add, ep = Ep[3 * i + a] + add;
+        Ed[3 * i + a] = ed;
+        Ep[3 * i + a] = ep;
+        ud[3 * i + a] = pol[i] * ed;
+        up[3 * i + a] = pol[i] * ep;
+    }
+}
+
+// FP64 dipole vectors -> R4 copies for the pair kernels ([2n], d then p)
+template <class R>
+__global__ void k_pack_u(int n, const double* __restrict__ ud, const double* __restrict__ up, R4<R>* __restrict__ u4) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    u4[i] = make_r4<R>((R)ud[3 * i], (R)ud[3 * i + 1], (R)ud[3 * i + 2], R(0));
+    u4[n + i] = make_r4<R>((R)up[3 * i], (R)up[3 * i + 1], (R)up[3 * i + 2], R(0));
+}
+
+// A v = v/alpha - (real + recip + self) field of v, both sets; pol = 0 sites
+// give 0.  phi: [2][n][4] reciprocal potentials (0 and first derivatives).
+__global__ void k_matvec_finish(int n, const double* __restrict__ vd, const double* __restrict__ vp,
+                                const double* __restrict__ Fd, const double* __restrict__ Fp,
+                                const double* __restrict__ phi, int ewald, double selfc,
+                                const double* __restrict__ pol, double* __restrict__ Ad, double* __restrict__ Ap) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double a = pol[i];
+    double ia = a > 0 ? 1.0 / a : 0.0;
+    for (int c = 0; c < 3; c++) {
+        double fd = Fd[3 * i + c], fp = Fp[3 * i + c];
+        if (ewald) {
+            fd += -phi[4 * (size_t)i + 1 + c] + selfc * vd[3 * i + c];
+            fp += -phi[4 * ((size_t)n + i) + 1 + c] + selfc * vp[3 * i + c];
+        }
+        Ad[3 * i + c] = a > 0 ? ia * vd[3 * i + c] - fd : 0.0;
+        Ap[3 * i + c] = a > 0 ? ia * vp[3 * i + c] - fp : 0.0;
+    }
+}
+
+// scalar slots of the PCG (device memory)
+enum Scal { RZ_D = 0, RZ_P, PAP_D, PAP_P, RZN_D, RZN_P, RR_D, RR_P, NSCAL };
+
+template <class T>
+__global__ void k_zero(T* __restrict__ p, size_t n) {
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = T(0);
+}
+
+// PCG control (one thread): counts the iteration, decides whether to
+// continue (residual above threshold and fewer than politer iterations) and,
+// inside a captured graph, sets the WHILE node's condition.  `first` marks the
+// decision taken right after the initial residual.
+__global__ void k_pcg_control(double* __restrict__ scal, int* __restrict__ iter, double thr2, int maxit, int first,
+                              cudaGraphConditionalHandle h, int use_handle, int* __restrict__ cont_out) {
+    int it = first ? 0 : *iter + 1;
+    *iter = it;
+    if (!first) {  // rz <- rz_new for the next direction update
+        scal[RZ_D] = scal[RZN_D];
+        scal[RZ_P] = scal[RZN_P];
+    }
+    double e2 = fmax(scal[RR_D], scal[RR_P]);
+    int cont = (e2 > thr2) && (it < maxit);
+    *cont_out = cont;
+    if (use_handle) cudaGraphSetConditional(h, cont ? 1u : 0u);
+}
+
+// r = E - A u, z = alpha r, p = z;  rz, rr
+__global__ void k_pcg_init(int n, const double* __restrict__ Ed, const double* __restrict__ Ep,
+                           const double* __restrict__ Aud, const double* __restrict__ Aup,
+                           const double* __restrict__ pol, double* __restrict__ rd, double* __restrict__ rp,
+                           double* __restrict__ zd, double* __restrict__ zp, double* __restrict__ pd,
+                           double* __restrict__ pp, double* __restrict__ scal) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double rzd = 0, rzp = 0, rrd = 0, rrp = 0;
+    if (i < n) {
+        double a = pol[i];
+        for (int c = 0; c < 3; c++) {
+            int q = 3 * i + c;
+            double r1 = a > 0 ? Ed[q] - Aud[q] : 0.0, r2 = a > 0 ? Ep[q] - Aup[q] : 0.0;
+            rd[q] = r1; rp[q] = r2;
+            double z1 = a * r1, z2 = a * r2;
+            zd[q] = z1; zp[q] = z2;
+            pd[q] = z1; pp[q] = z2;
+            rzd += r1 * z1; rzp += r2 * z2; rrd += r1 * r1; rrp += r2 * r2;
+        }
+    }
+    block_sum_add(rzd, scal + RZ_D);
+    block_sum_add(rzp, scal + RZ_P);
+    block_sum_add(rrd, scal + RR_D);
+    block_sum_add(rrp, scal + RR_P);
+}
+
+__global__ void k_dot2(int n3, const double* __restrict__ a1, const double* __restrict__ b1,
+                       const double* __restrict__ a2, const double* __restrict__ b2, double* __restrict__ o1,
+                       double* __restrict__ o2) {
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    double s1 = 0, s2 = 0;
+    if (q < n3) { s1 = a1[q] * b1[q]; s2 = a2[q] * b2[q]; }
+    block_sum_add(s1, o1);
+    block_sum_add(s2, o2);
+}
+
+// u += a p; r -= a Ap; z = alpha r; rz_new, rr  (a = rz / pAp per set)
+__global__ void k_pcg_update(int n, const double* __restrict__ pol, const double* __restrict__ pd,
+                             const double* __restrict__ pp, const double* __restrict__ Apd,
+                             const double* __restrict__ App, double* __restrict__ ud, double* __restrict__ up,
+                             double* __restrict__ rd, double* __restrict__ rp, double* __restrict__ zd,
+                             double* __restrict__ zp, double* __restrict__ scal) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double ad = scal[PAP_D] != 0 ? scal[RZ_D] / scal[PAP_D] : 0.0;
+    double ap = scal[PAP_P] != 0 ? scal[RZ_P] / scal[PAP_P] : 0.0;
+    double rzd = 0, rzp = 0, rrd = 0, rrp = 0;
+    if (i < n) {
+        double a = pol[i];
+        for (int c = 0; c < 3; c++) {
+            int q = 3 * i + c;
+            ud[q] += ad * pd[q];
+            up[q] += ap * pp[q];
+            double r1 = rd[q] - ad * Apd[q], r2 = rp[q] - ap * App[q];
+            rd[q] = r1; rp[q] = r2;
+            double z1 = a * r1, z2 = a * r2;
+            zd[q] = z1; zp[q] = z2;
+            rzd += r1 * z1; rzp += r2 * z2; rrd += r1 * r1; rrp += r2 * r2;
+        }
+    }
+    block_sum_add(rzd, scal + RZN_D);
+    block_sum_add(rzp, scal + RZN_P);
+    block_sum_add(rrd, scal + RR_D);
+    block_sum_add(rrp, scal + RR_P);
+}
+
+// p = z + (rz_new / rz) p; k_pcg_roll then moves rz_new into rz
+__global__ void k_pcg_dir(int n3, const double* __restrict__ zd, const double* __restrict__ zp,
+                          double* __restrict__ pd, double* __restrict__ pp, const double* __restrict__ scal) {
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n3) return;
+    double bd = scal[RZ_D] != 0 ? scal[RZN_D] / scal[RZ_D] : 0.0;
+    double bp = scal[RZ_P] != 0 ? scal[RZN_P] / scal[RZ_P] : 0.0;
+    pd[q] = zd[q] + bd * pd[q];
+    pp[q] = zp[q] + bp * pp[q];
+}
+
+__global__ void k_pcg_roll(double* scal) {
+    scal[RZ_D] = scal[RZN_D];
+    scal[RZ_P] = scal[RZN_P];
+}
+
+// One preconditioned correction step u += alpha r with the FP64 residual
+// r = E - A u, and the norms of that residual.
+__global__ void k_correct(int n, const double* __restrict__ Ed, const double* __restrict__ Ep,
+                          const double* __restrict__ Aud, const double* __restrict__ Aup,
+                          const double* __restrict__ pol, double* __restrict__ ud, double* __restrict__ up,
+                          double* __restrict__ resd, double* __restrict__ scal) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double rrd = 0, rrp = 0, urd = 0;
+    if (i < n) {
+        double a = pol[i];
+        for (int c = 0; c < 3; c++) {
+            int q = 3 * i + c;
+            double r1 = a > 0 ? Ed[q] - Aud[q] : 0.0, r2 = a > 0 ? Ep[q] - Aup[q] : 0.0;
+            rrd += r1 * r1; rrp += r2 * r2;
+            urd += up[q] * r1;   // up . r_d (before the update) for the stationary energy
+            resd[q] = r1;
+            ud[q] += a * r1;
+            up[q] += a * r2;
+        }
+    }
+    block_sum_add(rrd, scal + RR_D);
+    block_sum_add(rrp, scal + RR_P);
+    block_sum_add(urd, scal + RZN_D);
+}
+
+// ep = -1/2 f sum ud . Ep (per-site aep when requested); nep = sites with
+// nonzero energy
+__global__ void k_polar_energy(int n, const double* __restrict__ ud, const double* __restrict__ Ep, double f,
+                               double* __restrict__ eacc, double* __restrict__ aep,
+                               unsigned long long* __restrict__ nep) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double e = 0;
+    long long c = 0;
+    if (i < n) {
+        e = -0.5 * f * (ud[3 * i] * Ep[3 * i] + ud[3 * i + 1] * Ep[3 * i + 1] + ud[3 * i + 2] * Ep[3 * i + 2]);
+        if (aep) aep[i] = e;
+        c = e != 0.0;
+    }
+    block_sum_add(e, eacc);
+    block_sum_add_ll(c, nep);
+}
+
+// ---------------------------------------------------------------- reciprocal
+__device__ __forceinline__ double site_energy(const double* m, const double* p) {
+    return m[0] * p[0] + m[1] * p[1] + m[2] * p[2] + m[3] * p[3] + m[4] * p[4] + m[7] * p[5] + m[9] * p[6] +
+           2 * (m[5] * p[7] + m[6] * p[8] + m[8] * p[9]);
+}
+// d/dx_site (M . phi): q grad phi + d.grad grad phi + Q:grad^3 phi
+__device__ __forceinline__ V3<double> site_gradient(const double* m, const double* p) {
+    double q = m[0], dx = m[1], dy = m[2], dz = m[3], Qxx = m[4], Qxy = m[5], Qxz = m[6], Qyy = m[7], Qyz = m[8],
+           Qzz = m[9];
+    V3<double> g;
+    g.x = q * p[1] + dx * p[4] + dy * p[7] + dz * p[8] + Qxx * p[10] + Qyy * p[15] + Qzz * p[17] +
+          2 * (Qxy * p[13] + Qxz * p[14] + Qyz * p[19]);
+    g.y = q * p[2] + dx * p[7] + dy * p[5] + dz * p[9] + Qxx * p[13] + Qyy * p[11] + Qzz * p[18] +
+          2 * (Qxy * p[15] + Qxz * p[19] + Qyz * p[16]);
+    g.z = q * p[3] + dx * p[8] + dy * p[9] + dz * p[6] + Qxx * p[14] + Qyy * p[16] + Qzz * p[12] +
+          2 * (Qxy * p[19] + Qxz * p[17] + Qyz * p[18]);
+    return g;
+}
+// dipole-only version (v . grad grad phi)
+__device__ __forceinline__ V3<double> dipole_gradient(V3<double> v, const double* p) {
+    return v3<double>(v.x * p[4] + v.y * p[7] + v.z * p[8], v.x * p[7] + v.y * p[5] + v.z * p[9],
+                      v.x * p[8] + v.y * p[9] + v.z * p[6]);
+}
+// torque -dE/dtheta of E = M . phi
+__device__ __forceinline__ V3<double> site_torque(const double* m, const double* p) {
+    V3<double> d = v3<double>(m[1], m[2], m[3]);
+    V3<double> t = (-1.0) * cross(d, v3<double>(p[1], p[2], p[3]));
+    Sym<double> Q{m[4], m[5], m[6], m[7], m[8], m[9]};
+    Sym<double> H{p[4], p[7], p[8], p[5], p[9], p[6]};
+    return t - 2.0 * axial_prod(Q, H);
+}
+
+// permanent reciprocal energy 1/2 M.phi, gradient, torque; self energy;
+// per-site energies on request
+__global__ void k_recip_mpole(int n, const double* __restrict__ rp10, const double* __restrict__ phiM, double f,
+                              double alpha, double* __restrict__ grad, double* __restrict__ trq,
+                              double* __restrict__ eacc, double* __restrict__ aem, double* __restrict__ qsum) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double e = 0, q = 0;
+    if (i < n) {
+        const double* m = rp10 + 10 * i;
+        const double* p = phiM + 20 * (size_t)i;
+        double er = 0.5 * site_energy(m, p);
+        double d2 = m[1] * m[1] + m[2] * m[2] + m[3] * m[3];
+        double qq = m[4] * m[4] + m[7] * m[7] + m[9] * m[9] + 2 * (m[5] * m[5] + m[6] * m[6] + m[8] * m[8]);
+        double a2 = alpha * alpha;
+        double es = -(alpha / kSqrtPi) * (m[0] * m[0] + (2 * a2 / 3) * d2 + (8 * a2 * a2 / 5) * qq);
+        e = f * (er + es);
+        q = m[0];
+        V3<double> g = site_gradient(m, p), t = site_torque(m, p);
+        grad[3 * i] += f * g.x; grad[3 * i + 1] += f * g.y; grad[3 * i + 2] += f * g.z;
+        trq[3 * i] += f * t.x; trq[3 * i + 1] += f * t.y; trq[3 * i + 2] += f * t.z;
+        if (aem) aem[i] += e;
+    }
+    block_sum_add(e, eacc);
+    block_sum_add(q, qsum);
+}
+
+// reciprocal + self part of the polarization gradient and torques:
+//   dG/dx_i = 1/2 [(up+ud)_i . grad grad phiM + M_i . grad(phi_p + phi_d)
+//                  + up_i . grad grad phi_d + ud_i . grad grad phi_p]
+//   torque  = torque(M_i, (phi_d + phi_p)/2) + (selfc/2) d_i x (ud + up)_i
+__global__ void k_recip_polar(int n, const double* __restrict__ rp10, const double* __restrict__ phiM,
+                              const double* __restrict__ phid, const double* __restrict__ phip,
+                              const double* __restrict__ ud, const double* __restrict__ up, int mutual,
+                              double selfc, double f, double* __restrict__ grad, double* __restrict__ trq) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double* m = rp10 + 10 * i;
+    const double* pm = phiM + 20 * (size_t)i;
+    const double* pd = phid + 20 * (size_t)i;
+    const double* pp = phip + 20 * (size_t)i;
+    V3<double> udi = ld3(ud, i), upi = ld3(up, i);
+    double avg[20];
+    for (int j = 0; j < 20; j++) avg[j] = pd[j] + pp[j];
+    V3<double> g = dipole_gradient(udi + upi, pm) + site_gradient(m, avg);
+    if (mutual) g = g + dipole_gradient(upi, pd) + dipole_gradient(udi, pp);
+    g = (0.5 * f) * g;
+    for (int j = 0; j < 20; j++) avg[j] *= 0.5;
+    V3<double> t = site_torque(m, avg) + (0.5 * selfc) * cross(v3<double>(m[1], m[2], m[3]), udi + upi);
+    t = f * t;
+    grad[3 * i] += g.x; grad[3 * i + 1] += g.y; grad[3 * i + 2] += g.z;
+    trq[3 * i] += t.x; trq[3 * i + 1] += t.y; trq[3 * i + 2] += t.z;
+}
+
+// ---------------------------------------------------------------- torque
+// Site torques -> gradients on the frame atoms, restating the reference's
+// torque (src/md/torque.cpp:42-397; Popelier & Stone 1994, Sagui et al.
+// 2004).  Gradients are accumulated with FP64 atomics (frame atoms are shared).
+__global__ void k_torque(int n, const double* __restrict__ xyz, const int* __restrict__ zax,
+                         const int* __restrict__ xax, const int* __restrict__ yax, const int* __restrict__ axe,
+                         const double* __restrict__ trq, double* __restrict__ grad) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int ft = axe[i];
+    if (ft == AMG_FRAME_NONE) return;
+    using D = double;
+    auto P = [&](int a) { return v3<D>(xyz[3 * a], xyz[3 * a + 1], xyz[3 * a + 2]); };
+    auto unit = [](V3<D> v) { D s = 1.0 / sqrt(dot(v, v)); return s * v; };
+    int ia = zax[i] - 1, ib = i, ic = xax[i] - 1, id = abs(yax[i]) - 1;
+    V3<D> t = v3<D>(trq[3 * i], trq[3 * i + 1], trq[3 * i + 2]);
+    V3<D> u = P(ia) - P(ib);
+    D us = sqrt(dot(u, u));
+    V3<D> v;
+    D vs;
+    if (ft != AMG_FRAME_ZONLY) {
+        v = P(ic) - P(ib);
+        vs = sqrt(dot(v, v));
+    } else {
+        v = fabs(u.x / us) > 0.866 ? v3<D>(0, 1, 0) : v3<D>(1, 0, 0);
+        vs = 1;
+    }
+    V3<D> w = (ft == AMG_FRAME_ZBISECT || ft == AMG_FRAME_THREEFOLD) ? P(id) - P(ib) : cross(u, v);
+    D ws = sqrt(dot(w, w));
+    u = (1.0 / us) * u;
+    v = (1.0 / vs) * v;
+    w = (1.0 / ws) * w;
+    D dpu = -dot(t, u), dpv = -dot(t, v), dpw = -dot(t, w);
+    V3<D> uv = unit(cross(v, u)), uw = unit(cross(w, u)), vw = unit(cross(w, v));
+    D uvc = dot(u, v), uvsn = sqrt(1 - uvc * uvc);
+    auto add = [&](int at, V3<D> g) {
+        atomicAdd(grad + 3 * at, g.x);
+        atomicAdd(grad + 3 * at + 1, g.y);
+        atomicAdd(grad + 3 * at + 2, g.z);
+    };
+    if (ft == AMG_FRAME_ZONLY) {
+        V3<D> du = (dpv / (us * uvsn)) * uv + (dpw / us) * uw;
+        add(ia, du);
+        add(ib, (-1.0) * du);
+    } else if (ft == AMG_FRAME_ZTHENX) {
+        V3<D> du = (dpv / (us * uvsn)) * uv + (dpw / us) * uw;
+        V3<D> dv = (-dpu / (vs * uvsn)) * uv;
+        add(ia, du);
+        add(ic, dv);
+        add(ib, (-1.0) * (du + dv));
+    } else if (ft == AMG_FRAME_BISECTOR) {
+        V3<D> du = (dpv / (us * uvsn)) * uv + (0.5 * dpw / us) * uw;
+        V3<D> dv = (-dpu / (vs * uvsn)) * uv + (0.5 * dpw / vs) * vw;
+        add(ia, du);
+        add(ic, dv);
+        add(ib, (-1.0) * (du + dv));
+    } else if (ft == AMG_FRAME_ZBISECT) {
+        V3<D> r = unit(v + w);
+        V3<D> s = unit(cross(u, r));
+        D dpr = -dot(t, r), dps = -dot(t, s);
+        V3<D> ur = unit(cross(r, u)), us_ = unit(cross(s, u));
+        D urc = dot(u, r), ursn = sqrt(1 - urc * urc);
+        D vsc = dot(v, s), vssn = sqrt(1 - vsc * vsc);
+        D wsc = dot(w, s), wssn = sqrt(1 - wsc * wsc);
+        V3<D> t1 = unit(v - vsc * s), t2 = unit(w - wsc * s);
+        D ut1c = dot(u, t1), ut1s = sqrt(1 - ut1c * ut1c);
+        D ut2c = dot(u, t2), ut2s = sqrt(1 - ut2c * ut2c);
+        V3<D> du = (dpr / (us * ursn)) * ur + (dps / us) * us_;
+        V3<D> dv = (dpu / (vs * (ut1s + ut2s))) * (vssn * s - vsc * t1);
+        V3<D> dw = (dpu / (ws * (ut1s + ut2s))) * (wssn * s - wsc * t2);
+        add(ia, du);
+        add(ic, dv);
+        add(id, dw);
+        add(ib, (-1.0) * (du + dv + dw));
+    } else if (ft == AMG_FRAME_THREEFOLD) {
+        V3<D> sum = u + v + w;
+        D ps = sqrt(dot(sum, sum));
+        V3<D> p = (1.0 / ps) * sum;
+        D wpc = dot(w, p), upc = dot(u, p), vpc = dot(v, p);
+        auto leg = [&](V3<D> a1, V3<D> a2, V3<D> self, D selfsiz, D selfpc, int atom) {
+            V3<D> rr = unit(a1 + a2);
+            D c = dot(rr, self), sn = sqrt(1 - c * c);
+            D dpr_ = -dot(t, rr);
+            V3<D> del = unit(cross(rr, self));
+            D dpd = -dot(t, del);
+            V3<D> eps = cross(del, self);
+            V3<D> g = (dpr_ / (selfsiz * sn)) * del + (dpd * selfpc / (selfsiz * ps)) * eps;
+            add(atom, g);
+            add(ib, (-1.0) * g);
+        };
+        leg(u, v, w, ws, wpc, id);
+        leg(v, w, u, us, upc, ia);
+        leg(u, w, v, vs, vpc, ic);
+    }
+}
+
+}  // namespace amg

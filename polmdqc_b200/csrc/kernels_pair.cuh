@@ -1,0 +1,398 @@
+// kernels_pair.cuh -- real-space pair kernels (a lane group per site over
+// its exact neighbour list, both directions of every pair, warp-shuffle
+// reductions, no atomics) and the FP64 scaled-pair kernels.
+#pragma once
+#include "kernels.cuh"
+
+namespace amg {
+
+// All bulk pair kernels below give each site a group of LPA consecutive
+// lanes (LPA = 4, 8, 16 or 32); the lanes stride through the site's
+// neighbour slots nbr[i * cap + s] and the partial sums are combined with
+// warp shuffles.  Sites past n run with an empty list so every lane takes
+// part in the shuffles.
+template <int LPA, class T>
+__device__ __forceinline__ T group_sum(T v) {
+#pragma unroll
+    for (int o = LPA / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Permanent field at every site from all neighbours' multipoles, bulk
+// (scale 1, Thole damped, Ewald or bare).  Writes Ed = Ep (the d/p
+// differences come only from the scaled pairs).
+template <class R, bool EWALD, int LPA>
+__global__ void __launch_bounds__(128) k_perm_field(int n, const AtomR<R>* __restrict__ at, Box bx, R aewald,
+                                                    const int* __restrict__ nbr, int cap,
+                                                    const int* __restrict__ nnb, double* __restrict__ Ed,
+                                                    double* __restrict__ Ep) {
+    const int g = (blockIdx.x * blockDim.x + threadIdx.x) / LPA, lane = threadIdx.x % LPA;
+    const int i = min(g, n - 1);
+    const int cnt = g < n ? nnb[i] : 0;
+    AtomR<R> Ai = at[i];
+    V3<R> xi = v3<R>(Ai.a.x, Ai.a.y, Ai.a.z);
+    R pdi = Ai.e.y, thi = Ai.e.z;
+    double fx = 0, fy = 0, fz = 0;
+    const int* row = nbr + (size_t)i * cap;
+    for (int s = lane; s < cnt; s += LPA) {
+        int j = row[s];
+        AtomR<R> Aj = at[j];
+        V3<R> r = min_image<R>(xi - v3<R>(Aj.a.x, Aj.a.y, Aj.a.z), bx);  // target i - source j
+        R B[6];
+        bulk_radial<R, EWALD, true>(dot(r, r), aewald, pdi * Aj.e.y, pair_thole<R>(thi, Aj.e.z), B);
+        V3<R> E = field_of_mpole<R>(load_mpole(Aj), r, B[1], B[2], B[3]);
+        fx += E.x; fy += E.y; fz += E.z;
+    }
+    fx = group_sum<LPA>(fx); fy = group_sum<LPA>(fy); fz = group_sum<LPA>(fz);
+    if (lane == 0 && g < n) {
+        Ed[3 * i] = fx; Ed[3 * i + 1] = fy; Ed[3 * i + 2] = fz;
+        Ep[3 * i] = fx; Ep[3 * i + 1] = fy; Ep[3 * i + 2] = fz;
+    }
+}
+
+// Mutual field T u for two dipole sets (bulk, u-scale 1).  u4: [2n] R4
+// (ux,uy,uz,0) with the d set first, p set second.  Writes Fd, Fp.
+template <class R, bool EWALD, int LPA>
+__global__ void __launch_bounds__(128) k_Tu(int n, const AtomR<R>* __restrict__ at, const R4<R>* __restrict__ u4,
+                                            Box bx, R aewald, const int* __restrict__ nbr, int cap,
+                                            const int* __restrict__ nnb, double* __restrict__ Fd,
+                                            double* __restrict__ Fp) {
+    const int g = (blockIdx.x * blockDim.x + threadIdx.x) / LPA, lane = threadIdx.x % LPA;
+    const int i = min(g, n - 1);
+    const int cnt = g < n ? nnb[i] : 0;
+    R4<R> pi = at[i].a, ei = at[i].e;
+    V3<R> xi = v3<R>(pi.x, pi.y, pi.z);
+    R ax = 0, ay = 0, az = 0, bx_ = 0, by = 0, bz = 0;
+    const int* row = nbr + (size_t)i * cap;
+    for (int s = lane; s < cnt; s += LPA) {
+        int j = row[s];
+        R4<R> pj = at[j].a, ej = at[j].e;
+        V3<R> r = min_image<R>(xi - v3<R>(pj.x, pj.y, pj.z), bx);
+        R r2 = dot(r, r);
+        R rinv = rsqrt_<R>(r2);
+        R rr = r2 * rinv, rinv2 = rinv * rinv;
+        R B1, B2;
+        {
+            R b1 = rinv * rinv2, b2 = 3 * b1 * rinv2;
+            if (EWALD) {
+                R eb[3];
+                ewald_terms<R, 3>(rr, rinv2, aewald, eb);
+                B1 = eb[1]; B2 = eb[2];
+            } else {
+                B1 = b1; B2 = b2;
+            }
+            R damp = ei.y * ej.y;
+            if (damp != R(0)) {
+                R t = rr / damp;
+                R x = pair_thole<R>(ei.z, ej.z) * t * t * t;
+                R e = exp_<R>(-x);
+                B1 -= e * b1;                 // (1 - lambda3) = e
+                B2 -= (R(1) + x) * e * b2;    // (1 - lambda5) = (1 + x) e
+            }
+        }
+        R4<R> ud = u4[j], up = u4[n + j];
+        R ad = ud.x * r.x + ud.y * r.y + ud.z * r.z;
+        R ap = up.x * r.x + up.y * r.y + up.z * r.z;
+        ax += ad * B2 * r.x - B1 * ud.x; ay += ad * B2 * r.y - B1 * ud.y; az += ad * B2 * r.z - B1 * ud.z;
+        bx_ += ap * B2 * r.x - B1 * up.x; by += ap * B2 * r.y - B1 * up.y; bz += ap * B2 * r.z - B1 * up.z;
+    }
+    // FP32 partial sums over a few neighbours, combined in FP64
+    double sx = group_sum<LPA>((double)ax), sy = group_sum<LPA>((double)ay), sz = group_sum<LPA>((double)az);
+    double tx = group_sum<LPA>((double)bx_), ty = group_sum<LPA>((double)by), tz = group_sum<LPA>((double)bz);
+    if (lane == 0 && g < n) {
+        Fd[3 * i] = sx; Fd[3 * i + 1] = sy; Fd[3 * i + 2] = sz;
+        Fp[3 * i] = tx; Fp[3 * i + 1] = ty; Fp[3 * i + 2] = tz;
+    }
+}
+
+// Multipole energy (half of each directed pair), gradient and torque of site
+// i from all its neighbours (bulk, m-scale 1).  f = electric/dielec.
+// Analysis: per-site energy, nonzero pair count (directed), intermolecular.
+template <class R, bool EWALD, bool ANALYSIS, int LPA>
+__global__ void __launch_bounds__(128) k_mpole_pair(int n, const AtomR<R>* __restrict__ at, Box bx, R aewald,
+                                                    const int* __restrict__ nbr, int cap,
+                                                    const int* __restrict__ nnb, double f, double* __restrict__ grad,
+                                                    double* __restrict__ trq, double* __restrict__ eacc,
+                                                    double* __restrict__ aem, const int* __restrict__ mol,
+                                                    unsigned long long* __restrict__ npair) {
+    const int gi_ = (blockIdx.x * blockDim.x + threadIdx.x) / LPA, lane = threadIdx.x % LPA;
+    const int i = min(gi_, n - 1);
+    const int cnt = gi_ < n ? nnb[i] : 0;
+    double e_i = 0, einter = 0;
+    long long cntnz = 0;
+    AtomR<R> Ai = at[i];
+    Mpole<R> Mi = load_mpole(Ai);
+    V3<R> xi = v3<R>(Ai.a.x, Ai.a.y, Ai.a.z);
+    V3<R> g = v3<R>(0, 0, 0), t = v3<R>(0, 0, 0);
+    int mi = ANALYSIS && mol ? mol[i] : 0;
+    const int* row = nbr + (size_t)i * cap;
+    for (int s = lane; s < cnt; s += LPA) {
+        int j = row[s];
+        AtomR<R> Aj = at[j];
+        V3<R> r = min_image<R>(v3<R>(Aj.a.x, Aj.a.y, Aj.a.z) - xi, bx);  // x_k - x_i
+        R B[6];
+        bulk_radial<R, EWALD, false>(dot(r, r), aewald, R(0), R(0), B);
+        R E;
+        V3<R> gi, ti;
+        mm_pair_i<R>(Mi, load_mpole(Aj), r, B, E, gi, ti);
+        e_i += 0.5 * (double)E;
+        g = g + gi;
+        t = t + ti;
+        if (ANALYSIS) {
+            if (E != R(0)) cntnz++;
+            if (mol && mol[j] != mi) einter += 0.5 * (double)E;
+        }
+    }
+    double gx = group_sum<LPA>((double)g.x), gy = group_sum<LPA>((double)g.y), gz = group_sum<LPA>((double)g.z);
+    double tx = group_sum<LPA>((double)t.x), ty = group_sum<LPA>((double)t.y), tz = group_sum<LPA>((double)t.z);
+    double es = group_sum<LPA>(e_i);
+    if (lane == 0 && gi_ < n) {
+        grad[3 * i] += f * gx; grad[3 * i + 1] += f * gy; grad[3 * i + 2] += f * gz;
+        trq[3 * i] += f * tx; trq[3 * i + 1] += f * ty; trq[3 * i + 2] += f * tz;
+        if (ANALYSIS) aem[i] += f * es;
+    }
+    block_sum_add(f * e_i, eacc);
+    if (ANALYSIS) {
+        block_sum_add(f * einter, eacc + 1);
+        block_sum_add_ll(cntnz, npair);
+    }
+}
+
+// Polarization gradient and torque of site i (bulk, all scales 1):
+//   G = E(M_i, ubar_k) + E(ubar_i, M_k) + 1/2 [E(up_i, ud_k) + E(ud_i, up_k)]
+// with ubar = (ud + up)/2; dG/dx_i = -dG/dr, torque on M_i from ubar_k.
+// u4: [2n] R4, d set then p set.
+template <class R, bool EWALD, int LPA>
+__global__ void __launch_bounds__(128) k_polar_pair(int n, const AtomR<R>* __restrict__ at,
+                                                    const R4<R>* __restrict__ u4, Box bx, R aewald,
+                                                    const int* __restrict__ nbr, int cap,
+                                                    const int* __restrict__ nnb, int mutual, double f,
+                                                    double* __restrict__ grad, double* __restrict__ trq) {
+    const int gi_ = (blockIdx.x * blockDim.x + threadIdx.x) / LPA, lane = threadIdx.x % LPA;
+    const int i = min(gi_, n - 1);
+    const int cnt = gi_ < n ? nnb[i] : 0;
+    AtomR<R> Ai = at[i];
+    Mpole<R> Mi = load_mpole(Ai);
+    V3<R> xi = v3<R>(Ai.a.x, Ai.a.y, Ai.a.z);
+    R4<R> udi4 = u4[i], upi4 = u4[n + i];
+    V3<R> udi = v3<R>(udi4.x, udi4.y, udi4.z), upi = v3<R>(upi4.x, upi4.y, upi4.z);
+    V3<R> ubi = R(0.5) * (udi + upi);
+    V3<R> g = v3<R>(0, 0, 0), t = v3<R>(0, 0, 0);
+    const int* row = nbr + (size_t)i * cap;
+    for (int s = lane; s < cnt; s += LPA) {
+        int j = row[s];
+        AtomR<R> Aj = at[j];
+        V3<R> r = min_image<R>(v3<R>(Aj.a.x, Aj.a.y, Aj.a.z) - xi, bx);
+        R B[6];
+        bulk_radial<R, EWALD, true>(dot(r, r), aewald, Ai.e.y * Aj.e.y, pair_thole<R>(Ai.e.z, Aj.e.z), B);
+        R4<R> udk4 = u4[j], upk4 = u4[n + j];
+        V3<R> udk = v3<R>(udk4.x, udk4.y, udk4.z), upk = v3<R>(upk4.x, upk4.y, upk4.z);
+        V3<R> ubk = R(0.5) * (udk + upk);
+        Mpole<R> Mk = load_mpole(Aj);
+        SiteInv<R> si = invariants(Mi, r), sk = invariants(Mk, r);
+        V3<R> d1, ti;
+        md_pair<R>(Mi, si, ubk, r, B, d1, ti);
+        V3<R> dEdr = d1 + dm_pair<R>(ubi, Mk, sk, r, B);
+        if (mutual) dEdr = dEdr + R(0.5) * (dd_pair<R>(upi, udk, r, B) + dd_pair<R>(udi, upk, r, B));
+        g = g - dEdr;
+        t = t + ti;
+    }
+    double gx = group_sum<LPA>((double)g.x), gy = group_sum<LPA>((double)g.y), gz = group_sum<LPA>((double)g.z);
+    double tx = group_sum<LPA>((double)t.x), ty = group_sum<LPA>((double)t.y), tz = group_sum<LPA>((double)t.z);
+    if (lane == 0 && gi_ < n) {
+        grad[3 * i] += f * gx; grad[3 * i + 1] += f * gy; grad[3 * i + 2] += f * gz;
+        trq[3 * i] += f * tx; trq[3 * i + 1] += f * ty; trq[3 * i + 2] += f * tz;
+    }
+}
+
+// ------------------------------------------------------------ scaled pairs
+// Pairs with any scale != 1, from the 1-n and polarization-group lists.
+// They are removed from the bulk neighbour lists and evaluated whole here in
+// FP64: these are the short intramolecular pairs whose large bare terms would
+// otherwise pass through the FP32 bulk kernels and cancel against an FP64
+// correction.
+struct ScaledPair {
+    int i, k;
+    double m, p, d, u;
+};
+
+struct ScaledGeom {  // FP64 geometry and radial parts of one scaled pair
+    V3<double> r;    // x_k - x_i
+    bool inside;
+    double lam[5];
+    double bare[6];
+    double ew[6];
+};
+
+__device__ __forceinline__ ScaledGeom scaled_geom(const ScaledPair& sp, const double* __restrict__ xyz,
+                                                  const double* __restrict__ pdamp, const double* __restrict__ thole,
+                                                  Box bx, double cut2, double aewald) {
+    ScaledGeom G;
+    int i = sp.i, k = sp.k;
+    G.r = v3<double>(wrap1<double>(xyz[3 * k] - xyz[3 * i], bx.L[0], bx.iL[0]),
+                     wrap1<double>(xyz[3 * k + 1] - xyz[3 * i + 1], bx.L[1], bx.iL[1]),
+                     wrap1<double>(xyz[3 * k + 2] - xyz[3 * i + 2], bx.L[2], bx.iL[2]));
+    double r2 = dot(G.r, G.r);
+    G.inside = r2 <= cut2;
+    double rinv = 1.0 / sqrt(r2);
+    bare_terms<double, 6>(rinv, rinv * rinv, G.bare);
+    if (aewald > 0) ewald_terms<double, 6>(r2 * rinv, rinv * rinv, aewald, G.ew);
+    double damp = pdamp ? pdamp[i] * pdamp[k] : 0.0;
+    double a = thole ? pair_thole<double>(thole[i], thole[k]) : 0.0;
+    thole_lambda<double>(r2 * rinv, damp, a, G.lam);
+    return G;
+}
+
+// Full radial of a scaled pair (these pairs are left out of the bulk
+// neighbour lists and evaluated here, in FP64, with every channel):
+//   Ewald: B_n = ewald_n - (1 - s lambda_n) bare_n;  bare: s lambda_n bare_n
+__device__ __forceinline__ void scaled_radial(const ScaledGeom& G, double s, bool thole, bool ewald,
+                                              double (&B)[6]) {
+#pragma unroll
+    for (int n = 0; n < 6; n++) {
+        double sl = s * (thole && n >= 1 && n <= 4 ? G.lam[n] : 1.0);
+        B[n] = ewald ? G.ew[n] - (1.0 - sl) * G.bare[n] : sl * G.bare[n];
+    }
+}
+
+__device__ __forceinline__ Mpole<double> mpole64(const double* m) {
+    Mpole<double> M;
+    M.q = m[0];
+    M.d = v3<double>(m[1], m[2], m[3]);
+    M.Q = Sym<double>{m[4], m[5], m[6], m[7], m[8], m[9]};
+    return M;
+}
+__device__ __forceinline__ V3<double> ld3(const double* p, int i) { return v3<double>(p[3 * i], p[3 * i + 1], p[3 * i + 2]); }
+__device__ __forceinline__ void add3(double* p, int i, V3<double> v) {
+    atomicAdd(p + 3 * i, v.x);
+    atomicAdd(p + 3 * i + 1, v.y);
+    atomicAdd(p + 3 * i + 2, v.z);
+}
+
+__global__ void k_scaled_field(int np, const ScaledPair* __restrict__ sp, const double* __restrict__ xyz,
+                               const double* __restrict__ rp10, const double* __restrict__ pdamp,
+                               const double* __restrict__ thole, Box bx, double cut2, double aewald,
+                               double* __restrict__ Ed, double* __restrict__ Ep) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= np) return;
+    ScaledPair P = sp[t];
+    ScaledGeom G = scaled_geom(P, xyz, pdamp, thole, bx, cut2, aewald);
+    if (!G.inside) return;
+    Mpole<double> Mi = mpole64(rp10 + 10 * P.i), Mk = mpole64(rp10 + 10 * P.k);
+    double Bd[6], Bp[6];
+    scaled_radial(G, P.d, true, aewald > 0, Bd);
+    scaled_radial(G, P.p, true, aewald > 0, Bp);
+    V3<double> mr = (-1.0) * G.r;
+    add3(Ed, P.k, field_of_mpole<double>(Mi, G.r, Bd[1], Bd[2], Bd[3]));
+    add3(Ed, P.i, field_of_mpole<double>(Mk, mr, Bd[1], Bd[2], Bd[3]));
+    add3(Ep, P.k, field_of_mpole<double>(Mi, G.r, Bp[1], Bp[2], Bp[3]));
+    add3(Ep, P.i, field_of_mpole<double>(Mk, mr, Bp[1], Bp[2], Bp[3]));
+}
+
+__global__ void k_scaled_Tu(int np, const ScaledPair* __restrict__ sp, const double* __restrict__ xyz,
+                            const double* __restrict__ pdamp, const double* __restrict__ thole, Box bx, double cut2,
+                            double aewald, const double* __restrict__ ud, const double* __restrict__ up,
+                            double* __restrict__ Fd, double* __restrict__ Fp) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= np) return;
+    ScaledPair P = sp[t];
+    ScaledGeom G = scaled_geom(P, xyz, pdamp, thole, bx, cut2, aewald);
+    if (!G.inside) return;
+    double B[6];
+    scaled_radial(G, P.u, true, aewald > 0, B);
+    V3<double> mr = (-1.0) * G.r;
+    add3(Fd, P.k, field_of_dipole<double>(ld3(ud, P.i), G.r, B[1], B[2]));
+    add3(Fd, P.i, field_of_dipole<double>(ld3(ud, P.k), mr, B[1], B[2]));
+    add3(Fp, P.k, field_of_dipole<double>(ld3(up, P.i), G.r, B[1], B[2]));
+    add3(Fp, P.i, field_of_dipole<double>(ld3(up, P.k), mr, B[1], B[2]));
+}
+
+// scaled pairs' contribution to em, its gradient and the torques (both
+// sites, full pair in FP64)
+__global__ void k_scaled_mpole(int np, const ScaledPair* __restrict__ sp, const double* __restrict__ xyz,
+                               const double* __restrict__ rp10, Box bx, double cut2, double aewald, double f,
+                               double* __restrict__ grad, double* __restrict__ trq, double* __restrict__ eacc,
+                               double* __restrict__ aem, const int* __restrict__ mol,
+                               unsigned long long* __restrict__ npair) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    double e = 0, einter = 0;
+    long long nz = 0;
+    if (t < np) {
+        ScaledPair P = sp[t];
+        {
+            ScaledGeom G = scaled_geom(P, xyz, nullptr, nullptr, bx, cut2, aewald);
+            if (G.inside) {
+                double B[6];
+                scaled_radial(G, P.m, false, aewald > 0, B);
+                Mpole<double> Mi = mpole64(rp10 + 10 * P.i), Mk = mpole64(rp10 + 10 * P.k);
+                double E, E2;
+                V3<double> gi, ti, gk, tk;
+                mm_pair_i<double>(Mi, Mk, G.r, B, E, gi, ti);
+                mm_pair_i<double>(Mk, Mi, (-1.0) * G.r, B, E2, gk, tk);
+                e = f * E;
+                nz = 2 * (E != 0.0);   // counted as two directed pairs, like the bulk kernel
+                add3(grad, P.i, f * gi);
+                add3(grad, P.k, f * gk);
+                add3(trq, P.i, f * ti);
+                add3(trq, P.k, f * tk);
+                if (aem) {
+                    atomicAdd(aem + P.i, 0.5 * e);
+                    atomicAdd(aem + P.k, 0.5 * e);
+                }
+                if (mol && mol[P.i] != mol[P.k]) einter = e;
+            }
+        }
+    }
+    block_sum_add(e, eacc);
+    if (mol) block_sum_add(einter, eacc + 1);
+    if (npair) block_sum_add_ll(nz, npair);
+}
+
+// scaled pairs' polarization gradient and torques (full pair, FP64):
+//  1/2 [E^d(M_i, up_k) + E^d(up_i, M_k) + E^p(M_i, ud_k) + E^p(ud_i, M_k)
+//       + E^u(up_i, ud_k) + E^u(ud_i, up_k)]
+__global__ void k_scaled_polar(int np, const ScaledPair* __restrict__ sp, const double* __restrict__ xyz,
+                               const double* __restrict__ rp10, const double* __restrict__ pdamp,
+                               const double* __restrict__ thole, Box bx, double cut2, double aewald,
+                               const double* __restrict__ ud, const double* __restrict__ up, int mutual, double f,
+                               double* __restrict__ grad, double* __restrict__ trq) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= np) return;
+    ScaledPair P = sp[t];
+    ScaledGeom G = scaled_geom(P, xyz, pdamp, thole, bx, cut2, aewald);
+    if (!G.inside) return;
+    double Bd[6], Bp[6], Bu[6];
+    scaled_radial(G, P.d, true, aewald > 0, Bd);
+    scaled_radial(G, P.p, true, aewald > 0, Bp);
+    scaled_radial(G, P.u, true, aewald > 0, Bu);
+    const int i = P.i, k = P.k;
+    Mpole<double> Mi = mpole64(rp10 + 10 * i), Mk = mpole64(rp10 + 10 * k);
+    V3<double> r = G.r, mr = (-1.0) * G.r;
+    V3<double> udi = ld3(ud, i), upi = ld3(up, i), udk = ld3(ud, k), upk = ld3(up, k);
+    SiteInv<double> si = invariants(Mi, r), sk = invariants(Mk, r);
+    SiteInv<double> si_m = invariants(Mi, mr), sk_m = invariants(Mk, mr);
+    V3<double> dEdr = v3<double>(0, 0, 0), tqi = v3<double>(0, 0, 0), tqk = v3<double>(0, 0, 0);
+    V3<double> d1, t1;
+    // d channel: (M_i, up_k) and (up_i, M_k)
+    md_pair<double>(Mi, si, upk, r, Bd, d1, t1);
+    dEdr = dEdr + d1;
+    tqi = tqi + t1;
+    md_pair<double>(Mk, sk_m, upi, mr, Bd, d1, t1);   // E(M_k, up_i) seen from k: dE/d(x_i - x_k)
+    dEdr = dEdr - d1;
+    tqk = tqk + t1;
+    // p channel: (M_i, ud_k) and (ud_i, M_k)
+    md_pair<double>(Mi, si, udk, r, Bp, d1, t1);
+    dEdr = dEdr + d1;
+    tqi = tqi + t1;
+    md_pair<double>(Mk, sk_m, udi, mr, Bp, d1, t1);
+    dEdr = dEdr - d1;
+    tqk = tqk + t1;
+    if (mutual) dEdr = dEdr + dd_pair<double>(upi, udk, r, Bu) + dd_pair<double>(udi, upk, r, Bu);
+    dEdr = 0.5 * dEdr;
+    add3(grad, i, (-f) * dEdr);
+    add3(grad, k, f * dEdr);
+    add3(trq, i, (0.5 * f) * tqi);
+    add3(trq, k, (0.5 * f) * tqk);
+}
+
+}  // namespace amg

@@ -1,0 +1,256 @@
+// kernels_setup.cuh -- per-evaluation set-up: frames (rotpole/chkpole),
+// cell binning, exact neighbour lists, B-spline stencils.
+#pragma once
+#include "kernels.cuh"
+
+namespace amg {
+
+// Local-to-global rotation of site i and the rotated multipole, following
+// the frame definitions of the reference's rotmat / rotsite
+// (src/md/rotpole.cpp:102-345, 356-425) and the chirality test of chkpole
+// (src/md/chkpole.cpp:44-89), applied without mutating the inputs.
+__device__ inline void frame_and_rotate(int i, const double* __restrict__ xyz, const double* __restrict__ pole13,
+                                        const int* __restrict__ zax, const int* __restrict__ xax,
+                                        const int* __restrict__ yax, const int* __restrict__ axe, double out[10]) {
+    using D = double;
+    auto P = [&](int a) { return v3<D>(xyz[3 * a], xyz[3 * a + 1], xyz[3 * a + 2]); };
+    auto unit = [](V3<D> v) { D s = 1.0 / sqrt(dot(v, v)); return s * v; };
+    double sp[13];
+    for (int j = 0; j < 13; j++) sp[j] = pole13[13 * i + j];
+    int ft = axe[i];
+    V3<D> xi = P(i);
+    V3<D> zv = v3<D>(0, 0, 1), xv = v3<D>(1, 0, 0);
+    bool planar = false;
+    if (ft == AMG_FRAME_ZTHENX && yax[i] != 0) {
+        int k = yax[i];
+        V3<D> a = xi, b = P(zax[i] - 1), c = P(xax[i] - 1), d = P(abs(k) - 1);
+        D vol = dot(a - d, cross(b - d, c - d));
+        if ((k < 0 && vol > 0) || (k > 0 && vol < 0)) {
+            sp[2] = -sp[2]; sp[5] = -sp[5]; sp[7] = -sp[7]; sp[9] = -sp[9]; sp[11] = -sp[11];
+        }
+    }
+    if (ft == AMG_FRAME_ZONLY) {
+        zv = unit(P(zax[i] - 1) - xi);
+        V3<D> t = fabs(zv.x) > 0.707 ? v3<D>(0, 1, 0) : v3<D>(1, 0, 0);
+        xv = unit(t - dot(t, zv) * zv);
+    } else if (ft == AMG_FRAME_ZTHENX) {
+        zv = unit(P(zax[i] - 1) - xi);
+        V3<D> t = P(xax[i] - 1) - xi;
+        xv = unit(t - dot(t, zv) * zv);
+    } else if (ft == AMG_FRAME_BISECTOR) {
+        V3<D> u1 = unit(P(zax[i] - 1) - xi), u2 = unit(P(xax[i] - 1) - xi);
+        zv = unit(u1 + u2);
+        xv = unit(u2 - dot(u2, zv) * zv);
+    } else if (ft == AMG_FRAME_ZBISECT) {
+        zv = unit(P(zax[i] - 1) - xi);
+        V3<D> u1 = unit(P(xax[i] - 1) - xi), u2 = unit(P(abs(yax[i]) - 1) - xi);
+        V3<D> b = unit(u1 + u2);
+        D angle = 180.0 - (180.0 / kPi) * acos(dot(b, zv));
+        if (angle < 0.0) {
+            planar = true;
+            b = cross(u1, u2);
+            if (dot(b, zv) < 0) b = (-1.0) * b;
+        }
+        xv = unit(b - dot(b, zv) * zv);
+    } else if (ft == AMG_FRAME_THREEFOLD) {
+        V3<D> u1 = unit(P(zax[i] - 1) - xi), u2 = unit(P(xax[i] - 1) - xi), u3 = unit(P(abs(yax[i]) - 1) - xi);
+        zv = unit(u1 + u2 + u3);
+        xv = unit(u1 - dot(u1, zv) * zv);
+    }
+    if (planar) {
+        sp[1] = 0; sp[6] = 0; sp[10] = 0;
+        sp[4] = sp[8] = 0.5 * (sp[4] + sp[8]);
+    }
+    V3<D> yv = cross(zv, xv);
+    D a[3][3] = {{xv.x, xv.y, xv.z}, {yv.x, yv.y, yv.z}, {zv.x, zv.y, zv.z}};
+    out[0] = sp[0];
+    for (int c = 0; c < 3; c++) out[1 + c] = sp[1] * a[0][c] + sp[2] * a[1][c] + sp[3] * a[2][c];
+    D qg[3][3];
+    for (int p = 0; p < 3; p++)
+        for (int q = p; q < 3; q++) {
+            D v = 0;
+            for (int r = 0; r < 3; r++)
+                for (int t = 0; t < 3; t++) v += a[r][p] * a[t][q] * sp[4 + 3 * r + t];
+            qg[p][q] = v;
+        }
+    out[4] = qg[0][0]; out[5] = qg[0][1]; out[6] = qg[0][2];
+    out[7] = qg[1][1]; out[8] = qg[1][2]; out[9] = qg[2][2];
+}
+
+template <class R>
+__global__ void k_rotate(int n, const double* __restrict__ xyz, const double* __restrict__ pole13,
+                         const int* __restrict__ zax, const int* __restrict__ xax, const int* __restrict__ yax,
+                         const int* __restrict__ axe, const double* __restrict__ pdamp,
+                         const double* __restrict__ thole, const double* __restrict__ pol,
+                         double* __restrict__ rp10, AtomR<R>* __restrict__ atoms) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double m[10];
+    frame_and_rotate(i, xyz, pole13, zax, xax, yax, axe, m);
+    for (int j = 0; j < 10; j++) rp10[10 * i + j] = m[j];
+    AtomR<R> A;
+    A.a = make_r4<R>((R)xyz[3 * i], (R)xyz[3 * i + 1], (R)xyz[3 * i + 2], (R)m[0]);
+    A.b = make_r4<R>((R)m[1], (R)m[2], (R)m[3], (R)m[4]);
+    A.c = make_r4<R>((R)m[5], (R)m[6], (R)m[7], (R)m[8]);
+    A.e = make_r4<R>((R)m[9], pdamp ? (R)pdamp[i] : R(0), thole ? (R)thole[i] : R(0), pol ? (R)pol[i] : R(0));
+    atoms[i] = A;
+}
+
+// ---------------------------------------------------------------- cells
+struct CellGrid {
+    int nc[3];          // cells per axis
+    double origin[3];   // lower corner (non-periodic) or 0
+    double size[3];     // cell edge
+    int periodic;
+    int off_lo[3], off_hi[3];  // distinct stencil offsets per axis
+};
+
+__global__ void k_cell_index(int n, const double* __restrict__ xyz, CellGrid cg, Box bx, unsigned* __restrict__ keys,
+                             int* __restrict__ ids) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int c[3];
+    for (int a = 0; a < 3; a++) {
+        double x = xyz[3 * i + a];
+        double f;
+        if (cg.periodic) {
+            f = x * bx.iL[a];
+            f -= floor(f);
+            c[a] = min(cg.nc[a] - 1, (int)(f * cg.nc[a]));
+        } else {
+            c[a] = min(cg.nc[a] - 1, max(0, (int)((x - cg.origin[a]) / cg.size[a])));
+        }
+    }
+    keys[i] = (unsigned)((c[0] * cg.nc[1] + c[1]) * cg.nc[2] + c[2]);
+    ids[i] = i;
+}
+
+// cell start/end of the sorted keys, and the coordinates in cell order
+__global__ void k_cell_bounds(int n, const unsigned* __restrict__ skeys, const int* __restrict__ sids,
+                              const double* __restrict__ xyz, int* __restrict__ start, int* __restrict__ end,
+                              double4* __restrict__ spos) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    unsigned k = skeys[i];
+    if (i == 0 || skeys[i - 1] != k) start[k] = i;
+    if (i == n - 1 || skeys[i + 1] != k) end[k] = i + 1;
+    int a = sids[i];
+    spos[i] = make_double4(xyz[3 * a], xyz[3 * a + 1], xyz[3 * a + 2], 0.0);
+}
+
+// Exact neighbour list: all j != i with minimum-image |r| <= cutoff, decided
+// in FP64 so the pair set is the same in both precisions, leaving out the
+// scaled (1-n / polarization-group) partners of i (xoff/xidx, CSR), which
+// the FP64 scaled-pair kernels evaluate.  One warp per site (sites taken in
+// cell order); the lanes scan a stencil cell together and compact the hits
+// with a ballot, so each list is in cell order, then index order.  Stored
+// site-major: nbr[i * cap + s].
+__global__ void k_neighbors(int n, const double4* __restrict__ spos, const unsigned* __restrict__ skeys,
+                            const int* __restrict__ sids, const int* __restrict__ cstart,
+                            const int* __restrict__ cend, CellGrid cg, Box bx, double cut2, int cap,
+                            const int* __restrict__ xoff, const int* __restrict__ xidx,
+                            int* __restrict__ nbr, int* __restrict__ nnb, int* __restrict__ overflow) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (w >= n) return;  // whole warps exit together
+    const int i = sids[w];
+    const unsigned key = skeys[w];
+    const int c2 = key % cg.nc[2];
+    const int c1 = (key / cg.nc[2]) % cg.nc[1];
+    const int c0 = key / (cg.nc[2] * cg.nc[1]);
+    const double4 pi = spos[w];
+    const int x0 = xoff[i], x1 = xoff[i + 1];
+    int* row = nbr + (size_t)i * cap;
+    int cnt = 0;
+    for (int dx = cg.off_lo[0]; dx <= cg.off_hi[0]; dx++) {
+        int q0 = c0 + dx;
+        if (cg.periodic) q0 = (q0 + cg.nc[0]) % cg.nc[0];
+        else if (q0 < 0 || q0 >= cg.nc[0]) continue;
+        for (int dy = cg.off_lo[1]; dy <= cg.off_hi[1]; dy++) {
+            int q1 = c1 + dy;
+            if (cg.periodic) q1 = (q1 + cg.nc[1]) % cg.nc[1];
+            else if (q1 < 0 || q1 >= cg.nc[1]) continue;
+            for (int dz = cg.off_lo[2]; dz <= cg.off_hi[2]; dz++) {
+                int q2 = c2 + dz;
+                if (cg.periodic) q2 = (q2 + cg.nc[2]) % cg.nc[2];
+                else if (q2 < 0 || q2 >= cg.nc[2]) continue;
+                const int cell = (q0 * cg.nc[1] + q1) * cg.nc[2] + q2;
+                const int s = cstart[cell], e = cend[cell];
+                for (int base = s; base < e; base += 32) {
+                    const int p = base + lane;
+                    bool hit = false;
+                    int j = -1;
+                    if (p < e) {
+                        j = sids[p];
+                        double4 pj = spos[p];
+                        double rx = wrap1<double>(pj.x - pi.x, bx.L[0], bx.iL[0]);
+                        double ry = wrap1<double>(pj.y - pi.y, bx.L[1], bx.iL[1]);
+                        double rz = wrap1<double>(pj.z - pi.z, bx.L[2], bx.iL[2]);
+                        hit = j != i && rx * rx + ry * ry + rz * rz <= cut2;
+                        if (hit)
+                            for (int q = x0; q < x1; q++) hit &= (xidx[q] != j);
+                    }
+                    unsigned m = __ballot_sync(0xffffffffu, hit);
+                    if (hit) {
+                        int pos = cnt + __popc(m & ((1u << lane) - 1u));
+                        if (pos < cap) row[pos] = j;
+                    }
+                    cnt += __popc(m);
+                }
+            }
+        }
+    }
+    if (lane == 0) {
+        nnb[i] = min(cnt, cap);
+        if (cnt > cap) atomicMax(overflow, cnt);
+    }
+}
+
+// ---------------------------------------------------------------- B-splines
+// Cardinal B-spline weights of order P at the P grid points starting at
+// floor(u) - P + 1, and their first three derivatives (Essmann et al. 1995):
+//   b_n[s] = ((w + n - 1 - s) b_{n-1}[s-1] + (s + 1 - w) b_{n-1}[s]) / (n - 1)
+// with w = u - floor(u); derivatives from the lower orders by differences.
+template <class R, int P>
+__device__ __forceinline__ void bspline_weights(double w, R (&th)[4][P]) {
+    double b[P + 1][P];
+    for (int n = 0; n <= P; n++)
+        for (int s = 0; s < P; s++) b[n][s] = 0.0;
+    b[1][0] = 1.0;
+    for (int n = 2; n <= P; n++)
+        for (int s = 0; s < n; s++) {
+            double lo = s >= 1 ? b[n - 1][s - 1] : 0.0;
+            double hi = s < n - 1 ? b[n - 1][s] : 0.0;
+            b[n][s] = ((w + n - 1 - s) * lo + (s + 1 - w) * hi) / (n - 1);
+        }
+    auto B = [&](int n, int s) { return (s >= 0 && s < n) ? b[n][s] : 0.0; };
+    for (int s = 0; s < P; s++) {
+        th[0][s] = (R)b[P][s];
+        th[1][s] = (R)(B(P - 1, s - 1) - B(P - 1, s));
+        th[2][s] = (R)(B(P - 2, s - 2) - 2 * B(P - 2, s - 1) + B(P - 2, s));
+        th[3][s] = (R)(B(P - 3, s - 3) - 3 * B(P - 3, s - 2) + 3 * B(P - 3, s - 1) - B(P - 3, s));
+    }
+}
+
+template <class R, int P>
+__global__ void k_bspline(int n, const double* __restrict__ xyz, Box bx, int3 K, R* __restrict__ theta,
+                          int* __restrict__ k0) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int Ks[3] = {K.x, K.y, K.z};
+    for (int a = 0; a < 3; a++) {
+        double f = xyz[3 * i + a] * bx.iL[a];
+        f -= floor(f);
+        double u = f * Ks[a];
+        double fl = floor(u);
+        R th[4][P];
+        bspline_weights<R, P>(u - fl, th);
+        int start = (int)fl - P + 1;
+        if (start < 0) start += Ks[a];
+        k0[3 * i + a] = start;
+        R* o = theta + ((size_t)i * 3 + a) * 4 * P;
+        for (int d = 0; d < 4; d++)
+            for (int s = 0; s < P; s++) o[d * P + s] = th[d][s];
+    }
+}
+
+}  // namespace amg

@@ -154,6 +154,14 @@ class Engine:
         self._check(self.lib.amg_forward(self.ctx, flags, C.byref(r)), "amg_forward")
         return collect(r, bufs, self.n)
 
+    def forward_into(self, flags, dem=None, dep=None):
+        """amg_forward writing only the given gradient buffers (added to);
+        returns (em, ep, pcg_iters, pcg_eps)."""
+        r = abi.amg_results()
+        r.dem, r.dep = abi.dptr(dem), abi.dptr(dep)
+        self._check(self.lib.amg_forward(self.ctx, flags, C.byref(r)), "amg_forward")
+        return r.em, r.ep, r.pcg_iters, r.pcg_eps
+
     def backward(self, d_energy=1.0, d_uind=None, d_uinp=None):
         cot = abi.amg_cotangents(d_energy, abi.dptr(d_uind), abi.dptr(d_uinp))
         out = {"d_pole": np.zeros(13 * self.n), "d_polarity": np.zeros(self.n),
@@ -163,6 +171,21 @@ class Engine:
         out["d_pole"] = out["d_pole"].reshape(self.n, 13)
         out["d_xyz"] = out["d_xyz"].reshape(self.n, 3)
         return out
+
+    def bench(self, steps, flags=abi.DO_ENERGY | abi.DO_GRADIENT, flush_bytes=0):
+        """Device-resident evaluations: per-step ms (CUDA events) and the
+        number of this library's kernel launches."""
+        ms = np.zeros(steps)
+        launches = C.c_int64(0)
+        self._check(self.lib.amg_bench(self.ctx, flags, steps, flush_bytes, abi.dptr(ms), C.byref(launches)),
+                    "amg_bench")
+        return ms, int(launches.value)
+
+    def stats(self):
+        launches, graphed, lpa = C.c_int64(0), C.c_int32(0), C.c_int32(0)
+        self._check(self.lib.amg_last_stats(self.ctx, C.byref(launches), C.byref(graphed), C.byref(lpa)),
+                    "amg_last_stats")
+        return {"launches": int(launches.value), "graphed": bool(graphed.value), "lanes_per_site": int(lpa.value)}
 
     def timing(self):
         ms = np.zeros(5)

@@ -1,0 +1,249 @@
+"""Parity of the CUDA path (called through the C ABI) with the reference's
+golden vectors and with the FP64 oracle.
+
+Tolerances:
+  FP64 path vs oracle/reference: energies 1e-10 relative (reference goldens
+    at their own eps, 1e-10 / 1e-8), gradients 1e-8 absolute without
+    polarization; with polarization the PCG tolerance sets the floor
+    (dipoles converged to 1e-8 D: gradients 1e-5, ep 1e-8 relative).
+  mixed path (FP32 pairs/grids): |em - em_ref| / |em_ref| < 1e-6,
+    |ep - ep_ref| / |ep_ref| < 1e-6, force RMS < 1e-4 kcal/mol/A, as the
+    accuracy target of the mixed-precision design states.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden, ref_dump, ref_fixture
+from oracle import oracle
+from polmdqc_b200 import abi, systems
+from polmdqc_b200.engine import AmgError, Engine, Settings
+
+pytestmark = pytest.mark.gpu
+
+FP64, MIXED = abi.PREC_FP64, abi.PREC_MIXED
+ALL = abi.DO_ENERGY | abi.DO_GRADIENT | abi.DO_DIPOLES
+
+
+def rel(a, b):
+    return abs(a - b) / max(abs(b), 1e-300)
+
+
+def frms(g, o):
+    return float(np.sqrt(np.mean((g.dem + g.dep - o.dem - o.dep) ** 2)))
+
+
+def run(s, st, flags=ALL):
+    e = Engine(s, st)
+    try:
+        return e.forward(flags)
+    finally:
+        e.close()
+
+
+# ---------------------------------------------------------------- reference goldens
+@pytest.mark.parametrize("prec", [FP64, MIXED])
+def test_water_dimer_golden(prec):
+    """test/amoeba.cpp amoeba-1/-2 through the C ABI (non-Ewald multipoles)."""
+    g = golden("ref_tests.json")
+    d = ref_dump(ref_fixture("amoeba", "water09.xyz"))
+    s = systems.from_dump(d)
+    st = Settings(use_ewald=False, cutoff=d["mpolecut"], poltyp=abi.POL_NONE, precision=prec)
+    r = run(s, st, abi.DO_ENERGY | abi.DO_GRADIENT | abi.DO_ANALYSIS)
+    a1, a2 = g["amoeba1"], g["amoeba2"]
+    tol_e = a1["eps"] if prec == FP64 else 2e-6 * abs(a1["em"])
+    tol_g = a2["eps1"] if prec == FP64 else 1e-4
+    assert r.nem == a1["nem"]
+    assert abs(r.em - a1["em"]) < tol_e
+    assert abs(r.einter - a1["einter"]) < tol_e
+    np.testing.assert_allclose(r.aem, a1["aem"], atol=tol_e, rtol=0)
+    np.testing.assert_allclose(r.dem.reshape(-1), a2["dem"], atol=tol_g, rtol=0)
+
+
+def test_waterbox30_orthogonal_golden():
+    """test/bounds.cpp bounds-1: periodic 2,700 atoms, cutoff 9, em/nem/einter."""
+    g = golden("ref_tests.json")["bounds1"]
+    d = ref_dump(ref_fixture("bounds", "waterbox30.xyz"), ref_fixture("bounds", "orthogonal.key"))
+    s = systems.from_dump(d)
+    st = Settings(use_ewald=False, cutoff=d["mpolecut"], poltyp=abi.POL_NONE, precision=FP64)
+    r = run(s, st, abi.DO_ENERGY | abi.DO_GRADIENT | abi.DO_ANALYSIS)
+    assert r.nem == g["nem"]
+    assert abs(r.em - g["em"]) < g["eps"]
+    assert abs(r.einter - g["einter"]) < g["eps"]
+    np.testing.assert_allclose(r.dem.reshape(-1), d["dem"], atol=1e-8, rtol=0)
+
+
+def test_synthetic_box_matches_reference_run():
+    """Seeded 216-water box: the compiled reference's em/nem/dem (non-Ewald, 7 A)."""
+    d = golden("ref_water216.json")
+    s = systems.water_box(216, 18.643, seed=0)
+    s.xyz = np.stack([d["x"], d["y"], d["z"]], 1)
+    st = Settings(use_ewald=False, cutoff=d["mpolecut"], poltyp=abi.POL_NONE, precision=FP64)
+    r = run(s, st, abi.DO_ENERGY | abi.DO_GRADIENT | abi.DO_ANALYSIS)
+    assert r.nem == d["nem"]
+    assert rel(r.em, d["em"]) < 1e-10
+    np.testing.assert_allclose(r.dem.reshape(-1), d["dem"], atol=1e-8, rtol=0)
+
+
+# ---------------------------------------------------------------- oracle (Ewald + polarization)
+@pytest.fixture(scope="module")
+def w216():
+    return systems.water_box(216, 18.643, seed=0)
+
+
+@pytest.fixture(scope="module")
+def w216_oracle(w216):
+    st = Settings(nfft=(24, 24, 24), precision=FP64)
+    return oracle.forward(w216, st, tol=1e-11)
+
+
+def test_fp64_matches_oracle(w216, w216_oracle):
+    o = w216_oracle
+    g = run(w216, Settings(nfft=(24, 24, 24), precision=FP64, poleps=1e-8))
+    assert rel(g.em, o.em) < 1e-10
+    assert rel(g.ep, o.ep) < 1e-8
+    assert np.abs(g.dem - o.dem).max() < 1e-8
+    assert np.abs(g.dep - o.dep).max() < 1e-5
+    assert np.abs(g.uind - o.uind).max() < 1e-7
+    assert np.abs(g.uinp - o.uinp).max() < 1e-7
+    assert g.pcg_eps <= 1e-8
+
+
+def test_mixed_meets_accuracy_target(w216, w216_oracle):
+    o = w216_oracle
+    g = run(w216, Settings(nfft=(24, 24, 24), precision=MIXED))
+    assert rel(g.em, o.em) < 1e-6
+    assert rel(g.ep, o.ep) < 1e-6
+    assert frms(g, o) < 1e-4
+    assert g.pcg_eps <= 1e-6
+
+
+def test_multipoles_only_and_direct_polarization(w216):
+    for pol in (abi.POL_NONE, abi.POL_DIRECT):
+        st = Settings(nfft=(24, 24, 24), precision=FP64, poltyp=pol)
+        o = oracle.forward(w216, st)
+        g = run(w216, st)
+        assert rel(g.em, o.em) < 1e-10
+        if pol == abi.POL_DIRECT:
+            assert rel(g.ep, o.ep) < 1e-10
+            assert np.abs(g.dep - o.dep).max() < 1e-8
+        assert np.abs(g.dem - o.dem).max() < 1e-8
+
+
+def test_non_ewald_polarization_matches_oracle():
+    """Reference mode (no Ewald, finite cutoff) with mutual polarization."""
+    s = systems.water_box(64, 12.4, seed=5)
+    st = Settings(use_ewald=False, cutoff=6.0, precision=FP64, poleps=1e-9)
+    o = oracle.forward(s, st, tol=1e-11)
+    g = run(s, st)
+    assert rel(g.em, o.em) < 1e-10
+    assert rel(g.ep, o.ep) < 1e-8
+    assert np.abs(g.dep - o.dep).max() < 1e-5
+
+
+@pytest.mark.parametrize("prec", [FP64, MIXED])
+def test_ion_solution_matches_oracle(prec):
+    """amoebabio18 waters + Na+/Cl- (frame-less sites, large polarizability)."""
+    s = systems.ion_solution(n_waters=250, n_pairs=3, box_len=20.0, seed=4)
+    st = Settings(nfft=(25, 25, 25), precision=FP64)
+    o = oracle.forward(s, st, tol=1e-11)
+    g = run(s, Settings(nfft=(25, 25, 25), precision=prec, poleps=1e-8 if prec == FP64 else 1e-6))
+    if prec == FP64:
+        assert rel(g.em, o.em) < 1e-10 and rel(g.ep, o.ep) < 1e-8
+        assert np.abs(g.dem + g.dep - o.dem - o.dep).max() < 1e-5
+    else:
+        assert rel(g.em, o.em) < 1e-6 and rel(g.ep, o.ep) < 1e-6
+        assert frms(g, o) < 1e-4
+
+
+def test_gradients_match_finite_differences():
+    """GPU FP64 gradients vs central differences of GPU energies."""
+    s = systems.water_box(27, 9.32, seed=3)
+    st = Settings(aewald=0.7, nfft=(24, 24, 24), cutoff=4.6, precision=FP64, poleps=1e-10)
+    e = Engine(s, st)
+    try:
+        r = e.forward()
+        h = 1e-5
+        for (i, a) in ((0, 0), (2, 1), (40, 2)):
+            x = s.xyz.copy()
+            x[i, a] += h
+            e.set_coords(x)
+            p = e.forward(abi.DO_ENERGY)
+            x[i, a] -= 2 * h
+            e.set_coords(x)
+            m = e.forward(abi.DO_ENERGY)
+            assert abs((p.em - m.em) / (2 * h) - r.dem[i, a]) < 1e-6
+            assert abs((p.ep - m.ep) / (2 * h) - r.dep[i, a]) < 1e-5
+    finally:
+        e.close()
+
+
+# ---------------------------------------------------------------- benchmark sizes
+@pytest.fixture(scope="module")
+def w4096():
+    return systems.water_box(4096, 49.7, seed=0)
+
+
+def test_config_4096_waters_vs_oracle(w4096):
+    """The benchmark workload (4,096 waters, 54^3 grid): FP64 GPU vs oracle,
+    mixed GPU vs FP64 GPU at the accuracy target."""
+    st = Settings(nfft=(54, 54, 54), precision=FP64, poleps=1e-8)
+    o = oracle.forward(w4096, st, tol=1e-10)
+    g64 = run(w4096, st)
+    assert rel(g64.em, o.em) < 1e-10 and rel(g64.ep, o.ep) < 1e-8
+    assert np.abs(g64.dem + g64.dep - o.dem - o.dep).max() < 1e-5
+    gm = run(w4096, Settings(nfft=(54, 54, 54), precision=MIXED))
+    assert rel(gm.em, o.em) < 1e-6 and rel(gm.ep, o.ep) < 1e-6
+    assert frms(gm, o) < 1e-4
+
+
+def test_config_32768_waters_properties():
+    """98,304 atoms, 108^3 grid: mixed vs FP64 on the GPU at the target error,
+    net force ~ 0, and translation invariance."""
+    s = systems.water_box(32768, 99.3, seed=0)
+    g64 = run(s, Settings(nfft=(108, 108, 108), precision=FP64))
+    gm = run(s, Settings(nfft=(108, 108, 108), precision=MIXED))
+    assert gm.pcg_eps <= 1e-6 and g64.pcg_eps <= 1e-6
+    assert rel(gm.em, g64.em) < 1e-6 and rel(gm.ep, g64.ep) < 1e-6
+    assert frms(gm, g64) < 1e-4
+    net = (g64.dem + g64.dep).sum(0)
+    assert np.abs(net).max() < 1e-3 * np.abs(g64.dem + g64.dep).max()
+    shifted = systems.water_box(32768, 99.3, seed=0)
+    shifted.xyz = shifted.xyz + np.array([0.37, -1.21, 2.5])
+    gs = run(shifted, Settings(nfft=(108, 108, 108), precision=FP64))
+    # PME is not exactly translation invariant; the drift is far below the target
+    assert rel(gs.em + gs.ep, g64.em + g64.ep) < 1e-6
+
+
+# ---------------------------------------------------------------- status codes
+def test_status_codes():
+    s = systems.water_box(64, 12.4, seed=5)
+    with pytest.raises(AmgError, match="NO_CONVERGE"):
+        run(s, Settings(nfft=(16, 16, 16), cutoff=6.0, politer=1, poleps=1e-9))
+    bad = systems.water_box(8, 10.0, seed=0)
+    with pytest.raises(AmgError, match="BAD_ARG"):
+        run(bad, Settings(nfft=(16, 16, 16), cutoff=7.0))   # cutoff > box/2
+    e = Engine(s, Settings(nfft=(16, 16, 16), cutoff=6.0))
+    try:
+        x = s.xyz.copy()
+        x[3, 1] = np.nan
+        with pytest.raises(AmgError, match="NAN"):
+            e.set_coords(x)
+    finally:
+        e.close()
+
+
+def test_repeated_calls_reuse_the_captured_graph(w216):
+    e = Engine(w216, Settings(nfft=(24, 24, 24), precision=MIXED))
+    try:
+        a = e.forward()
+        b = e.forward()
+        x = w216.xyz + 0.01
+        e.set_coords(x)
+        c = e.forward()
+        e.set_coords(w216.xyz)
+        d = e.forward()
+    finally:
+        e.close()
+    assert rel(a.em, b.em) < 1e-12 and rel(a.ep, b.ep) < 1e-12
+    assert rel(a.em + a.ep, c.em + c.ep) > 1e-9
+    assert rel(a.em, d.em) < 1e-12 and np.abs(a.dep - d.dep).max() < 1e-9

@@ -1,0 +1,75 @@
+"""Internal consistency of the oracle's restatement of the parts the reference
+does not implement (Ewald real space, PME, self terms, induced dipoles,
+polarization forces): the checks that pin it in place of golden vectors."""
+import copy
+
+import numpy as np
+import pytest
+
+from oracle import oracle
+from polmdqc_b200 import abi, systems
+from polmdqc_b200.engine import Settings
+
+
+@pytest.fixture(scope="module")
+def box27():
+    return systems.water_box(27, 9.32, seed=3)
+
+
+def test_pme_converges_to_explicit_ewald_sum(box27):
+    """PME (B-splines, order 5) -> explicit k-space sum as the grid is refined,
+    for charges, dipoles and quadrupoles separately."""
+    for mask in ([0], [1, 2, 3], list(range(4, 13))):
+        s = copy.deepcopy(box27)
+        keep = np.zeros(13, bool)
+        keep[mask] = True
+        s.pole = s.pole * keep
+        st = Settings(aewald=0.7, nfft=(64, 64, 64), cutoff=4.6, poltyp=abi.POL_NONE)
+        ek = oracle.forward(s, st, flags=abi.DO_ENERGY, kmax=9.0).em
+        ep = oracle.forward(s, st, flags=abi.DO_ENERGY).em
+        assert abs(ep - ek) < 2e-5 * abs(ek) + 2e-5
+
+
+def test_ewald_total_independent_of_alpha():
+    """With converged real-space cutoff and reciprocal sum, em does not depend on alpha."""
+    s = systems.water_box(216, 18.643, seed=0)
+    vals = []
+    for a in (0.55, 0.6, 0.65):
+        st = Settings(aewald=a, nfft=(24, 24, 24), cutoff=9.0, poltyp=abi.POL_NONE)
+        vals.append(oracle.forward(s, st, flags=abi.DO_ENERGY, kmax=7.0).em)
+    assert max(vals) - min(vals) < 2e-6 * abs(vals[0])
+
+
+@pytest.mark.parametrize("ewald", [True, False])
+def test_forces_match_finite_differences(box27, ewald):
+    """Analytic em/ep gradients (real, reciprocal, self, torques, mutual dipoles)
+    against central differences of the energies (the reference's testgrad
+    pattern, src/md/testgrad.cpp:273-333)."""
+    s = copy.deepcopy(box27)
+    if not ewald:
+        s.use_bounds = False
+    st = (Settings(aewald=0.7, nfft=(24, 24, 24), cutoff=4.6, poleps=1e-11) if ewald
+          else Settings(use_ewald=False, cutoff=100.0, poleps=1e-11))
+    r = oracle.forward(s, st)
+    h = 1e-5
+    for (i, a) in ((0, 0), (1, 2), (40, 1), (77, 2)):
+        x = s.xyz.copy()
+        x[i, a] += h
+        p = oracle.forward(s, st, xyz=x, flags=abi.DO_ENERGY)
+        x[i, a] -= 2 * h
+        m = oracle.forward(s, st, xyz=x, flags=abi.DO_ENERGY)
+        assert abs((p.em - m.em) / (2 * h) - r.dem[i, a]) < 1e-6
+        assert abs((p.ep - m.ep) / (2 * h) - r.dep[i, a]) < 1e-6
+
+
+def test_dipoles_solve_the_linear_system(box27):
+    """Converged PCG dipoles satisfy (1/alpha) u - T u = E: the direct
+    polarization model gives u = alpha E exactly, and the mutual solution's
+    energy is stationary (a perturbed solve changes ep at second order)."""
+    st = Settings(aewald=0.7, nfft=(24, 24, 24), cutoff=4.6, poleps=1e-12)
+    r = oracle.forward(box27, st)
+    assert r.pcg_eps < 1e-12
+    loose = oracle.forward(box27, Settings(aewald=0.7, nfft=(24, 24, 24), cutoff=4.6, poleps=1e-5), check=False)
+    assert abs(loose.ep - r.ep) < 1e-3 * abs(r.ep)
+    d = oracle.forward(box27, Settings(aewald=0.7, nfft=(24, 24, 24), cutoff=4.6, poltyp=abi.POL_DIRECT))
+    assert d.pcg_iters == 0 and d.ep != 0

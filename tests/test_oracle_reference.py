@@ -1,0 +1,74 @@
+"""The FP64 oracle against the reference's own golden vectors and against the
+compiled reference run on the seeded synthetic box (non-Ewald multipoles,
+the only electrostatics mode the reference implements)."""
+import numpy as np
+import pytest
+
+from conftest import golden, ref_dump, ref_fixture
+from oracle import oracle
+from polmdqc_b200 import abi, systems
+from polmdqc_b200.engine import Settings
+
+
+def nonewald(cut):
+    return Settings(use_ewald=False, cutoff=cut, poltyp=abi.POL_NONE)
+
+
+def test_water_dimer_golden():
+    """test/amoeba.cpp amoeba-1/-2: em, aem, nem, einter at 1e-10; analytic dem at 1e-10."""
+    g = golden("ref_tests.json")
+    d = ref_dump(ref_fixture("amoeba", "water09.xyz"))
+    s = systems.from_dump(d)
+    r = oracle.forward(s, nonewald(d["mpolecut"]), flags=abi.DO_ENERGY | abi.DO_GRADIENT | abi.DO_ANALYSIS)
+    a1, a2 = g["amoeba1"], g["amoeba2"]
+    assert abs(r.em - a1["em"]) < a1["eps"]
+    assert abs(r.einter - a1["einter"]) < a1["eps"]
+    assert r.nem == a1["nem"]
+    np.testing.assert_allclose(r.aem, a1["aem"], atol=a1["eps"], rtol=0)
+    np.testing.assert_allclose(r.dem.reshape(-1), a2["dem"], atol=a2["eps1"], rtol=0)
+
+
+def test_waterbox30_orthogonal_golden():
+    """test/bounds.cpp bounds-1: 2,700-atom periodic box, cutoff 9, em and nem at 1e-8."""
+    g = golden("ref_tests.json")["bounds1"]
+    d = ref_dump(ref_fixture("bounds", "waterbox30.xyz"), ref_fixture("bounds", "orthogonal.key"))
+    s = systems.from_dump(d)
+    r = oracle.forward(s, nonewald(d["mpolecut"]), flags=abi.DO_ENERGY | abi.DO_GRADIENT | abi.DO_ANALYSIS)
+    assert r.nem == g["nem"]
+    assert abs(r.em - g["em"]) < g["eps"]
+    assert abs(r.einter - g["einter"]) < g["eps"]
+    np.testing.assert_allclose(r.dem.reshape(-1), d["dem"], atol=1e-9, rtol=0)
+
+
+def test_synthetic_box_matches_reference_run():
+    """216-water seeded box: oracle = compiled reference (em, nem, dem, rpole)."""
+    d = golden("ref_water216.json")
+    s = systems.water_box(216, 18.643, seed=0)
+    s.xyz = np.stack([d["x"], d["y"], d["z"]], 1)   # the coordinates the reference read
+    r = oracle.forward(s, nonewald(d["mpolecut"]), flags=abi.DO_ENERGY | abi.DO_GRADIENT | abi.DO_ANALYSIS)
+    assert r.nem == d["nem"]
+    assert abs(r.em - d["em"]) < 1e-9 * abs(d["em"])
+    np.testing.assert_allclose(r.dem.reshape(-1), d["dem"], atol=1e-9, rtol=0)
+    np.testing.assert_allclose(r.rpole.reshape(-1)[: len(d["rpole"])], d["rpole"], atol=1e-13, rtol=0)
+
+
+@pytest.mark.parametrize("name", ["water03", "amoebabio18"])
+def test_parameter_assignment_matches_reference(name):
+    """systems.* assigns the same pole/frames/polarizabilities/groups as the
+    reference's mechanic() (kmpole, kpolar, polargrp) for the synthetic inputs."""
+    p = golden("ref_params.json")[name]
+    s = (systems.water_box(27, 9.32, seed=1) if name == "water03"
+         else systems.ion_solution(n_waters=60, n_pairs=2, box_len=14.0, seed=2))
+    idx = p["atoms"]
+    assert s.n == p["n"]
+    np.testing.assert_allclose(s.pole[idx], p["pole"], atol=1e-15)
+    for k in ("zaxis", "xaxis", "yaxis", "polaxe", "molcule"):
+        np.testing.assert_array_equal(getattr(s, k)[idx], p[k], err_msg=k)
+    for k in ("polarity", "thole", "pdamp"):
+        np.testing.assert_allclose(getattr(s, k)[idx], p[k], rtol=1e-14, err_msg=k)
+    for k in ("i12", "i13", "ip11", "ip12"):
+        assert [sorted(s.lists[k][i]) for i in idx] == [sorted(v) for v in p[k]], k
+    for k, ref in (("m_scale", "mscale"), ("p_scale", "pscale"), ("p_iscale", "piscale"), ("d_scale", "dscale"),
+                   ("u_scale", "uscale")):
+        assert getattr(s, k) == p[ref], k
+    assert p["aeewald"] == 0.5446 and p["nefft"] == [24, 24, 24] and p["bseorder"] == 5

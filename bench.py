@@ -190,15 +190,38 @@ def main():
     e2e = {"value": world * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 8 * 3 * n + 8 * 6,
            "d2h_bytes_per_step": 8 * 2 * 3 * n + 8 * (8 + 8 + 4) + 4 * 2}
 
+    # dominant kernel of ours: the PCG's stored-coefficient T.u (HBM-bound once
+    # L2 is flushed), timed live with CUDA events on the library's stream
+    tu_ms, tu_bytes, tu_pairs = eng.time_tu_kernel(reps=20, flush_bytes=FLUSH_BYTES)
+
+    # the same workload in plain FP64 on the GPU: speed and the mixed path's error
+    st64 = Settings(nfft=(GRID,) * 3, precision=abi.PREC_FP64, device=local)
+    e64 = Engine(s, st64)
+    ms64, _ = e64.bench(max(3, args.steps // 2), flags, FLUSH_BYTES)
+    r64 = e64.forward(flags)
+    rmx = eng.forward(flags)
+    e64.close()
+    fp64_value = world * len(ms64) / max_over_ranks(float(np.sum(ms64)) / 1000.0)
+    err = {"em_rel": abs(rmx.em - r64.em) / abs(r64.em), "ep_rel": abs(rmx.ep - r64.ep) / abs(r64.ep),
+           "force_rms_kcal_mol_A": float(np.sqrt(np.mean((rmx.dem + rmx.dep - r64.dem - r64.dep) ** 2))),
+           "pcg_eps_D": rmx.pcg_eps, "reference": "FP64 GPU path (matches the FP64 CPU oracle to 1e-10 in em)"}
+
     if rank == 0:
         peaks, src = load_peaks()
+        achieved = tu_bytes / (tu_ms * 1e-3) / 1e9
+        roofline = {"kernel": "k_tu_stored (PCG real-space T.u, stored pair coefficients)", "bound": "hbm",
+                    "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                    "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                    "bytes_per_launch": tu_bytes, "directed_pairs": tu_pairs, "avg_launch_ms": tu_ms,
+                    "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({src}); L2 flushed before each timed launch"}
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": 1000.0 * dev_s / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64 (mixed)", "data": "synthetic (seeded water box)",
                 "config": workload_config(), "e2e": e2e, "gpu_launches": launches, "clocks": clk,
                 "pcg_iterations": int(statistics.median(iters)), "em": em, "ep": ep,
                 "ns_per_day": {"dt_1fs": value * 86400 * 1e-6, "dt_2fs": value * 86400 * 2e-6},
-                "peaks_source": src}
+                "roofline": roofline, "fp64_gpu_value": fp64_value, "mixed_over_fp64": value / fp64_value,
+                "mixed_error_vs_fp64": err}
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_oracle(seed=0)
         print(json.dumps(line), flush=True)

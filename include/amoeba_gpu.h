@@ -193,6 +193,14 @@ int amg_last_timing(amg_ctx* ctx, double ms[5]);
 int amg_bench(amg_ctx* ctx, int32_t flags, int32_t steps, int64_t flush_bytes, double* ms_steps,
               int64_t* launches);
 
+/* Benchmark support (no counterpart in the reference): average device time
+ * of the PCG's real-space T.u kernel run on its own (`reps` launches, each
+ * after writing flush_bytes to evict L2), with its algorithmic bytes per
+ * launch and the number of directed pairs it processes.  Needs a previous
+ * amg_forward with mutual polarization. */
+int amg_time_tu_kernel(amg_ctx* ctx, int32_t reps, int64_t flush_bytes, double* ms_avg, double* bytes_per_launch,
+                       int64_t* directed_pairs);
+
 /* Kernel launches of the last amg_forward, whether it ran as one captured
  * CUDA graph, and the lanes per site of the pair kernels. */
 int amg_last_stats(amg_ctx* ctx, int64_t* launches, int32_t* graphed, int32_t* lanes_per_site);

@@ -23,10 +23,18 @@ MD_SRC  = $(filter-out %Exe $(EXCLUDE),$(MD_ALL))
 OBJS    = $(addprefix $(OUT)/obj/md_,$(addsuffix .o,$(MD_SRC))) \
           $(OUT)/obj/mod.o $(OUT)/obj/promo.o $(OUT)/obj/rootdir.o $(OUT)/obj/finalqm.o
 
-# The library without empole.o / energy.o is what the drop-in shim links against.
-CORE_OBJS = $(filter-out $(OUT)/obj/md_empole.o $(OUT)/obj/md_energy.o,$(OBJS))
+# The library without empole.o is what the drop-in shim
+# (polmdqc_b200/host/polmdqc_shim.cpp) links against.
+CORE_OBJS = $(filter-out $(OUT)/obj/md_empole.o,$(OBJS))
+GPULIB    = polmdqc_b200/_lib/libamoeba_gpu.so
+SHIM      = polmdqc_b200/host/polmdqc_shim.cpp
 
-all: $(OUT)/libpolmdqc.a $(OUT)/libpolmdqc_core.a $(OUT)/ref_dump $(OUT)/data.stamp
+all: $(OUT)/libpolmdqc.a $(OUT)/libpolmdqc_noempole.a $(OUT)/ref_dump $(OUT)/data.stamp
+
+# The reference's own programs with the shim in place of empole.o: the
+# drop-in demonstration (analyze_gpu, testgrad_gpu) and ref_dump_gpu, the
+# dump driver running the same path on the GPU (used by the GPU tests).
+shim: $(OUT)/ref_dump_gpu $(OUT)/analyze_gpu $(OUT)/testgrad_gpu
 
 $(OUT)/obj/md_%.o: $(REF)/src/md/%.cpp
 	@mkdir -p $(dir $@)
@@ -48,8 +56,20 @@ $(OUT)/obj/finalqm.o: $(REF)/src/qc/finalqm.cpp
 $(OUT)/libpolmdqc.a: $(OBJS)
 	rm -f $@ && ar rcs $@ $^
 
-$(OUT)/libpolmdqc_core.a: $(CORE_OBJS)
+$(OUT)/libpolmdqc_noempole.a: $(CORE_OBJS)
 	rm -f $@ && ar rcs $@ $^
+
+SHIMFLAGS = $(FLAGS) -Iinclude $(SHIM) $(OUT)/libpolmdqc_noempole.a -Lpolmdqc_b200/_lib -lamoeba_gpu \
+            -Wl,-rpath,'$$ORIGIN/../../polmdqc_b200/_lib'
+
+$(OUT)/ref_dump_gpu: oracle/ref_dump.cpp $(SHIM) $(OUT)/libpolmdqc_noempole.a $(GPULIB)
+	$(REFCXX) $(INC) oracle/ref_dump.cpp $(SHIMFLAGS) -o $@
+
+$(OUT)/analyze_gpu: $(REF)/src/md/analyzeExe.cpp $(SHIM) $(OUT)/libpolmdqc_noempole.a $(GPULIB)
+	$(REFCXX) $(INC) $< $(SHIMFLAGS) -o $@
+
+$(OUT)/testgrad_gpu: $(REF)/src/md/testgradExe.cpp $(SHIM) $(OUT)/libpolmdqc_noempole.a $(GPULIB)
+	$(REFCXX) $(INC) $< $(SHIMFLAGS) -o $@
 
 # ref_dump: our own driver (oracle/ref_dump.cpp) around the reference library;
 # runs initial/getcart/mechanic/energy and prints the globals as JSON.
@@ -64,4 +84,4 @@ $(OUT)/data.stamp: $(wildcard $(REF)/params/*.prm)
 	cp -r $(REF)/test/testFiles/amoeba $(REF)/test/testFiles/bounds $(REF)/test/testFiles/rotpole $(OUT)/testFiles/
 	touch $@
 
-.PHONY: all
+.PHONY: all shim

@@ -103,7 +103,7 @@ int main(int argc, char** argv)
     mechanic();
 
     energy<CalcMode::Analysis>();
-    double em_a = em, einter_a = einter;
+    double em_a = em, einter_a = einter, ep_a = ep;
     int nem_a = nem;
     std::vector<double> aem_a(n);
     for (int i = 0; i < n; i++) aem_a[i] = aem[i];
@@ -178,6 +178,12 @@ int main(int argc, char** argv)
     darr("aem", n, [&](int i) { return aem_a[i]; });
     num("em_virial_call", em);
     darr("dem", 3 * n, [](int i) { return dem[i]; });
+    num("ep", ep_a);
+    if (have_pol) {
+        darr("dep", 3 * n, [](int i) { return dep[i]; });
+        darr("uind", 3 * n, [](int i) { return uind[i / 3][i % 3]; });
+        darr("uinp", 3 * n, [](int i) { return uinp[i / 3][i % 3]; });
+    }
     darr("vir", 9, [](int i) { return vir[i / 3][i % 3]; });
     fputs("\n}\n", fo);
     if (fo != stdout) fclose(fo);

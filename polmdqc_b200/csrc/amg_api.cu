@@ -67,7 +67,8 @@ struct CufftTypes<double> {
 template <class R>
 struct Pme {
     bool ready = false;
-    R* grid = nullptr;                       // [2][K1 K2 K3]
+    R* grid = nullptr;                       // [2][K1 K2 K3] spreading grids (kept zeroed)
+    R* phig = nullptr;                       // [2][K1 K2 K3] convolved potential grids
     typename CufftTypes<R>::C* cgrid = nullptr;  // [2][K1 K2 (K3/2+1)]
     R* infl = nullptr;                       // [K1 K2 (K3/2+1)]
     R* theta = nullptr;                      // [n][3][4][P]
@@ -80,7 +81,11 @@ struct Pme {
 template <class R>
 struct Atoms {
     AtomR<R>* at = nullptr;
-    R4<R>* u4 = nullptr;  // [2n]
+    R4<R>* u4 = nullptr;  // [n][2] dipoles
+    R4<R>* p4 = nullptr;  // [n][2] PCG directions
+    R4<R>* c0 = nullptr;  // [n][cap] stored T coefficients (r, B1)
+    R* c1 = nullptr;      // [n][cap] B2
+    int cap = 0;
 };
 
 }  // namespace
@@ -246,7 +251,7 @@ std::vector<ScaledPair> build_scaled(const amg_params* P) {
             mark[k] = 0;
             if (k <= i) continue;
             const S& s = sc[k];
-            if (s.m != 1 || s.p != 1 || s.d != 1 || s.u != 1) out.push_back(ScaledPair{i, k, s.m, s.p, s.d, s.u});
+            if (s.m != 1 || s.p != 1 || s.d != 1 || s.u != 1) out.push_back(ScaledPair{i, k, 0, 0, s.m, s.p, s.d, s.u});
         }
         if (P->ip11.offsets)
             for (int j = P->ip11.offsets[i]; j < P->ip11.offsets[i + 1]; j++) ingrp[P->ip11.indices[j]] = 0;
@@ -294,6 +299,8 @@ void pme_prepare(amg_ctx* ctx, Pme<R>& pm) {
         pm.G = (size_t)K1 * K2 * K3;
         pm.Gc = (size_t)K1 * K2 * (K3 / 2 + 1);
         dalloc(ctx, pm.grid, 2 * pm.G);
+        dalloc(ctx, pm.phig, 2 * pm.G);
+        CK(cudaMemset(pm.grid, 0, sizeof(R) * 2 * pm.G));
         dalloc(ctx, pm.cgrid, 2 * pm.Gc);
         dalloc(ctx, pm.infl, pm.Gc);
         dalloc(ctx, pm.theta, (size_t)ctx->n * 3 * 4 * kOrder);
@@ -336,7 +343,7 @@ void pme_destroy(Pme<R>& pm) {
     cufftHandle* hs[4] = {&pm.f1, &pm.i1, &pm.f2, &pm.i2};
     for (int k = 0; k < 4; k++)
         if (*hs[k]) { cufftDestroy(*hs[k]); *hs[k] = 0; }
-    dfree(pm.grid); dfree(pm.cgrid); dfree(pm.infl); dfree(pm.theta); dfree(pm.k0);
+    dfree(pm.grid); dfree(pm.phig); dfree(pm.cgrid); dfree(pm.infl); dfree(pm.theta); dfree(pm.k0);
     pm.ready = false;
 }
 
@@ -402,6 +409,15 @@ void cell_grid(amg_ctx* ctx, const double* hxyz) {
     ctx->cell_volume = vol;
 }
 
+template <class R>
+void ensure_coeff_buffers(amg_ctx* ctx, Atoms<R>& A) {
+    if (A.cap == ctx->cap && A.c0) return;
+    dalloc(ctx, A.c0, (size_t)ctx->cap * ctx->n);
+    dalloc(ctx, A.c1, (size_t)ctx->cap * ctx->n);
+    A.cap = ctx->cap;
+    ctx->graph_dirty = true;
+}
+
 void ensure_list_buffers(amg_ctx* ctx) {
     const int n = ctx->n;
     size_t ncell = (size_t)ctx->cg.nc[0] * ctx->cg.nc[1] * ctx->cg.nc[2];
@@ -426,8 +442,14 @@ void ensure_list_buffers(amg_ctx* ctx) {
     }
     if (ctx->cap == 0) {
         double rho = n / ctx->cell_volume;
+        int nx = 0;
+        {
+            std::vector<int> off(n + 1);
+            CK(cudaMemcpy(off.data(), ctx->xoff, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost));
+            for (int i = 0; i < n; i++) nx = std::max(nx, off[i + 1] - off[i]);
+        }
         double est = 4.0 / 3.0 * kPi * ctx->cut * ctx->cut * ctx->cut * rho;
-        int cap = (int)std::min<double>(n - 1, std::ceil(1.4 * est) + 64);
+        int cap = (int)std::min<double>(n - 1 + nx, std::ceil(1.4 * est) + 64 + nx);
         ctx->cap = std::max(cap, 1);
         dalloc(ctx, ctx->nbr, (size_t)ctx->cap * n);
         ctx->graph_dirty = true;
@@ -473,20 +495,35 @@ void pme_mpole(amg_ctx* ctx, cudaStream_t s) {
     Pme<R>& pm = pme_of<R>(ctx);
     int3 K = make_int3(ctx->K[0], ctx->K[1], ctx->K[2]);
     double sc[3] = {ctx->K[0] / ctx->box[0], ctx->K[1] / ctx->box[1], ctx->K[2] / ctx->box[2]};
-    k_zero<R><<<nblk(pm.G, 256), 256, 0, s>>>(pm.grid, pm.G);
-    KCHECK();
     k_spread_mpole<R, kOrder><<<nblk(ctx->n), kThreads, 0, s>>>(ctx->n, ctx->rp10, pm.theta, pm.k0, K, (R)sc[0],
                                                                 (R)sc[1], (R)sc[2], pm.grid);
     KCHECK();
     CKFFT(cufftSetStream(pm.f1, s));
     CKFFT(cufftSetStream(pm.i1, s));
     CKFFT(CufftTypes<R>::fwd(pm.f1, pm.grid, pm.cgrid));
-    k_convolve<R><<<nblk(pm.Gc, 256), 256, 0, s>>>(pm.Gc, 1, pm.infl, (typename Cplx<R>::type*)pm.cgrid);
+    k_convolve<R><<<nblk(pm.Gc, 256), 256, 0, s>>>(pm.Gc, 1, pm.infl, (typename Cplx<R>::type*)pm.cgrid, pm.grid, pm.G);
     KCHECK();
-    CKFFT(CufftTypes<R>::inv(pm.i1, pm.cgrid, pm.grid));
-    k_gather<R, kOrder, 20><<<nblk(ctx->n), kThreads, 0, s>>>(ctx->n, pm.grid, pm.theta, pm.k0, K, sc[0], sc[1], sc[2],
+    CKFFT(CufftTypes<R>::inv(pm.i1, pm.cgrid, pm.phig));
+    k_gather<R, kOrder, 20><<<nblk(ctx->n), kThreads, 0, s>>>(ctx->n, pm.phig, pm.theta, pm.k0, K, sc[0], sc[1], sc[2],
                                                               ctx->phiM);
     KCHECK();
+}
+
+// spread two dipole sets, transform, convolve, transform back into pm.phig
+template <class R>
+void pme_dipole_grids(amg_ctx* ctx, cudaStream_t s, const double* vd, const double* vp) {
+    Pme<R>& pm = pme_of<R>(ctx);
+    int3 K = make_int3(ctx->K[0], ctx->K[1], ctx->K[2]);
+    double sc[3] = {ctx->K[0] / ctx->box[0], ctx->K[1] / ctx->box[1], ctx->K[2] / ctx->box[2]};
+    k_spread_dipoles_pt<R, kOrder><<<ctx->n, 128, 0, s>>>(ctx->n, vd, vp, pm.theta, pm.k0, K, (R)sc[0], (R)sc[1],
+                                                           (R)sc[2], pm.grid, pm.G);
+    KCHECK();
+    CKFFT(cufftSetStream(pm.f2, s));
+    CKFFT(cufftSetStream(pm.i2, s));
+    CKFFT(CufftTypes<R>::fwd(pm.f2, pm.grid, pm.cgrid));
+    k_convolve<R><<<nblk(pm.Gc, 256), 256, 0, s>>>(pm.Gc, 2, pm.infl, (typename Cplx<R>::type*)pm.cgrid, pm.grid, pm.G);
+    KCHECK();
+    CKFFT(CufftTypes<R>::inv(pm.i2, pm.cgrid, pm.phig));
 }
 
 // reciprocal potentials of two dipole sets -> phi [2][n][NC]
@@ -495,19 +532,9 @@ void pme_dipoles(amg_ctx* ctx, cudaStream_t s, const double* vd, const double* v
     Pme<R>& pm = pme_of<R>(ctx);
     int3 K = make_int3(ctx->K[0], ctx->K[1], ctx->K[2]);
     double sc[3] = {ctx->K[0] / ctx->box[0], ctx->K[1] / ctx->box[1], ctx->K[2] / ctx->box[2]};
-    k_zero<R><<<nblk(2 * pm.G, 256), 256, 0, s>>>(pm.grid, 2 * pm.G);
-    KCHECK();
-    k_spread_dipoles<R, kOrder><<<nblk(ctx->n), kThreads, 0, s>>>(ctx->n, vd, vp, pm.theta, pm.k0, K, (R)sc[0],
-                                                                  (R)sc[1], (R)sc[2], pm.grid, pm.G);
-    KCHECK();
-    CKFFT(cufftSetStream(pm.f2, s));
-    CKFFT(cufftSetStream(pm.i2, s));
-    CKFFT(CufftTypes<R>::fwd(pm.f2, pm.grid, pm.cgrid));
-    k_convolve<R><<<nblk(pm.Gc, 256), 256, 0, s>>>(pm.Gc, 2, pm.infl, (typename Cplx<R>::type*)pm.cgrid);
-    KCHECK();
-    CKFFT(CufftTypes<R>::inv(pm.i2, pm.cgrid, pm.grid));
+    pme_dipole_grids<R>(ctx, s, vd, vp);
     for (int b = 0; b < 2; b++) {
-        k_gather<R, kOrder, NC><<<nblk(ctx->n), kThreads, 0, s>>>(ctx->n, pm.grid + b * pm.G, pm.theta, pm.k0, K, sc[0],
+        k_gather<R, kOrder, NC><<<nblk(ctx->n), kThreads, 0, s>>>(ctx->n, pm.phig + b * pm.G, pm.theta, pm.k0, K, sc[0],
                                                                   sc[1], sc[2], phi + (size_t)b * NC * ctx->n);
         KCHECK();
     }
@@ -520,7 +547,8 @@ double self_coef(const amg_ctx* ctx) {
     return ctx->ewald ? 4.0 * a * a * a / (3.0 * kSqrtPi) : 0.0;
 }
 
-// A v for both dipole sets (v/alpha - field of v)
+// A v for both dipole sets (v/alpha - field of v), pair tensors computed on
+// the fly (FP64 correction sweep)
 template <class R>
 void matvec(amg_ctx* ctx, cudaStream_t s, const double* vd, const double* vp, double* Ad, double* Ap) {
     const int n = ctx->n;
@@ -547,6 +575,53 @@ void matvec(amg_ctx* ctx, cudaStream_t s, const double* vd, const double* vp, do
     KCHECK();
 }
 
+// pair coefficients of the real-space T for the whole solve
+template <class R>
+void build_tu_coeffs(amg_ctx* ctx, cudaStream_t s) {
+    const int n = ctx->n;
+    Atoms<R>& A = atoms_of<R>(ctx);
+    LPA_DISPATCH(ctx->lpa, {
+        if (ctx->ewald)
+            k_tu_coeffs<R, true, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(n, A.at, ctx->bx, (R)ctx->aewald, ctx->nbr,
+                                                                             ctx->cap, ctx->nnb, A.c0, A.c1);
+        else
+            k_tu_coeffs<R, false, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(n, A.at, ctx->bx, (R)0, ctx->nbr, ctx->cap,
+                                                                              ctx->nnb, A.c0, A.c1);
+    });
+    KCHECK();
+    if (ctx->nsp) {
+        k_scaled_coeffs<R><<<nblk(ctx->nsp), kThreads, 0, s>>>(ctx->nsp, ctx->sp, ctx->xyz, ctx->pdamp, ctx->thole,
+                                                              ctx->bx, ctx->cut * ctx->cut, ewald_alpha(ctx), ctx->nnb,
+                                                              ctx->cap, ctx->nbr, A.c0, A.c1);
+        KCHECK();
+    }
+}
+
+// A v with the stored coefficients; v4 is the R4 copy of (vd, vp)
+template <class R>
+void matvec_stored(amg_ctx* ctx, cudaStream_t s, const R4<R>* v4, const double* vd, const double* vp, double* Ad,
+                   double* Ap) {
+    const int n = ctx->n;
+    Atoms<R>& A = atoms_of<R>(ctx);
+    LPA_DISPATCH(ctx->lpa, {
+        k_tu_stored<R, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(n, ctx->nbr, A.c0, A.c1, ctx->cap, ctx->nnb, ctx->xoff,
+                                                                    v4, ctx->Fd, ctx->Fp);
+    });
+    KCHECK();
+    if (ctx->ewald) {
+        Pme<R>& pm = pme_of<R>(ctx);
+        pme_dipole_grids<R>(ctx, s, vd, vp);
+        int3 K = make_int3(ctx->K[0], ctx->K[1], ctx->K[2]);
+        double sc[3] = {ctx->K[0] / ctx->box[0], ctx->K[1] / ctx->box[1], ctx->K[2] / ctx->box[2]};
+        k_gather_field_pt<R, kOrder><<<n, 128, 0, s>>>(n, pm.phig, pm.G, pm.theta, pm.k0, K, sc[0], sc[1], sc[2], vd, vp,
+                                                        ctx->Fd, ctx->Fp, self_coef(ctx), ctx->pol, Ad, Ap);
+        KCHECK();
+    } else {
+        k_matvec_finish<<<nblk(n), kThreads, 0, s>>>(n, vd, vp, ctx->Fd, ctx->Fp, ctx->phiU4, 0, 0.0, ctx->pol, Ad, Ap);
+        KCHECK();
+    }
+}
+
 bool iterative(const amg_ctx* ctx) { return ctx->has_pol && ctx->poltyp == AMG_POL_MUTUAL && ctx->npolar > 0; }
 
 double pcg_threshold(const amg_ctx* ctx) {
@@ -559,6 +634,7 @@ double pcg_threshold(const amg_ctx* ctx) {
 template <class R>
 void enqueue_pcg_init(amg_ctx* ctx, cudaStream_t s, cudaGraphConditionalHandle h, int use_handle) {
     const int n = ctx->n;
+    Atoms<R>& A = atoms_of<R>(ctx);
     if (!ctx->guess) {
         k_zero<double><<<nblk(3 * n, 256), 256, 0, s>>>(ctx->ud, 3 * (size_t)n);
         KCHECK();
@@ -567,9 +643,14 @@ void enqueue_pcg_init(amg_ctx* ctx, cudaStream_t s, cudaGraphConditionalHandle h
     }
     k_zero<double><<<1, 32, 0, s>>>(ctx->scal, NSCAL);
     KCHECK();
-    matvec<R>(ctx, s, ctx->ud, ctx->up, ctx->Apd, ctx->App);
+    build_tu_coeffs<R>(ctx, s);
+    k_pack_u<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->ud, ctx->up, A.u4);
+    KCHECK();
+    matvec_stored<R>(ctx, s, A.u4, ctx->ud, ctx->up, ctx->Apd, ctx->App);
     k_pcg_init<<<nblk(n), kThreads, 0, s>>>(n, ctx->Ed, ctx->Ep, ctx->Apd, ctx->App, ctx->pol, ctx->rd, ctx->rp, ctx->zd,
                                             ctx->zp, ctx->pd, ctx->pp, ctx->scal);
+    KCHECK();
+    k_pack_u<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->pd, ctx->pp, A.p4);
     KCHECK();
     k_pcg_control<<<1, 1, 0, s>>>(ctx->scal, ctx->iter, pcg_threshold(ctx), ctx->politer, 1, h, use_handle, ctx->cont);
     KCHECK();
@@ -579,15 +660,14 @@ void enqueue_pcg_init(amg_ctx* ctx, cudaStream_t s, cudaGraphConditionalHandle h
 template <class R>
 void enqueue_pcg_iter(amg_ctx* ctx, cudaStream_t s, cudaGraphConditionalHandle h, int use_handle) {
     const int n = ctx->n, n3 = 3 * n;
-    k_zero<double><<<1, 32, 0, s>>>(ctx->scal + PAP_D, 6);
-    KCHECK();
-    matvec<R>(ctx, s, ctx->pd, ctx->pp, ctx->Apd, ctx->App);
+    Atoms<R>& A = atoms_of<R>(ctx);
+    matvec_stored<R>(ctx, s, A.p4, ctx->pd, ctx->pp, ctx->Apd, ctx->App);
     k_dot2<<<nblk(n3, 256), 256, 0, s>>>(n3, ctx->pd, ctx->Apd, ctx->pp, ctx->App, ctx->scal + PAP_D, ctx->scal + PAP_P);
     KCHECK();
     k_pcg_update<<<nblk(n), kThreads, 0, s>>>(n, ctx->pol, ctx->pd, ctx->pp, ctx->Apd, ctx->App, ctx->ud, ctx->up,
                                               ctx->rd, ctx->rp, ctx->zd, ctx->zp, ctx->scal);
     KCHECK();
-    k_pcg_dir<<<nblk(n3, 256), 256, 0, s>>>(n3, ctx->zd, ctx->zp, ctx->pd, ctx->pp, ctx->scal);
+    k_pcg_dir<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->zd, ctx->zp, ctx->pd, ctx->pp, ctx->scal, A.p4);
     KCHECK();
     k_pcg_control<<<1, 1, 0, s>>>(ctx->scal, ctx->iter, pcg_threshold(ctx), ctx->politer, 0, h, use_handle, ctx->cont);
     KCHECK();
@@ -616,7 +696,15 @@ void enqueue_front(amg_ctx* ctx, cudaStream_t s) {
     enqueue_lists(ctx, s);
     if (ctx->ewald) {
         pme_stencils<R>(ctx, s);
-        if (mixed && iterative(ctx)) pme_stencils<double>(ctx, s);
+        Pme<R>& pm = pme_of<R>(ctx);
+        k_zero<R><<<nblk(2 * pm.G, 256), 256, 0, s>>>(pm.grid, 2 * pm.G);
+        KCHECK();
+        if (mixed && iterative(ctx)) {
+            pme_stencils<double>(ctx, s);
+            Pme<double>& pd = pme_of<double>(ctx);
+            k_zero<double><<<nblk(2 * pd.G, 256), 256, 0, s>>>(pd.grid, 2 * pd.G);
+            KCHECK();
+        }
     }
     k_zero<double><<<1, 32, 0, s>>>(ctx->eacc, 8);
     KCHECK();
@@ -856,6 +944,7 @@ int forward_impl(amg_ctx* ctx, int flags, amg_results* res) {
     cudaStream_t st = ctx->st;
     for (int attempt = 0; attempt < 2; attempt++) {
         ensure_list_buffers(ctx);
+        if (iterative(ctx)) ensure_coeff_buffers<R>(ctx, atoms_of<R>(ctx));
         if (ctx->ewald) {
             pme_prepare<R>(ctx, pme_of<R>(ctx));
             if (ctx->prec == AMG_PREC_MIXED && iterative(ctx)) pme_prepare<double>(ctx, pme_of<double>(ctx));
@@ -983,6 +1072,7 @@ void release(amg_ctx* ctx) {
     if (ctx->cubtmp) cudaFree(ctx->cubtmp);
     ctx->cubtmp = nullptr;
     dfree(ctx->af.at); dfree(ctx->af.u4); dfree(ctx->ad.at); dfree(ctx->ad.u4);
+    dfree(ctx->af.p4); dfree(ctx->ad.p4); dfree(ctx->af.c0); dfree(ctx->af.c1); dfree(ctx->ad.c0); dfree(ctx->ad.c1);
     pme_destroy(ctx->pmf);
     pme_destroy(ctx->pmd);
     for (auto& e : ctx->ev)
@@ -1052,23 +1142,32 @@ int create_impl(amg_ctx* ctx, const amg_params* P) {
     upload(ctx, ctx->pdamp, ctx->has_pol ? P->pdamp : zeros.data(), n);
     std::vector<ScaledPair> sp = build_scaled(P);
     ctx->nsp = (int)sp.size();
-    upload(ctx, ctx->sp, sp.data(), sp.size());
     {
+        // scaled partners of each site (CSR); si/sk locate each pair in the
+        // two rows so the stored-coefficient rows can append them
         std::vector<int> off(n + 1, 0), idx(2 * sp.size() + 1);
         for (const ScaledPair& q : sp) { off[q.i + 1]++; off[q.k + 1]++; }
         for (int i = 0; i < n; i++) off[i + 1] += off[i];
         std::vector<int> fill(off.begin(), off.end() - 1);
-        for (const ScaledPair& q : sp) { idx[fill[q.i]++] = q.k; idx[fill[q.k]++] = q.i; }
+        for (ScaledPair& q : sp) {
+            q.si = fill[q.i] - off[q.i];
+            idx[fill[q.i]++] = q.k;
+            q.sk = fill[q.k] - off[q.k];
+            idx[fill[q.k]++] = q.i;
+        }
         upload(ctx, ctx->xoff, off.data(), off.size());
         upload(ctx, ctx->xidx, idx.data(), idx.size());
     }
+    upload(ctx, ctx->sp, sp.data(), sp.size());
     dalloc(ctx, ctx->xyz, 3 * (size_t)n);
     dalloc(ctx, ctx->rp10, 10 * (size_t)n);
     dalloc(ctx, ctx->ad.at, n);
     dalloc(ctx, ctx->ad.u4, 2 * (size_t)n);
+    dalloc(ctx, ctx->ad.p4, 2 * (size_t)n);
     if (ctx->prec == AMG_PREC_MIXED) {
         dalloc(ctx, ctx->af.at, n);
         dalloc(ctx, ctx->af.u4, 2 * (size_t)n);
+        dalloc(ctx, ctx->af.p4, 2 * (size_t)n);
     }
     double** vecs[] = {&ctx->Ed, &ctx->Ep, &ctx->ud, &ctx->up, &ctx->rd, &ctx->rp, &ctx->zd, &ctx->zp, &ctx->pd,
                        &ctx->pp, &ctx->Apd, &ctx->App, &ctx->Fd, &ctx->Fp, &ctx->resd, &ctx->grad_m, &ctx->grad_p,
@@ -1280,6 +1379,66 @@ int amg_bench(amg_ctx* ctx, int32_t flags, int32_t steps, int64_t flush_bytes, d
             ctx->err = "neighbour list overflow during the benchmark";
             return AMG_ERR_CUDA;
         }
+    } catch (Fail& f) {
+        return f.code;
+    }
+    return AMG_OK;
+}
+
+// Times the stored-coefficient T.u kernel (the PCG's real-space matvec) on
+// its own: `reps` launches on the context's stream, each after an L2 flush of
+// flush_bytes, using the coefficients and dipoles of the last evaluation.
+// Reports the average device time and the kernel's algorithmic bytes per
+// launch (coefficient rows streamed + the dipoles and fields of each site).
+int amg_time_tu_kernel(amg_ctx* ctx, int32_t reps, int64_t flush_bytes, double* ms_avg, double* bytes_per_launch,
+                       int64_t* directed_pairs) {
+    if (!ctx || reps <= 0 || !ms_avg) return AMG_ERR_BAD_ARG;
+    if (!ctx->have_forward || !iterative(ctx)) {
+        ctx->err = "needs a previous evaluation with mutual polarization";
+        return AMG_ERR_BAD_ARG;
+    }
+    try {
+        CK(cudaSetDevice(ctx->device));
+        const int n = ctx->n;
+        std::vector<int> nnb(n), off(n + 1);
+        CK(cudaMemcpy(nnb.data(), ctx->nnb, sizeof(int) * n, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(off.data(), ctx->xoff, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost));
+        long long pairs = 0;
+        for (int i = 0; i < n; i++) pairs += nnb[i] + (off[i + 1] - off[i]);
+        if (flush_bytes > 0 && (size_t)flush_bytes > ctx->flush_bytes) {
+            dalloc(ctx, ctx->flushbuf, (size_t)flush_bytes);
+            ctx->flush_bytes = (size_t)flush_bytes;
+        }
+        cudaEvent_t a, b;
+        CK(cudaEventCreate(&a));
+        CK(cudaEventCreate(&b));
+        double tot = 0;
+        const bool mixed = ctx->prec == AMG_PREC_MIXED;
+        size_t rs = mixed ? sizeof(float) : sizeof(double);
+        for (int k = 0; k < reps; k++) {
+            if (flush_bytes > 0) CK(cudaMemsetAsync(ctx->flushbuf, k & 0xff, (size_t)flush_bytes, ctx->st));
+            CK(cudaEventRecord(a, ctx->st));
+            LPA_DISPATCH(ctx->lpa, {
+                if (mixed)
+                    k_tu_stored<float, L><<<nblk((size_t)n * L), kThreads, 0, ctx->st>>>(
+                        n, ctx->nbr, ctx->af.c0, ctx->af.c1, ctx->cap, ctx->nnb, ctx->xoff, ctx->af.p4, ctx->Fd, ctx->Fp);
+                else
+                    k_tu_stored<double, L><<<nblk((size_t)n * L), kThreads, 0, ctx->st>>>(
+                        n, ctx->nbr, ctx->ad.c0, ctx->ad.c1, ctx->cap, ctx->nnb, ctx->xoff, ctx->ad.p4, ctx->Fd, ctx->Fp);
+            });
+            KCHECK();
+            CK(cudaEventRecord(b, ctx->st));
+            CK(cudaEventSynchronize(b));
+            float ms = 0;
+            CK(cudaEventElapsedTime(&ms, a, b));
+            tot += ms;
+        }
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        *ms_avg = tot / reps;
+        if (bytes_per_launch)
+            *bytes_per_launch = (double)pairs * (4.0 + 5.0 * rs) + (double)n * (2 * 4 * rs + 2 * 3 * 8.0 + 8.0);
+        if (directed_pairs) *directed_pairs = pairs;
     } catch (Fail& f) {
         return f.code;
     }

@@ -22,13 +22,13 @@ __global__ void k_field_finish(int n, const double* __restrict__ phiM, int ewald
     }
 }
 
-// FP64 dipole vectors -> R4 copies for the pair kernels ([2n], d then p)
+// FP64 dipole vectors -> R4 copies for the pair kernels ([n][2], d then p)
 template <class R>
 __global__ void k_pack_u(int n, const double* __restrict__ ud, const double* __restrict__ up, R4<R>* __restrict__ u4) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    u4[i] = make_r4<R>((R)ud[3 * i], (R)ud[3 * i + 1], (R)ud[3 * i + 2], R(0));
-    u4[n + i] = make_r4<R>((R)up[3 * i], (R)up[3 * i + 1], (R)up[3 * i + 2], R(0));
+    u4[2 * i] = make_r4<R>((R)ud[3 * i], (R)ud[3 * i + 1], (R)ud[3 * i + 2], R(0));
+    u4[2 * i + 1] = make_r4<R>((R)up[3 * i], (R)up[3 * i + 1], (R)up[3 * i + 2], R(0));
 }
 
 // A v = v/alpha - (real + recip + self) field of v, both sets; pol = 0 sites
@@ -76,6 +76,11 @@ __global__ void k_pcg_control(double* __restrict__ scal, int* __restrict__ iter,
     double e2 = fmax(scal[RR_D], scal[RR_P]);
     int cont = (e2 > thr2) && (it < maxit);
     *cont_out = cont;
+    if (cont) {  // accumulators of the next iteration
+        scal[PAP_D] = scal[PAP_P] = 0;
+        scal[RZN_D] = scal[RZN_P] = 0;
+        scal[RR_D] = scal[RR_P] = 0;
+    }
     if (use_handle) cudaGraphSetConditional(h, cont ? 1u : 0u);
 }
 
@@ -145,14 +150,24 @@ __global__ void k_pcg_update(int n, const double* __restrict__ pol, const double
 }
 
 // p = z + (rz_new / rz) p; k_pcg_roll then moves rz_new into rz
-__global__ void k_pcg_dir(int n3, const double* __restrict__ zd, const double* __restrict__ zp,
-                          double* __restrict__ pd, double* __restrict__ pp, const double* __restrict__ scal) {
-    int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= n3) return;
+template <class R>
+__global__ void k_pcg_dir(int n, const double* __restrict__ zd, const double* __restrict__ zp,
+                          double* __restrict__ pd, double* __restrict__ pp, const double* __restrict__ scal,
+                          R4<R>* __restrict__ p4) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
     double bd = scal[RZ_D] != 0 ? scal[RZN_D] / scal[RZ_D] : 0.0;
     double bp = scal[RZ_P] != 0 ? scal[RZN_P] / scal[RZ_P] : 0.0;
-    pd[q] = zd[q] + bd * pd[q];
-    pp[q] = zp[q] + bp * pp[q];
+    double a[3], b[3];
+    for (int c = 0; c < 3; c++) {
+        int q = 3 * i + c;
+        a[c] = zd[q] + bd * pd[q];
+        b[c] = zp[q] + bp * pp[q];
+        pd[q] = a[c];
+        pp[q] = b[c];
+    }
+    p4[2 * i] = make_r4<R>((R)a[0], (R)a[1], (R)a[2], R(0));
+    p4[2 * i + 1] = make_r4<R>((R)b[0], (R)b[1], (R)b[2], R(0));
 }
 
 __global__ void k_pcg_roll(double* scal) {

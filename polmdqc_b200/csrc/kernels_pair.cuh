@@ -50,8 +50,9 @@ __global__ void __launch_bounds__(128) k_perm_field(int n, const AtomR<R>* __res
     }
 }
 
-// Mutual field T u for two dipole sets (bulk, u-scale 1).  u4: [2n] R4
-// (ux,uy,uz,0) with the d set first, p set second.  Writes Fd, Fp.
+// Mutual field T u for two dipole sets (bulk, u-scale 1), computing the
+// pair tensors on the fly (used by the FP64 correction sweep).  u4: [n][2]
+// R4 (ux,uy,uz,0), d set then p set per site.  Writes Fd, Fp.
 template <class R, bool EWALD, int LPA>
 __global__ void __launch_bounds__(128) k_Tu(int n, const AtomR<R>* __restrict__ at, const R4<R>* __restrict__ u4,
                                             Box bx, R aewald, const int* __restrict__ nbr, int cap,
@@ -90,7 +91,7 @@ __global__ void __launch_bounds__(128) k_Tu(int n, const AtomR<R>* __restrict__ 
                 B2 -= (R(1) + x) * e * b2;    // (1 - lambda5) = (1 + x) e
             }
         }
-        R4<R> ud = u4[j], up = u4[n + j];
+        R4<R> ud = u4[2 * j], up = u4[2 * j + 1];
         R ad = ud.x * r.x + ud.y * r.y + ud.z * r.z;
         R ap = up.x * r.x + up.y * r.y + up.z * r.z;
         ax += ad * B2 * r.x - B1 * ud.x; ay += ad * B2 * r.y - B1 * ud.y; az += ad * B2 * r.z - B1 * ud.z;
@@ -161,7 +162,7 @@ __global__ void __launch_bounds__(128) k_mpole_pair(int n, const AtomR<R>* __res
 // Polarization gradient and torque of site i (bulk, all scales 1):
 //   G = E(M_i, ubar_k) + E(ubar_i, M_k) + 1/2 [E(up_i, ud_k) + E(ud_i, up_k)]
 // with ubar = (ud + up)/2; dG/dx_i = -dG/dr, torque on M_i from ubar_k.
-// u4: [2n] R4, d set then p set.
+// u4: [n][2] R4, d set then p set per site.
 template <class R, bool EWALD, int LPA>
 __global__ void __launch_bounds__(128) k_polar_pair(int n, const AtomR<R>* __restrict__ at,
                                                     const R4<R>* __restrict__ u4, Box bx, R aewald,
@@ -174,7 +175,7 @@ __global__ void __launch_bounds__(128) k_polar_pair(int n, const AtomR<R>* __res
     AtomR<R> Ai = at[i];
     Mpole<R> Mi = load_mpole(Ai);
     V3<R> xi = v3<R>(Ai.a.x, Ai.a.y, Ai.a.z);
-    R4<R> udi4 = u4[i], upi4 = u4[n + i];
+    R4<R> udi4 = u4[2 * i], upi4 = u4[2 * i + 1];
     V3<R> udi = v3<R>(udi4.x, udi4.y, udi4.z), upi = v3<R>(upi4.x, upi4.y, upi4.z);
     V3<R> ubi = R(0.5) * (udi + upi);
     V3<R> g = v3<R>(0, 0, 0), t = v3<R>(0, 0, 0);
@@ -185,7 +186,7 @@ __global__ void __launch_bounds__(128) k_polar_pair(int n, const AtomR<R>* __res
         V3<R> r = min_image<R>(v3<R>(Aj.a.x, Aj.a.y, Aj.a.z) - xi, bx);
         R B[6];
         bulk_radial<R, EWALD, true>(dot(r, r), aewald, Ai.e.y * Aj.e.y, pair_thole<R>(Ai.e.z, Aj.e.z), B);
-        R4<R> udk4 = u4[j], upk4 = u4[n + j];
+        R4<R> udk4 = u4[2 * j], upk4 = u4[2 * j + 1];
         V3<R> udk = v3<R>(udk4.x, udk4.y, udk4.z), upk = v3<R>(upk4.x, upk4.y, upk4.z);
         V3<R> ubk = R(0.5) * (udk + upk);
         Mpole<R> Mk = load_mpole(Aj);
@@ -205,6 +206,82 @@ __global__ void __launch_bounds__(128) k_polar_pair(int n, const AtomR<R>* __res
     }
 }
 
+// ------------------------------------------------------------ stored T
+// The dipole interaction tensor does not change during the PCG solve, so its
+// pair coefficients are computed once per evaluation and streamed by every
+// matvec: per slot (r = x_i - x_j, B1) as R4 and B2 as R; the neighbour
+// index is the list entry itself.  Rows hold the bulk neighbours followed by
+// the scaled partners (filled by k_scaled_coeffs), so one kernel applies the
+// whole real-space T.
+template <class R, bool EWALD, int LPA>
+__global__ void __launch_bounds__(128) k_tu_coeffs(int n, const AtomR<R>* __restrict__ at, Box bx, R aewald,
+                                                   const int* __restrict__ nbr, int cap, const int* __restrict__ nnb,
+                                                   R4<R>* __restrict__ c0, R* __restrict__ c1) {
+    const int g = (blockIdx.x * blockDim.x + threadIdx.x) / LPA, lane = threadIdx.x % LPA;
+    if (g >= n) return;
+    const int i = g;
+    const int cnt = nnb[i];
+    R4<R> pi = at[i].a, ei = at[i].e;
+    V3<R> xi = v3<R>(pi.x, pi.y, pi.z);
+    const size_t base = (size_t)i * cap;
+    for (int s = lane; s < cnt; s += LPA) {
+        int j = nbr[base + s];
+        R4<R> pj = at[j].a, ej = at[j].e;
+        V3<R> r = min_image<R>(xi - v3<R>(pj.x, pj.y, pj.z), bx);
+        R r2 = dot(r, r);
+        R rinv = rsqrt_<R>(r2);
+        R rr = r2 * rinv, rinv2 = rinv * rinv;
+        R b1 = rinv * rinv2, b2 = 3 * b1 * rinv2;
+        R B1 = b1, B2 = b2;
+        if (EWALD) {
+            R eb[3];
+            ewald_terms<R, 3>(rr, rinv2, aewald, eb);
+            B1 = eb[1]; B2 = eb[2];
+        }
+        R damp = ei.y * ej.y;
+        if (damp != R(0)) {
+            R t = rr / damp;
+            R x = pair_thole<R>(ei.z, ej.z) * t * t * t;
+            R e = exp_<R>(-x);
+            B1 -= e * b1;
+            B2 -= (R(1) + x) * e * b2;
+        }
+        c0[base + s] = make_r4<R>(r.x, r.y, r.z, B1);
+        c1[base + s] = B2;
+    }
+}
+
+// T v with the stored coefficients (both dipole sets): rows of nnb[i] bulk
+// slots plus the site's scaled partners.  u4: [n][2] R4.
+template <class R, int LPA>
+__global__ void __launch_bounds__(128) k_tu_stored(int n, const int* __restrict__ nbr,
+                                                   const R4<R>* __restrict__ c0, const R* __restrict__ c1, int cap,
+                                                   const int* __restrict__ nnb, const int* __restrict__ xoff,
+                                                   const R4<R>* __restrict__ u4, double* __restrict__ Fd,
+                                                   double* __restrict__ Fp) {
+    const int g = (blockIdx.x * blockDim.x + threadIdx.x) / LPA, lane = threadIdx.x % LPA;
+    const int i = min(g, n - 1);
+    const int cnt = g < n ? nnb[i] + (xoff[i + 1] - xoff[i]) : 0;
+    const size_t base = (size_t)i * cap;
+    R ax = 0, ay = 0, az = 0, bx_ = 0, by = 0, bz = 0;
+    for (int s = lane; s < cnt; s += LPA) {
+        int j = nbr[base + s];
+        R4<R> c = c0[base + s];
+        R B2 = c1[base + s];
+        R4<R> ud = u4[2 * j], up = u4[2 * j + 1];
+        R ad = (ud.x * c.x + ud.y * c.y + ud.z * c.z) * B2;
+        R ap = (up.x * c.x + up.y * c.y + up.z * c.z) * B2;
+        ax += ad * c.x - c.w * ud.x; ay += ad * c.y - c.w * ud.y; az += ad * c.z - c.w * ud.z;
+        bx_ += ap * c.x - c.w * up.x; by += ap * c.y - c.w * up.y; bz += ap * c.z - c.w * up.z;
+    }
+    double sx = group_sum<LPA>((double)ax), sy = group_sum<LPA>((double)ay), sz = group_sum<LPA>((double)az);
+    double tx = group_sum<LPA>((double)bx_), ty = group_sum<LPA>((double)by), tz = group_sum<LPA>((double)bz);
+    if (lane == 0 && g < n) {
+        Fd[3 * i] = sx; Fd[3 * i + 1] = sy; Fd[3 * i + 2] = sz;
+        Fp[3 * i] = tx; Fp[3 * i + 1] = ty; Fp[3 * i + 2] = tz;
+    }
+}
+
 // ------------------------------------------------------------ scaled pairs
 // Pairs with any scale != 1, from the 1-n and polarization-group lists.
 // They are removed from the bulk neighbour lists and evaluated whole here in
@@ -213,6 +290,7 @@ __global__ void __launch_bounds__(128) k_polar_pair(int n, const AtomR<R>* __res
 // correction.
 struct ScaledPair {
     int i, k;
+    int si, sk;  // position of k among i's scaled partners and of i among k's
     double m, p, d, u;
 };
 
@@ -305,6 +383,31 @@ __global__ void k_scaled_Tu(int np, const ScaledPair* __restrict__ sp, const dou
     add3(Fd, P.i, field_of_dipole<double>(ld3(ud, P.k), mr, B[1], B[2]));
     add3(Fp, P.k, field_of_dipole<double>(ld3(up, P.i), G.r, B[1], B[2]));
     add3(Fp, P.i, field_of_dipole<double>(ld3(up, P.k), mr, B[1], B[2]));
+}
+
+// u-channel coefficients of the scaled pairs (FP64 radial, stored in R) in
+// the slots after each row's bulk neighbours; pairs beyond the cutoff get
+// zero coefficients.
+template <class R>
+__global__ void k_scaled_coeffs(int np, const ScaledPair* __restrict__ sp, const double* __restrict__ xyz,
+                                const double* __restrict__ pdamp, const double* __restrict__ thole, Box bx,
+                                double cut2, double aewald, const int* __restrict__ nnb, int cap,
+                                int* __restrict__ nbr, R4<R>* __restrict__ c0, R* __restrict__ c1) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= np) return;
+    ScaledPair P = sp[t];
+    ScaledGeom G = scaled_geom(P, xyz, pdamp, thole, bx, cut2, aewald);
+    double B[6] = {0, 0, 0, 0, 0, 0};
+    if (G.inside) scaled_radial(G, P.u, true, aewald > 0, B);
+    V3<double> r = G.inside ? G.r : v3<double>(0, 0, 0);
+    size_t si = (size_t)P.i * cap + nnb[P.i] + P.si;
+    size_t sk = (size_t)P.k * cap + nnb[P.k] + P.sk;
+    nbr[si] = P.k;
+    nbr[sk] = P.i;
+    c0[si] = make_r4<R>((R)(-r.x), (R)(-r.y), (R)(-r.z), (R)B[1]);   // x_i - x_k
+    c0[sk] = make_r4<R>((R)r.x, (R)r.y, (R)r.z, (R)B[1]);
+    c1[si] = (R)B[2];
+    c1[sk] = (R)B[2];
 }
 
 // scaled pairs' contribution to em, its gradient and the torques (both

@@ -88,21 +88,106 @@ __global__ void k_spread_dipoles(int n, const double* __restrict__ ud, const dou
     }
 }
 
+// Point-parallel spreading of two dipole sets: one block of 128 threads per
+// site, thread t < P^3 owns stencil point (a,b,c) = (t / P^2, t / P % P, t % P)
+// and issues one fire-and-forget atomic add per grid; consecutive threads
+// write consecutive z addresses.
+template <class R, int P>
+__global__ void __launch_bounds__(128) k_spread_dipoles_pt(int n, const double* __restrict__ ud,
+                                                           const double* __restrict__ up,
+                                                           const R* __restrict__ theta, const int* __restrict__ k0,
+                                                           int3 K, R sc0, R sc1, R sc2, R* __restrict__ grid,
+                                                           size_t gstride) {
+    const int i = blockIdx.x, t = threadIdx.x;
+    if (t >= P * P * P) return;
+    const int a = t / (P * P), b = (t / P) % P, c = t % P;
+    const R* th = theta + (size_t)i * 3 * 4 * P;
+    R t0 = th[a], t1 = th[P + a];
+    R u0 = th[4 * P + b], u1 = th[5 * P + b];
+    R v0 = th[8 * P + c], v1 = th[9 * P + c];
+    R d0 = (R)ud[3 * i] * sc0, d1 = (R)ud[3 * i + 1] * sc1, d2 = (R)ud[3 * i + 2] * sc2;
+    R p0 = (R)up[3 * i] * sc0, p1 = (R)up[3 * i + 1] * sc1, p2 = (R)up[3 * i + 2] * sc2;
+    R w100 = t1 * u0 * v0, w010 = t0 * u1 * v0, w001 = t0 * u0 * v1;
+    int ga = k0[3 * i] + a; if (ga >= K.x) ga -= K.x;
+    int gb = k0[3 * i + 1] + b; if (gb >= K.y) gb -= K.y;
+    int gc = k0[3 * i + 2] + c; if (gc >= K.z) gc -= K.z;
+    const int g = gidx(ga, gb, gc, K);
+    atomicAdd(grid + g, d0 * w100 + d1 * w010 + d2 * w001);
+    atomicAdd(grid + gstride + g, p0 * w100 + p1 * w010 + p2 * w001);
+}
+
+// Point-parallel gather of the field of two dipole grids (first derivatives
+// only) fused with the matvec assembly:
+//   A v = v/alpha - (F_real + F_recip + selfc v),  F_recip = -grad phi
+// One block per site; the P^3 stencil points are reduced with shuffles and
+// shared memory.
+template <class R, int P>
+__global__ void __launch_bounds__(128) k_gather_field_pt(int n, const R* __restrict__ phigrid, size_t gstride,
+                                                         const R* __restrict__ theta, const int* __restrict__ k0,
+                                                         int3 K, double sc0, double sc1, double sc2,
+                                                         const double* __restrict__ vd,
+                                                         const double* __restrict__ vp,
+                                                         const double* __restrict__ Fd,
+                                                         const double* __restrict__ Fp, double selfc,
+                                                         const double* __restrict__ pol, double* __restrict__ Ad,
+                                                         double* __restrict__ Ap) {
+    const int i = blockIdx.x, t = threadIdx.x;
+    R f[6] = {0, 0, 0, 0, 0, 0};
+    if (t < P * P * P) {
+        const int a = t / (P * P), b = (t / P) % P, c = t % P;
+        const R* th = theta + (size_t)i * 3 * 4 * P;
+        R t0 = th[a], t1 = th[P + a];
+        R u0 = th[4 * P + b], u1 = th[5 * P + b];
+        R v0 = th[8 * P + c], v1 = th[9 * P + c];
+        int ga = k0[3 * i] + a; if (ga >= K.x) ga -= K.x;
+        int gb = k0[3 * i + 1] + b; if (gb >= K.y) gb -= K.y;
+        int gc = k0[3 * i + 2] + c; if (gc >= K.z) gc -= K.z;
+        const int g = gidx(ga, gb, gc, K);
+        R qd = phigrid[g], qp = phigrid[gstride + g];
+        R w100 = t1 * u0 * v0, w010 = t0 * u1 * v0, w001 = t0 * u0 * v1;
+        f[0] = w100 * qd; f[1] = w010 * qd; f[2] = w001 * qd;
+        f[3] = w100 * qp; f[4] = w010 * qp; f[5] = w001 * qp;
+    }
+    __shared__ R part[4][6];
+#pragma unroll
+    for (int k = 0; k < 6; k++) f[k] = warp_sum(f[k]);
+    if ((t & 31) == 0)
+        for (int k = 0; k < 6; k++) part[t >> 5][k] = f[k];
+    __syncthreads();
+    if (t < 6) {
+        double v = (double)part[0][t] + (double)part[1][t] + (double)part[2][t] + (double)part[3][t];
+        double scv = t % 3 == 0 ? sc0 : t % 3 == 1 ? sc1 : sc2;
+        const int c = t % 3;
+        const bool dset = t < 3;
+        const double* vv = dset ? vd : vp;
+        const double* FF = dset ? Fd : Fp;
+        double* AA = dset ? Ad : Ap;
+        double alpha = pol[i];
+        double field = FF[3 * i + c] - v * scv + selfc * vv[3 * i + c];
+        AA[3 * i + c] = alpha > 0 ? vv[3 * i + c] / alpha - field : 0.0;
+    }
+}
+
 // Multiply the transformed grids by the influence function
 //   G(m) = exp(-pi^2 |h|^2 / alpha^2) / (pi V |h|^2 bsmod1 bsmod2 bsmod3)
 // precomputed in FP64 on the host (half-complex layout, G(0) = 0).
+// The same kernel clears the real spreading grids ([batch][nreal], already
+// consumed by the forward FFT) for the next spreading pass.
 template <class R>
 __global__ void k_convolve(size_t ncomplex, int batch, const R* __restrict__ infl,
-                           typename Cplx<R>::type* __restrict__ cg) {
+                           typename Cplx<R>::type* __restrict__ cg, R* __restrict__ spread, size_t nreal) {
     size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= ncomplex) return;
-    R g = infl[t];
-    for (int b = 0; b < batch; b++) {
-        auto v = cg[b * ncomplex + t];
-        v.x *= g;
-        v.y *= g;
-        cg[b * ncomplex + t] = v;
+    if (t < ncomplex) {
+        R g = infl[t];
+        for (int b = 0; b < batch; b++) {
+            auto v = cg[b * ncomplex + t];
+            v.x *= g;
+            v.y *= g;
+            cg[b * ncomplex + t] = v;
+        }
     }
+    if (spread)
+        for (size_t q = t; q < (size_t)batch * nreal; q += (size_t)gridDim.x * blockDim.x) spread[q] = R(0);
 }
 
 // Gather NC (4, 10 or 20) Cartesian potential derivatives per site from

@@ -159,6 +159,7 @@ __global__ void k_neighbors(int n, const double4* __restrict__ spos, const unsig
     const int c0 = key / (cg.nc[2] * cg.nc[1]);
     const double4 pi = spos[w];
     const int x0 = xoff[i], x1 = xoff[i + 1];
+    const int limit = cap - (x1 - x0);  // the row's tail holds the scaled partners
     int* row = nbr + (size_t)i * cap;
     int cnt = 0;
     for (int dx = cg.off_lo[0]; dx <= cg.off_hi[0]; dx++) {
@@ -192,7 +193,7 @@ __global__ void k_neighbors(int n, const double4* __restrict__ spos, const unsig
                     unsigned m = __ballot_sync(0xffffffffu, hit);
                     if (hit) {
                         int pos = cnt + __popc(m & ((1u << lane) - 1u));
-                        if (pos < cap) row[pos] = j;
+                        if (pos < limit) row[pos] = j;
                     }
                     cnt += __popc(m);
                 }
@@ -200,8 +201,8 @@ __global__ void k_neighbors(int n, const double4* __restrict__ spos, const unsig
         }
     }
     if (lane == 0) {
-        nnb[i] = min(cnt, cap);
-        if (cnt > cap) atomicMax(overflow, cnt);
+        nnb[i] = min(cnt, limit);
+        if (cnt > limit) atomicMax(overflow, cnt + (x1 - x0));
     }
 }
 

@@ -181,6 +181,14 @@ class Engine:
                     "amg_bench")
         return ms, int(launches.value)
 
+    def time_tu_kernel(self, reps=20, flush_bytes=256 << 20):
+        """(avg ms, algorithmic bytes per launch, directed pairs) of the PCG's
+        stored-coefficient T.u kernel, each launch after an L2 flush."""
+        ms, by, pairs = C.c_double(0), C.c_double(0), C.c_int64(0)
+        self._check(self.lib.amg_time_tu_kernel(self.ctx, reps, flush_bytes, C.byref(ms), C.byref(by), C.byref(pairs)),
+                    "amg_time_tu_kernel")
+        return ms.value, by.value, int(pairs.value)
+
     def stats(self):
         launches, graphed, lpa = C.c_int64(0), C.c_int32(0), C.c_int32(0)
         self._check(self.lib.amg_last_stats(self.ctx, C.byref(launches), C.byref(graphed), C.byref(lpa)),

@@ -52,7 +52,7 @@ class Clocks:
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(gpu), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+                                       "-lms", "20"], stdout=self.f, stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
 
@@ -71,6 +71,17 @@ class Clocks:
         reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].strip() == "Active"})
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]), "reasons": reasons,
                 "samples": len(rows)}
+
+
+def ncu_traffic(kernel):
+    """DRAM bytes (read + write) per launch of `kernel` on this workload from
+    the committed ncu capture summary, or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
+            d = json.load(f)[kernel]
+        return d["dram_bytes_read"] + d["dram_bytes_write"]
+    except (OSError, KeyError):
+        return None
 
 
 def workload_config():
@@ -124,7 +135,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -211,7 +222,7 @@ def main():
         achieved = tu_bytes / (tu_ms * 1e-3) / 1e9
         roofline = {"kernel": "k_tu_stored (PCG real-space T.u, stored pair coefficients)", "bound": "hbm",
                     "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                    "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                    "frac": achieved / peaks["hbm_gbs"], "traffic": ncu_traffic("k_tu_stored"),
                     "bytes_per_launch": tu_bytes, "directed_pairs": tu_pairs, "avg_launch_ms": tu_ms,
                     "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({src}); L2 flushed before each timed launch"}
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

@@ -1,0 +1,381 @@
+// kernels_adjoint.cuh -- the hand-written adjoint (amg_backward), FP64.
+//
+// For L = c (em + ep) + <g_d, u_d> + <g_p, u_p>, with A u_d = E_d, A u_p = E_p
+// (A = alpha^-1 - T symmetric) and ep = -1/2 f u_d . E_p, one adjoint solve
+// A w = g (both right-hand sides, the forward's PCG) gives every parameter
+// gradient as the gradient, at fixed vectors, of the bilinear function
+//   G_L = c em + U_d(b_d <-> M) + U_p(b_p <-> M) + U_u(P1 <-> Q1) + U_u(P2 <-> Q2)
+// with b_d = c f/2 u_p - w_d, b_p = c f/2 u_d - w_p, (P1, Q1) = (b_d, u_d),
+// (P2, Q2) = (-w_p, u_p), U(a <-> b) the interaction energy of two sets, plus
+// the diagonal term -(b_d.u_d - w_p.u_p)_i / alpha_i^2 for dL/dalpha_i.
+// (For c = 1, g = 0 this is the forward's force function.)  Pair
+// intermediates are recomputed, never stored.
+#pragma once
+#include "kernels.cuh"
+#include "kernels_pair.cuh"
+
+namespace amg {
+
+// d(lambda_n)/dx of the Thole factors (n = 1..4 <-> lambda_3,5,7,9)
+__device__ __forceinline__ void thole_dlambda_dx(double x, double e, double (&d)[5]) {
+    d[0] = 0;
+    d[1] = e;
+    d[2] = x * e;
+    d[3] = (0.6 * x * x - 0.2 * x) * e;
+    d[4] = ((9.0 / 35.0) * x * x * x - (9.0 / 35.0) * x * x - (1.0 / 35.0) * x) * e;
+}
+
+// radial derivatives of a Thole channel: dB_n/d(damp) and dB_n/d(a)
+// (B_n = ... + scale lambda_n bare_n), n = 1..4; zero without damping
+__device__ __forceinline__ void thole_radial_derivs(double r, double damp, double a, double scale,
+                                                    const double (&bare)[6], double (&dBd)[6], double (&dBa)[6]) {
+    for (int k = 0; k < 6; k++) dBd[k] = dBa[k] = 0;
+    if (damp == 0.0) return;
+    double t = r / damp;
+    double x = a * t * t * t;
+    double e = exp(-x);
+    double dl[5];
+    thole_dlambda_dx(x, e, dl);
+    for (int n = 1; n <= 4; n++) {
+        dBd[n] = scale * bare[n] * dl[n] * (-3.0 * x / damp);
+        dBa[n] = a != 0.0 ? scale * bare[n] * dl[n] * (x / a) : 0.0;
+    }
+}
+
+// pair energies (for the parameter derivatives) -------------------------------
+__device__ __forceinline__ double md_energy(const Mpole<double>& Mi, const SiteInv<double>& si, V3<double> v,
+                                            V3<double> r, const double (&B)[6]) {
+    double av = dot(v, r);
+    return (-Mi.q * av + dot(Mi.d, v)) * B[1] + (-si.a * av + 2 * dot(v, si.Qr)) * B[2] - av * si.b * B[3];
+}
+__device__ __forceinline__ double dm_energy(V3<double> w, const Mpole<double>& Mk, const SiteInv<double>& sk,
+                                            V3<double> r, const double (&B)[6]) {
+    double aw = dot(w, r);
+    return (Mk.q * aw + dot(w, Mk.d)) * B[1] + (-aw * sk.a - 2 * dot(w, sk.Qr)) * B[2] + aw * sk.b * B[3];
+}
+__device__ __forceinline__ double dd_energy(V3<double> a, V3<double> b, V3<double> r, const double (&B)[6]) {
+    return dot(a, b) * B[1] - dot(a, r) * dot(b, r) * B[2];
+}
+
+// potential derivatives (phi, grad phi, grad grad phi: 10) at the target of
+// a multipole at the source, r = x_target - x_source, order xx yy zz xy xz yz
+__device__ __forceinline__ void mpole_potential10(const Mpole<double>& M, V3<double> r, const double (&B)[6],
+                                                  double (&p)[10]) {
+    SiteInv<double> s = invariants(M, r);
+    double rr[3] = {r.x, r.y, r.z}, d[3] = {M.d.x, M.d.y, M.d.z}, qr[3] = {s.Qr.x, s.Qr.y, s.Qr.z};
+    double Q[3][3] = {{M.Q.xx, M.Q.xy, M.Q.xz}, {M.Q.xy, M.Q.yy, M.Q.yz}, {M.Q.xz, M.Q.yz, M.Q.zz}};
+    p[0] = M.q * B[0] + s.a * B[1] + s.b * B[2];
+    for (int a = 0; a < 3; a++)
+        p[1 + a] = -M.q * rr[a] * B[1] + d[a] * B[1] - s.a * rr[a] * B[2] + 2 * qr[a] * B[2] - s.b * rr[a] * B[3];
+    const int ia[6] = {0, 1, 2, 0, 0, 1}, ib[6] = {0, 1, 2, 1, 2, 2};
+    double c2 = M.q * B[2] + s.a * B[3] + s.b * B[4], c1 = M.q * B[1] + s.a * B[2] + s.b * B[3];
+    for (int k = 0; k < 6; k++) {
+        int a = ia[k], b = ib[k];
+        double v = rr[a] * rr[b] * c2 - (d[a] * rr[b] + d[b] * rr[a]) * B[2] + 2 * Q[a][b] * B[2] -
+                   2 * (qr[a] * rr[b] + qr[b] * rr[a]) * B[3];
+        if (a == b) v -= c1;
+        p[4 + k] = v;
+    }
+}
+
+__device__ __forceinline__ V3<double> ld3v(const double* p, int i) { return v3<double>(p[3 * i], p[3 * i + 1], p[3 * i + 2]); }
+
+// effective vectors of the adjoint (all FP64, [3n] each)
+__global__ void k_adj_vectors(int n, double cf, const double* __restrict__ ud, const double* __restrict__ up,
+                              const double* __restrict__ wd, const double* __restrict__ wp, double* __restrict__ bd,
+                              double* __restrict__ bp, double* __restrict__ vbar, double* __restrict__ mwp,
+                              const double* __restrict__ pol, double* __restrict__ dpol) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double s = 0;
+    for (int c = 0; c < 3; c++) {
+        int q = 3 * i + c;
+        double a = 0.5 * cf * up[q] - (wd ? wd[q] : 0.0);
+        double b = 0.5 * cf * ud[q] - (wp ? wp[q] : 0.0);
+        bd[q] = a;
+        bp[q] = b;
+        vbar[q] = a + b;
+        mwp[q] = wp ? -wp[q] : 0.0;
+        s += a * ud[q] - (wp ? wp[q] * up[q] : 0.0);
+    }
+    // diagonal part of dA/dalpha_i: d(1/alpha)/dalpha = -1/alpha^2
+    dpol[i] = pol[i] > 0 ? -s / (pol[i] * pol[i]) : 0.0;
+}
+
+// Bulk real-space part of the adjoint, site i over its neighbour list:
+// gradient dG_L/dx_i, torque on M_i, the per-site potentials dG_L/dM_i (10),
+// and dG_L/d(pdamp_i), dG_L/d(thole_i).  Vectors as R4 [n][5]:
+// vbar, P1, Q1, P2, Q2.  mscale channel for M-M uses the cm factor (= c f).
+template <bool EWALD, int LPA>
+__global__ void __launch_bounds__(128) k_adjoint_pair(int n, const AtomR<double>* __restrict__ at,
+                                                      const double4* __restrict__ vec, Box bx, double aewald,
+                                                      const int* __restrict__ nbr, int cap,
+                                                      const int* __restrict__ nnb, int mutual, double cm,
+                                                      double* __restrict__ grad, double* __restrict__ trq,
+                                                      double* __restrict__ pot, double* __restrict__ dpd,
+                                                      double* __restrict__ dth) {
+    const int g = (blockIdx.x * blockDim.x + threadIdx.x) / LPA, lane = threadIdx.x % LPA;
+    const int i = min(g, n - 1);
+    const int cnt = g < n ? nnb[i] : 0;
+    const AtomR<double> Ai = at[i];
+    const Mpole<double> Mi = load_mpole(Ai);
+    const V3<double> xi = v3<double>(Ai.a.x, Ai.a.y, Ai.a.z);
+    auto V = [&](int j, int k) { double4 t = vec[5 * (size_t)j + k]; return v3<double>(t.x, t.y, t.z); };
+    const V3<double> vb_i = V(i, 0), p1_i = V(i, 1), q1_i = V(i, 2), p2_i = V(i, 3), q2_i = V(i, 4);
+    V3<double> gacc = v3<double>(0, 0, 0), tacc = v3<double>(0, 0, 0);
+    double pacc[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    double dpd_acc = 0, dth_acc = 0;
+    const int* row = nbr + (size_t)i * cap;
+    for (int s = lane; s < cnt; s += LPA) {
+        const int j = row[s];
+        const AtomR<double> Aj = at[j];
+        const Mpole<double> Mk = load_mpole(Aj);
+        const V3<double> r = min_image<double>(v3<double>(Aj.a.x, Aj.a.y, Aj.a.z) - xi, bx);  // x_k - x_i
+        const double r2 = dot(r, r), rr = sqrt(r2);
+        // multipole-multipole (em), no Thole, scale 1
+        double Bm[6];
+        bulk_radial<double, EWALD, false>(r2, aewald, 0.0, 0.0, Bm);
+        double E;
+        V3<double> gi, ti;
+        mm_pair_i<double>(Mi, Mk, r, Bm, E, gi, ti);
+        gacc = gacc + cm * gi;
+        tacc = tacc + cm * ti;
+        double pm[10];
+        mpole_potential10(Mk, (-1.0) * r, Bm, pm);  // potential of M_k at i
+        for (int k = 0; k < 10; k++) pacc[k] += cm * pm[k];
+        // polarization channels (Thole, scale 1)
+        const double damp = Ai.e.y * Aj.e.y, a = pair_thole<double>(Ai.e.z, Aj.e.z);
+        double B[6];
+        bulk_radial<double, EWALD, true>(r2, aewald, damp, a, B);
+        const V3<double> vb_k = V(j, 0), p1_k = V(j, 1), q1_k = V(j, 2), p2_k = V(j, 3), q2_k = V(j, 4);
+        const SiteInv<double> si = invariants(Mi, r), sk = invariants(Mk, r);
+        V3<double> d1, t1;
+        md_pair<double>(Mi, si, vb_k, r, B, d1, t1);
+        V3<double> dEdr = d1 + dm_pair<double>(vb_i, Mk, sk, r, B);
+        if (mutual)
+            dEdr = dEdr + dd_pair<double>(p1_i, q1_k, r, B) + dd_pair<double>(q1_i, p1_k, r, B) +
+                   dd_pair<double>(p2_i, q2_k, r, B) + dd_pair<double>(q2_i, p2_k, r, B);
+        gacc = gacc - dEdr;
+        tacc = tacc + t1;
+        // potential of the dipoles vbar_k at i (d/p channels coincide here)
+        Mpole<double> Dk;
+        Dk.q = 0;
+        Dk.d = vb_k;
+        Dk.Q = Sym<double>{0, 0, 0, 0, 0, 0};
+        double pd_[10];
+        mpole_potential10(Dk, (-1.0) * r, B, pd_);
+        for (int k = 0; k < 10; k++) pacc[k] += pd_[k];
+        // damping derivatives: the same pair energies with dB
+        double bare[6], dBd[6], dBa[6];
+        double rinv = 1.0 / rr;
+        bare_terms<double, 6>(rinv, rinv * rinv, bare);
+        thole_radial_derivs(rr, damp, a, 1.0, bare, dBd, dBa);
+        auto Gwith = [&](const double (&D)[6]) {
+            double e = md_energy(Mi, si, vb_k, r, D) + dm_energy(vb_i, Mk, sk, r, D);
+            if (mutual)
+                e += dd_energy(p1_i, q1_k, r, D) + dd_energy(q1_i, p1_k, r, D) + dd_energy(p2_i, q2_k, r, D) +
+                     dd_energy(q2_i, p2_k, r, D);
+            return e;
+        };
+        dpd_acc += Gwith(dBd) * Aj.e.y;  // d damp / d pdamp_i = pdamp_k
+        double ga = Gwith(dBa);
+        double ti_ = Ai.e.z, tk_ = Aj.e.z;
+        double lo = fmin(ti_, tk_);
+        double own = (lo == 0.0) ? (ti_ > tk_ ? 1.0 : ti_ == tk_ ? 0.5 : 0.0)
+                                 : (ti_ < tk_ ? 1.0 : ti_ == tk_ ? 0.5 : 0.0);
+        dth_acc += own * ga;
+    }
+    double out[18] = {gacc.x, gacc.y, gacc.z, tacc.x, tacc.y, tacc.z, dpd_acc, dth_acc};
+    for (int k = 0; k < 10; k++) out[8 + k] = pacc[k];
+#pragma unroll
+    for (int k = 0; k < 18; k++) out[k] = group_sum<LPA>(out[k]);
+    if (lane == 0 && g < n) {
+        for (int c = 0; c < 3; c++) {
+            grad[3 * i + c] += out[c];
+            trq[3 * i + c] += out[3 + c];
+        }
+        dpd[i] += out[6];
+        dth[i] += out[7];
+        for (int k = 0; k < 10; k++) pot[10 * (size_t)i + k] += out[8 + k];
+    }
+}
+
+// scaled pairs: the same quantities with each channel's own scale (FP64,
+// both sites, atomics)
+__global__ void k_adjoint_scaled(int np, const ScaledPair* __restrict__ sp, const double* __restrict__ xyz,
+                                 const double* __restrict__ rp10, const double* __restrict__ pdamp,
+                                 const double* __restrict__ thole, Box bx, double cut2, double aewald,
+                                 const double* __restrict__ bd, const double* __restrict__ bp,
+                                 const double* __restrict__ P1, const double* __restrict__ Q1,
+                                 const double* __restrict__ P2, const double* __restrict__ Q2, int mutual, double cm,
+                                 double* __restrict__ grad, double* __restrict__ trq, double* __restrict__ pot,
+                                 double* __restrict__ dpd, double* __restrict__ dth) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= np) return;
+    ScaledPair P = sp[t];
+    ScaledGeom G = scaled_geom(P, xyz, pdamp, thole, bx, cut2, aewald);
+    if (!G.inside) return;
+    const int i = P.i, k = P.k;
+    const V3<double> r = G.r, mr = (-1.0) * G.r;
+    const double rr = sqrt(dot(r, r));
+    Mpole<double> Mi = mpole64(rp10 + 10 * i), Mk = mpole64(rp10 + 10 * k);
+    double Bm[6], Bd[6], Bp[6], Bu[6];
+    scaled_radial(G, P.m, false, aewald > 0, Bm);
+    scaled_radial(G, P.d, true, aewald > 0, Bd);
+    scaled_radial(G, P.p, true, aewald > 0, Bp);
+    scaled_radial(G, P.u, true, aewald > 0, Bu);
+    // em
+    double E, E2;
+    V3<double> gi, ti, gk, tk;
+    mm_pair_i<double>(Mi, Mk, r, Bm, E, gi, ti);
+    mm_pair_i<double>(Mk, Mi, mr, Bm, E2, gk, tk);
+    add3(grad, i, cm * gi);
+    add3(grad, k, cm * gk);
+    add3(trq, i, cm * ti);
+    add3(trq, k, cm * tk);
+    double pim[10], pkm[10];
+    mpole_potential10(Mk, mr, Bm, pim);  // at i from M_k
+    mpole_potential10(Mi, r, Bm, pkm);   // at k from M_i
+    // polarization
+    V3<double> bdi = ld3(bd, i), bdk = ld3(bd, k), bpi = ld3(bp, i), bpk = ld3(bp, k);
+    SiteInv<double> si = invariants(Mi, r), sk_m = invariants(Mk, mr), sk = invariants(Mk, r);
+    V3<double> dEdr = v3<double>(0, 0, 0), tqi = v3<double>(0, 0, 0), tqk = v3<double>(0, 0, 0), d1, t1;
+    md_pair<double>(Mi, si, bdk, r, Bd, d1, t1);           // U_d(b_d,k ; M_i)
+    dEdr = dEdr + d1; tqi = tqi + t1;
+    md_pair<double>(Mk, sk_m, bdi, mr, Bd, d1, t1);        // U_d(b_d,i ; M_k)
+    dEdr = dEdr - d1; tqk = tqk + t1;
+    md_pair<double>(Mi, si, bpk, r, Bp, d1, t1);           // U_p(b_p,k ; M_i)
+    dEdr = dEdr + d1; tqi = tqi + t1;
+    md_pair<double>(Mk, sk_m, bpi, mr, Bp, d1, t1);        // U_p(b_p,i ; M_k)
+    dEdr = dEdr - d1; tqk = tqk + t1;
+    V3<double> p1i = ld3(P1, i), p1k = ld3(P1, k), q1i = ld3(Q1, i), q1k = ld3(Q1, k);
+    V3<double> p2i = ld3(P2, i), p2k = ld3(P2, k), q2i = ld3(Q2, i), q2k = ld3(Q2, k);
+    if (mutual)
+        dEdr = dEdr + dd_pair<double>(p1i, q1k, r, Bu) + dd_pair<double>(q1i, p1k, r, Bu) +
+               dd_pair<double>(p2i, q2k, r, Bu) + dd_pair<double>(q2i, p2k, r, Bu);
+    add3(grad, i, (-1.0) * dEdr);
+    add3(grad, k, dEdr);
+    add3(trq, i, tqi);
+    add3(trq, k, tqk);
+    // potentials at i and k from the other site's dipoles (d and p channels)
+    auto dip = [](V3<double> v) {
+        Mpole<double> D;
+        D.q = 0;
+        D.d = v;
+        D.Q = Sym<double>{0, 0, 0, 0, 0, 0};
+        return D;
+    };
+    double a1[10], a2[10], b1[10], b2[10];
+    mpole_potential10(dip(bdk), mr, Bd, a1);
+    mpole_potential10(dip(bpk), mr, Bp, a2);
+    mpole_potential10(dip(bdi), r, Bd, b1);
+    mpole_potential10(dip(bpi), r, Bp, b2);
+    for (int q = 0; q < 10; q++) {
+        atomicAdd(pot + 10 * (size_t)i + q, cm * pim[q] + a1[q] + a2[q]);
+        atomicAdd(pot + 10 * (size_t)k + q, cm * pkm[q] + b1[q] + b2[q]);
+    }
+    // damping derivatives
+    const double damp = pdamp[i] * pdamp[k];
+    const double a = pair_thole<double>(thole[i], thole[k]);
+    double dBd_d[6], dBd_a[6], dBp_d[6], dBp_a[6], dBu_d[6], dBu_a[6];
+    thole_radial_derivs(rr, damp, a, P.d, G.bare, dBd_d, dBd_a);
+    thole_radial_derivs(rr, damp, a, P.p, G.bare, dBp_d, dBp_a);
+    thole_radial_derivs(rr, damp, a, P.u, G.bare, dBu_d, dBu_a);
+    auto Gwith = [&](const double (&Dd)[6], const double (&Dp)[6], const double (&Du)[6]) {
+        double e = md_energy(Mi, si, bdk, r, Dd) + dm_energy(bdi, Mk, sk, r, Dd) + md_energy(Mi, si, bpk, r, Dp) +
+                   dm_energy(bpi, Mk, sk, r, Dp);
+        if (mutual)
+            e += dd_energy(p1i, q1k, r, Du) + dd_energy(q1i, p1k, r, Du) + dd_energy(p2i, q2k, r, Du) +
+                 dd_energy(q2i, p2k, r, Du);
+        return e;
+    };
+    double gdamp = Gwith(dBd_d, dBp_d, dBu_d), ga = Gwith(dBd_a, dBp_a, dBu_a);
+    atomicAdd(dpd + i, gdamp * pdamp[k]);
+    atomicAdd(dpd + k, gdamp * pdamp[i]);
+    double ti_ = thole[i], tk_ = thole[k], lo = fmin(ti_, tk_);
+    double own_i = (lo == 0.0) ? (ti_ > tk_ ? 1.0 : ti_ == tk_ ? 0.5 : 0.0) : (ti_ < tk_ ? 1.0 : ti_ == tk_ ? 0.5 : 0.0);
+    atomicAdd(dth + i, own_i * ga);
+    atomicAdd(dth + k, (1.0 - own_i) * ga);
+}
+
+// reciprocal + self parts of the adjoint:
+//   grad_k += vbar_k.gg(phiM) + M_k.g(phi_vbar) + P1_k.gg(phi_Q1) + Q1_k.gg(phi_P1)
+//             + P2_k.gg(phi_Q2) + Q2_k.gg(phi_P2)
+//   torque  = torque(M_k, phi_vbar) + selfc d_k x vbar_k
+//   pot    += c f (phiM + M self) + phi_vbar - selfc vbar (dipole slots)
+__global__ void k_adjoint_recip(int n, const double* __restrict__ rp10, const double* __restrict__ phiM,
+                                const double* __restrict__ phv, const double* __restrict__ ph1,
+                                const double* __restrict__ phq1, const double* __restrict__ ph2,
+                                const double* __restrict__ phq2, const double* __restrict__ vbar,
+                                const double* __restrict__ P1, const double* __restrict__ Q1,
+                                const double* __restrict__ P2, const double* __restrict__ Q2, int mutual,
+                                double selfc, double alpha, double cm, double* __restrict__ grad,
+                                double* __restrict__ trq, double* __restrict__ pot) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double* m = rp10 + 10 * i;
+    const double* pm = phiM + 20 * (size_t)i;
+    const double* pv = phv + 20 * (size_t)i;
+    V3<double> vb = ld3(vbar, i);
+    V3<double> g = cm * site_gradient(m, pm) + dipole_gradient(vb, pm) + site_gradient(m, pv);
+    if (mutual) {
+        g = g + dipole_gradient(ld3(P1, i), phq1 + 20 * (size_t)i) + dipole_gradient(ld3(Q1, i), ph1 + 20 * (size_t)i) +
+            dipole_gradient(ld3(P2, i), phq2 + 20 * (size_t)i) + dipole_gradient(ld3(Q2, i), ph2 + 20 * (size_t)i);
+    }
+    V3<double> d = v3<double>(m[1], m[2], m[3]);
+    V3<double> t = cm * site_torque(m, pm) + site_torque(m, pv) + selfc * cross(d, vb);
+    for (int c = 0; c < 3; c++) {
+        grad[3 * i + c] += c == 0 ? g.x : c == 1 ? g.y : g.z;
+        trq[3 * i + c] += c == 0 ? t.x : c == 1 ? t.y : t.z;
+    }
+    // potentials: recip of multipoles and of vbar; self of the multipoles
+    // (-T_erf(0) M) and of the induced-permanent coupling (-selfc vbar on d)
+    const double a2 = alpha * alpha, sp = 1.0 / kSqrtPi;
+    double self[10] = {-2 * alpha * sp * m[0],
+                       -(4 * a2 * alpha / 3) * sp * m[1], -(4 * a2 * alpha / 3) * sp * m[2],
+                       -(4 * a2 * alpha / 3) * sp * m[3],
+                       -(16 * a2 * a2 * alpha / 5) * sp * m[4], -(16 * a2 * a2 * alpha / 5) * sp * m[7],
+                       -(16 * a2 * a2 * alpha / 5) * sp * m[9], -(16 * a2 * a2 * alpha / 5) * sp * m[5],
+                       -(16 * a2 * a2 * alpha / 5) * sp * m[6], -(16 * a2 * a2 * alpha / 5) * sp * m[8]};
+    for (int k = 0; k < 10; k++) pot[10 * (size_t)i + k] += cm * (pm[k] + self[k]) + pv[k];
+    pot[10 * (size_t)i + 1] -= selfc * vb.x;
+    pot[10 * (size_t)i + 2] -= selfc * vb.y;
+    pot[10 * (size_t)i + 3] -= selfc * vb.z;
+}
+
+// dL/d(local pole): chain the global-frame potentials through the rotation
+// (d_g = A^T d_l, Q_g = A^T Q_l A), the chirality sign and the planar rule.
+// pot: [n][10] = dL/dq, dL/dd (3), dL/dQ element-wise xx yy zz xy xz yz.
+__global__ void k_pole_grad_local(int n, const double* __restrict__ xyz, const double* __restrict__ pole13,
+                                  const int* __restrict__ zax, const int* __restrict__ xax,
+                                  const int* __restrict__ yax, const int* __restrict__ axe,
+                                  const double* __restrict__ pot, double* __restrict__ dpole) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double a[3][3];
+    bool flip, planar;
+    frame_matrix(i, xyz, pole13, zax, xax, yax, axe, a, flip, planar);
+    const double* p = pot + 10 * (size_t)i;
+    double G[3][3] = {{p[4], p[7], p[8]}, {p[7], p[5], p[9]}, {p[8], p[9], p[6]}};
+    double out[13];
+    out[0] = p[0];
+    for (int r = 0; r < 3; r++) out[1 + r] = a[r][0] * p[1] + a[r][1] * p[2] + a[r][2] * p[3];
+    for (int r = 0; r < 3; r++)
+        for (int t = 0; t < 3; t++) {
+            double v = 0;
+            for (int pp = 0; pp < 3; pp++)
+                for (int q = 0; q < 3; q++) v += a[r][pp] * a[t][q] * G[pp][q];
+            out[4 + 3 * r + t] = v;
+        }
+    if (planar) {  // sp[1] = sp[6] = sp[10] = 0; sp[4] = sp[8] = (sp[4] + sp[8]) / 2
+        out[1] = out[6] = out[10] = 0;
+        double m = 0.5 * (out[4] + out[8]);
+        out[4] = out[8] = m;
+    }
+    if (flip) {
+        out[2] = -out[2]; out[5] = -out[5]; out[7] = -out[7]; out[9] = -out[9]; out[11] = -out[11];
+    }
+    for (int k = 0; k < 13; k++) dpole[13 * (size_t)i + k] = out[k];
+}
+
+}  // namespace amg

@@ -1,0 +1,34 @@
+"""Profiling driver: a few evaluations of a seeded water box, for ncu.
+
+    python -m polmdqc_b200.profile --waters 4096 --evals 3 [--fp64]
+
+Box sizes and PME grids are those of the benchmark configurations (216, 4,096
+and 32,768 waters).  Set AMG_NO_GRAPH=1 to run the eager path, whose kernels
+ncu can profile (it cannot see kernels inside graphs with conditional nodes).
+"""
+import argparse
+
+from . import abi, systems
+from .engine import Engine, Settings
+
+BOXES = {216: (18.643, 24), 4096: (49.7, 54), 32768: (99.3, 108)}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--waters", type=int, default=4096, choices=sorted(BOXES))
+    ap.add_argument("--evals", type=int, default=3)
+    ap.add_argument("--fp64", action="store_true")
+    a = ap.parse_args()
+    box, grid = BOXES[a.waters]
+    s = systems.water_box(a.waters, box, seed=0)
+    prec = abi.PREC_FP64 if a.fp64 else abi.PREC_MIXED
+    e = Engine(s, Settings(nfft=(grid,) * 3, precision=prec))
+    for _ in range(a.evals):
+        r = e.forward(abi.DO_ENERGY | abi.DO_GRADIENT)
+    print(f"em {r.em:.6f} ep {r.ep:.6f} pcg {r.pcg_iters} {e.stats()}")
+    e.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -16,6 +16,7 @@
 
 #include <algorithm>
 #include <initializer_list>
+#include <mutex>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -1469,3 +1470,182 @@ void amg_destroy(amg_ctx* ctx) {
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Allocation-free entry point.
+//
+// Some callers cannot let a library allocate device memory: codes that carve
+// all device memory out of one arena at start-up and forbid later allocation,
+// and codes that must not allocate between steps because cudaMalloc and
+// cudaFree synchronize the whole device.  amg_empole_direct_noalloc serves
+// them: it evaluates the reference's own electrostatics mode -- non-Ewald
+// multipoles, pairs within a cutoff, 1-n exclusion scaling (the empole_a loop
+// of src/md/empole.cpp:96-357) -- with every buffer supplied by the caller and
+// the kernels' scratch (rotated multipoles, site torques, per-block energy
+// partials) in one fixed device array declared below.  It calls no
+// cudaMalloc/cudaFree and no allocating library routine.
+// ===========================================================================
+
+namespace {
+
+constexpr int kNoAllocMaxAtoms = 16384;  // AMG_NOALLOC_MAX_ATOMS
+constexpr int kNoAllocLanes = 32;
+constexpr int kNoAllocThreads = 128;
+constexpr int kNoAllocBlocks = kNoAllocMaxAtoms * kNoAllocLanes / kNoAllocThreads;
+// scratch layout (doubles): rotated multipoles [n][10], torques [n][3],
+// energy partials [blocks]
+constexpr size_t kNoAllocScratch = (size_t)kNoAllocMaxAtoms * 13 + kNoAllocBlocks;
+
+// Every GPU that loads the library holds this array (about 1.7 MB) until exit.
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratch];
+
+// host-side device address of the scratch array, per device (the symbol's
+// name is only a host-side stand-in, not a device address)
+std::mutex g_noalloc_mutex;
+double* g_noalloc_ptr[64] = {};
+
+// rotate the multipoles (as the main path's frame code) into scratch
+__global__ void k_noalloc_rotate(int n, const double* __restrict__ xyz, const double* __restrict__ pole13,
+                                 const int* __restrict__ zax, const int* __restrict__ xax,
+                                 const int* __restrict__ yax, const int* __restrict__ axe,
+                                 double* __restrict__ rp10) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double m[10];
+    frame_and_rotate(i, xyz, pole13, zax, xax, yax, axe, m);
+    for (int j = 0; j < 10; j++) rp10[10 * i + j] = m[j];
+}
+
+// m-scale of pair (i, k) from i's 1-2..1-5 lists (later lists overwrite)
+__device__ __forceinline__ double noalloc_mscale(int i, int k, const int* const* off, const int* const* idx,
+                                                 const double* ms) {
+    double s = 1.0;
+    for (int b = 0; b < 4; b++)
+        for (int q = off[b][i]; q < off[b][i + 1]; q++)
+            if (idx[b][q] == k) s = ms[b];
+    return s;
+}
+
+struct NoAllocLists {
+    const int* off[4];
+    const int* idx[4];
+    double ms[4];
+};
+
+// all pairs within the cutoff (32 lanes per site), bare radial scaled by the
+// pair's m-scale; writes site torques, adds site gradients to dem, and one
+// energy partial per block
+__global__ void __launch_bounds__(kNoAllocThreads) k_noalloc_pairs(int n, const double* __restrict__ xyz,
+                                                                   const double* __restrict__ rp10, NoAllocLists L,
+                                                                   double L0, double L1, double L2, double cut2,
+                                                                   double f, double* __restrict__ trq,
+                                                                   double* __restrict__ dem,
+                                                                   double* __restrict__ partial) {
+    const int g = (blockIdx.x * blockDim.x + threadIdx.x) / kNoAllocLanes, lane = threadIdx.x % kNoAllocLanes;
+    const int i = min(g, n - 1);
+    const bool live = g < n;
+    Mpole<double> Mi = mpole64(rp10 + 10 * i);
+    double e = 0;
+    V3<double> gsum = v3<double>(0, 0, 0), tsum = v3<double>(0, 0, 0);
+    for (int k = lane; live && k < n; k += kNoAllocLanes) {
+        if (k == i) continue;
+        V3<double> r = v3<double>(xyz[3 * k] - xyz[3 * i], xyz[3 * k + 1] - xyz[3 * i + 1],
+                                  xyz[3 * k + 2] - xyz[3 * i + 2]);
+        if (L0 > 0) r.x -= L0 * rint(r.x / L0);
+        if (L1 > 0) r.y -= L1 * rint(r.y / L1);
+        if (L2 > 0) r.z -= L2 * rint(r.z / L2);
+        double r2 = dot(r, r);
+        if (r2 > cut2) continue;
+        double s = noalloc_mscale(i, k, L.off, L.idx, L.ms);
+        double B[6];
+        double rinv = 1.0 / sqrt(r2);
+        bare_terms<double, 6>(rinv, rinv * rinv, B);
+        for (int q = 0; q < 6; q++) B[q] *= s;
+        double E;
+        V3<double> gi, ti;
+        mm_pair_i<double>(Mi, mpole64(rp10 + 10 * k), r, B, E, gi, ti);
+        e += 0.5 * E;
+        gsum = gsum + gi;
+        tsum = tsum + ti;
+    }
+    double v[7] = {e, gsum.x, gsum.y, gsum.z, tsum.x, tsum.y, tsum.z};
+    for (int q = 0; q < 7; q++) v[q] = warp_sum(v[q]);
+    if (lane == 0 && live) {
+        dem[3 * i] += f * v[1]; dem[3 * i + 1] += f * v[2]; dem[3 * i + 2] += f * v[3];
+        trq[3 * i] = f * v[4]; trq[3 * i + 1] = f * v[5]; trq[3 * i + 2] = f * v[6];
+    }
+    __shared__ double blk[kNoAllocThreads / kNoAllocLanes];
+    if (lane == 0) blk[threadIdx.x / kNoAllocLanes] = live ? f * v[0] : 0.0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0;
+        for (int w = 0; w < kNoAllocThreads / kNoAllocLanes; w++) s += blk[w];
+        partial[blockIdx.x] = s;
+    }
+}
+
+// fixed-order sum of the block partials into *em
+__global__ void k_noalloc_energy(int nb, const double* __restrict__ partial, double* __restrict__ em) {
+    __shared__ double s[256];
+    double v = 0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) v += partial[b];
+    s[threadIdx.x] = v;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *em = s[0];
+}
+
+}  // namespace
+
+extern "C" int amg_empole_direct_noalloc(int32_t n, const double* xyz, const double* pole, const int32_t* zaxis,
+                                         const int32_t* xaxis, const int32_t* yaxis, const int32_t* polaxe,
+                                         const amg_list* bonded, const double m_scale[4], const double box[3],
+                                         double cutoff, double f, double* em, double* dem, void* stream) {
+    if (n <= 0 || !xyz || !pole || !zaxis || !xaxis || !yaxis || !polaxe || !bonded || !m_scale || !em || !dem ||
+        cutoff <= 0)
+        return AMG_ERR_BAD_ARG;
+    if (n > kNoAllocMaxAtoms) return AMG_ERR_OUT_OF_RANGE;  // scratch holds AMG_NOALLOC_MAX_ATOMS sites
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return AMG_ERR_NO_DEVICE;
+    double* scratch = nullptr;
+    {
+        // once per device, with that device current: the scratch array's
+        // device address (the first call on a device does this set-up)
+        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+        if (!g_noalloc_ptr[dev]) {
+            void* p = nullptr;
+            if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
+                cudaGetLastError();
+                return AMG_ERR_CUDA;
+            }
+            g_noalloc_ptr[dev] = (double*)p;
+        }
+        scratch = g_noalloc_ptr[dev];
+    }
+    if (box)
+        for (int a = 0; a < 3; a++)
+            if (box[a] > 0 && cutoff > 0.5 * box[a]) return AMG_ERR_BAD_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    double* rp10 = scratch;
+    double* trq = scratch + 10 * (size_t)kNoAllocMaxAtoms;
+    double* partial = scratch + 13 * (size_t)kNoAllocMaxAtoms;
+    NoAllocLists L;
+    for (int b = 0; b < 4; b++) {
+        if (!bonded[b].offsets || !bonded[b].indices) return AMG_ERR_BAD_ARG;
+        L.off[b] = bonded[b].offsets;
+        L.idx[b] = bonded[b].indices;
+        L.ms[b] = m_scale[b];
+    }
+    const unsigned nb = (unsigned)(((size_t)n * kNoAllocLanes + kNoAllocThreads - 1) / kNoAllocThreads);
+    k_noalloc_rotate<<<(n + 127) / 128, 128, 0, st>>>(n, xyz, pole, zaxis, xaxis, yaxis, polaxe, rp10);
+    k_noalloc_pairs<<<nb, kNoAllocThreads, 0, st>>>(n, xyz, rp10, L, box ? box[0] : 0.0, box ? box[1] : 0.0,
+                                                    box ? box[2] : 0.0, cutoff * cutoff, f, trq, dem, partial);
+    k_noalloc_energy<<<1, 256, 0, st>>>((int)nb, partial, em);
+    k_torque<<<(n + 127) / 128, 128, 0, st>>>(n, xyz, zaxis, xaxis, yaxis, polaxe, trq, dem);
+    if (cudaGetLastError() != cudaSuccess) return AMG_ERR_CUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return AMG_ERR_CUDA;
+    return AMG_OK;
+}

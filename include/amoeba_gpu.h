@@ -150,7 +150,9 @@ typedef struct amg_cotangents {
     const double* d_uinp;     /* [n*3] dL/duinp, or NULL */
 } amg_cotangents;
 
-/* Gradients of L with respect to the parameters; any pointer may be NULL. */
+/* Gradients of L with respect to the parameters (overwritten); any pointer
+ * may be NULL.  The quadrupole entries of d_pole are the gradient restricted
+ * to traceless quadrupoles (AMOEBA quadrupoles are traceless). */
 typedef struct amg_param_grads {
     double* d_pole;       /* [n*13] dL/d(local-frame pole) */
     double* d_polarity;   /* [n] dL/dpolarity (includes the pdamp = alpha^(1/6) path) */

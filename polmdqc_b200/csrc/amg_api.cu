@@ -10,6 +10,7 @@
 #include "kernels_pme.cuh"
 #include "kernels_pair.cuh"
 #include "kernels_misc.cuh"
+#include "kernels_adjoint.cuh"
 
 #include <cub/device/device_radix_sort.cuh>
 #include <cufft.h>
@@ -146,6 +147,13 @@ struct amg_ctx {
     long long kcount = 0, kmain = 0, kbody = 0, klast = 0;
     char* flushbuf = nullptr;
     size_t flush_bytes = 0;
+    // adjoint buffers (allocated on the first amg_backward)
+    double *adj = nullptr;       // [3n] x 11 vectors: gd gp wd wp bd bp vbar mwp grad trq zero
+    double *adj_pot = nullptr;   // [n][10]
+    double *adj_n = nullptr;     // [n] x 4: dpd dth dpol zero-pad
+    double4* adj_vec = nullptr;  // [n][5]
+    double* adj_phi = nullptr;   // [3][2][n][20]
+    double* adj_dpole = nullptr; // [n][13]
     std::string graph_note;
     double timing[5] = {0, 0, 0, 0, 0};
     // last forward state for the adjoint
@@ -1082,6 +1090,8 @@ void release(amg_ctx* ctx) {
     dfree(ctx->iter);
     dfree(ctx->cont);
     dfree(ctx->flushbuf);
+    dfree(ctx->adj); dfree(ctx->adj_pot); dfree(ctx->adj_n); dfree(ctx->adj_vec); dfree(ctx->adj_phi);
+    dfree(ctx->adj_dpole);
     if (ctx->st) { cudaStreamDestroy(ctx->st); ctx->st = nullptr; }
     if (ctx->st2) { cudaStreamDestroy(ctx->st2); ctx->st2 = nullptr; }
 }
@@ -1233,6 +1243,174 @@ int validate(const amg_params* P, std::string& why) {
     return AMG_OK;
 }
 
+__global__ void k_adj_pack(int n, const double* __restrict__ vbar, const double* __restrict__ p1,
+                           const double* __restrict__ q1, const double* __restrict__ p2,
+                           const double* __restrict__ q2, double4* __restrict__ vec) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double* src[5] = {vbar, p1, q1, p2, q2};
+    for (int k = 0; k < 5; k++)
+        vec[5 * (size_t)i + k] = make_double4(src[k][3 * i], src[k][3 * i + 1], src[k][3 * i + 2], 0.0);
+}
+
+__global__ void k_scale3(int n, const double* __restrict__ pol, const double* __restrict__ g, double* __restrict__ w) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int c = 0; c < 3; c++) w[3 * i + c] = pol[i] * g[3 * i + c];
+}
+
+// amg_backward: FP64 throughout (see kernels_adjoint.cuh for the algebra)
+int backward_impl(amg_ctx* ctx, const amg_cotangents* cot, amg_param_grads* gr) {
+    const int n = ctx->n;
+    cudaStream_t s = ctx->st;
+    const size_t n3 = 3 * (size_t)n;
+    if (!ctx->adj) {
+        dalloc(ctx, ctx->adj, 11 * n3);
+        dalloc(ctx, ctx->adj_pot, 10 * (size_t)n);
+        dalloc(ctx, ctx->adj_n, 4 * (size_t)n);
+        dalloc(ctx, ctx->adj_vec, 5 * (size_t)n);
+        dalloc(ctx, ctx->adj_phi, 3 * 2 * 20 * (size_t)n);
+        dalloc(ctx, ctx->adj_dpole, 13 * (size_t)n);
+    }
+    double *gd = ctx->adj, *gp = gd + n3, *wd = gp + n3, *wp = wd + n3, *bd = wp + n3, *bp = bd + n3,
+           *vbar = bp + n3, *mwp = vbar + n3, *grad = mwp + n3, *trq = grad + n3, *zeros = trq + n3;
+    double *dpd = ctx->adj_n, *dth = dpd + n, *dpol = dth + n;
+    const bool have_g = cot->d_uind || cot->d_uinp;
+    const bool iter = iterative(ctx);
+    // FP64 copies of the sites, stencils and T coefficients
+    rotate_and_pack<double>(ctx, s);
+    if (ctx->ewald) {
+        pme_prepare<double>(ctx, pme_of<double>(ctx));
+        pme_stencils<double>(ctx, s);
+    }
+    k_zero<double><<<nblk(2 * n3, 256), 256, 0, s>>>(wd, 2 * n3);
+    KCHECK();
+    k_zero<double><<<nblk(n3, 256), 256, 0, s>>>(zeros, n3);
+    KCHECK();
+    if (have_g && ctx->has_pol) {
+        // adjoint solve A w = g for both right-hand sides (the forward's PCG)
+        std::vector<double> h(n3, 0.0);
+        if (cot->d_uind) std::memcpy(h.data(), cot->d_uind, sizeof(double) * n3);
+        CK(cudaMemcpyAsync(gd, h.data(), sizeof(double) * n3, cudaMemcpyHostToDevice, s));
+        CK(cudaStreamSynchronize(s));
+        std::fill(h.begin(), h.end(), 0.0);
+        if (cot->d_uinp) std::memcpy(h.data(), cot->d_uinp, sizeof(double) * n3);
+        CK(cudaMemcpyAsync(gp, h.data(), sizeof(double) * n3, cudaMemcpyHostToDevice, s));
+        CK(cudaStreamSynchronize(s));
+        if (ctx->poltyp == AMG_POL_DIRECT) {
+            k_scale3<<<nblk(n), kThreads, 0, s>>>(n, ctx->pol, gd, wd);
+            KCHECK();
+            k_scale3<<<nblk(n), kThreads, 0, s>>>(n, ctx->pol, gp, wp);
+            KCHECK();
+        } else if (iter) {
+            ensure_coeff_buffers<double>(ctx, atoms_of<double>(ctx));
+            double *Ed = ctx->Ed, *Ep = ctx->Ep, *ud = ctx->ud, *up = ctx->up;
+            ctx->Ed = gd; ctx->Ep = gp; ctx->ud = wd; ctx->up = wp;
+            int guess = ctx->guess;
+            ctx->guess = 1;
+            k_scale3<<<nblk(n), kThreads, 0, s>>>(n, ctx->pol, gd, wd);
+            KCHECK();
+            k_scale3<<<nblk(n), kThreads, 0, s>>>(n, ctx->pol, gp, wp);
+            KCHECK();
+            bool ok = true;
+            try {
+                enqueue_pcg_init<double>(ctx, s, 0, 0);
+                int cont = 1;
+                while (true) {
+                    CK(cudaMemcpyAsync(&cont, ctx->cont, sizeof(int), cudaMemcpyDeviceToHost, s));
+                    CK(cudaStreamSynchronize(s));
+                    if (!cont) break;
+                    enqueue_pcg_iter<double>(ctx, s, 0, 0);
+                }
+            } catch (Fail&) {
+                ok = false;
+            }
+            ctx->Ed = Ed; ctx->Ep = Ep; ctx->ud = ud; ctx->up = up;
+            ctx->guess = guess;
+            if (!ok) throw Fail{AMG_ERR_CUDA};
+        }
+    }
+    const double c = cot->d_energy, f = ctx->f, cf = c * f;
+    k_adj_vectors<<<nblk(n), kThreads, 0, s>>>(n, cf, ctx->has_pol ? ctx->ud : zeros, ctx->has_pol ? ctx->up : zeros,
+                                               wd, wp, bd, bp, vbar, mwp, ctx->pol, dpol);
+    KCHECK();
+    k_adj_pack<<<nblk(n), kThreads, 0, s>>>(n, vbar, bd, ctx->ud, mwp, ctx->up, ctx->adj_vec);
+    KCHECK();
+    k_zero<double><<<nblk(2 * n3, 256), 256, 0, s>>>(grad, 2 * n3);
+    KCHECK();
+    k_zero<double><<<nblk(10 * (size_t)n, 256), 256, 0, s>>>(ctx->adj_pot, 10 * (size_t)n);
+    KCHECK();
+    k_zero<double><<<nblk(2 * (size_t)n, 256), 256, 0, s>>>(dpd, 2 * (size_t)n);
+    KCHECK();
+    const int mutual = ctx->poltyp == AMG_POL_MUTUAL;
+    LPA_DISPATCH(ctx->lpa, {
+        if (ctx->ewald)
+            k_adjoint_pair<true, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(
+                n, ctx->ad.at, ctx->adj_vec, ctx->bx, ctx->aewald, ctx->nbr, ctx->cap, ctx->nnb, mutual, cf, grad, trq,
+                ctx->adj_pot, dpd, dth);
+        else
+            k_adjoint_pair<false, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(
+                n, ctx->ad.at, ctx->adj_vec, ctx->bx, 0.0, ctx->nbr, ctx->cap, ctx->nnb, mutual, cf, grad, trq,
+                ctx->adj_pot, dpd, dth);
+    });
+    KCHECK();
+    if (ctx->nsp) {
+        k_adjoint_scaled<<<nblk(ctx->nsp), kThreads, 0, s>>>(ctx->nsp, ctx->sp, ctx->xyz, ctx->rp10, ctx->pdamp,
+                                                            ctx->thole, ctx->bx, ctx->cut * ctx->cut, ewald_alpha(ctx),
+                                                            bd, bp, bd, ctx->ud, mwp, ctx->up, mutual, cf, grad, trq,
+                                                            ctx->adj_pot, dpd, dth);
+        KCHECK();
+    }
+    double qtot = 0;
+    if (ctx->ewald) {
+        pme_mpole<double>(ctx, s);  // FP64 permanent potentials (overwrites the forward's phiM)
+        double* ph = ctx->adj_phi;
+        const size_t blk = 2 * 20 * (size_t)n;
+        pme_dipoles<double, 20>(ctx, s, vbar, bd, ph);              // phi of vbar, P1
+        pme_dipoles<double, 20>(ctx, s, ctx->ud, ctx->up, ph + blk);  // phi of Q1, Q2
+        pme_dipoles<double, 20>(ctx, s, mwp, zeros, ph + 2 * blk);    // phi of P2
+        const size_t one = 20 * (size_t)n;
+        k_adjoint_recip<<<nblk(n), kThreads, 0, s>>>(n, ctx->rp10, ctx->phiM, ph, ph + one, ph + blk, ph + 2 * blk,
+                                                     ph + blk + one, vbar, bd, ctx->ud, mwp, ctx->up, mutual,
+                                                     self_coef(ctx), ctx->aewald, cf, grad, trq, ctx->adj_pot);
+        KCHECK();
+        std::vector<double> r10(10 * (size_t)n);
+        CK(cudaMemcpyAsync(r10.data(), ctx->rp10, sizeof(double) * 10 * n, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        for (int i = 0; i < n; i++) qtot += r10[10 * (size_t)i];
+    }
+    k_torque<<<nblk(n), kThreads, 0, s>>>(n, ctx->xyz, ctx->zax, ctx->xax, ctx->yax, ctx->axe, trq, grad);
+    KCHECK();
+    k_pole_grad_local<<<nblk(n), kThreads, 0, s>>>(n, ctx->xyz, ctx->pole13, ctx->zax, ctx->xax, ctx->yax, ctx->axe,
+                                                   ctx->adj_pot, ctx->adj_dpole);
+    KCHECK();
+    std::vector<double> hx(n3), hpole(13 * (size_t)n), hn(3 * (size_t)n), hpol(n), hpd(n);
+    CK(cudaMemcpyAsync(hx.data(), grad, sizeof(double) * n3, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(hpole.data(), ctx->adj_dpole, sizeof(double) * 13 * n, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(hn.data(), dpd, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(hpol.data(), ctx->pol, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(hpd.data(), ctx->pdamp, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    // net-charge term of the Ewald energy, -f pi Q^2 / (2 V alpha^2): dq_i
+    double dq = 0;
+    if (ctx->ewald) {
+        double V = ctx->box[0] * ctx->box[1] * ctx->box[2];
+        dq = -cf * kPi * qtot / (V * ctx->aewald * ctx->aewald);
+    }
+    if (gr->d_xyz) std::memcpy(gr->d_xyz, hx.data(), sizeof(double) * n3);
+    if (gr->d_pole)
+        for (int i = 0; i < n; i++)
+            for (int k = 0; k < 13; k++) gr->d_pole[13 * (size_t)i + k] = hpole[13 * (size_t)i + k] + (k == 0 ? dq : 0.0);
+    for (int i = 0; i < n; i++) {
+        double dpd_i = hn[i], dth_i = hn[n + i], dpol_i = hn[2 * n + i];
+        // pdamp = alpha^(1/6): dpdamp/dalpha = pdamp / (6 alpha)
+        double chain = hpol[i] > 0 ? hpd[i] / (6.0 * hpol[i]) : 0.0;
+        if (gr->d_polarity) gr->d_polarity[i] = ctx->has_pol ? dpol_i + dpd_i * chain : 0.0;
+        if (gr->d_thole) gr->d_thole[i] = ctx->has_pol ? dth_i : 0.0;
+    }
+    return AMG_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1321,8 +1499,16 @@ int amg_forward(amg_ctx* ctx, int32_t flags, amg_results* res) {
 
 int amg_backward(amg_ctx* ctx, const amg_cotangents* cot, amg_param_grads* grads) {
     if (!ctx || !cot || !grads) return AMG_ERR_BAD_ARG;
-    ctx->err = "backward not implemented yet";
-    return AMG_ERR_UNSUPPORTED;
+    if (!ctx->have_forward) {
+        ctx->err = "amg_backward needs an amg_forward at the current coordinates";
+        return AMG_ERR_BAD_ARG;
+    }
+    try {
+        CK(cudaSetDevice(ctx->device));
+        return backward_impl(ctx, cot, grads);
+    } catch (Fail& f) {
+        return f.code;
+    }
 }
 
 int amg_bench(amg_ctx* ctx, int32_t flags, int32_t steps, int64_t flush_bytes, double* ms_steps,

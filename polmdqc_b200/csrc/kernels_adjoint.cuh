@@ -344,8 +344,9 @@ __global__ void k_adjoint_recip(int n, const double* __restrict__ rp10, const do
 }
 
 // dL/d(local pole): chain the global-frame potentials through the rotation
-// (d_g = A^T d_l, Q_g = A^T Q_l A), the chirality sign and the planar rule.
-// pot: [n][10] = dL/dq, dL/dd (3), dL/dQ element-wise xx yy zz xy xz yz.
+// (d_g = A^T d_l, Q_g = A^T Q_l A on the upper triangle), the chirality sign
+// and the planar rule.  pot: [n][10] = dL/dq, dL/dd (3), and the potential
+// second derivatives xx yy zz xy xz yz that multiply Q_g element-wise.
 __global__ void k_pole_grad_local(int n, const double* __restrict__ xyz, const double* __restrict__ pole13,
                                   const int* __restrict__ zax, const int* __restrict__ xax,
                                   const int* __restrict__ yax, const int* __restrict__ axe,
@@ -354,9 +355,11 @@ __global__ void k_pole_grad_local(int n, const double* __restrict__ xyz, const d
     if (i >= n) return;
     double a[3][3];
     bool flip, planar;
-    frame_matrix(i, xyz, pole13, zax, xax, yax, axe, a, flip, planar);
+    frame_matrix(i, xyz, zax, xax, yax, axe, a, flip, planar);
     const double* p = pot + 10 * (size_t)i;
-    double G[3][3] = {{p[4], p[7], p[8]}, {p[7], p[5], p[9]}, {p[8], p[9], p[6]}};
+    // the rotation uses the upper triangle of Q_g (p <= q), as the
+    // reference's rotsite; the compact off-diagonal derivative is 2 phi_pq
+    double G[3][3] = {{p[4], 2 * p[7], 2 * p[8]}, {0, p[5], 2 * p[9]}, {0, 0, p[6]}};
     double out[13];
     out[0] = p[0];
     for (int r = 0; r < 3; r++) out[1 + r] = a[r][0] * p[1] + a[r][1] * p[2] + a[r][2] * p[3];
@@ -367,6 +370,13 @@ __global__ void k_pole_grad_local(int n, const double* __restrict__ xyz, const d
                 for (int q = 0; q < 3; q++) v += a[r][pp] * a[t][q] * G[pp][q];
             out[4 + 3 * r + t] = v;
         }
+    // AMOEBA quadrupoles are traceless and the pair formulas assume it (as the
+    // reference's include/md/pairMpole.h does): report the gradient restricted
+    // to traceless quadrupoles
+    {
+        double tr = (out[4] + out[8] + out[12]) / 3.0;
+        out[4] -= tr; out[8] -= tr; out[12] -= tr;
+    }
     if (planar) {  // sp[1] = sp[6] = sp[10] = 0; sp[4] = sp[8] = (sp[4] + sp[8]) / 2
         out[1] = out[6] = out[10] = 0;
         double m = 0.5 * (out[4] + out[8]);

@@ -5,29 +5,28 @@
 
 namespace amg {
 
-// Local-to-global rotation of site i and the rotated multipole, following
-// the frame definitions of the reference's rotmat / rotsite
-// (src/md/rotpole.cpp:102-345, 356-425) and the chirality test of chkpole
-// (src/md/chkpole.cpp:44-89), applied without mutating the inputs.
-__device__ inline void frame_and_rotate(int i, const double* __restrict__ xyz, const double* __restrict__ pole13,
-                                        const int* __restrict__ zax, const int* __restrict__ xax,
-                                        const int* __restrict__ yax, const int* __restrict__ axe, double out[10]) {
+// Local-to-global rotation matrix of site i (rows: local x, y, z axes in
+// global coordinates), following the frame definitions of the reference's
+// rotmat (src/md/rotpole.cpp:102-345), with the chirality test of chkpole
+// (src/md/chkpole.cpp:44-89) reported as `flip` (the y-components of the
+// local multipole change sign) instead of mutating the inputs, and the
+// Z-Bisect planarity case reported as `planar`.
+__device__ inline void frame_matrix(int i, const double* __restrict__ xyz, const int* __restrict__ zax,
+                                    const int* __restrict__ xax, const int* __restrict__ yax,
+                                    const int* __restrict__ axe, double (&a)[3][3], bool& flip, bool& planar) {
     using D = double;
-    auto P = [&](int a) { return v3<D>(xyz[3 * a], xyz[3 * a + 1], xyz[3 * a + 2]); };
+    auto P = [&](int q) { return v3<D>(xyz[3 * q], xyz[3 * q + 1], xyz[3 * q + 2]); };
     auto unit = [](V3<D> v) { D s = 1.0 / sqrt(dot(v, v)); return s * v; };
-    double sp[13];
-    for (int j = 0; j < 13; j++) sp[j] = pole13[13 * i + j];
-    int ft = axe[i];
-    V3<D> xi = P(i);
+    const int ft = axe[i];
+    const V3<D> xi = P(i);
     V3<D> zv = v3<D>(0, 0, 1), xv = v3<D>(1, 0, 0);
-    bool planar = false;
+    flip = false;
+    planar = false;
     if (ft == AMG_FRAME_ZTHENX && yax[i] != 0) {
         int k = yax[i];
-        V3<D> a = xi, b = P(zax[i] - 1), c = P(xax[i] - 1), d = P(abs(k) - 1);
-        D vol = dot(a - d, cross(b - d, c - d));
-        if ((k < 0 && vol > 0) || (k > 0 && vol < 0)) {
-            sp[2] = -sp[2]; sp[5] = -sp[5]; sp[7] = -sp[7]; sp[9] = -sp[9]; sp[11] = -sp[11];
-        }
+        V3<D> pa = xi, pb = P(zax[i] - 1), pc = P(xax[i] - 1), pd = P(abs(k) - 1);
+        D vol = dot(pa - pd, cross(pb - pd, pc - pd));
+        flip = (k < 0 && vol > 0) || (k > 0 && vol < 0);
     }
     if (ft == AMG_FRAME_ZONLY) {
         zv = unit(P(zax[i] - 1) - xi);
@@ -57,18 +56,36 @@ __device__ inline void frame_and_rotate(int i, const double* __restrict__ xyz, c
         zv = unit(u1 + u2 + u3);
         xv = unit(u1 - dot(u1, zv) * zv);
     }
+    V3<D> yv = cross(zv, xv);
+    a[0][0] = xv.x; a[0][1] = xv.y; a[0][2] = xv.z;
+    a[1][0] = yv.x; a[1][1] = yv.y; a[1][2] = yv.z;
+    a[2][0] = zv.x; a[2][1] = zv.y; a[2][2] = zv.z;
+}
+
+// The rotated (global-frame) multipole of site i, compact [q, d, Qxx, Qxy,
+// Qxz, Qyy, Qyz, Qzz], as the reference's rotsite (src/md/rotpole.cpp:356-425):
+// d_g = A^T d_l, Q_g = A^T Q_l A.
+__device__ inline void frame_and_rotate(int i, const double* __restrict__ xyz, const double* __restrict__ pole13,
+                                        const int* __restrict__ zax, const int* __restrict__ xax,
+                                        const int* __restrict__ yax, const int* __restrict__ axe, double out[10]) {
+    double a[3][3];
+    bool flip, planar;
+    frame_matrix(i, xyz, zax, xax, yax, axe, a, flip, planar);
+    double sp[13];
+    for (int j = 0; j < 13; j++) sp[j] = pole13[13 * i + j];
+    if (flip) {
+        sp[2] = -sp[2]; sp[5] = -sp[5]; sp[7] = -sp[7]; sp[9] = -sp[9]; sp[11] = -sp[11];
+    }
     if (planar) {
         sp[1] = 0; sp[6] = 0; sp[10] = 0;
         sp[4] = sp[8] = 0.5 * (sp[4] + sp[8]);
     }
-    V3<D> yv = cross(zv, xv);
-    D a[3][3] = {{xv.x, xv.y, xv.z}, {yv.x, yv.y, yv.z}, {zv.x, zv.y, zv.z}};
     out[0] = sp[0];
     for (int c = 0; c < 3; c++) out[1 + c] = sp[1] * a[0][c] + sp[2] * a[1][c] + sp[3] * a[2][c];
-    D qg[3][3];
+    double qg[3][3];
     for (int p = 0; p < 3; p++)
         for (int q = p; q < 3; q++) {
-            D v = 0;
+            double v = 0;
             for (int r = 0; r < 3; r++)
                 for (int t = 0; t < 3; t++) v += a[r][p] * a[t][q] * sp[4 + 3 * r + t];
             qg[p][q] = v;

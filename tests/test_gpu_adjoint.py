@@ -1,0 +1,148 @@
+"""The hand-written adjoint (amg_backward) against finite differences and the
+analytic forces.
+
+Configuration: the 216-water box (648 atoms, PME 24^3) with seeded per-type
+1% Gaussian perturbations of the multipoles and polarizabilities, FP64,
+mutual polarization converged to 1e-10 D.  Central differences of the
+forward energy (step h) check d/d(pole), d/d(polarity) (through pdamp =
+alpha^(1/6) as well), d/d(thole) and d/dx; the dipole cotangents check the
+extra adjoint PCG solve.
+"""
+import copy
+
+import numpy as np
+import pytest
+
+from polmdqc_b200 import abi, systems
+from polmdqc_b200.engine import Engine, Settings
+
+pytestmark = pytest.mark.gpu
+
+FP64 = abi.PREC_FP64
+ST = Settings(nfft=(24, 24, 24), precision=FP64, poleps=1e-10, politer=200)
+
+
+def perturbed_box(seed=3):
+    """216 waters with 1% per-type Gaussian perturbations of pole and polarity."""
+    s = systems.water_box(216, 18.643, seed=0)
+    rng = np.random.default_rng(seed)
+    for t in np.unique(s.types):
+        m = s.types == t
+        s.pole[m] = s.pole[m] * (1 + 0.01 * rng.standard_normal(13))
+        s.pole[m, 5], s.pole[m, 6], s.pole[m, 9] = s.pole[m, 7], s.pole[m, 10], s.pole[m, 11]  # keep Q symmetric
+        tr = (s.pole[m, 4] + s.pole[m, 8] + s.pole[m, 12]) / 3                                  # and traceless
+        s.pole[m, 4] -= tr; s.pole[m, 8] -= tr; s.pole[m, 12] -= tr
+        s.polarity[m] = s.polarity[m] * (1 + 0.01 * rng.standard_normal())
+        s.thole[m] = s.thole[m] * (1 + 0.01 * rng.standard_normal())
+    s.pdamp = s.polarity ** (1 / 6)
+    return s
+
+
+def energy(s, flags=abi.DO_ENERGY, dipoles=False):
+    e = Engine(s, ST)
+    try:
+        r = e.forward(flags | (abi.DO_DIPOLES if dipoles else 0))
+    finally:
+        e.close()
+    return r
+
+
+@pytest.fixture(scope="module")
+def box():
+    return perturbed_box()
+
+
+@pytest.fixture(scope="module")
+def grads(box):
+    e = Engine(box, ST)
+    try:
+        r = e.forward(abi.DO_ENERGY | abi.DO_GRADIENT | abi.DO_DIPOLES)
+        g = e.backward(d_energy=1.0)
+    finally:
+        e.close()
+    return r, g
+
+
+def fd(box, mutate, h):
+    a, b = copy.deepcopy(box), copy.deepcopy(box)
+    mutate(a, +h)
+    mutate(b, -h)
+    ea, eb = energy(a), energy(b)
+    return ((ea.em + ea.ep) - (eb.em + eb.ep)) / (2 * h)
+
+
+def test_coordinate_gradient_equals_forces(grads):
+    r, g = grads
+    np.testing.assert_allclose(g["d_xyz"], r.dem + r.dep, atol=1e-8, rtol=0)
+
+
+# (atom, {pole entry: weight}): charges, dipoles, and symmetric traceless
+# quadrupole directions (the gradient is defined on traceless quadrupoles)
+DIRECTIONS = [(0, {0: 1.0}), (0, {3: 1.0}), (0, {4: 1.0, 8: -1.0}), (1, {1: 1.0}), (1, {12: 1.0, 4: -1.0}),
+              (1, {5: 1.0, 7: 1.0}), (4, {9: 1.0, 11: 1.0}), (5, {3: 1.0})]
+
+
+@pytest.mark.parametrize("atom,direction", DIRECTIONS)
+def test_pole_gradient_matches_fd(box, grads, atom, direction):
+    _, g = grads
+    h = 1e-5
+
+    def mutate(s, d):
+        for c, w in direction.items():
+            s.pole[atom, c] += w * d
+
+    an = sum(w * g["d_pole"][atom, c] for c, w in direction.items())
+    assert abs(fd(box, mutate, h) - an) < 1e-5 * max(1.0, abs(an))
+
+
+@pytest.mark.parametrize("atom", [0, 1, 7])
+def test_polarizability_and_thole_gradients_match_fd(box, grads, atom):
+    _, g = grads
+    h = 1e-5
+
+    def mut_pol(s, d):
+        s.polarity[atom] += d
+        s.pdamp = s.polarity ** (1 / 6)
+
+    def mut_thl(s, d):
+        s.thole[atom] += d
+
+    assert abs(fd(box, mut_pol, h) - g["d_polarity"][atom]) < 1e-5 * max(1.0, abs(g["d_polarity"][atom]))
+    assert abs(fd(box, mut_thl, h) - g["d_thole"][atom]) < 1e-5 * max(1.0, abs(g["d_thole"][atom]))
+
+
+def test_dipole_cotangents_need_the_adjoint_solve(box):
+    """L = <g_d, uind> + <g_p, uinp>: the extra PCG solve A w = g."""
+    rng = np.random.default_rng(11)
+    gd = rng.standard_normal(3 * box.n)
+    gp = rng.standard_normal(3 * box.n)
+    e = Engine(box, ST)
+    try:
+        e.forward(abi.DO_ENERGY | abi.DO_GRADIENT | abi.DO_DIPOLES)
+        g = e.backward(d_energy=0.0, d_uind=gd, d_uinp=gp)
+    finally:
+        e.close()
+
+    def L(s):
+        r = energy(s, dipoles=True)
+        return gd @ r.uind.reshape(-1) + gp @ r.uinp.reshape(-1)
+
+    h = 1e-5
+    for atom, comp in ((0, 0), (2, 3)):
+        a, b = copy.deepcopy(box), copy.deepcopy(box)
+        a.pole[atom, comp] += h
+        b.pole[atom, comp] -= h
+        num = (L(a) - L(b)) / (2 * h)
+        assert abs(num - g["d_pole"][atom, comp]) < 1e-5 * max(1.0, abs(num))
+    a, b = copy.deepcopy(box), copy.deepcopy(box)
+    a.polarity[3] += h
+    b.polarity[3] -= h
+    a.pdamp, b.pdamp = a.polarity ** (1 / 6), b.polarity ** (1 / 6)
+    num = (L(a) - L(b)) / (2 * h)
+    assert abs(num - g["d_polarity"][3]) < 1e-5 * max(1.0, abs(num))
+    for atom, ax in ((3, 1),):
+        a, b = copy.deepcopy(box), copy.deepcopy(box)
+        a.xyz[atom, ax] += h
+        b.xyz[atom, ax] -= h
+        num = (L(a) - L(b)) / (2 * h)
+        assert abs(num - g["d_xyz"][atom, ax]) < 1e-5 * max(1.0, abs(num))

@@ -198,19 +198,21 @@ def test_config_4096_waters_vs_oracle(w4096):
 
 def test_config_32768_waters_properties():
     """98,304 atoms, 108^3 grid: mixed vs FP64 on the GPU at the target error,
-    and translation invariance.  (The net force is not checked: smooth PME
-    does not conserve momentum exactly.)"""
+    and invariance under a shift by whole grid spacings.  (The net force is
+    not checked: smooth PME does not conserve momentum exactly.)"""
     s = systems.water_box(32768, 99.3, seed=0)
     g64 = run(s, Settings(nfft=(108, 108, 108), precision=FP64))
     gm = run(s, Settings(nfft=(108, 108, 108), precision=MIXED))
     assert gm.pcg_eps <= 1e-6 and g64.pcg_eps <= 1e-6
     assert rel(gm.em, g64.em) < 1e-6 and rel(gm.ep, g64.ep) < 1e-6
     assert frms(gm, g64) < 1e-4
+    # a shift by whole PME grid spacings changes no B-spline weight and no
+    # pair distance: the energy is unchanged to round-off (an arbitrary shift
+    # changes the PME interpolation error, ~1e-5 relative at this grid)
     shifted = systems.water_box(32768, 99.3, seed=0)
-    shifted.xyz = shifted.xyz + np.array([0.37, -1.21, 2.5])
+    shifted.xyz = shifted.xyz + np.array([3.0, -2.0, 5.0]) * (99.3 / 108)
     gs = run(shifted, Settings(nfft=(108, 108, 108), precision=FP64))
-    # PME is not exactly translation invariant; the drift is far below the target
-    assert rel(gs.em + gs.ep, g64.em + g64.ep) < 1e-6
+    assert rel(gs.em, g64.em) < 1e-10 and rel(gs.ep, g64.ep) < 1e-8
 
 
 # ---------------------------------------------------------------- status codes
@@ -231,8 +233,12 @@ def test_status_codes():
         e.close()
 
 
-def test_repeated_calls_reuse_the_captured_graph(w216):
-    e = Engine(w216, Settings(nfft=(24, 24, 24), precision=MIXED))
+@pytest.mark.parametrize("prec,tol", [(FP64, 1e-12), (MIXED, 1e-6)])
+def test_repeated_calls_reuse_the_captured_graph(w216, prec, tol):
+    """Replaying the captured evaluation, and again after new coordinates.
+    PME spreading adds with atomics, so results agree to round-off only
+    (FP32 grids in the mixed path)."""
+    e = Engine(w216, Settings(nfft=(24, 24, 24), precision=prec))
     try:
         a = e.forward()
         b = e.forward()
@@ -243,6 +249,6 @@ def test_repeated_calls_reuse_the_captured_graph(w216):
         d = e.forward()
     finally:
         e.close()
-    assert rel(a.em, b.em) < 1e-12 and rel(a.ep, b.ep) < 1e-12
-    assert rel(a.em + a.ep, c.em + c.ep) > 1e-9
-    assert rel(a.em, d.em) < 1e-12 and np.abs(a.dep - d.dep).max() < 1e-9
+    assert rel(a.em, b.em) < tol and rel(a.ep, b.ep) < tol
+    assert rel(a.em + a.ep, c.em + c.ep) > 1e-5
+    assert rel(a.em, d.em) < tol and np.abs(a.dep - d.dep).max() < 1e3 * tol

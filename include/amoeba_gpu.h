@@ -46,7 +46,7 @@
 extern "C" {
 #endif
 
-#define AMG_ABI_VERSION 1
+#define AMG_ABI_VERSION 2
 
 /* status codes */
 #define AMG_OK               0
@@ -121,6 +121,12 @@ typedef struct amg_params {
     int32_t precision;               /* AMG_PREC_* */
     int32_t pcg_guess;               /* polpcg.h pcgguess: start from direct dipoles */
     int32_t device;                  /* CUDA device ordinal */
+    /* Appended in ABI version 2 (zero keeps the version-1 behaviour): */
+    int32_t pcg_prec;                /* polpcg.h pcgprec: 1 = sparse preconditioner
+                                        M = 2 alpha + alpha T_u alpha over pairs within
+                                        usolvcut (Thole-damped, u-scaled, no Ewald);
+                                        0 = diagonal (alpha) */
+    double usolvcut;                 /* limits.h usolvcut (Angstrom), at most cutoff */
 } amg_params;
 
 typedef struct amg_results {

@@ -23,8 +23,12 @@
 //       Thole damping: Thole (1981) exponential charge smearing as used by
 //       AMOEBA (Ren & Ponder 2002/2003), pdamp = polarity^(1/6)
 //       (src/md/kpolar.cpp:474), pair thole = min (src/md/kpolar.cpp:516);
-//       induced dipoles: preconditioned conjugate gradients (diagonal
-//       preconditioner) on (alpha^-1 - T) u = E, two right-hand sides;
+//       induced dipoles: preconditioned conjugate gradients on
+//       (alpha^-1 - T) u = E, two right-hand sides, with the diagonal
+//       preconditioner alpha or (pcgprec, src/md/kpolar.cpp:84, cutoff
+//       usolvcut, src/md/cutoffs.cpp:61) the sparse first-order Neumann
+//       preconditioner M = w alpha + alpha T_u alpha over pairs within
+//       usolvcut (Thole-damped bare tensor, u-scaled), w = 2;
 //   * scale-factor semantics: src/md/empole.cpp:224-235 for m-scales; the
 //     p/d/u meanings documented in include/md/polpot.h:18-45.
 //
@@ -95,6 +99,8 @@ struct System {
     double poleps = 1e-6, debye = 4.80321;
     int politer = 100;
     bool guess = true;
+    bool prec = false;      // sparse preconditioner within usolvcut
+    double usolvcut = 0;
 };
 
 inline uint64_t pkey(int i, int k) {
@@ -836,6 +842,35 @@ int solve_dipoles(Work& w, Result& R, double tol_override, int maxit_override) {
             Au[i] = ia * up[i] - Fp[i];
         }
     };
+    // preconditioner z = M r: z_i = alpha_i (w r_i + sum_k T_ik alpha_k r_k),
+    // T over the pairs within usolvcut (bare Thole-damped, u-scaled)
+    constexpr double kPrecDiag = 2.0;
+    std::vector<Pair> upairs;
+    if (s.prec)
+        for (const Pair& P : w.pairs)
+            if (P.rr <= s.usolvcut) upairs.push_back(P);
+    auto precond = [&](const std::vector<V3>& r, std::vector<V3>& z) {
+        z.assign(s.n, V3{0, 0, 0});
+        if (!s.prec) {
+            for (int i = 0; i < s.n; i++) z[i] = s.pol[i] * r[i];
+            return;
+        }
+        std::vector<V3> sr(s.n);
+        for (int i = 0; i < s.n; i++) sr[i] = s.pol[i] * r[i];
+        std::vector<V3> acc(s.n, V3{0, 0, 0});
+        for (const Pair& P : upairs) {
+            double lam[6];
+            thole_lambda(s, P.i, P.k, P.rr, lam);
+            double su = pair_scales(s, P.i, P.k).u;
+            double bare[6];
+            bare_terms(P.rr, bare);
+            double B1 = su * lam[1] * bare[1], B2 = su * lam[2] * bare[2];
+            // field of a dipole v at separation r: B2 (r.v) r - B1 v (even in r)
+            acc[P.i] = acc[P.i] + B2 * dot(P.r, sr[P.k]) * P.r - B1 * sr[P.k];
+            acc[P.k] = acc[P.k] + B2 * dot(P.r, sr[P.i]) * P.r - B1 * sr[P.i];
+        }
+        for (int i = 0; i < s.n; i++) z[i] = s.pol[i] * (kPrecDiag * r[i] + acc[i]);
+    };
     std::vector<V3> ud = R.ud, up = R.up;
     if (!s.guess) { ud.assign(s.n, V3{0, 0, 0}); up.assign(s.n, V3{0, 0, 0}); }
     std::vector<V3> Ad, Ap;
@@ -843,11 +878,13 @@ int solve_dipoles(Work& w, Result& R, double tol_override, int maxit_override) {
     std::vector<V3> rd(s.n), rp(s.n), zd(s.n), zp(s.n), pd(s.n), pp(s.n);
     double rzd = 0, rzp = 0;
     for (int i = 0; i < s.n; i++) {
-        if (s.pol[i] <= 0) { rd[i] = rp[i] = zd[i] = zp[i] = pd[i] = pp[i] = V3{0, 0, 0}; continue; }
+        if (s.pol[i] <= 0) { rd[i] = rp[i] = V3{0, 0, 0}; continue; }
         rd[i] = R.Ed[i] - Ad[i];
         rp[i] = R.Ep[i] - Ap[i];
-        zd[i] = s.pol[i] * rd[i];
-        zp[i] = s.pol[i] * rp[i];
+    }
+    precond(rd, zd);
+    precond(rp, zp);
+    for (int i = 0; i < s.n; i++) {
         pd[i] = zd[i];
         pp[i] = zp[i];
         rzd += dot(rd[i], zd[i]);
@@ -871,8 +908,10 @@ int solve_dipoles(Work& w, Result& R, double tol_override, int maxit_override) {
             up[i] = up[i] + ap * pp[i];
             rd[i] = rd[i] - ad * Ad[i];
             rp[i] = rp[i] - ap * Ap[i];
-            zd[i] = s.pol[i] * rd[i];
-            zp[i] = s.pol[i] * rp[i];
+        }
+        precond(rd, zd);
+        precond(rp, zp);
+        for (int i = 0; i < s.n; i++) {
             nzd += dot(rd[i], zd[i]);
             nzp += dot(rp[i], zp[i]);
         }
@@ -1166,6 +1205,9 @@ int orc_forward(const amg_params* P, const double* xyz, const double box[6], int
     s.politer = P->politer;
     s.debye = P->debye;
     s.guess = P->pcg_guess;
+    s.prec = P->pcg_prec != 0;
+    s.usolvcut = std::min(P->usolvcut, P->cutoff);
+    if (s.prec && !(s.usolvcut > 0)) return AMG_ERR_BAD_ARG;
     if (opt) w.opt.kmax = opt->kmax;
     build_scales(s, P);
     rotate_multipoles(s, P);

@@ -52,6 +52,7 @@ class amg_params(C.Structure):
         ("poltyp", C.c_int32), ("poleps", C.c_double), ("politer", C.c_int32),
         ("electric", C.c_double), ("dielec", C.c_double), ("debye", C.c_double),
         ("precision", C.c_int32), ("pcg_guess", C.c_int32), ("device", C.c_int32),
+        ("pcg_prec", C.c_int32), ("usolvcut", C.c_double),
     ]
 
 

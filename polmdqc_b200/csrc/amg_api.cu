@@ -66,6 +66,14 @@ struct CufftTypes<double> {
     using C = cufftDoubleComplex;
 };
 
+// sites staged per batch by the brick spreading kernel, and its shared memory
+template <class R>
+constexpr int kBrickSites = sizeof(R) == 4 ? 256 : 128;
+template <class R>
+size_t brick_smem_bytes(size_t RE) {
+    return (2 * RE + (size_t)kBrickSites<R> * (6 * kOrder + 6)) * sizeof(R) + (size_t)kBrickSites<R> * sizeof(int);
+}
+
 template <class R>
 struct Pme {
     bool ready = false;
@@ -78,6 +86,14 @@ struct Pme {
     cufftHandle f1 = 0, i1 = 0, f2 = 0, i2 = 0;
     double infl_box[3] = {0, 0, 0};
     size_t G = 0, Gc = 0;
+    // sites sorted by the brick of their stencil start (dipole spreading)
+    Bricks bk{};
+    int nbricks = 0;
+    R* regions = nullptr;                    // [nbricks][2][E^3]
+    unsigned *bkeys = nullptr, *bskeys = nullptr;
+    int *bids = nullptr, *bsids = nullptr, *bstart = nullptr, *bend = nullptr;
+    char* btmp = nullptr;
+    size_t btmp_bytes = 0;
 };
 
 template <class R>
@@ -85,8 +101,11 @@ struct Atoms {
     AtomR<R>* at = nullptr;
     R4<R>* u4 = nullptr;  // [n][2] dipoles
     R4<R>* p4 = nullptr;  // [n][2] PCG directions
+    R4<R>* s4 = nullptr;  // [n][2] alpha r, input of the sparse preconditioner
     R4<R>* c0 = nullptr;  // [n][cap] stored T coefficients (r, B1)
     R* c1 = nullptr;      // [n][cap] B2
+    R4<R>* cu0 = nullptr; // [n][cap] sparse preconditioner coefficients (r, B1), rows nbru
+    R* cu1 = nullptr;     // [n][cap] B2
     int cap = 0;
 };
 
@@ -118,8 +137,14 @@ struct amg_ctx {
     size_t cubtmp_bytes = 0;
     int* nbr = nullptr;
     int* nnb = nullptr;
-    int cap = 0, lpa = 16;
+    int cap = 0, lpa = 16, num_sms = 148;
     int* overflow = nullptr;
+    // sparse PCG preconditioner (pcgprec): rows of the pairs within usolvcut,
+    // a subset of the neighbour rows, so they share the capacity cap
+    bool sparse_prec = false;
+    double usolvcut = 0;
+    int *nbru = nullptr, *nnbu = nullptr;
+    int capu = 0;
     double4* spos = nullptr;  // coordinates in cell order
     // vectors
     double *Ed = nullptr, *Ep = nullptr, *ud = nullptr, *up = nullptr, *rd = nullptr, *rp = nullptr, *zd = nullptr,
@@ -133,6 +158,11 @@ struct amg_ctx {
     Pme<float> pmf;
     Pme<double> pmd;
     cudaStream_t st = nullptr, st2 = nullptr;
+    // side streams: real-space pair kernels run there while the PME chain
+    // runs on the main stream; side[0] pairs with st, side[1] with st2 (the
+    // PCG loop body is captured on st2 into its own graph)
+    cudaStream_t side[2] = {nullptr, nullptr};
+    cudaEvent_t efork[2] = {}, ejoin[2] = {};
     cudaEvent_t ev[6] = {};
     CellGrid cg{};
     double cell_volume = 1.0;
@@ -321,6 +351,33 @@ void pme_prepare(amg_ctx* ctx, Pme<R>& pm) {
         CKFFT(cufftPlanMany(&pm.i2, 3, dims, nullptr, 1, 0, nullptr, 1, 0, CufftTypes<R>::c2r, 2));
         cufftHandle hs[4] = {pm.f1, pm.i1, pm.f2, pm.i2};
         for (int k = 0; k < 4; k++) CKFFT(cufftSetStream(hs[k], ctx->st));
+        // bricks: edge 12 or less, the last brick of an axis at least P-1 long
+        int Bv[3], nbv[3];
+        for (int a = 0; a < 3; a++) {
+            const int K = ctx->K[a];
+            int B = K <= 12 ? K : 12;
+            while (B > 6 && K % B != 0 && K % B < kOrder - 1) B--;
+            Bv[a] = B;
+            nbv[a] = (K + B - 1) / B;
+        }
+        pm.bk.B = make_int3(Bv[0], Bv[1], Bv[2]);
+        pm.bk.nb = make_int3(nbv[0], nbv[1], nbv[2]);
+        pm.bk.E = make_int3(Bv[0] + kOrder - 1, Bv[1] + kOrder - 1, Bv[2] + kOrder - 1);
+        pm.nbricks = nbv[0] * nbv[1] * nbv[2];
+        const size_t RE = (size_t)pm.bk.E.x * pm.bk.E.y * pm.bk.E.z;
+        dalloc(ctx, pm.regions, (size_t)pm.nbricks * 2 * RE);
+        dalloc(ctx, pm.bkeys, ctx->n);
+        dalloc(ctx, pm.bskeys, ctx->n);
+        dalloc(ctx, pm.bids, ctx->n);
+        dalloc(ctx, pm.bsids, ctx->n);
+        dalloc(ctx, pm.bstart, pm.nbricks);
+        dalloc(ctx, pm.bend, pm.nbricks);
+        size_t bytes = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, bytes, pm.bkeys, pm.bskeys, pm.bids, pm.bsids, ctx->n);
+        dalloc(ctx, pm.btmp, bytes);
+        pm.btmp_bytes = bytes;
+        CK(cudaFuncSetAttribute(k_spread_dipoles_brick<R, kOrder, kBrickSites<R>>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)brick_smem_bytes<R>(RE)));
         pm.ready = true;
     }
     if (pm.infl_box[0] != ctx->box[0] || pm.infl_box[1] != ctx->box[1] || pm.infl_box[2] != ctx->box[2]) {
@@ -353,6 +410,8 @@ void pme_destroy(Pme<R>& pm) {
     for (int k = 0; k < 4; k++)
         if (*hs[k]) { cufftDestroy(*hs[k]); *hs[k] = 0; }
     dfree(pm.grid); dfree(pm.phig); dfree(pm.cgrid); dfree(pm.infl); dfree(pm.theta); dfree(pm.k0);
+    dfree(pm.regions); dfree(pm.bkeys); dfree(pm.bskeys); dfree(pm.bids); dfree(pm.bsids); dfree(pm.bstart);
+    dfree(pm.bend); dfree(pm.btmp);
     pm.ready = false;
 }
 
@@ -420,9 +479,20 @@ void cell_grid(amg_ctx* ctx, const double* hxyz) {
 
 template <class R>
 void ensure_coeff_buffers(amg_ctx* ctx, Atoms<R>& A) {
+    if (ctx->sparse_prec && ctx->capu != ctx->cap) {
+        dalloc(ctx, ctx->nbru, (size_t)ctx->cap * ctx->n);
+        if (!ctx->nnbu) dalloc(ctx, ctx->nnbu, ctx->n);
+        ctx->capu = ctx->cap;
+        ctx->graph_dirty = true;
+    }
     if (A.cap == ctx->cap && A.c0) return;
     dalloc(ctx, A.c0, (size_t)ctx->cap * ctx->n);
     dalloc(ctx, A.c1, (size_t)ctx->cap * ctx->n);
+    if (ctx->sparse_prec) {
+        dalloc(ctx, A.cu0, (size_t)ctx->cap * ctx->n);
+        dalloc(ctx, A.cu1, (size_t)ctx->cap * ctx->n);
+        if (!A.s4) dalloc(ctx, A.s4, 2 * (size_t)ctx->n);
+    }
     A.cap = ctx->cap;
     ctx->graph_dirty = true;
 }
@@ -484,17 +554,58 @@ void enqueue_lists(amg_ctx* ctx, cudaStream_t s) {
     CK(cub::DeviceRadixSort::SortPairs(ctx->cubtmp, bytes, ctx->keys, ctx->skeys, ctx->ids, ctx->sids, n, 0, nbits, s));
     k_cell_bounds<<<nblk(n), kThreads, 0, s>>>(n, ctx->skeys, ctx->sids, ctx->xyz, ctx->cstart, ctx->cend, ctx->spos);
     KCHECK();
-    k_neighbors<<<nblk((size_t)n * 32), kThreads, 0, s>>>(n, ctx->spos, ctx->skeys, ctx->sids, ctx->cstart, ctx->cend,
-                                                          cg, ctx->bx, ctx->cut * ctx->cut, ctx->cap, ctx->xoff,
-                                                          ctx->xidx, ctx->nbr, ctx->nnb, ctx->overflow);
+    const double cut2 = ctx->cut * ctx->cut;
+    if (!cg.periodic || (cg.nc[0] >= 3 && cg.nc[1] >= 3 && cg.nc[2] >= 3)) {
+        // block per cell, stencil staged in shared memory; FP32 test with an
+        // FP64 decision within 1e-3 cut^2 of the cutoff
+        k_neighbors_cells<<<(unsigned)ncell, kNbrThreads, 0, s>>>(ctx->spos, ctx->sids, ctx->cstart, ctx->cend, cg,
+                                                                  ctx->bx, cut2, 1e-3 * cut2, ctx->cap, ctx->xoff,
+                                                                  ctx->xidx, ctx->nbr, ctx->nnb, ctx->overflow);
+    } else {
+        k_neighbors<<<nblk((size_t)n * 32), kThreads, 0, s>>>(n, ctx->spos, ctx->skeys, ctx->sids, ctx->cstart,
+                                                              ctx->cend, cg, ctx->bx, cut2, ctx->cap, ctx->xoff,
+                                                              ctx->xidx, ctx->nbr, ctx->nnb, ctx->overflow);
+    }
     KCHECK();
 }
 
+// Fork: the side stream of s starts after everything enqueued on s so far.
+// Join: s continues only after everything enqueued on the side stream.
+// Under stream capture these become graph edges.
+int side_index(const amg_ctx* ctx, cudaStream_t s) { return s == ctx->st2 ? 1 : 0; }
+
+cudaStream_t fork_side(amg_ctx* ctx, cudaStream_t s) {
+    const int k = side_index(ctx, s);
+    CK(cudaEventRecord(ctx->efork[k], s));
+    CK(cudaStreamWaitEvent(ctx->side[k], ctx->efork[k], 0));
+    return ctx->side[k];
+}
+
+void join_side(amg_ctx* ctx, cudaStream_t s) {
+    const int k = side_index(ctx, s);
+    CK(cudaEventRecord(ctx->ejoin[k], ctx->side[k]));
+    CK(cudaStreamWaitEvent(s, ctx->ejoin[k], 0));
+}
+
+// B-spline stencils of every site, and the sites sorted by brick
 template <class R>
 void pme_stencils(amg_ctx* ctx, cudaStream_t s) {
     Pme<R>& pm = pme_of<R>(ctx);
-    k_bspline<R, kOrder><<<nblk(ctx->n), kThreads, 0, s>>>(ctx->n, ctx->xyz, ctx->bx,
-                                                           make_int3(ctx->K[0], ctx->K[1], ctx->K[2]), pm.theta, pm.k0);
+    const int n = ctx->n;
+    k_bspline<R, kOrder><<<nblk(n), kThreads, 0, s>>>(n, ctx->xyz, ctx->bx, make_int3(ctx->K[0], ctx->K[1], ctx->K[2]),
+                                                      pm.theta, pm.k0);
+    KCHECK();
+    k_brick_keys<<<nblk(n), kThreads, 0, s>>>(n, pm.k0, pm.bk, pm.bkeys, pm.bids);
+    KCHECK();
+    int nbits = 1;
+    while ((1ull << nbits) < (unsigned long long)pm.nbricks) nbits++;
+    size_t bytes = pm.btmp_bytes;
+    CK(cub::DeviceRadixSort::SortPairs(pm.btmp, bytes, pm.bkeys, pm.bskeys, pm.bids, pm.bsids, n, 0, nbits, s));
+    k_zero<int><<<nblk(pm.nbricks, 256), 256, 0, s>>>(pm.bstart, pm.nbricks);
+    KCHECK();
+    k_zero<int><<<nblk(pm.nbricks, 256), 256, 0, s>>>(pm.bend, pm.nbricks);
+    KCHECK();
+    k_brick_bounds<<<nblk(n), kThreads, 0, s>>>(n, pm.bskeys, pm.bstart, pm.bend);
     KCHECK();
 }
 
@@ -524,8 +635,11 @@ void pme_dipole_grids(amg_ctx* ctx, cudaStream_t s, const double* vd, const doub
     Pme<R>& pm = pme_of<R>(ctx);
     int3 K = make_int3(ctx->K[0], ctx->K[1], ctx->K[2]);
     double sc[3] = {ctx->K[0] / ctx->box[0], ctx->K[1] / ctx->box[1], ctx->K[2] / ctx->box[2]};
-    k_spread_dipoles_pt<R, kOrder><<<ctx->n, 128, 0, s>>>(ctx->n, vd, vp, pm.theta, pm.k0, K, (R)sc[0], (R)sc[1],
-                                                           (R)sc[2], pm.grid, pm.G);
+    const size_t RE = (size_t)pm.bk.E.x * pm.bk.E.y * pm.bk.E.z;
+    k_spread_dipoles_brick<R, kOrder, kBrickSites<R>><<<pm.nbricks, 256, brick_smem_bytes<R>(RE), s>>>(
+        pm.bk, pm.bsids, pm.bstart, pm.bend, vd, vp, pm.theta, pm.k0, (R)sc[0], (R)sc[1], (R)sc[2], pm.regions);
+    KCHECK();
+    k_sum_bricks<R, kOrder><<<nblk(pm.G, 256), 256, 0, s>>>(pm.bk, K, pm.regions, pm.grid, pm.G);
     KCHECK();
     CKFFT(cufftSetStream(pm.f2, s));
     CKFFT(cufftSetStream(pm.i2, s));
@@ -564,21 +678,26 @@ void matvec(amg_ctx* ctx, cudaStream_t s, const double* vd, const double* vp, do
     Atoms<R>& A = atoms_of<R>(ctx);
     k_pack_u<R><<<nblk(n), kThreads, 0, s>>>(n, vd, vp, A.u4);
     KCHECK();
+    // real space on the side stream, PME on s
+    cudaStream_t r = ctx->ewald ? fork_side(ctx, s) : s;
     LPA_DISPATCH(ctx->lpa, {
         if (ctx->ewald)
-            k_Tu<R, true, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(n, A.at, A.u4, ctx->bx, (R)ctx->aewald, ctx->nbr,
+            k_Tu<R, true, L><<<nblk((size_t)n * L), kThreads, 0, r>>>(n, A.at, A.u4, ctx->bx, (R)ctx->aewald, ctx->nbr,
                                                                       ctx->cap, ctx->nnb, ctx->Fd, ctx->Fp);
         else
-            k_Tu<R, false, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(n, A.at, A.u4, ctx->bx, (R)0, ctx->nbr, ctx->cap,
+            k_Tu<R, false, L><<<nblk((size_t)n * L), kThreads, 0, r>>>(n, A.at, A.u4, ctx->bx, (R)0, ctx->nbr, ctx->cap,
                                                                        ctx->nnb, ctx->Fd, ctx->Fp);
     });
     KCHECK();
     if (ctx->nsp) {
-        k_scaled_Tu<<<nblk(ctx->nsp), kThreads, 0, s>>>(ctx->nsp, ctx->sp, ctx->xyz, ctx->pdamp, ctx->thole, ctx->bx,
+        k_scaled_Tu<<<nblk(ctx->nsp), kThreads, 0, r>>>(ctx->nsp, ctx->sp, ctx->xyz, ctx->pdamp, ctx->thole, ctx->bx,
                                                        ctx->cut * ctx->cut, ewald_alpha(ctx), vd, vp, ctx->Fd, ctx->Fp);
         KCHECK();
     }
-    if (ctx->ewald) pme_dipoles<R, 4>(ctx, s, vd, vp, ctx->phiU4);
+    if (ctx->ewald) {
+        pme_dipoles<R, 4>(ctx, s, vd, vp, ctx->phiU4);
+        join_side(ctx, s);
+    }
     k_matvec_finish<<<nblk(n), kThreads, 0, s>>>(n, vd, vp, ctx->Fd, ctx->Fp, ctx->phiU4, ctx->ewald, self_coef(ctx),
                                                  ctx->pol, Ad, Ap);
     KCHECK();
@@ -589,19 +708,27 @@ template <class R>
 void build_tu_coeffs(amg_ctx* ctx, cudaStream_t s) {
     const int n = ctx->n;
     Atoms<R>& A = atoms_of<R>(ctx);
+    const bool sp = ctx->sparse_prec;
+    const double u2 = ctx->usolvcut * ctx->usolvcut;
+    int* nbru = sp ? ctx->nbru : nullptr;
+    int* nnbu = sp ? ctx->nnbu : nullptr;
+    R4<R>* cu0 = sp ? A.cu0 : nullptr;
+    R* cu1 = sp ? A.cu1 : nullptr;
     LPA_DISPATCH(ctx->lpa, {
         if (ctx->ewald)
             k_tu_coeffs<R, true, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(n, A.at, ctx->bx, (R)ctx->aewald, ctx->nbr,
-                                                                             ctx->cap, ctx->nnb, A.c0, A.c1);
+                                                                             ctx->cap, ctx->nnb, A.c0, A.c1, (R)u2, nbru,
+                                                                             cu0, cu1, nnbu);
         else
             k_tu_coeffs<R, false, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(n, A.at, ctx->bx, (R)0, ctx->nbr, ctx->cap,
-                                                                              ctx->nnb, A.c0, A.c1);
+                                                                              ctx->nnb, A.c0, A.c1, (R)u2, nbru, cu0,
+                                                                              cu1, nnbu);
     });
     KCHECK();
     if (ctx->nsp) {
         k_scaled_coeffs<R><<<nblk(ctx->nsp), kThreads, 0, s>>>(ctx->nsp, ctx->sp, ctx->xyz, ctx->pdamp, ctx->thole,
                                                               ctx->bx, ctx->cut * ctx->cut, ewald_alpha(ctx), ctx->nnb,
-                                                              ctx->cap, ctx->nbr, A.c0, A.c1);
+                                                              ctx->cap, ctx->nbr, A.c0, A.c1, u2, nnbu, nbru, cu0, cu1);
         KCHECK();
     }
 }
@@ -612,18 +739,23 @@ void matvec_stored(amg_ctx* ctx, cudaStream_t s, const R4<R>* v4, const double* 
                    double* Ap) {
     const int n = ctx->n;
     Atoms<R>& A = atoms_of<R>(ctx);
+    // real space on the side stream, PME on s
+    cudaStream_t r = ctx->ewald ? fork_side(ctx, s) : s;
     LPA_DISPATCH(ctx->lpa, {
-        k_tu_stored<R, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(n, ctx->nbr, A.c0, A.c1, ctx->cap, ctx->nnb, ctx->xoff,
+        k_tu_stored<R, L><<<nblk((size_t)n * L), kThreads, 0, r>>>(n, ctx->nbr, A.c0, A.c1, ctx->cap, ctx->nnb, ctx->xoff,
                                                                     v4, ctx->Fd, ctx->Fp);
     });
     KCHECK();
     if (ctx->ewald) {
         Pme<R>& pm = pme_of<R>(ctx);
         pme_dipole_grids<R>(ctx, s, vd, vp);
+        join_side(ctx, s);
         int3 K = make_int3(ctx->K[0], ctx->K[1], ctx->K[2]);
         double sc[3] = {ctx->K[0] / ctx->box[0], ctx->K[1] / ctx->box[1], ctx->K[2] / ctx->box[2]};
-        k_gather_field_pt<R, kOrder><<<n, 128, 0, s>>>(n, pm.phig, pm.G, pm.theta, pm.k0, K, sc[0], sc[1], sc[2], vd, vp,
-                                                        ctx->Fd, ctx->Fp, self_coef(ctx), ctx->pol, Ad, Ap);
+        constexpr int G = 8;  // lanes per site
+        k_gather_field<R, kOrder, G><<<nblk((size_t)n * G), kThreads, 0, s>>>(
+            n, pm.phig, pm.G, pm.theta, pm.k0, K, sc[0], sc[1], sc[2], vd, vp, ctx->Fd, ctx->Fp, self_coef(ctx), ctx->pol,
+            Ad, Ap);
         KCHECK();
     } else {
         k_matvec_finish<<<nblk(n), kThreads, 0, s>>>(n, vd, vp, ctx->Fd, ctx->Fp, ctx->phiU4, 0, 0.0, ctx->pol, Ad, Ap);
@@ -636,6 +768,29 @@ bool iterative(const amg_ctx* ctx) { return ctx->has_pol && ctx->poltyp == AMG_P
 double pcg_threshold(const amg_ctx* ctx) {
     double t = ctx->poleps / ctx->debye;
     return t * t * ctx->npolar;
+}
+
+// diagonal weight of the sparse preconditioner M = w alpha + alpha T_u alpha
+// (2: fewest iterations on water boxes, with M safely positive definite)
+constexpr double kPrecDiag = 2.0;
+
+// z = M r for both residual sets from the packed s = alpha r (A.s4); adds
+// r.z to rz_out[0..1]; `first` also starts the directions p = z
+template <class R>
+void precondition(amg_ctx* ctx, cudaStream_t s, bool first, double* rz_out) {
+    const int n = ctx->n;
+    Atoms<R>& A = atoms_of<R>(ctx);
+    constexpr int L = 4;  // lanes per site: the rows are short
+    const unsigned blocks = (unsigned)std::min<size_t>(nblk((size_t)n * L), (size_t)ctx->num_sms * 8);
+    if (first)
+        k_precond<R, L, true><<<blocks, kThreads, 0, s>>>(n, ctx->nbru, A.cu0, A.cu1, ctx->cap, ctx->nnbu, ctx->xoff,
+                                                          A.s4, ctx->pol, kPrecDiag, ctx->rd, ctx->rp, ctx->zd, ctx->zp,
+                                                          ctx->pd, ctx->pp, A.p4, rz_out);
+    else
+        k_precond<R, L, false><<<blocks, kThreads, 0, s>>>(n, ctx->nbru, A.cu0, A.cu1, ctx->cap, ctx->nnbu, ctx->xoff,
+                                                           A.s4, ctx->pol, kPrecDiag, ctx->rd, ctx->rp, ctx->zd,
+                                                           ctx->zp, ctx->pd, ctx->pp, A.p4, rz_out);
+    KCHECK();
 }
 
 // set-up of the solve: r = E - A u0, z = p = alpha r, and the first control
@@ -656,11 +811,16 @@ void enqueue_pcg_init(amg_ctx* ctx, cudaStream_t s, cudaGraphConditionalHandle h
     k_pack_u<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->ud, ctx->up, A.u4);
     KCHECK();
     matvec_stored<R>(ctx, s, A.u4, ctx->ud, ctx->up, ctx->Apd, ctx->App);
-    k_pcg_init<<<nblk(n), kThreads, 0, s>>>(n, ctx->Ed, ctx->Ep, ctx->Apd, ctx->App, ctx->pol, ctx->rd, ctx->rp, ctx->zd,
-                                            ctx->zp, ctx->pd, ctx->pp, ctx->scal);
+    k_pcg_init<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->Ed, ctx->Ep, ctx->Apd, ctx->App, ctx->pol, ctx->rd, ctx->rp,
+                                               ctx->zd, ctx->zp, ctx->pd, ctx->pp, ctx->scal,
+                                               ctx->sparse_prec ? A.s4 : nullptr);
     KCHECK();
-    k_pack_u<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->pd, ctx->pp, A.p4);
-    KCHECK();
+    if (ctx->sparse_prec) {
+        precondition<R>(ctx, s, true, ctx->scal + RZ_D);
+    } else {
+        k_pack_u<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->pd, ctx->pp, A.p4);
+        KCHECK();
+    }
     k_pcg_control<<<1, 1, 0, s>>>(ctx->scal, ctx->iter, pcg_threshold(ctx), ctx->politer, 1, h, use_handle, ctx->cont);
     KCHECK();
 }
@@ -673,9 +833,11 @@ void enqueue_pcg_iter(amg_ctx* ctx, cudaStream_t s, cudaGraphConditionalHandle h
     matvec_stored<R>(ctx, s, A.p4, ctx->pd, ctx->pp, ctx->Apd, ctx->App);
     k_dot2<<<nblk(n3, 256), 256, 0, s>>>(n3, ctx->pd, ctx->Apd, ctx->pp, ctx->App, ctx->scal + PAP_D, ctx->scal + PAP_P);
     KCHECK();
-    k_pcg_update<<<nblk(n), kThreads, 0, s>>>(n, ctx->pol, ctx->pd, ctx->pp, ctx->Apd, ctx->App, ctx->ud, ctx->up,
-                                              ctx->rd, ctx->rp, ctx->zd, ctx->zp, ctx->scal);
+    k_pcg_update<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->pol, ctx->pd, ctx->pp, ctx->Apd, ctx->App, ctx->ud, ctx->up,
+                                                 ctx->rd, ctx->rp, ctx->zd, ctx->zp, ctx->scal,
+                                                 ctx->sparse_prec ? A.s4 : nullptr);
     KCHECK();
+    if (ctx->sparse_prec) precondition<R>(ctx, s, false, ctx->scal + RZN_D);
     k_pcg_dir<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->zd, ctx->zp, ctx->pd, ctx->pp, ctx->scal, A.p4);
     KCHECK();
     k_pcg_control<<<1, 1, 0, s>>>(ctx->scal, ctx->iter, pcg_threshold(ctx), ctx->politer, 0, h, use_handle, ctx->cont);
@@ -702,7 +864,14 @@ void enqueue_front(amg_ctx* ctx, cudaStream_t s) {
     CK(cudaEventRecord(ctx->ev[0], s));
     rotate_and_pack<R>(ctx, s);
     if (mixed && iterative(ctx)) rotate_and_pack<double>(ctx, s);
-    enqueue_lists(ctx, s);
+    k_zero<double><<<1, 32, 0, s>>>(ctx->eacc, 8);
+    KCHECK();
+    k_zero<unsigned long long><<<1, 32, 0, s>>>(ctx->cnt, 4);
+    KCHECK();
+    // neighbour list and real-space permanent field on the side stream; PME
+    // stencils and the reciprocal permanent potential on s
+    cudaStream_t r = fork_side(ctx, s);
+    enqueue_lists(ctx, r);
     if (ctx->ewald) {
         pme_stencils<R>(ctx, s);
         Pme<R>& pm = pme_of<R>(ctx);
@@ -715,31 +884,28 @@ void enqueue_front(amg_ctx* ctx, cudaStream_t s) {
             KCHECK();
         }
     }
-    k_zero<double><<<1, 32, 0, s>>>(ctx->eacc, 8);
-    KCHECK();
-    k_zero<unsigned long long><<<1, 32, 0, s>>>(ctx->cnt, 4);
-    KCHECK();
     CK(cudaEventRecord(ctx->ev[1], s));
     Atoms<R>& A = atoms_of<R>(ctx);
     const R aew = (R)ctx->aewald;
     if (ctx->has_pol) {
         LPA_DISPATCH(ctx->lpa, {
             if (ctx->ewald)
-                k_perm_field<R, true, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(n, A.at, ctx->bx, aew, ctx->nbr, ctx->cap,
+                k_perm_field<R, true, L><<<nblk((size_t)n * L), kThreads, 0, r>>>(n, A.at, ctx->bx, aew, ctx->nbr, ctx->cap,
                                                                                   ctx->nnb, ctx->Ed, ctx->Ep);
             else
-                k_perm_field<R, false, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(n, A.at, ctx->bx, aew, ctx->nbr,
+                k_perm_field<R, false, L><<<nblk((size_t)n * L), kThreads, 0, r>>>(n, A.at, ctx->bx, aew, ctx->nbr,
                                                                                    ctx->cap, ctx->nnb, ctx->Ed, ctx->Ep);
         });
         KCHECK();
         if (ctx->nsp) {
-            k_scaled_field<<<nblk(ctx->nsp), kThreads, 0, s>>>(ctx->nsp, ctx->sp, ctx->xyz, ctx->rp10, ctx->pdamp,
+            k_scaled_field<<<nblk(ctx->nsp), kThreads, 0, r>>>(ctx->nsp, ctx->sp, ctx->xyz, ctx->rp10, ctx->pdamp,
                                                               ctx->thole, ctx->bx, ctx->cut * ctx->cut, ewald_alpha(ctx),
                                                               ctx->Ed, ctx->Ep);
             KCHECK();
         }
     }
     if (ctx->ewald) pme_mpole<R>(ctx, s);
+    join_side(ctx, s);
     if (ctx->has_pol) {
         k_field_finish<<<nblk(n), kThreads, 0, s>>>(n, ctx->phiM, ctx->ewald, ctx->rp10, self_coef(ctx), ctx->pol, ctx->Ed,
                                                     ctx->Ep, ctx->ud, ctx->up);
@@ -754,9 +920,11 @@ void enqueue_back(amg_ctx* ctx, cudaStream_t s, int flags) {
     const int n = ctx->n;
     const bool grad = flags & AMG_DO_GRADIENT;
     const bool analysis = flags & AMG_DO_ANALYSIS;
+    const bool polgrad = grad && ctx->has_pol;
     const double cut2 = ctx->cut * ctx->cut;
     Atoms<R>& A = atoms_of<R>(ctx);
     const R aew = (R)ctx->aewald;
+    const int mutual = ctx->poltyp == AMG_POL_MUTUAL;
     CK(cudaEventRecord(ctx->ev[3], s));
     k_zero<double><<<nblk(3 * n, 256), 256, 0, s>>>(ctx->grad_m, 3 * (size_t)n);
     KCHECK();
@@ -764,74 +932,83 @@ void enqueue_back(amg_ctx* ctx, cudaStream_t s, int flags) {
     KCHECK();
     k_zero<double><<<nblk(n, 256), 256, 0, s>>>(ctx->aem, (size_t)n);
     KCHECK();
+    if (polgrad) {
+        k_zero<double><<<nblk(3 * n, 256), 256, 0, s>>>(ctx->grad_p, 3 * (size_t)n);
+        KCHECK();
+        k_zero<double><<<nblk(3 * n, 256), 256, 0, s>>>(ctx->trq_p, 3 * (size_t)n);
+        KCHECK();
+        k_pack_u<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->ud, ctx->up, A.u4);
+        KCHECK();
+    }
+    // Real-space pair kernels (atomic accumulation) on the side stream; the
+    // PME dipole potentials and the polarization energy on s.  The
+    // reciprocal-space force kernels add to the same arrays without atomics,
+    // so they run after the join.
+    cudaStream_t r = fork_side(ctx, s);
     const int* mol = ctx->mol;
     LPA_DISPATCH(ctx->lpa, {
         const size_t nb = nblk((size_t)n * L);
         if (ctx->ewald) {
             if (analysis)
-                k_mpole_pair<R, true, true, L><<<nb, kThreads, 0, s>>>(n, A.at, ctx->bx, aew, ctx->nbr, ctx->cap, ctx->nnb,
+                k_mpole_pair<R, true, true, L><<<nb, kThreads, 0, r>>>(n, A.at, ctx->bx, aew, ctx->nbr, ctx->cap, ctx->nnb,
                                                                        ctx->f, ctx->grad_m, ctx->trq_m, ctx->eacc,
                                                                        ctx->aem, mol, ctx->cnt);
             else
-                k_mpole_pair<R, true, false, L><<<nb, kThreads, 0, s>>>(n, A.at, ctx->bx, aew, ctx->nbr, ctx->cap,
+                k_mpole_pair<R, true, false, L><<<nb, kThreads, 0, r>>>(n, A.at, ctx->bx, aew, ctx->nbr, ctx->cap,
                                                                         ctx->nnb, ctx->f, ctx->grad_m, ctx->trq_m,
                                                                         ctx->eacc, nullptr, nullptr, nullptr);
         } else {
             if (analysis)
-                k_mpole_pair<R, false, true, L><<<nb, kThreads, 0, s>>>(n, A.at, ctx->bx, aew, ctx->nbr, ctx->cap,
+                k_mpole_pair<R, false, true, L><<<nb, kThreads, 0, r>>>(n, A.at, ctx->bx, aew, ctx->nbr, ctx->cap,
                                                                         ctx->nnb, ctx->f, ctx->grad_m, ctx->trq_m,
                                                                         ctx->eacc, ctx->aem, mol, ctx->cnt);
             else
-                k_mpole_pair<R, false, false, L><<<nb, kThreads, 0, s>>>(n, A.at, ctx->bx, aew, ctx->nbr, ctx->cap,
+                k_mpole_pair<R, false, false, L><<<nb, kThreads, 0, r>>>(n, A.at, ctx->bx, aew, ctx->nbr, ctx->cap,
                                                                          ctx->nnb, ctx->f, ctx->grad_m, ctx->trq_m,
                                                                          ctx->eacc, nullptr, nullptr, nullptr);
         }
     });
     KCHECK();
     if (ctx->nsp) {
-        k_scaled_mpole<<<nblk(ctx->nsp), kThreads, 0, s>>>(ctx->nsp, ctx->sp, ctx->xyz, ctx->rp10, ctx->bx, cut2,
+        k_scaled_mpole<<<nblk(ctx->nsp), kThreads, 0, r>>>(ctx->nsp, ctx->sp, ctx->xyz, ctx->rp10, ctx->bx, cut2,
                                                           ewald_alpha(ctx), ctx->f, ctx->grad_m, ctx->trq_m, ctx->eacc,
                                                           analysis ? ctx->aem : nullptr, analysis ? mol : nullptr,
                                                           analysis ? ctx->cnt : nullptr);
         KCHECK();
     }
-    if (ctx->ewald) {
-        k_recip_mpole<<<nblk(n), kThreads, 0, s>>>(n, ctx->rp10, ctx->phiM, ctx->f, ctx->aewald, ctx->grad_m, ctx->trq_m,
-                                                   ctx->eacc + 2, analysis ? ctx->aem : nullptr, ctx->eacc + 3);
+    if (polgrad) {
+        LPA_DISPATCH(ctx->lpa, {
+            if (ctx->ewald)
+                k_polar_pair<R, true, L><<<nblk((size_t)n * L), kThreads, 0, r>>>(n, A.at, A.u4, ctx->bx, aew, ctx->nbr,
+                                                                                  ctx->cap, ctx->nnb, mutual, ctx->f,
+                                                                                  ctx->grad_p, ctx->trq_p);
+            else
+                k_polar_pair<R, false, L><<<nblk((size_t)n * L), kThreads, 0, r>>>(n, A.at, A.u4, ctx->bx, aew, ctx->nbr,
+                                                                                   ctx->cap, ctx->nnb, mutual, ctx->f,
+                                                                                   ctx->grad_p, ctx->trq_p);
+        });
         KCHECK();
+        if (ctx->nsp) {
+            k_scaled_polar<<<nblk(ctx->nsp), kThreads, 0, r>>>(ctx->nsp, ctx->sp, ctx->xyz, ctx->rp10, ctx->pdamp,
+                                                              ctx->thole, ctx->bx, cut2, ewald_alpha(ctx), ctx->ud,
+                                                              ctx->up, mutual, ctx->f, ctx->grad_p, ctx->trq_p);
+            KCHECK();
+        }
     }
     if (ctx->has_pol) {
         k_polar_energy<<<nblk(n), kThreads, 0, s>>>(n, ctx->ud, ctx->Ep, ctx->f, ctx->eacc + 4,
                                                     analysis ? ctx->aep : nullptr, ctx->cnt + 1);
         KCHECK();
     }
-    if (grad && ctx->has_pol) {
-        k_zero<double><<<nblk(3 * n, 256), 256, 0, s>>>(ctx->grad_p, 3 * (size_t)n);
+    if (polgrad && ctx->ewald) pme_dipoles<R, 20>(ctx, s, ctx->ud, ctx->up, ctx->phiU);
+    join_side(ctx, s);
+    if (ctx->ewald) {
+        k_recip_mpole<<<nblk(n), kThreads, 0, s>>>(n, ctx->rp10, ctx->phiM, ctx->f, ctx->aewald, ctx->grad_m, ctx->trq_m,
+                                                   ctx->eacc + 2, analysis ? ctx->aem : nullptr, ctx->eacc + 3);
         KCHECK();
-        k_zero<double><<<nblk(3 * n, 256), 256, 0, s>>>(ctx->trq_p, 3 * (size_t)n);
-        KCHECK();
-        int mutual = ctx->poltyp == AMG_POL_MUTUAL;
-        k_pack_u<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->ud, ctx->up, A.u4);
-        KCHECK();
-        LPA_DISPATCH(ctx->lpa, {
-            if (ctx->ewald)
-                k_polar_pair<R, true, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(n, A.at, A.u4, ctx->bx, aew, ctx->nbr,
-                                                                                  ctx->cap, ctx->nnb, mutual, ctx->f,
-                                                                                  ctx->grad_p, ctx->trq_p);
-            else
-                k_polar_pair<R, false, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(n, A.at, A.u4, ctx->bx, aew, ctx->nbr,
-                                                                                   ctx->cap, ctx->nnb, mutual, ctx->f,
-                                                                                   ctx->grad_p, ctx->trq_p);
-        });
-        KCHECK();
-        if (ctx->nsp) {
-            k_scaled_polar<<<nblk(ctx->nsp), kThreads, 0, s>>>(ctx->nsp, ctx->sp, ctx->xyz, ctx->rp10, ctx->pdamp,
-                                                              ctx->thole, ctx->bx, cut2, ewald_alpha(ctx), ctx->ud,
-                                                              ctx->up, mutual, ctx->f, ctx->grad_p, ctx->trq_p);
-            KCHECK();
-        }
+    }
+    if (polgrad) {
         if (ctx->ewald) {
-            pme_dipoles<R, 20>(ctx, s, ctx->ud, ctx->up, ctx->phiU);
             k_recip_polar<<<nblk(n), kThreads, 0, s>>>(n, ctx->rp10, ctx->phiM, ctx->phiU, ctx->phiU + 20 * (size_t)n,
                                                        ctx->ud, ctx->up, mutual, self_coef(ctx), ctx->f, ctx->grad_p,
                                                        ctx->trq_p);
@@ -1082,10 +1259,17 @@ void release(amg_ctx* ctx) {
     ctx->cubtmp = nullptr;
     dfree(ctx->af.at); dfree(ctx->af.u4); dfree(ctx->ad.at); dfree(ctx->ad.u4);
     dfree(ctx->af.p4); dfree(ctx->ad.p4); dfree(ctx->af.c0); dfree(ctx->af.c1); dfree(ctx->ad.c0); dfree(ctx->ad.c1);
+    dfree(ctx->af.s4); dfree(ctx->ad.s4); dfree(ctx->af.cu0); dfree(ctx->af.cu1); dfree(ctx->ad.cu0);
+    dfree(ctx->ad.cu1); dfree(ctx->nbru); dfree(ctx->nnbu);
     pme_destroy(ctx->pmf);
     pme_destroy(ctx->pmd);
     for (auto& e : ctx->ev)
         if (e) { cudaEventDestroy(e); e = nullptr; }
+    for (int k = 0; k < 2; k++) {
+        if (ctx->efork[k]) { cudaEventDestroy(ctx->efork[k]); ctx->efork[k] = nullptr; }
+        if (ctx->ejoin[k]) { cudaEventDestroy(ctx->ejoin[k]); ctx->ejoin[k] = nullptr; }
+        if (ctx->side[k]) { cudaStreamDestroy(ctx->side[k]); ctx->side[k] = nullptr; }
+    }
     if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
     dfree(ctx->iter);
     dfree(ctx->cont);
@@ -1109,6 +1293,7 @@ int create_impl(amg_ctx* ctx, const amg_params* P) {
     CK(cudaSetDevice(P->device));
     cudaDeviceProp prop;
     CK(cudaGetDeviceProperties(&prop, P->device));
+    ctx->num_sms = prop.multiProcessorCount;
     if (prop.major < 10) {
         ctx->err = "libamoeba_gpu is built for sm_100a (B200)";
         return AMG_ERR_NO_DEVICE;
@@ -1128,9 +1313,16 @@ int create_impl(amg_ctx* ctx, const amg_params* P) {
     ctx->guess = P->pcg_guess;
     ctx->has_pol = P->polarity != nullptr && P->poltyp != AMG_POL_NONE;
     ctx->poltyp = ctx->has_pol ? P->poltyp : AMG_POL_NONE;
+    ctx->sparse_prec = ctx->has_pol && ctx->poltyp == AMG_POL_MUTUAL && P->pcg_prec != 0;
+    ctx->usolvcut = std::min(P->usolvcut, P->cutoff);
     for (int a = 0; a < 3; a++) ctx->K[a] = P->nfft[a];
     CK(cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&ctx->st2, cudaStreamNonBlocking));
+    for (int k = 0; k < 2; k++) {
+        CK(cudaStreamCreateWithFlags(&ctx->side[k], cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&ctx->efork[k], cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&ctx->ejoin[k], cudaEventDisableTiming));
+    }
     if (const char* g = getenv("AMG_NO_GRAPH")) ctx->use_graphs = !(g[0] == '1');
     ctx->lpa = n < 50000 ? 16 : 8;
     if (const char* l = getenv("AMG_LPA")) ctx->lpa = atoi(l);
@@ -1229,6 +1421,10 @@ int validate(const amg_params* P, std::string& why) {
     if (P->poltyp != AMG_POL_NONE && P->poltyp != AMG_POL_MUTUAL && P->poltyp != AMG_POL_DIRECT) {
         why = "unknown polarization model";
         return AMG_ERR_UNSUPPORTED;
+    }
+    if (P->pcg_prec && !(P->usolvcut > 0)) {
+        why = "the sparse preconditioner needs usolvcut > 0";
+        return AMG_ERR_BAD_ARG;
     }
     for (int i = 0; i < P->n; i++) {
         int ft = P->polaxe[i];

@@ -33,6 +33,15 @@ __device__ __forceinline__ T warp_sum(T v) {
     return v;
 }
 
+// sum over an aligned group of G consecutive lanes (G = 2..32), the result in
+// every lane of the group; all 32 lanes of the warp must take part
+template <int G, class T>
+__device__ __forceinline__ T group_sum(T v) {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
 // block-wide sum of one double per thread; lane 0 of warp 0 adds the result
 // to *out (one atomic per block).  blockDim.x must be a multiple of 32.
 __device__ __forceinline__ void block_sum_add(double v, double* out) {

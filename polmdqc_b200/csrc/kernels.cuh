@@ -4,8 +4,8 @@
 //   AtomR<R> : 4 x R4  = (x,y,z,q) (dx,dy,dz,Qxx) (Qxy,Qxz,Qyy,Qyz)
 //              (Qzz, pdamp, thole, polarity)   -- 64 B per atom in FP32
 //   induced dipoles (and PCG vectors) as double[3n]; R4 copies for the
-//   pair kernels; neighbour list neighbour-major (nbr[slot*n + i]) so that a
-//   warp of consecutive atoms reads one slot coalesced.
+//   pair kernels; neighbour rows site-major (nbr[i*cap + slot]), read by a
+//   lane group per site.
 #pragma once
 #include "device_util.cuh"
 #include "pair_math.cuh"

@@ -84,28 +84,42 @@ __global__ void k_pcg_control(double* __restrict__ scal, int* __restrict__ iter,
     if (use_handle) cudaGraphSetConditional(h, cont ? 1u : 0u);
 }
 
-// r = E - A u, z = alpha r, p = z;  rz, rr
+// r = E - A u and rr.  Diagonal preconditioner (s4 null): z = alpha r,
+// p = z and rz.  Sparse preconditioner: s = alpha r packed into s4 for
+// k_precond, which forms z, p and rz.
+template <class R>
 __global__ void k_pcg_init(int n, const double* __restrict__ Ed, const double* __restrict__ Ep,
                            const double* __restrict__ Aud, const double* __restrict__ Aup,
                            const double* __restrict__ pol, double* __restrict__ rd, double* __restrict__ rp,
                            double* __restrict__ zd, double* __restrict__ zp, double* __restrict__ pd,
-                           double* __restrict__ pp, double* __restrict__ scal) {
+                           double* __restrict__ pp, double* __restrict__ scal, R4<R>* __restrict__ s4) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double rzd = 0, rzp = 0, rrd = 0, rrp = 0;
     if (i < n) {
         double a = pol[i];
+        double sv[6];
         for (int c = 0; c < 3; c++) {
             int q = 3 * i + c;
             double r1 = a > 0 ? Ed[q] - Aud[q] : 0.0, r2 = a > 0 ? Ep[q] - Aup[q] : 0.0;
             rd[q] = r1; rp[q] = r2;
             double z1 = a * r1, z2 = a * r2;
-            zd[q] = z1; zp[q] = z2;
-            pd[q] = z1; pp[q] = z2;
-            rzd += r1 * z1; rzp += r2 * z2; rrd += r1 * r1; rrp += r2 * r2;
+            sv[c] = z1; sv[3 + c] = z2;
+            if (!s4) {
+                zd[q] = z1; zp[q] = z2;
+                pd[q] = z1; pp[q] = z2;
+                rzd += r1 * z1; rzp += r2 * z2;
+            }
+            rrd += r1 * r1; rrp += r2 * r2;
+        }
+        if (s4) {
+            s4[2 * i] = make_r4<R>((R)sv[0], (R)sv[1], (R)sv[2], R(0));
+            s4[2 * i + 1] = make_r4<R>((R)sv[3], (R)sv[4], (R)sv[5], R(0));
         }
     }
-    block_sum_add(rzd, scal + RZ_D);
-    block_sum_add(rzp, scal + RZ_P);
+    if (!s4) {
+        block_sum_add(rzd, scal + RZ_D);
+        block_sum_add(rzp, scal + RZ_P);
+    }
     block_sum_add(rrd, scal + RR_D);
     block_sum_add(rrp, scal + RR_P);
 }
@@ -120,18 +134,22 @@ __global__ void k_dot2(int n3, const double* __restrict__ a1, const double* __re
     block_sum_add(s2, o2);
 }
 
-// u += a p; r -= a Ap; z = alpha r; rz_new, rr  (a = rz / pAp per set)
+// u += a p; r -= a Ap; rr  (a = rz / pAp per set).  Diagonal
+// preconditioner (s4 null): z = alpha r and rz_new; sparse preconditioner:
+// s = alpha r packed into s4 for k_precond.
+template <class R>
 __global__ void k_pcg_update(int n, const double* __restrict__ pol, const double* __restrict__ pd,
                              const double* __restrict__ pp, const double* __restrict__ Apd,
                              const double* __restrict__ App, double* __restrict__ ud, double* __restrict__ up,
                              double* __restrict__ rd, double* __restrict__ rp, double* __restrict__ zd,
-                             double* __restrict__ zp, double* __restrict__ scal) {
+                             double* __restrict__ zp, double* __restrict__ scal, R4<R>* __restrict__ s4) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double ad = scal[PAP_D] != 0 ? scal[RZ_D] / scal[PAP_D] : 0.0;
     double ap = scal[PAP_P] != 0 ? scal[RZ_P] / scal[PAP_P] : 0.0;
     double rzd = 0, rzp = 0, rrd = 0, rrp = 0;
     if (i < n) {
         double a = pol[i];
+        double sv[6];
         for (int c = 0; c < 3; c++) {
             int q = 3 * i + c;
             ud[q] += ad * pd[q];
@@ -139,12 +157,22 @@ __global__ void k_pcg_update(int n, const double* __restrict__ pol, const double
             double r1 = rd[q] - ad * Apd[q], r2 = rp[q] - ap * App[q];
             rd[q] = r1; rp[q] = r2;
             double z1 = a * r1, z2 = a * r2;
-            zd[q] = z1; zp[q] = z2;
-            rzd += r1 * z1; rzp += r2 * z2; rrd += r1 * r1; rrp += r2 * r2;
+            sv[c] = z1; sv[3 + c] = z2;
+            if (!s4) {
+                zd[q] = z1; zp[q] = z2;
+                rzd += r1 * z1; rzp += r2 * z2;
+            }
+            rrd += r1 * r1; rrp += r2 * r2;
+        }
+        if (s4) {
+            s4[2 * i] = make_r4<R>((R)sv[0], (R)sv[1], (R)sv[2], R(0));
+            s4[2 * i + 1] = make_r4<R>((R)sv[3], (R)sv[4], (R)sv[5], R(0));
         }
     }
-    block_sum_add(rzd, scal + RZN_D);
-    block_sum_add(rzp, scal + RZN_P);
+    if (!s4) {
+        block_sum_add(rzd, scal + RZN_D);
+        block_sum_add(rzp, scal + RZN_P);
+    }
     block_sum_add(rrd, scal + RR_D);
     block_sum_add(rrp, scal + RR_P);
 }

@@ -9,14 +9,8 @@ namespace amg {
 // All bulk pair kernels below give each site a group of LPA consecutive
 // lanes (LPA = 4, 8, 16 or 32); the lanes stride through the site's
 // neighbour slots nbr[i * cap + s] and the partial sums are combined with
-// warp shuffles.  Sites past n run with an empty list so every lane takes
-// part in the shuffles.
-template <int LPA, class T>
-__device__ __forceinline__ T group_sum(T v) {
-#pragma unroll
-    for (int o = LPA / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
+// warp shuffles (group_sum).  Sites past n run with an empty list so every
+// lane takes part in the shuffles.
 
 // Permanent field at every site from all neighbours' multipoles, bulk
 // (scale 1, Thole damped, Ewald or bare).  Writes Ed = Ep (the d/p
@@ -216,39 +210,67 @@ __global__ void __launch_bounds__(128) k_polar_pair(int n, const AtomR<R>* __res
 template <class R, bool EWALD, int LPA>
 __global__ void __launch_bounds__(128) k_tu_coeffs(int n, const AtomR<R>* __restrict__ at, Box bx, R aewald,
                                                    const int* __restrict__ nbr, int cap, const int* __restrict__ nnb,
-                                                   R4<R>* __restrict__ c0, R* __restrict__ c1) {
+                                                   R4<R>* __restrict__ c0, R* __restrict__ c1, R usolv2,
+                                                   int* __restrict__ nbru, R4<R>* __restrict__ cu0,
+                                                   R* __restrict__ cu1, int* __restrict__ nnbu) {
     const int g = (blockIdx.x * blockDim.x + threadIdx.x) / LPA, lane = threadIdx.x % LPA;
-    if (g >= n) return;
+    if (g >= n) return;  // whole lane groups leave together
     const int i = g;
     const int cnt = nnb[i];
     R4<R> pi = at[i].a, ei = at[i].e;
     V3<R> xi = v3<R>(pi.x, pi.y, pi.z);
     const size_t base = (size_t)i * cap;
-    for (int s = lane; s < cnt; s += LPA) {
-        int j = nbr[base + s];
-        R4<R> pj = at[j].a, ej = at[j].e;
-        V3<R> r = min_image<R>(xi - v3<R>(pj.x, pj.y, pj.z), bx);
-        R r2 = dot(r, r);
-        R rinv = rsqrt_<R>(r2);
-        R rr = r2 * rinv, rinv2 = rinv * rinv;
-        R b1 = rinv * rinv2, b2 = 3 * b1 * rinv2;
-        R B1 = b1, B2 = b2;
-        if (EWALD) {
-            R eb[3];
-            ewald_terms<R, 3>(rr, rinv2, aewald, eb);
-            B1 = eb[1]; B2 = eb[2];
+    // lanes of this group within the warp, and the lanes below this one
+    const unsigned gmask = LPA == 32 ? 0xffffffffu : ((1u << LPA) - 1u) << ((threadIdx.x & 31) / LPA * LPA);
+    const unsigned below = (1u << (threadIdx.x & 31)) - 1u;
+    int nu = 0;  // preconditioner entries of this row so far
+    for (int s0 = 0; s0 < cnt; s0 += LPA) {
+        const int s = s0 + lane;
+        const bool ok = s < cnt;
+        R r2 = 0, P1 = 0, P2 = 0;
+        V3<R> r = v3<R>(0, 0, 0);
+        int j = 0;
+        if (ok) {
+            j = nbr[base + s];
+            R4<R> pj = at[j].a, ej = at[j].e;
+            r = min_image<R>(xi - v3<R>(pj.x, pj.y, pj.z), bx);
+            r2 = dot(r, r);
+            R rinv = rsqrt_<R>(r2);
+            R rr = r2 * rinv, rinv2 = rinv * rinv;
+            R b1 = rinv * rinv2, b2 = 3 * b1 * rinv2;
+            R B1 = b1, B2 = b2;
+            if (EWALD) {
+                R eb[3];
+                ewald_terms<R, 3>(rr, rinv2, aewald, eb);
+                B1 = eb[1]; B2 = eb[2];
+            }
+            P1 = b1; P2 = b2;
+            R damp = ei.y * ej.y;
+            if (damp != R(0)) {
+                R t = rr / damp;
+                R x = pair_thole<R>(ei.z, ej.z) * t * t * t;
+                R e = exp_<R>(-x);
+                B1 -= e * b1;
+                B2 -= (R(1) + x) * e * b2;
+                P1 -= e * b1;
+                P2 -= (R(1) + x) * e * b2;
+            }
+            c0[base + s] = make_r4<R>(r.x, r.y, r.z, B1);
+            c1[base + s] = B2;
         }
-        R damp = ei.y * ej.y;
-        if (damp != R(0)) {
-            R t = rr / damp;
-            R x = pair_thole<R>(ei.z, ej.z) * t * t * t;
-            R e = exp_<R>(-x);
-            B1 -= e * b1;
-            B2 -= (R(1) + x) * e * b2;
+        if (cu0) {  // sparse preconditioner: bare Thole-damped T within usolvcut, compacted in order
+            const bool take = ok && r2 <= usolv2;
+            const unsigned b = __ballot_sync(gmask, take) & gmask;
+            if (take) {
+                const size_t q = base + nu + __popc(b & below);
+                nbru[q] = j;
+                cu0[q] = make_r4<R>(r.x, r.y, r.z, P1);
+                cu1[q] = P2;
+            }
+            nu += __popc(b);
         }
-        c0[base + s] = make_r4<R>(r.x, r.y, r.z, B1);
-        c1[base + s] = B2;
     }
+    if (cu0 && lane == 0) nnbu[i] = nu;
 }
 
 // T v with the stored coefficients (both dipole sets): rows of nnb[i] bulk
@@ -264,15 +286,36 @@ __global__ void __launch_bounds__(128) k_tu_stored(int n, const int* __restrict_
     const int cnt = g < n ? nnb[i] + (xoff[i + 1] - xoff[i]) : 0;
     const size_t base = (size_t)i * cap;
     R ax = 0, ay = 0, az = 0, bx_ = 0, by = 0, bz = 0;
-    for (int s = lane; s < cnt; s += LPA) {
-        int j = nbr[base + s];
-        R4<R> c = c0[base + s];
-        R B2 = c1[base + s];
-        R4<R> ud = u4[2 * j], up = u4[2 * j + 1];
-        R ad = (ud.x * c.x + ud.y * c.y + ud.z * c.z) * B2;
-        R ap = (up.x * c.x + up.y * c.y + up.z * c.z) * B2;
-        ax += ad * c.x - c.w * ud.x; ay += ad * c.y - c.w * ud.y; az += ad * c.z - c.w * ud.z;
-        bx_ += ap * c.x - c.w * up.x; by += ap * c.y - c.w * up.y; bz += ap * c.z - c.w * up.z;
+    // U slots per lane in flight: all loads of a batch are issued before any
+    // is consumed (the kernel is bound by memory latency, not bandwidth)
+    constexpr int U = 4;
+    for (int s0 = lane; s0 < cnt; s0 += U * LPA) {
+        int j[U];
+        R4<R> c[U];
+        R B2[U];
+#pragma unroll
+        for (int q = 0; q < U; q++) {
+            const int s = s0 + q * LPA;
+            const bool ok = s < cnt;
+            j[q] = ok ? nbr[base + s] : i;
+            c[q] = ok ? c0[base + s] : make_r4<R>(0, 0, 0, 0);
+            B2[q] = ok ? c1[base + s] : R(0);
+        }
+        R4<R> ud[U], up[U];
+#pragma unroll
+        for (int q = 0; q < U; q++) {
+            ud[q] = u4[2 * j[q]];
+            up[q] = u4[2 * j[q] + 1];
+        }
+#pragma unroll
+        for (int q = 0; q < U; q++) {
+            R ad = (ud[q].x * c[q].x + ud[q].y * c[q].y + ud[q].z * c[q].z) * B2[q];
+            R ap = (up[q].x * c[q].x + up[q].y * c[q].y + up[q].z * c[q].z) * B2[q];
+            ax += ad * c[q].x - c[q].w * ud[q].x; ay += ad * c[q].y - c[q].w * ud[q].y;
+            az += ad * c[q].z - c[q].w * ud[q].z;
+            bx_ += ap * c[q].x - c[q].w * up[q].x; by += ap * c[q].y - c[q].w * up[q].y;
+            bz += ap * c[q].z - c[q].w * up[q].z;
+        }
     }
     double sx = group_sum<LPA>((double)ax), sy = group_sum<LPA>((double)ay), sz = group_sum<LPA>((double)az);
     double tx = group_sum<LPA>((double)bx_), ty = group_sum<LPA>((double)by), tz = group_sum<LPA>((double)bz);
@@ -392,7 +435,9 @@ template <class R>
 __global__ void k_scaled_coeffs(int np, const ScaledPair* __restrict__ sp, const double* __restrict__ xyz,
                                 const double* __restrict__ pdamp, const double* __restrict__ thole, Box bx,
                                 double cut2, double aewald, const int* __restrict__ nnb, int cap,
-                                int* __restrict__ nbr, R4<R>* __restrict__ c0, R* __restrict__ c1) {
+                                int* __restrict__ nbr, R4<R>* __restrict__ c0, R* __restrict__ c1, double usolv2,
+                                const int* __restrict__ nnbu, int* __restrict__ nbru, R4<R>* __restrict__ cu0,
+                                R* __restrict__ cu1) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= np) return;
     ScaledPair P = sp[t];
@@ -408,6 +453,109 @@ __global__ void k_scaled_coeffs(int np, const ScaledPair* __restrict__ sp, const
     c0[sk] = make_r4<R>((R)r.x, (R)r.y, (R)r.z, (R)B[1]);
     c1[si] = (R)B[2];
     c1[sk] = (R)B[2];
+    if (cu0) {  // preconditioner slots after the row's compacted bulk entries; zero beyond usolvcut
+        double U[6] = {0, 0, 0, 0, 0, 0};
+        const bool in = G.inside && dot(G.r, G.r) <= usolv2;
+        if (in) scaled_radial(G, P.u, true, false, U);
+        size_t ui = (size_t)P.i * cap + nnbu[P.i] + P.si;
+        size_t uk = (size_t)P.k * cap + nnbu[P.k] + P.sk;
+        nbru[ui] = P.k;
+        nbru[uk] = P.i;
+        cu0[ui] = make_r4<R>((R)(-r.x), (R)(-r.y), (R)(-r.z), (R)U[1]);
+        cu0[uk] = make_r4<R>((R)r.x, (R)r.y, (R)r.z, (R)U[1]);
+        cu1[ui] = (R)U[2];
+        cu1[uk] = (R)U[2];
+    }
+}
+
+// Sparse preconditioner z = M r for both residuals:
+//   z_i = alpha_i (w r_i + sum_j T_ij s_j),  s = alpha r  (packed in s4),
+// T over the rows built by k_tu_coeffs / k_scaled_coeffs (bulk pairs within
+// usolvcut, then the scaled partners).  Adds r.z of both sets to
+// rz_out[0], rz_out[1]; FIRST also starts the directions p = z.  Blocks
+// stride over the sites (a grid of a few blocks per SM), so each block adds
+// its r.z once.
+template <class R, int LPA, bool FIRST>
+__global__ void __launch_bounds__(128) k_precond(int n, const int* __restrict__ nbru, const R4<R>* __restrict__ cu0,
+                                                 const R* __restrict__ cu1, int cap, const int* __restrict__ nnbu,
+                                                 const int* __restrict__ xoff, const R4<R>* __restrict__ s4,
+                                                 const double* __restrict__ pol, double wdiag,
+                                                 const double* __restrict__ rd, const double* __restrict__ rp,
+                                                 double* __restrict__ zd, double* __restrict__ zp,
+                                                 double* __restrict__ pd, double* __restrict__ pp,
+                                                 R4<R>* __restrict__ p4, double* __restrict__ rz_out) {
+    const int lane = threadIdx.x % LPA, per_block = blockDim.x / LPA;
+    double rzd = 0, rzp = 0;
+    for (int g0 = blockIdx.x * per_block; g0 < n; g0 += gridDim.x * per_block) {
+        const int g = g0 + threadIdx.x / LPA;
+        const int i = min(g, n - 1);
+        const int cnt = g < n ? nnbu[i] + (xoff[i + 1] - xoff[i]) : 0;
+        const size_t base = (size_t)i * cap;
+        R ax = 0, ay = 0, az = 0, bx_ = 0, by = 0, bz = 0;
+        constexpr int U = 4;
+        for (int s0 = lane; s0 < cnt; s0 += U * LPA) {
+            int j[U];
+            R4<R> c[U];
+            R B2[U];
+#pragma unroll
+            for (int q = 0; q < U; q++) {
+                const int s = s0 + q * LPA;
+                const bool ok = s < cnt;
+                j[q] = ok ? nbru[base + s] : i;
+                c[q] = ok ? cu0[base + s] : make_r4<R>(0, 0, 0, 0);
+                B2[q] = ok ? cu1[base + s] : R(0);
+            }
+            R4<R> vd[U], vp[U];
+#pragma unroll
+            for (int q = 0; q < U; q++) {
+                vd[q] = s4[2 * j[q]];
+                vp[q] = s4[2 * j[q] + 1];
+            }
+#pragma unroll
+            for (int q = 0; q < U; q++) {
+                R ad = (vd[q].x * c[q].x + vd[q].y * c[q].y + vd[q].z * c[q].z) * B2[q];
+                R ap = (vp[q].x * c[q].x + vp[q].y * c[q].y + vp[q].z * c[q].z) * B2[q];
+                ax += ad * c[q].x - c[q].w * vd[q].x; ay += ad * c[q].y - c[q].w * vd[q].y;
+                az += ad * c[q].z - c[q].w * vd[q].z;
+                bx_ += ap * c[q].x - c[q].w * vp[q].x; by += ap * c[q].y - c[q].w * vp[q].y;
+                bz += ap * c[q].z - c[q].w * vp[q].z;
+            }
+        }
+        double S[6];
+        S[0] = group_sum<LPA>((double)ax); S[1] = group_sum<LPA>((double)ay); S[2] = group_sum<LPA>((double)az);
+        S[3] = group_sum<LPA>((double)bx_); S[4] = group_sum<LPA>((double)by); S[5] = group_sum<LPA>((double)bz);
+        // the group's lanes finish the six components (k = lane, lane + LPA, ...)
+        if (g < n) {
+            const double a = pol[i];
+            for (int k = lane; k < 6; k += LPA) {
+                const int c = k % 3;
+                const bool dset = k < 3;
+                const double Sv = k == 0 ? S[0] : k == 1 ? S[1] : k == 2 ? S[2] : k == 3 ? S[3] : k == 4 ? S[4] : S[5];
+                const int q = 3 * i + c;
+                const double rv = dset ? rd[q] : rp[q];
+                const double z = a > 0 ? a * (wdiag * rv + Sv) : 0.0;
+                (dset ? zd : zp)[q] = z;
+                if (dset) rzd += rv * z; else rzp += rv * z;
+                if (FIRST) (dset ? pd : pp)[q] = z;
+            }
+        }
+        if (FIRST) {
+            // the R4 copy of p = z for the first matvec (lane 0 of the group)
+            if (g < n && lane == 0) {
+                const double a = pol[i];
+                double z[6];
+#pragma unroll
+                for (int k = 0; k < 6; k++) {
+                    const double rv = k < 3 ? rd[3 * i + k] : rp[3 * i + k - 3];
+                    z[k] = a > 0 ? a * (wdiag * rv + S[k]) : 0.0;
+                }
+                p4[2 * i] = make_r4<R>((R)z[0], (R)z[1], (R)z[2], R(0));
+                p4[2 * i + 1] = make_r4<R>((R)z[3], (R)z[4], (R)z[5], R(0));
+            }
+        }
+    }
+    block_sum_add(rzd, rz_out);
+    block_sum_add(rzp, rz_out + 1);
 }
 
 // scaled pairs' contribution to em, its gradient and the torques (both

@@ -223,6 +223,164 @@ __global__ void k_neighbors(int n, const double4* __restrict__ spos, const unsig
     }
 }
 
+// The same exact neighbour list, one block per home cell, for boxes with at
+// least 3 cells on every periodic axis.  The atoms of the (up to) 27 stencil
+// cells are staged in shared memory as FP32 positions relative to the home
+// cell's corner (periodic coordinates first wrapped into the box, as the
+// cell index does), each moved by its stencil cell's periodic image, so
+// the inner loop is three FP32 differences and a dot product.  A pair whose
+// FP32 squared distance lies within `margin` of cut^2 is decided again by the
+// FP64 minimum-image test of k_neighbors, so both kernels give the same pair
+// set; candidates are taken in the same order (stencil cells in x, y, z
+// order, each in sorted order), so the rows are identical too.  Staging is
+// chunked (kNbrChunk candidates, kNbrHome home atoms at a time), so any cell
+// occupancy works.
+constexpr int kNbrChunk = 1536;
+constexpr int kNbrHome = 128;
+constexpr int kNbrThreads = 256;
+
+__global__ void __launch_bounds__(kNbrThreads) k_neighbors_cells(
+    const double4* __restrict__ spos, const int* __restrict__ sids, const int* __restrict__ cstart,
+    const int* __restrict__ cend, CellGrid cg, Box bx, double cut2, double margin, int cap,
+    const int* __restrict__ xoff, const int* __restrict__ xidx, int* __restrict__ nbr, int* __restrict__ nnb,
+    int* __restrict__ overflow) {
+    __shared__ float4 cpos[kNbrChunk];
+    __shared__ int csrt[kNbrChunk];  // sorted index
+    __shared__ int cid[kNbrChunk];   // site index
+    __shared__ int hcnt[kNbrHome];
+    __shared__ int rstart[27], rpre[28];
+    __shared__ double rshift[27][3];
+    __shared__ int nst;
+    const int cell = blockIdx.x;
+    const int hs = cstart[cell], he = cend[cell];
+    if (he <= hs) return;  // empty cell: the whole block leaves
+    const int c2 = cell % cg.nc[2], c1 = (cell / cg.nc[2]) % cg.nc[1], c0 = cell / (cg.nc[2] * cg.nc[1]);
+    const int cc[3] = {c0, c1, c2};
+    double corner[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) corner[a] = cg.origin[a] + cc[a] * cg.size[a];
+    if (threadIdx.x == 0) {
+        int k = 0, pre = 0;
+        for (int dx = cg.off_lo[0]; dx <= cg.off_hi[0]; dx++)
+            for (int dy = cg.off_lo[1]; dy <= cg.off_hi[1]; dy++)
+                for (int dz = cg.off_lo[2]; dz <= cg.off_hi[2]; dz++) {
+                    const int d[3] = {dx, dy, dz};
+                    int q[3];
+                    double sh[3];
+                    bool skip = false;
+                    for (int a = 0; a < 3; a++) {
+                        q[a] = cc[a] + d[a];
+                        sh[a] = 0.0;
+                        if (cg.periodic) {
+                            if (q[a] < 0) { q[a] += cg.nc[a]; sh[a] = -bx.L[a]; }
+                            else if (q[a] >= cg.nc[a]) { q[a] -= cg.nc[a]; sh[a] = bx.L[a]; }
+                        } else if (q[a] < 0 || q[a] >= cg.nc[a]) {
+                            skip = true;
+                        }
+                    }
+                    if (skip) continue;
+                    const int qc = (q[0] * cg.nc[1] + q[1]) * cg.nc[2] + q[2];
+                    const int len = cend[qc] - cstart[qc];
+                    rstart[k] = cstart[qc];
+                    rpre[k] = pre;
+                    for (int a = 0; a < 3; a++) rshift[k][a] = sh[a];
+                    pre += len > 0 ? len : 0;
+                    k++;
+                }
+        rpre[k] = pre;
+        nst = k;
+    }
+    __syncthreads();
+    const int M = rpre[nst];
+    // position in the box (periodic) relative to the home cell's corner
+    auto rel = [&](double x, int a) {
+        if (cg.periodic) x -= bx.L[a] * floor(x * bx.iL[a]);
+        return x - corner[a];
+    };
+    const float lo2 = (float)(cut2 - margin), hi2 = (float)(cut2 + margin);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+    const unsigned below = (1u << lane) - 1u;
+    for (int h0 = hs; h0 < he; h0 += kNbrHome) {
+        const int hn = min(kNbrHome, he - h0);
+        for (int t = threadIdx.x; t < hn; t += blockDim.x) hcnt[t] = 0;
+        for (int m0 = 0; m0 < M; m0 += kNbrChunk) {
+            const int mn = min(kNbrChunk, M - m0);
+            __syncthreads();  // the previous chunk is consumed and hcnt is initialised
+            // stage the chunk one stencil cell at a time (cells overlapping it)
+            for (int k = 0; k < nst; k++) {
+                const int f0 = max(rpre[k], m0), f1 = min(rpre[k + 1], m0 + mn);
+                for (int f = f0 + threadIdx.x; f < f1; f += blockDim.x) {
+                    const int p = rstart[k] + (f - rpre[k]);
+                    const double4 x = spos[p];
+                    const int t = f - m0;
+                    cpos[t] = make_float4((float)(rel(x.x, 0) + rshift[k][0]), (float)(rel(x.y, 1) + rshift[k][1]),
+                                          (float)(rel(x.z, 2) + rshift[k][2]), 0.f);
+                    csrt[t] = p;
+                    cid[t] = sids[p];
+                }
+            }
+            __syncthreads();
+            for (int hh = warp; hh < hn; hh += nwarp) {
+                const int ph = h0 + hh;
+                const int i = sids[ph];
+                const double4 xi = spos[ph];
+                const float hx = (float)rel(xi.x, 0), hy = (float)rel(xi.y, 1), hz = (float)rel(xi.z, 2);
+                const int x0 = xoff[i], x1 = xoff[i + 1];
+                const int limit = cap - (x1 - x0);  // the row's tail holds the scaled partners
+                // the first kExcl scaled partners in registers, the rest read when needed
+                constexpr int kExcl = 8;
+                int ex[kExcl];
+#pragma unroll
+                for (int q = 0; q < kExcl; q++) ex[q] = x0 + q < x1 ? xidx[x0 + q] : -1;
+                int* row = nbr + (size_t)i * cap;
+                int cnt = hcnt[hh];
+                for (int b = 0; b < mn; b += 32) {
+                    const int t = b + lane;
+                    bool hit = false;
+                    int j = -1;
+                    if (t < mn) {
+                        const float4 c = cpos[t];
+                        const float dx = c.x - hx, dy = c.y - hy, dz = c.z - hz;
+                        const float r2 = dx * dx + dy * dy + dz * dz;
+                        if (r2 <= hi2) {
+                            j = cid[t];
+                            hit = j != i;
+                            if (hit && r2 > lo2) {  // near the cutoff: the FP64 test
+                                const double4 pj = spos[csrt[t]];
+                                const double rx = wrap1<double>(pj.x - xi.x, bx.L[0], bx.iL[0]);
+                                const double ry = wrap1<double>(pj.y - xi.y, bx.L[1], bx.iL[1]);
+                                const double rz = wrap1<double>(pj.z - xi.z, bx.L[2], bx.iL[2]);
+                                hit = rx * rx + ry * ry + rz * rz <= cut2;
+                            }
+                            if (hit) {
+#pragma unroll
+                                for (int q = 0; q < kExcl; q++) hit &= (ex[q] != j);
+                                for (int q = x0 + kExcl; q < x1; q++) hit &= (xidx[q] != j);
+                            }
+                        }
+                    }
+                    const unsigned m = __ballot_sync(0xffffffffu, hit);
+                    if (hit) {
+                        const int pos = cnt + __popc(m & below);
+                        if (pos < limit) row[pos] = j;
+                    }
+                    cnt += __popc(m);
+                }
+                if (lane == 0) hcnt[hh] = cnt;
+            }
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < hn; t += blockDim.x) {
+            const int i = sids[h0 + t];
+            const int nx = xoff[i + 1] - xoff[i];
+            const int limit = cap - nx, cnt = hcnt[t];
+            nnb[i] = min(cnt, limit);
+            if (cnt > limit) atomicMax(overflow, cnt + nx);
+        }
+        __syncthreads();
+    }
+}
+
 // ---------------------------------------------------------------- B-splines
 // Cardinal B-spline weights of order P at the P grid points starting at
 // floor(u) - P + 1, and their first three derivatives (Essmann et al. 1995):

@@ -30,6 +30,8 @@ class Settings:
     politer: int = 100
     precision: int = abi.PREC_MIXED
     pcg_guess: bool = True
+    pcg_prec: bool = True             # sparse preconditioner within usolvcut (reference default)
+    usolvcut: float = 4.5             # Angstrom
     electric: float = COULOMB
     dielec: float = 1.0
     device: int = 0
@@ -80,6 +82,8 @@ class Params:
         p.precision = st.precision
         p.pcg_guess = int(st.pcg_guess)
         p.device = st.device
+        p.pcg_prec = int(st.pcg_prec)
+        p.usolvcut = st.usolvcut
         self.struct = p
         self.n = s.n
 

@@ -168,6 +168,8 @@ void ensure_context(bool want_polar)
     p.precision = (prec && prec[0] == 'f') ? AMG_PREC_FP64 : AMG_PREC_MIXED;
     p.pcg_guess = pcgguess;
     p.device = 0;
+    p.pcg_prec = pcgprec;
+    p.usolvcut = usolvcut;
     int rc = amg_create(&p, &dev.ctx);
     if (rc != AMG_OK) {
         printf("\n AMOEBA GPU  --  amg_create failed (status %d)\n", rc);

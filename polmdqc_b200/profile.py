@@ -19,6 +19,7 @@ def main():
     ap.add_argument("--waters", type=int, default=4096, choices=sorted(BOXES))
     ap.add_argument("--evals", type=int, default=3)
     ap.add_argument("--fp64", action="store_true")
+    ap.add_argument("--bench", type=int, default=0, help="also time this many device-resident evaluations")
     a = ap.parse_args()
     box, grid = BOXES[a.waters]
     s = systems.water_box(a.waters, box, seed=0)
@@ -27,6 +28,11 @@ def main():
     for _ in range(a.evals):
         r = e.forward(abi.DO_ENERGY | abi.DO_GRADIENT)
     print(f"em {r.em:.6f} ep {r.ep:.6f} pcg {r.pcg_iters} {e.stats()}")
+    print("phase ms (total, set-up, field, solve, forces; eager path only):", " ".join(f"{t:.3f}" for t in e.timing()))
+    if a.bench:
+        ms, launches = e.bench(a.bench, flush_bytes=256 << 20)
+        print(f"device ms per evaluation: median {sorted(ms)[len(ms) // 2]:.3f} min {ms.min():.3f} "
+              f"launches {launches}")
     e.close()
 
 

@@ -18,7 +18,7 @@ def test_library_exports_header_symbols():
     assert {"amg_create", "amg_set_coords", "amg_forward", "amg_backward", "amg_destroy"} <= set(declared)
     for name in declared:
         assert hasattr(lib, name), name
-    assert lib.amg_abi_version() == 1
+    assert lib.amg_abi_version() == 2
 
 
 def test_struct_layout_matches_header():

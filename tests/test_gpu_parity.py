@@ -108,6 +108,24 @@ def test_fp64_matches_oracle(w216, w216_oracle):
     assert g.pcg_eps <= 1e-8
 
 
+@pytest.mark.parametrize("sparse", [False, True])
+def test_preconditioners_follow_the_oracle(w216, sparse):
+    """Diagonal and sparse (pcgprec, usolvcut 4.5 A) preconditioners: the
+    FP64 path takes the oracle's iteration count and lands on its dipoles."""
+    # converged to 1e-8 D: the GPU's final FP64 correction step (which the
+    # oracle does not take) then moves ep by less than 1e-8 relative
+    st = Settings(nfft=(24, 24, 24), precision=FP64, pcg_prec=sparse, poleps=1e-8)
+    o = oracle.forward(w216, st)
+    g = run(w216, st)
+    assert g.pcg_iters == o.pcg_iters
+    assert rel(g.ep, o.ep) < 1e-8
+    assert np.abs(g.uind - o.uind).max() < 1e-7
+    m = run(w216, Settings(nfft=(24, 24, 24), precision=MIXED, pcg_prec=sparse))
+    o6 = oracle.forward(w216, Settings(nfft=(24, 24, 24), precision=FP64, pcg_prec=sparse))
+    assert abs(m.pcg_iters - o6.pcg_iters) <= 1
+    assert rel(m.ep, o6.ep) < 1e-6
+
+
 def test_mixed_meets_accuracy_target(w216, w216_oracle):
     o = w216_oracle
     g = run(w216, Settings(nfft=(24, 24, 24), precision=MIXED))

@@ -132,6 +132,35 @@ def run_reference(args):
     return 0
 
 
+def ion_solution_timings(device, reps):
+    """8,000 waters + 22 Na+ + 22 Cl- (amoebabio18), 62.1 A, PME 72^3: mixed
+    and FP64 forward (device time, L2 flushed) and forward + adjoint (host
+    wall clock per pair of synchronous calls)."""
+    from polmdqc_b200 import abi, systems
+    from polmdqc_b200.engine import Engine, Settings
+    s = systems.ion_solution(seed=0)
+    flags = abi.DO_ENERGY | abi.DO_GRADIENT
+    out = {"config": "8000 waters + 22 Na+ + 22 Cl- (amoebabio18), 24,044 atoms, 62.1 A, PME 72^3 order 5, "
+                     "cutoff 7 A, mutual polarization 1e-6 D"}
+    for name, prec in (("mixed", abi.PREC_MIXED), ("fp64", abi.PREC_FP64)):
+        e = Engine(s, Settings(nfft=(72, 72, 72), precision=prec, device=device))
+        try:
+            e.bench(3, flags, FLUSH_BYTES)
+            ms, _ = e.bench(reps, flags, FLUSH_BYTES)
+            e.forward(flags)
+            e.backward(1.0)
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                e.forward(flags)
+                e.backward(1.0)
+            fb = 1000.0 * (time.perf_counter() - t0) / reps
+            out[name] = {"forward_ms": float(np.median(ms)), "forward_plus_adjoint_ms": fb}
+        finally:
+            e.close()
+    out["mixed_over_fp64_forward"] = out["fp64"]["forward_ms"] / out["mixed"]["forward_ms"]
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -217,6 +246,20 @@ def main():
            "force_rms_kcal_mol_A": float(np.sqrt(np.mean((rmx.dem + rmx.dep - r64.dem - r64.dep) ** 2))),
            "pcg_eps_D": rmx.pcg_eps, "reference": "FP64 GPU path (matches the FP64 CPU oracle to 1e-10 in em)"}
 
+    # the adjoint (amg_backward after a forward): wall time of the synchronous
+    # call, gradients copied to the host, on the bench box
+    eng.forward(flags)
+    for _ in range(2):
+        eng.backward(1.0)
+    nb = max(3, min(20, args.steps // 5))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(nb):
+        eng.backward(1.0)
+    barrier()
+    adjoint_ms = max_over_ranks(1000.0 * (time.perf_counter() - t0) / nb)
+    ions = ion_solution_timings(local, nb) if world == 1 else None
+
     if rank == 0:
         peaks, src = load_peaks()
         achieved = tu_bytes / (tu_ms * 1e-3) / 1e9
@@ -232,7 +275,12 @@ def main():
                 "pcg_iterations": int(statistics.median(iters)), "em": em, "ep": ep,
                 "ns_per_day": {"dt_1fs": value * 86400 * 1e-6, "dt_2fs": value * 86400 * 2e-6},
                 "roofline": roofline, "fp64_gpu_value": fp64_value, "mixed_over_fp64": value / fp64_value,
-                "mixed_error_vs_fp64": err}
+                "mixed_error_vs_fp64": err,
+                "adjoint_ms": {"value": adjoint_ms, "calls": nb,
+                               "what": "amg_backward after one forward (d/d coordinates, local multipoles, "
+                                       "polarizabilities, Thole factors), synchronous, host wall clock"}}
+        if ions:
+            line["ion_solution"] = ions
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_oracle(seed=0)
         print(json.dumps(line), flush=True)

@@ -53,26 +53,20 @@ template <class R>
 struct CufftTypes;
 template <>
 struct CufftTypes<float> {
-    static constexpr cufftType r2c = CUFFT_R2C, c2r = CUFFT_C2R;
+    static constexpr cufftType r2c = CUFFT_R2C, c2r = CUFFT_C2R, c2c = CUFFT_C2C;
     static cufftResult fwd(cufftHandle p, float* i, cufftComplex* o) { return cufftExecR2C(p, i, o); }
     static cufftResult inv(cufftHandle p, cufftComplex* i, float* o) { return cufftExecC2R(p, i, o); }
+    static cufftResult cc(cufftHandle p, cufftComplex* g, int dir) { return cufftExecC2C(p, g, g, dir); }
     using C = cufftComplex;
 };
 template <>
 struct CufftTypes<double> {
-    static constexpr cufftType r2c = CUFFT_D2Z, c2r = CUFFT_Z2D;
+    static constexpr cufftType r2c = CUFFT_D2Z, c2r = CUFFT_Z2D, c2c = CUFFT_Z2Z;
     static cufftResult fwd(cufftHandle p, double* i, cufftDoubleComplex* o) { return cufftExecD2Z(p, i, o); }
     static cufftResult inv(cufftHandle p, cufftDoubleComplex* i, double* o) { return cufftExecZ2D(p, i, o); }
+    static cufftResult cc(cufftHandle p, cufftDoubleComplex* g, int dir) { return cufftExecZ2Z(p, g, g, dir); }
     using C = cufftDoubleComplex;
 };
-
-// sites staged per batch by the brick spreading kernel, and its shared memory
-template <class R>
-constexpr int kBrickSites = sizeof(R) == 4 ? 256 : 128;
-template <class R>
-size_t brick_smem_bytes(size_t RE) {
-    return (2 * RE + (size_t)kBrickSites<R> * (6 * kOrder + 6)) * sizeof(R) + (size_t)kBrickSites<R> * sizeof(int);
-}
 
 template <class R>
 struct Pme {
@@ -83,17 +77,12 @@ struct Pme {
     R* infl = nullptr;                       // [K1 K2 (K3/2+1)]
     R* theta = nullptr;                      // [n][3][4][P]
     int* k0 = nullptr;                       // [n][3]
-    cufftHandle f1 = 0, i1 = 0, f2 = 0, i2 = 0;
+    cufftHandle f1 = 0, i1 = 0, zplan = 0;
+    // dipole grids: d + i p interleaved, transformed in place
+    typename Cplx<R>::type* zg = nullptr;    // [K1 K2 K3]
+    R* Gfull = nullptr;                      // [K1 K2 K3] influence function on the full grid
     double infl_box[3] = {0, 0, 0};
     size_t G = 0, Gc = 0;
-    // sites sorted by the brick of their stencil start (dipole spreading)
-    Bricks bk{};
-    int nbricks = 0;
-    R* regions = nullptr;                    // [nbricks][2][E^3]
-    unsigned *bkeys = nullptr, *bskeys = nullptr;
-    int *bids = nullptr, *bsids = nullptr, *bstart = nullptr, *bend = nullptr;
-    char* btmp = nullptr;
-    size_t btmp_bytes = 0;
 };
 
 template <class R>
@@ -347,37 +336,13 @@ void pme_prepare(amg_ctx* ctx, Pme<R>& pm) {
         int dims[3] = {K1, K2, K3};
         CKFFT(cufftPlanMany(&pm.f1, 3, dims, nullptr, 1, 0, nullptr, 1, 0, CufftTypes<R>::r2c, 1));
         CKFFT(cufftPlanMany(&pm.i1, 3, dims, nullptr, 1, 0, nullptr, 1, 0, CufftTypes<R>::c2r, 1));
-        CKFFT(cufftPlanMany(&pm.f2, 3, dims, nullptr, 1, 0, nullptr, 1, 0, CufftTypes<R>::r2c, 2));
-        CKFFT(cufftPlanMany(&pm.i2, 3, dims, nullptr, 1, 0, nullptr, 1, 0, CufftTypes<R>::c2r, 2));
-        cufftHandle hs[4] = {pm.f1, pm.i1, pm.f2, pm.i2};
-        for (int k = 0; k < 4; k++) CKFFT(cufftSetStream(hs[k], ctx->st));
-        // bricks: edge 12 or less, the last brick of an axis at least P-1 long
-        int Bv[3], nbv[3];
-        for (int a = 0; a < 3; a++) {
-            const int K = ctx->K[a];
-            int B = K <= 12 ? K : 12;
-            while (B > 6 && K % B != 0 && K % B < kOrder - 1) B--;
-            Bv[a] = B;
-            nbv[a] = (K + B - 1) / B;
-        }
-        pm.bk.B = make_int3(Bv[0], Bv[1], Bv[2]);
-        pm.bk.nb = make_int3(nbv[0], nbv[1], nbv[2]);
-        pm.bk.E = make_int3(Bv[0] + kOrder - 1, Bv[1] + kOrder - 1, Bv[2] + kOrder - 1);
-        pm.nbricks = nbv[0] * nbv[1] * nbv[2];
-        const size_t RE = (size_t)pm.bk.E.x * pm.bk.E.y * pm.bk.E.z;
-        dalloc(ctx, pm.regions, (size_t)pm.nbricks * 2 * RE);
-        dalloc(ctx, pm.bkeys, ctx->n);
-        dalloc(ctx, pm.bskeys, ctx->n);
-        dalloc(ctx, pm.bids, ctx->n);
-        dalloc(ctx, pm.bsids, ctx->n);
-        dalloc(ctx, pm.bstart, pm.nbricks);
-        dalloc(ctx, pm.bend, pm.nbricks);
-        size_t bytes = 0;
-        cub::DeviceRadixSort::SortPairs(nullptr, bytes, pm.bkeys, pm.bskeys, pm.bids, pm.bsids, ctx->n);
-        dalloc(ctx, pm.btmp, bytes);
-        pm.btmp_bytes = bytes;
-        CK(cudaFuncSetAttribute(k_spread_dipoles_brick<R, kOrder, kBrickSites<R>>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)brick_smem_bytes<R>(RE)));
+        cufftHandle hs[2] = {pm.f1, pm.i1};
+        for (int k = 0; k < 2; k++) CKFFT(cufftSetStream(hs[k], ctx->st));
+        dalloc(ctx, pm.zg, pm.G);
+        dalloc(ctx, pm.Gfull, pm.G);
+        // in-place complex transform of the dipole grid (d + i p)
+        CKFFT(cufftPlan3d(&pm.zplan, K1, K2, K3, CufftTypes<R>::c2c));
+        CKFFT(cufftSetStream(pm.zplan, ctx->st));
         pm.ready = true;
     }
     if (pm.infl_box[0] != ctx->box[0] || pm.infl_box[1] != ctx->box[1] || pm.infl_box[2] != ctx->box[2]) {
@@ -400,18 +365,28 @@ void pme_prepare(amg_ctx* ctx, Pme<R>& pm) {
                     h[id] = (R)(pref * exp(-kPi * kPi * h2 / a2) / h2 / (b1[a] * b2[b] * b3[c]));
                 }
         CK(cudaMemcpy(pm.infl, h.data(), sizeof(R) * pm.Gc, cudaMemcpyHostToDevice));
+        // the same function on the full grid (even: G(m) = G(-m))
+        std::vector<R> hf(pm.G);
+        for (int a = 0; a < K1; a++)
+            for (int b = 0; b < K2; b++)
+                for (int c = 0; c < K3; c++) {
+                    const int a2 = a == 0 ? 0 : K1 - a, b2 = b == 0 ? 0 : K2 - b;
+                    // c > K3/2: G(a,b,c) = G(-a,-b,K3-c), held in the half-complex layout
+                    hf[((size_t)a * K2 + b) * K3 + c] =
+                        c < K3h ? h[((size_t)a * K2 + b) * K3h + c] : h[((size_t)a2 * K2 + b2) * K3h + (K3 - c)];
+                }
+        CK(cudaMemcpy(pm.Gfull, hf.data(), sizeof(R) * pm.G, cudaMemcpyHostToDevice));
         for (int a = 0; a < 3; a++) pm.infl_box[a] = ctx->box[a];
     }
 }
 
 template <class R>
 void pme_destroy(Pme<R>& pm) {
-    cufftHandle* hs[4] = {&pm.f1, &pm.i1, &pm.f2, &pm.i2};
-    for (int k = 0; k < 4; k++)
+    cufftHandle* hs[3] = {&pm.f1, &pm.i1, &pm.zplan};
+    for (int k = 0; k < 3; k++)
         if (*hs[k]) { cufftDestroy(*hs[k]); *hs[k] = 0; }
+    dfree(pm.zg); dfree(pm.Gfull);
     dfree(pm.grid); dfree(pm.phig); dfree(pm.cgrid); dfree(pm.infl); dfree(pm.theta); dfree(pm.k0);
-    dfree(pm.regions); dfree(pm.bkeys); dfree(pm.bskeys); dfree(pm.bids); dfree(pm.bsids); dfree(pm.bstart);
-    dfree(pm.bend); dfree(pm.btmp);
     pm.ready = false;
 }
 
@@ -587,25 +562,12 @@ void join_side(amg_ctx* ctx, cudaStream_t s) {
     CK(cudaStreamWaitEvent(s, ctx->ejoin[k], 0));
 }
 
-// B-spline stencils of every site, and the sites sorted by brick
+// B-spline stencils of every site
 template <class R>
 void pme_stencils(amg_ctx* ctx, cudaStream_t s) {
     Pme<R>& pm = pme_of<R>(ctx);
-    const int n = ctx->n;
-    k_bspline<R, kOrder><<<nblk(n), kThreads, 0, s>>>(n, ctx->xyz, ctx->bx, make_int3(ctx->K[0], ctx->K[1], ctx->K[2]),
-                                                      pm.theta, pm.k0);
-    KCHECK();
-    k_brick_keys<<<nblk(n), kThreads, 0, s>>>(n, pm.k0, pm.bk, pm.bkeys, pm.bids);
-    KCHECK();
-    int nbits = 1;
-    while ((1ull << nbits) < (unsigned long long)pm.nbricks) nbits++;
-    size_t bytes = pm.btmp_bytes;
-    CK(cub::DeviceRadixSort::SortPairs(pm.btmp, bytes, pm.bkeys, pm.bskeys, pm.bids, pm.bsids, n, 0, nbits, s));
-    k_zero<int><<<nblk(pm.nbricks, 256), 256, 0, s>>>(pm.bstart, pm.nbricks);
-    KCHECK();
-    k_zero<int><<<nblk(pm.nbricks, 256), 256, 0, s>>>(pm.bend, pm.nbricks);
-    KCHECK();
-    k_brick_bounds<<<nblk(n), kThreads, 0, s>>>(n, pm.bskeys, pm.bstart, pm.bend);
+    k_bspline<R, kOrder><<<nblk(ctx->n), kThreads, 0, s>>>(ctx->n, ctx->xyz, ctx->bx,
+                                                           make_int3(ctx->K[0], ctx->K[1], ctx->K[2]), pm.theta, pm.k0);
     KCHECK();
 }
 
@@ -624,29 +586,27 @@ void pme_mpole(amg_ctx* ctx, cudaStream_t s) {
     k_convolve<R><<<nblk(pm.Gc, 256), 256, 0, s>>>(pm.Gc, 1, pm.infl, (typename Cplx<R>::type*)pm.cgrid, pm.grid, pm.G);
     KCHECK();
     CKFFT(CufftTypes<R>::inv(pm.i1, pm.cgrid, pm.phig));
-    k_gather<R, kOrder, 20><<<nblk(ctx->n), kThreads, 0, s>>>(ctx->n, pm.phig, pm.theta, pm.k0, K, sc[0], sc[1], sc[2],
+    k_gather<R, kOrder, 20><<<nblk(ctx->n), kThreads, 0, s>>>(ctx->n, pm.phig, 1, pm.theta, pm.k0, K, sc[0], sc[1], sc[2],
                                                               ctx->phiM);
     KCHECK();
 }
 
-// spread two dipole sets, transform, convolve, transform back into pm.phig
+// spread two dipole sets into the complex grid pm.zg (d + i p), transform,
+// convolve and transform back in place
 template <class R>
 void pme_dipole_grids(amg_ctx* ctx, cudaStream_t s, const double* vd, const double* vp) {
     Pme<R>& pm = pme_of<R>(ctx);
     int3 K = make_int3(ctx->K[0], ctx->K[1], ctx->K[2]);
     double sc[3] = {ctx->K[0] / ctx->box[0], ctx->K[1] / ctx->box[1], ctx->K[2] / ctx->box[2]};
-    const size_t RE = (size_t)pm.bk.E.x * pm.bk.E.y * pm.bk.E.z;
-    k_spread_dipoles_brick<R, kOrder, kBrickSites<R>><<<pm.nbricks, 256, brick_smem_bytes<R>(RE), s>>>(
-        pm.bk, pm.bsids, pm.bstart, pm.bend, vd, vp, pm.theta, pm.k0, (R)sc[0], (R)sc[1], (R)sc[2], pm.regions);
+    CK(cudaMemsetAsync(pm.zg, 0, sizeof(typename Cplx<R>::type) * pm.G, s));
+    k_spread_dipoles<R, kOrder><<<ctx->n, 128, 0, s>>>(ctx->n, ctx->sids, vd, vp, pm.theta, pm.k0, K, (R)sc[0],
+                                                        (R)sc[1], (R)sc[2], pm.zg);
     KCHECK();
-    k_sum_bricks<R, kOrder><<<nblk(pm.G, 256), 256, 0, s>>>(pm.bk, K, pm.regions, pm.grid, pm.G);
+    CKFFT(cufftSetStream(pm.zplan, s));
+    CKFFT(CufftTypes<R>::cc(pm.zplan, pm.zg, CUFFT_FORWARD));
+    k_scale_grid<R><<<nblk(pm.G, 256), 256, 0, s>>>(pm.G, pm.Gfull, pm.zg);
     KCHECK();
-    CKFFT(cufftSetStream(pm.f2, s));
-    CKFFT(cufftSetStream(pm.i2, s));
-    CKFFT(CufftTypes<R>::fwd(pm.f2, pm.grid, pm.cgrid));
-    k_convolve<R><<<nblk(pm.Gc, 256), 256, 0, s>>>(pm.Gc, 2, pm.infl, (typename Cplx<R>::type*)pm.cgrid, pm.grid, pm.G);
-    KCHECK();
-    CKFFT(CufftTypes<R>::inv(pm.i2, pm.cgrid, pm.phig));
+    CKFFT(CufftTypes<R>::cc(pm.zplan, pm.zg, CUFFT_INVERSE));
 }
 
 // reciprocal potentials of two dipole sets -> phi [2][n][NC]
@@ -657,7 +617,8 @@ void pme_dipoles(amg_ctx* ctx, cudaStream_t s, const double* vd, const double* v
     double sc[3] = {ctx->K[0] / ctx->box[0], ctx->K[1] / ctx->box[1], ctx->K[2] / ctx->box[2]};
     pme_dipole_grids<R>(ctx, s, vd, vp);
     for (int b = 0; b < 2; b++) {
-        k_gather<R, kOrder, NC><<<nblk(ctx->n), kThreads, 0, s>>>(ctx->n, pm.phig + b * pm.G, pm.theta, pm.k0, K, sc[0],
+        k_gather<R, kOrder, NC><<<nblk(ctx->n), kThreads, 0, s>>>(ctx->n, reinterpret_cast<const R*>(pm.zg) + b, 2,
+                                                                  pm.theta, pm.k0, K, sc[0],
                                                                   sc[1], sc[2], phi + (size_t)b * NC * ctx->n);
         KCHECK();
     }
@@ -733,10 +694,11 @@ void build_tu_coeffs(amg_ctx* ctx, cudaStream_t s) {
     }
 }
 
-// A v with the stored coefficients; v4 is the R4 copy of (vd, vp)
+// A v with the stored coefficients; v4 is the R4 copy of (vd, vp).  With
+// vAv (Ewald only) the dot products v.Av are added to vAv[0..1].
 template <class R>
 void matvec_stored(amg_ctx* ctx, cudaStream_t s, const R4<R>* v4, const double* vd, const double* vp, double* Ad,
-                   double* Ap) {
+                   double* Ap, double* vAv = nullptr) {
     const int n = ctx->n;
     Atoms<R>& A = atoms_of<R>(ctx);
     // real space on the side stream, PME on s
@@ -753,9 +715,10 @@ void matvec_stored(amg_ctx* ctx, cudaStream_t s, const R4<R>* v4, const double* 
         int3 K = make_int3(ctx->K[0], ctx->K[1], ctx->K[2]);
         double sc[3] = {ctx->K[0] / ctx->box[0], ctx->K[1] / ctx->box[1], ctx->K[2] / ctx->box[2]};
         constexpr int G = 8;  // lanes per site
-        k_gather_field<R, kOrder, G><<<nblk((size_t)n * G), kThreads, 0, s>>>(
-            n, pm.phig, pm.G, pm.theta, pm.k0, K, sc[0], sc[1], sc[2], vd, vp, ctx->Fd, ctx->Fp, self_coef(ctx), ctx->pol,
-            Ad, Ap);
+        const unsigned blocks = (unsigned)std::min<size_t>(nblk((size_t)n * G), (size_t)ctx->num_sms * 8);
+        k_gather_field<R, kOrder, G><<<blocks, kThreads, 0, s>>>(n, pm.zg, pm.theta, pm.k0, K, sc[0], sc[1], sc[2], vd,
+                                                                 vp, ctx->Fd, ctx->Fp, self_coef(ctx), ctx->pol, Ad,
+                                                                 Ap, vAv);
         KCHECK();
     } else {
         k_matvec_finish<<<nblk(n), kThreads, 0, s>>>(n, vd, vp, ctx->Fd, ctx->Fp, ctx->phiU4, 0, 0.0, ctx->pol, Ad, Ap);
@@ -830,9 +793,13 @@ template <class R>
 void enqueue_pcg_iter(amg_ctx* ctx, cudaStream_t s, cudaGraphConditionalHandle h, int use_handle) {
     const int n = ctx->n, n3 = 3 * n;
     Atoms<R>& A = atoms_of<R>(ctx);
-    matvec_stored<R>(ctx, s, A.p4, ctx->pd, ctx->pp, ctx->Apd, ctx->App);
-    k_dot2<<<nblk(n3, 256), 256, 0, s>>>(n3, ctx->pd, ctx->Apd, ctx->pp, ctx->App, ctx->scal + PAP_D, ctx->scal + PAP_P);
-    KCHECK();
+    // p.Ap: fused into the PME gather with Ewald, a separate pass without
+    matvec_stored<R>(ctx, s, A.p4, ctx->pd, ctx->pp, ctx->Apd, ctx->App, ctx->ewald ? ctx->scal + PAP_D : nullptr);
+    if (!ctx->ewald) {
+        k_dot2<<<nblk(n3, 256), 256, 0, s>>>(n3, ctx->pd, ctx->Apd, ctx->pp, ctx->App, ctx->scal + PAP_D,
+                                              ctx->scal + PAP_P);
+        KCHECK();
+    }
     k_pcg_update<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->pol, ctx->pd, ctx->pp, ctx->Apd, ctx->App, ctx->ud, ctx->up,
                                                  ctx->rd, ctx->rp, ctx->zd, ctx->zp, ctx->scal,
                                                  ctx->sparse_prec ? A.s4 : nullptr);

@@ -126,6 +126,19 @@ def test_preconditioners_follow_the_oracle(w216, sparse):
     assert rel(m.ep, o6.ep) < 1e-6
 
 
+@pytest.mark.parametrize("nfft", [(30, 25, 32), (28, 28, 28)])
+def test_pme_grid_sizes_match_oracle(w216, nfft):
+    """The packed complex dipole grid (d + i p) and its influence function
+    on non-cubic grids and odd lengths, FP64 against the oracle."""
+    st = Settings(nfft=nfft, precision=FP64, poleps=1e-8)
+    o = oracle.forward(w216, st, tol=1e-11)
+    g = run(w216, st)
+    assert rel(g.em, o.em) < 1e-10
+    assert rel(g.ep, o.ep) < 1e-8
+    assert np.abs(g.dep - o.dep).max() < 1e-5
+    assert np.abs(g.uind - o.uind).max() < 1e-7
+
+
 def test_mixed_meets_accuracy_target(w216, w216_oracle):
     o = w216_oracle
     g = run(w216, Settings(nfft=(24, 24, 24), precision=MIXED))

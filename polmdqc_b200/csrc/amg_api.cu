@@ -643,10 +643,10 @@ void matvec(amg_ctx* ctx, cudaStream_t s, const double* vd, const double* vp, do
     cudaStream_t r = ctx->ewald ? fork_side(ctx, s) : s;
     LPA_DISPATCH(ctx->lpa, {
         if (ctx->ewald)
-            k_Tu<R, true, L><<<nblk((size_t)n * L), kThreads, 0, r>>>(n, A.at, A.u4, ctx->bx, (R)ctx->aewald, ctx->nbr,
+            k_Tu<R, true, L><<<nblk((size_t)n * L), kThreads, 0, r>>>(n, ctx->sids, A.at, A.u4, ctx->bx, (R)ctx->aewald, ctx->nbr,
                                                                       ctx->cap, ctx->nnb, ctx->Fd, ctx->Fp);
         else
-            k_Tu<R, false, L><<<nblk((size_t)n * L), kThreads, 0, r>>>(n, A.at, A.u4, ctx->bx, (R)0, ctx->nbr, ctx->cap,
+            k_Tu<R, false, L><<<nblk((size_t)n * L), kThreads, 0, r>>>(n, ctx->sids, A.at, A.u4, ctx->bx, (R)0, ctx->nbr, ctx->cap,
                                                                        ctx->nnb, ctx->Fd, ctx->Fp);
     });
     KCHECK();
@@ -677,11 +677,11 @@ void build_tu_coeffs(amg_ctx* ctx, cudaStream_t s) {
     R* cu1 = sp ? A.cu1 : nullptr;
     LPA_DISPATCH(ctx->lpa, {
         if (ctx->ewald)
-            k_tu_coeffs<R, true, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(n, A.at, ctx->bx, (R)ctx->aewald, ctx->nbr,
+            k_tu_coeffs<R, true, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(n, ctx->sids, A.at, ctx->bx, (R)ctx->aewald, ctx->nbr,
                                                                              ctx->cap, ctx->nnb, A.c0, A.c1, (R)u2, nbru,
                                                                              cu0, cu1, nnbu);
         else
-            k_tu_coeffs<R, false, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(n, A.at, ctx->bx, (R)0, ctx->nbr, ctx->cap,
+            k_tu_coeffs<R, false, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(n, ctx->sids, A.at, ctx->bx, (R)0, ctx->nbr, ctx->cap,
                                                                               ctx->nnb, A.c0, A.c1, (R)u2, nbru, cu0,
                                                                               cu1, nnbu);
     });
@@ -704,7 +704,7 @@ void matvec_stored(amg_ctx* ctx, cudaStream_t s, const R4<R>* v4, const double* 
     // real space on the side stream, PME on s
     cudaStream_t r = ctx->ewald ? fork_side(ctx, s) : s;
     LPA_DISPATCH(ctx->lpa, {
-        k_tu_stored<R, L><<<nblk((size_t)n * L), kThreads, 0, r>>>(n, ctx->nbr, A.c0, A.c1, ctx->cap, ctx->nnb, ctx->xoff,
+        k_tu_stored<R, L><<<nblk((size_t)n * L), kThreads, 0, r>>>(n, ctx->sids, ctx->nbr, A.c0, A.c1, ctx->cap, ctx->nnb, ctx->xoff,
                                                                     v4, ctx->Fd, ctx->Fp);
     });
     KCHECK();
@@ -746,11 +746,11 @@ void precondition(amg_ctx* ctx, cudaStream_t s, bool first, double* rz_out) {
     constexpr int L = 4;  // lanes per site: the rows are short
     const unsigned blocks = (unsigned)std::min<size_t>(nblk((size_t)n * L), (size_t)ctx->num_sms * 8);
     if (first)
-        k_precond<R, L, true><<<blocks, kThreads, 0, s>>>(n, ctx->nbru, A.cu0, A.cu1, ctx->cap, ctx->nnbu, ctx->xoff,
+        k_precond<R, L, true><<<blocks, kThreads, 0, s>>>(n, ctx->sids, ctx->nbru, A.cu0, A.cu1, ctx->cap, ctx->nnbu, ctx->xoff,
                                                           A.s4, ctx->pol, kPrecDiag, ctx->rd, ctx->rp, ctx->zd, ctx->zp,
                                                           ctx->pd, ctx->pp, A.p4, rz_out);
     else
-        k_precond<R, L, false><<<blocks, kThreads, 0, s>>>(n, ctx->nbru, A.cu0, A.cu1, ctx->cap, ctx->nnbu, ctx->xoff,
+        k_precond<R, L, false><<<blocks, kThreads, 0, s>>>(n, ctx->sids, ctx->nbru, A.cu0, A.cu1, ctx->cap, ctx->nnbu, ctx->xoff,
                                                            A.s4, ctx->pol, kPrecDiag, ctx->rd, ctx->rp, ctx->zd,
                                                            ctx->zp, ctx->pd, ctx->pp, A.p4, rz_out);
     KCHECK();
@@ -857,10 +857,10 @@ void enqueue_front(amg_ctx* ctx, cudaStream_t s) {
     if (ctx->has_pol) {
         LPA_DISPATCH(ctx->lpa, {
             if (ctx->ewald)
-                k_perm_field<R, true, L><<<nblk((size_t)n * L), kThreads, 0, r>>>(n, A.at, ctx->bx, aew, ctx->nbr, ctx->cap,
+                k_perm_field<R, true, L><<<nblk((size_t)n * L), kThreads, 0, r>>>(n, ctx->sids, A.at, ctx->bx, aew, ctx->nbr, ctx->cap,
                                                                                   ctx->nnb, ctx->Ed, ctx->Ep);
             else
-                k_perm_field<R, false, L><<<nblk((size_t)n * L), kThreads, 0, r>>>(n, A.at, ctx->bx, aew, ctx->nbr,
+                k_perm_field<R, false, L><<<nblk((size_t)n * L), kThreads, 0, r>>>(n, ctx->sids, A.at, ctx->bx, aew, ctx->nbr,
                                                                                    ctx->cap, ctx->nnb, ctx->Ed, ctx->Ep);
         });
         KCHECK();
@@ -917,20 +917,20 @@ void enqueue_back(amg_ctx* ctx, cudaStream_t s, int flags) {
         const size_t nb = nblk((size_t)n * L);
         if (ctx->ewald) {
             if (analysis)
-                k_mpole_pair<R, true, true, L><<<nb, kThreads, 0, r>>>(n, A.at, ctx->bx, aew, ctx->nbr, ctx->cap, ctx->nnb,
+                k_mpole_pair<R, true, true, L><<<nb, kThreads, 0, r>>>(n, ctx->sids, A.at, ctx->bx, aew, ctx->nbr, ctx->cap, ctx->nnb,
                                                                        ctx->f, ctx->grad_m, ctx->trq_m, ctx->eacc,
                                                                        ctx->aem, mol, ctx->cnt);
             else
-                k_mpole_pair<R, true, false, L><<<nb, kThreads, 0, r>>>(n, A.at, ctx->bx, aew, ctx->nbr, ctx->cap,
+                k_mpole_pair<R, true, false, L><<<nb, kThreads, 0, r>>>(n, ctx->sids, A.at, ctx->bx, aew, ctx->nbr, ctx->cap,
                                                                         ctx->nnb, ctx->f, ctx->grad_m, ctx->trq_m,
                                                                         ctx->eacc, nullptr, nullptr, nullptr);
         } else {
             if (analysis)
-                k_mpole_pair<R, false, true, L><<<nb, kThreads, 0, r>>>(n, A.at, ctx->bx, aew, ctx->nbr, ctx->cap,
+                k_mpole_pair<R, false, true, L><<<nb, kThreads, 0, r>>>(n, ctx->sids, A.at, ctx->bx, aew, ctx->nbr, ctx->cap,
                                                                         ctx->nnb, ctx->f, ctx->grad_m, ctx->trq_m,
                                                                         ctx->eacc, ctx->aem, mol, ctx->cnt);
             else
-                k_mpole_pair<R, false, false, L><<<nb, kThreads, 0, r>>>(n, A.at, ctx->bx, aew, ctx->nbr, ctx->cap,
+                k_mpole_pair<R, false, false, L><<<nb, kThreads, 0, r>>>(n, ctx->sids, A.at, ctx->bx, aew, ctx->nbr, ctx->cap,
                                                                          ctx->nnb, ctx->f, ctx->grad_m, ctx->trq_m,
                                                                          ctx->eacc, nullptr, nullptr, nullptr);
         }
@@ -946,11 +946,11 @@ void enqueue_back(amg_ctx* ctx, cudaStream_t s, int flags) {
     if (polgrad) {
         LPA_DISPATCH(ctx->lpa, {
             if (ctx->ewald)
-                k_polar_pair<R, true, L><<<nblk((size_t)n * L), kThreads, 0, r>>>(n, A.at, A.u4, ctx->bx, aew, ctx->nbr,
+                k_polar_pair<R, true, L><<<nblk((size_t)n * L), kThreads, 0, r>>>(n, ctx->sids, A.at, A.u4, ctx->bx, aew, ctx->nbr,
                                                                                   ctx->cap, ctx->nnb, mutual, ctx->f,
                                                                                   ctx->grad_p, ctx->trq_p);
             else
-                k_polar_pair<R, false, L><<<nblk((size_t)n * L), kThreads, 0, r>>>(n, A.at, A.u4, ctx->bx, aew, ctx->nbr,
+                k_polar_pair<R, false, L><<<nblk((size_t)n * L), kThreads, 0, r>>>(n, ctx->sids, A.at, A.u4, ctx->bx, aew, ctx->nbr,
                                                                                    ctx->cap, ctx->nnb, mutual, ctx->f,
                                                                                    ctx->grad_p, ctx->trq_p);
         });
@@ -1509,11 +1509,11 @@ int backward_impl(amg_ctx* ctx, const amg_cotangents* cot, amg_param_grads* gr) 
     LPA_DISPATCH(ctx->lpa, {
         if (ctx->ewald)
             k_adjoint_pair<true, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(
-                n, ctx->ad.at, ctx->adj_vec, ctx->bx, ctx->aewald, ctx->nbr, ctx->cap, ctx->nnb, mutual, cf, grad, trq,
+                n, ctx->sids, ctx->ad.at, ctx->adj_vec, ctx->bx, ctx->aewald, ctx->nbr, ctx->cap, ctx->nnb, mutual, cf, grad, trq,
                 ctx->adj_pot, dpd, dth);
         else
             k_adjoint_pair<false, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(
-                n, ctx->ad.at, ctx->adj_vec, ctx->bx, 0.0, ctx->nbr, ctx->cap, ctx->nnb, mutual, cf, grad, trq,
+                n, ctx->sids, ctx->ad.at, ctx->adj_vec, ctx->bx, 0.0, ctx->nbr, ctx->cap, ctx->nnb, mutual, cf, grad, trq,
                 ctx->adj_pot, dpd, dth);
     });
     KCHECK();
@@ -1771,10 +1771,12 @@ int amg_time_tu_kernel(amg_ctx* ctx, int32_t reps, int64_t flush_bytes, double* 
             LPA_DISPATCH(ctx->lpa, {
                 if (mixed)
                     k_tu_stored<float, L><<<nblk((size_t)n * L), kThreads, 0, ctx->st>>>(
-                        n, ctx->nbr, ctx->af.c0, ctx->af.c1, ctx->cap, ctx->nnb, ctx->xoff, ctx->af.p4, ctx->Fd, ctx->Fp);
+                        n, ctx->sids, ctx->nbr, ctx->af.c0, ctx->af.c1, ctx->cap, ctx->nnb, ctx->xoff, ctx->af.p4,
+                        ctx->Fd, ctx->Fp);
                 else
                     k_tu_stored<double, L><<<nblk((size_t)n * L), kThreads, 0, ctx->st>>>(
-                        n, ctx->nbr, ctx->ad.c0, ctx->ad.c1, ctx->cap, ctx->nnb, ctx->xoff, ctx->ad.p4, ctx->Fd, ctx->Fp);
+                        n, ctx->sids, ctx->nbr, ctx->ad.c0, ctx->ad.c1, ctx->cap, ctx->nnb, ctx->xoff, ctx->ad.p4,
+                        ctx->Fd, ctx->Fp);
             });
             KCHECK();
             CK(cudaEventRecord(b, ctx->st));

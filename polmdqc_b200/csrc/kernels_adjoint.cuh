@@ -107,7 +107,7 @@ __global__ void k_adj_vectors(int n, double cf, const double* __restrict__ ud, c
 // and dG_L/d(pdamp_i), dG_L/d(thole_i).  Vectors as R4 [n][5]:
 // vbar, P1, Q1, P2, Q2.  mscale channel for M-M uses the cm factor (= c f).
 template <bool EWALD, int LPA>
-__global__ void __launch_bounds__(128) k_adjoint_pair(int n, const AtomR<double>* __restrict__ at,
+__global__ void __launch_bounds__(128) k_adjoint_pair(int n, const int* __restrict__ order, const AtomR<double>* __restrict__ at,
                                                       const double4* __restrict__ vec, Box bx, double aewald,
                                                       const int* __restrict__ nbr, int cap,
                                                       const int* __restrict__ nnb, int mutual, double cm,
@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(128) k_adjoint_pair(int n, const AtomR<double>
                                                       double* __restrict__ pot, double* __restrict__ dpd,
                                                       double* __restrict__ dth) {
     const int g = (blockIdx.x * blockDim.x + threadIdx.x) / LPA, lane = threadIdx.x % LPA;
-    const int i = min(g, n - 1);
+    const int i = order[min(g, n - 1)];
     const int cnt = g < n ? nnb[i] : 0;
     const AtomR<double> Ai = at[i];
     const Mpole<double> Mi = load_mpole(Ai);

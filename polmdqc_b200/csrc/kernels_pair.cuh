@@ -16,12 +16,12 @@ namespace amg {
 // (scale 1, Thole damped, Ewald or bare).  Writes Ed = Ep (the d/p
 // differences come only from the scaled pairs).
 template <class R, bool EWALD, int LPA>
-__global__ void __launch_bounds__(128) k_perm_field(int n, const AtomR<R>* __restrict__ at, Box bx, R aewald,
+__global__ void __launch_bounds__(128) k_perm_field(int n, const int* __restrict__ order, const AtomR<R>* __restrict__ at, Box bx, R aewald,
                                                     const int* __restrict__ nbr, int cap,
                                                     const int* __restrict__ nnb, double* __restrict__ Ed,
                                                     double* __restrict__ Ep) {
     const int g = (blockIdx.x * blockDim.x + threadIdx.x) / LPA, lane = threadIdx.x % LPA;
-    const int i = min(g, n - 1);
+    const int i = order[min(g, n - 1)];
     const int cnt = g < n ? nnb[i] : 0;
     AtomR<R> Ai = at[i];
     V3<R> xi = v3<R>(Ai.a.x, Ai.a.y, Ai.a.z);
@@ -48,12 +48,12 @@ __global__ void __launch_bounds__(128) k_perm_field(int n, const AtomR<R>* __res
 // pair tensors on the fly (used by the FP64 correction sweep).  u4: [n][2]
 // R4 (ux,uy,uz,0), d set then p set per site.  Writes Fd, Fp.
 template <class R, bool EWALD, int LPA>
-__global__ void __launch_bounds__(128) k_Tu(int n, const AtomR<R>* __restrict__ at, const R4<R>* __restrict__ u4,
+__global__ void __launch_bounds__(128) k_Tu(int n, const int* __restrict__ order, const AtomR<R>* __restrict__ at, const R4<R>* __restrict__ u4,
                                             Box bx, R aewald, const int* __restrict__ nbr, int cap,
                                             const int* __restrict__ nnb, double* __restrict__ Fd,
                                             double* __restrict__ Fp) {
     const int g = (blockIdx.x * blockDim.x + threadIdx.x) / LPA, lane = threadIdx.x % LPA;
-    const int i = min(g, n - 1);
+    const int i = order[min(g, n - 1)];
     const int cnt = g < n ? nnb[i] : 0;
     R4<R> pi = at[i].a, ei = at[i].e;
     V3<R> xi = v3<R>(pi.x, pi.y, pi.z);
@@ -104,14 +104,14 @@ __global__ void __launch_bounds__(128) k_Tu(int n, const AtomR<R>* __restrict__ 
 // i from all its neighbours (bulk, m-scale 1).  f = electric/dielec.
 // Analysis: per-site energy, nonzero pair count (directed), intermolecular.
 template <class R, bool EWALD, bool ANALYSIS, int LPA>
-__global__ void __launch_bounds__(128) k_mpole_pair(int n, const AtomR<R>* __restrict__ at, Box bx, R aewald,
+__global__ void __launch_bounds__(128) k_mpole_pair(int n, const int* __restrict__ order, const AtomR<R>* __restrict__ at, Box bx, R aewald,
                                                     const int* __restrict__ nbr, int cap,
                                                     const int* __restrict__ nnb, double f, double* __restrict__ grad,
                                                     double* __restrict__ trq, double* __restrict__ eacc,
                                                     double* __restrict__ aem, const int* __restrict__ mol,
                                                     unsigned long long* __restrict__ npair) {
     const int gi_ = (blockIdx.x * blockDim.x + threadIdx.x) / LPA, lane = threadIdx.x % LPA;
-    const int i = min(gi_, n - 1);
+    const int i = order[min(gi_, n - 1)];
     const int cnt = gi_ < n ? nnb[i] : 0;
     double e_i = 0, einter = 0;
     long long cntnz = 0;
@@ -158,13 +158,13 @@ __global__ void __launch_bounds__(128) k_mpole_pair(int n, const AtomR<R>* __res
 // with ubar = (ud + up)/2; dG/dx_i = -dG/dr, torque on M_i from ubar_k.
 // u4: [n][2] R4, d set then p set per site.
 template <class R, bool EWALD, int LPA>
-__global__ void __launch_bounds__(128) k_polar_pair(int n, const AtomR<R>* __restrict__ at,
+__global__ void __launch_bounds__(128) k_polar_pair(int n, const int* __restrict__ order, const AtomR<R>* __restrict__ at,
                                                     const R4<R>* __restrict__ u4, Box bx, R aewald,
                                                     const int* __restrict__ nbr, int cap,
                                                     const int* __restrict__ nnb, int mutual, double f,
                                                     double* __restrict__ grad, double* __restrict__ trq) {
     const int gi_ = (blockIdx.x * blockDim.x + threadIdx.x) / LPA, lane = threadIdx.x % LPA;
-    const int i = min(gi_, n - 1);
+    const int i = order[min(gi_, n - 1)];
     const int cnt = gi_ < n ? nnb[i] : 0;
     AtomR<R> Ai = at[i];
     Mpole<R> Mi = load_mpole(Ai);
@@ -208,14 +208,14 @@ __global__ void __launch_bounds__(128) k_polar_pair(int n, const AtomR<R>* __res
 // the scaled partners (filled by k_scaled_coeffs), so one kernel applies the
 // whole real-space T.
 template <class R, bool EWALD, int LPA>
-__global__ void __launch_bounds__(128) k_tu_coeffs(int n, const AtomR<R>* __restrict__ at, Box bx, R aewald,
+__global__ void __launch_bounds__(128) k_tu_coeffs(int n, const int* __restrict__ order, const AtomR<R>* __restrict__ at, Box bx, R aewald,
                                                    const int* __restrict__ nbr, int cap, const int* __restrict__ nnb,
                                                    R4<R>* __restrict__ c0, R* __restrict__ c1, R usolv2,
                                                    int* __restrict__ nbru, R4<R>* __restrict__ cu0,
                                                    R* __restrict__ cu1, int* __restrict__ nnbu) {
     const int g = (blockIdx.x * blockDim.x + threadIdx.x) / LPA, lane = threadIdx.x % LPA;
     if (g >= n) return;  // whole lane groups leave together
-    const int i = g;
+    const int i = order[g];
     const int cnt = nnb[i];
     R4<R> pi = at[i].a, ei = at[i].e;
     V3<R> xi = v3<R>(pi.x, pi.y, pi.z);
@@ -276,13 +276,13 @@ __global__ void __launch_bounds__(128) k_tu_coeffs(int n, const AtomR<R>* __rest
 // T v with the stored coefficients (both dipole sets): rows of nnb[i] bulk
 // slots plus the site's scaled partners.  u4: [n][2] R4.
 template <class R, int LPA>
-__global__ void __launch_bounds__(128) k_tu_stored(int n, const int* __restrict__ nbr,
+__global__ void __launch_bounds__(128) k_tu_stored(int n, const int* __restrict__ order, const int* __restrict__ nbr,
                                                    const R4<R>* __restrict__ c0, const R* __restrict__ c1, int cap,
                                                    const int* __restrict__ nnb, const int* __restrict__ xoff,
                                                    const R4<R>* __restrict__ u4, double* __restrict__ Fd,
                                                    double* __restrict__ Fp) {
     const int g = (blockIdx.x * blockDim.x + threadIdx.x) / LPA, lane = threadIdx.x % LPA;
-    const int i = min(g, n - 1);
+    const int i = order[min(g, n - 1)];
     const int cnt = g < n ? nnb[i] + (xoff[i + 1] - xoff[i]) : 0;
     const size_t base = (size_t)i * cap;
     R ax = 0, ay = 0, az = 0, bx_ = 0, by = 0, bz = 0;
@@ -476,7 +476,7 @@ __global__ void k_scaled_coeffs(int np, const ScaledPair* __restrict__ sp, const
 // stride over the sites (a grid of a few blocks per SM), so each block adds
 // its r.z once.
 template <class R, int LPA, bool FIRST>
-__global__ void __launch_bounds__(128) k_precond(int n, const int* __restrict__ nbru, const R4<R>* __restrict__ cu0,
+__global__ void __launch_bounds__(128) k_precond(int n, const int* __restrict__ order, const int* __restrict__ nbru, const R4<R>* __restrict__ cu0,
                                                  const R* __restrict__ cu1, int cap, const int* __restrict__ nnbu,
                                                  const int* __restrict__ xoff, const R4<R>* __restrict__ s4,
                                                  const double* __restrict__ pol, double wdiag,
@@ -488,7 +488,7 @@ __global__ void __launch_bounds__(128) k_precond(int n, const int* __restrict__ 
     double rzd = 0, rzp = 0;
     for (int g0 = blockIdx.x * per_block; g0 < n; g0 += gridDim.x * per_block) {
         const int g = g0 + threadIdx.x / LPA;
-        const int i = min(g, n - 1);
+        const int i = order[min(g, n - 1)];
         const int cnt = g < n ? nnbu[i] + (xoff[i + 1] - xoff[i]) : 0;
         const size_t base = (size_t)i * cap;
         R ax = 0, ay = 0, az = 0, bx_ = 0, by = 0, bz = 0;

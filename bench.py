@@ -55,6 +55,14 @@ class Clocks:
                                        "-lms", "20"], stdout=self.f, stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
+            return
+        # the timed region is short: start it only once samples are flowing
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and self.p.poll() is None:
+            self.f.flush()
+            if os.path.getsize(self.f.name) > 0:
+                break
+            time.sleep(0.02)
 
     def stop(self):
         if self.p is None:

@@ -29,7 +29,8 @@ using namespace amg;
 
 namespace {
 
-constexpr int kOrder = 5;  // B-spline order compiled in (pme.h bseorder default)
+constexpr int kOrder = 5;
+constexpr int kGatherLanes = 8;  // lanes per site in the PME derivative gathers  // B-spline order compiled in (pme.h bseorder default)
 constexpr int kThreads = 128;
 
 inline unsigned nblk(size_t n, int t = kThreads) { return (unsigned)((n + t - 1) / t); }
@@ -586,8 +587,8 @@ void pme_mpole(amg_ctx* ctx, cudaStream_t s) {
     k_convolve<R><<<nblk(pm.Gc, 256), 256, 0, s>>>(pm.Gc, 1, pm.infl, (typename Cplx<R>::type*)pm.cgrid, pm.grid, pm.G);
     KCHECK();
     CKFFT(CufftTypes<R>::inv(pm.i1, pm.cgrid, pm.phig));
-    k_gather<R, kOrder, 20><<<nblk(ctx->n), kThreads, 0, s>>>(ctx->n, pm.phig, 1, pm.theta, pm.k0, K, sc[0], sc[1], sc[2],
-                                                              ctx->phiM);
+    k_gather<R, kOrder, 20, kGatherLanes, 1><<<nblk((size_t)ctx->n * kGatherLanes), kThreads, 0, s>>>(
+        ctx->n, pm.phig, pm.theta, pm.k0, K, sc[0], sc[1], sc[2], ctx->phiM);
     KCHECK();
 }
 
@@ -616,12 +617,9 @@ void pme_dipoles(amg_ctx* ctx, cudaStream_t s, const double* vd, const double* v
     int3 K = make_int3(ctx->K[0], ctx->K[1], ctx->K[2]);
     double sc[3] = {ctx->K[0] / ctx->box[0], ctx->K[1] / ctx->box[1], ctx->K[2] / ctx->box[2]};
     pme_dipole_grids<R>(ctx, s, vd, vp);
-    for (int b = 0; b < 2; b++) {
-        k_gather<R, kOrder, NC><<<nblk(ctx->n), kThreads, 0, s>>>(ctx->n, reinterpret_cast<const R*>(pm.zg) + b, 2,
-                                                                  pm.theta, pm.k0, K, sc[0],
-                                                                  sc[1], sc[2], phi + (size_t)b * NC * ctx->n);
-        KCHECK();
-    }
+    k_gather<R, kOrder, NC, kGatherLanes, 2><<<nblk((size_t)ctx->n * kGatherLanes), kThreads, 0, s>>>(
+        ctx->n, pm.zg, pm.theta, pm.k0, K, sc[0], sc[1], sc[2], phi);
+    KCHECK();
 }
 
 double ewald_alpha(const amg_ctx* ctx) { return ctx->ewald ? ctx->aewald : 0.0; }

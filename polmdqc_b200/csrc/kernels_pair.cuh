@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(128) k_Tu(int n, const int* __restrict__ order
             }
             R damp = ei.y * ej.y;
             if (damp != R(0)) {
-                R t = rr / damp;
+                R t = ratio_<R>(rr, damp);
                 R x = pair_thole<R>(ei.z, ej.z) * t * t * t;
                 R e = exp_<R>(-x);
                 B1 -= e * b1;                 // (1 - lambda3) = e
@@ -247,7 +247,7 @@ __global__ void __launch_bounds__(128) k_tu_coeffs(int n, const int* __restrict_
             P1 = b1; P2 = b2;
             R damp = ei.y * ej.y;
             if (damp != R(0)) {
-                R t = rr / damp;
+                R t = ratio_<R>(rr, damp);
                 R x = pair_thole<R>(ei.z, ej.z) * t * t * t;
                 R e = exp_<R>(-x);
                 B1 -= e * b1;

@@ -217,73 +217,118 @@ __global__ void k_convolve(size_t ncomplex, int batch, const R* __restrict__ inf
         for (size_t q = t; q < (size_t)batch * nreal; q += (size_t)gridDim.x * blockDim.x) spread[q] = R(0);
 }
 
-// Gather NC (4, 10 or 20) Cartesian potential derivatives per site from
-// a convolved grid (element g at grid[g * gs]: gs = 1 for a real grid, 2
-// for one part of an interleaved complex grid): phi_tuv = (K1/L1)^t (K2/L2)^u (K3/L3)^v sum_g theta...
-// Output order: 0; x y z; xx yy zz xy xz yz; xxx yyy zzz xxy xxz xyy yyz xzz yzz xyz
-template <class R, int P, int NC>
-__global__ void k_gather(int n, const R* __restrict__ grid, int gs, const R* __restrict__ theta,
-                         const int* __restrict__ k0, int3 K, double sc0, double sc1, double sc2,
-                         double* __restrict__ phi) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+// Gather NC (4, 10 or 20) Cartesian potential derivatives per site:
+//   phi_tuv = (K1/L1)^t (K2/L2)^u (K3/L3)^v sum_abc theta1^(t)_a theta2^(u)_b theta3^(v)_c grid
+// from a real grid (NS = 1: grid[g]) or from both parts of the complex
+// dipole grid at once (NS = 2: zg[g].x into phi, zg[g].y into phi + NC n).
+// G consecutive lanes per site; each lane takes whole z-lines (a, b) of the
+// P^3 stencil, contracts the line's P values with the z weights of orders
+// 0..3 and adds them with the x and y weights; the lanes' sums are combined
+// with shuffles.  Output order: 0; x y z; xx yy zz xy xz yz;
+// xxx yyy zzz xxy xxz xyy yyz xzz yzz xyz.
+template <class R, int NC>
+__device__ __forceinline__ void add_derivs(R (&f)[NC], const R (&x)[4], const R (&y)[4], const R (&z)[4]) {
+    f[0] += x[0] * y[0] * z[0];
+    f[1] += x[1] * y[0] * z[0];
+    f[2] += x[0] * y[1] * z[0];
+    f[3] += x[0] * y[0] * z[1];
+    if constexpr (NC >= 10) {
+        f[4] += x[2] * y[0] * z[0];
+        f[5] += x[0] * y[2] * z[0];
+        f[6] += x[0] * y[0] * z[2];
+        f[7] += x[1] * y[1] * z[0];
+        f[8] += x[1] * y[0] * z[1];
+        f[9] += x[0] * y[1] * z[1];
+    }
+    if constexpr (NC >= 20) {
+        f[10] += x[3] * y[0] * z[0];
+        f[11] += x[0] * y[3] * z[0];
+        f[12] += x[0] * y[0] * z[3];
+        f[13] += x[2] * y[1] * z[0];
+        f[14] += x[2] * y[0] * z[1];
+        f[15] += x[1] * y[2] * z[0];
+        f[16] += x[0] * y[2] * z[1];
+        f[17] += x[1] * y[0] * z[2];
+        f[18] += x[0] * y[1] * z[2];
+        f[19] += x[1] * y[1] * z[1];
+    }
+}
+
+template <class R, int P, int NC, int G, int NS>
+__global__ void __launch_bounds__(128) k_gather(int n, const void* __restrict__ gridv, const R* __restrict__ theta,
+                                                const int* __restrict__ k0, int3 K, double sc0, double sc1,
+                                                double sc2, double* __restrict__ phi) {
+    constexpr int ND = NC == 4 ? 2 : NC == 10 ? 3 : 4;  // derivative orders per axis
+    using C = typename Cplx<R>::type;
+    const int g = (blockIdx.x * blockDim.x + threadIdx.x) / G, lane = threadIdx.x % G;
+    const int i = min(g, n - 1);
     const R* t1 = theta + ((size_t)i * 3 + 0) * 4 * P;
     const R* t2 = theta + ((size_t)i * 3 + 1) * 4 * P;
     const R* t3 = theta + ((size_t)i * 3 + 2) * 4 * P;
-    int a0 = k0[3 * i], b0 = k0[3 * i + 1], c0 = k0[3 * i + 2];
-    R f[20];
+    const int a0 = k0[3 * i], b0 = k0[3 * i + 1], c0 = k0[3 * i + 2];
+    int zc[P];
 #pragma unroll
-    for (int j = 0; j < 20; j++) f[j] = 0;
     for (int c = 0; c < P; c++) {
-        R v0 = t3[c], v1 = t3[P + c], v2 = t3[2 * P + c], v3 = t3[3 * P + c];
-        int gc = c0 + c; if (gc >= K.z) gc -= K.z;
-        for (int b = 0; b < P; b++) {
-            R u0 = t2[b], u1 = t2[P + b], u2 = t2[2 * P + b], u3 = t2[3 * P + b];
-            int gb = b0 + b; if (gb >= K.y) gb -= K.y;
-            // x-sums: s_k = sum_a t1^(k)[a] grid
-            R s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-            for (int a = 0; a < P; a++) {
-                int ga = a0 + a; if (ga >= K.x) ga -= K.x;
-                R g = grid[(size_t)gidx(ga, gb, gc, K) * gs];
-                s0 += t1[a] * g;
-                s1 += t1[P + a] * g;
-                if (NC >= 10) s2 += t1[2 * P + a] * g;
-                if (NC >= 20) s3 += t1[3 * P + a] * g;
+        int gc = c0 + c;
+        if (gc >= K.z) gc -= K.z;
+        zc[c] = gc;
+    }
+    R f[NS][NC];
+#pragma unroll
+    for (int s = 0; s < NS; s++)
+#pragma unroll
+        for (int j = 0; j < NC; j++) f[s][j] = 0;
+    for (int l = lane; l < P * P; l += G) {
+        const int a = l / P, b = l - (l / P) * P;
+        int ga = a0 + a; if (ga >= K.x) ga -= K.x;
+        int gb = b0 + b; if (gb >= K.y) gb -= K.y;
+        const size_t line = ((size_t)ga * K.y + gb) * K.z;
+        R z[NS][4], x[4], y[4];
+#pragma unroll
+        for (int d = 0; d < 4; d++) {
+            x[d] = d < ND ? t1[d * P + a] : R(0);
+            y[d] = d < ND ? t2[d * P + b] : R(0);
+#pragma unroll
+            for (int s = 0; s < NS; s++) z[s][d] = 0;
+        }
+#pragma unroll
+        for (int c = 0; c < P; c++) {
+            R q[NS];
+            if constexpr (NS == 2) {
+                const C v = static_cast<const C*>(gridv)[line + zc[c]];
+                q[0] = v.x;
+                q[NS - 1] = v.y;
+            } else {
+                q[0] = static_cast<const R*>(gridv)[line + zc[c]];
             }
-            f[0] += s0 * u0 * v0;
-            f[1] += s1 * u0 * v0;
-            f[2] += s0 * u1 * v0;
-            f[3] += s0 * u0 * v1;
-            if (NC >= 10) {
-                f[4] += s2 * u0 * v0;
-                f[5] += s0 * u2 * v0;
-                f[6] += s0 * u0 * v2;
-                f[7] += s1 * u1 * v0;
-                f[8] += s1 * u0 * v1;
-                f[9] += s0 * u1 * v1;
-            }
-            if (NC >= 20) {
-                f[10] += s3 * u0 * v0;
-                f[11] += s0 * u3 * v0;
-                f[12] += s0 * u0 * v3;
-                f[13] += s2 * u1 * v0;
-                f[14] += s2 * u0 * v1;
-                f[15] += s1 * u2 * v0;
-                f[16] += s0 * u2 * v1;
-                f[17] += s1 * u0 * v2;
-                f[18] += s0 * u1 * v2;
-                f[19] += s1 * u1 * v1;
+#pragma unroll
+            for (int d = 0; d < ND; d++) {
+                const R w = t3[d * P + c];
+#pragma unroll
+                for (int s = 0; s < NS; s++) z[s][d] += w * q[s];
             }
         }
+#pragma unroll
+        for (int s = 0; s < NS; s++) add_derivs<R, NC>(f[s], x, y, z[s]);
     }
+    double sum[NS][NC];
+#pragma unroll
+    for (int s = 0; s < NS; s++)
+#pragma unroll
+        for (int j = 0; j < NC; j++) sum[s][j] = group_sum<G>((double)f[s][j]);
+    if (g >= n) return;
     const int ex[20][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {2, 0, 0}, {0, 2, 0}, {0, 0, 2},
                            {1, 1, 0}, {1, 0, 1}, {0, 1, 1}, {3, 0, 0}, {0, 3, 0}, {0, 0, 3}, {2, 1, 0},
                            {2, 0, 1}, {1, 2, 0}, {0, 2, 1}, {1, 0, 2}, {0, 1, 2}, {1, 1, 1}};
-    double p0[4] = {1, sc0, sc0 * sc0, sc0 * sc0 * sc0};
-    double p1[4] = {1, sc1, sc1 * sc1, sc1 * sc1 * sc1};
-    double p2[4] = {1, sc2, sc2 * sc2, sc2 * sc2 * sc2};
+    const double p0[4] = {1, sc0, sc0 * sc0, sc0 * sc0 * sc0};
+    const double p1[4] = {1, sc1, sc1 * sc1, sc1 * sc1 * sc1};
+    const double p2[4] = {1, sc2, sc2 * sc2, sc2 * sc2 * sc2};
 #pragma unroll
-    for (int j = 0; j < NC; j++) phi[(size_t)NC * i + j] = (double)f[j] * p0[ex[j][0]] * p1[ex[j][1]] * p2[ex[j][2]];
+    for (int s = 0; s < NS; s++)
+#pragma unroll
+        for (int j = 0; j < NC; j++)
+            if (j % G == lane)
+                phi[(size_t)s * NC * n + (size_t)NC * i + j] = sum[s][j] * p0[ex[j][0]] * p1[ex[j][1]] * p2[ex[j][2]];
 }
 
 }  // namespace amg

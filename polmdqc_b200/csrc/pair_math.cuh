@@ -95,6 +95,15 @@ __device__ __forceinline__ float exp_<float>(float x) { return __expf(x); }
 template <>
 __device__ __forceinline__ double exp_<double>(double x) { return exp(x); }
 
+// quotient for the damping ratio r / damp: the fast FP32 division (a few
+// ulp, within the FP32 pair arithmetic's error) or the exact FP64 one
+template <class R>
+__device__ __forceinline__ R ratio_(R a, R b);
+template <>
+__device__ __forceinline__ float ratio_<float>(float a, float b) { return __fdividef(a, b); }
+template <>
+__device__ __forceinline__ double ratio_<double>(double a, double b) { return a / b; }
+
 template <class R>
 __device__ __forceinline__ R erfc_(R x);
 template <>
@@ -131,7 +140,7 @@ template <class R>
 __device__ __forceinline__ void thole_lambda(R r, R damp, R a, R (&lam)[5]) {
     lam[0] = lam[1] = lam[2] = lam[3] = lam[4] = R(1);
     if (damp != R(0)) {
-        R t = r / damp;
+        R t = ratio_<R>(r, damp);
         R x = a * t * t * t;
         R e = exp_<R>(-x);
         lam[1] = R(1) - e;

@@ -166,6 +166,16 @@ struct amg_ctx {
     // launches outside the PCG loop and per loop iteration
     long long kcount = 0, kmain = 0, kbody = 0, klast = 0;
     char* flushbuf = nullptr;
+    // pinned host staging of one evaluation's read-back (status, scalars,
+    // gradients), filled by asynchronous copies behind one synchronisation
+    struct Readback {
+        int over, iters;
+        double e[8];
+        unsigned long long c[4];
+        double hs[8];
+    };
+    Readback* rb = nullptr;
+    double* rb_grad = nullptr;  // [2][3n]
     size_t flush_bytes = 0;
     // adjoint buffers (allocated on the first amg_backward)
     double *adj = nullptr;       // [3n] x 11 vectors: gd gp wd wp bd bp vbar mwp grad trq zero
@@ -662,7 +672,22 @@ void matvec(amg_ctx* ctx, cudaStream_t s, const double* vd, const double* vp, do
     KCHECK();
 }
 
-// pair coefficients of the real-space T for the whole solve
+// the scaled partners' coefficients in the rows' tails (after the bulk
+// pairs, whose counts must be final)
+template <class R>
+void build_scaled_coeffs(amg_ctx* ctx, cudaStream_t s) {
+    if (!ctx->nsp) return;
+    Atoms<R>& A = atoms_of<R>(ctx);
+    const bool sp = ctx->sparse_prec;
+    k_scaled_coeffs<R><<<nblk(ctx->nsp), kThreads, 0, s>>>(
+        ctx->nsp, ctx->sp, ctx->xyz, ctx->pdamp, ctx->thole, ctx->bx, ctx->cut * ctx->cut, ewald_alpha(ctx), ctx->nnb,
+        ctx->cap, ctx->nbr, A.c0, A.c1, ctx->usolvcut * ctx->usolvcut, sp ? ctx->nnbu : nullptr,
+        sp ? ctx->nbru : nullptr, sp ? A.cu0 : nullptr, sp ? A.cu1 : nullptr);
+    KCHECK();
+}
+
+// pair coefficients of the real-space T for the whole solve (the adjoint's
+// FP64 solve; the forward builds them with the permanent field)
 template <class R>
 void build_tu_coeffs(amg_ctx* ctx, cudaStream_t s) {
     const int n = ctx->n;
@@ -684,12 +709,7 @@ void build_tu_coeffs(amg_ctx* ctx, cudaStream_t s) {
                                                                               cu1, nnbu);
     });
     KCHECK();
-    if (ctx->nsp) {
-        k_scaled_coeffs<R><<<nblk(ctx->nsp), kThreads, 0, s>>>(ctx->nsp, ctx->sp, ctx->xyz, ctx->pdamp, ctx->thole,
-                                                              ctx->bx, ctx->cut * ctx->cut, ewald_alpha(ctx), ctx->nnb,
-                                                              ctx->cap, ctx->nbr, A.c0, A.c1, u2, nnbu, nbru, cu0, cu1);
-        KCHECK();
-    }
+    build_scaled_coeffs<R>(ctx, s);
 }
 
 // A v with the stored coefficients; v4 is the R4 copy of (vd, vp).  With
@@ -757,7 +777,8 @@ void precondition(amg_ctx* ctx, cudaStream_t s, bool first, double* rz_out) {
 // set-up of the solve: r = E - A u0, z = p = alpha r, and the first control
 // decision (continue while rr > threshold and iterations < politer)
 template <class R>
-void enqueue_pcg_init(amg_ctx* ctx, cudaStream_t s, cudaGraphConditionalHandle h, int use_handle) {
+void enqueue_pcg_init(amg_ctx* ctx, cudaStream_t s, cudaGraphConditionalHandle h, int use_handle,
+                      bool coeffs_built) {
     const int n = ctx->n;
     Atoms<R>& A = atoms_of<R>(ctx);
     if (!ctx->guess) {
@@ -768,7 +789,7 @@ void enqueue_pcg_init(amg_ctx* ctx, cudaStream_t s, cudaGraphConditionalHandle h
     }
     k_zero<double><<<1, 32, 0, s>>>(ctx->scal, NSCAL);
     KCHECK();
-    build_tu_coeffs<R>(ctx, s);
+    if (!coeffs_built) build_tu_coeffs<R>(ctx, s);
     k_pack_u<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->ud, ctx->up, A.u4);
     KCHECK();
     matvec_stored<R>(ctx, s, A.u4, ctx->ud, ctx->up, ctx->Apd, ctx->App);
@@ -853,15 +874,27 @@ void enqueue_front(amg_ctx* ctx, cudaStream_t s) {
     Atoms<R>& A = atoms_of<R>(ctx);
     const R aew = (R)ctx->aewald;
     if (ctx->has_pol) {
+        // with a solve to follow, the same pass fills the PCG's coefficient rows
+        const bool coef = iterative(ctx);
+        const bool sp = coef && ctx->sparse_prec;
+        const R u2 = (R)(ctx->usolvcut * ctx->usolvcut);
+        auto launch = [&](auto kern, unsigned nb) {
+            kern<<<nb, kThreads, 0, r>>>(n, ctx->sids, A.at, ctx->bx, aew, ctx->nbr, ctx->cap, ctx->nnb, ctx->Ed, ctx->Ep,
+                                         coef ? A.c0 : nullptr, coef ? A.c1 : nullptr, u2, sp ? ctx->nbru : nullptr,
+                                         sp ? A.cu0 : nullptr, sp ? A.cu1 : nullptr, sp ? ctx->nnbu : nullptr);
+        };
         LPA_DISPATCH(ctx->lpa, {
-            if (ctx->ewald)
-                k_perm_field<R, true, L><<<nblk((size_t)n * L), kThreads, 0, r>>>(n, ctx->sids, A.at, ctx->bx, aew, ctx->nbr, ctx->cap,
-                                                                                  ctx->nnb, ctx->Ed, ctx->Ep);
-            else
-                k_perm_field<R, false, L><<<nblk((size_t)n * L), kThreads, 0, r>>>(n, ctx->sids, A.at, ctx->bx, aew, ctx->nbr,
-                                                                                   ctx->cap, ctx->nnb, ctx->Ed, ctx->Ep);
+            const unsigned nb = nblk((size_t)n * L);
+            if (ctx->ewald) {
+                if (coef) launch(k_perm_field<R, true, L, true>, nb);
+                else launch(k_perm_field<R, true, L, false>, nb);
+            } else {
+                if (coef) launch(k_perm_field<R, false, L, true>, nb);
+                else launch(k_perm_field<R, false, L, false>, nb);
+            }
         });
         KCHECK();
+        if (coef) build_scaled_coeffs<R>(ctx, r);
         if (ctx->nsp) {
             k_scaled_field<<<nblk(ctx->nsp), kThreads, 0, r>>>(ctx->nsp, ctx->sp, ctx->xyz, ctx->rp10, ctx->pdamp,
                                                               ctx->thole, ctx->bx, ctx->cut * ctx->cut, ewald_alpha(ctx),
@@ -1024,7 +1057,7 @@ bool capture_graph(amg_ctx* ctx, int flags) {
             cudaGraphConditionalHandle h;
             e = cudaGraphConditionalHandleCreate(&h, graph, 0, 0);
             if (e != cudaSuccess) return fail("conditional handle", e);
-            enqueue_pcg_init<R>(ctx, s, h, 1);
+            enqueue_pcg_init<R>(ctx, s, h, 1, true);
             e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &graph, &deps, &ndeps);
             if (e != cudaSuccess) return fail("capture info", e);
             cudaGraphNodeParams cp = {};
@@ -1074,7 +1107,7 @@ void enqueue_eager(amg_ctx* ctx, int flags) {
     cudaStream_t s = ctx->st;
     enqueue_front<R>(ctx, s);
     if (iterative(ctx)) {
-        enqueue_pcg_init<R>(ctx, s, 0, 0);
+        enqueue_pcg_init<R>(ctx, s, 0, 0, true);
         int cont = 1;
         while (true) {
             CK(cudaMemcpyAsync(&cont, ctx->cont, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -1093,6 +1126,10 @@ int forward_impl(amg_ctx* ctx, int flags, amg_results* res) {
     const bool grad = flags & AMG_DO_GRADIENT;
     const bool analysis = flags & AMG_DO_ANALYSIS;
     cudaStream_t st = ctx->st;
+    if (!ctx->rb) {
+        CK(cudaMallocHost((void**)&ctx->rb, sizeof(amg_ctx::Readback)));
+        CK(cudaMallocHost((void**)&ctx->rb_grad, sizeof(double) * 6 * (size_t)n));
+    }
     for (int attempt = 0; attempt < 2; attempt++) {
         ensure_list_buffers(ctx);
         if (iterative(ctx)) ensure_coeff_buffers<R>(ctx, atoms_of<R>(ctx));
@@ -1111,9 +1148,19 @@ int forward_impl(amg_ctx* ctx, int flags, amg_results* res) {
         }
         if (!graphed) enqueue_eager<R>(ctx, flags);
         ctx->klast = graphed ? -1 : ctx->kcount - kstart;  // graph: completed below from the iteration count
-        int over = 0;
-        CK(cudaMemcpyAsync(&over, ctx->overflow, sizeof(int), cudaMemcpyDeviceToHost, st));
+        // status, scalars and gradients behind one synchronisation
+        amg_ctx::Readback* rb = ctx->rb;
+        CK(cudaMemcpyAsync(&rb->over, ctx->overflow, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(rb->e, ctx->eacc, sizeof(rb->e), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(rb->c, ctx->cnt, sizeof(rb->c), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(rb->hs, ctx->scal, sizeof(double) * NSCAL, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&rb->iters, ctx->iter, sizeof(int), cudaMemcpyDeviceToHost, st));
+        if (grad && res->dem) CK(cudaMemcpyAsync(ctx->rb_grad, ctx->grad_m, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, st));
+        if (grad && res->dep && ctx->has_pol)
+            CK(cudaMemcpyAsync(ctx->rb_grad + 3 * (size_t)n, ctx->grad_p, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost,
+                               st));
         CK(cudaStreamSynchronize(st));
+        const int over = rb->over;
         if (over <= ctx->cap) break;
         if (attempt == 1) {
             ctx->err = "neighbour list overflow";
@@ -1125,14 +1172,10 @@ int forward_impl(amg_ctx* ctx, int flags, amg_results* res) {
     }
     ctx->graphed_last = ctx->use_graphs && ctx->bounds && ctx->gexec != nullptr;
     // ---- results
-    double e[8], hs[NSCAL];
-    unsigned long long c[4];
-    int iters = 0;
-    CK(cudaMemcpyAsync(e, ctx->eacc, sizeof(e), cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(c, ctx->cnt, sizeof(c), cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(hs, ctx->scal, sizeof(hs), cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(&iters, ctx->iter, sizeof(int), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
+    const double* e = ctx->rb->e;
+    const double* hs = ctx->rb->hs;
+    const unsigned long long* c = ctx->rb->c;
+    int iters = ctx->rb->iters;
     double eps = 0;
     int status = AMG_OK;
     if (ctx->klast < 0) ctx->klast = ctx->kmain + (long long)iters * ctx->kbody;
@@ -1142,14 +1185,6 @@ int forward_impl(amg_ctx* ctx, int flags, amg_results* res) {
     } else {
         iters = 0;
     }
-    std::vector<double> h;
-    auto fetch_add = [&](double* dst, const double* src, size_t cnt) {
-        if (!dst) return;
-        h.resize(cnt);
-        CK(cudaMemcpyAsync(h.data(), src, sizeof(double) * cnt, cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        for (size_t k = 0; k < cnt; k++) dst[k] += h[k];
-    };
     auto fetch = [&](double* dst, const double* src, size_t cnt) {
         if (!dst) return;
         CK(cudaMemcpyAsync(dst, src, sizeof(double) * cnt, cudaMemcpyDeviceToHost, st));
@@ -1167,9 +1202,11 @@ int forward_impl(amg_ctx* ctx, int flags, amg_results* res) {
     res->nep = (int64_t)c[1];
     res->pcg_iters = iters;
     res->pcg_eps = eps;
-    if (grad) {
-        fetch_add(res->dem, ctx->grad_m, 3 * (size_t)n);
-        if (ctx->has_pol) fetch_add(res->dep, ctx->grad_p, 3 * (size_t)n);
+    if (grad) {  // the gradients were read back with the scalars; added to the caller's arrays
+        if (res->dem)
+            for (size_t k = 0; k < 3 * (size_t)n; k++) res->dem[k] += ctx->rb_grad[k];
+        if (res->dep && ctx->has_pol)
+            for (size_t k = 0; k < 3 * (size_t)n; k++) res->dep[k] += ctx->rb_grad[3 * (size_t)n + k];
     }
     if (analysis) {
         fetch(res->aem, ctx->aem, n);
@@ -1207,6 +1244,8 @@ int forward_impl(amg_ctx* ctx, int flags, amg_results* res) {
 }
 
 void release(amg_ctx* ctx) {
+    if (ctx->rb) { cudaFreeHost(ctx->rb); ctx->rb = nullptr; }
+    if (ctx->rb_grad) { cudaFreeHost(ctx->rb_grad); ctx->rb_grad = nullptr; }
     double** dbl[] = {&ctx->pole13, &ctx->pol, &ctx->thole, &ctx->pdamp, &ctx->xyz, &ctx->rp10, &ctx->Ed, &ctx->Ep,
                       &ctx->ud, &ctx->up, &ctx->rd, &ctx->rp, &ctx->zd, &ctx->zp, &ctx->pd, &ctx->pp, &ctx->Apd,
                       &ctx->App, &ctx->Fd, &ctx->Fp, &ctx->resd, &ctx->scal, &ctx->eacc, &ctx->grad_m, &ctx->grad_p,
@@ -1289,7 +1328,7 @@ int create_impl(amg_ctx* ctx, const amg_params* P) {
         CK(cudaEventCreateWithFlags(&ctx->ejoin[k], cudaEventDisableTiming));
     }
     if (const char* g = getenv("AMG_NO_GRAPH")) ctx->use_graphs = !(g[0] == '1');
-    ctx->lpa = n < 50000 ? 16 : 8;
+    ctx->lpa = 8;  // lanes per site (8 measured fastest at 12k and 98k sites)
     if (const char* l = getenv("AMG_LPA")) ctx->lpa = atoi(l);
     if (ctx->lpa != 8 && ctx->lpa != 16 && ctx->lpa != 32) ctx->lpa = 16;
     dalloc(ctx, ctx->iter, 1);
@@ -1475,7 +1514,7 @@ int backward_impl(amg_ctx* ctx, const amg_cotangents* cot, amg_param_grads* gr) 
             KCHECK();
             bool ok = true;
             try {
-                enqueue_pcg_init<double>(ctx, s, 0, 0);
+                enqueue_pcg_init<double>(ctx, s, 0, 0, false);
                 int cont = 1;
                 while (true) {
                     CK(cudaMemcpyAsync(&cont, ctx->cont, sizeof(int), cudaMemcpyDeviceToHost, s));

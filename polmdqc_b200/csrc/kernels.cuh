@@ -71,4 +71,27 @@ __device__ __forceinline__ void bulk_radial(R r2, R aewald, R damp, R thl, R (&B
     }
 }
 
+// bulk_radial with Thole damping that also returns the bare Thole-damped
+// lambda_3 b_1 and lambda_5 b_2 (the sparse preconditioner's tensor)
+template <class R, bool EWALD>
+__device__ __forceinline__ void bulk_radial_prec(R r2, R aewald, R damp, R thl, R (&B)[6], R& P1, R& P2) {
+    R rinv = rsqrt_<R>(r2);
+    R r = r2 * rinv;
+    R rinv2 = rinv * rinv;
+    R bare[6];
+    bare_terms<R, 6>(rinv, rinv2, bare);
+    if (EWALD) {
+        ewald_terms<R, 6>(r, rinv2, aewald, B);
+    } else {
+#pragma unroll
+        for (int n = 0; n < 6; n++) B[n] = bare[n];
+    }
+    R lam[5];
+    thole_lambda<R>(r, damp, thl, lam);
+#pragma unroll
+    for (int n = 1; n < 5; n++) B[n] -= (R(1) - lam[n]) * bare[n];
+    P1 = lam[1] * bare[1];
+    P2 = lam[2] * bare[2];
+}
+
 }  // namespace amg

@@ -14,12 +14,19 @@ namespace amg {
 
 // Permanent field at every site from all neighbours' multipoles, bulk
 // (scale 1, Thole damped, Ewald or bare).  Writes Ed = Ep (the d/p
-// differences come only from the scaled pairs).
-template <class R, bool EWALD, int LPA>
+// differences come only from the scaled pairs).  With COEF the same radial
+// factors also fill the PCG's stored coefficient rows (see k_tu_coeffs:
+// c0 = (x_i - x_j, B1), c1 = B2) and the sparse preconditioner's rows (pairs
+// within usolvcut, compacted in row order, when cu0 is given), so the
+// solve's set-up recomputes nothing.
+template <class R, bool EWALD, int LPA, bool COEF>
 __global__ void __launch_bounds__(128) k_perm_field(int n, const int* __restrict__ order, const AtomR<R>* __restrict__ at, Box bx, R aewald,
                                                     const int* __restrict__ nbr, int cap,
                                                     const int* __restrict__ nnb, double* __restrict__ Ed,
-                                                    double* __restrict__ Ep) {
+                                                    double* __restrict__ Ep, R4<R>* __restrict__ c0,
+                                                    R* __restrict__ c1, R usolv2, int* __restrict__ nbru,
+                                                    R4<R>* __restrict__ cu0, R* __restrict__ cu1,
+                                                    int* __restrict__ nnbu) {
     const int g = (blockIdx.x * blockDim.x + threadIdx.x) / LPA, lane = threadIdx.x % LPA;
     const int i = order[min(g, n - 1)];
     const int cnt = g < n ? nnb[i] : 0;
@@ -27,16 +34,47 @@ __global__ void __launch_bounds__(128) k_perm_field(int n, const int* __restrict
     V3<R> xi = v3<R>(Ai.a.x, Ai.a.y, Ai.a.z);
     R pdi = Ai.e.y, thi = Ai.e.z;
     double fx = 0, fy = 0, fz = 0;
-    const int* row = nbr + (size_t)i * cap;
-    for (int s = lane; s < cnt; s += LPA) {
-        int j = row[s];
-        AtomR<R> Aj = at[j];
-        V3<R> r = min_image<R>(xi - v3<R>(Aj.a.x, Aj.a.y, Aj.a.z), bx);  // target i - source j
-        R B[6];
-        bulk_radial<R, EWALD, true>(dot(r, r), aewald, pdi * Aj.e.y, pair_thole<R>(thi, Aj.e.z), B);
-        V3<R> E = field_of_mpole<R>(load_mpole(Aj), r, B[1], B[2], B[3]);
-        fx += E.x; fy += E.y; fz += E.z;
+    const size_t base = (size_t)i * cap;
+    const int* row = nbr + base;
+    // lanes of this group within the warp, and the lanes below this one
+    const unsigned gmask = LPA == 32 ? 0xffffffffu : ((1u << LPA) - 1u) << ((threadIdx.x & 31) / LPA * LPA);
+    const unsigned below = (1u << (threadIdx.x & 31)) - 1u;
+    int nu = 0;  // preconditioner entries of this row so far
+    for (int s0 = 0; s0 < cnt; s0 += LPA) {  // all lanes of a group take the same trips
+        const int s = s0 + lane;
+        const bool ok = s < cnt;
+        int j = 0;
+        V3<R> r = v3<R>(0, 0, 0);
+        R P1 = 0, P2 = 0, r2 = 0;
+        if (ok) {
+            j = row[s];
+            AtomR<R> Aj = at[j];
+            r = min_image<R>(xi - v3<R>(Aj.a.x, Aj.a.y, Aj.a.z), bx);  // target i - source j
+            r2 = dot(r, r);
+            R B[6];
+            if (COEF) {
+                bulk_radial_prec<R, EWALD>(r2, aewald, pdi * Aj.e.y, pair_thole<R>(thi, Aj.e.z), B, P1, P2);
+                c0[base + s] = make_r4<R>(r.x, r.y, r.z, B[1]);
+                c1[base + s] = B[2];
+            } else {
+                bulk_radial<R, EWALD, true>(r2, aewald, pdi * Aj.e.y, pair_thole<R>(thi, Aj.e.z), B);
+            }
+            V3<R> E = field_of_mpole<R>(load_mpole(Aj), r, B[1], B[2], B[3]);
+            fx += E.x; fy += E.y; fz += E.z;
+        }
+        if (COEF && cu0) {
+            const bool take = ok && r2 <= usolv2;
+            const unsigned b = __ballot_sync(gmask, take) & gmask;
+            if (take) {
+                const size_t q = base + nu + __popc(b & below);
+                nbru[q] = j;
+                cu0[q] = make_r4<R>(r.x, r.y, r.z, P1);
+                cu1[q] = P2;
+            }
+            nu += __popc(b);
+        }
     }
+    if (COEF && cu0 && lane == 0 && g < n) nnbu[i] = nu;
     fx = group_sum<LPA>(fx); fy = group_sum<LPA>(fy); fz = group_sum<LPA>(fz);
     if (lane == 0 && g < n) {
         Ed[3 * i] = fx; Ed[3 * i + 1] = fy; Ed[3 * i + 2] = fz;

@@ -80,7 +80,8 @@ struct Pme {
     int* k0 = nullptr;                       // [n][3]
     cufftHandle f1 = 0, i1 = 0, zplan = 0;
     // dipole grids: d + i p interleaved, transformed in place
-    typename Cplx<R>::type* zg = nullptr;    // [K1 K2 K3]
+    typename Cplx<R>::type* zg = nullptr;    // [K1 K2 K3] spreading grid, zero between uses
+    typename Cplx<R>::type* zq = nullptr;    // [K1 K2 K3] convolved potentials (d + i p)
     R* Gfull = nullptr;                      // [K1 K2 K3] influence function on the full grid
     double infl_box[3] = {0, 0, 0};
     size_t G = 0, Gc = 0;
@@ -158,6 +159,7 @@ struct amg_ctx {
     double cell_volume = 1.0;
     int npolar = 0;
     int *iter = nullptr, *cont = nullptr;
+    int* dir_done = nullptr;  // block counter of k_pcg_dir (back to 0 after every launch)
     // captured evaluation (periodic systems)
     bool use_graphs = true, graph_dirty = true, graphed_last = false;
     cudaGraphExec_t gexec = nullptr;
@@ -172,7 +174,7 @@ struct amg_ctx {
         int over, iters;
         double e[8];
         unsigned long long c[4];
-        double hs[8];
+        double hs[NSCAL];
     };
     Readback* rb = nullptr;
     double* rb_grad = nullptr;  // [2][3n]
@@ -350,6 +352,8 @@ void pme_prepare(amg_ctx* ctx, Pme<R>& pm) {
         cufftHandle hs[2] = {pm.f1, pm.i1};
         for (int k = 0; k < 2; k++) CKFFT(cufftSetStream(hs[k], ctx->st));
         dalloc(ctx, pm.zg, pm.G);
+        dalloc(ctx, pm.zq, pm.G);
+        CK(cudaMemset(pm.zg, 0, sizeof(typename Cplx<R>::type) * pm.G));
         dalloc(ctx, pm.Gfull, pm.G);
         // in-place complex transform of the dipole grid (d + i p)
         CKFFT(cufftPlan3d(&pm.zplan, K1, K2, K3, CufftTypes<R>::c2c));
@@ -396,7 +400,7 @@ void pme_destroy(Pme<R>& pm) {
     cufftHandle* hs[3] = {&pm.f1, &pm.i1, &pm.zplan};
     for (int k = 0; k < 3; k++)
         if (*hs[k]) { cufftDestroy(*hs[k]); *hs[k] = 0; }
-    dfree(pm.zg); dfree(pm.Gfull);
+    dfree(pm.zg); dfree(pm.zq); dfree(pm.Gfull);
     dfree(pm.grid); dfree(pm.phig); dfree(pm.cgrid); dfree(pm.infl); dfree(pm.theta); dfree(pm.k0);
     pm.ready = false;
 }
@@ -603,21 +607,33 @@ void pme_mpole(amg_ctx* ctx, cudaStream_t s) {
 }
 
 // spread two dipole sets into the complex grid pm.zg (d + i p), transform,
-// convolve and transform back in place
+// convolve into pm.zq (clearing pm.zg for the next spreading) and transform
+// pm.zq back in place.  `spread` false: the grid already holds the spread
+// dipoles (the PCG's fused direction update put them there).  The PCG's
+// last direction update leaves a spread grid behind, so every other caller
+// clears it first.
 template <class R>
-void pme_dipole_grids(amg_ctx* ctx, cudaStream_t s, const double* vd, const double* vp) {
+void spread_dipoles(amg_ctx* ctx, cudaStream_t s, const double* vd, const double* vp) {
     Pme<R>& pm = pme_of<R>(ctx);
     int3 K = make_int3(ctx->K[0], ctx->K[1], ctx->K[2]);
     double sc[3] = {ctx->K[0] / ctx->box[0], ctx->K[1] / ctx->box[1], ctx->K[2] / ctx->box[2]};
-    CK(cudaMemsetAsync(pm.zg, 0, sizeof(typename Cplx<R>::type) * pm.G, s));
     k_spread_dipoles<R, kOrder><<<ctx->n, 128, 0, s>>>(ctx->n, ctx->sids, vd, vp, pm.theta, pm.k0, K, (R)sc[0],
                                                         (R)sc[1], (R)sc[2], pm.zg);
     KCHECK();
+}
+
+template <class R>
+void pme_dipole_grids(amg_ctx* ctx, cudaStream_t s, const double* vd, const double* vp, bool spread = true) {
+    Pme<R>& pm = pme_of<R>(ctx);
+    if (spread) {
+        CK(cudaMemsetAsync(pm.zg, 0, sizeof(typename Cplx<R>::type) * pm.G, s));
+        spread_dipoles<R>(ctx, s, vd, vp);
+    }
     CKFFT(cufftSetStream(pm.zplan, s));
     CKFFT(CufftTypes<R>::cc(pm.zplan, pm.zg, CUFFT_FORWARD));
-    k_scale_grid<R><<<nblk(pm.G, 256), 256, 0, s>>>(pm.G, pm.Gfull, pm.zg);
+    k_scale_grid<R><<<nblk(pm.G, 256), 256, 0, s>>>(pm.G, pm.Gfull, pm.zg, pm.zq);  // also clears zg
     KCHECK();
-    CKFFT(CufftTypes<R>::cc(pm.zplan, pm.zg, CUFFT_INVERSE));
+    CKFFT(CufftTypes<R>::cc(pm.zplan, pm.zq, CUFFT_INVERSE));
 }
 
 // reciprocal potentials of two dipole sets -> phi [2][n][NC]
@@ -628,7 +644,7 @@ void pme_dipoles(amg_ctx* ctx, cudaStream_t s, const double* vd, const double* v
     double sc[3] = {ctx->K[0] / ctx->box[0], ctx->K[1] / ctx->box[1], ctx->K[2] / ctx->box[2]};
     pme_dipole_grids<R>(ctx, s, vd, vp);
     k_gather<R, kOrder, NC, kGatherLanes, 2><<<nblk((size_t)ctx->n * kGatherLanes), kThreads, 0, s>>>(
-        ctx->n, pm.zg, pm.theta, pm.k0, K, sc[0], sc[1], sc[2], phi);
+        ctx->n, pm.zq, pm.theta, pm.k0, K, sc[0], sc[1], sc[2], phi);
     KCHECK();
 }
 
@@ -716,7 +732,7 @@ void build_tu_coeffs(amg_ctx* ctx, cudaStream_t s) {
 // vAv (Ewald only) the dot products v.Av are added to vAv[0..1].
 template <class R>
 void matvec_stored(amg_ctx* ctx, cudaStream_t s, const R4<R>* v4, const double* vd, const double* vp, double* Ad,
-                   double* Ap, double* vAv = nullptr) {
+                   double* Ap, double* vAv = nullptr, bool spread = true) {
     const int n = ctx->n;
     Atoms<R>& A = atoms_of<R>(ctx);
     // real space on the side stream, PME on s
@@ -728,13 +744,13 @@ void matvec_stored(amg_ctx* ctx, cudaStream_t s, const R4<R>* v4, const double* 
     KCHECK();
     if (ctx->ewald) {
         Pme<R>& pm = pme_of<R>(ctx);
-        pme_dipole_grids<R>(ctx, s, vd, vp);
+        pme_dipole_grids<R>(ctx, s, vd, vp, spread);
         join_side(ctx, s);
         int3 K = make_int3(ctx->K[0], ctx->K[1], ctx->K[2]);
         double sc[3] = {ctx->K[0] / ctx->box[0], ctx->K[1] / ctx->box[1], ctx->K[2] / ctx->box[2]};
         constexpr int G = 8;  // lanes per site
         const unsigned blocks = (unsigned)std::min<size_t>(nblk((size_t)n * G), (size_t)ctx->num_sms * 8);
-        k_gather_field<R, kOrder, G><<<blocks, kThreads, 0, s>>>(n, pm.zg, pm.theta, pm.k0, K, sc[0], sc[1], sc[2], vd,
+        k_gather_field<R, kOrder, G><<<blocks, kThreads, 0, s>>>(n, pm.zq, pm.theta, pm.k0, K, sc[0], sc[1], sc[2], vd,
                                                                  vp, ctx->Fd, ctx->Fp, self_coef(ctx), ctx->pol, Ad,
                                                                  Ap, vAv);
         KCHECK();
@@ -757,20 +773,44 @@ constexpr double kPrecDiag = 2.0;
 
 // z = M r for both residual sets from the packed s = alpha r (A.s4); adds
 // r.z to rz_out[0..1]; `first` also starts the directions p = z
+// (and, its last block, the PCG control decision)
 template <class R>
-void precondition(amg_ctx* ctx, cudaStream_t s, bool first, double* rz_out) {
+void precondition(amg_ctx* ctx, cudaStream_t s, bool first, double* rz_out, cudaGraphConditionalHandle h,
+                  int use_handle) {
     const int n = ctx->n;
     Atoms<R>& A = atoms_of<R>(ctx);
     constexpr int L = 4;  // lanes per site: the rows are short
     const unsigned blocks = (unsigned)std::min<size_t>(nblk((size_t)n * L), (size_t)ctx->num_sms * 8);
+    const double thr = pcg_threshold(ctx);
     if (first)
-        k_precond<R, L, true><<<blocks, kThreads, 0, s>>>(n, ctx->sids, ctx->nbru, A.cu0, A.cu1, ctx->cap, ctx->nnbu, ctx->xoff,
-                                                          A.s4, ctx->pol, kPrecDiag, ctx->rd, ctx->rp, ctx->zd, ctx->zp,
-                                                          ctx->pd, ctx->pp, A.p4, rz_out);
+        k_precond<R, L, true><<<blocks, kThreads, 0, s>>>(
+            n, ctx->sids, ctx->nbru, A.cu0, A.cu1, ctx->cap, ctx->nnbu, ctx->xoff, A.s4, ctx->pol, kPrecDiag, ctx->rd,
+            ctx->rp, ctx->zd, ctx->zp, ctx->pd, ctx->pp, A.p4, rz_out, ctx->dir_done, ctx->iter, thr, ctx->politer, h,
+            use_handle, ctx->cont);
     else
-        k_precond<R, L, false><<<blocks, kThreads, 0, s>>>(n, ctx->sids, ctx->nbru, A.cu0, A.cu1, ctx->cap, ctx->nnbu, ctx->xoff,
-                                                           A.s4, ctx->pol, kPrecDiag, ctx->rd, ctx->rp, ctx->zd,
-                                                           ctx->zp, ctx->pd, ctx->pp, A.p4, rz_out);
+        k_precond<R, L, false><<<blocks, kThreads, 0, s>>>(
+            n, ctx->sids, ctx->nbru, A.cu0, A.cu1, ctx->cap, ctx->nnbu, ctx->xoff, A.s4, ctx->pol, kPrecDiag, ctx->rd,
+            ctx->rp, ctx->zd, ctx->zp, ctx->pd, ctx->pp, A.p4, rz_out, ctx->dir_done, ctx->iter, thr, ctx->politer, h,
+            use_handle, ctx->cont);
+    KCHECK();
+}
+
+// p = z + beta p after the control decision; with Ewald fused with the
+// spreading of p for the next matvec
+template <class R>
+void direction(amg_ctx* ctx, cudaStream_t s) {
+    const int n = ctx->n;
+    Atoms<R>& A = atoms_of<R>(ctx);
+    if (ctx->ewald) {
+        Pme<R>& pm = pme_of<R>(ctx);
+        const int3 K = make_int3(ctx->K[0], ctx->K[1], ctx->K[2]);
+        k_pcg_dir_spread<R, kOrder><<<n, 128, 0, s>>>(n, ctx->zd, ctx->zp, ctx->pd, ctx->pp, ctx->scal, A.p4, pm.theta,
+                                                       pm.k0, K, (R)(ctx->K[0] / ctx->box[0]),
+                                                       (R)(ctx->K[1] / ctx->box[1]), (R)(ctx->K[2] / ctx->box[2]),
+                                                       pm.zg);
+    } else {
+        k_pcg_dir<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->zd, ctx->zp, ctx->pd, ctx->pp, ctx->scal, A.p4);
+    }
     KCHECK();
 }
 
@@ -798,22 +838,28 @@ void enqueue_pcg_init(amg_ctx* ctx, cudaStream_t s, cudaGraphConditionalHandle h
                                                ctx->sparse_prec ? A.s4 : nullptr);
     KCHECK();
     if (ctx->sparse_prec) {
-        precondition<R>(ctx, s, true, ctx->scal + RZ_D);
+        precondition<R>(ctx, s, true, ctx->scal + RZ_D, h, use_handle);  // with the first control decision
     } else {
         k_pack_u<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->pd, ctx->pp, A.p4);
         KCHECK();
+        k_pcg_control<<<1, 1, 0, s>>>(ctx->scal, ctx->iter, pcg_threshold(ctx), ctx->politer, 1, h, use_handle,
+                                      ctx->cont);
+        KCHECK();
     }
-    k_pcg_control<<<1, 1, 0, s>>>(ctx->scal, ctx->iter, pcg_threshold(ctx), ctx->politer, 1, h, use_handle, ctx->cont);
-    KCHECK();
+    // the iterations' matvecs find p already spread (the direction update
+    // spreads the next one); the grid is clear after the first matvec
+    if (ctx->ewald) spread_dipoles<R>(ctx, s, ctx->pd, ctx->pp);
 }
 
-// one PCG iteration (both right-hand sides), ending with the control kernel
+// one PCG iteration (both right-hand sides): matvec, update, preconditioner
+// and control decision, direction update
 template <class R>
 void enqueue_pcg_iter(amg_ctx* ctx, cudaStream_t s, cudaGraphConditionalHandle h, int use_handle) {
     const int n = ctx->n, n3 = 3 * n;
     Atoms<R>& A = atoms_of<R>(ctx);
     // p.Ap: fused into the PME gather with Ewald, a separate pass without
-    matvec_stored<R>(ctx, s, A.p4, ctx->pd, ctx->pp, ctx->Apd, ctx->App, ctx->ewald ? ctx->scal + PAP_D : nullptr);
+    matvec_stored<R>(ctx, s, A.p4, ctx->pd, ctx->pp, ctx->Apd, ctx->App, ctx->ewald ? ctx->scal + PAP_D : nullptr,
+                     false);
     if (!ctx->ewald) {
         k_dot2<<<nblk(n3, 256), 256, 0, s>>>(n3, ctx->pd, ctx->Apd, ctx->pp, ctx->App, ctx->scal + PAP_D,
                                               ctx->scal + PAP_P);
@@ -823,11 +869,14 @@ void enqueue_pcg_iter(amg_ctx* ctx, cudaStream_t s, cudaGraphConditionalHandle h
                                                  ctx->rd, ctx->rp, ctx->zd, ctx->zp, ctx->scal,
                                                  ctx->sparse_prec ? A.s4 : nullptr);
     KCHECK();
-    if (ctx->sparse_prec) precondition<R>(ctx, s, false, ctx->scal + RZN_D);
-    k_pcg_dir<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->zd, ctx->zp, ctx->pd, ctx->pp, ctx->scal, A.p4);
-    KCHECK();
-    k_pcg_control<<<1, 1, 0, s>>>(ctx->scal, ctx->iter, pcg_threshold(ctx), ctx->politer, 0, h, use_handle, ctx->cont);
-    KCHECK();
+    if (ctx->sparse_prec) {
+        precondition<R>(ctx, s, false, ctx->scal + RZN_D, h, use_handle);  // with the control decision
+    } else {
+        k_pcg_control<<<1, 1, 0, s>>>(ctx->scal, ctx->iter, pcg_threshold(ctx), ctx->politer, 0, h, use_handle,
+                                      ctx->cont);
+        KCHECK();
+    }
+    direction<R>(ctx, s);
 }
 
 // FP64 correction sweep: the true residual with every term in FP64, one
@@ -1277,6 +1326,7 @@ void release(amg_ctx* ctx) {
     if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
     dfree(ctx->iter);
     dfree(ctx->cont);
+    dfree(ctx->dir_done);
     dfree(ctx->flushbuf);
     dfree(ctx->adj); dfree(ctx->adj_pot); dfree(ctx->adj_n); dfree(ctx->adj_vec); dfree(ctx->adj_phi);
     dfree(ctx->adj_dpole);
@@ -1333,6 +1383,8 @@ int create_impl(amg_ctx* ctx, const amg_params* P) {
     if (ctx->lpa != 8 && ctx->lpa != 16 && ctx->lpa != 32) ctx->lpa = 16;
     dalloc(ctx, ctx->iter, 1);
     dalloc(ctx, ctx->cont, 1);
+    dalloc(ctx, ctx->dir_done, 1);
+    CK(cudaMemset(ctx->dir_done, 0, sizeof(int)));
     CK(cudaMemset(ctx->iter, 0, sizeof(int)));
     if (ctx->has_pol)
         for (int i = 0; i < n; i++) ctx->npolar += P->polarity[i] > 0;

@@ -94,4 +94,34 @@ __device__ __forceinline__ void bulk_radial_prec(R r2, R aewald, R damp, R thl, 
     P2 = lam[2] * bare[2];
 }
 
+// PCG scalars: rz (current), p.Ap, rz of the next iteration, r.r, and the
+// previous rz for the direction update
+enum Scal { RZ_D = 0, RZ_P, PAP_D, PAP_P, RZN_D, RZN_P, RR_D, RR_P, RZO_D, RZO_P, NSCAL };
+
+// PCG control (one thread): counts the iteration, decides whether to
+// continue (residual above threshold and fewer than politer iterations) and,
+// inside a captured graph, sets the WHILE node's condition.  `first` marks the
+// decision taken right after the initial residual.
+__device__ __forceinline__ void pcg_decide(double* __restrict__ scal, int* __restrict__ iter, double thr2, int maxit,
+                                           int first, cudaGraphConditionalHandle h, int use_handle,
+                                           int* __restrict__ cont_out) {
+    int it = first ? 0 : *iter + 1;
+    *iter = it;
+    if (!first) {  // rz_old <- rz, rz <- rz_new: the direction update follows
+        scal[RZO_D] = scal[RZ_D];
+        scal[RZO_P] = scal[RZ_P];
+        scal[RZ_D] = scal[RZN_D];
+        scal[RZ_P] = scal[RZN_P];
+    }
+    double e2 = fmax(scal[RR_D], scal[RR_P]);
+    int cont = (e2 > thr2) && (it < maxit);
+    *cont_out = cont;
+    if (cont) {  // accumulators of the next iteration
+        scal[PAP_D] = scal[PAP_P] = 0;
+        scal[RZN_D] = scal[RZN_P] = 0;
+        scal[RR_D] = scal[RR_P] = 0;
+    }
+    if (use_handle) cudaGraphSetConditional(h, cont ? 1u : 0u);
+}
+
 }  // namespace amg

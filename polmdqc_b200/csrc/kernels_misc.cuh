@@ -2,6 +2,7 @@
 // updates (FP64 vectors, FP64 dot products), energies and torque -> force.
 #pragma once
 #include "kernels.cuh"
+#include "kernels_pme.cuh"
 
 namespace amg {
 
@@ -53,7 +54,6 @@ __global__ void k_matvec_finish(int n, const double* __restrict__ vd, const doub
 }
 
 // scalar slots of the PCG (device memory)
-enum Scal { RZ_D = 0, RZ_P, PAP_D, PAP_P, RZN_D, RZN_P, RR_D, RR_P, NSCAL };
 
 template <class T>
 __global__ void k_zero(T* __restrict__ p, size_t n) {
@@ -61,27 +61,10 @@ __global__ void k_zero(T* __restrict__ p, size_t n) {
     if (i < n) p[i] = T(0);
 }
 
-// PCG control (one thread): counts the iteration, decides whether to
-// continue (residual above threshold and fewer than politer iterations) and,
-// inside a captured graph, sets the WHILE node's condition.  `first` marks the
-// decision taken right after the initial residual.
+
 __global__ void k_pcg_control(double* __restrict__ scal, int* __restrict__ iter, double thr2, int maxit, int first,
                               cudaGraphConditionalHandle h, int use_handle, int* __restrict__ cont_out) {
-    int it = first ? 0 : *iter + 1;
-    *iter = it;
-    if (!first) {  // rz <- rz_new for the next direction update
-        scal[RZ_D] = scal[RZN_D];
-        scal[RZ_P] = scal[RZN_P];
-    }
-    double e2 = fmax(scal[RR_D], scal[RR_P]);
-    int cont = (e2 > thr2) && (it < maxit);
-    *cont_out = cont;
-    if (cont) {  // accumulators of the next iteration
-        scal[PAP_D] = scal[PAP_P] = 0;
-        scal[RZN_D] = scal[RZN_P] = 0;
-        scal[RR_D] = scal[RR_P] = 0;
-    }
-    if (use_handle) cudaGraphSetConditional(h, cont ? 1u : 0u);
+    pcg_decide(scal, iter, thr2, maxit, first, h, use_handle, cont_out);
 }
 
 // r = E - A u and rr.  Diagonal preconditioner (s4 null): z = alpha r,
@@ -177,15 +160,21 @@ __global__ void k_pcg_update(int n, const double* __restrict__ pol, const double
     block_sum_add(rrp, scal + RR_P);
 }
 
-// p = z + (rz_new / rz) p; k_pcg_roll then moves rz_new into rz
+// beta = rz / rz_old after the control decision has rolled the scalars
+__device__ __forceinline__ void pcg_beta(const double* __restrict__ scal, double& bd, double& bp) {
+    bd = scal[RZO_D] != 0 ? scal[RZ_D] / scal[RZO_D] : 0.0;
+    bp = scal[RZO_P] != 0 ? scal[RZ_P] / scal[RZO_P] : 0.0;
+}
+
+// p = z + beta p and its R4 copy (runs after the control decision)
 template <class R>
 __global__ void k_pcg_dir(int n, const double* __restrict__ zd, const double* __restrict__ zp,
                           double* __restrict__ pd, double* __restrict__ pp, const double* __restrict__ scal,
                           R4<R>* __restrict__ p4) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    double bd = scal[RZ_D] != 0 ? scal[RZN_D] / scal[RZ_D] : 0.0;
-    double bp = scal[RZ_P] != 0 ? scal[RZN_P] / scal[RZ_P] : 0.0;
+    double bd, bp;
+    pcg_beta(scal, bd, bp);
     double a[3], b[3];
     for (int c = 0; c < 3; c++) {
         int q = 3 * i + c;
@@ -198,9 +187,47 @@ __global__ void k_pcg_dir(int n, const double* __restrict__ zd, const double* __
     p4[2 * i + 1] = make_r4<R>((R)b[0], (R)b[1], (R)b[2], R(0));
 }
 
-__global__ void k_pcg_roll(double* scal) {
-    scal[RZ_D] = scal[RZN_D];
-    scal[RZ_P] = scal[RZN_P];
+// The direction update fused with the spreading of the new direction for
+// the next matvec: one block of 128 threads per site; threads 0..5 form
+// p = z + beta p (and its R4 copy), then thread t < P^3 adds stencil point t
+// of both sets to the complex grid zg (one vector atomic add; zg holds the
+// cleared grid left by the previous transform).
+template <class R, int P>
+__global__ void __launch_bounds__(128) k_pcg_dir_spread(int n, const double* __restrict__ zd,
+                                                        const double* __restrict__ zp, double* __restrict__ pd,
+                                                        double* __restrict__ pp, const double* __restrict__ scal,
+                                                        R4<R>* __restrict__ p4, const R* __restrict__ theta,
+                                                        const int* __restrict__ k0, int3 K, R sc0, R sc1, R sc2,
+                                                        typename Cplx<R>::type* __restrict__ zg) {
+    __shared__ double pv[6];
+    const int i = blockIdx.x, t = threadIdx.x;
+    if (t < 6) {
+        double bd, bp;
+        pcg_beta(scal, bd, bp);
+        const int c = t % 3;
+        const int q = 3 * i + c;
+        const double v = t < 3 ? zd[q] + bd * pd[q] : zp[q] + bp * pp[q];
+        (t < 3 ? pd : pp)[q] = v;
+        pv[t] = v;
+    }
+    __syncthreads();
+    if (t == 0) {
+        p4[2 * i] = make_r4<R>((R)pv[0], (R)pv[1], (R)pv[2], R(0));
+        p4[2 * i + 1] = make_r4<R>((R)pv[3], (R)pv[4], (R)pv[5], R(0));
+    }
+    if (t >= P * P * P) return;
+    const int a = t / (P * P), b = (t / P) % P, c = t % P;
+    const R* th = theta + (size_t)i * 3 * 4 * P;
+    const R t0 = th[a], t1 = th[P + a];
+    const R u0 = th[4 * P + b], u1 = th[5 * P + b];
+    const R v0 = th[8 * P + c], v1 = th[9 * P + c];
+    const R w100 = t1 * u0 * v0, w010 = t0 * u1 * v0, w001 = t0 * u0 * v1;
+    const R d0 = (R)pv[0] * sc0, d1 = (R)pv[1] * sc1, d2 = (R)pv[2] * sc2;
+    const R q0 = (R)pv[3] * sc0, q1 = (R)pv[4] * sc1, q2 = (R)pv[5] * sc2;
+    int ga = k0[3 * i] + a; if (ga >= K.x) ga -= K.x;
+    int gb = k0[3 * i + 1] + b; if (gb >= K.y) gb -= K.y;
+    int gc = k0[3 * i + 2] + c; if (gc >= K.z) gc -= K.z;
+    add_cplx<R>(zg + gidx(ga, gb, gc, K), d0 * w100 + d1 * w010 + d2 * w001, q0 * w100 + q1 * w010 + q2 * w001);
 }
 
 // One preconditioned correction step u += alpha r with the FP64 residual

@@ -512,7 +512,8 @@ __global__ void k_scaled_coeffs(int np, const ScaledPair* __restrict__ sp, const
 // usolvcut, then the scaled partners).  Adds r.z of both sets to
 // rz_out[0], rz_out[1]; FIRST also starts the directions p = z.  Blocks
 // stride over the sites (a grid of a few blocks per SM), so each block adds
-// its r.z once.
+// its r.z once; with `done`, the last block then takes the PCG control
+// decision (rz_out points into the scalar block at RZ_D (FIRST) or RZN_D).
 template <class R, int LPA, bool FIRST>
 __global__ void __launch_bounds__(128) k_precond(int n, const int* __restrict__ order, const int* __restrict__ nbru, const R4<R>* __restrict__ cu0,
                                                  const R* __restrict__ cu1, int cap, const int* __restrict__ nnbu,
@@ -521,7 +522,10 @@ __global__ void __launch_bounds__(128) k_precond(int n, const int* __restrict__ 
                                                  const double* __restrict__ rd, const double* __restrict__ rp,
                                                  double* __restrict__ zd, double* __restrict__ zp,
                                                  double* __restrict__ pd, double* __restrict__ pp,
-                                                 R4<R>* __restrict__ p4, double* __restrict__ rz_out) {
+                                                 R4<R>* __restrict__ p4, double* __restrict__ rz_out,
+                                                 int* __restrict__ done, int* __restrict__ iter, double thr2,
+                                                 int maxit, cudaGraphConditionalHandle h, int use_handle,
+                                                 int* __restrict__ cont_out) {
     const int lane = threadIdx.x % LPA, per_block = blockDim.x / LPA;
     double rzd = 0, rzp = 0;
     for (int g0 = blockIdx.x * per_block; g0 < n; g0 += gridDim.x * per_block) {
@@ -594,6 +598,16 @@ __global__ void __launch_bounds__(128) k_precond(int n, const int* __restrict__ 
     }
     block_sum_add(rzd, rz_out);
     block_sum_add(rzp, rz_out + 1);
+    // the last block to finish (counted in *done, which it resets) takes the
+    // PCG control decision: every block has added its r.z by then
+    if (done && threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(done, 1) == (int)gridDim.x - 1) {
+            __threadfence();
+            *done = 0;
+            pcg_decide(rz_out - (FIRST ? (int)RZ_D : (int)RZN_D), iter, thr2, maxit, FIRST ? 1 : 0, h, use_handle, cont_out);
+        }
+    }
 }
 
 // scaled pairs' contribution to em, its gradient and the torques (both

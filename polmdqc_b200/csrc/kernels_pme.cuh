@@ -183,15 +183,19 @@ __global__ void __launch_bounds__(128) k_gather_field(int n, const typename Cplx
     }
 }
 
-// G . g on the transformed complex dipole grid (G real, on the full grid)
+// out = G . g on the transformed complex dipole grid (G real, on the full
+// grid), and g cleared for the next spreading
 template <class R>
-__global__ void k_scale_grid(size_t npts, const R* __restrict__ G, typename Cplx<R>::type* __restrict__ g) {
+__global__ void k_scale_grid(size_t npts, const R* __restrict__ G, typename Cplx<R>::type* __restrict__ g,
+                             typename Cplx<R>::type* __restrict__ out) {
     size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= npts) return;
     auto v = g[t];
     const R w = G[t];
     v.x *= w;
     v.y *= w;
+    out[t] = v;
+    v.x = v.y = R(0);
     g[t] = v;
 }
 

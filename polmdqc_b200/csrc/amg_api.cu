@@ -16,6 +16,7 @@
 #include <cufft.h>
 
 #include <algorithm>
+#include <climits>
 #include <initializer_list>
 #include <mutex>
 #include <cmath>
@@ -118,6 +119,7 @@ struct amg_ctx {
     int *zax = nullptr, *xax = nullptr, *yax = nullptr, *axe = nullptr, *mol = nullptr;
     ScaledPair* sp = nullptr;
     int *xoff = nullptr, *xidx = nullptr;  // scaled partners of each atom (CSR)
+    int2* xrange = nullptr;                // smallest and largest scaled-partner index of each atom
     Atoms<float> af;
     Atoms<double> ad;
     // cell list / neighbour list
@@ -550,11 +552,11 @@ void enqueue_lists(amg_ctx* ctx, cudaStream_t s) {
         // FP64 decision within 1e-3 cut^2 of the cutoff
         k_neighbors_cells<<<(unsigned)ncell, kNbrThreads, 0, s>>>(ctx->spos, ctx->sids, ctx->cstart, ctx->cend, cg,
                                                                   ctx->bx, cut2, 1e-3 * cut2, ctx->cap, ctx->xoff,
-                                                                  ctx->xidx, ctx->nbr, ctx->nnb, ctx->overflow);
+                                                                  ctx->xidx, ctx->xrange, ctx->nbr, ctx->nnb, ctx->overflow);
     } else {
         k_neighbors<<<nblk((size_t)n * 32), kThreads, 0, s>>>(n, ctx->spos, ctx->skeys, ctx->sids, ctx->cstart,
                                                               ctx->cend, cg, ctx->bx, cut2, ctx->cap, ctx->xoff,
-                                                              ctx->xidx, ctx->nbr, ctx->nnb, ctx->overflow);
+                                                              ctx->xidx, ctx->xrange, ctx->nbr, ctx->nnb, ctx->overflow);
     }
     KCHECK();
 }
@@ -1302,6 +1304,7 @@ void release(amg_ctx* ctx) {
     for (double** p : dbl) dfree(*p);
     int** ints[] = {&ctx->zax, &ctx->xax, &ctx->yax, &ctx->axe, &ctx->mol, &ctx->ids, &ctx->sids, &ctx->cstart,
                     &ctx->cend, &ctx->nbr, &ctx->nnb, &ctx->overflow, &ctx->xoff, &ctx->xidx};
+    dfree(ctx->xrange);
     for (int** p : ints) dfree(*p);
     dfree(ctx->keys);
     dfree(ctx->skeys);
@@ -1416,6 +1419,13 @@ int create_impl(amg_ctx* ctx, const amg_params* P) {
         }
         upload(ctx, ctx->xoff, off.data(), off.size());
         upload(ctx, ctx->xidx, idx.data(), idx.size());
+        std::vector<int2> xr(n, make_int2(INT_MAX, -1));  // empty range when no partners
+        for (int i = 0; i < n; i++)
+            for (int q = off[i]; q < off[i + 1]; q++) {
+                xr[i].x = std::min(xr[i].x, idx[q]);
+                xr[i].y = std::max(xr[i].y, idx[q]);
+            }
+        upload(ctx, ctx->xrange, xr.data(), xr.size());
     }
     upload(ctx, ctx->sp, sp.data(), sp.size());
     dalloc(ctx, ctx->xyz, 3 * (size_t)n);

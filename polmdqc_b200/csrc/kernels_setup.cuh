@@ -165,7 +165,7 @@ __global__ void k_cell_bounds(int n, const unsigned* __restrict__ skeys, const i
 __global__ void k_neighbors(int n, const double4* __restrict__ spos, const unsigned* __restrict__ skeys,
                             const int* __restrict__ sids, const int* __restrict__ cstart,
                             const int* __restrict__ cend, CellGrid cg, Box bx, double cut2, int cap,
-                            const int* __restrict__ xoff, const int* __restrict__ xidx,
+                            const int* __restrict__ xoff, const int* __restrict__ xidx, const int2* __restrict__ xrange,
                             int* __restrict__ nbr, int* __restrict__ nnb, int* __restrict__ overflow) {
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (w >= n) return;  // whole warps exit together
@@ -176,6 +176,7 @@ __global__ void k_neighbors(int n, const double4* __restrict__ spos, const unsig
     const int c0 = key / (cg.nc[2] * cg.nc[1]);
     const double4 pi = spos[w];
     const int x0 = xoff[i], x1 = xoff[i + 1];
+    const int2 xr = xrange[i];  // index range of i's scaled partners
     const int limit = cap - (x1 - x0);  // the row's tail holds the scaled partners
     int* row = nbr + (size_t)i * cap;
     int cnt = 0;
@@ -204,7 +205,7 @@ __global__ void k_neighbors(int n, const double4* __restrict__ spos, const unsig
                         double ry = wrap1<double>(pj.y - pi.y, bx.L[1], bx.iL[1]);
                         double rz = wrap1<double>(pj.z - pi.z, bx.L[2], bx.iL[2]);
                         hit = j != i && rx * rx + ry * ry + rz * rz <= cut2;
-                        if (hit)
+                        if (hit && j >= xr.x && j <= xr.y)
                             for (int q = x0; q < x1; q++) hit &= (xidx[q] != j);
                     }
                     unsigned m = __ballot_sync(0xffffffffu, hit);
@@ -242,7 +243,7 @@ constexpr int kNbrThreads = 256;
 __global__ void __launch_bounds__(kNbrThreads) k_neighbors_cells(
     const double4* __restrict__ spos, const int* __restrict__ sids, const int* __restrict__ cstart,
     const int* __restrict__ cend, CellGrid cg, Box bx, double cut2, double margin, int cap,
-    const int* __restrict__ xoff, const int* __restrict__ xidx, int* __restrict__ nbr, int* __restrict__ nnb,
+    const int* __restrict__ xoff, const int* __restrict__ xidx, const int2* __restrict__ xrange, int* __restrict__ nbr, int* __restrict__ nnb,
     int* __restrict__ overflow) {
     __shared__ float4 cpos[kNbrChunk];
     __shared__ int csrt[kNbrChunk];  // sorted index
@@ -326,6 +327,7 @@ __global__ void __launch_bounds__(kNbrThreads) k_neighbors_cells(
                 const double4 xi = spos[ph];
                 const float hx = (float)rel(xi.x, 0), hy = (float)rel(xi.y, 1), hz = (float)rel(xi.z, 2);
                 const int x0 = xoff[i], x1 = xoff[i + 1];
+                const int2 xr = xrange[i];  // index range of i's scaled partners
                 const int limit = cap - (x1 - x0);  // the row's tail holds the scaled partners
                 // the first kExcl scaled partners in registers, the rest read when needed
                 constexpr int kExcl = 8;
@@ -352,7 +354,7 @@ __global__ void __launch_bounds__(kNbrThreads) k_neighbors_cells(
                                 const double rz = wrap1<double>(pj.z - xi.z, bx.L[2], bx.iL[2]);
                                 hit = rx * rx + ry * ry + rz * rz <= cut2;
                             }
-                            if (hit) {
+                            if (hit && j >= xr.x && j <= xr.y) {  // only then can j be a scaled partner
 #pragma unroll
                                 for (int q = 0; q < kExcl; q++) hit &= (ex[q] != j);
                                 for (int q = x0 + kExcl; q < x1; q++) hit &= (xidx[q] != j);

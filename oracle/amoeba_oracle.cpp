@@ -64,6 +64,14 @@ inline V3 cross(V3 a, V3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b
 inline double norm(V3 a) { return std::sqrt(dot(a, a)); }
 inline V3 unit(V3 a) { return (1.0 / norm(a)) * a; }
 
+// W_ab += g_a r_b: strain derivative of a pair term whose gradient with
+// respect to the separation r is g.
+inline void add_outer(double W[3][3], V3 g, V3 r) {
+    const double gv[3] = {g.x, g.y, g.z}, rv[3] = {r.x, r.y, r.z};
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) W[a][b] += gv[a] * rv[b];
+}
+
 // compact multipole: [q, dx, dy, dz, Qxx, Qxy, Qxz, Qyy, Qyz, Qzz]
 struct Mp { double c[10]; };
 
@@ -229,7 +237,7 @@ void rotate_multipoles(System& s, const amg_params* P) {
 // algorithm of src/md/torque.cpp:42-397 (Popelier & Stone 1994; Sagui et al.
 // 2004).  grad receives dE/dx contributions.
 void torque_to_gradient(const System& s, const amg_params* P, const std::vector<V3>& trq,
-                        std::vector<V3>& grad) {
+                        std::vector<V3>& grad, double (*vir)[3] = nullptr) {
     for (int i = 0; i < s.n; i++) {
         int ft = P->polaxe[i];
         if (ft == AMG_FRAME_NONE) continue;
@@ -264,7 +272,12 @@ void torque_to_gradient(const System& s, const amg_params* P, const std::vector<
         }
         V3 uv = unit(cross(v, u)), uw = unit(cross(w, u)), vw = unit(cross(w, v));
         double uvc = dot(u, v), uvsn = std::sqrt(1 - uvc * uvc);
-        auto add = [&](int at, V3 g) { grad[at] = grad[at] + g; };
+        // the frame atoms' share of the virial: each gradient times the
+        // frame atom's offset from the site (src/md/torque.cpp:360-395)
+        auto add = [&](int at, V3 g) {
+            grad[at] = grad[at] + g;
+            if (vir && at != ib) add_outer(vir, g, min_image(s, s.x[at] - s.x[ib]));
+        };
         if (ft == AMG_FRAME_ZONLY) {
             V3 du = (dpv / (us * uvsn)) * uv + (dpw / us) * uw;
             add(ia, du);
@@ -639,7 +652,8 @@ inline int gidx(const Pme& pm, int a, int b, int c) {
 // Reciprocal-space potential derivatives (Cartesian, 20 per atom) of a set of
 // multipoles (only sites with `use` nonzero spread).  Returns also the
 // reciprocal energy 1/2 sum_i M_i . phi_i for that set.
-void pme_potential(const System& s, const Pme& pm, const std::vector<Mp>& M, std::vector<double>& phi) {
+void pme_potential(const System& s, const Pme& pm, const std::vector<Mp>& M, std::vector<double>& phi,
+                   std::vector<cd>* transform = nullptr) {
     const int p = pm.p;
     const size_t G = (size_t)pm.K[0] * pm.K[1] * pm.K[2];
     std::vector<cd> grid(G, 0.0);
@@ -666,6 +680,7 @@ void pme_potential(const System& s, const Pme& pm, const std::vector<Mp>& M, std
         }
     }
     dft3(grid, pm.K, -1);
+    if (transform) *transform = grid;
     const double pref = 1.0 / (kPi * pm.V);
     for (int a = 0; a < pm.K[0]; a++)
         for (int b = 0; b < pm.K[1]; b++)
@@ -700,6 +715,56 @@ void pme_potential(const System& s, const Pme& pm, const std::vector<Mp>& M, std
             phi[20 * (size_t)i + j] = f[j] * std::pow(sc[0], e[0]) * std::pow(sc[1], e[1]) * std::pow(sc[2], e[2]);
         }
     }
+}
+
+// Strain derivative of the reciprocal bilinear form
+//   U(X, Y) = sum_m g(m) Re[S_X(m) conj S_Y(m)]
+// through g alone (h -> (1 - eps^T) h and V -> V (1 + tr eps) at fixed
+// fractional coordinates):
+//   dg/deps_ab = g (-delta_ab + 2 (1/h^2 + pi^2/alpha^2) h_a h_b),
+// the reciprocal virial of Essmann et al. (1995) in dE/d(strain) form.  Adds
+// `weight` times that sum to W.  The dependence of S on the multipole
+// orientation relative to h is the separate multipole term (mpole_virial).
+void pme_kvir(const System& s, const Pme& pm, const std::vector<cd>& SX, const std::vector<cd>& SY, double weight,
+              double W[3][3]) {
+    const double pref = 1.0 / (kPi * pm.V);
+    const double c2 = kPi * kPi / (s.alpha * s.alpha);
+    double acc[3][3] = {};
+    for (int a = 0; a < pm.K[0]; a++)
+        for (int b = 0; b < pm.K[1]; b++)
+            for (int c = 0; c < pm.K[2]; c++) {
+                if (a == 0 && b == 0 && c == 0) continue;
+                size_t id = ((size_t)a * pm.K[1] + b) * pm.K[2] + c;
+                int ma = a <= pm.K[0] / 2 ? a : a - pm.K[0];
+                int mb = b <= pm.K[1] / 2 ? b : b - pm.K[1];
+                int mc = c <= pm.K[2] / 2 ? c : c - pm.K[2];
+                double h[3] = {ma / pm.L[0], mb / pm.L[1], mc / pm.L[2]};
+                double h2 = h[0] * h[0] + h[1] * h[1] + h[2] * h[2];
+                double g = pref * std::exp(-c2 * h2) / h2 / (pm.bsmod[0][a] * pm.bsmod[1][b] * pm.bsmod[2][c]);
+                double e = g * (SX[id] * std::conj(SY[id])).real();
+                double t = 2.0 * (1.0 / h2 + c2);
+                for (int i = 0; i < 3; i++)
+                    for (int j = 0; j < 3; j++) acc[i][j] += e * (t * h[i] * h[j] - (i == j ? 1.0 : 0.0));
+            }
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) W[i][j] += weight * acc[i][j];
+}
+
+// Multipole term of the reciprocal strain derivative.  At fixed fractional
+// coordinates a strain acts on S(m) as if each source were deformed,
+// d -> (1 - eps) d and Q -> Q - eps Q - Q eps^T, so for a bilinear energy
+// whose derivative with respect to the source X_j is the potential set phi:
+//   W_ab -= phi_a d_b + 2 (H Q)_ab,   H = grad grad phi.
+void mpole_virial(const Mp& X, const double* p, double W[3][3]) {
+    const double d[3] = {X.c[1], X.c[2], X.c[3]};
+    const double Q[3][3] = {{X.c[4], X.c[5], X.c[6]}, {X.c[5], X.c[7], X.c[8]}, {X.c[6], X.c[8], X.c[9]}};
+    const double H[3][3] = {{p[4], p[7], p[8]}, {p[7], p[5], p[9]}, {p[8], p[9], p[6]}};
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) {
+            double v = p[1 + a] * d[b];
+            for (int c = 0; c < 3; c++) v += 2 * H[a][c] * Q[c][b];
+            W[a][b] -= v;
+        }
 }
 
 // Explicit Ewald k-space sum (no B-splines) for validation: potential
@@ -751,9 +816,10 @@ struct Work {
     Options opt;
 };
 
-void recip_potential(Work& w, const std::vector<Mp>& M, std::vector<double>& phi) {
+void recip_potential(Work& w, const std::vector<Mp>& M, std::vector<double>& phi,
+                     std::vector<cd>* transform = nullptr) {
     if (w.opt.kmax > 0) kspace_potential(w.s, M, w.opt.kmax, phi);
-    else pme_potential(w.s, w.pm, M, phi);
+    else pme_potential(w.s, w.pm, M, phi, transform);
 }
 
 // field (= -grad phi) at every site from all sources in M, real + recip +
@@ -804,6 +870,7 @@ void total_field(Work& w, const std::vector<Mp>& M, int which, std::vector<V3>& 
 
 struct Result {
     double em = 0, ep = 0, einter = 0;
+    double vir[3][3] = {};  // dE/d(strain), not yet symmetrised
     long nem = 0, nep = 0;
     std::vector<V3> dem, dep;
     std::vector<double> aem, aep;
@@ -933,7 +1000,7 @@ int solve_dipoles(Work& w, Result& R, double tol_override, int maxit_override) {
 }
 
 
-struct Flags { bool grad, analysis; };
+struct Flags { bool grad, analysis, virial; };
 
 void evaluate(Work& w, Flags fl, Result& R, double tol_override, int maxit_override, int& status) {
     System& s = w.s;
@@ -953,7 +1020,7 @@ void evaluate(Work& w, Flags fl, Result& R, double tol_override, int maxit_overr
         {
             std::vector<V3> gl(s.n, V3{0, 0, 0}), tl(s.n, V3{0, 0, 0});
             std::vector<double> al(s.n, 0.0);
-            double el = 0, eil = 0;
+            double el = 0, eil = 0, wl[3][3] = {};
             long nl = 0;
 #pragma omp for schedule(dynamic, 256)
             for (size_t pi = 0; pi < w.pairs.size(); pi++) {
@@ -982,12 +1049,15 @@ void evaluate(Work& w, Flags fl, Result& R, double tol_override, int maxit_overr
                 gl[P.i] = gl[P.i] - gk;
                 tl[P.k] = tl[P.k] + tk;
                 tl[P.i] = tl[P.i] + ti;
+                if (fl.virial) add_outer(wl, gk, P.r);
             }
 #pragma omp critical
             {
                 em += el;
                 einter += eil;
                 nem += nl;
+                for (int a = 0; a < 3; a++)
+                    for (int b = 0; b < 3; b++) R.vir[a][b] += wl[a][b];
                 for (int i = 0; i < s.n; i++) {
                     R.dem[i] = R.dem[i] + gl[i];
                     tm[i] = tm[i] + tl[i];
@@ -1001,8 +1071,10 @@ void evaluate(Work& w, Flags fl, Result& R, double tol_override, int maxit_overr
     }
     // ---- permanent multipoles, reciprocal + self + net-charge terms
     std::vector<double> phiM;
+    std::vector<cd> SM;  // forward transform of the permanent grid (virial)
+    const bool kvir = fl.virial && w.opt.kmax <= 0;
     if (s.ewald) {
-        recip_potential(w, M, phiM);
+        recip_potential(w, M, phiM, kvir ? &SM : nullptr);
         double er = 0;
         for (int i = 0; i < s.n; i++) {
             const double* ph = &phiM[20 * (size_t)i];
@@ -1011,7 +1083,9 @@ void evaluate(Work& w, Flags fl, Result& R, double tol_override, int maxit_overr
             R.aem[i] += e;
             R.dem[i] = R.dem[i] + site_gradient(M[i], ph);
             tm[i] = tm[i] + site_torque(M[i], ph);
+            if (fl.virial) mpole_virial(M[i], ph, R.vir);
         }
+        if (kvir) pme_kvir(s, w.pm, SM, SM, 0.5, R.vir);
         double a = s.alpha, es = 0, qt = 0;
         for (int i = 0; i < s.n; i++) {
             const Mp& m = M[i];
@@ -1026,11 +1100,13 @@ void evaluate(Work& w, Flags fl, Result& R, double tol_override, int maxit_overr
         double V = s.L[0] * s.L[1] * s.L[2];
         double echg = -kPi * qt * qt / (2 * V * a * a);
         R.em += er + es + echg;
+        for (int c = 0; c < 3; c++) R.vir[c][c] -= echg;  // echg ~ 1/V
     }
     R.em *= s.f;
     R.einter *= s.f;
     for (int i = 0; i < s.n; i++) { R.dem[i] = s.f * R.dem[i]; tm[i] = s.f * tm[i]; R.aem[i] *= s.f; }
-    if (fl.grad) torque_to_gradient(s, w.P, tm, R.dem);
+    for (auto& row : R.vir) for (double& v : row) v *= s.f;
+    if (fl.grad) torque_to_gradient(s, w.P, tm, R.dem, fl.virial ? R.vir : nullptr);
 
     // ---- polarization
     if (s.poltyp == AMG_POL_NONE) return;
@@ -1046,9 +1122,11 @@ void evaluate(Work& w, Flags fl, Result& R, double tol_override, int maxit_overr
     if (!fl.grad) return;
     const bool mutual = s.poltyp == AMG_POL_MUTUAL;
     // real space: gradient of G = 1/2 [U_d(up<->M) + U_p(ud<->M) + U_u(up<->ud)]
+    double wpol[3][3] = {};
 #pragma omp parallel
     {
         std::vector<V3> gl(s.n, V3{0, 0, 0}), tl(s.n, V3{0, 0, 0});
+        double wl[3][3] = {};
 #pragma omp for schedule(dynamic, 256)
         for (size_t pi = 0; pi < w.pairs.size(); pi++) {
             const Pair& P = w.pairs[pi];
@@ -1079,6 +1157,7 @@ void evaluate(Work& w, Flags fl, Result& R, double tol_override, int maxit_overr
             gk = 0.5 * gk;
             gl[k] = gl[k] + gk;
             gl[i] = gl[i] - gk;
+            if (fl.virial) add_outer(wl, gk, P.r);
             // torques on the permanent multipoles
             double b1[20], b2[20];
             source_potential(Tdm, upk, 2, b1);   // up_k at i, d channel
@@ -1091,14 +1170,25 @@ void evaluate(Work& w, Flags fl, Result& R, double tol_override, int maxit_overr
             tl[k] = tl[k] + site_torque(M[k], c1);
         }
 #pragma omp critical
-        for (int i = 0; i < s.n; i++) { R.dep[i] = R.dep[i] + gl[i]; tp[i] = tp[i] + tl[i]; }
+        {
+            for (int i = 0; i < s.n; i++) { R.dep[i] = R.dep[i] + gl[i]; tp[i] = tp[i] + tl[i]; }
+            for (int a = 0; a < 3; a++)
+                for (int b = 0; b < 3; b++) wpol[a][b] += wl[a][b];
+        }
     }
     if (s.ewald) {
         std::vector<Mp> Md(s.n), Mpv(s.n);
         for (int i = 0; i < s.n; i++) { Md[i] = dipole_only(R.ud[i]); Mpv[i] = dipole_only(R.up[i]); }
         std::vector<double> phd, php;
-        recip_potential(w, Md, phd);
-        recip_potential(w, Mpv, php);
+        std::vector<cd> Sd, Sp;
+        recip_potential(w, Md, phd, kvir ? &Sd : nullptr);
+        recip_potential(w, Mpv, php, kvir ? &Sp : nullptr);
+        // G = 1/2 [U(up, M) + U(ud, M) + U(up, ud)] in reciprocal space
+        if (kvir) {
+            pme_kvir(s, w.pm, SM, Sp, 0.5, wpol);
+            pme_kvir(s, w.pm, SM, Sd, 0.5, wpol);
+            if (mutual) pme_kvir(s, w.pm, Sp, Sd, 0.5, wpol);
+        }
         double self = 4.0 * s.alpha * s.alpha * s.alpha / (3.0 * kSqrtPi);
         for (int i = 0; i < s.n; i++) {
             const double* pm = &phiM[20 * (size_t)i];
@@ -1113,10 +1203,25 @@ void evaluate(Work& w, Flags fl, Result& R, double tol_override, int maxit_overr
             tp[i] = tp[i] + site_torque(M[i], avg);
             V3 di{M[i].c[1], M[i].c[2], M[i].c[3]};
             tp[i] = tp[i] + (0.5 * self) * cross(di, R.ud[i] + R.up[i]);
+            if (fl.virial) {
+                double wj[3][3] = {};
+                mpole_virial(upi, pm, wj);
+                mpole_virial(udi, pm, wj);
+                mpole_virial(M[i], pp, wj);
+                mpole_virial(M[i], pd, wj);
+                if (mutual) {
+                    mpole_virial(upi, pd, wj);
+                    mpole_virial(udi, pp, wj);
+                }
+                for (int a = 0; a < 3; a++)
+                    for (int b = 0; b < 3; b++) wpol[a][b] += 0.5 * wj[a][b];
+            }
         }
     }
     for (int i = 0; i < s.n; i++) { R.dep[i] = s.f * R.dep[i]; tp[i] = s.f * tp[i]; }
-    torque_to_gradient(s, w.P, tp, R.dep);
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) R.vir[a][b] += s.f * wpol[a][b];
+    torque_to_gradient(s, w.P, tp, R.dep, fl.virial ? R.vir : nullptr);
 }
 
 // Builds the scaled-pair table from the 1-n and group lists, restating the
@@ -1171,6 +1276,8 @@ typedef struct orc_options {
     double tol;      /* > 0: overrides poleps */
     int32_t maxit;   /* > 0: overrides politer */
     double alpha;    /* > 0: overrides aewald */
+    int32_t raw_virial; /* 1: return dE/d(strain) unsymmetrised (its antisymmetric
+                           part vanishes for a rotation-invariant energy) */
 } orc_options;
 
 int orc_forward(const amg_params* P, const double* xyz, const double box[6], int32_t flags,
@@ -1215,7 +1322,8 @@ int orc_forward(const amg_params* P, const double* xyz, const double box[6], int
     if (s.ewald && w.opt.kmax <= 0) pme_setup(s, w.pm);
     Result R;
     int status;
-    Flags fl{(flags & AMG_DO_GRADIENT) != 0, (flags & AMG_DO_ANALYSIS) != 0};
+    const bool vir = (flags & AMG_DO_VIRIAL) != 0;
+    Flags fl{(flags & AMG_DO_GRADIENT) != 0 || vir, (flags & AMG_DO_ANALYSIS) != 0, vir};
     evaluate(w, fl, R, opt ? opt->tol : 0, opt ? opt->maxit : 0, status);
     res->em = R.em;
     res->ep = R.ep;
@@ -1233,6 +1341,11 @@ int orc_forward(const amg_params* P, const double* xyz, const double box[6], int
         if (res->uinp && !R.up.empty()) { res->uinp[3 * i] = R.up[i].x; res->uinp[3 * i + 1] = R.up[i].y; res->uinp[3 * i + 2] = R.up[i].z; }
     }
     if (res->rpole) std::memcpy(res->rpole, s.rpole13.data(), sizeof(double) * 13 * s.n);
+    if (vir) {
+        const bool raw = opt && opt->raw_virial;
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) res->vir[3 * a + b] += raw ? R.vir[a][b] : 0.5 * (R.vir[a][b] + R.vir[b][a]);
+    }
     for (double v : {R.em, R.ep})
         if (!std::isfinite(v)) return AMG_ERR_NAN;
     return status;

@@ -22,7 +22,8 @@ REF = os.path.join(HERE, "_ref")
 
 
 class orc_options(C.Structure):
-    _fields_ = [("kmax", C.c_double), ("tol", C.c_double), ("maxit", C.c_int32), ("alpha", C.c_double)]
+    _fields_ = [("kmax", C.c_double), ("tol", C.c_double), ("maxit", C.c_int32), ("alpha", C.c_double),
+                ("raw_virial", C.c_int32)]
 
 
 def build(force=False):
@@ -49,13 +50,13 @@ def lib():
 
 
 def forward(system, settings: Settings, xyz=None, flags=abi.DO_ENERGY | abi.DO_GRADIENT | abi.DO_DIPOLES,
-            kmax=0.0, tol=0.0, maxit=0, alpha=0.0, params=None, check=True):
+            kmax=0.0, tol=0.0, maxit=0, alpha=0.0, params=None, check=True, raw_virial=False):
     """FP64 evaluation of em/ep (+gradients, dipoles) for `system`."""
     P = params or Params(system, settings)
     x = np.ascontiguousarray(system.xyz if xyz is None else xyz, np.float64).reshape(-1)
     box = np.ascontiguousarray(system.box, np.float64)
     r, bufs = new_results(system.n)
-    opt = orc_options(kmax, tol, maxit, alpha)
+    opt = orc_options(kmax, tol, maxit, alpha, int(raw_virial))
     rc = lib().orc_forward(C.byref(P.struct), abi.dptr(x), abi.dptr(box), flags, C.byref(opt), C.byref(r))
     if check and rc not in (abi.AMG_OK,):
         raise RuntimeError(f"oracle failed: {abi.STATUS.get(rc, rc)}")

@@ -10,7 +10,7 @@ and the reference source tree (default /root/reference).  Writes:
                         headers, with the input files they apply to;
   ref_water216.json     the reference run (oracle/_ref/ref_dump) on the
                         seeded 216-water box in its only electrostatics mode
-                        (non-Ewald multipoles, 7 A cutoff): em, nem, dem,
+                        (non-Ewald multipoles, 7 A cutoff): em, nem, dem, vir,
                         einter, rotated multipoles, and the coordinates it read;
   ref_params.json       the reference's parameter assignment (mechanic() with
                         Ewald + mutual polarization keys) for the first
@@ -83,7 +83,7 @@ def main(ref_root="/root/reference"):
         systems.write_tinker(s, xyz, key, os.path.join(prm_dir, "water03.prm"),
                              ["multipoleterm only", "mpole-cutoff 7.0", "digits 10"])
         d = run_dump(xyz, key, tmp)
-        keep = {k: d[k] for k in ("n", "x", "y", "z", "em", "nem", "einter", "dem", "mpolecut", "box")}
+        keep = {k: d[k] for k in ("n", "x", "y", "z", "em", "nem", "einter", "dem", "vir", "mpolecut", "box")}
         keep["rpole"] = d["rpole"][: 13 * 30]
         keep["generator"] = "systems.water_box(216, 18.643, seed=0); keys: multipoleterm only, mpole-cutoff 7.0"
         json.dump(keep, open(os.path.join(HERE, "ref_water216.json"), "w"))

@@ -92,3 +92,52 @@ def test_sparse_preconditioner_same_solution_fewer_iterations():
     j6 = oracle.forward(s, dataclasses.replace(base, poleps=1e-6, pcg_prec=False))
     s6 = oracle.forward(s, dataclasses.replace(base, poleps=1e-6, pcg_prec=True))
     assert s6.pcg_iters < j6.pcg_iters
+
+
+def _strained(s, a, b, h):
+    """Copy of s with coordinates (and, for a diagonal strain of a periodic
+    box, the box edge) deformed by 1 + h e_a e_b^T."""
+    t = copy.deepcopy(s)
+    E = np.eye(3)
+    E[a, b] += h
+    t.xyz = s.xyz @ E.T
+    if s.use_bounds:
+        t.box = s.box.copy()
+        t.box[a] *= 1 + h
+    return t
+
+
+@pytest.mark.parametrize("case", ["ewald_mutual", "ewald_direct", "periodic_bare"])
+def test_virial_is_the_strain_derivative(box27, case):
+    """CalcMode::Virial: W = dE/d(strain) of em + ep, with the box deformed
+    with the coordinates (PME grid and alpha fixed).  An orthogonal box admits
+    diagonal strains only, so the off-diagonal part is pinned by the rotation
+    invariance of the energy: the unsymmetrised W has no antisymmetric part."""
+    s = copy.deepcopy(box27)
+    s.box = np.array([9.32, 9.9, 10.4, 90.0, 90.0, 90.0])
+    st = {"ewald_mutual": Settings(aewald=0.7, nfft=(24, 25, 27), cutoff=4.6, poleps=1e-11),
+          "ewald_direct": Settings(aewald=0.7, nfft=(24, 25, 27), cutoff=4.6, poltyp=abi.POL_DIRECT),
+          "periodic_bare": Settings(use_ewald=False, cutoff=4.6, poleps=1e-11)}[case]
+    W = oracle.forward(s, st, flags=abi.DO_ENERGY | abi.DO_VIRIAL, raw_virial=True).vir
+    h = 1e-5
+    for a in range(3):
+        p = oracle.forward(_strained(s, a, a, h), st, flags=abi.DO_ENERGY)
+        m = oracle.forward(_strained(s, a, a, -h), st, flags=abi.DO_ENERGY)
+        fd = (p.em + p.ep - m.em - m.ep) / (2 * h)
+        assert abs(W[a, a] - fd) < 1e-8 * np.abs(W).max()
+    assert np.abs(W - W.T).max() < 1e-9 * np.abs(W).max()
+    sym = oracle.forward(s, st, flags=abi.DO_ENERGY | abi.DO_VIRIAL).vir
+    np.testing.assert_allclose(sym, 0.5 * (W + W.T), rtol=0, atol=1e-12 * np.abs(W).max())
+
+
+def test_virial_shear_components_without_a_box(box27):
+    """Off-diagonal strains of an open (non-periodic) cluster, all terms."""
+    s = copy.deepcopy(box27)
+    s.use_bounds = False
+    st = Settings(use_ewald=False, cutoff=100.0, poleps=1e-11)
+    W = oracle.forward(s, st, flags=abi.DO_ENERGY | abi.DO_VIRIAL, raw_virial=True).vir
+    h = 1e-5
+    for (a, b) in ((0, 1), (0, 2), (1, 2), (2, 0)):
+        p = oracle.forward(_strained(s, a, b, h), st, flags=abi.DO_ENERGY)
+        m = oracle.forward(_strained(s, a, b, -h), st, flags=abi.DO_ENERGY)
+        assert abs(W[a, b] - (p.em + p.ep - m.em - m.ep) / (2 * h)) < 1e-8 * np.abs(W).max()

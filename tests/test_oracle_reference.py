@@ -41,14 +41,19 @@ def test_waterbox30_orthogonal_golden():
 
 
 def test_synthetic_box_matches_reference_run():
-    """216-water seeded box: oracle = compiled reference (em, nem, dem, rpole)."""
+    """216-water seeded box: oracle = compiled reference (em, nem, dem, virial,
+    rpole).  The virial is the reference's CalcMode::Virial result: pair terms
+    (include/md/pairMpole.h:166-173) plus the frame atoms' torque share
+    (src/md/torque.cpp:360-395)."""
     d = golden("ref_water216.json")
     s = systems.water_box(216, 18.643, seed=0)
     s.xyz = np.stack([d["x"], d["y"], d["z"]], 1)   # the coordinates the reference read
-    r = oracle.forward(s, nonewald(d["mpolecut"]), flags=abi.DO_ENERGY | abi.DO_GRADIENT | abi.DO_ANALYSIS)
+    r = oracle.forward(s, nonewald(d["mpolecut"]),
+                       flags=abi.DO_ENERGY | abi.DO_GRADIENT | abi.DO_ANALYSIS | abi.DO_VIRIAL)
     assert r.nem == d["nem"]
     assert abs(r.em - d["em"]) < 1e-9 * abs(d["em"])
     np.testing.assert_allclose(r.dem.reshape(-1), d["dem"], atol=1e-9, rtol=0)
+    np.testing.assert_allclose(r.vir.reshape(-1), d["vir"], atol=1e-8, rtol=0)
     np.testing.assert_allclose(r.rpole.reshape(-1)[: len(d["rpole"])], d["rpole"], atol=1e-13, rtol=0)
 
 

@@ -46,7 +46,7 @@
 extern "C" {
 #endif
 
-#define AMG_ABI_VERSION 2
+#define AMG_ABI_VERSION 3
 
 /* status codes */
 #define AMG_OK               0
@@ -70,6 +70,14 @@ extern "C" {
 #define AMG_PREC_FP64   0  /* every kernel in double precision */
 #define AMG_PREC_MIXED  1  /* FP32 pair/grid work; FP64 PCG dots, norms,
                               accumulators and one FP64 correction sweep */
+
+/* periodic cell shapes (boxes.h): the lattice follows from the box angles
+ * (orthogonal, monoclinic with only beta != 90, else triclinic) unless the
+ * cell is a truncated octahedron or a rhombic dodecahedron (boxes.h
+ * octahedron / dodecadron, whose box angles are all 90) */
+#define AMG_CELL_FROM_ANGLES   0
+#define AMG_CELL_OCTAHEDRON    1
+#define AMG_CELL_DODECAHEDRON  2
 
 /* polarization models (polpot.h poltyp) */
 #define AMG_POL_NONE    0
@@ -127,6 +135,11 @@ typedef struct amg_params {
                                         usolvcut (Thole-damped, u-scaled, no Ewald);
                                         0 = diagonal (alpha) */
     double usolvcut;                 /* limits.h usolvcut (Angstrom), at most cutoff */
+    /* Appended in ABI version 3 (zero keeps the version-2 behaviour): */
+    int32_t cell_shape;              /* AMG_CELL_*; a cell other than orthogonal
+                                        is supported without Ewald (the reference's
+                                        multipole mode) and returns UNSUPPORTED
+                                        with it */
 } amg_params;
 
 typedef struct amg_results {
@@ -135,7 +148,7 @@ typedef struct amg_results {
     double einter;      /* intermolecular part of em+ep (AMG_DO_ANALYSIS) */
     int64_t nem;        /* multipole pairs with nonzero energy (AMG_DO_ANALYSIS) */
     int64_t nep;        /* polarization sites with nonzero energy (AMG_DO_ANALYSIS) */
-    double vir[9];      /* added to with AMG_DO_VIRIAL (real-space part only) */
+    double vir[9];      /* added to with AMG_DO_VIRIAL: dE/d(strain), symmetric (virial.h vir) */
     double* dem;        /* [n*3] gradient of em, ADDED to; may be NULL */
     double* dep;        /* [n*3] gradient of ep, ADDED to; may be NULL */
     double* aem;        /* [n] per-atom em (AMG_DO_ANALYSIS), overwritten; may be NULL */
@@ -174,7 +187,9 @@ int amg_create(const amg_params* params, amg_ctx** out);
 
 /* Sets coordinates [n*3] (Angstrom) and the box: a,b,c (Angstrom) and
  * alpha,beta,gamma (degrees) as boxes.h xbox,ybox,zbox,alphaA,betaA,gammaA.
- * Only orthogonal boxes are supported with use_bounds (else UNSUPPORTED). */
+ * With use_bounds, the minimum image of the cell shape (params cell_shape and
+ * the angles) is the reference's image() (src/md/image.cpp:37-124).  Ewald
+ * needs an orthogonal box (else UNSUPPORTED). */
 int amg_set_coords(amg_ctx* ctx, const double* xyz, const double box[6]);
 
 /* Evaluates em and ep (and their gradients, analysis data, dipoles) for the
@@ -208,6 +223,12 @@ int amg_bench(amg_ctx* ctx, int32_t flags, int32_t steps, int64_t flush_bytes, d
  * amg_forward with mutual polarization. */
 int amg_time_tu_kernel(amg_ctx* ctx, int32_t reps, int64_t flush_bytes, double* ms_avg, double* bytes_per_launch,
                        int64_t* directed_pairs);
+
+/* The two parts of the last amg_forward's virial (AMG_DO_VIRIAL), as added
+ * to amg_results.vir: the em terms and the ep terms (the reference keeps one
+ * vir array and adds each term's share from its own routine, empole / epolar,
+ * virial.h).  Either pointer may be NULL. */
+int amg_last_virial(amg_ctx* ctx, double vir_em[9], double vir_ep[9]);
 
 /* Kernel launches of the last amg_forward, whether it ran as one captured
  * CUDA graph, and the lanes per site of the pair kernels. */

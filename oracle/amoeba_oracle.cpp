@@ -101,6 +101,10 @@ struct System {
     std::unordered_map<uint64_t, Scales> scaled;
     bool ewald = false, bounds = false;
     double L[3] = {0, 0, 0};
+    // cell shape (src/md/lattice.cpp:60-110): 0 orthogonal, 1 monoclinic,
+    // 2 triclinic, 3 truncated octahedron, 4 rhombic dodecahedron
+    int shape = 0;
+    double bsin = 1, bcos = 0, gsin = 1, gcos = 0, bterm = 0, gterm = 1;
     double alpha = 0, cut = 0, f = 0;
     int K[3] = {0, 0, 0}, order = 5;
     int poltyp = AMG_POL_NONE;
@@ -121,13 +125,51 @@ inline Scales pair_scales(const System& s, int i, int k) {
     return it == s.scaled.end() ? Scales{} : it->second;
 }
 
-// minimum image for an orthogonal box (src/md/image.cpp:41-53 restated)
+// minimum image, restating the reference's image() for the five cell shapes
+// (src/md/image.cpp:37-124): wrap along the cell axes in scaled fractional
+// coordinates (monoclinic, triclinic), and remove the corner images of the
+// truncated octahedron and the rhombic dodecahedron
+inline double wrap(double x, double L) { return x - L * std::nearbyint(x / L); }
+
 inline V3 min_image(const System& s, V3 d) {
     if (!s.bounds) return d;
-    d.x -= s.L[0] * std::nearbyint(d.x / s.L[0]);
-    d.y -= s.L[1] * std::nearbyint(d.y / s.L[1]);
-    d.z -= s.L[2] * std::nearbyint(d.z / s.L[2]);
-    return d;
+    const double* L = s.L;
+    switch (s.shape) {
+        case 1: {  // monoclinic: c in the xz plane
+            double z = d.z / s.bsin, x = d.x - z * s.bcos;
+            x = wrap(x, L[0]);
+            double y = wrap(d.y, L[1]);
+            z = wrap(z, L[2]);
+            return {x + z * s.bcos, y, z * s.bsin};
+        }
+        case 2: {  // triclinic: a along x, b in the xy plane
+            double z = d.z / s.gterm, y = (d.y - z * s.bterm) / s.gsin, x = d.x - y * s.gcos - z * s.bcos;
+            x = wrap(x, L[0]);
+            y = wrap(y, L[1]);
+            z = wrap(z, L[2]);
+            return {x + y * s.gcos + z * s.bcos, y * s.gsin + z * s.bterm, z * s.gterm};
+        }
+        case 3: {  // truncated octahedron in a cube of edge L
+            V3 r{wrap(d.x, L[0]), wrap(d.y, L[1]), wrap(d.z, L[2])};
+            if (std::fabs(r.x) + std::fabs(r.y) + std::fabs(r.z) > 0.75 * L[0]) {
+                r.x -= std::copysign(0.5 * L[0], r.x);
+                r.y -= std::copysign(0.5 * L[1], r.y);
+                r.z -= std::copysign(0.5 * L[2], r.z);
+            }
+            return r;
+        }
+        case 4: {  // rhombic dodecahedron, zbox = sqrt(2) xbox
+            const double r2 = std::sqrt(2.0);
+            V3 r{wrap(d.x, L[0]), wrap(d.y, L[1]), d.z - r2 * L[2] * std::round(d.z / (L[2] * r2))};
+            double corr = 0.5 * L[0] * (int)(std::fabs(r.x / L[0]) + std::fabs(r.y / L[1]) + std::fabs(r2 * r.z / L[2]));
+            r.x -= std::copysign(corr, r.x);
+            r.y -= std::copysign(corr, r.y);
+            r.z -= std::copysign(corr, r.z) * r2;
+            return r;
+        }
+        default:
+            return {wrap(d.x, L[0]), wrap(d.y, L[1]), wrap(d.z, L[2])};
+    }
 }
 
 // ---------------------------------------------------------------- frames
@@ -498,7 +540,7 @@ struct Pair { int i, k; V3 r; double rr; };
 std::vector<Pair> build_pairs(const System& s) {
     std::vector<Pair> out;
     const double c2 = s.cut * s.cut;
-    if (!s.bounds || s.n < 200) {
+    if (!s.bounds || s.n < 200 || s.shape != 0) {
         for (int i = 0; i < s.n; i++)
             for (int k = i + 1; k < s.n; k++) {
                 V3 r = min_image(s, s.x[k] - s.x[i]);
@@ -1298,10 +1340,32 @@ int orc_forward(const amg_params* P, const double* xyz, const double box[6], int
     s.ewald = P->use_ewald;
     s.bounds = P->use_bounds;
     if (s.bounds) {
-        if (!box || box[3] != 90.0 || box[4] != 90.0 || box[5] != 90.0) return AMG_ERR_UNSUPPORTED;
+        if (!box) return AMG_ERR_BAD_ARG;
         for (int a = 0; a < 3; a++) s.L[a] = box[a];
+        const bool right = box[3] == 90.0 && box[4] == 90.0 && box[5] == 90.0;
+        if (P->cell_shape == AMG_CELL_OCTAHEDRON || P->cell_shape == AMG_CELL_DODECAHEDRON) {
+            if (!right) return AMG_ERR_BAD_ARG;
+            s.shape = P->cell_shape == AMG_CELL_OCTAHEDRON ? 3 : 4;
+        } else if (!right) {
+            // lattice terms of src/md/lattice.cpp:80-110
+            const double rad = 180.0 / kPi;
+            const double ca = std::cos(box[3] / rad);
+            s.bsin = std::sin(box[4] / rad);
+            s.bcos = std::cos(box[4] / rad);
+            if (box[3] == 90.0 && box[5] == 90.0) {
+                s.shape = 1;
+                s.gterm = s.bsin;
+            } else {
+                s.shape = 2;
+                s.gsin = std::sin(box[5] / rad);
+                s.gcos = std::cos(box[5] / rad);
+                s.bterm = (ca - s.bcos * s.gcos) / s.gsin;
+                s.gterm = std::sqrt(s.bsin * s.bsin - s.bterm * s.bterm);
+            }
+        }
     }
     if (s.ewald && !s.bounds) return AMG_ERR_BAD_ARG;
+    if (s.ewald && s.shape != 0) return AMG_ERR_UNSUPPORTED;
     s.alpha = (opt && opt->alpha > 0) ? opt->alpha : P->aewald;
     s.cut = P->cutoff;
     s.f = P->electric / P->dielec;

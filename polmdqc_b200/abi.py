@@ -25,6 +25,7 @@ STATUS = {0: "OK", 1: "BAD_ARG", 2: "UNSUPPORTED", 3: "NO_CONVERGE", 4: "NAN",
 FRAME_NONE, FRAME_ZTHENX, FRAME_ZONLY, FRAME_BISECTOR, FRAME_ZBISECT, FRAME_THREEFOLD = range(6)
 PREC_FP64, PREC_MIXED = 0, 1
 POL_NONE, POL_MUTUAL, POL_DIRECT = 0, 1, 2
+CELL_FROM_ANGLES, CELL_OCTAHEDRON, CELL_DODECAHEDRON = 0, 1, 2
 DO_ENERGY, DO_ANALYSIS, DO_GRADIENT, DO_VIRIAL, DO_DIPOLES = 1, 2, 4, 8, 16
 
 _dp = C.POINTER(C.c_double)
@@ -53,6 +54,7 @@ class amg_params(C.Structure):
         ("electric", C.c_double), ("dielec", C.c_double), ("debye", C.c_double),
         ("precision", C.c_int32), ("pcg_guess", C.c_int32), ("device", C.c_int32),
         ("pcg_prec", C.c_int32), ("usolvcut", C.c_double),
+        ("cell_shape", C.c_int32),
     ]
 
 
@@ -116,13 +118,14 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.amg_bench.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int64, _dp, C.POINTER(C.c_int64)]
     lib.amg_time_tu_kernel.argtypes = [C.c_void_p, C.c_int32, C.c_int64, _dp, _dp, C.POINTER(C.c_int64)]
     lib.amg_last_stats.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+    lib.amg_last_virial.argtypes = [C.c_void_p, _dp, _dp]
     lib.amg_last_error.argtypes = [C.c_void_p]
     lib.amg_last_error.restype = C.c_char_p
     lib.amg_abi_version.argtypes = []
     lib.amg_destroy.argtypes = [C.c_void_p]
     lib.amg_destroy.restype = None
     for name in ("amg_create", "amg_set_coords", "amg_forward", "amg_backward", "amg_last_timing",
-                 "amg_abi_version", "amg_bench", "amg_last_stats", "amg_time_tu_kernel"):
+                 "amg_abi_version", "amg_bench", "amg_last_stats", "amg_time_tu_kernel", "amg_last_virial"):
         getattr(lib, name).restype = C.c_int
     _lib = lib
     return lib

@@ -30,9 +30,15 @@ using namespace amg;
 
 namespace {
 
-constexpr int kOrder = 5;
-constexpr int kGatherLanes = 8;  // lanes per site in the PME derivative gathers  // B-spline order compiled in (pme.h bseorder default)
+constexpr int kOrder = 5;        // B-spline order compiled in (pme.h bseorder default)
+constexpr int kGatherLanes = 8;  // lanes per site in the PME derivative gathers
 constexpr int kThreads = 128;
+// FP64 accumulators (eacc): em real 0, einter 1, em reciprocal 2, net charge
+// 3, ep 4; the virial's six sums (xx yy zz xy xz yz) of em from kVir and of
+// ep from kVirP
+constexpr int kVir = 8;
+constexpr int kVirP = 14;
+constexpr int kEacc = 20;
 
 inline unsigned nblk(size_t n, int t = kThreads) { return (unsigned)((n + t - 1) / t); }
 
@@ -111,6 +117,7 @@ struct amg_ctx {
     int K[3] = {0, 0, 0}, order = kOrder;
     std::string err;
     double box[6] = {0, 0, 0, 90, 90, 90};
+    int cell_shape = AMG_CELL_FROM_ANGLES;  // amg_params cell_shape
     Box bx{};
     bool have_coords = false;
     int nsp = 0;
@@ -143,7 +150,10 @@ struct amg_ctx {
     double *Ed = nullptr, *Ep = nullptr, *ud = nullptr, *up = nullptr, *rd = nullptr, *rp = nullptr, *zd = nullptr,
            *zp = nullptr, *pd = nullptr, *pp = nullptr, *Apd = nullptr, *App = nullptr, *Fd = nullptr, *Fp = nullptr,
            *resd = nullptr;
-    double *scal = nullptr, *eacc = nullptr;
+    double *scal = nullptr, *eacc = nullptr;  // eacc: [kEacc]
+    bool want_vir = false;                    // this evaluation adds the virial (eacc + kVir, + kVirP)
+    bool have_vir = false;
+    double vir_parts[2][9] = {};              // last evaluation's virial: em part, ep part
     unsigned long long* cnt = nullptr;
     double *grad_m = nullptr, *grad_p = nullptr, *trq_m = nullptr, *trq_p = nullptr, *aem = nullptr,
            *aep = nullptr;
@@ -174,7 +184,7 @@ struct amg_ctx {
     // gradients), filled by asynchronous copies behind one synchronisation
     struct Readback {
         int over, iters;
-        double e[8];
+        double e[kEacc];
         unsigned long long c[4];
         double hs[NSCAL];
     };
@@ -433,10 +443,62 @@ void rotate_and_pack(amg_ctx* ctx, cudaStream_t s) {
 
 // Cell grid for the current box (periodic) or coordinate bounding box
 // (non-periodic), computed on the host when coordinates are set.
+// Cell shape and lattice terms of a periodic box (src/md/lattice.cpp:36-110
+// restated): truncated octahedron and rhombic dodecahedron by the context's
+// cell_shape (right angles required), else orthogonal / monoclinic (only beta
+// off 90) / triclinic by the angles.
+bool set_lattice(amg_ctx* ctx, const double box[6], Box& b) {
+    const bool right = box[3] == 90.0 && box[4] == 90.0 && box[5] == 90.0;
+    b.shape = 0;
+    b.bsin = 1; b.bcos = 0; b.gsin = 1; b.gcos = 0; b.bterm = 0; b.gterm = 1;
+    if (ctx->cell_shape != AMG_CELL_FROM_ANGLES) {
+        if (!right) {
+            ctx->err = "octahedron and dodecahedron cells take right angles";
+            return false;
+        }
+        b.shape = ctx->cell_shape == AMG_CELL_OCTAHEDRON ? 3 : 4;
+        return true;
+    }
+    if (right) return true;
+    const double rad = 180.0 / kPi;
+    b.bsin = std::sin(box[4] / rad);
+    b.bcos = std::cos(box[4] / rad);
+    if (box[3] == 90.0 && box[5] == 90.0) {
+        b.shape = 1;
+        b.gterm = b.bsin;
+        return true;
+    }
+    b.shape = 2;
+    b.gsin = std::sin(box[5] / rad);
+    b.gcos = std::cos(box[5] / rad);
+    b.bterm = (std::cos(box[3] / rad) - b.bcos * b.gcos) / b.gsin;
+    const double g2 = b.bsin * b.bsin - b.bterm * b.bterm;
+    if (!(g2 > 0)) {
+        ctx->err = "box angles do not form a cell";
+        return false;
+    }
+    b.gterm = std::sqrt(g2);
+    return true;
+}
+
+// Cell grid of the neighbour-list build.  A non-orthogonal cell is one cell
+// with every atom a candidate of every other (the minimum image decides);
+// the orthogonal box and open systems get cells of at least the cutoff.
 void cell_grid(amg_ctx* ctx, const double* hxyz) {
     CellGrid& cg = ctx->cg;
     cg = CellGrid{};
     cg.periodic = ctx->bounds;
+    if (ctx->bounds && ctx->bx.shape != 0) {
+        const Box& b = ctx->bx;
+        double vol = ctx->box[0] * ctx->box[1] * ctx->box[2];
+        vol *= b.shape == 1 ? b.bsin : b.shape == 2 ? b.gsin * b.gterm : 0.5;
+        for (int a = 0; a < 3; a++) {
+            cg.nc[a] = 1;
+            cg.size[a] = ctx->box[a];
+        }
+        ctx->cell_volume = vol;
+        return;
+    }
     double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
     if (!ctx->bounds) {
         for (int a = 0; a < 3; a++) { lo[a] = 1e300; hi[a] = -1e300; }
@@ -588,9 +650,17 @@ void pme_stencils(amg_ctx* ctx, cudaStream_t s) {
     KCHECK();
 }
 
-// reciprocal potential derivatives of the permanent multipoles -> phiM [n][20]
+// k-space constants of the reciprocal virial: inverse box edges, pi^2/alpha^2
+inline double3 inv_edges(const amg_ctx* ctx) {
+    return make_double3(1.0 / ctx->box[0], 1.0 / ctx->box[1], 1.0 / ctx->box[2]);
+}
+inline double kvir_c2(const amg_ctx* ctx) { return kPi * kPi / (ctx->aewald * ctx->aewald); }
+
+// reciprocal potential derivatives of the permanent multipoles -> phiM [n][20];
+// with `vir`, also the k-space part of the permanent virial (six sums) and a
+// copy of the grid's transform (second half of cgrid) for the polarization's
 template <class R>
-void pme_mpole(amg_ctx* ctx, cudaStream_t s) {
+void pme_mpole(amg_ctx* ctx, cudaStream_t s, double* vir = nullptr) {
     Pme<R>& pm = pme_of<R>(ctx);
     int3 K = make_int3(ctx->K[0], ctx->K[1], ctx->K[2]);
     double sc[3] = {ctx->K[0] / ctx->box[0], ctx->K[1] / ctx->box[1], ctx->K[2] / ctx->box[2]};
@@ -600,6 +670,13 @@ void pme_mpole(amg_ctx* ctx, cudaStream_t s) {
     CKFFT(cufftSetStream(pm.f1, s));
     CKFFT(cufftSetStream(pm.i1, s));
     CKFFT(CufftTypes<R>::fwd(pm.f1, pm.grid, pm.cgrid));
+    if (vir) {
+        using C = typename Cplx<R>::type;
+        k_kvir_mpole<R><<<(unsigned)ctx->num_sms * 2, 256, 0, s>>>(pm.Gc, K, inv_edges(ctx), kvir_c2(ctx), ctx->f,
+                                                                   pm.infl, (const C*)pm.cgrid,
+                                                                   (C*)pm.cgrid + pm.Gc, vir);
+        KCHECK();
+    }
     k_convolve<R><<<nblk(pm.Gc, 256), 256, 0, s>>>(pm.Gc, 1, pm.infl, (typename Cplx<R>::type*)pm.cgrid, pm.grid, pm.G);
     KCHECK();
     CKFFT(CufftTypes<R>::inv(pm.i1, pm.cgrid, pm.phig));
@@ -624,8 +701,11 @@ void spread_dipoles(amg_ctx* ctx, cudaStream_t s, const double* vd, const double
     KCHECK();
 }
 
+// `vir`: the k-space part of the polarization virial (six sums), from this
+// transform and the permanent one saved by pme_mpole
 template <class R>
-void pme_dipole_grids(amg_ctx* ctx, cudaStream_t s, const double* vd, const double* vp, bool spread = true) {
+void pme_dipole_grids(amg_ctx* ctx, cudaStream_t s, const double* vd, const double* vp, bool spread = true,
+                      double* vir = nullptr) {
     Pme<R>& pm = pme_of<R>(ctx);
     if (spread) {
         CK(cudaMemsetAsync(pm.zg, 0, sizeof(typename Cplx<R>::type) * pm.G, s));
@@ -633,6 +713,13 @@ void pme_dipole_grids(amg_ctx* ctx, cudaStream_t s, const double* vd, const doub
     }
     CKFFT(cufftSetStream(pm.zplan, s));
     CKFFT(CufftTypes<R>::cc(pm.zplan, pm.zg, CUFFT_FORWARD));
+    if (vir) {
+        using C = typename Cplx<R>::type;
+        k_kvir_polar<R><<<(unsigned)ctx->num_sms * 2, 256, 0, s>>>(
+            pm.G, make_int3(ctx->K[0], ctx->K[1], ctx->K[2]), inv_edges(ctx), kvir_c2(ctx), ctx->f,
+            ctx->poltyp == AMG_POL_MUTUAL, pm.Gfull, pm.zg, (const C*)pm.cgrid + pm.Gc, vir);
+        KCHECK();
+    }
     k_scale_grid<R><<<nblk(pm.G, 256), 256, 0, s>>>(pm.G, pm.Gfull, pm.zg, pm.zq);  // also clears zg
     KCHECK();
     CKFFT(CufftTypes<R>::cc(pm.zplan, pm.zq, CUFFT_INVERSE));
@@ -640,11 +727,12 @@ void pme_dipole_grids(amg_ctx* ctx, cudaStream_t s, const double* vd, const doub
 
 // reciprocal potentials of two dipole sets -> phi [2][n][NC]
 template <class R, int NC>
-void pme_dipoles(amg_ctx* ctx, cudaStream_t s, const double* vd, const double* vp, double* phi) {
+void pme_dipoles(amg_ctx* ctx, cudaStream_t s, const double* vd, const double* vp, double* phi,
+                 double* vir = nullptr) {
     Pme<R>& pm = pme_of<R>(ctx);
     int3 K = make_int3(ctx->K[0], ctx->K[1], ctx->K[2]);
     double sc[3] = {ctx->K[0] / ctx->box[0], ctx->K[1] / ctx->box[1], ctx->K[2] / ctx->box[2]};
-    pme_dipole_grids<R>(ctx, s, vd, vp);
+    pme_dipole_grids<R>(ctx, s, vd, vp, true, vir);
     k_gather<R, kOrder, NC, kGatherLanes, 2><<<nblk((size_t)ctx->n * kGatherLanes), kThreads, 0, s>>>(
         ctx->n, pm.zq, pm.theta, pm.k0, K, sc[0], sc[1], sc[2], phi);
     KCHECK();
@@ -901,7 +989,7 @@ void enqueue_front(amg_ctx* ctx, cudaStream_t s) {
     CK(cudaEventRecord(ctx->ev[0], s));
     rotate_and_pack<R>(ctx, s);
     if (mixed && iterative(ctx)) rotate_and_pack<double>(ctx, s);
-    k_zero<double><<<1, 32, 0, s>>>(ctx->eacc, 8);
+    k_zero<double><<<1, 32, 0, s>>>(ctx->eacc, kEacc);
     KCHECK();
     k_zero<unsigned long long><<<1, 32, 0, s>>>(ctx->cnt, 4);
     KCHECK();
@@ -953,7 +1041,7 @@ void enqueue_front(amg_ctx* ctx, cudaStream_t s) {
             KCHECK();
         }
     }
-    if (ctx->ewald) pme_mpole<R>(ctx, s);
+    if (ctx->ewald) pme_mpole<R>(ctx, s, ctx->want_vir ? ctx->eacc + kVir : nullptr);
     join_side(ctx, s);
     if (ctx->has_pol) {
         k_field_finish<<<nblk(n), kThreads, 0, s>>>(n, ctx->phiM, ctx->ewald, ctx->rp10, self_coef(ctx), ctx->pol, ctx->Ed,
@@ -995,26 +1083,23 @@ void enqueue_back(amg_ctx* ctx, cudaStream_t s, int flags) {
     // so they run after the join.
     cudaStream_t r = fork_side(ctx, s);
     const int* mol = ctx->mol;
+    double* vir = ctx->want_vir ? ctx->eacc + kVir : nullptr;    // em terms
+    double* virp = ctx->want_vir ? ctx->eacc + kVirP : nullptr;  // ep terms
+    // Analysis and Virial outputs come from the EXTRA pair kernels
+    const bool extra = analysis || vir;
     LPA_DISPATCH(ctx->lpa, {
         const size_t nb = nblk((size_t)n * L);
+        auto launch = [&](auto kern) {
+            kern<<<nb, kThreads, 0, r>>>(n, ctx->sids, A.at, ctx->bx, aew, ctx->nbr, ctx->cap, ctx->nnb, ctx->f,
+                                         ctx->grad_m, ctx->trq_m, ctx->eacc, analysis ? ctx->aem : nullptr,
+                                         analysis ? mol : nullptr, analysis ? ctx->cnt : nullptr, vir);
+        };
         if (ctx->ewald) {
-            if (analysis)
-                k_mpole_pair<R, true, true, L><<<nb, kThreads, 0, r>>>(n, ctx->sids, A.at, ctx->bx, aew, ctx->nbr, ctx->cap, ctx->nnb,
-                                                                       ctx->f, ctx->grad_m, ctx->trq_m, ctx->eacc,
-                                                                       ctx->aem, mol, ctx->cnt);
-            else
-                k_mpole_pair<R, true, false, L><<<nb, kThreads, 0, r>>>(n, ctx->sids, A.at, ctx->bx, aew, ctx->nbr, ctx->cap,
-                                                                        ctx->nnb, ctx->f, ctx->grad_m, ctx->trq_m,
-                                                                        ctx->eacc, nullptr, nullptr, nullptr);
+            if (extra) launch(k_mpole_pair<R, true, true, L>);
+            else launch(k_mpole_pair<R, true, false, L>);
         } else {
-            if (analysis)
-                k_mpole_pair<R, false, true, L><<<nb, kThreads, 0, r>>>(n, ctx->sids, A.at, ctx->bx, aew, ctx->nbr, ctx->cap,
-                                                                        ctx->nnb, ctx->f, ctx->grad_m, ctx->trq_m,
-                                                                        ctx->eacc, ctx->aem, mol, ctx->cnt);
-            else
-                k_mpole_pair<R, false, false, L><<<nb, kThreads, 0, r>>>(n, ctx->sids, A.at, ctx->bx, aew, ctx->nbr, ctx->cap,
-                                                                         ctx->nnb, ctx->f, ctx->grad_m, ctx->trq_m,
-                                                                         ctx->eacc, nullptr, nullptr, nullptr);
+            if (extra) launch(k_mpole_pair<R, false, true, L>);
+            else launch(k_mpole_pair<R, false, false, L>);
         }
     });
     KCHECK();
@@ -1022,25 +1107,28 @@ void enqueue_back(amg_ctx* ctx, cudaStream_t s, int flags) {
         k_scaled_mpole<<<nblk(ctx->nsp), kThreads, 0, r>>>(ctx->nsp, ctx->sp, ctx->xyz, ctx->rp10, ctx->bx, cut2,
                                                           ewald_alpha(ctx), ctx->f, ctx->grad_m, ctx->trq_m, ctx->eacc,
                                                           analysis ? ctx->aem : nullptr, analysis ? mol : nullptr,
-                                                          analysis ? ctx->cnt : nullptr);
+                                                          analysis ? ctx->cnt : nullptr, vir);
         KCHECK();
     }
     if (polgrad) {
-        LPA_DISPATCH(ctx->lpa, {
-            if (ctx->ewald)
-                k_polar_pair<R, true, L><<<nblk((size_t)n * L), kThreads, 0, r>>>(n, ctx->sids, A.at, A.u4, ctx->bx, aew, ctx->nbr,
-                                                                                  ctx->cap, ctx->nnb, mutual, ctx->f,
-                                                                                  ctx->grad_p, ctx->trq_p);
-            else
-                k_polar_pair<R, false, L><<<nblk((size_t)n * L), kThreads, 0, r>>>(n, ctx->sids, A.at, A.u4, ctx->bx, aew, ctx->nbr,
-                                                                                   ctx->cap, ctx->nnb, mutual, ctx->f,
-                                                                                   ctx->grad_p, ctx->trq_p);
-        });
+        auto launch = [&](auto kern, int lanes) {
+            kern<<<nblk((size_t)n * lanes), kThreads, 0, r>>>(n, ctx->sids, A.at, A.u4, ctx->bx, aew, ctx->nbr, ctx->cap,
+                                                              ctx->nnb, mutual, ctx->f, ctx->grad_p, ctx->trq_p, virp);
+        };
+        if (vir) {  // one lane count for the virial variants
+            if (ctx->ewald) launch(k_polar_pair<R, true, 8, true>, 8);
+            else launch(k_polar_pair<R, false, 8, true>, 8);
+        } else {
+            LPA_DISPATCH(ctx->lpa, {
+                if (ctx->ewald) launch(k_polar_pair<R, true, L, false>, L);
+                else launch(k_polar_pair<R, false, L, false>, L);
+            });
+        }
         KCHECK();
         if (ctx->nsp) {
             k_scaled_polar<<<nblk(ctx->nsp), kThreads, 0, r>>>(ctx->nsp, ctx->sp, ctx->xyz, ctx->rp10, ctx->pdamp,
                                                               ctx->thole, ctx->bx, cut2, ewald_alpha(ctx), ctx->ud,
-                                                              ctx->up, mutual, ctx->f, ctx->grad_p, ctx->trq_p);
+                                                              ctx->up, mutual, ctx->f, ctx->grad_p, ctx->trq_p, virp);
             KCHECK();
         }
     }
@@ -1049,27 +1137,27 @@ void enqueue_back(amg_ctx* ctx, cudaStream_t s, int flags) {
                                                     analysis ? ctx->aep : nullptr, ctx->cnt + 1);
         KCHECK();
     }
-    if (polgrad && ctx->ewald) pme_dipoles<R, 20>(ctx, s, ctx->ud, ctx->up, ctx->phiU);
+    if (polgrad && ctx->ewald) pme_dipoles<R, 20>(ctx, s, ctx->ud, ctx->up, ctx->phiU, virp);
     join_side(ctx, s);
     if (ctx->ewald) {
         k_recip_mpole<<<nblk(n), kThreads, 0, s>>>(n, ctx->rp10, ctx->phiM, ctx->f, ctx->aewald, ctx->grad_m, ctx->trq_m,
-                                                   ctx->eacc + 2, analysis ? ctx->aem : nullptr, ctx->eacc + 3);
+                                                   ctx->eacc + 2, analysis ? ctx->aem : nullptr, ctx->eacc + 3, vir);
         KCHECK();
     }
     if (polgrad) {
         if (ctx->ewald) {
             k_recip_polar<<<nblk(n), kThreads, 0, s>>>(n, ctx->rp10, ctx->phiM, ctx->phiU, ctx->phiU + 20 * (size_t)n,
                                                        ctx->ud, ctx->up, mutual, self_coef(ctx), ctx->f, ctx->grad_p,
-                                                       ctx->trq_p);
+                                                       ctx->trq_p, virp);
             KCHECK();
         }
         k_torque<<<nblk(n), kThreads, 0, s>>>(n, ctx->xyz, ctx->zax, ctx->xax, ctx->yax, ctx->axe, ctx->trq_p,
-                                              ctx->grad_p);
+                                              ctx->grad_p, virp);
         KCHECK();
     }
     if (grad) {
         k_torque<<<nblk(n), kThreads, 0, s>>>(n, ctx->xyz, ctx->zax, ctx->xax, ctx->yax, ctx->axe, ctx->trq_m,
-                                              ctx->grad_m);
+                                              ctx->grad_m, vir);
         KCHECK();
     }
     CK(cudaEventRecord(ctx->ev[4], s));
@@ -1176,6 +1264,7 @@ int forward_impl(amg_ctx* ctx, int flags, amg_results* res) {
     const int n = ctx->n;
     const bool grad = flags & AMG_DO_GRADIENT;
     const bool analysis = flags & AMG_DO_ANALYSIS;
+    ctx->want_vir = (flags & AMG_DO_VIRIAL) != 0;
     cudaStream_t st = ctx->st;
     if (!ctx->rb) {
         CK(cudaMallocHost((void**)&ctx->rb, sizeof(amg_ctx::Readback)));
@@ -1240,11 +1329,24 @@ int forward_impl(amg_ctx* ctx, int flags, amg_results* res) {
         if (!dst) return;
         CK(cudaMemcpyAsync(dst, src, sizeof(double) * cnt, cudaMemcpyDeviceToHost, st));
     };
-    double em = e[0] + e[2];
+    double em = e[0] + e[2], echg = 0;
     if (ctx->ewald) {
         double V = ctx->box[0] * ctx->box[1] * ctx->box[2];
         double qt = e[3];
-        em += -ctx->f * kPi * qt * qt / (2 * V * ctx->aewald * ctx->aewald);
+        echg = -ctx->f * kPi * qt * qt / (2 * V * ctx->aewald * ctx->aewald);
+        em += echg;
+    }
+    ctx->have_vir = ctx->want_vir;
+    if (ctx->want_vir) {  // six sums -> symmetric 3x3, added; the net-charge term goes as 1/V
+        for (int part = 0; part < 2; part++) {
+            const double* v = e + (part ? kVirP : kVir);
+            const double c = part ? 0.0 : echg;
+            const double w[9] = {v[0] - c, v[3], v[4], v[3], v[1] - c, v[5], v[4], v[5], v[2] - c};
+            for (int k = 0; k < 9; k++) {
+                ctx->vir_parts[part][k] = w[k];
+                res->vir[k] += w[k];
+            }
+        }
     }
     res->em = em;
     res->ep = ctx->has_pol ? e[4] : 0.0;
@@ -1372,6 +1474,7 @@ int create_impl(amg_ctx* ctx, const amg_params* P) {
     ctx->poltyp = ctx->has_pol ? P->poltyp : AMG_POL_NONE;
     ctx->sparse_prec = ctx->has_pol && ctx->poltyp == AMG_POL_MUTUAL && P->pcg_prec != 0;
     ctx->usolvcut = std::min(P->usolvcut, P->cutoff);
+    ctx->cell_shape = P->cell_shape;
     for (int a = 0; a < 3; a++) ctx->K[a] = P->nfft[a];
     CK(cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&ctx->st2, cudaStreamNonBlocking));
@@ -1448,7 +1551,7 @@ int create_impl(amg_ctx* ctx, const amg_params* P) {
     dalloc(ctx, ctx->aem, n);
     dalloc(ctx, ctx->aep, n);
     dalloc(ctx, ctx->scal, 16);
-    dalloc(ctx, ctx->eacc, 8);
+    dalloc(ctx, ctx->eacc, kEacc);
     dalloc(ctx, ctx->cnt, 4);
     dalloc(ctx, ctx->phiM, 20 * (size_t)n);
     CK(cudaMemset(ctx->phiM, 0, sizeof(double) * 20 * n));
@@ -1490,6 +1593,10 @@ int validate(const amg_params* P, std::string& why) {
     }
     if (P->pcg_prec && !(P->usolvcut > 0)) {
         why = "the sparse preconditioner needs usolvcut > 0";
+        return AMG_ERR_BAD_ARG;
+    }
+    if (P->cell_shape < AMG_CELL_FROM_ANGLES || P->cell_shape > AMG_CELL_DODECAHEDRON) {
+        why = "unknown cell shape";
         return AMG_ERR_BAD_ARG;
     }
     for (int i = 0; i < P->n; i++) {
@@ -1641,7 +1748,7 @@ int backward_impl(amg_ctx* ctx, const amg_cotangents* cot, amg_param_grads* gr) 
         CK(cudaStreamSynchronize(s));
         for (int i = 0; i < n; i++) qtot += r10[10 * (size_t)i];
     }
-    k_torque<<<nblk(n), kThreads, 0, s>>>(n, ctx->xyz, ctx->zax, ctx->xax, ctx->yax, ctx->axe, trq, grad);
+    k_torque<<<nblk(n), kThreads, 0, s>>>(n, ctx->xyz, ctx->zax, ctx->xax, ctx->yax, ctx->axe, trq, grad, nullptr);
     KCHECK();
     k_pole_grad_local<<<nblk(n), kThreads, 0, s>>>(n, ctx->xyz, ctx->pole13, ctx->zax, ctx->xax, ctx->yax, ctx->axe,
                                                    ctx->adj_pot, ctx->adj_dpole);
@@ -1709,10 +1816,14 @@ int amg_set_coords(amg_ctx* ctx, const double* xyz, const double box[6]) {
                 ctx->err = "periodic box lengths must be positive";
                 return AMG_ERR_BAD_ARG;
             }
-            if (box[3] != 90.0 || box[4] != 90.0 || box[5] != 90.0) {
-                ctx->err = "only orthogonal boxes are supported";
+            Box nb = ctx->bx;
+            if (!set_lattice(ctx, box, nb)) return AMG_ERR_BAD_ARG;
+            if (ctx->ewald && nb.shape != 0) {
+                ctx->err = "Ewald needs an orthogonal box";
                 return AMG_ERR_UNSUPPORTED;
             }
+            if (nb.shape != ctx->bx.shape) ctx->graph_dirty = true;
+            ctx->bx = nb;
             for (int a = 0; a < 3; a++)
                 if (ctx->cut > 0.5 * box[a] + 1e-12) {
                     ctx->err = "cutoff exceeds half the box (minimum image)";
@@ -1746,10 +1857,7 @@ int amg_forward(amg_ctx* ctx, int32_t flags, amg_results* res) {
         ctx->err = "amg_set_coords not called";
         return AMG_ERR_BAD_ARG;
     }
-    if (flags & AMG_DO_VIRIAL) {
-        ctx->err = "virial not implemented";
-        return AMG_ERR_UNSUPPORTED;
-    }
+    if (flags & AMG_DO_VIRIAL) flags |= AMG_DO_GRADIENT;  // the virial needs the torques' frame forces
     try {
         CK(cudaSetDevice(ctx->device));
         if (ctx->prec == AMG_PREC_MIXED) return forward_impl<float>(ctx, flags, res);
@@ -1780,6 +1888,7 @@ int amg_bench(amg_ctx* ctx, int32_t flags, int32_t steps, int64_t flush_bytes, d
         ctx->err = "amg_set_coords not called";
         return AMG_ERR_BAD_ARG;
     }
+    if (flags & AMG_DO_VIRIAL) flags |= AMG_DO_GRADIENT;  // as amg_forward
     amg_results res{};
     int rc = amg_forward(ctx, flags, &res);  // captures the graph and sizes the lists
     if (rc != AMG_OK) return rc;
@@ -1901,6 +2010,19 @@ int amg_last_stats(amg_ctx* ctx, int64_t* launches, int32_t* graphed, int32_t* l
     if (launches) *launches = ctx->klast;
     if (graphed) *graphed = ctx->graphed_last;
     if (lanes_per_site) *lanes_per_site = ctx->lpa;
+    return AMG_OK;
+}
+
+int amg_last_virial(amg_ctx* ctx, double vir_em[9], double vir_ep[9]) {
+    if (!ctx) return AMG_ERR_BAD_ARG;
+    if (!ctx->have_vir) {
+        ctx->err = "the last amg_forward did not compute the virial";
+        return AMG_ERR_BAD_ARG;
+    }
+    for (int k = 0; k < 9; k++) {
+        if (vir_em) vir_em[k] = ctx->vir_parts[0][k];
+        if (vir_ep) vir_ep[k] = ctx->vir_parts[1][k];
+    }
     return AMG_OK;
 }
 
@@ -2094,7 +2216,7 @@ extern "C" int amg_empole_direct_noalloc(int32_t n, const double* xyz, const dou
     k_noalloc_pairs<<<nb, kNoAllocThreads, 0, st>>>(n, xyz, rp10, L, box ? box[0] : 0.0, box ? box[1] : 0.0,
                                                     box ? box[2] : 0.0, cutoff * cutoff, f, trq, dem, partial);
     k_noalloc_energy<<<1, 256, 0, st>>>((int)nb, partial, em);
-    k_torque<<<(n + 127) / 128, 128, 0, st>>>(n, xyz, zaxis, xaxis, yaxis, polaxe, trq, dem);
+    k_torque<<<(n + 127) / 128, 128, 0, st>>>(n, xyz, zaxis, xaxis, yaxis, polaxe, trq, dem, nullptr);
     if (cudaGetLastError() != cudaSuccess) return AMG_ERR_CUDA;
     if (cudaStreamSynchronize(st) != cudaSuccess) return AMG_ERR_CUDA;
     return AMG_OK;

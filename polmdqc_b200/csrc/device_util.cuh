@@ -74,6 +74,26 @@ __device__ __forceinline__ void block_sum_add_ll(long long v, unsigned long long
     __syncthreads();
 }
 
+// Virial (dE/d(strain), symmetrised) as six sums: xx yy zz xy xz yz.
+// v += s sym(g (x) r): the strain derivative of a term whose gradient with
+// respect to the separation r is g.
+__device__ __forceinline__ void vir_outer(double (&v)[6], double gx, double gy, double gz, double rx, double ry,
+                                          double rz, double s) {
+    v[0] += s * gx * rx;
+    v[1] += s * gy * ry;
+    v[2] += s * gz * rz;
+    v[3] += 0.5 * s * (gx * ry + gy * rx);
+    v[4] += 0.5 * s * (gx * rz + gz * rx);
+    v[5] += 0.5 * s * (gy * rz + gz * ry);
+}
+
+// block-wide sums of the six virial components into out[0..5]; every thread
+// of the block must call it
+__device__ __forceinline__ void block_vir_add(const double (&v)[6], double* out) {
+#pragma unroll
+    for (int c = 0; c < 6; c++) block_sum_add(v[c], out + c);
+}
+
 // minimum image in an orthogonal box (box <= 0 on an axis: no wrapping)
 template <class R>
 __device__ __forceinline__ R wrap1(R d, R L, R iL) {

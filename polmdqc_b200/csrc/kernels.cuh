@@ -23,6 +23,11 @@ struct AtomR {
 struct Box {
     double L[3];       // box lengths (0: no periodic wrapping on that axis)
     double iL[3];
+    // cell shape: 0 orthogonal, 1 monoclinic, 2 triclinic, 3 truncated
+    // octahedron, 4 rhombic dodecahedron; lattice terms of the reference's
+    // lattice (src/md/lattice.cpp:80-110)
+    int shape;
+    double bsin, bcos, gsin, gcos, bterm, gterm;
 };
 
 template <class R>
@@ -34,8 +39,57 @@ __device__ __forceinline__ Mpole<R> load_mpole(const AtomR<R>& A) {
     return M;
 }
 
+// Minimum image of the non-orthogonal cells, restating the reference's
+// image() (src/md/image.cpp:37-124): wrap along the cell axes in scaled
+// fractional coordinates (monoclinic, triclinic), or wrap in the enclosing
+// box and remove the corner images (truncated octahedron, rhombic
+// dodecahedron with zbox = sqrt(2) xbox).
 template <class R>
+__device__ __noinline__ V3<R> image_cell(V3<R> d, const Box bx) {
+    const R L0 = (R)bx.L[0], L1 = (R)bx.L[1], L2 = (R)bx.L[2];
+    const R i0 = (R)bx.iL[0], i1 = (R)bx.iL[1], i2 = (R)bx.iL[2];
+    if (bx.shape == 1) {
+        const R bs = (R)bx.bsin, bc = (R)bx.bcos;
+        R z = d.z / bs, x = d.x - z * bc;
+        x = wrap1<R>(x, L0, i0);
+        const R y = wrap1<R>(d.y, L1, i1);
+        z = wrap1<R>(z, L2, i2);
+        return v3<R>(x + z * bc, y, z * bs);
+    }
+    if (bx.shape == 2) {
+        const R gs = (R)bx.gsin, gc = (R)bx.gcos, bc = (R)bx.bcos, bt = (R)bx.bterm, gt = (R)bx.gterm;
+        R z = d.z / gt, y = (d.y - z * bt) / gs, x = d.x - y * gc - z * bc;
+        x = wrap1<R>(x, L0, i0);
+        y = wrap1<R>(y, L1, i1);
+        z = wrap1<R>(z, L2, i2);
+        return v3<R>(x + y * gc + z * bc, y * gs + z * bt, z * gt);
+    }
+    V3<R> r;
+    if (bx.shape == 3) {
+        r = v3<R>(wrap1<R>(d.x, L0, i0), wrap1<R>(d.y, L1, i1), wrap1<R>(d.z, L2, i2));
+        if (fabs(r.x) + fabs(r.y) + fabs(r.z) > R(0.75) * L0) {
+            r.x -= copysign(R(0.5) * L0, r.x);
+            r.y -= copysign(R(0.5) * L1, r.y);
+            r.z -= copysign(R(0.5) * L2, r.z);
+        }
+        return r;
+    }
+    // rhombic dodecahedron
+    const R r2 = (R)1.41421356237309504880;
+    r = v3<R>(wrap1<R>(d.x, L0, i0), wrap1<R>(d.y, L1, i1), d.z - r2 * L2 * round(d.z / (L2 * r2)));
+    const R corr = R(0.5) * L0 * (R)(int)(fabs(r.x * i0) + fabs(r.y * i1) + fabs(r2 * r.z * i2));
+    r.x -= copysign(corr, r.x);
+    r.y -= copysign(corr, r.y);
+    r.z -= copysign(corr, r.z) * r2;
+    return r;
+}
+
+// CELLS false: the box is orthogonal (or absent) by construction, as in
+// every Ewald kernel; true: any cell shape, the non-orthogonal ones through
+// image_cell.
+template <class R, bool CELLS = true>
 __device__ __forceinline__ V3<R> min_image(V3<R> d, const Box& bx) {
+    if (CELLS && bx.shape != 0) return image_cell<R>(d, bx);
     return v3<R>(wrap1<R>(d.x, (R)bx.L[0], (R)bx.iL[0]), wrap1<R>(d.y, (R)bx.L[1], (R)bx.iL[1]),
                  wrap1<R>(d.z, (R)bx.L[2], (R)bx.iL[2]));
 }

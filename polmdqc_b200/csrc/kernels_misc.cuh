@@ -304,13 +304,41 @@ __device__ __forceinline__ V3<double> site_torque(const double* m, const double*
     return t - 2.0 * axial_prod(Q, H);
 }
 
+// Multipole term of the reciprocal virial: at fixed fractional coordinates a
+// strain acts on the structure factor as if each source were deformed,
+// d -> (1 - eps) d, Q -> Q - eps Q - Q eps^T; with phi the derivative of the
+// energy with respect to the source, v += s sym(-(grad phi) (x) d - 2 H Q),
+// H = grad grad phi.  Q is skipped for a dipole-only source (m[4] unused).
+__device__ __forceinline__ void vir_source(double (&v)[6], const double* m, bool quad, const double* p, double s) {
+    vir_outer(v, p[1], p[2], p[3], m[1], m[2], m[3], -s);
+    if (!quad) return;
+    const double Q[3][3] = {{m[4], m[5], m[6]}, {m[5], m[7], m[8]}, {m[6], m[8], m[9]}};
+    const double H[3][3] = {{p[4], p[7], p[8]}, {p[7], p[5], p[9]}, {p[8], p[9], p[6]}};
+    double HQ[3][3];
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) HQ[a][b] = H[a][0] * Q[0][b] + H[a][1] * Q[1][b] + H[a][2] * Q[2][b];
+    v[0] -= 2 * s * HQ[0][0];
+    v[1] -= 2 * s * HQ[1][1];
+    v[2] -= 2 * s * HQ[2][2];
+    v[3] -= s * (HQ[0][1] + HQ[1][0]);
+    v[4] -= s * (HQ[0][2] + HQ[2][0]);
+    v[5] -= s * (HQ[1][2] + HQ[2][1]);
+}
+
+__device__ __forceinline__ void vir_dipole(double (&v)[6], V3<double> u, const double* p, double s) {
+    const double m[4] = {0, u.x, u.y, u.z};
+    vir_source(v, m, false, p, s);
+}
+
 // permanent reciprocal energy 1/2 M.phi, gradient, torque; self energy;
-// per-site energies on request
+// per-site energies on request; the multipole term of the reciprocal virial
+// into vir when set
 __global__ void k_recip_mpole(int n, const double* __restrict__ rp10, const double* __restrict__ phiM, double f,
                               double alpha, double* __restrict__ grad, double* __restrict__ trq,
-                              double* __restrict__ eacc, double* __restrict__ aem, double* __restrict__ qsum) {
+                              double* __restrict__ eacc, double* __restrict__ aem, double* __restrict__ qsum,
+                              double* __restrict__ vir) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    double e = 0, q = 0;
+    double e = 0, q = 0, w[6] = {0, 0, 0, 0, 0, 0};
     if (i < n) {
         const double* m = rp10 + 10 * i;
         const double* p = phiM + 20 * (size_t)i;
@@ -325,49 +353,80 @@ __global__ void k_recip_mpole(int n, const double* __restrict__ rp10, const doub
         grad[3 * i] += f * g.x; grad[3 * i + 1] += f * g.y; grad[3 * i + 2] += f * g.z;
         trq[3 * i] += f * t.x; trq[3 * i + 1] += f * t.y; trq[3 * i + 2] += f * t.z;
         if (aem) aem[i] += e;
+        if (vir) vir_source(w, m, true, p, f);
     }
     block_sum_add(e, eacc);
     block_sum_add(q, qsum);
+    if (vir) block_vir_add(w, vir);
 }
 
 // reciprocal + self part of the polarization gradient and torques:
 //   dG/dx_i = 1/2 [(up+ud)_i . grad grad phiM + M_i . grad(phi_p + phi_d)
 //                  + up_i . grad grad phi_d + ud_i . grad grad phi_p]
 //   torque  = torque(M_i, (phi_d + phi_p)/2) + (selfc/2) d_i x (ud + up)_i
+// and, into vir when set, the multipole terms of the reciprocal virial of
+//   G = 1/2 [U(up, M) + U(ud, M) + U(up, ud)].
 __global__ void k_recip_polar(int n, const double* __restrict__ rp10, const double* __restrict__ phiM,
                               const double* __restrict__ phid, const double* __restrict__ phip,
                               const double* __restrict__ ud, const double* __restrict__ up, int mutual,
-                              double selfc, double f, double* __restrict__ grad, double* __restrict__ trq) {
+                              double selfc, double f, double* __restrict__ grad, double* __restrict__ trq,
+                              double* __restrict__ vir) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const double* m = rp10 + 10 * i;
-    const double* pm = phiM + 20 * (size_t)i;
-    const double* pd = phid + 20 * (size_t)i;
-    const double* pp = phip + 20 * (size_t)i;
-    V3<double> udi = ld3(ud, i), upi = ld3(up, i);
-    double avg[20];
-    for (int j = 0; j < 20; j++) avg[j] = pd[j] + pp[j];
-    V3<double> g = dipole_gradient(udi + upi, pm) + site_gradient(m, avg);
-    if (mutual) g = g + dipole_gradient(upi, pd) + dipole_gradient(udi, pp);
-    g = (0.5 * f) * g;
-    for (int j = 0; j < 20; j++) avg[j] *= 0.5;
-    V3<double> t = site_torque(m, avg) + (0.5 * selfc) * cross(v3<double>(m[1], m[2], m[3]), udi + upi);
-    t = f * t;
-    grad[3 * i] += g.x; grad[3 * i + 1] += g.y; grad[3 * i + 2] += g.z;
-    trq[3 * i] += t.x; trq[3 * i + 1] += t.y; trq[3 * i + 2] += t.z;
+    double w[6] = {0, 0, 0, 0, 0, 0};
+    if (i < n) {
+        const double* m = rp10 + 10 * i;
+        const double* pm = phiM + 20 * (size_t)i;
+        const double* pd = phid + 20 * (size_t)i;
+        const double* pp = phip + 20 * (size_t)i;
+        V3<double> udi = ld3(ud, i), upi = ld3(up, i);
+        double avg[20];
+        for (int j = 0; j < 20; j++) avg[j] = pd[j] + pp[j];
+        V3<double> g = dipole_gradient(udi + upi, pm) + site_gradient(m, avg);
+        if (mutual) g = g + dipole_gradient(upi, pd) + dipole_gradient(udi, pp);
+        g = (0.5 * f) * g;
+        for (int j = 0; j < 20; j++) avg[j] *= 0.5;
+        V3<double> t = site_torque(m, avg) + (0.5 * selfc) * cross(v3<double>(m[1], m[2], m[3]), udi + upi);
+        t = f * t;
+        grad[3 * i] += g.x; grad[3 * i + 1] += g.y; grad[3 * i + 2] += g.z;
+        trq[3 * i] += t.x; trq[3 * i + 1] += t.y; trq[3 * i + 2] += t.z;
+        if (vir) {
+            const double h = 0.5 * f;
+            vir_dipole(w, upi + udi, pm, h);   // U(up, M) + U(ud, M): dipoles in phiM
+            vir_source(w, m, true, avg, f);    // ... and M in phi_p + phi_d (avg holds half the sum)
+            if (mutual) {                      // U(up, ud)
+                vir_dipole(w, upi, pd, h);
+                vir_dipole(w, udi, pp, h);
+            }
+        }
+    }
+    if (vir) block_vir_add(w, vir);
 }
 
 // ---------------------------------------------------------------- torque
 // Site torques -> gradients on the frame atoms, restating the reference's
 // torque (src/md/torque.cpp:42-397; Popelier & Stone 1994, Sagui et al.
 // 2004).  Gradients are accumulated with FP64 atomics (frame atoms are shared).
+// With vir set, the frame atoms' share of the virial: each frame atom's
+// gradient times its offset from the site (src/md/torque.cpp:360-395).
+__device__ __forceinline__ void torque_site(int i, const double* __restrict__ xyz, const int* __restrict__ zax,
+                                            const int* __restrict__ xax, const int* __restrict__ yax,
+                                            const int* __restrict__ axe, const double* __restrict__ trq,
+                                            double* __restrict__ grad, double (*vacc)[6]);
+
 __global__ void k_torque(int n, const double* __restrict__ xyz, const int* __restrict__ zax,
                          const int* __restrict__ xax, const int* __restrict__ yax, const int* __restrict__ axe,
-                         const double* __restrict__ trq, double* __restrict__ grad) {
+                         const double* __restrict__ trq, double* __restrict__ grad, double* __restrict__ vir) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    int ft = axe[i];
-    if (ft == AMG_FRAME_NONE) return;
+    double w[6] = {0, 0, 0, 0, 0, 0};
+    if (i < n && axe[i] != AMG_FRAME_NONE) torque_site(i, xyz, zax, xax, yax, axe, trq, grad, vir ? &w : nullptr);
+    if (vir) block_vir_add(w, vir);
+}
+
+__device__ __forceinline__ void torque_site(int i, const double* __restrict__ xyz, const int* __restrict__ zax,
+                                            const int* __restrict__ xax, const int* __restrict__ yax,
+                                            const int* __restrict__ axe, const double* __restrict__ trq,
+                                            double* __restrict__ grad, double (*vacc)[6]) {
+    const int ft = axe[i];
     using D = double;
     auto P = [&](int a) { return v3<D>(xyz[3 * a], xyz[3 * a + 1], xyz[3 * a + 2]); };
     auto unit = [](V3<D> v) { D s = 1.0 / sqrt(dot(v, v)); return s * v; };
@@ -396,6 +455,10 @@ __global__ void k_torque(int n, const double* __restrict__ xyz, const int* __res
         atomicAdd(grad + 3 * at, g.x);
         atomicAdd(grad + 3 * at + 1, g.y);
         atomicAdd(grad + 3 * at + 2, g.z);
+        if (vacc && at != ib) {
+            V3<D> o = P(at) - P(ib);
+            vir_outer(*vacc, g.x, g.y, g.z, o.x, o.y, o.z, 1.0);
+        }
     };
     if (ft == AMG_FRAME_ZONLY) {
         V3<D> du = (dpv / (us * uvsn)) * uv + (dpw / us) * uw;

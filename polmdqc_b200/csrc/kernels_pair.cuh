@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(128) k_perm_field(int n, const int* __restrict
         if (ok) {
             j = row[s];
             AtomR<R> Aj = at[j];
-            r = min_image<R>(xi - v3<R>(Aj.a.x, Aj.a.y, Aj.a.z), bx);  // target i - source j
+            r = min_image<R, !EWALD>(xi - v3<R>(Aj.a.x, Aj.a.y, Aj.a.z), bx);  // target i - source j
             r2 = dot(r, r);
             R B[6];
             if (COEF) {
@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(128) k_Tu(int n, const int* __restrict__ order
     for (int s = lane; s < cnt; s += LPA) {
         int j = row[s];
         R4<R> pj = at[j].a, ej = at[j].e;
-        V3<R> r = min_image<R>(xi - v3<R>(pj.x, pj.y, pj.z), bx);
+        V3<R> r = min_image<R, !EWALD>(xi - v3<R>(pj.x, pj.y, pj.z), bx);
         R r2 = dot(r, r);
         R rinv = rsqrt_<R>(r2);
         R rr = r2 * rinv, rinv2 = rinv * rinv;
@@ -140,29 +140,32 @@ __global__ void __launch_bounds__(128) k_Tu(int n, const int* __restrict__ order
 
 // Multipole energy (half of each directed pair), gradient and torque of site
 // i from all its neighbours (bulk, m-scale 1).  f = electric/dielec.
-// Analysis: per-site energy, nonzero pair count (directed), intermolecular.
-template <class R, bool EWALD, bool ANALYSIS, int LPA>
+// EXTRA: the outputs of the Analysis and Virial modes, each written when its
+// pointer is set -- per-site energy, nonzero pair count (directed) and
+// intermolecular energy (aem, npair, mol); the pair virial (vir, six sums),
+// half of -g_i (x) r per directed pair.
+template <class R, bool EWALD, bool EXTRA, int LPA>
 __global__ void __launch_bounds__(128) k_mpole_pair(int n, const int* __restrict__ order, const AtomR<R>* __restrict__ at, Box bx, R aewald,
                                                     const int* __restrict__ nbr, int cap,
                                                     const int* __restrict__ nnb, double f, double* __restrict__ grad,
                                                     double* __restrict__ trq, double* __restrict__ eacc,
                                                     double* __restrict__ aem, const int* __restrict__ mol,
-                                                    unsigned long long* __restrict__ npair) {
+                                                    unsigned long long* __restrict__ npair, double* __restrict__ vir) {
     const int gi_ = (blockIdx.x * blockDim.x + threadIdx.x) / LPA, lane = threadIdx.x % LPA;
     const int i = order[min(gi_, n - 1)];
     const int cnt = gi_ < n ? nnb[i] : 0;
-    double e_i = 0, einter = 0;
+    double e_i = 0, einter = 0, w[6] = {0, 0, 0, 0, 0, 0};
     long long cntnz = 0;
     AtomR<R> Ai = at[i];
     Mpole<R> Mi = load_mpole(Ai);
     V3<R> xi = v3<R>(Ai.a.x, Ai.a.y, Ai.a.z);
     V3<R> g = v3<R>(0, 0, 0), t = v3<R>(0, 0, 0);
-    int mi = ANALYSIS && mol ? mol[i] : 0;
+    int mi = EXTRA && mol ? mol[i] : 0;
     const int* row = nbr + (size_t)i * cap;
     for (int s = lane; s < cnt; s += LPA) {
         int j = row[s];
         AtomR<R> Aj = at[j];
-        V3<R> r = min_image<R>(v3<R>(Aj.a.x, Aj.a.y, Aj.a.z) - xi, bx);  // x_k - x_i
+        V3<R> r = min_image<R, !EWALD>(v3<R>(Aj.a.x, Aj.a.y, Aj.a.z) - xi, bx);  // x_k - x_i
         R B[6];
         bulk_radial<R, EWALD, false>(dot(r, r), aewald, R(0), R(0), B);
         R E;
@@ -171,9 +174,10 @@ __global__ void __launch_bounds__(128) k_mpole_pair(int n, const int* __restrict
         e_i += 0.5 * (double)E;
         g = g + gi;
         t = t + ti;
-        if (ANALYSIS) {
+        if (EXTRA) {
             if (E != R(0)) cntnz++;
             if (mol && mol[j] != mi) einter += 0.5 * (double)E;
+            vir_outer(w, gi.x, gi.y, gi.z, r.x, r.y, r.z, -0.5 * f);
         }
     }
     double gx = group_sum<LPA>((double)g.x), gy = group_sum<LPA>((double)g.y), gz = group_sum<LPA>((double)g.z);
@@ -182,25 +186,28 @@ __global__ void __launch_bounds__(128) k_mpole_pair(int n, const int* __restrict
     if (lane == 0 && gi_ < n) {
         grad[3 * i] += f * gx; grad[3 * i + 1] += f * gy; grad[3 * i + 2] += f * gz;
         trq[3 * i] += f * tx; trq[3 * i + 1] += f * ty; trq[3 * i + 2] += f * tz;
-        if (ANALYSIS) aem[i] += f * es;
+        if (EXTRA && aem) aem[i] += f * es;
     }
     block_sum_add(f * e_i, eacc);
-    if (ANALYSIS) {
+    if (EXTRA && npair) {
         block_sum_add(f * einter, eacc + 1);
         block_sum_add_ll(cntnz, npair);
     }
+    if (EXTRA && vir) block_vir_add(w, vir);
 }
 
 // Polarization gradient and torque of site i (bulk, all scales 1):
 //   G = E(M_i, ubar_k) + E(ubar_i, M_k) + 1/2 [E(up_i, ud_k) + E(ud_i, up_k)]
 // with ubar = (ud + up)/2; dG/dx_i = -dG/dr, torque on M_i from ubar_k.
-// u4: [n][2] R4, d set then p set per site.
-template <class R, bool EWALD, int LPA>
+// u4: [n][2] R4, d set then p set per site.  VIR: the pair virial into
+// vir (six sums), half of dG/dr (x) r per directed pair.
+template <class R, bool EWALD, int LPA, bool VIR>
 __global__ void __launch_bounds__(128) k_polar_pair(int n, const int* __restrict__ order, const AtomR<R>* __restrict__ at,
                                                     const R4<R>* __restrict__ u4, Box bx, R aewald,
                                                     const int* __restrict__ nbr, int cap,
                                                     const int* __restrict__ nnb, int mutual, double f,
-                                                    double* __restrict__ grad, double* __restrict__ trq) {
+                                                    double* __restrict__ grad, double* __restrict__ trq,
+                                                    double* __restrict__ vir) {
     const int gi_ = (blockIdx.x * blockDim.x + threadIdx.x) / LPA, lane = threadIdx.x % LPA;
     const int i = order[min(gi_, n - 1)];
     const int cnt = gi_ < n ? nnb[i] : 0;
@@ -211,11 +218,12 @@ __global__ void __launch_bounds__(128) k_polar_pair(int n, const int* __restrict
     V3<R> udi = v3<R>(udi4.x, udi4.y, udi4.z), upi = v3<R>(upi4.x, upi4.y, upi4.z);
     V3<R> ubi = R(0.5) * (udi + upi);
     V3<R> g = v3<R>(0, 0, 0), t = v3<R>(0, 0, 0);
+    double w[6] = {0, 0, 0, 0, 0, 0};
     const int* row = nbr + (size_t)i * cap;
     for (int s = lane; s < cnt; s += LPA) {
         int j = row[s];
         AtomR<R> Aj = at[j];
-        V3<R> r = min_image<R>(v3<R>(Aj.a.x, Aj.a.y, Aj.a.z) - xi, bx);
+        V3<R> r = min_image<R, !EWALD>(v3<R>(Aj.a.x, Aj.a.y, Aj.a.z) - xi, bx);
         R B[6];
         bulk_radial<R, EWALD, true>(dot(r, r), aewald, Ai.e.y * Aj.e.y, pair_thole<R>(Ai.e.z, Aj.e.z), B);
         R4<R> udk4 = u4[2 * j], upk4 = u4[2 * j + 1];
@@ -229,6 +237,7 @@ __global__ void __launch_bounds__(128) k_polar_pair(int n, const int* __restrict
         if (mutual) dEdr = dEdr + R(0.5) * (dd_pair<R>(upi, udk, r, B) + dd_pair<R>(udi, upk, r, B));
         g = g - dEdr;
         t = t + ti;
+        if (VIR) vir_outer(w, dEdr.x, dEdr.y, dEdr.z, r.x, r.y, r.z, 0.5 * f);
     }
     double gx = group_sum<LPA>((double)g.x), gy = group_sum<LPA>((double)g.y), gz = group_sum<LPA>((double)g.z);
     double tx = group_sum<LPA>((double)t.x), ty = group_sum<LPA>((double)t.y), tz = group_sum<LPA>((double)t.z);
@@ -236,6 +245,7 @@ __global__ void __launch_bounds__(128) k_polar_pair(int n, const int* __restrict
         grad[3 * i] += f * gx; grad[3 * i + 1] += f * gy; grad[3 * i + 2] += f * gz;
         trq[3 * i] += f * tx; trq[3 * i + 1] += f * ty; trq[3 * i + 2] += f * tz;
     }
+    if (VIR) block_vir_add(w, vir);
 }
 
 // ------------------------------------------------------------ stored T
@@ -271,7 +281,7 @@ __global__ void __launch_bounds__(128) k_tu_coeffs(int n, const int* __restrict_
         if (ok) {
             j = nbr[base + s];
             R4<R> pj = at[j].a, ej = at[j].e;
-            r = min_image<R>(xi - v3<R>(pj.x, pj.y, pj.z), bx);
+            r = min_image<R, !EWALD>(xi - v3<R>(pj.x, pj.y, pj.z), bx);
             r2 = dot(r, r);
             R rinv = rsqrt_<R>(r2);
             R rr = r2 * rinv, rinv2 = rinv * rinv;
@@ -388,9 +398,8 @@ __device__ __forceinline__ ScaledGeom scaled_geom(const ScaledPair& sp, const do
                                                   Box bx, double cut2, double aewald) {
     ScaledGeom G;
     int i = sp.i, k = sp.k;
-    G.r = v3<double>(wrap1<double>(xyz[3 * k] - xyz[3 * i], bx.L[0], bx.iL[0]),
-                     wrap1<double>(xyz[3 * k + 1] - xyz[3 * i + 1], bx.L[1], bx.iL[1]),
-                     wrap1<double>(xyz[3 * k + 2] - xyz[3 * i + 2], bx.L[2], bx.iL[2]));
+    G.r = min_image<double>(v3<double>(xyz[3 * k] - xyz[3 * i], xyz[3 * k + 1] - xyz[3 * i + 1],
+                                       xyz[3 * k + 2] - xyz[3 * i + 2]), bx);
     double r2 = dot(G.r, G.r);
     G.inside = r2 <= cut2;
     double rinv = 1.0 / sqrt(r2);
@@ -611,14 +620,14 @@ __global__ void __launch_bounds__(128) k_precond(int n, const int* __restrict__ 
 }
 
 // scaled pairs' contribution to em, its gradient and the torques (both
-// sites, full pair in FP64)
+// sites, full pair in FP64); the pair virial g_k (x) r into vir when set
 __global__ void k_scaled_mpole(int np, const ScaledPair* __restrict__ sp, const double* __restrict__ xyz,
                                const double* __restrict__ rp10, Box bx, double cut2, double aewald, double f,
                                double* __restrict__ grad, double* __restrict__ trq, double* __restrict__ eacc,
                                double* __restrict__ aem, const int* __restrict__ mol,
-                               unsigned long long* __restrict__ npair) {
+                               unsigned long long* __restrict__ npair, double* __restrict__ vir) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
-    double e = 0, einter = 0;
+    double e = 0, einter = 0, w[6] = {0, 0, 0, 0, 0, 0};
     long long nz = 0;
     if (t < np) {
         ScaledPair P = sp[t];
@@ -643,25 +652,25 @@ __global__ void k_scaled_mpole(int np, const ScaledPair* __restrict__ sp, const 
                     atomicAdd(aem + P.k, 0.5 * e);
                 }
                 if (mol && mol[P.i] != mol[P.k]) einter = e;
+                vir_outer(w, gk.x, gk.y, gk.z, G.r.x, G.r.y, G.r.z, f);
             }
         }
     }
     block_sum_add(e, eacc);
     if (mol) block_sum_add(einter, eacc + 1);
     if (npair) block_sum_add_ll(nz, npair);
+    if (vir) block_vir_add(w, vir);
 }
 
 // scaled pairs' polarization gradient and torques (full pair, FP64):
 //  1/2 [E^d(M_i, up_k) + E^d(up_i, M_k) + E^p(M_i, ud_k) + E^p(ud_i, M_k)
 //       + E^u(up_i, ud_k) + E^u(ud_i, up_k)]
-__global__ void k_scaled_polar(int np, const ScaledPair* __restrict__ sp, const double* __restrict__ xyz,
-                               const double* __restrict__ rp10, const double* __restrict__ pdamp,
-                               const double* __restrict__ thole, Box bx, double cut2, double aewald,
-                               const double* __restrict__ ud, const double* __restrict__ up, int mutual, double f,
-                               double* __restrict__ grad, double* __restrict__ trq) {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= np) return;
-    ScaledPair P = sp[t];
+__device__ __forceinline__ void scaled_polar_pair(const ScaledPair& P, const double* __restrict__ xyz,
+                                                  const double* __restrict__ rp10, const double* __restrict__ pdamp,
+                                                  const double* __restrict__ thole, Box bx, double cut2, double aewald,
+                                                  const double* __restrict__ ud, const double* __restrict__ up,
+                                                  int mutual, double f, double* __restrict__ grad,
+                                                  double* __restrict__ trq, double (&w)[6]) {
     ScaledGeom G = scaled_geom(P, xyz, pdamp, thole, bx, cut2, aewald);
     if (!G.inside) return;
     double Bd[6], Bp[6], Bu[6];
@@ -696,6 +705,19 @@ __global__ void k_scaled_polar(int np, const ScaledPair* __restrict__ sp, const 
     add3(grad, k, f * dEdr);
     add3(trq, i, (0.5 * f) * tqi);
     add3(trq, k, (0.5 * f) * tqk);
+    vir_outer(w, dEdr.x, dEdr.y, dEdr.z, r.x, r.y, r.z, f);
+}
+
+// The pair virial dG/dr (x) r goes into vir when set.
+__global__ void k_scaled_polar(int np, const ScaledPair* __restrict__ sp, const double* __restrict__ xyz,
+                               const double* __restrict__ rp10, const double* __restrict__ pdamp,
+                               const double* __restrict__ thole, Box bx, double cut2, double aewald,
+                               const double* __restrict__ ud, const double* __restrict__ up, int mutual, double f,
+                               double* __restrict__ grad, double* __restrict__ trq, double* __restrict__ vir) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    double w[6] = {0, 0, 0, 0, 0, 0};
+    if (t < np) scaled_polar_pair(sp[t], xyz, rp10, pdamp, thole, bx, cut2, aewald, ud, up, mutual, f, grad, trq, w);
+    if (vir) block_vir_add(w, vir);
 }
 
 }  // namespace amg

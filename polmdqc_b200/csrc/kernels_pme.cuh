@@ -199,6 +199,89 @@ __global__ void k_scale_grid(size_t npts, const R* __restrict__ G, typename Cplx
     g[t] = v;
 }
 
+// Reciprocal virial through the influence function.  A strain eps moves the
+// reciprocal vectors h -> (1 - eps^T) h and the volume V -> V (1 + tr eps) at
+// fixed fractional coordinates, so for an energy term e(m) = g(m) X(m)
+// (X a product of structure factors)
+//   de/deps_ab = e (2 (1/h^2 + pi^2/alpha^2) h_a h_b - delta_ab)
+// (the reciprocal virial of Essmann et al., J. Chem. Phys. 103, 8577 (1995),
+// in dE/d(strain) form).  `c2` = pi^2/alpha^2, `iL` the inverse box edges.
+__device__ __forceinline__ void kvir_point(double (&v)[6], int ma, int mb, int mc, double3 iL, double c2, double e) {
+    const double hx = ma * iL.x, hy = mb * iL.y, hz = mc * iL.z;
+    const double h2 = hx * hx + hy * hy + hz * hz;
+    const double t = 2.0 * (1.0 / h2 + c2) * e;
+    v[0] += t * hx * hx - e;
+    v[1] += t * hy * hy - e;
+    v[2] += t * hz * hz - e;
+    v[3] += t * hx * hy;
+    v[4] += t * hx * hz;
+    v[5] += t * hy * hz;
+}
+
+// Permanent multipoles: e(m) = f/2 g(m) |S(m)|^2 over the half-complex
+// transform cg (before the convolution); points 0 < c < K3/2 stand for m and
+// -m.  Saves the transform into `save` for the polarization cross terms.
+template <class R>
+__global__ void k_kvir_mpole(size_t ncomplex, int3 K, double3 iL, double c2, double f, const R* __restrict__ infl,
+                             const typename Cplx<R>::type* __restrict__ cg, typename Cplx<R>::type* __restrict__ save,
+                             double* __restrict__ vir) {
+    const int K3h = K.z / 2 + 1;
+    double v[6] = {0, 0, 0, 0, 0, 0};
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < ncomplex; t += (size_t)gridDim.x * blockDim.x) {
+        const auto S = cg[t];
+        if (save) save[t] = S;
+        if (t == 0) continue;
+        const int c = (int)(t % K3h);
+        const int b = (int)((t / K3h) % K.y);
+        const int a = (int)(t / ((size_t)K3h * K.y));
+        const int ma = a <= K.x / 2 ? a : a - K.x, mb = b <= K.y / 2 ? b : b - K.y;
+        const double wgt = (c == 0 || 2 * c == K.z) ? 1.0 : 2.0;
+        const double e = 0.5 * f * wgt * (double)infl[t] * ((double)S.x * S.x + (double)S.y * S.y);
+        kvir_point(v, ma, mb, c, iL, c2, e);
+    }
+    block_vir_add(v, vir);
+}
+
+// Polarization, G = 1/2 [U(up, M) + U(ud, M) + mutual U(up, ud)] with
+//   U(X, Y) = sum_m g(m) Re[S_X(m) conj S_Y(m)],
+// over the full grid: z is the transform of the dipole grid Q_d + i Q_p (so
+// S_d(m) = (z(m) + conj z(-m))/2, S_p(m) = (z(m) - conj z(-m))/(2i)), sM the
+// saved half-complex transform of the permanent grid, G the influence
+// function on the full grid.
+template <class R>
+__global__ void k_kvir_polar(size_t npts, int3 K, double3 iL, double c2, double f, int mutual,
+                             const R* __restrict__ G, const typename Cplx<R>::type* __restrict__ z,
+                             const typename Cplx<R>::type* __restrict__ sM, double* __restrict__ vir) {
+    const int K3h = K.z / 2 + 1;
+    double v[6] = {0, 0, 0, 0, 0, 0};
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < npts; t += (size_t)gridDim.x * blockDim.x) {
+        if (t == 0) continue;
+        const int c = (int)(t % K.z);
+        const int b = (int)((t / K.z) % K.y);
+        const int a = (int)(t / ((size_t)K.z * K.y));
+        const int an = a ? K.x - a : 0, bn = b ? K.y - b : 0, cn = c ? K.z - c : 0;
+        const auto zp = z[t];
+        const auto zn = z[((size_t)an * K.y + bn) * K.z + cn];
+        const double dx = 0.5 * ((double)zp.x + zn.x), dy = 0.5 * ((double)zp.y - zn.y);
+        const double px = 0.5 * ((double)zp.y + zn.y), py = -0.5 * ((double)zp.x - zn.x);
+        double mx, my;
+        if (c < K3h) {
+            const auto m = sM[((size_t)a * K.y + b) * K3h + c];
+            mx = m.x;
+            my = m.y;
+        } else {  // S_M(m) = conj S_M(-m), held at (an, bn, K3 - c)
+            const auto m = sM[((size_t)an * K.y + bn) * K3h + cn];
+            mx = m.x;
+            my = -(double)m.y;
+        }
+        double x = mx * (px + dx) + my * (py + dy);
+        if (mutual) x += px * dx + py * dy;
+        const int ma = a <= K.x / 2 ? a : a - K.x, mb = b <= K.y / 2 ? b : b - K.y, mc = c <= K.z / 2 ? c : c - K.z;
+        kvir_point(v, ma, mb, mc, iL, c2, 0.5 * f * (double)G[t] * x);
+    }
+    block_vir_add(v, vir);
+}
+
 // Multiply the transformed grids by the influence function
 //   G(m) = exp(-pi^2 |h|^2 / alpha^2) / (pi V |h|^2 bsmod1 bsmod2 bsmod3)
 // precomputed in FP64 on the host (half-complex layout, G(0) = 0).

@@ -201,10 +201,8 @@ __global__ void k_neighbors(int n, const double4* __restrict__ spos, const unsig
                     if (p < e) {
                         j = sids[p];
                         double4 pj = spos[p];
-                        double rx = wrap1<double>(pj.x - pi.x, bx.L[0], bx.iL[0]);
-                        double ry = wrap1<double>(pj.y - pi.y, bx.L[1], bx.iL[1]);
-                        double rz = wrap1<double>(pj.z - pi.z, bx.L[2], bx.iL[2]);
-                        hit = j != i && rx * rx + ry * ry + rz * rz <= cut2;
+                        V3<double> r = min_image<double>(v3<double>(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z), bx);
+                        hit = j != i && dot(r, r) <= cut2;
                         if (hit && j >= xr.x && j <= xr.y)
                             for (int q = x0; q < x1; q++) hit &= (xidx[q] != j);
                     }

@@ -68,6 +68,7 @@ class Params:
                 arr[j] = v
         p.use_ewald = int(st.use_ewald)
         p.use_bounds = int(s.use_bounds)
+        p.cell_shape = int(getattr(s, "cell_shape", 0))
         p.aewald = st.aewald
         for j in range(3):
             p.nfft[j] = st.nfft[j]
@@ -198,6 +199,12 @@ class Engine:
         self._check(self.lib.amg_last_stats(self.ctx, C.byref(launches), C.byref(graphed), C.byref(lpa)),
                     "amg_last_stats")
         return {"launches": int(launches.value), "graphed": bool(graphed.value), "lanes_per_site": int(lpa.value)}
+
+    def virial_parts(self):
+        """The em and ep parts (3x3 each) of the last forward's virial."""
+        vm, vp = np.zeros(9), np.zeros(9)
+        self._check(self.lib.amg_last_virial(self.ctx, abi.dptr(vm), abi.dptr(vp)), "amg_last_virial")
+        return vm.reshape(3, 3), vp.reshape(3, 3)
 
     def timing(self):
         ms = np.zeros(5)

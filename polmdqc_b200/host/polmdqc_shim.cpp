@@ -170,6 +170,7 @@ void ensure_context(bool want_polar)
     p.device = 0;
     p.pcg_prec = pcgprec;
     p.usolvcut = usolvcut;
+    p.cell_shape = octahedron ? AMG_CELL_OCTAHEDRON : dodecadron ? AMG_CELL_DODECAHEDRON : AMG_CELL_FROM_ANGLES;
     int rc = amg_create(&p, &dev.ctx);
     if (rc != AMG_OK) {
         printf("\n AMOEBA GPU  --  amg_create failed (status %d)\n", rc);
@@ -191,6 +192,7 @@ void evaluate(bool fill_mpole, bool fill_polar)
     int32_t f = AMG_DO_ENERGY | AMG_DO_DIPOLES;
     if (flags.do_analysis) f |= AMG_DO_ANALYSIS;
     if (flags.do_gradient) f |= AMG_DO_GRADIENT;
+    if (flags.do_virial) f |= AMG_DO_VIRIAL;
     amg_results r{};
     std::vector<double> gm, gp, am, ap, ui, up;
     if (flags.do_gradient && fill_mpole) { gm.assign(3 * (size_t)n, 0.0); r.dem = gm.data(); }
@@ -219,6 +221,17 @@ void evaluate(bool fill_mpole, bool fill_polar)
         }
         for (int i = 0; i < n; i++)
             for (int j = 0; j < 3; j++) { uind[i][j] = ui[3 * i + j]; uinp[i][j] = up[3 * i + j]; }
+    }
+    // virial (virial.h vir, added to like the reference's empole_a and torque
+    // do): both parts when this call filled em and ep, else the ep part
+    if (flags.do_virial) {
+        double vm[9], vp[9];
+        rc = amg_last_virial(dev.ctx, vm, vp);
+        if (rc != AMG_OK) fail("amg_last_virial", rc);
+        const bool polar = fill_polar && want_polar;
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++)
+                vir[a][b] += (fill_mpole ? vm[3 * a + b] : 0.0) + (polar ? vp[3 * a + b] : 0.0);
     }
 }
 }  // namespace

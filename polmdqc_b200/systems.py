@@ -22,6 +22,7 @@ import os
 
 import numpy as np
 
+from . import abi
 from . import prm as prm_mod
 
 DATA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
@@ -55,6 +56,7 @@ class System:
     box: np.ndarray            # [6] a,b,c,alpha,beta,gamma (zeros: no box)
     use_bounds: bool
     prm_name: str = ""
+    cell_shape: int = 0        # abi.CELL_*: octahedron / dodecahedron, else from the angles
 
     def csr(self, name):
         lists = self.lists[name]
@@ -364,7 +366,9 @@ def from_dump(d: dict, prm_name: str = "") -> System:
                   pdamp=np.array(d["pdamp"]) if has_pol else np.zeros(n),
                   lists=lists, m_scale=d["mscale"], p_scale=d["pscale"], p_iscale=d["piscale"],
                   d_scale=d["dscale"], u_scale=d["uscale"], box=box,
-                  use_bounds=bool(d["use_bounds"]), prm_name=prm_name)
+                  use_bounds=bool(d["use_bounds"]), prm_name=prm_name,
+                  cell_shape=(abi.CELL_OCTAHEDRON if d.get("octahedron") else
+                              abi.CELL_DODECAHEDRON if d.get("dodecadron") else abi.CELL_FROM_ANGLES))
 
 
 def write_tinker(sys_: System, xyz_path: str, key_path: str, prm_path: str, keys: list):

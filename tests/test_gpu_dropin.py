@@ -43,11 +43,30 @@ def test_dropin_water_dimer_golden():
     np.testing.assert_allclose(d["dem"], a2["dem"], atol=a2["eps1"], rtol=0)
 
 
-def test_dropin_waterbox30_golden():
-    g = golden("ref_tests.json")["bounds1"]
-    d = dump_gpu(ref_fixture("bounds", "waterbox30.xyz"), ref_fixture("bounds", "orthogonal.key"))
+@pytest.mark.parametrize("case,shape", [("bounds1", "orthogonal"), ("bounds2", "monoclinic"),
+                                        ("bounds3", "triclinic"), ("bounds4", "octahedron"),
+                                        ("bounds5", "dodecahedron")])
+def test_dropin_waterbox30_golden(case, shape):
+    """test/bounds.cpp bounds-1..5 through the reference's program with the
+    shim: the keyfile's cell shape reaches the library."""
+    g = golden("ref_tests.json")[case]
+    d = dump_gpu(ref_fixture("bounds", "waterbox30.xyz"), ref_fixture("bounds", shape + ".key"))
     assert d["nem"] == g["nem"]
     assert abs(d["em"] - g["em"]) < g["eps"]
+    assert abs(d["einter"] - g["einter"]) < g["eps"]
+
+
+def test_dropin_virial_matches_reference():
+    """energy<CalcMode::Virial> with the shim: the seeded 216-water box in the
+    reference's non-Ewald mode gives the reference's own vir."""
+    g = golden("ref_water216.json")
+    s = systems.water_box(216, 18.643, seed=0)
+    with tempfile.TemporaryDirectory() as tmp:
+        xyz, key = os.path.join(tmp, "w.xyz"), os.path.join(tmp, "w.key")
+        prm = os.path.join(REF_BUILD, "params", "water03.prm")
+        systems.write_tinker(s, xyz, key, prm, ["multipoleterm only", "mpole-cutoff 7.0", "digits 10"])
+        d = dump_gpu(xyz, key)
+    np.testing.assert_allclose(d["vir"], g["vir"], atol=1e-8 * np.abs(g["vir"]).max(), rtol=0)
 
 
 def test_dropin_ewald_polarization_matches_oracle():
@@ -64,8 +83,9 @@ def test_dropin_ewald_polarization_matches_oracle():
         d = dump_gpu(xyz, key)
     sd = systems.from_dump(d)
     st = Settings(aewald=d["aeewald"], nfft=tuple(d["nefft"]), cutoff=d["ewaldcut"], precision=abi.PREC_FP64)
-    o = oracle.forward(sd, st, tol=1e-11)
+    o = oracle.forward(sd, st, tol=1e-11, flags=abi.DO_ENERGY | abi.DO_GRADIENT | abi.DO_DIPOLES | abi.DO_VIRIAL)
     assert abs(d["em"] - o.em) < 1e-9 * abs(o.em)
+    np.testing.assert_allclose(d["vir"], o.vir.reshape(-1), atol=1e-7 * np.abs(o.vir).max(), rtol=0)
     assert abs(d["ep"] - o.ep) < 1e-7 * abs(o.ep)
     np.testing.assert_allclose(d["dem"], o.dem.reshape(-1), atol=1e-7)
     np.testing.assert_allclose(d["dep"], o.dep.reshape(-1), atol=1e-5)

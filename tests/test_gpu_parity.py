@@ -72,16 +72,44 @@ def test_waterbox30_orthogonal_golden():
     np.testing.assert_allclose(r.dem.reshape(-1), d["dem"], atol=1e-8, rtol=0)
 
 
+@pytest.mark.parametrize("prec", [FP64, MIXED])
+@pytest.mark.parametrize("case,shape", [("bounds2", "monoclinic"), ("bounds3", "triclinic"),
+                                        ("bounds4", "octahedron"), ("bounds5", "dodecahedron")])
+def test_waterbox30_cell_shapes_golden(case, shape, prec):
+    """test/bounds.cpp bounds-2..5: monoclinic, triclinic, truncated
+    octahedron and rhombic dodecahedron cells through the C ABI (the
+    reference's image(), one candidate cell and an FP64 list decision)."""
+    g = golden("ref_tests.json")[case]
+    d = ref_dump(ref_fixture("bounds", "waterbox30.xyz"), ref_fixture("bounds", shape + ".key"))
+    s = systems.from_dump(d)
+    st = Settings(use_ewald=False, cutoff=d["mpolecut"], poltyp=abi.POL_NONE, precision=prec)
+    r = run(s, st, abi.DO_ENERGY | abi.DO_GRADIENT | abi.DO_ANALYSIS)
+    tol = g["eps"] if prec == FP64 else 1e-6 * abs(g["em"])
+    assert r.nem == g["nem"]
+    assert abs(r.em - g["em"]) < tol
+    assert abs(r.einter - g["einter"]) < tol
+    np.testing.assert_allclose(r.dem.reshape(-1), d["dem"], atol=1e-8 if prec == FP64 else 1e-3, rtol=0)
+
+
+def test_ewald_needs_an_orthogonal_cell():
+    d = ref_dump(ref_fixture("bounds", "waterbox30.xyz"), ref_fixture("bounds", "triclinic.key"))
+    s = systems.from_dump(d)
+    with pytest.raises(AmgError, match="UNSUPPORTED"):
+        run(s, Settings(nfft=(32, 32, 32), cutoff=9.0, poltyp=abi.POL_NONE))
+
+
 def test_synthetic_box_matches_reference_run():
     """Seeded 216-water box: the compiled reference's em/nem/dem (non-Ewald, 7 A)."""
     d = golden("ref_water216.json")
     s = systems.water_box(216, 18.643, seed=0)
     s.xyz = np.stack([d["x"], d["y"], d["z"]], 1)
     st = Settings(use_ewald=False, cutoff=d["mpolecut"], poltyp=abi.POL_NONE, precision=FP64)
-    r = run(s, st, abi.DO_ENERGY | abi.DO_GRADIENT | abi.DO_ANALYSIS)
+    r = run(s, st, abi.DO_ENERGY | abi.DO_GRADIENT | abi.DO_ANALYSIS | abi.DO_VIRIAL)
     assert r.nem == d["nem"]
     assert rel(r.em, d["em"]) < 1e-10
     np.testing.assert_allclose(r.dem.reshape(-1), d["dem"], atol=1e-8, rtol=0)
+    # the reference's CalcMode::Virial: pair terms plus the torque share
+    np.testing.assert_allclose(r.vir.reshape(-1), d["vir"], atol=1e-8 * np.abs(d["vir"]).max(), rtol=0)
 
 
 # ---------------------------------------------------------------- oracle (Ewald + polarization)
@@ -137,6 +165,44 @@ def test_pme_grid_sizes_match_oracle(w216, nfft):
     assert rel(g.ep, o.ep) < 1e-8
     assert np.abs(g.dep - o.dep).max() < 1e-5
     assert np.abs(g.uind - o.uind).max() < 1e-7
+
+
+@pytest.mark.parametrize("prec", [FP64, MIXED])
+def test_virial_matches_oracle(w216, prec):
+    """CalcMode::Virial with Ewald and mutual polarization: real-space pairs,
+    torque share, the reciprocal k-space and multipole terms and the net
+    charge term, summed (symmetric 3x3) and split into the em and ep parts.
+    The oracle's virial is pinned to the reference (non-Ewald) and to strain
+    derivatives of the energy.  Tolerances relative to max |W|: 1e-8 (FP64;
+    dipoles converged to 1e-8 D), 1e-5 (mixed)."""
+    st = Settings(nfft=(24, 24, 24), precision=prec, poleps=1e-8 if prec == FP64 else 1e-6)
+    flags = ALL | abi.DO_VIRIAL
+    o = oracle.forward(w216, Settings(nfft=(24, 24, 24), precision=FP64), tol=1e-11, flags=flags)
+    om = oracle.forward(w216, Settings(nfft=(24, 24, 24), precision=FP64, poltyp=abi.POL_NONE),
+                        flags=abi.DO_ENERGY | abi.DO_VIRIAL)
+    e = Engine(w216, st)
+    try:
+        g = e.forward(flags)
+        vm, vp = e.virial_parts()
+    finally:
+        e.close()
+    scale = np.abs(o.vir).max()
+    tol = 1e-8 if prec == FP64 else 1e-5
+    err, err_m = np.abs(g.vir - o.vir).max() / scale, np.abs(vm - om.vir).max() / scale
+    print(f"virial prec={prec} max|W|={scale:.4g} err={err:.3g} em-part err={err_m:.3g}")
+    assert np.allclose(g.vir, g.vir.T, rtol=0, atol=1e-12 * scale)
+    assert err < tol and err_m < tol
+    np.testing.assert_allclose(vm + vp, g.vir, rtol=0, atol=1e-12 * scale)
+    # Virial mode implies the gradient
+    assert np.abs(g.dem - o.dem).max() < (1e-8 if prec == FP64 else 1e-3)
+
+
+def test_virial_non_ewald_polarization_matches_oracle():
+    s = systems.water_box(64, 12.4, seed=5)
+    st = Settings(use_ewald=False, cutoff=6.0, precision=FP64, poleps=1e-9)
+    o = oracle.forward(s, st, tol=1e-11, flags=ALL | abi.DO_VIRIAL)
+    g = run(s, st, ALL | abi.DO_VIRIAL)
+    assert np.abs(g.vir - o.vir).max() < 1e-7 * np.abs(o.vir).max()
 
 
 def test_mixed_meets_accuracy_target(w216, w216_oracle):

@@ -28,6 +28,22 @@ def test_water_dimer_golden():
     np.testing.assert_allclose(r.dem.reshape(-1), a2["dem"], atol=a2["eps1"], rtol=0)
 
 
+@pytest.mark.parametrize("case,shape", [("bounds2", "monoclinic"), ("bounds3", "triclinic"),
+                                        ("bounds4", "octahedron"), ("bounds5", "dodecahedron")])
+def test_waterbox30_cell_shapes_golden(case, shape):
+    """test/bounds.cpp bounds-2..5: the same box as a monoclinic, triclinic,
+    truncated-octahedron and rhombic-dodecahedron cell (the reference's
+    image(), src/md/image.cpp:37-124): em, nem, einter at 1e-8."""
+    g = golden("ref_tests.json")[case]
+    d = ref_dump(ref_fixture("bounds", "waterbox30.xyz"), ref_fixture("bounds", shape + ".key"))
+    s = systems.from_dump(d)
+    r = oracle.forward(s, nonewald(d["mpolecut"]), flags=abi.DO_ENERGY | abi.DO_GRADIENT | abi.DO_ANALYSIS)
+    assert r.nem == g["nem"]
+    assert abs(r.em - g["em"]) < g["eps"]
+    assert abs(r.einter - g["einter"]) < g["eps"]
+    np.testing.assert_allclose(r.dem.reshape(-1), d["dem"], atol=1e-8, rtol=0)
+
+
 def test_waterbox30_orthogonal_golden():
     """test/bounds.cpp bounds-1: 2,700-atom periodic box, cutoff 9, em and nem at 1e-8."""
     g = golden("ref_tests.json")["bounds1"]

@@ -83,6 +83,8 @@ extern "C" {
 #define AMG_POL_NONE    0
 #define AMG_POL_MUTUAL  1
 #define AMG_POL_DIRECT  2
+#define AMG_POL_OPT     3  /* extrapolated perturbation theory, coefficients opt_coef */
+#define AMG_MAX_OPT     6  /* highest OPT order (polopt.h maxopt) */
 
 /* CalcMode flags for amg_forward (reference calcMode.h:18-45) */
 #define AMG_DO_ENERGY    1
@@ -140,6 +142,11 @@ typedef struct amg_params {
                                         is supported without Ewald (the reference's
                                         multipole mode) and returns UNSUPPORTED
                                         with it */
+    double opt_coef[AMG_MAX_OPT + 1]; /* polopt.h copt: with AMG_POL_OPT the dipoles
+                                        are sum_k (sum_{j>=k} copt_j) u^(k), u^(0) =
+                                        alpha E, u^(k) = alpha T u^(k-1); the order is
+                                        the last nonzero entry (src/md/kpolar.cpp:
+                                        108-153, 228-236) */
 } amg_params;
 
 typedef struct amg_results {

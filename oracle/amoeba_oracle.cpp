@@ -108,6 +108,9 @@ struct System {
     double alpha = 0, cut = 0, f = 0;
     int K[3] = {0, 0, 0}, order = 5;
     int poltyp = AMG_POL_NONE;
+    // OPT: u = sum_k copm_k u^(k), copm_k = sum_{j>=k} copt_j (src/md/kpolar.cpp:228-236)
+    std::vector<double> copm;
+    int optorder = 0;
     double poleps = 1e-6, debye = 4.80321;
     int politer = 100;
     bool guess = true;
@@ -917,6 +920,7 @@ struct Result {
     std::vector<V3> dem, dep;
     std::vector<double> aem, aep;
     std::vector<V3> ud, up, Ed, Ep;
+    std::vector<std::vector<V3>> ukd, ukp;  // OPT: perturbation orders u^(k), k = 0..optorder
     int iters = 0;
     double eps = 0;
 };
@@ -935,6 +939,30 @@ int solve_dipoles(Work& w, Result& R, double tol_override, int maxit_override) {
         R.up[i] = s.pol[i] * R.Ep[i];
     }
     if (s.poltyp == AMG_POL_DIRECT || npolar == 0) return AMG_OK;
+    if (s.poltyp == AMG_POL_OPT) {
+        // perturbation orders u^(k) = alpha T u^(k-1) (T: the full dipole field,
+        // u-scaled real space + reciprocal + self), mixed with copm
+        R.ukd.assign(1, R.ud);
+        R.ukp.assign(1, R.up);
+        for (int k = 1; k <= s.optorder; k++) {
+            std::vector<Mp> Md(s.n), Mpv(s.n);
+            for (int i = 0; i < s.n; i++) { Md[i] = dipole_only(R.ukd[k - 1][i]); Mpv[i] = dipole_only(R.ukp[k - 1][i]); }
+            std::vector<V3> Fd, Fp;
+            total_field(w, Md, 2, Fd, 1);
+            total_field(w, Mpv, 2, Fp, 1);
+            for (int i = 0; i < s.n; i++) { Fd[i] = s.pol[i] * Fd[i]; Fp[i] = s.pol[i] * Fp[i]; }
+            R.ukd.push_back(Fd);
+            R.ukp.push_back(Fp);
+        }
+        for (int i = 0; i < s.n; i++) {
+            V3 a{0, 0, 0}, b{0, 0, 0};
+            for (int k = 0; k <= s.optorder; k++) { a = a + s.copm[k] * R.ukd[k][i]; b = b + s.copm[k] * R.ukp[k][i]; }
+            R.ud[i] = a;
+            R.up[i] = b;
+        }
+        R.iters = s.optorder;
+        return AMG_OK;
+    }
     double tol = tol_override > 0 ? tol_override : s.poleps;
     int maxit = maxit_override > 0 ? maxit_override : s.politer;
     auto apply = [&](const std::vector<V3>& ud, const std::vector<V3>& up, std::vector<V3>& Ad, std::vector<V3>& Au) {
@@ -1163,7 +1191,25 @@ void evaluate(Work& w, Flags fl, Result& R, double tol_override, int maxit_overr
     R.ep = ep;
     if (!fl.grad) return;
     const bool mutual = s.poltyp == AMG_POL_MUTUAL;
-    // real space: gradient of G = 1/2 [U_d(up<->M) + U_p(ud<->M) + U_u(up<->ud)]
+    // real space: gradient of G = 1/2 [U_d(up<->M) + U_p(ud<->M) + sum_c U_u(X_c<->Y_c)]
+    // with the dipole-dipole sets (X_c, Y_c): mutual (up, ud); OPT, from
+    // E = -1/2 sum_k copm_k (alpha T)^k alpha E_d . E_p and
+    // d(alpha T)^k = sum_{a+b=k-1} (alpha T)^a alpha dT (alpha T)^b:
+    // (V_b, ud^(b)), V_b = sum_a copm_{a+b+1} up^(a), b = 0..optorder-1
+    std::vector<std::vector<V3>> cX, cY;
+    if (mutual) {
+        cX.push_back(R.up);
+        cY.push_back(R.ud);
+    } else if (s.poltyp == AMG_POL_OPT) {
+        for (int b = 0; b < s.optorder; b++) {
+            std::vector<V3> V(s.n, V3{0, 0, 0});
+            for (int a = 0; a + b + 1 <= s.optorder; a++)
+                for (int i = 0; i < s.n; i++) V[i] = V[i] + s.copm[a + b + 1] * R.ukp[a][i];
+            cX.push_back(V);
+            cY.push_back(R.ukd[b]);
+        }
+    }
+    const int ncross = (int)cX.size();
     double wpol[3][3] = {};
 #pragma omp parallel
     {
@@ -1191,10 +1237,10 @@ void evaluate(Work& w, Flags fl, Result& R, double tol_override, int maxit_overr
             source_potential(Td, upi, 3, a3);    // up_i at k, d channel
             source_potential(Tp, udi, 3, a4);    // ud_i at k, p channel
             V3 gk = site_gradient(upk, a1) + site_gradient(udk, a2) + site_gradient(M[k], a3) + site_gradient(M[k], a4);
-            if (mutual) {
-                source_potential(Tu, udi, 2, a5);  // ud_i at k, u channel
-                source_potential(Tu, upi, 2, a6);  // up_i at k, u channel
-                gk = gk + site_gradient(upk, a5) + site_gradient(udk, a6);
+            for (int c = 0; c < ncross; c++) {
+                source_potential(Tu, dipole_only(cY[c][i]), 2, a5);  // Y_i at k, u channel
+                source_potential(Tu, dipole_only(cX[c][i]), 2, a6);  // X_i at k, u channel
+                gk = gk + site_gradient(dipole_only(cX[c][k]), a5) + site_gradient(dipole_only(cY[c][k]), a6);
             }
             gk = 0.5 * gk;
             gl[k] = gl[k] + gk;
@@ -1225,11 +1271,24 @@ void evaluate(Work& w, Flags fl, Result& R, double tol_override, int maxit_overr
         std::vector<cd> Sd, Sp;
         recip_potential(w, Md, phd, kvir ? &Sd : nullptr);
         recip_potential(w, Mpv, php, kvir ? &Sp : nullptr);
-        // G = 1/2 [U(up, M) + U(ud, M) + U(up, ud)] in reciprocal space
+        // potentials of the dipole-dipole sets (mutual: those of up and ud)
+        std::vector<std::vector<double>> phX(ncross), phY(ncross);
+        std::vector<std::vector<cd>> SX(ncross), SY(ncross);
+        for (int c = 0; c < ncross; c++) {
+            if (mutual) {
+                phX[c] = php; phY[c] = phd; SX[c] = Sp; SY[c] = Sd;
+                continue;
+            }
+            std::vector<Mp> MX(s.n), MY(s.n);
+            for (int i = 0; i < s.n; i++) { MX[i] = dipole_only(cX[c][i]); MY[i] = dipole_only(cY[c][i]); }
+            recip_potential(w, MX, phX[c], kvir ? &SX[c] : nullptr);
+            recip_potential(w, MY, phY[c], kvir ? &SY[c] : nullptr);
+        }
+        // G = 1/2 [U(up, M) + U(ud, M) + sum_c U(X_c, Y_c)] in reciprocal space
         if (kvir) {
             pme_kvir(s, w.pm, SM, Sp, 0.5, wpol);
             pme_kvir(s, w.pm, SM, Sd, 0.5, wpol);
-            if (mutual) pme_kvir(s, w.pm, Sp, Sd, 0.5, wpol);
+            for (int c = 0; c < ncross; c++) pme_kvir(s, w.pm, SX[c], SY[c], 0.5, wpol);
         }
         double self = 4.0 * s.alpha * s.alpha * s.alpha / (3.0 * kSqrtPi);
         for (int i = 0; i < s.n; i++) {
@@ -1238,7 +1297,9 @@ void evaluate(Work& w, Flags fl, Result& R, double tol_override, int maxit_overr
             const double* pp = &php[20 * (size_t)i];
             Mp upi = dipole_only(R.up[i]), udi = dipole_only(R.ud[i]);
             V3 g = site_gradient(upi, pm) + site_gradient(udi, pm) + site_gradient(M[i], pp) + site_gradient(M[i], pd);
-            if (mutual) g = g + site_gradient(upi, pd) + site_gradient(udi, pp);
+            for (int c = 0; c < ncross; c++)
+                g = g + site_gradient(dipole_only(cX[c][i]), &phY[c][20 * (size_t)i]) +
+                    site_gradient(dipole_only(cY[c][i]), &phX[c][20 * (size_t)i]);
             R.dep[i] = R.dep[i] + 0.5 * g;
             double avg[20];
             for (int j = 0; j < 20; j++) avg[j] = 0.5 * (pd[j] + pp[j]);
@@ -1251,9 +1312,9 @@ void evaluate(Work& w, Flags fl, Result& R, double tol_override, int maxit_overr
                 mpole_virial(udi, pm, wj);
                 mpole_virial(M[i], pp, wj);
                 mpole_virial(M[i], pd, wj);
-                if (mutual) {
-                    mpole_virial(upi, pd, wj);
-                    mpole_virial(udi, pp, wj);
+                for (int c = 0; c < ncross; c++) {
+                    mpole_virial(dipole_only(cX[c][i]), &phY[c][20 * (size_t)i], wj);
+                    mpole_virial(dipole_only(cY[c][i]), &phX[c][20 * (size_t)i], wj);
                 }
                 for (int a = 0; a < 3; a++)
                     for (int b = 0; b < 3; b++) wpol[a][b] += 0.5 * wj[a][b];
@@ -1372,6 +1433,16 @@ int orc_forward(const amg_params* P, const double* xyz, const double box[6], int
     for (int a = 0; a < 3; a++) s.K[a] = P->nfft[a];
     s.order = P->bsorder;
     s.poltyp = P->polarity ? P->poltyp : AMG_POL_NONE;
+    if (s.poltyp == AMG_POL_OPT) {
+        for (int k = 0; k <= AMG_MAX_OPT; k++)
+            if (P->opt_coef[k] != 0.0) s.optorder = k;
+        if (s.optorder < 1) return AMG_ERR_BAD_ARG;
+        s.copm.assign(s.optorder + 1, 0.0);
+        for (int k = 0; k <= s.optorder; k++)
+            for (int j = k; j <= s.optorder; j++) s.copm[k] += P->opt_coef[j];
+    } else if (s.poltyp != AMG_POL_NONE && s.poltyp != AMG_POL_MUTUAL && s.poltyp != AMG_POL_DIRECT) {
+        return AMG_ERR_UNSUPPORTED;
+    }
     s.poleps = P->poleps;
     s.politer = P->politer;
     s.debye = P->debye;

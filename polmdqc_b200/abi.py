@@ -24,7 +24,7 @@ STATUS = {0: "OK", 1: "BAD_ARG", 2: "UNSUPPORTED", 3: "NO_CONVERGE", 4: "NAN",
 
 FRAME_NONE, FRAME_ZTHENX, FRAME_ZONLY, FRAME_BISECTOR, FRAME_ZBISECT, FRAME_THREEFOLD = range(6)
 PREC_FP64, PREC_MIXED = 0, 1
-POL_NONE, POL_MUTUAL, POL_DIRECT = 0, 1, 2
+POL_NONE, POL_MUTUAL, POL_DIRECT, POL_OPT = 0, 1, 2, 3
 CELL_FROM_ANGLES, CELL_OCTAHEDRON, CELL_DODECAHEDRON = 0, 1, 2
 DO_ENERGY, DO_ANALYSIS, DO_GRADIENT, DO_VIRIAL, DO_DIPOLES = 1, 2, 4, 8, 16
 
@@ -55,6 +55,7 @@ class amg_params(C.Structure):
         ("precision", C.c_int32), ("pcg_guess", C.c_int32), ("device", C.c_int32),
         ("pcg_prec", C.c_int32), ("usolvcut", C.c_double),
         ("cell_shape", C.c_int32),
+        ("opt_coef", C.c_double * 7),
     ]
 
 

@@ -172,6 +172,11 @@ struct amg_ctx {
     int npolar = 0;
     int *iter = nullptr, *cont = nullptr;
     int* dir_done = nullptr;  // block counter of k_pcg_dir (back to 0 after every launch)
+    // OPT: order, copm_k = sum_{j>=k} copt_j, and the perturbation orders
+    // u^(k) [K+1][2][3n] followed by one [3n] scratch vector
+    int optorder = 0;
+    OptCoef copm{};
+    double* uopt = nullptr;
     // captured evaluation (periodic systems)
     bool use_graphs = true, graph_dirty = true, graphed_last = false;
     cudaGraphExec_t gexec = nullptr;
@@ -705,7 +710,7 @@ void spread_dipoles(amg_ctx* ctx, cudaStream_t s, const double* vd, const double
 // transform and the permanent one saved by pme_mpole
 template <class R>
 void pme_dipole_grids(amg_ctx* ctx, cudaStream_t s, const double* vd, const double* vp, bool spread = true,
-                      double* vir = nullptr) {
+                      double* vir = nullptr, bool mterms = true) {
     Pme<R>& pm = pme_of<R>(ctx);
     if (spread) {
         CK(cudaMemsetAsync(pm.zg, 0, sizeof(typename Cplx<R>::type) * pm.G, s));
@@ -717,7 +722,7 @@ void pme_dipole_grids(amg_ctx* ctx, cudaStream_t s, const double* vd, const doub
         using C = typename Cplx<R>::type;
         k_kvir_polar<R><<<(unsigned)ctx->num_sms * 2, 256, 0, s>>>(
             pm.G, make_int3(ctx->K[0], ctx->K[1], ctx->K[2]), inv_edges(ctx), kvir_c2(ctx), ctx->f,
-            ctx->poltyp == AMG_POL_MUTUAL, pm.Gfull, pm.zg, (const C*)pm.cgrid + pm.Gc, vir);
+            mterms ? ctx->poltyp == AMG_POL_MUTUAL : 1, mterms, pm.Gfull, pm.zg, (const C*)pm.cgrid + pm.Gc, vir);
         KCHECK();
     }
     k_scale_grid<R><<<nblk(pm.G, 256), 256, 0, s>>>(pm.G, pm.Gfull, pm.zg, pm.zq);  // also clears zg
@@ -728,11 +733,11 @@ void pme_dipole_grids(amg_ctx* ctx, cudaStream_t s, const double* vd, const doub
 // reciprocal potentials of two dipole sets -> phi [2][n][NC]
 template <class R, int NC>
 void pme_dipoles(amg_ctx* ctx, cudaStream_t s, const double* vd, const double* vp, double* phi,
-                 double* vir = nullptr) {
+                 double* vir = nullptr, bool mterms = true) {
     Pme<R>& pm = pme_of<R>(ctx);
     int3 K = make_int3(ctx->K[0], ctx->K[1], ctx->K[2]);
     double sc[3] = {ctx->K[0] / ctx->box[0], ctx->K[1] / ctx->box[1], ctx->K[2] / ctx->box[2]};
-    pme_dipole_grids<R>(ctx, s, vd, vp, true, vir);
+    pme_dipole_grids<R>(ctx, s, vd, vp, true, vir, mterms);
     k_gather<R, kOrder, NC, kGatherLanes, 2><<<nblk((size_t)ctx->n * kGatherLanes), kThreads, 0, s>>>(
         ctx->n, pm.zq, pm.theta, pm.k0, K, sc[0], sc[1], sc[2], phi);
     KCHECK();
@@ -1051,6 +1056,72 @@ void enqueue_front(amg_ctx* ctx, cudaStream_t s) {
     CK(cudaEventRecord(ctx->ev[2], s));
 }
 
+// OPT dipoles (extrapolated perturbation theory): from the direct dipoles
+// u^(0) = alpha E left in (ud, up) by the permanent field, optorder
+// applications of the dipole field, u^(k) = alpha T u^(k-1) = v - alpha A v,
+// mixed into u = sum_k copm_k u^(k); every u^(k) is kept for the forces
+template <class R>
+void enqueue_opt(amg_ctx* ctx, cudaStream_t s) {
+    const int n3 = 3 * ctx->n;
+    const size_t blk = 6 * (size_t)ctx->n;  // one order: d set then p set
+    double* uo = ctx->uopt;
+    k_opt_init<<<nblk(n3), kThreads, 0, s>>>(n3, ctx->copm.c[0], ctx->ud, ctx->up, uo, uo + n3);
+    KCHECK();
+    for (int k = 1; k <= ctx->optorder; k++) {
+        const double* vd = uo + (k - 1) * blk;
+        matvec<R>(ctx, s, vd, vd + n3, ctx->Apd, ctx->App);
+        k_opt_step<<<nblk(n3), kThreads, 0, s>>>(n3, ctx->pol, vd, vd + n3, ctx->Apd, ctx->App, ctx->copm.c[k],
+                                                 uo + k * blk, uo + k * blk + n3, ctx->ud, ctx->up);
+        KCHECK();
+    }
+}
+
+// OPT force terms between perturbation orders: for b = 0..K-1 the
+// dipole-dipole interaction of ud^(b) with V_b = sum_a copm_{a+b+1} up^(a)
+// (from d(alpha T)^k = sum_{a+b=k-1} (alpha T)^a alpha dT (alpha T)^b), in
+// real space (bulk and scaled pairs) and reciprocal space, on stream s
+template <class R>
+void enqueue_opt_cross(amg_ctx* ctx, cudaStream_t s, double* virp) {
+    const int n = ctx->n, n3 = 3 * n;
+    const size_t blk = 6 * (size_t)n;
+    double* uo = ctx->uopt;
+    double* V = uo + (ctx->optorder + 1) * blk;
+    Atoms<R>& A = atoms_of<R>(ctx);
+    const R aew = (R)ctx->aewald;
+    for (int b = 0; b < ctx->optorder; b++) {
+        const double* Y = uo + b * blk;  // ud^(b)
+        k_opt_cross<<<nblk(n3), kThreads, 0, s>>>(n3, ctx->optorder, b, ctx->copm, uo, V);
+        KCHECK();
+        k_pack_u<R><<<nblk(n), kThreads, 0, s>>>(n, Y, V, A.u4);
+        KCHECK();
+        auto launch = [&](auto kern) {
+            kern<<<nblk((size_t)n * 8), kThreads, 0, s>>>(n, ctx->sids, A.at, A.u4, ctx->bx, aew, ctx->nbr, ctx->cap,
+                                                          ctx->nnb, 1, ctx->f, ctx->grad_p, ctx->trq_p, virp);
+        };
+        if (ctx->ewald) {
+            if (virp) launch(k_polar_pair<R, true, 8, true, true>);
+            else launch(k_polar_pair<R, true, 8, false, true>);
+        } else {
+            if (virp) launch(k_polar_pair<R, false, 8, true, true>);
+            else launch(k_polar_pair<R, false, 8, false, true>);
+        }
+        KCHECK();
+        if (ctx->nsp) {
+            k_scaled_polar<<<nblk(ctx->nsp), kThreads, 0, s>>>(ctx->nsp, ctx->sp, ctx->xyz, ctx->rp10, ctx->pdamp,
+                                                              ctx->thole, ctx->bx, ctx->cut * ctx->cut, ewald_alpha(ctx),
+                                                              Y, V, 1, 1, ctx->f, ctx->grad_p, ctx->trq_p, virp);
+            KCHECK();
+        }
+        if (ctx->ewald) {
+            pme_dipoles<R, 20>(ctx, s, Y, V, ctx->phiU, virp, false);
+            k_recip_polar<<<nblk(n), kThreads, 0, s>>>(n, ctx->rp10, ctx->phiM, ctx->phiU, ctx->phiU + 20 * (size_t)n,
+                                                       Y, V, 1, 1, self_coef(ctx), ctx->f, ctx->grad_p, ctx->trq_p,
+                                                       virp);
+            KCHECK();
+        }
+    }
+}
+
 // everything after the solve: energies, gradients, torques
 template <class R>
 void enqueue_back(amg_ctx* ctx, cudaStream_t s, int flags) {
@@ -1128,7 +1199,7 @@ void enqueue_back(amg_ctx* ctx, cudaStream_t s, int flags) {
         if (ctx->nsp) {
             k_scaled_polar<<<nblk(ctx->nsp), kThreads, 0, r>>>(ctx->nsp, ctx->sp, ctx->xyz, ctx->rp10, ctx->pdamp,
                                                               ctx->thole, ctx->bx, cut2, ewald_alpha(ctx), ctx->ud,
-                                                              ctx->up, mutual, ctx->f, ctx->grad_p, ctx->trq_p, virp);
+                                                              ctx->up, mutual, 0, ctx->f, ctx->grad_p, ctx->trq_p, virp);
             KCHECK();
         }
     }
@@ -1147,10 +1218,11 @@ void enqueue_back(amg_ctx* ctx, cudaStream_t s, int flags) {
     if (polgrad) {
         if (ctx->ewald) {
             k_recip_polar<<<nblk(n), kThreads, 0, s>>>(n, ctx->rp10, ctx->phiM, ctx->phiU, ctx->phiU + 20 * (size_t)n,
-                                                       ctx->ud, ctx->up, mutual, self_coef(ctx), ctx->f, ctx->grad_p,
+                                                       ctx->ud, ctx->up, mutual, 0, self_coef(ctx), ctx->f, ctx->grad_p,
                                                        ctx->trq_p, virp);
             KCHECK();
         }
+        if (ctx->poltyp == AMG_POL_OPT && ctx->npolar > 0) enqueue_opt_cross<R>(ctx, s, virp);
         k_torque<<<nblk(n), kThreads, 0, s>>>(n, ctx->xyz, ctx->zax, ctx->xax, ctx->yax, ctx->axe, ctx->trq_p,
                                               ctx->grad_p, virp);
         KCHECK();
@@ -1187,6 +1259,7 @@ bool capture_graph(amg_ctx* ctx, int flags) {
     long long kb = 0;
     try {
         enqueue_front<R>(ctx, s);
+        if (ctx->poltyp == AMG_POL_OPT && ctx->npolar > 0) enqueue_opt<R>(ctx, s);
         if (iterative(ctx)) {
             const cudaGraphNode_t* deps = nullptr;
             size_t ndeps = 0;
@@ -1245,6 +1318,7 @@ template <class R>
 void enqueue_eager(amg_ctx* ctx, int flags) {
     cudaStream_t s = ctx->st;
     enqueue_front<R>(ctx, s);
+    if (ctx->poltyp == AMG_POL_OPT && ctx->npolar > 0) enqueue_opt<R>(ctx, s);
     if (iterative(ctx)) {
         enqueue_pcg_init<R>(ctx, s, 0, 0, true);
         int cont = 1;
@@ -1323,7 +1397,7 @@ int forward_impl(amg_ctx* ctx, int flags, amg_results* res) {
         eps = ctx->debye * std::sqrt(std::max(hs[RR_D], hs[RR_P]) / ctx->npolar);
         if (eps > ctx->poleps) status = AMG_ERR_NO_CONVERGE;
     } else {
-        iters = 0;
+        iters = ctx->poltyp == AMG_POL_OPT ? ctx->optorder : 0;
     }
     auto fetch = [&](double* dst, const double* src, size_t cnt) {
         if (!dst) return;
@@ -1402,7 +1476,8 @@ void release(amg_ctx* ctx) {
     double** dbl[] = {&ctx->pole13, &ctx->pol, &ctx->thole, &ctx->pdamp, &ctx->xyz, &ctx->rp10, &ctx->Ed, &ctx->Ep,
                       &ctx->ud, &ctx->up, &ctx->rd, &ctx->rp, &ctx->zd, &ctx->zp, &ctx->pd, &ctx->pp, &ctx->Apd,
                       &ctx->App, &ctx->Fd, &ctx->Fp, &ctx->resd, &ctx->scal, &ctx->eacc, &ctx->grad_m, &ctx->grad_p,
-                      &ctx->trq_m, &ctx->trq_p, &ctx->aem, &ctx->aep, &ctx->phiM, &ctx->phiU, &ctx->phiU4};
+                      &ctx->trq_m, &ctx->trq_p, &ctx->aem, &ctx->aep, &ctx->phiM, &ctx->phiU, &ctx->phiU4,
+                      &ctx->uopt};
     for (double** p : dbl) dfree(*p);
     int** ints[] = {&ctx->zax, &ctx->xax, &ctx->yax, &ctx->axe, &ctx->mol, &ctx->ids, &ctx->sids, &ctx->cstart,
                     &ctx->cend, &ctx->nbr, &ctx->nnb, &ctx->overflow, &ctx->xoff, &ctx->xidx};
@@ -1494,6 +1569,13 @@ int create_impl(amg_ctx* ctx, const amg_params* P) {
     CK(cudaMemset(ctx->iter, 0, sizeof(int)));
     if (ctx->has_pol)
         for (int i = 0; i < n; i++) ctx->npolar += P->polarity[i] > 0;
+    if (ctx->poltyp == AMG_POL_OPT) {  // src/md/kpolar.cpp:226-236 restated
+        for (int k = 1; k <= AMG_MAX_OPT; k++)
+            if (P->opt_coef[k] != 0.0) ctx->optorder = k;
+        for (int k = 0; k <= ctx->optorder; k++)
+            for (int j = k; j <= ctx->optorder; j++) ctx->copm.c[k] += P->opt_coef[j];
+        dalloc(ctx, ctx->uopt, (size_t)(ctx->optorder + 1) * 6 * n + 3 * (size_t)n);
+    }
     for (auto& e : ctx->ev) CK(cudaEventCreate(&e));
     upload(ctx, ctx->pole13, P->pole, 13 * (size_t)n);
     upload(ctx, ctx->zax, P->zaxis, n);
@@ -1587,7 +1669,15 @@ int validate(const amg_params* P, std::string& why) {
         why = "polarization needs thole and pdamp";
         return AMG_ERR_BAD_ARG;
     }
-    if (P->poltyp != AMG_POL_NONE && P->poltyp != AMG_POL_MUTUAL && P->poltyp != AMG_POL_DIRECT) {
+    if (P->poltyp == AMG_POL_OPT) {
+        int order = 0;
+        for (int k = 1; k <= AMG_MAX_OPT; k++)
+            if (P->opt_coef[k] != 0.0) order = k;
+        if (order < 1) {
+            why = "OPT needs a nonzero coefficient of order 1 or more";
+            return AMG_ERR_BAD_ARG;
+        }
+    } else if (P->poltyp != AMG_POL_NONE && P->poltyp != AMG_POL_MUTUAL && P->poltyp != AMG_POL_DIRECT) {
         why = "unknown polarization model";
         return AMG_ERR_UNSUPPORTED;
     }
@@ -1872,6 +1962,10 @@ int amg_backward(amg_ctx* ctx, const amg_cotangents* cot, amg_param_grads* grads
     if (!ctx->have_forward) {
         ctx->err = "amg_backward needs an amg_forward at the current coordinates";
         return AMG_ERR_BAD_ARG;
+    }
+    if (ctx->poltyp == AMG_POL_OPT) {
+        ctx->err = "the adjoint covers the mutual and direct models";
+        return AMG_ERR_UNSUPPORTED;
     }
     try {
         CK(cudaSetDevice(ctx->device));

@@ -366,14 +366,25 @@ __global__ void k_recip_mpole(int n, const double* __restrict__ rp10, const doub
 //   torque  = torque(M_i, (phi_d + phi_p)/2) + (selfc/2) d_i x (ud + up)_i
 // and, into vir when set, the multipole terms of the reciprocal virial of
 //   G = 1/2 [U(up, M) + U(ud, M) + U(up, ud)].
+// ddonly: the dipole-dipole part alone, 1/2 U(up, ud) (the OPT cross terms).
 __global__ void k_recip_polar(int n, const double* __restrict__ rp10, const double* __restrict__ phiM,
                               const double* __restrict__ phid, const double* __restrict__ phip,
                               const double* __restrict__ ud, const double* __restrict__ up, int mutual,
-                              double selfc, double f, double* __restrict__ grad, double* __restrict__ trq,
-                              double* __restrict__ vir) {
+                              int ddonly, double selfc, double f, double* __restrict__ grad,
+                              double* __restrict__ trq, double* __restrict__ vir) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double w[6] = {0, 0, 0, 0, 0, 0};
-    if (i < n) {
+    if (i < n && ddonly) {
+        const double* pd = phid + 20 * (size_t)i;
+        const double* pp = phip + 20 * (size_t)i;
+        V3<double> udi = ld3(ud, i), upi = ld3(up, i);
+        V3<double> g = (0.5 * f) * (dipole_gradient(upi, pd) + dipole_gradient(udi, pp));
+        grad[3 * i] += g.x; grad[3 * i + 1] += g.y; grad[3 * i + 2] += g.z;
+        if (vir) {
+            vir_dipole(w, upi, pd, 0.5 * f);
+            vir_dipole(w, udi, pp, 0.5 * f);
+        }
+    } else if (i < n) {
         const double* m = rp10 + 10 * i;
         const double* pm = phiM + 20 * (size_t)i;
         const double* pd = phid + 20 * (size_t)i;
@@ -400,6 +411,49 @@ __global__ void k_recip_polar(int n, const double* __restrict__ rp10, const doub
         }
     }
     if (vir) block_vir_add(w, vir);
+}
+
+// ---------------------------------------------------------------- OPT
+// Extrapolated perturbation theory: u^(0) = alpha E, u^(k) = alpha T u^(k-1),
+// u = sum_k copm_k u^(k) for both sets.  uo: [K+1][2][3n] (d then p).
+struct OptCoef {
+    double c[8];
+};
+
+// u^(0) from the direct dipoles (ud, up), which become copm_0 u^(0)
+__global__ void k_opt_init(int n3, double c0, double* __restrict__ ud, double* __restrict__ up,
+                           double* __restrict__ u0d, double* __restrict__ u0p) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n3) return;
+    u0d[t] = ud[t];
+    u0p[t] = up[t];
+    ud[t] *= c0;
+    up[t] *= c0;
+}
+
+// u^(k) = alpha T v = v - alpha (A v), A v = v/alpha - T v; u += c u^(k)
+__global__ void k_opt_step(int n3, const double* __restrict__ pol, const double* __restrict__ vd,
+                           const double* __restrict__ vp, const double* __restrict__ Ad, const double* __restrict__ Ap,
+                           double c, double* __restrict__ od, double* __restrict__ op, double* __restrict__ ud,
+                           double* __restrict__ up) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n3) return;
+    const double a = pol[t / 3];
+    const double d = vd[t] - a * Ad[t], p = vp[t] - a * Ap[t];
+    od[t] = d;
+    op[t] = p;
+    ud[t] += c * d;
+    up[t] += c * p;
+}
+
+// V_b = sum_{a + b + 1 <= K} copm_{a+b+1} up^(a): the p-side partner of
+// ud^(b) in the dipole-dipole force terms
+__global__ void k_opt_cross(int n3, int K, int b, OptCoef cm, const double* __restrict__ uo, double* __restrict__ out) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n3) return;
+    double v = 0;
+    for (int a = 0; a + b + 1 <= K; a++) v += cm.c[a + b + 1] * uo[(size_t)(2 * a + 1) * n3 + t];
+    out[t] = v;
 }
 
 // ---------------------------------------------------------------- torque

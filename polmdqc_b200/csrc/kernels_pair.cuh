@@ -200,8 +200,10 @@ __global__ void __launch_bounds__(128) k_mpole_pair(int n, const int* __restrict
 //   G = E(M_i, ubar_k) + E(ubar_i, M_k) + 1/2 [E(up_i, ud_k) + E(ud_i, up_k)]
 // with ubar = (ud + up)/2; dG/dx_i = -dG/dr, torque on M_i from ubar_k.
 // u4: [n][2] R4, d set then p set per site.  VIR: the pair virial into
-// vir (six sums), half of dG/dr (x) r per directed pair.
-template <class R, bool EWALD, int LPA, bool VIR>
+// vir (six sums), half of dG/dr (x) r per directed pair.  DDONLY: only the
+// dipole-dipole term 1/2 [E(up_i, ud_k) + E(ud_i, up_k)] (the OPT cross
+// terms between perturbation orders; no torques).
+template <class R, bool EWALD, int LPA, bool VIR, bool DDONLY = false>
 __global__ void __launch_bounds__(128) k_polar_pair(int n, const int* __restrict__ order, const AtomR<R>* __restrict__ at,
                                                     const R4<R>* __restrict__ u4, Box bx, R aewald,
                                                     const int* __restrict__ nbr, int cap,
@@ -228,22 +230,27 @@ __global__ void __launch_bounds__(128) k_polar_pair(int n, const int* __restrict
         bulk_radial<R, EWALD, true>(dot(r, r), aewald, Ai.e.y * Aj.e.y, pair_thole<R>(Ai.e.z, Aj.e.z), B);
         R4<R> udk4 = u4[2 * j], upk4 = u4[2 * j + 1];
         V3<R> udk = v3<R>(udk4.x, udk4.y, udk4.z), upk = v3<R>(upk4.x, upk4.y, upk4.z);
-        V3<R> ubk = R(0.5) * (udk + upk);
-        Mpole<R> Mk = load_mpole(Aj);
-        SiteInv<R> si = invariants(Mi, r), sk = invariants(Mk, r);
-        V3<R> d1, ti;
-        md_pair<R>(Mi, si, ubk, r, B, d1, ti);
-        V3<R> dEdr = d1 + dm_pair<R>(ubi, Mk, sk, r, B);
-        if (mutual) dEdr = dEdr + R(0.5) * (dd_pair<R>(upi, udk, r, B) + dd_pair<R>(udi, upk, r, B));
+        V3<R> dEdr;
+        if constexpr (DDONLY) {
+            dEdr = R(0.5) * (dd_pair<R>(upi, udk, r, B) + dd_pair<R>(udi, upk, r, B));
+        } else {
+            V3<R> ubk = R(0.5) * (udk + upk);
+            Mpole<R> Mk = load_mpole(Aj);
+            SiteInv<R> si = invariants(Mi, r), sk = invariants(Mk, r);
+            V3<R> d1, ti;
+            md_pair<R>(Mi, si, ubk, r, B, d1, ti);
+            dEdr = d1 + dm_pair<R>(ubi, Mk, sk, r, B);
+            if (mutual) dEdr = dEdr + R(0.5) * (dd_pair<R>(upi, udk, r, B) + dd_pair<R>(udi, upk, r, B));
+            t = t + ti;
+        }
         g = g - dEdr;
-        t = t + ti;
         if (VIR) vir_outer(w, dEdr.x, dEdr.y, dEdr.z, r.x, r.y, r.z, 0.5 * f);
     }
     double gx = group_sum<LPA>((double)g.x), gy = group_sum<LPA>((double)g.y), gz = group_sum<LPA>((double)g.z);
     double tx = group_sum<LPA>((double)t.x), ty = group_sum<LPA>((double)t.y), tz = group_sum<LPA>((double)t.z);
     if (lane == 0 && gi_ < n) {
         grad[3 * i] += f * gx; grad[3 * i + 1] += f * gy; grad[3 * i + 2] += f * gz;
-        trq[3 * i] += f * tx; trq[3 * i + 1] += f * ty; trq[3 * i + 2] += f * tz;
+        if (!DDONLY) { trq[3 * i] += f * tx; trq[3 * i + 1] += f * ty; trq[3 * i + 2] += f * tz; }
     }
     if (VIR) block_vir_add(w, vir);
 }
@@ -669,7 +676,7 @@ __device__ __forceinline__ void scaled_polar_pair(const ScaledPair& P, const dou
                                                   const double* __restrict__ rp10, const double* __restrict__ pdamp,
                                                   const double* __restrict__ thole, Box bx, double cut2, double aewald,
                                                   const double* __restrict__ ud, const double* __restrict__ up,
-                                                  int mutual, double f, double* __restrict__ grad,
+                                                  int mutual, int ddonly, double f, double* __restrict__ grad,
                                                   double* __restrict__ trq, double (&w)[6]) {
     ScaledGeom G = scaled_geom(P, xyz, pdamp, thole, bx, cut2, aewald);
     if (!G.inside) return;
@@ -685,20 +692,22 @@ __device__ __forceinline__ void scaled_polar_pair(const ScaledPair& P, const dou
     SiteInv<double> si_m = invariants(Mi, mr), sk_m = invariants(Mk, mr);
     V3<double> dEdr = v3<double>(0, 0, 0), tqi = v3<double>(0, 0, 0), tqk = v3<double>(0, 0, 0);
     V3<double> d1, t1;
-    // d channel: (M_i, up_k) and (up_i, M_k)
-    md_pair<double>(Mi, si, upk, r, Bd, d1, t1);
-    dEdr = dEdr + d1;
-    tqi = tqi + t1;
-    md_pair<double>(Mk, sk_m, upi, mr, Bd, d1, t1);   // E(M_k, up_i) seen from k: dE/d(x_i - x_k)
-    dEdr = dEdr - d1;
-    tqk = tqk + t1;
-    // p channel: (M_i, ud_k) and (ud_i, M_k)
-    md_pair<double>(Mi, si, udk, r, Bp, d1, t1);
-    dEdr = dEdr + d1;
-    tqi = tqi + t1;
-    md_pair<double>(Mk, sk_m, udi, mr, Bp, d1, t1);
-    dEdr = dEdr - d1;
-    tqk = tqk + t1;
+    if (!ddonly) {  // ddonly: only the dipole-dipole term (OPT cross terms)
+        // d channel: (M_i, up_k) and (up_i, M_k)
+        md_pair<double>(Mi, si, upk, r, Bd, d1, t1);
+        dEdr = dEdr + d1;
+        tqi = tqi + t1;
+        md_pair<double>(Mk, sk_m, upi, mr, Bd, d1, t1);   // E(M_k, up_i) seen from k: dE/d(x_i - x_k)
+        dEdr = dEdr - d1;
+        tqk = tqk + t1;
+        // p channel: (M_i, ud_k) and (ud_i, M_k)
+        md_pair<double>(Mi, si, udk, r, Bp, d1, t1);
+        dEdr = dEdr + d1;
+        tqi = tqi + t1;
+        md_pair<double>(Mk, sk_m, udi, mr, Bp, d1, t1);
+        dEdr = dEdr - d1;
+        tqk = tqk + t1;
+    }
     if (mutual) dEdr = dEdr + dd_pair<double>(upi, udk, r, Bu) + dd_pair<double>(udi, upk, r, Bu);
     dEdr = 0.5 * dEdr;
     add3(grad, i, (-f) * dEdr);
@@ -712,11 +721,13 @@ __device__ __forceinline__ void scaled_polar_pair(const ScaledPair& P, const dou
 __global__ void k_scaled_polar(int np, const ScaledPair* __restrict__ sp, const double* __restrict__ xyz,
                                const double* __restrict__ rp10, const double* __restrict__ pdamp,
                                const double* __restrict__ thole, Box bx, double cut2, double aewald,
-                               const double* __restrict__ ud, const double* __restrict__ up, int mutual, double f,
-                               double* __restrict__ grad, double* __restrict__ trq, double* __restrict__ vir) {
+                               const double* __restrict__ ud, const double* __restrict__ up, int mutual, int ddonly,
+                               double f, double* __restrict__ grad, double* __restrict__ trq,
+                               double* __restrict__ vir) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     double w[6] = {0, 0, 0, 0, 0, 0};
-    if (t < np) scaled_polar_pair(sp[t], xyz, rp10, pdamp, thole, bx, cut2, aewald, ud, up, mutual, f, grad, trq, w);
+    if (t < np)
+        scaled_polar_pair(sp[t], xyz, rp10, pdamp, thole, bx, cut2, aewald, ud, up, mutual, ddonly, f, grad, trq, w);
     if (vir) block_vir_add(w, vir);
 }
 

@@ -247,9 +247,10 @@ __global__ void k_kvir_mpole(size_t ncomplex, int3 K, double3 iL, double c2, dou
 // over the full grid: z is the transform of the dipole grid Q_d + i Q_p (so
 // S_d(m) = (z(m) + conj z(-m))/2, S_p(m) = (z(m) - conj z(-m))/(2i)), sM the
 // saved half-complex transform of the permanent grid, G the influence
-// function on the full grid.
+// function on the full grid.  mterms 0: the U(up, ud) term alone (OPT cross
+// terms).
 template <class R>
-__global__ void k_kvir_polar(size_t npts, int3 K, double3 iL, double c2, double f, int mutual,
+__global__ void k_kvir_polar(size_t npts, int3 K, double3 iL, double c2, double f, int mutual, int mterms,
                              const R* __restrict__ G, const typename Cplx<R>::type* __restrict__ z,
                              const typename Cplx<R>::type* __restrict__ sM, double* __restrict__ vir) {
     const int K3h = K.z / 2 + 1;
@@ -274,7 +275,7 @@ __global__ void k_kvir_polar(size_t npts, int3 K, double3 iL, double c2, double 
             mx = m.x;
             my = -(double)m.y;
         }
-        double x = mx * (px + dx) + my * (py + dy);
+        double x = mterms ? mx * (px + dx) + my * (py + dy) : 0.0;
         if (mutual) x += px * dx + py * dy;
         const int ma = a <= K.x / 2 ? a : a - K.x, mb = b <= K.y / 2 ? b : b - K.y, mc = c <= K.z / 2 ? c : c - K.z;
         kvir_point(v, ma, mb, mc, iL, c2, 0.5 * f * (double)G[t] * x);

@@ -18,6 +18,18 @@ from .prm import COULOMB, DEBYE
 from .systems import System
 
 
+# OPT extrapolation coefficients copt_0..copt_k per order, the reference's
+# table (src/md/kpolar.cpp:115-153)
+OPT_COEF = {
+    1: (0.530, 0.604),
+    2: (0.042, 0.635, 0.414),
+    3: (-0.132, 0.218, 0.637, 0.293),
+    4: (-0.071, -0.096, 0.358, 0.587, 0.216),
+    5: (-0.005, -0.129, -0.026, 0.465, 0.528, 0.161),
+    6: (0.014, -0.041, -0.172, 0.073, 0.535, 0.467, 0.122),
+}
+
+
 @dataclasses.dataclass
 class Settings:
     use_ewald: bool = True
@@ -32,6 +44,7 @@ class Settings:
     pcg_guess: bool = True
     pcg_prec: bool = True             # sparse preconditioner within usolvcut (reference default)
     usolvcut: float = 4.5             # Angstrom
+    opt_order: int = 4                # poltyp POL_OPT: OPT1..OPT6 (the reference's "OPT" is OPT4)
     electric: float = COULOMB
     dielec: float = 1.0
     device: int = 0
@@ -85,6 +98,9 @@ class Params:
         p.device = st.device
         p.pcg_prec = int(st.pcg_prec)
         p.usolvcut = st.usolvcut
+        if st.poltyp == abi.POL_OPT:
+            for k, c in enumerate(OPT_COEF[st.opt_order]):
+                p.opt_coef[k] = c
         self.struct = p
         self.n = s.n
 

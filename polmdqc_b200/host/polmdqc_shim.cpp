@@ -41,6 +41,7 @@
 #include "pme.h"
 #include "polar.h"
 #include "polgrp.h"
+#include "polopt.h"
 #include "polpcg.h"
 #include "polpot.h"
 #include "potent.h"
@@ -149,7 +150,9 @@ void ensure_context(bool want_polar)
         dev.g14 = csr(n, [](int i) { return np14[i]; }, [](int i, int j) { return ip14[i][j]; });
         p.polarity = dev.polar_.data(); p.thole = dev.thole_.data(); p.pdamp = dev.pdamp_.data();
         p.ip11 = dev.g11.view(); p.ip12 = dev.g12.view(); p.ip13 = dev.g13.view(); p.ip14 = dev.g14.view();
-        p.poltyp = poltyp == "DIRECT" ? AMG_POL_DIRECT : AMG_POL_MUTUAL;
+        p.poltyp = poltyp == "DIRECT" ? AMG_POL_DIRECT : poltyp == "OPT" ? AMG_POL_OPT : AMG_POL_MUTUAL;
+        if (poltyp == "OPT")
+            for (int k = 0; k <= maxopt && k <= AMG_MAX_OPT; k++) p.opt_coef[k] = copt[k];
     } else {
         p.poltyp = AMG_POL_NONE;
     }

@@ -197,6 +197,28 @@ def test_virial_matches_oracle(w216, prec):
     assert np.abs(g.dem - o.dem).max() < (1e-8 if prec == FP64 else 1e-3)
 
 
+@pytest.mark.parametrize("prec,order", [(FP64, 4), (FP64, 1), (MIXED, 4)])
+def test_opt_polarization_matches_oracle(w216, prec, order):
+    """OPT (extrapolated perturbation theory, the reference's kpolar
+    coefficients): orders u^(k) by repeated dipole-field applications, their
+    mix, and the forces with the dipole-dipole terms between every pair of
+    orders (real, scaled and reciprocal), plus the virial."""
+    st = Settings(nfft=(24, 24, 24), precision=prec, poltyp=abi.POL_OPT, opt_order=order)
+    flags = ALL | abi.DO_VIRIAL
+    o = oracle.forward(w216, Settings(nfft=(24, 24, 24), precision=FP64, poltyp=abi.POL_OPT, opt_order=order),
+                       flags=flags)
+    g = run(w216, st, flags)
+    tol = 1e-10 if prec == FP64 else 1e-6
+    assert g.pcg_iters == order
+    assert rel(g.em, o.em) < tol and rel(g.ep, o.ep) < tol
+    assert np.abs(g.uind - o.uind).max() < (1e-10 if prec == FP64 else 1e-5)
+    if prec == FP64:
+        assert np.abs(g.dep - o.dep).max() < 1e-8
+    else:
+        assert frms(g, o) < 1e-4
+    assert np.abs(g.vir - o.vir).max() < (1e-8 if prec == FP64 else 1e-5) * np.abs(o.vir).max()
+
+
 def test_virial_non_ewald_polarization_matches_oracle():
     s = systems.water_box(64, 12.4, seed=5)
     st = Settings(use_ewald=False, cutoff=6.0, precision=FP64, poleps=1e-9)

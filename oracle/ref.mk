@@ -80,8 +80,10 @@ $(OUT)/ref_dump: oracle/ref_dump.cpp $(OUT)/libpolmdqc.a
 # to the build so that runs on another machine can find them.
 $(OUT)/data.stamp: $(wildcard $(REF)/params/*.prm)
 	@mkdir -p $(OUT)/params $(OUT)/testFiles
-	cp $(REF)/params/water03.prm $(REF)/params/amoebabio09.prm $(REF)/params/amoebabio18.prm $(OUT)/params/
-	cp -r $(REF)/test/testFiles/amoeba $(REF)/test/testFiles/bounds $(REF)/test/testFiles/rotpole $(OUT)/testFiles/
+	cp $(REF)/params/water03.prm $(REF)/params/amoebabio09.prm $(REF)/params/amoebabio18.prm \
+	   $(REF)/params/amoebaplus.prm $(OUT)/params/
+	cp -r $(REF)/test/testFiles/amoeba $(REF)/test/testFiles/bounds $(REF)/test/testFiles/rotpole \
+	   $(REF)/test/testFiles/amoebap $(OUT)/testFiles/
 	touch $@
 
 .PHONY: all shim

@@ -185,6 +185,14 @@ template <CalcMode M>
 void evaluate(bool fill_mpole, bool fill_polar)
 {
     constexpr CalcFlag flags = getCalculationFlags<M>();
+    // charge penetration (pairMpoleCP, include/md/pairMpole.h:186-389) and
+    // charge flux (dcflux) are not on the GPU: stop, as the reference's
+    // fatal() does, rather than return plain multipole energies
+    if (pentype != PenTyp::None || use_chgflx) {
+        printf("\n AMOEBA GPU  --  charge penetration / charge flux are not supported (status %d)\n",
+               AMG_ERR_UNSUPPORTED);
+        fatal();
+    }
     const bool want_polar = use_polar && polarity.size() >= n;
     ensure_context(want_polar);
     std::vector<double> xyz(3 * (size_t)n);

@@ -105,6 +105,11 @@ struct System {
     // 2 triclinic, 3 truncated octahedron, 4 rhombic dodecahedron
     int shape = 0;
     double bsin = 1, bcos = 0, gsin = 1, gcos = 0, bterm = 0, gterm = 1;
+    // lattice vectors as rows (a along x, b in the xy plane; src/md/lattice.cpp:
+    // 122-140), their inverse Ri (fractional f = x Ri, reciprocal vectors as
+    // its columns) and the cell volume
+    double A[3][3] = {}, Ri[3][3] = {};
+    double vol = 0;
     double alpha = 0, cut = 0, f = 0;
     int K[3] = {0, 0, 0}, order = 5;
     int poltyp = AMG_POL_NONE;
@@ -599,6 +604,11 @@ std::vector<Pair> build_pairs(const System& s) {
 struct Pme {
     int K[3], p;
     double L[3], V;
+    double Mf[3][3];  // d/dx_i = sum_j Mf[i][j] d/du_j (grid units u)
+    double Ri[3][3];  // inverse lattice: reciprocal vectors as columns
+    void recip_vec(int m0, int m1, int m2, double h[3]) const {
+        for (int i = 0; i < 3; i++) h[i] = Ri[i][0] * m0 + Ri[i][1] * m1 + Ri[i][2] * m2;
+    }
     std::vector<double> bsmod[3];
     // per-atom stencils
     std::vector<int> k0;               // [n*3] first grid index (may be negative -> wrap)
@@ -619,7 +629,11 @@ double bspline_deriv(int order, int d, double x) {  // d-th derivative of M_orde
 void pme_setup(const System& s, Pme& pm) {
     pm.p = s.order;
     for (int a = 0; a < 3; a++) { pm.K[a] = s.K[a]; pm.L[a] = s.L[a]; }
-    pm.V = s.L[0] * s.L[1] * s.L[2];
+    pm.V = s.vol;
+    std::memcpy(pm.Ri, s.Ri, sizeof(pm.Ri));
+    // d/dx_i = sum_j Mf[i][j] d/du_j with u_j = K_j f_j
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) pm.Mf[i][j] = s.Ri[i][j] * s.K[j];
     for (int a = 0; a < 3; a++) {
         int K = pm.K[a];
         pm.bsmod[a].assign(K, 0.0);
@@ -639,7 +653,7 @@ void pme_setup(const System& s, Pme& pm) {
     for (int i = 0; i < s.n; i++) {
         double xs[3] = {s.x[i].x, s.x[i].y, s.x[i].z};
         for (int a = 0; a < 3; a++) {
-            double f = xs[a] / s.L[a];
+            double f = xs[0] * s.Ri[0][a] + xs[1] * s.Ri[1][a] + xs[2] * s.Ri[2][a];
             f -= std::floor(f);
             double u = f * pm.K[a];
             int fl = (int)std::floor(u);
@@ -651,6 +665,33 @@ void pme_setup(const System& s, Pme& pm) {
                     pm.th[(((size_t)i * 3 + a) * 4 + d) * p + sidx] = bspline_deriv(p, d, arg);
             }
         }
+    }
+}
+
+// Cartesian potential derivatives from the derivatives in grid units:
+// d/dx_a = sum_j Mf[a][j] d/du_j, so an order-n Cartesian derivative is the
+// order-n grid-unit tensor contracted with Mf on every index
+void frac_to_cart(const double f[20], const double Mf[3][3], double out[20]) {
+    for (int j = 0; j < 20; j++) {
+        int ax[3], n = 0;
+        for (int a = 0; a < 3; a++)
+            for (int r = 0; r < kDer[j][a]; r++) ax[n++] = a;
+        if (n == 0) { out[j] = f[j]; continue; }
+        double v = 0;
+        const int tuples = n == 1 ? 3 : n == 2 ? 9 : 27;
+        for (int t = 0; t < tuples; t++) {
+            int cnt[3] = {0, 0, 0};
+            double w = 1;
+            int r = t;
+            for (int k = 0; k < n; k++) {
+                const int q = r % 3;
+                r /= 3;
+                cnt[q]++;
+                w *= Mf[ax[k]][q];
+            }
+            v += w * f[der_index(cnt[0], cnt[1], cnt[2])];
+        }
+        out[j] = v;
     }
 }
 
@@ -702,14 +743,23 @@ void pme_potential(const System& s, const Pme& pm, const std::vector<Mp>& M, std
     const int p = pm.p;
     const size_t G = (size_t)pm.K[0] * pm.K[1] * pm.K[2];
     std::vector<cd> grid(G, 0.0);
-    double sc[3] = {pm.K[0] / pm.L[0], pm.K[1] / pm.L[1], pm.K[2] / pm.L[2]};
+    const auto& Mf = pm.Mf;
     for (int i = 0; i < s.n; i++) {
         const Mp& m = M[i];
-        // fractional multipoles
+        // fractional multipoles: d_f = Mf^T d, Q_f = Mf^T Q Mf
         double q = m.c[0];
-        double d1 = m.c[1] * sc[0], d2 = m.c[2] * sc[1], d3 = m.c[3] * sc[2];
-        double q11 = m.c[4] * sc[0] * sc[0], q22 = m.c[7] * sc[1] * sc[1], q33 = m.c[9] * sc[2] * sc[2];
-        double q12 = 2 * m.c[5] * sc[0] * sc[1], q13 = 2 * m.c[6] * sc[0] * sc[2], q23 = 2 * m.c[8] * sc[1] * sc[2];
+        const double dc[3] = {m.c[1], m.c[2], m.c[3]};
+        const double Qc[3][3] = {{m.c[4], m.c[5], m.c[6]}, {m.c[5], m.c[7], m.c[8]}, {m.c[6], m.c[8], m.c[9]}};
+        double df[3] = {0, 0, 0}, Qf[3][3] = {};
+        for (int j = 0; j < 3; j++)
+            for (int a = 0; a < 3; a++) df[j] += dc[a] * Mf[a][j];
+        for (int j = 0; j < 3; j++)
+            for (int k = 0; k < 3; k++)
+                for (int a = 0; a < 3; a++)
+                    for (int b = 0; b < 3; b++) Qf[j][k] += Mf[a][j] * Qc[a][b] * Mf[b][k];
+        double d1 = df[0], d2 = df[1], d3 = df[2];
+        double q11 = Qf[0][0], q22 = Qf[1][1], q33 = Qf[2][2];
+        double q12 = 2 * Qf[0][1], q13 = 2 * Qf[0][2], q23 = 2 * Qf[1][2];
         for (int a = 0; a < p; a++) {
             double t0 = theta(pm, i, 0, 0, a), t1 = theta(pm, i, 0, 1, a), t2 = theta(pm, i, 0, 2, a);
             for (int b = 0; b < p; b++) {
@@ -735,8 +785,9 @@ void pme_potential(const System& s, const Pme& pm, const std::vector<Mp>& M, std
                 int ma = a <= pm.K[0] / 2 ? a : a - pm.K[0];
                 int mb = b <= pm.K[1] / 2 ? b : b - pm.K[1];
                 int mc = c <= pm.K[2] / 2 ? c : c - pm.K[2];
-                double hx = ma / pm.L[0], hy = mb / pm.L[1], hz = mc / pm.L[2];
-                double h2 = hx * hx + hy * hy + hz * hz;
+                double h[3];
+                pm.recip_vec(ma, mb, mc, h);
+                double h2 = h[0] * h[0] + h[1] * h[1] + h[2] * h[2];
                 double g = pref * std::exp(-kPi * kPi * h2 / (s.alpha * s.alpha)) / h2 /
                            (pm.bsmod[0][a] * pm.bsmod[1][b] * pm.bsmod[2][c]);
                 grid[id] *= g;
@@ -755,10 +806,7 @@ void pme_potential(const System& s, const Pme& pm, const std::vector<Mp>& M, std
                         f[j] += theta(pm, i, 0, e[0], a) * theta(pm, i, 1, e[1], b) * theta(pm, i, 2, e[2], c) * val;
                     }
                 }
-        for (int j = 0; j < 20; j++) {
-            const int* e = kDer[j];
-            phi[20 * (size_t)i + j] = f[j] * std::pow(sc[0], e[0]) * std::pow(sc[1], e[1]) * std::pow(sc[2], e[2]);
-        }
+        frac_to_cart(f, Mf, &phi[20 * (size_t)i]);
     }
 }
 
@@ -783,7 +831,8 @@ void pme_kvir(const System& s, const Pme& pm, const std::vector<cd>& SX, const s
                 int ma = a <= pm.K[0] / 2 ? a : a - pm.K[0];
                 int mb = b <= pm.K[1] / 2 ? b : b - pm.K[1];
                 int mc = c <= pm.K[2] / 2 ? c : c - pm.K[2];
-                double h[3] = {ma / pm.L[0], mb / pm.L[1], mc / pm.L[2]};
+                double h[3];
+                pm.recip_vec(ma, mb, mc, h);
                 double h2 = h[0] * h[0] + h[1] * h[1] + h[2] * h[2];
                 double g = pref * std::exp(-c2 * h2) / h2 / (pm.bsmod[0][a] * pm.bsmod[1][b] * pm.bsmod[2][c]);
                 double e = g * (SX[id] * std::conj(SY[id])).real();
@@ -816,14 +865,19 @@ void mpole_virial(const Mp& X, const double* p, double W[3][3]) {
 // derivatives at each site from all multipoles, |k| up to kmax (1/Angstrom).
 void kspace_potential(const System& s, const std::vector<Mp>& M, double kmax, std::vector<double>& phi) {
     phi.assign((size_t)s.n * 20, 0.0);
-    double V = s.L[0] * s.L[1] * s.L[2];
+    double V = s.vol;
     int mm[3];
-    for (int a = 0; a < 3; a++) mm[a] = (int)std::ceil(kmax * s.L[a] / (2 * kPi));
+    for (int a = 0; a < 3; a++) {
+        const double len = std::sqrt(s.A[a][0] * s.A[a][0] + s.A[a][1] * s.A[a][1] + s.A[a][2] * s.A[a][2]);
+        mm[a] = (int)std::ceil(kmax * len / (2 * kPi));  // |k . a_j| = 2 pi |m_j| <= kmax |a_j|
+    }
     for (int a = -mm[0]; a <= mm[0]; a++)
         for (int b = -mm[1]; b <= mm[1]; b++)
             for (int c = -mm[2]; c <= mm[2]; c++) {
                 if (!a && !b && !c) continue;
-                V3 k{2 * kPi * a / s.L[0], 2 * kPi * b / s.L[1], 2 * kPi * c / s.L[2]};
+                V3 k{2 * kPi * (s.Ri[0][0] * a + s.Ri[0][1] * b + s.Ri[0][2] * c),
+                     2 * kPi * (s.Ri[1][0] * a + s.Ri[1][1] * b + s.Ri[1][2] * c),
+                     2 * kPi * (s.Ri[2][0] * a + s.Ri[2][1] * b + s.Ri[2][2] * c)};
                 double k2 = dot(k, k);
                 if (k2 > kmax * kmax) continue;
                 double gk = (4 * kPi / V) * std::exp(-k2 / (4 * s.alpha * s.alpha)) / k2;
@@ -1167,7 +1221,7 @@ void evaluate(Work& w, Flags fl, Result& R, double tol_override, int maxit_overr
             R.aem[i] += e;
             qt += m.c[0];
         }
-        double V = s.L[0] * s.L[1] * s.L[2];
+        double V = s.vol;
         double echg = -kPi * qt * qt / (2 * V * a * a);
         R.em += er + es + echg;
         for (int c = 0; c < 3; c++) R.vir[c][c] -= echg;  // echg ~ 1/V
@@ -1426,7 +1480,25 @@ int orc_forward(const amg_params* P, const double* xyz, const double box[6], int
         }
     }
     if (s.ewald && !s.bounds) return AMG_ERR_BAD_ARG;
-    if (s.ewald && s.shape != 0) return AMG_ERR_UNSUPPORTED;
+    if (s.ewald && s.shape > 2) return AMG_ERR_UNSUPPORTED;
+    if (s.bounds) {  // lattice rows and their inverse (lower triangular)
+        double (&A)[3][3] = s.A;
+        A[0][0] = s.L[0];
+        A[1][0] = s.L[1] * s.gcos;
+        A[1][1] = s.L[1] * s.gsin;
+        A[2][0] = s.L[2] * s.bcos;
+        A[2][1] = s.L[2] * s.bterm;
+        A[2][2] = s.L[2] * s.gterm;
+        double (&R)[3][3] = s.Ri;
+        R[0][0] = 1 / A[0][0];
+        R[1][1] = 1 / A[1][1];
+        R[2][2] = 1 / A[2][2];
+        R[1][0] = -A[1][0] * R[0][0] / A[1][1];
+        R[2][1] = -A[2][1] * R[1][1] / A[2][2];
+        R[2][0] = -(A[2][0] * R[0][0] + A[2][1] * R[1][0]) / A[2][2];
+        s.vol = A[0][0] * A[1][1] * A[2][2];
+        if (s.shape >= 3) s.vol *= 0.5;
+    }
     s.alpha = (opt && opt->alpha > 0) ? opt->alpha : P->aewald;
     s.cut = P->cutoff;
     s.f = P->electric / P->dielec;

@@ -90,7 +90,7 @@ struct Pme {
     typename Cplx<R>::type* zg = nullptr;    // [K1 K2 K3] spreading grid, zero between uses
     typename Cplx<R>::type* zq = nullptr;    // [K1 K2 K3] convolved potentials (d + i p)
     R* Gfull = nullptr;                      // [K1 K2 K3] influence function on the full grid
-    double infl_box[3] = {0, 0, 0};
+    double infl_box[6] = {0, 0, 0, 0, 0, 0};
     size_t G = 0, Gc = 0;
 };
 
@@ -118,6 +118,9 @@ struct amg_ctx {
     std::string err;
     double box[6] = {0, 0, 0, 90, 90, 90};
     int cell_shape = AMG_CELL_FROM_ANGLES;  // amg_params cell_shape
+    // PME lattice transform (grid units per Cartesian axis) and cell volume
+    Frac frac{};
+    double vol = 0;
     Box bx{};
     bool have_coords = false;
     int nsp = 0;
@@ -377,13 +380,14 @@ void pme_prepare(amg_ctx* ctx, Pme<R>& pm) {
         CKFFT(cufftSetStream(pm.zplan, ctx->st));
         pm.ready = true;
     }
-    if (pm.infl_box[0] != ctx->box[0] || pm.infl_box[1] != ctx->box[1] || pm.infl_box[2] != ctx->box[2]) {
+    if (!std::equal(ctx->box, ctx->box + 6, pm.infl_box)) {
         std::vector<double> b1, b2, b3;
         bsmod_axis(K1, kOrder, b1);
         bsmod_axis(K2, kOrder, b2);
         bsmod_axis(K3, kOrder, b3);
-        const double L1 = ctx->box[0], L2 = ctx->box[1], L3 = ctx->box[2], V = L1 * L2 * L3;
+        const double V = ctx->vol;
         const double pref = 1.0 / (kPi * V), a2 = ctx->aewald * ctx->aewald;
+        const Frac& F = ctx->frac;  // reciprocal vector b_j = (column j of F.m) / K_j
         std::vector<R> h(pm.Gc);
         const int K3h = K3 / 2 + 1;
         for (int a = 0; a < K1; a++)
@@ -392,7 +396,11 @@ void pme_prepare(amg_ctx* ctx, Pme<R>& pm) {
                     size_t id = ((size_t)a * K2 + b) * K3h + c;
                     if (a == 0 && b == 0 && c == 0) { h[id] = 0; continue; }
                     int ma = a <= K1 / 2 ? a : a - K1, mb = b <= K2 / 2 ? b : b - K2, mc = c;
-                    double hx = ma / L1, hy = mb / L2, hz = mc / L3;
+                    const double fa = (double)ma / K1, fb = (double)mb / K2, fc = (double)mc / K3;
+                    double hx = F.m[0][0] * fa + F.m[0][1] * fb + F.m[0][2] * fc;
+                    double hy = F.m[1][0] * fa + F.m[1][1] * fb + F.m[1][2] * fc;
+                    double hz = F.m[2][0] * fa + F.m[2][1] * fb + F.m[2][2] * fc;
+                    if (!F.general) { hx = ma / ctx->box[0]; hy = mb / ctx->box[1]; hz = mc / ctx->box[2]; }
                     double h2 = hx * hx + hy * hy + hz * hz;
                     h[id] = (R)(pref * exp(-kPi * kPi * h2 / a2) / h2 / (b1[a] * b2[b] * b3[c]));
                 }
@@ -408,7 +416,7 @@ void pme_prepare(amg_ctx* ctx, Pme<R>& pm) {
                         c < K3h ? h[((size_t)a * K2 + b) * K3h + c] : h[((size_t)a2 * K2 + b2) * K3h + (K3 - c)];
                 }
         CK(cudaMemcpy(pm.Gfull, hf.data(), sizeof(R) * pm.G, cudaMemcpyHostToDevice));
-        for (int a = 0; a < 3; a++) pm.infl_box[a] = ctx->box[a];
+        std::copy(ctx->box, ctx->box + 6, pm.infl_box);
     }
 }
 
@@ -484,6 +492,37 @@ bool set_lattice(amg_ctx* ctx, const double box[6], Box& b) {
     }
     b.gterm = std::sqrt(g2);
     return true;
+}
+
+// Lattice rows (a along x, b in the xy plane; src/md/lattice.cpp:122-140),
+// their inverse and the PME transform m[i][j] = inverse[i][j] K_j; for an
+// orthogonal box m = diag(K/L) exactly as the orthogonal kernels scale.
+void set_frac(amg_ctx* ctx) {
+    const Box& b = ctx->bx;
+    Frac& F = ctx->frac;
+    F = Frac{};
+    if (b.shape == 0) {
+        for (int a = 0; a < 3; a++) F.m[a][a] = ctx->K[a] / ctx->box[a];
+        ctx->vol = ctx->box[0] * ctx->box[1] * ctx->box[2];
+        return;
+    }
+    double A[3][3] = {}, R[3][3] = {};
+    A[0][0] = ctx->box[0];
+    A[1][0] = ctx->box[1] * b.gcos;
+    A[1][1] = ctx->box[1] * b.gsin;
+    A[2][0] = ctx->box[2] * b.bcos;
+    A[2][1] = ctx->box[2] * b.bterm;
+    A[2][2] = ctx->box[2] * b.gterm;
+    R[0][0] = 1 / A[0][0];
+    R[1][1] = 1 / A[1][1];
+    R[2][2] = 1 / A[2][2];
+    R[1][0] = -A[1][0] * R[0][0] / A[1][1];
+    R[2][1] = -A[2][1] * R[1][1] / A[2][2];
+    R[2][0] = -(A[2][0] * R[0][0] + A[2][1] * R[1][0]) / A[2][2];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) F.m[i][j] = R[i][j] * ctx->K[j];
+    F.general = 1;
+    ctx->vol = A[0][0] * A[1][1] * A[2][2] * (b.shape >= 3 ? 0.5 : 1.0);
 }
 
 // Cell grid of the neighbour-list build.  A non-orthogonal cell is one cell
@@ -650,15 +689,12 @@ void join_side(amg_ctx* ctx, cudaStream_t s) {
 template <class R>
 void pme_stencils(amg_ctx* ctx, cudaStream_t s) {
     Pme<R>& pm = pme_of<R>(ctx);
-    k_bspline<R, kOrder><<<nblk(ctx->n), kThreads, 0, s>>>(ctx->n, ctx->xyz, ctx->bx,
+    k_bspline<R, kOrder><<<nblk(ctx->n), kThreads, 0, s>>>(ctx->n, ctx->xyz, ctx->bx, ctx->frac,
                                                            make_int3(ctx->K[0], ctx->K[1], ctx->K[2]), pm.theta, pm.k0);
     KCHECK();
 }
 
-// k-space constants of the reciprocal virial: inverse box edges, pi^2/alpha^2
-inline double3 inv_edges(const amg_ctx* ctx) {
-    return make_double3(1.0 / ctx->box[0], 1.0 / ctx->box[1], 1.0 / ctx->box[2]);
-}
+// k-space constant of the reciprocal virial, pi^2/alpha^2
 inline double kvir_c2(const amg_ctx* ctx) { return kPi * kPi / (ctx->aewald * ctx->aewald); }
 
 // reciprocal potential derivatives of the permanent multipoles -> phiM [n][20];
@@ -668,16 +704,15 @@ template <class R>
 void pme_mpole(amg_ctx* ctx, cudaStream_t s, double* vir = nullptr) {
     Pme<R>& pm = pme_of<R>(ctx);
     int3 K = make_int3(ctx->K[0], ctx->K[1], ctx->K[2]);
-    double sc[3] = {ctx->K[0] / ctx->box[0], ctx->K[1] / ctx->box[1], ctx->K[2] / ctx->box[2]};
-    k_spread_mpole<R, kOrder><<<nblk(ctx->n), kThreads, 0, s>>>(ctx->n, ctx->rp10, pm.theta, pm.k0, K, (R)sc[0],
-                                                                (R)sc[1], (R)sc[2], pm.grid);
+    k_spread_mpole<R, kOrder><<<nblk(ctx->n), kThreads, 0, s>>>(ctx->n, ctx->rp10, pm.theta, pm.k0, K, ctx->frac,
+                                                                pm.grid);
     KCHECK();
     CKFFT(cufftSetStream(pm.f1, s));
     CKFFT(cufftSetStream(pm.i1, s));
     CKFFT(CufftTypes<R>::fwd(pm.f1, pm.grid, pm.cgrid));
     if (vir) {
         using C = typename Cplx<R>::type;
-        k_kvir_mpole<R><<<(unsigned)ctx->num_sms * 2, 256, 0, s>>>(pm.Gc, K, inv_edges(ctx), kvir_c2(ctx), ctx->f,
+        k_kvir_mpole<R><<<(unsigned)ctx->num_sms * 2, 256, 0, s>>>(pm.Gc, K, ctx->frac, kvir_c2(ctx), ctx->f,
                                                                    pm.infl, (const C*)pm.cgrid,
                                                                    (C*)pm.cgrid + pm.Gc, vir);
         KCHECK();
@@ -686,7 +721,7 @@ void pme_mpole(amg_ctx* ctx, cudaStream_t s, double* vir = nullptr) {
     KCHECK();
     CKFFT(CufftTypes<R>::inv(pm.i1, pm.cgrid, pm.phig));
     k_gather<R, kOrder, 20, kGatherLanes, 1><<<nblk((size_t)ctx->n * kGatherLanes), kThreads, 0, s>>>(
-        ctx->n, pm.phig, pm.theta, pm.k0, K, sc[0], sc[1], sc[2], ctx->phiM);
+        ctx->n, pm.phig, pm.theta, pm.k0, K, ctx->frac, ctx->phiM);
     KCHECK();
 }
 
@@ -700,9 +735,8 @@ template <class R>
 void spread_dipoles(amg_ctx* ctx, cudaStream_t s, const double* vd, const double* vp) {
     Pme<R>& pm = pme_of<R>(ctx);
     int3 K = make_int3(ctx->K[0], ctx->K[1], ctx->K[2]);
-    double sc[3] = {ctx->K[0] / ctx->box[0], ctx->K[1] / ctx->box[1], ctx->K[2] / ctx->box[2]};
-    k_spread_dipoles<R, kOrder><<<ctx->n, 128, 0, s>>>(ctx->n, ctx->sids, vd, vp, pm.theta, pm.k0, K, (R)sc[0],
-                                                        (R)sc[1], (R)sc[2], pm.zg);
+    k_spread_dipoles<R, kOrder><<<ctx->n, 128, 0, s>>>(ctx->n, ctx->sids, vd, vp, pm.theta, pm.k0, K, ctx->frac,
+                                                        pm.zg);
     KCHECK();
 }
 
@@ -721,7 +755,7 @@ void pme_dipole_grids(amg_ctx* ctx, cudaStream_t s, const double* vd, const doub
     if (vir) {
         using C = typename Cplx<R>::type;
         k_kvir_polar<R><<<(unsigned)ctx->num_sms * 2, 256, 0, s>>>(
-            pm.G, make_int3(ctx->K[0], ctx->K[1], ctx->K[2]), inv_edges(ctx), kvir_c2(ctx), ctx->f,
+            pm.G, make_int3(ctx->K[0], ctx->K[1], ctx->K[2]), ctx->frac, kvir_c2(ctx), ctx->f,
             mterms ? ctx->poltyp == AMG_POL_MUTUAL : 1, mterms, pm.Gfull, pm.zg, (const C*)pm.cgrid + pm.Gc, vir);
         KCHECK();
     }
@@ -736,10 +770,9 @@ void pme_dipoles(amg_ctx* ctx, cudaStream_t s, const double* vd, const double* v
                  double* vir = nullptr, bool mterms = true) {
     Pme<R>& pm = pme_of<R>(ctx);
     int3 K = make_int3(ctx->K[0], ctx->K[1], ctx->K[2]);
-    double sc[3] = {ctx->K[0] / ctx->box[0], ctx->K[1] / ctx->box[1], ctx->K[2] / ctx->box[2]};
     pme_dipole_grids<R>(ctx, s, vd, vp, true, vir, mterms);
     k_gather<R, kOrder, NC, kGatherLanes, 2><<<nblk((size_t)ctx->n * kGatherLanes), kThreads, 0, s>>>(
-        ctx->n, pm.zq, pm.theta, pm.k0, K, sc[0], sc[1], sc[2], phi);
+        ctx->n, pm.zq, pm.theta, pm.k0, K, ctx->frac, phi);
     KCHECK();
 }
 
@@ -749,6 +782,9 @@ double self_coef(const amg_ctx* ctx) {
     double a = ctx->aewald;
     return ctx->ewald ? 4.0 * a * a * a / (3.0 * kSqrtPi) : 0.0;
 }
+
+// Ewald in a monoclinic or triclinic cell: the pair kernels' CELLS instances
+bool ewald_cells(const amg_ctx* ctx) { return ctx->ewald && ctx->bx.shape != 0; }
 
 // A v for both dipole sets (v/alpha - field of v), pair tensors computed on
 // the fly (FP64 correction sweep)
@@ -761,7 +797,10 @@ void matvec(amg_ctx* ctx, cudaStream_t s, const double* vd, const double* vp, do
     // real space on the side stream, PME on s
     cudaStream_t r = ctx->ewald ? fork_side(ctx, s) : s;
     LPA_DISPATCH(ctx->lpa, {
-        if (ctx->ewald)
+        if (ewald_cells(ctx))
+            k_Tu<R, true, 8, true><<<nblk((size_t)n * 8), kThreads, 0, r>>>(n, ctx->sids, A.at, A.u4, ctx->bx, (R)ctx->aewald,
+                                                                            ctx->nbr, ctx->cap, ctx->nnb, ctx->Fd, ctx->Fp);
+        else if (ctx->ewald)
             k_Tu<R, true, L><<<nblk((size_t)n * L), kThreads, 0, r>>>(n, ctx->sids, A.at, A.u4, ctx->bx, (R)ctx->aewald, ctx->nbr,
                                                                       ctx->cap, ctx->nnb, ctx->Fd, ctx->Fp);
         else
@@ -810,7 +849,11 @@ void build_tu_coeffs(amg_ctx* ctx, cudaStream_t s) {
     R4<R>* cu0 = sp ? A.cu0 : nullptr;
     R* cu1 = sp ? A.cu1 : nullptr;
     LPA_DISPATCH(ctx->lpa, {
-        if (ctx->ewald)
+        if (ewald_cells(ctx))
+            k_tu_coeffs<R, true, 8, true><<<nblk((size_t)n * 8), kThreads, 0, s>>>(n, ctx->sids, A.at, ctx->bx, (R)ctx->aewald,
+                                                                                   ctx->nbr, ctx->cap, ctx->nnb, A.c0, A.c1,
+                                                                                   (R)u2, nbru, cu0, cu1, nnbu);
+        else if (ctx->ewald)
             k_tu_coeffs<R, true, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(n, ctx->sids, A.at, ctx->bx, (R)ctx->aewald, ctx->nbr,
                                                                              ctx->cap, ctx->nnb, A.c0, A.c1, (R)u2, nbru,
                                                                              cu0, cu1, nnbu);
@@ -842,10 +885,9 @@ void matvec_stored(amg_ctx* ctx, cudaStream_t s, const R4<R>* v4, const double* 
         pme_dipole_grids<R>(ctx, s, vd, vp, spread);
         join_side(ctx, s);
         int3 K = make_int3(ctx->K[0], ctx->K[1], ctx->K[2]);
-        double sc[3] = {ctx->K[0] / ctx->box[0], ctx->K[1] / ctx->box[1], ctx->K[2] / ctx->box[2]};
         constexpr int G = 8;  // lanes per site
         const unsigned blocks = (unsigned)std::min<size_t>(nblk((size_t)n * G), (size_t)ctx->num_sms * 8);
-        k_gather_field<R, kOrder, G><<<blocks, kThreads, 0, s>>>(n, pm.zq, pm.theta, pm.k0, K, sc[0], sc[1], sc[2], vd,
+        k_gather_field<R, kOrder, G><<<blocks, kThreads, 0, s>>>(n, pm.zq, pm.theta, pm.k0, K, ctx->frac, vd,
                                                                  vp, ctx->Fd, ctx->Fp, self_coef(ctx), ctx->pol, Ad,
                                                                  Ap, vAv);
         KCHECK();
@@ -900,9 +942,7 @@ void direction(amg_ctx* ctx, cudaStream_t s) {
         Pme<R>& pm = pme_of<R>(ctx);
         const int3 K = make_int3(ctx->K[0], ctx->K[1], ctx->K[2]);
         k_pcg_dir_spread<R, kOrder><<<n, 128, 0, s>>>(n, ctx->zd, ctx->zp, ctx->pd, ctx->pp, ctx->scal, A.p4, pm.theta,
-                                                       pm.k0, K, (R)(ctx->K[0] / ctx->box[0]),
-                                                       (R)(ctx->K[1] / ctx->box[1]), (R)(ctx->K[2] / ctx->box[2]),
-                                                       pm.zg);
+                                                       pm.k0, K, ctx->frac, pm.zg);
     } else {
         k_pcg_dir<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->zd, ctx->zp, ctx->pd, ctx->pp, ctx->scal, A.p4);
     }
@@ -1029,7 +1069,10 @@ void enqueue_front(amg_ctx* ctx, cudaStream_t s) {
         };
         LPA_DISPATCH(ctx->lpa, {
             const unsigned nb = nblk((size_t)n * L);
-            if (ctx->ewald) {
+            if (ewald_cells(ctx)) {  // Ewald in a monoclinic or triclinic cell: 8 lanes
+                if (coef) launch(k_perm_field<R, true, 8, true, true>, nblk((size_t)n * 8));
+                else launch(k_perm_field<R, true, 8, false, true>, nblk((size_t)n * 8));
+            } else if (ctx->ewald) {
                 if (coef) launch(k_perm_field<R, true, L, true>, nb);
                 else launch(k_perm_field<R, true, L, false>, nb);
             } else {
@@ -1098,7 +1141,10 @@ void enqueue_opt_cross(amg_ctx* ctx, cudaStream_t s, double* virp) {
             kern<<<nblk((size_t)n * 8), kThreads, 0, s>>>(n, ctx->sids, A.at, A.u4, ctx->bx, aew, ctx->nbr, ctx->cap,
                                                           ctx->nnb, 1, ctx->f, ctx->grad_p, ctx->trq_p, virp);
         };
-        if (ctx->ewald) {
+        if (ewald_cells(ctx)) {
+            if (virp) launch(k_polar_pair<R, true, 8, true, true, true>);
+            else launch(k_polar_pair<R, true, 8, false, true, true>);
+        } else if (ctx->ewald) {
             if (virp) launch(k_polar_pair<R, true, 8, true, true>);
             else launch(k_polar_pair<R, true, 8, false, true>);
         } else {
@@ -1160,12 +1206,17 @@ void enqueue_back(amg_ctx* ctx, cudaStream_t s, int flags) {
     const bool extra = analysis || vir;
     LPA_DISPATCH(ctx->lpa, {
         const size_t nb = nblk((size_t)n * L);
-        auto launch = [&](auto kern) {
-            kern<<<nb, kThreads, 0, r>>>(n, ctx->sids, A.at, ctx->bx, aew, ctx->nbr, ctx->cap, ctx->nnb, ctx->f,
-                                         ctx->grad_m, ctx->trq_m, ctx->eacc, analysis ? ctx->aem : nullptr,
-                                         analysis ? mol : nullptr, analysis ? ctx->cnt : nullptr, vir);
+        auto launch_n = [&](auto kern, size_t blocks) {
+            kern<<<blocks, kThreads, 0, r>>>(n, ctx->sids, A.at, ctx->bx, aew, ctx->nbr, ctx->cap, ctx->nnb, ctx->f,
+                                             ctx->grad_m, ctx->trq_m, ctx->eacc, analysis ? ctx->aem : nullptr,
+                                             analysis ? mol : nullptr, analysis ? ctx->cnt : nullptr, vir);
         };
-        if (ctx->ewald) {
+        auto launch = [&](auto kern) { launch_n(kern, nb); };
+        auto launch_cells = [&](auto kern) { launch_n(kern, nblk((size_t)n * 8)); };
+        if (ewald_cells(ctx)) {
+            if (extra) launch_cells(k_mpole_pair<R, true, true, 8, true>);
+            else launch_cells(k_mpole_pair<R, true, false, 8, true>);
+        } else if (ctx->ewald) {
             if (extra) launch(k_mpole_pair<R, true, true, L>);
             else launch(k_mpole_pair<R, true, false, L>);
         } else {
@@ -1186,7 +1237,10 @@ void enqueue_back(amg_ctx* ctx, cudaStream_t s, int flags) {
             kern<<<nblk((size_t)n * lanes), kThreads, 0, r>>>(n, ctx->sids, A.at, A.u4, ctx->bx, aew, ctx->nbr, ctx->cap,
                                                               ctx->nnb, mutual, ctx->f, ctx->grad_p, ctx->trq_p, virp);
         };
-        if (vir) {  // one lane count for the virial variants
+        if (ewald_cells(ctx)) {  // one lane count for the cell variants
+            if (vir) launch(k_polar_pair<R, true, 8, true, false, true>, 8);
+            else launch(k_polar_pair<R, true, 8, false, false, true>, 8);
+        } else if (vir) {  // one lane count for the virial variants
             if (ctx->ewald) launch(k_polar_pair<R, true, 8, true>, 8);
             else launch(k_polar_pair<R, false, 8, true>, 8);
         } else {
@@ -1405,7 +1459,7 @@ int forward_impl(amg_ctx* ctx, int flags, amg_results* res) {
     };
     double em = e[0] + e[2], echg = 0;
     if (ctx->ewald) {
-        double V = ctx->box[0] * ctx->box[1] * ctx->box[2];
+        double V = ctx->vol;
         double qt = e[3];
         echg = -ctx->f * kPi * qt * qt / (2 * V * ctx->aewald * ctx->aewald);
         em += echg;
@@ -1853,7 +1907,7 @@ int backward_impl(amg_ctx* ctx, const amg_cotangents* cot, amg_param_grads* gr) 
     // net-charge term of the Ewald energy, -f pi Q^2 / (2 V alpha^2): dq_i
     double dq = 0;
     if (ctx->ewald) {
-        double V = ctx->box[0] * ctx->box[1] * ctx->box[2];
+        double V = ctx->vol;
         dq = -cf * kPi * qtot / (V * ctx->aewald * ctx->aewald);
     }
     if (gr->d_xyz) std::memcpy(gr->d_xyz, hx.data(), sizeof(double) * n3);
@@ -1908,11 +1962,13 @@ int amg_set_coords(amg_ctx* ctx, const double* xyz, const double box[6]) {
             }
             Box nb = ctx->bx;
             if (!set_lattice(ctx, box, nb)) return AMG_ERR_BAD_ARG;
-            if (ctx->ewald && nb.shape != 0) {
-                ctx->err = "Ewald needs an orthogonal box";
+            if (ctx->ewald && nb.shape > 2) {
+                ctx->err = "Ewald needs a prism cell (orthogonal, monoclinic or triclinic)";
                 return AMG_ERR_UNSUPPORTED;
             }
             if (nb.shape != ctx->bx.shape) ctx->graph_dirty = true;
+            for (int a = 3; a < 6; a++)
+                if (ctx->box[a] != box[a]) ctx->graph_dirty = true;
             ctx->bx = nb;
             for (int a = 0; a < 3; a++)
                 if (ctx->cut > 0.5 * box[a] + 1e-12) {
@@ -1923,6 +1979,7 @@ int amg_set_coords(amg_ctx* ctx, const double* xyz, const double box[6]) {
                 if (ctx->box[a] != box[a]) ctx->graph_dirty = true;
             for (int a = 0; a < 6; a++) ctx->box[a] = box[a];
             for (int a = 0; a < 3; a++) { ctx->bx.L[a] = box[a]; ctx->bx.iL[a] = 1.0 / box[a]; }
+            set_frac(ctx);
         } else {
             for (int a = 0; a < 3; a++) { ctx->bx.L[a] = 0; ctx->bx.iL[a] = 0; }
         }

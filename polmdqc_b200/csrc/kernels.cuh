@@ -30,6 +30,15 @@ struct Box {
     double bsin, bcos, gsin, gcos, bterm, gterm;
 };
 
+// Cartesian -> grid units of the PME: u_j = sum_i x_i m[i][j] (m = inverse
+// lattice times K_j), so d/dx_i = sum_j m[i][j] d/du_j.  For an orthogonal
+// box m is diagonal (K/L) and `general` is 0: the kernels then take the
+// diagonal scalings alone.
+struct Frac {
+    double m[3][3];
+    int general;
+};
+
 template <class R>
 __device__ __forceinline__ Mpole<R> load_mpole(const AtomR<R>& A) {
     Mpole<R> M;
@@ -85,8 +94,9 @@ __device__ __noinline__ V3<R> image_cell(V3<R> d, const Box bx) {
 }
 
 // CELLS false: the box is orthogonal (or absent) by construction, as in
-// every Ewald kernel; true: any cell shape, the non-orthogonal ones through
-// image_cell.
+// the default instances of the Ewald pair kernels; true: any cell shape, the
+// non-orthogonal ones through image_cell (the pair kernels' CELLS instances,
+// launched for Ewald in a monoclinic or triclinic cell).
 template <class R, bool CELLS = true>
 __device__ __forceinline__ V3<R> min_image(V3<R> d, const Box& bx) {
     if (CELLS && bx.shape != 0) return image_cell<R>(d, bx);

@@ -197,7 +197,7 @@ __global__ void __launch_bounds__(128) k_pcg_dir_spread(int n, const double* __r
                                                         const double* __restrict__ zp, double* __restrict__ pd,
                                                         double* __restrict__ pp, const double* __restrict__ scal,
                                                         R4<R>* __restrict__ p4, const R* __restrict__ theta,
-                                                        const int* __restrict__ k0, int3 K, R sc0, R sc1, R sc2,
+                                                        const int* __restrict__ k0, int3 K, Frac F,
                                                         typename Cplx<R>::type* __restrict__ zg) {
     __shared__ double pv[6];
     const int i = blockIdx.x, t = threadIdx.x;
@@ -222,8 +222,9 @@ __global__ void __launch_bounds__(128) k_pcg_dir_spread(int n, const double* __r
     const R u0 = th[4 * P + b], u1 = th[5 * P + b];
     const R v0 = th[8 * P + c], v1 = th[9 * P + c];
     const R w100 = t1 * u0 * v0, w010 = t0 * u1 * v0, w001 = t0 * u0 * v1;
-    const R d0 = (R)pv[0] * sc0, d1 = (R)pv[1] * sc1, d2 = (R)pv[2] * sc2;
-    const R q0 = (R)pv[3] * sc0, q1 = (R)pv[4] * sc1, q2 = (R)pv[5] * sc2;
+    R d0, d1, d2, q0, q1, q2;
+    frac_dipole<R>(F, pv[0], pv[1], pv[2], d0, d1, d2);
+    frac_dipole<R>(F, pv[3], pv[4], pv[5], q0, q1, q2);
     int ga = k0[3 * i] + a; if (ga >= K.x) ga -= K.x;
     int gb = k0[3 * i + 1] + b; if (gb >= K.y) gb -= K.y;
     int gc = k0[3 * i + 2] + c; if (gc >= K.z) gc -= K.z;

@@ -19,7 +19,7 @@ namespace amg {
 // c0 = (x_i - x_j, B1), c1 = B2) and the sparse preconditioner's rows (pairs
 // within usolvcut, compacted in row order, when cu0 is given), so the
 // solve's set-up recomputes nothing.
-template <class R, bool EWALD, int LPA, bool COEF>
+template <class R, bool EWALD, int LPA, bool COEF, bool CELLS = false>
 __global__ void __launch_bounds__(128) k_perm_field(int n, const int* __restrict__ order, const AtomR<R>* __restrict__ at, Box bx, R aewald,
                                                     const int* __restrict__ nbr, int cap,
                                                     const int* __restrict__ nnb, double* __restrict__ Ed,
@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(128) k_perm_field(int n, const int* __restrict
         if (ok) {
             j = row[s];
             AtomR<R> Aj = at[j];
-            r = min_image<R, !EWALD>(xi - v3<R>(Aj.a.x, Aj.a.y, Aj.a.z), bx);  // target i - source j
+            r = min_image<R, !EWALD || CELLS>(xi - v3<R>(Aj.a.x, Aj.a.y, Aj.a.z), bx);  // target i - source j
             r2 = dot(r, r);
             R B[6];
             if (COEF) {
@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(128) k_perm_field(int n, const int* __restrict
 // Mutual field T u for two dipole sets (bulk, u-scale 1), computing the
 // pair tensors on the fly (used by the FP64 correction sweep).  u4: [n][2]
 // R4 (ux,uy,uz,0), d set then p set per site.  Writes Fd, Fp.
-template <class R, bool EWALD, int LPA>
+template <class R, bool EWALD, int LPA, bool CELLS = false>
 __global__ void __launch_bounds__(128) k_Tu(int n, const int* __restrict__ order, const AtomR<R>* __restrict__ at, const R4<R>* __restrict__ u4,
                                             Box bx, R aewald, const int* __restrict__ nbr, int cap,
                                             const int* __restrict__ nnb, double* __restrict__ Fd,
@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(128) k_Tu(int n, const int* __restrict__ order
     for (int s = lane; s < cnt; s += LPA) {
         int j = row[s];
         R4<R> pj = at[j].a, ej = at[j].e;
-        V3<R> r = min_image<R, !EWALD>(xi - v3<R>(pj.x, pj.y, pj.z), bx);
+        V3<R> r = min_image<R, !EWALD || CELLS>(xi - v3<R>(pj.x, pj.y, pj.z), bx);
         R r2 = dot(r, r);
         R rinv = rsqrt_<R>(r2);
         R rr = r2 * rinv, rinv2 = rinv * rinv;
@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(128) k_Tu(int n, const int* __restrict__ order
 // pointer is set -- per-site energy, nonzero pair count (directed) and
 // intermolecular energy (aem, npair, mol); the pair virial (vir, six sums),
 // half of -g_i (x) r per directed pair.
-template <class R, bool EWALD, bool EXTRA, int LPA>
+template <class R, bool EWALD, bool EXTRA, int LPA, bool CELLS = false>
 __global__ void __launch_bounds__(128) k_mpole_pair(int n, const int* __restrict__ order, const AtomR<R>* __restrict__ at, Box bx, R aewald,
                                                     const int* __restrict__ nbr, int cap,
                                                     const int* __restrict__ nnb, double f, double* __restrict__ grad,
@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(128) k_mpole_pair(int n, const int* __restrict
     for (int s = lane; s < cnt; s += LPA) {
         int j = row[s];
         AtomR<R> Aj = at[j];
-        V3<R> r = min_image<R, !EWALD>(v3<R>(Aj.a.x, Aj.a.y, Aj.a.z) - xi, bx);  // x_k - x_i
+        V3<R> r = min_image<R, !EWALD || CELLS>(v3<R>(Aj.a.x, Aj.a.y, Aj.a.z) - xi, bx);  // x_k - x_i
         R B[6];
         bulk_radial<R, EWALD, false>(dot(r, r), aewald, R(0), R(0), B);
         R E;
@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(128) k_mpole_pair(int n, const int* __restrict
 // vir (six sums), half of dG/dr (x) r per directed pair.  DDONLY: only the
 // dipole-dipole term 1/2 [E(up_i, ud_k) + E(ud_i, up_k)] (the OPT cross
 // terms between perturbation orders; no torques).
-template <class R, bool EWALD, int LPA, bool VIR, bool DDONLY = false>
+template <class R, bool EWALD, int LPA, bool VIR, bool DDONLY = false, bool CELLS = false>
 __global__ void __launch_bounds__(128) k_polar_pair(int n, const int* __restrict__ order, const AtomR<R>* __restrict__ at,
                                                     const R4<R>* __restrict__ u4, Box bx, R aewald,
                                                     const int* __restrict__ nbr, int cap,
@@ -225,7 +225,7 @@ __global__ void __launch_bounds__(128) k_polar_pair(int n, const int* __restrict
     for (int s = lane; s < cnt; s += LPA) {
         int j = row[s];
         AtomR<R> Aj = at[j];
-        V3<R> r = min_image<R, !EWALD>(v3<R>(Aj.a.x, Aj.a.y, Aj.a.z) - xi, bx);
+        V3<R> r = min_image<R, !EWALD || CELLS>(v3<R>(Aj.a.x, Aj.a.y, Aj.a.z) - xi, bx);
         R B[6];
         bulk_radial<R, EWALD, true>(dot(r, r), aewald, Ai.e.y * Aj.e.y, pair_thole<R>(Ai.e.z, Aj.e.z), B);
         R4<R> udk4 = u4[2 * j], upk4 = u4[2 * j + 1];
@@ -262,7 +262,7 @@ __global__ void __launch_bounds__(128) k_polar_pair(int n, const int* __restrict
 // index is the list entry itself.  Rows hold the bulk neighbours followed by
 // the scaled partners (filled by k_scaled_coeffs), so one kernel applies the
 // whole real-space T.
-template <class R, bool EWALD, int LPA>
+template <class R, bool EWALD, int LPA, bool CELLS = false>
 __global__ void __launch_bounds__(128) k_tu_coeffs(int n, const int* __restrict__ order, const AtomR<R>* __restrict__ at, Box bx, R aewald,
                                                    const int* __restrict__ nbr, int cap, const int* __restrict__ nnb,
                                                    R4<R>* __restrict__ c0, R* __restrict__ c1, R usolv2,
@@ -288,7 +288,7 @@ __global__ void __launch_bounds__(128) k_tu_coeffs(int n, const int* __restrict_
         if (ok) {
             j = nbr[base + s];
             R4<R> pj = at[j].a, ej = at[j].e;
-            r = min_image<R, !EWALD>(xi - v3<R>(pj.x, pj.y, pj.z), bx);
+            r = min_image<R, !EWALD || CELLS>(xi - v3<R>(pj.x, pj.y, pj.z), bx);
             r2 = dot(r, r);
             R rinv = rsqrt_<R>(r2);
             R rr = r2 * rinv, rinv2 = rinv * rinv;

@@ -26,19 +26,81 @@ struct Cplx<double> {
 
 __device__ __forceinline__ int gidx(int a, int b, int c, int3 K) { return (a * K.y + b) * K.z + c; }
 
+// fractional dipole d'_j = sum_i d_i m[i][j]
+template <class R>
+__device__ __forceinline__ void frac_dipole(const Frac& F, double x, double y, double z, R& a, R& b, R& c) {
+    if (!F.general) {
+        a = (R)x * (R)F.m[0][0];
+        b = (R)y * (R)F.m[1][1];
+        c = (R)z * (R)F.m[2][2];
+        return;
+    }
+    a = (R)(x * F.m[0][0] + y * F.m[1][0] + z * F.m[2][0]);
+    b = (R)(x * F.m[0][1] + y * F.m[1][1] + z * F.m[2][1]);
+    c = (R)(x * F.m[0][2] + y * F.m[1][2] + z * F.m[2][2]);
+}
+
+// Exponents (x, y, z) of the 20 potential derivatives in output order:
+// 0; x y z; xx yy zz xy xz yz; xxx yyy zzz xxy xxz xyy yyz xzz yzz xyz
+__constant__ int kDerEx[20][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {2, 0, 0}, {0, 2, 0}, {0, 0, 2},
+                                  {1, 1, 0}, {1, 0, 1}, {0, 1, 1}, {3, 0, 0}, {0, 3, 0}, {0, 0, 3}, {2, 1, 0},
+                                  {2, 0, 1}, {1, 2, 0}, {0, 2, 1}, {1, 0, 2}, {0, 1, 2}, {1, 1, 1}};
+
+// Cartesian derivative j of the potential from the grid-unit derivatives f[]
+// (same ordering) in a general cell: the grid-unit tensor contracted with m
+// on every index.  Called only for non-orthogonal cells.
+__device__ __noinline__ double cart_deriv(const Frac F, const double* f, int nc, int j) {
+    int ax[3], n = 0;
+    for (int a = 0; a < 3; a++)
+        for (int r = 0; r < kDerEx[j][a]; r++) ax[n++] = a;
+    if (n == 0) return f[0];
+    const int tuples = n == 1 ? 3 : n == 2 ? 9 : 27;
+    double v = 0;
+    for (int t = 0; t < tuples; t++) {
+        int cnt[3] = {0, 0, 0};
+        double w = 1;
+        int r = t;
+        for (int k = 0; k < n; k++) {
+            const int q = r % 3;
+            r /= 3;
+            cnt[q]++;
+            w *= F.m[ax[k]][q];
+        }
+        for (int q = 0; q < nc; q++)
+            if (kDerEx[q][0] == cnt[0] && kDerEx[q][1] == cnt[1] && kDerEx[q][2] == cnt[2]) v += w * f[q];
+    }
+    return v;
+}
+
 // Spread the permanent multipoles (global frame, FP64 rp10) as fractional
 // multipoles: grid(g) += q t0u0v0 + sum_a d'_a (first derivative in a) +
-// sum_ab Q'_ab (second derivatives), with d' = (K/L) d, Q' = (K/L)(K/L) Q.
+// sum_ab Q'_ab (second derivatives), with d' = m^T d, Q' = m^T Q m.
 template <class R, int P>
 __global__ void k_spread_mpole(int n, const double* __restrict__ rp10, const R* __restrict__ theta,
-                               const int* __restrict__ k0, int3 K, R sc0, R sc1, R sc2, R* __restrict__ grid) {
+                               const int* __restrict__ k0, int3 K, Frac F, R* __restrict__ grid) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double* m = rp10 + 10 * i;
     R q = (R)m[0];
-    R d1 = (R)m[1] * sc0, d2 = (R)m[2] * sc1, d3 = (R)m[3] * sc2;
-    R q11 = (R)m[4] * sc0 * sc0, q22 = (R)m[7] * sc1 * sc1, q33 = (R)m[9] * sc2 * sc2;
-    R q12 = 2 * (R)m[5] * sc0 * sc1, q13 = 2 * (R)m[6] * sc0 * sc2, q23 = 2 * (R)m[8] * sc1 * sc2;
+    R d1, d2, d3, q11, q22, q33, q12, q13, q23;
+    frac_dipole<R>(F, m[1], m[2], m[3], d1, d2, d3);
+    if (!F.general) {
+        const R sc0 = (R)F.m[0][0], sc1 = (R)F.m[1][1], sc2 = (R)F.m[2][2];
+        q11 = (R)m[4] * sc0 * sc0; q22 = (R)m[7] * sc1 * sc1; q33 = (R)m[9] * sc2 * sc2;
+        q12 = 2 * (R)m[5] * sc0 * sc1; q13 = 2 * (R)m[6] * sc0 * sc2; q23 = 2 * (R)m[8] * sc1 * sc2;
+    } else {
+        const double Qc[3][3] = {{m[4], m[5], m[6]}, {m[5], m[7], m[8]}, {m[6], m[8], m[9]}};
+        double Qf[3][3];
+        for (int j = 0; j < 3; j++)
+            for (int k = 0; k < 3; k++) {
+                double v = 0;
+                for (int a = 0; a < 3; a++)
+                    for (int b = 0; b < 3; b++) v += F.m[a][j] * Qc[a][b] * F.m[b][k];
+                Qf[j][k] = v;
+            }
+        q11 = (R)Qf[0][0]; q22 = (R)Qf[1][1]; q33 = (R)Qf[2][2];
+        q12 = (R)(2 * Qf[0][1]); q13 = (R)(2 * Qf[0][2]); q23 = (R)(2 * Qf[1][2]);
+    }
     const R* t1 = theta + ((size_t)i * 3 + 0) * 4 * P;
     const R* t2 = theta + ((size_t)i * 3 + 1) * 4 * P;
     const R* t3 = theta + ((size_t)i * 3 + 2) * 4 * P;
@@ -85,7 +147,7 @@ __global__ void __launch_bounds__(128) k_spread_dipoles(int n, const int* __rest
                                                         const double* __restrict__ ud,
                                                         const double* __restrict__ up,
                                                         const R* __restrict__ theta, const int* __restrict__ k0,
-                                                        int3 K, R sc0, R sc1, R sc2,
+                                                        int3 K, Frac F,
                                                         typename Cplx<R>::type* __restrict__ zg) {
     const int t = threadIdx.x;
     if (t >= P * P * P) return;
@@ -95,8 +157,9 @@ __global__ void __launch_bounds__(128) k_spread_dipoles(int n, const int* __rest
     const R t0 = th[a], t1 = th[P + a];
     const R u0 = th[4 * P + b], u1 = th[5 * P + b];
     const R v0 = th[8 * P + c], v1 = th[9 * P + c];
-    const R d0 = (R)ud[3 * i] * sc0, d1 = (R)ud[3 * i + 1] * sc1, d2 = (R)ud[3 * i + 2] * sc2;
-    const R p0 = (R)up[3 * i] * sc0, p1 = (R)up[3 * i + 1] * sc1, p2 = (R)up[3 * i + 2] * sc2;
+    R d0, d1, d2, p0, p1, p2;
+    frac_dipole<R>(F, ud[3 * i], ud[3 * i + 1], ud[3 * i + 2], d0, d1, d2);
+    frac_dipole<R>(F, up[3 * i], up[3 * i + 1], up[3 * i + 2], p0, p1, p2);
     const R w100 = t1 * u0 * v0, w010 = t0 * u1 * v0, w001 = t0 * u0 * v1;
     int ga = k0[3 * i] + a; if (ga >= K.x) ga -= K.x;
     int gb = k0[3 * i + 1] + b; if (gb >= K.y) gb -= K.y;
@@ -116,7 +179,7 @@ __global__ void __launch_bounds__(128) k_spread_dipoles(int n, const int* __rest
 template <class R, int P, int G>
 __global__ void __launch_bounds__(128) k_gather_field(int n, const typename Cplx<R>::type* __restrict__ zg,
                                                       const R* __restrict__ theta, const int* __restrict__ k0,
-                                                      int3 K, double sc0, double sc1, double sc2,
+                                                      int3 K, Frac F,
                                                       const double* __restrict__ vd, const double* __restrict__ vp,
                                                       const double* __restrict__ Fd, const double* __restrict__ Fp,
                                                       double selfc, const double* __restrict__ pol,
@@ -163,14 +226,16 @@ __global__ void __launch_bounds__(128) k_gather_field(int n, const typename Cplx
         for (int k = 0; k < 6; k++) sum[k] = group_sum<G>((double)f[k]);
         if (g < n && lane < 6) {
             const int t = lane, c = t % 3;
-            const double v = t == 0 ? sum[0] : t == 1 ? sum[1] : t == 2 ? sum[2] : t == 3 ? sum[3] : t == 4 ? sum[4] : sum[5];
-            const double scv = c == 0 ? sc0 : c == 1 ? sc1 : sc2;
             const bool dset = t < 3;
+            // d phi / dx_c from the grid-unit first derivatives of this set
+            const double s0 = dset ? sum[0] : sum[3], s1 = dset ? sum[1] : sum[4], s2 = dset ? sum[2] : sum[5];
+            const double dphi = F.general ? F.m[c][0] * s0 + F.m[c][1] * s1 + F.m[c][2] * s2
+                                          : F.m[c][c] * (c == 0 ? s0 : c == 1 ? s1 : s2);
             const double* vv = dset ? vd : vp;
             const double* FF = dset ? Fd : Fp;
             double* AA = dset ? Ad : Ap;
             const double alpha = pol[i];
-            const double field = FF[3 * i + c] - v * scv + selfc * vv[3 * i + c];
+            const double field = FF[3 * i + c] - dphi + selfc * vv[3 * i + c];
             const double av = alpha > 0 ? vv[3 * i + c] / alpha - field : 0.0;
             AA[3 * i + c] = av;
             if (dset) dotd += vv[3 * i + c] * av;
@@ -205,9 +270,14 @@ __global__ void k_scale_grid(size_t npts, const R* __restrict__ G, typename Cplx
 // (X a product of structure factors)
 //   de/deps_ab = e (2 (1/h^2 + pi^2/alpha^2) h_a h_b - delta_ab)
 // (the reciprocal virial of Essmann et al., J. Chem. Phys. 103, 8577 (1995),
-// in dE/d(strain) form).  `c2` = pi^2/alpha^2, `iL` the inverse box edges.
-__device__ __forceinline__ void kvir_point(double (&v)[6], int ma, int mb, int mc, double3 iL, double c2, double e) {
-    const double hx = ma * iL.x, hy = mb * iL.y, hz = mc * iL.z;
+// in dE/d(strain) form).  `c2` = pi^2/alpha^2; h = sum_j m_j b_j with the
+// reciprocal vectors b_j = (column j of F.m) / K_j.
+__device__ __forceinline__ void kvir_point(double (&v)[6], int ma, int mb, int mc, const Frac& F, int3 K, double c2,
+                                           double e) {
+    const double fa = (double)ma / K.x, fb = (double)mb / K.y, fc = (double)mc / K.z;
+    const double hx = F.m[0][0] * fa + F.m[0][1] * fb + F.m[0][2] * fc;
+    const double hy = F.m[1][0] * fa + F.m[1][1] * fb + F.m[1][2] * fc;
+    const double hz = F.m[2][0] * fa + F.m[2][1] * fb + F.m[2][2] * fc;
     const double h2 = hx * hx + hy * hy + hz * hz;
     const double t = 2.0 * (1.0 / h2 + c2) * e;
     v[0] += t * hx * hx - e;
@@ -222,7 +292,7 @@ __device__ __forceinline__ void kvir_point(double (&v)[6], int ma, int mb, int m
 // transform cg (before the convolution); points 0 < c < K3/2 stand for m and
 // -m.  Saves the transform into `save` for the polarization cross terms.
 template <class R>
-__global__ void k_kvir_mpole(size_t ncomplex, int3 K, double3 iL, double c2, double f, const R* __restrict__ infl,
+__global__ void k_kvir_mpole(size_t ncomplex, int3 K, Frac F, double c2, double f, const R* __restrict__ infl,
                              const typename Cplx<R>::type* __restrict__ cg, typename Cplx<R>::type* __restrict__ save,
                              double* __restrict__ vir) {
     const int K3h = K.z / 2 + 1;
@@ -237,7 +307,7 @@ __global__ void k_kvir_mpole(size_t ncomplex, int3 K, double3 iL, double c2, dou
         const int ma = a <= K.x / 2 ? a : a - K.x, mb = b <= K.y / 2 ? b : b - K.y;
         const double wgt = (c == 0 || 2 * c == K.z) ? 1.0 : 2.0;
         const double e = 0.5 * f * wgt * (double)infl[t] * ((double)S.x * S.x + (double)S.y * S.y);
-        kvir_point(v, ma, mb, c, iL, c2, e);
+        kvir_point(v, ma, mb, c, F, K, c2, e);
     }
     block_vir_add(v, vir);
 }
@@ -250,7 +320,7 @@ __global__ void k_kvir_mpole(size_t ncomplex, int3 K, double3 iL, double c2, dou
 // function on the full grid.  mterms 0: the U(up, ud) term alone (OPT cross
 // terms).
 template <class R>
-__global__ void k_kvir_polar(size_t npts, int3 K, double3 iL, double c2, double f, int mutual, int mterms,
+__global__ void k_kvir_polar(size_t npts, int3 K, Frac F, double c2, double f, int mutual, int mterms,
                              const R* __restrict__ G, const typename Cplx<R>::type* __restrict__ z,
                              const typename Cplx<R>::type* __restrict__ sM, double* __restrict__ vir) {
     const int K3h = K.z / 2 + 1;
@@ -278,7 +348,7 @@ __global__ void k_kvir_polar(size_t npts, int3 K, double3 iL, double c2, double 
         double x = mterms ? mx * (px + dx) + my * (py + dy) : 0.0;
         if (mutual) x += px * dx + py * dy;
         const int ma = a <= K.x / 2 ? a : a - K.x, mb = b <= K.y / 2 ? b : b - K.y, mc = c <= K.z / 2 ? c : c - K.z;
-        kvir_point(v, ma, mb, mc, iL, c2, 0.5 * f * (double)G[t] * x);
+        kvir_point(v, ma, mb, mc, F, K, c2, 0.5 * f * (double)G[t] * x);
     }
     block_vir_add(v, vir);
 }
@@ -344,8 +414,8 @@ __device__ __forceinline__ void add_derivs(R (&f)[NC], const R (&x)[4], const R 
 
 template <class R, int P, int NC, int G, int NS>
 __global__ void __launch_bounds__(128) k_gather(int n, const void* __restrict__ gridv, const R* __restrict__ theta,
-                                                const int* __restrict__ k0, int3 K, double sc0, double sc1,
-                                                double sc2, double* __restrict__ phi) {
+                                                const int* __restrict__ k0, int3 K, Frac F,
+                                                double* __restrict__ phi) {
     constexpr int ND = NC == 4 ? 2 : NC == 10 ? 3 : 4;  // derivative orders per axis
     using C = typename Cplx<R>::type;
     const int g = (blockIdx.x * blockDim.x + threadIdx.x) / G, lane = threadIdx.x % G;
@@ -408,6 +478,17 @@ __global__ void __launch_bounds__(128) k_gather(int n, const void* __restrict__ 
     const int ex[20][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {2, 0, 0}, {0, 2, 0}, {0, 0, 2},
                            {1, 1, 0}, {1, 0, 1}, {0, 1, 1}, {3, 0, 0}, {0, 3, 0}, {0, 0, 3}, {2, 1, 0},
                            {2, 0, 1}, {1, 2, 0}, {0, 2, 1}, {1, 0, 2}, {0, 1, 2}, {1, 1, 1}};
+    if (F.general) {
+#pragma unroll
+        for (int s = 0; s < NS; s++) {
+            double fs[NC];
+#pragma unroll
+            for (int j = 0; j < NC; j++) fs[j] = sum[s][j];
+            for (int j = lane; j < NC; j += G) phi[(size_t)s * NC * n + (size_t)NC * i + j] = cart_deriv(F, fs, NC, j);
+        }
+        return;
+    }
+    const double sc0 = F.m[0][0], sc1 = F.m[1][1], sc2 = F.m[2][2];
     const double p0[4] = {1, sc0, sc0 * sc0, sc0 * sc0 * sc0};
     const double p1[4] = {1, sc1, sc1 * sc1, sc1 * sc1 * sc1};
     const double p2[4] = {1, sc2, sc2 * sc2, sc2 * sc2 * sc2};

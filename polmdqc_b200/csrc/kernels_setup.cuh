@@ -408,13 +408,16 @@ __device__ __forceinline__ void bspline_weights(double w, R (&th)[4][P]) {
 }
 
 template <class R, int P>
-__global__ void k_bspline(int n, const double* __restrict__ xyz, Box bx, int3 K, R* __restrict__ theta,
+__global__ void k_bspline(int n, const double* __restrict__ xyz, Box bx, Frac F, int3 K, R* __restrict__ theta,
                           int* __restrict__ k0) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int Ks[3] = {K.x, K.y, K.z};
+    const double x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2];
     for (int a = 0; a < 3; a++) {
-        double f = xyz[3 * i + a] * bx.iL[a];
+        // fractional coordinate (grid units / K) along cell axis a
+        double f = F.general ? (x * F.m[0][a] + y * F.m[1][a] + z * F.m[2][a]) / Ks[a]
+                             : (a == 0 ? x : a == 1 ? y : z) * bx.iL[a];
         f -= floor(f);
         double u = f * Ks[a];
         double fl = floor(u);

@@ -91,11 +91,36 @@ def test_waterbox30_cell_shapes_golden(case, shape, prec):
     np.testing.assert_allclose(r.dem.reshape(-1), d["dem"], atol=1e-8 if prec == FP64 else 1e-3, rtol=0)
 
 
-def test_ewald_needs_an_orthogonal_cell():
-    d = ref_dump(ref_fixture("bounds", "waterbox30.xyz"), ref_fixture("bounds", "triclinic.key"))
+def test_ewald_needs_a_prism_cell():
+    """Ewald runs in orthogonal, monoclinic and triclinic cells; the truncated
+    octahedron and rhombic dodecahedron return UNSUPPORTED."""
+    d = ref_dump(ref_fixture("bounds", "waterbox30.xyz"), ref_fixture("bounds", "octahedron.key"))
     s = systems.from_dump(d)
     with pytest.raises(AmgError, match="UNSUPPORTED"):
         run(s, Settings(nfft=(32, 32, 32), cutoff=9.0, poltyp=abi.POL_NONE))
+
+
+@pytest.mark.parametrize("prec", [FP64, MIXED])
+@pytest.mark.parametrize("box", [(18.9, 19.3, 19.6, 90.0, 97.0, 90.0), (18.9, 19.3, 19.6, 84.0, 97.0, 93.0)])
+def test_ewald_in_prism_cells_matches_oracle(w216, box, prec):
+    """Monoclinic and triclinic cells with Ewald and mutual polarization: the
+    pair kernels' cell-image instances, the PME through the inverse lattice
+    (fractional multipoles, stencils, derivative transform, influence
+    function on the general reciprocal vectors) and the virial."""
+    import copy
+    s = copy.deepcopy(w216)
+    s.box = np.array(box)
+    flags = ALL | abi.DO_VIRIAL
+    o = oracle.forward(s, Settings(nfft=(24, 24, 24), precision=FP64), tol=1e-11, flags=flags)
+    g = run(s, Settings(nfft=(24, 24, 24), precision=prec, poleps=1e-8 if prec == FP64 else 1e-6), flags)
+    if prec == FP64:
+        assert rel(g.em, o.em) < 1e-10 and rel(g.ep, o.ep) < 1e-8
+        assert np.abs(g.dem - o.dem).max() < 1e-8 and np.abs(g.dep - o.dep).max() < 1e-5
+        assert np.abs(g.vir - o.vir).max() < 1e-7 * np.abs(o.vir).max()
+    else:
+        assert rel(g.em, o.em) < 1e-6 and rel(g.ep, o.ep) < 1e-6
+        assert frms(g, o) < 1e-4
+        assert np.abs(g.vir - o.vir).max() < 1e-5 * np.abs(o.vir).max()
 
 
 def test_synthetic_box_matches_reference_run():

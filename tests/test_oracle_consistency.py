@@ -175,3 +175,107 @@ def test_opt_approaches_the_mutual_solution(box27):
         errs.append(abs(o.ep - mu.ep) / abs(mu.ep))
     assert errs[2] < 1e-3 and errs[3] < 1e-2
     assert max(errs[1:]) < errs[0]
+
+
+TRICLINIC = np.array([9.9, 10.1, 10.4, 86.0, 95.0, 92.0])
+
+
+def _rows(box):
+    """Lattice rows of a (a, b, c, alpha, beta, gamma) cell, a along x and b
+    in the xy plane (the reference's lattice, src/md/lattice.cpp:122-140)."""
+    a, b, c = box[:3]
+    al, be, ga = np.radians(box[3:])
+    bterm = (np.cos(al) - np.cos(be) * np.cos(ga)) / np.sin(ga)
+    return np.array([[a, 0, 0], [b * np.cos(ga), b * np.sin(ga), 0],
+                     [c * np.cos(be), c * bterm, c * np.sqrt(np.sin(be) ** 2 - bterm ** 2)]])
+
+
+def _box_of(rows):
+    L = np.linalg.norm(rows, axis=1)
+    ang = lambda u, v: np.degrees(np.arccos(np.dot(u, v) / (np.linalg.norm(u) * np.linalg.norm(v))))
+    return np.array([L[0], L[1], L[2], ang(rows[1], rows[2]), ang(rows[0], rows[2]), ang(rows[0], rows[1])])
+
+
+@pytest.fixture(scope="module")
+def tric27(box27):
+    s = copy.deepcopy(box27)
+    s.box = TRICLINIC.copy()
+    return s
+
+
+def test_triclinic_pme_converges_to_explicit_ewald_sum(tric27):
+    """PME in a triclinic cell (fractional multipoles through the inverse
+    lattice, derivatives back through it) against the explicit k-space sum."""
+    for mask in ([0], [1, 2, 3], list(range(4, 13))):
+        s = copy.deepcopy(tric27)
+        keep = np.zeros(13, bool)
+        keep[mask] = True
+        s.pole = s.pole * keep
+        st = Settings(aewald=0.7, nfft=(64, 64, 64), cutoff=4.6, poltyp=abi.POL_NONE)
+        ek = oracle.forward(s, st, flags=abi.DO_ENERGY, kmax=9.0).em
+        ep = oracle.forward(s, st, flags=abi.DO_ENERGY).em
+        assert abs(ep - ek) < 2e-5 * abs(ek) + 2e-5
+
+
+def test_triclinic_ewald_forces_and_virial(tric27):
+    """Triclinic Ewald with mutual polarization: gradients against central
+    differences, and the virial's diagonal against strains of the cell (the
+    strained rows keep a along x and b in the xy plane)."""
+    s = tric27
+    st = Settings(aewald=0.7, nfft=(24, 25, 27), cutoff=4.6, poleps=1e-11)
+    r = oracle.forward(s, st, flags=abi.DO_ENERGY | abi.DO_GRADIENT | abi.DO_VIRIAL, raw_virial=True)
+    h = 1e-5
+    for (i, a) in ((0, 0), (40, 1), (77, 2)):
+        x = s.xyz.copy()
+        x[i, a] += h
+        p = oracle.forward(s, st, xyz=x, flags=abi.DO_ENERGY)
+        x[i, a] -= 2 * h
+        m = oracle.forward(s, st, xyz=x, flags=abi.DO_ENERGY)
+        assert abs((p.em - m.em) / (2 * h) - r.dem[i, a]) < 1e-6
+        assert abs((p.ep - m.ep) / (2 * h) - r.dep[i, a]) < 1e-6
+    W = r.vir
+    rows = _rows(s.box)
+    for a in range(3):
+        e = []
+        for sgn in (1, -1):
+            E = np.eye(3)
+            E[a, a] += sgn * h
+            t = copy.deepcopy(s)
+            t.xyz = s.xyz @ E.T
+            t.box = _box_of(rows @ E.T)
+            q = oracle.forward(t, st, flags=abi.DO_ENERGY)
+            e.append(q.em + q.ep)
+        assert abs(W[a, a] - (e[0] - e[1]) / (2 * h)) < 1e-8 * np.abs(W).max()
+    assert np.abs(W - W.T).max() < 1e-9 * np.abs(W).max()
+
+
+def test_triclinic_ewald_total_independent_of_alpha(tric27):
+    """Real space (the reference's fractional-coordinate image), reciprocal
+    space and self terms together: em does not depend on alpha."""
+    vals = []
+    for a in (0.8, 0.9, 1.0):
+        st = Settings(aewald=a, nfft=(24, 24, 24), cutoff=4.9, poltyp=abi.POL_NONE)
+        vals.append(oracle.forward(tric27, st, flags=abi.DO_ENERGY, kmax=11.0).em)
+    assert max(vals) - min(vals) < 1e-6 * abs(vals[0])
+
+
+@pytest.mark.parametrize("poltyp", [abi.POL_NONE, abi.POL_MUTUAL])
+def test_periodic_ewald_virial_shear_components(box27, poltyp):
+    """Off-diagonal virial of a periodic Ewald system: shearing the cubic cell
+    (x += h y, x += h z, y += h z keep a along x and b in the xy plane) makes
+    it triclinic, which the PME handles, so the shear derivative of em + ep
+    pins W_xy, W_xz and W_yz directly."""
+    st = Settings(aewald=0.7, nfft=(24, 24, 24), cutoff=4.6, poltyp=poltyp, poleps=1e-11)
+    W = oracle.forward(box27, st, flags=abi.DO_ENERGY | abi.DO_VIRIAL).vir
+    rows, h = _rows(box27.box), 1e-5
+    for (a, b) in ((0, 1), (0, 2), (1, 2)):
+        e = []
+        for sgn in (1, -1):
+            E = np.eye(3)
+            E[a, b] += sgn * h
+            t = copy.deepcopy(box27)
+            t.xyz = box27.xyz @ E.T
+            t.box = _box_of(rows @ E.T)
+            q = oracle.forward(t, st, flags=abi.DO_ENERGY)
+            e.append(q.em + q.ep)
+        assert abs(W[a, b] - (e[0] - e[1]) / (2 * h)) < 1e-8 * np.abs(W).max()

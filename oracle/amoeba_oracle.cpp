@@ -609,6 +609,21 @@ struct Pme {
     void recip_vec(int m0, int m1, int m2, double h[3]) const {
         for (int i = 0; i < 3; i++) h[i] = Ri[i][0] * m0 + Ri[i][1] * m1 + Ri[i][2] * m2;
     }
+    // Integer frequency of grid point (a, b, c): index k -> k (k <= K/2) or
+    // k - K.  A point past the half-complex range (c > K3/2) takes the
+    // frequency of its partner (-a, -b, K3 - c) there: the influence function
+    // is the even extension of its half-complex values, as a real-to-complex
+    // transform implies, which matters on the Nyquist planes only
+    void freq(int a, int b, int c, int m[3]) const {
+        if (c > K[2] / 2) {
+            a = a ? K[0] - a : 0;
+            b = b ? K[1] - b : 0;
+            c = K[2] - c;
+        }
+        m[0] = a <= K[0] / 2 ? a : a - K[0];
+        m[1] = b <= K[1] / 2 ? b : b - K[1];
+        m[2] = c;
+    }
     std::vector<double> bsmod[3];
     // per-atom stencils
     std::vector<int> k0;               // [n*3] first grid index (may be negative -> wrap)
@@ -782,11 +797,10 @@ void pme_potential(const System& s, const Pme& pm, const std::vector<Mp>& M, std
             for (int c = 0; c < pm.K[2]; c++) {
                 size_t id = ((size_t)a * pm.K[1] + b) * pm.K[2] + c;
                 if (a == 0 && b == 0 && c == 0) { grid[id] = 0; continue; }
-                int ma = a <= pm.K[0] / 2 ? a : a - pm.K[0];
-                int mb = b <= pm.K[1] / 2 ? b : b - pm.K[1];
-                int mc = c <= pm.K[2] / 2 ? c : c - pm.K[2];
+                int mm[3];
+                pm.freq(a, b, c, mm);
                 double h[3];
-                pm.recip_vec(ma, mb, mc, h);
+                pm.recip_vec(mm[0], mm[1], mm[2], h);
                 double h2 = h[0] * h[0] + h[1] * h[1] + h[2] * h[2];
                 double g = pref * std::exp(-kPi * kPi * h2 / (s.alpha * s.alpha)) / h2 /
                            (pm.bsmod[0][a] * pm.bsmod[1][b] * pm.bsmod[2][c]);
@@ -828,11 +842,10 @@ void pme_kvir(const System& s, const Pme& pm, const std::vector<cd>& SX, const s
             for (int c = 0; c < pm.K[2]; c++) {
                 if (a == 0 && b == 0 && c == 0) continue;
                 size_t id = ((size_t)a * pm.K[1] + b) * pm.K[2] + c;
-                int ma = a <= pm.K[0] / 2 ? a : a - pm.K[0];
-                int mb = b <= pm.K[1] / 2 ? b : b - pm.K[1];
-                int mc = c <= pm.K[2] / 2 ? c : c - pm.K[2];
+                int mm[3];
+                pm.freq(a, b, c, mm);
                 double h[3];
-                pm.recip_vec(ma, mb, mc, h);
+                pm.recip_vec(mm[0], mm[1], mm[2], h);
                 double h2 = h[0] * h[0] + h[1] * h[1] + h[2] * h[2];
                 double g = pref * std::exp(-c2 * h2) / h2 / (pm.bsmod[0][a] * pm.bsmod[1][b] * pm.bsmod[2][c]);
                 double e = g * (SX[id] * std::conj(SY[id])).real();

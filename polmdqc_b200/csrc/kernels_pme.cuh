@@ -347,8 +347,13 @@ __global__ void k_kvir_polar(size_t npts, int3 K, Frac F, double c2, double f, i
         }
         double x = mterms ? mx * (px + dx) + my * (py + dy) : 0.0;
         if (mutual) x += px * dx + py * dy;
-        const int ma = a <= K.x / 2 ? a : a - K.x, mb = b <= K.y / 2 ? b : b - K.y, mc = c <= K.z / 2 ? c : c - K.z;
-        kvir_point(v, ma, mb, mc, F, K, c2, 0.5 * f * (double)G[t] * x);
+        // frequency of the point, or past the half-complex range that of its
+        // partner (-a, -b, K3 - c): G is the even extension of the
+        // half-complex influence function, so its strain derivative follows
+        // the partner's reciprocal vector (different on the Nyquist planes)
+        const int ea = c < K3h ? a : an, eb = c < K3h ? b : bn, ec = c < K3h ? c : cn;
+        const int ma = ea <= K.x / 2 ? ea : ea - K.x, mb = eb <= K.y / 2 ? eb : eb - K.y;
+        kvir_point(v, ma, mb, ec, F, K, c2, 0.5 * f * (double)G[t] * x);
     }
     block_vir_add(v, vir);
 }

@@ -117,6 +117,23 @@ def cpu_baseline_oracle(seed=0):
                       f"({dt:.2f} s)"}
 
 
+def reduce_max(x, dist, device):
+    """Maximum over the ranks of a float (x itself without a process group):
+    the slowest rank's time, as the replica timing rule asks."""
+    if not dist:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(world, steps, seconds):
+    """Whole-job rate of independent replicas: every rank's evaluations over
+    the slowest rank's time."""
+    return world * steps / seconds
+
+
 def run_reference(args):
     """CPU reference arm: the oracle port of the full path (the reference
     itself implements only non-Ewald multipoles, src/md/empole.cpp:53-64)."""
@@ -199,11 +216,7 @@ def main():
             dist.barrier()
 
     def max_over_ranks(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(x, dist, "cuda")
 
     s = systems.water_box(WATERS, BOX, seed=rank)
     st = Settings(nfft=(GRID,) * 3, precision=abi.PREC_MIXED, device=local)
@@ -216,7 +229,7 @@ def main():
     barrier()
     clk = clocks.stop() if clocks else None
     dev_s = max_over_ranks(float(np.sum(ms)) / 1000.0)
-    value = world * args.steps / dev_s
+    value = replica_rate(world, args.steps, dev_s)
 
     # end to end through the C ABI: host coordinates (pinned) in, gradients out
     n = s.n

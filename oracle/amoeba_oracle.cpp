@@ -1450,10 +1450,10 @@ typedef struct orc_options {
                            part vanishes for a rotation-invariant energy) */
 } orc_options;
 
-int orc_forward(const amg_params* P, const double* xyz, const double box[6], int32_t flags,
-                const orc_options* opt, amg_results* res) {
-    if (!P || !xyz || !res || P->n <= 0) return AMG_ERR_BAD_ARG;
-    Work w;
+// Everything orc_forward sets up before evaluating: the system from the
+// parameters, coordinates and cell, scaled pairs, rotated multipoles, the pair
+// list and the PME stencils.
+static int setup_work(const amg_params* P, const double* xyz, const double box[6], const orc_options* opt, Work& w) {
     w.P = P;
     System& s = w.s;
     s.n = P->n;
@@ -1540,6 +1540,18 @@ int orc_forward(const amg_params* P, const double* xyz, const double box[6], int
     rotate_multipoles(s, P);
     w.pairs = build_pairs(s);
     if (s.ewald && w.opt.kmax <= 0) pme_setup(s, w.pm);
+    return AMG_OK;
+}
+
+
+
+int orc_forward(const amg_params* P, const double* xyz, const double box[6], int32_t flags,
+                const orc_options* opt, amg_results* res) {
+    if (!P || !xyz || !res || P->n <= 0) return AMG_ERR_BAD_ARG;
+    Work w;
+    const int rc = setup_work(P, xyz, box, opt, w);
+    if (rc != AMG_OK) return rc;
+    System& s = w.s;
     Result R;
     int status;
     const bool vir = (flags & AMG_DO_VIRIAL) != 0;
@@ -1569,6 +1581,23 @@ int orc_forward(const amg_params* P, const double* xyz, const double box[6], int
     for (double v : {R.em, R.ep})
         if (!std::isfinite(v)) return AMG_ERR_NAN;
     return status;
+}
+
+/* Field (u channel: u-scaled, Thole-damped real space, reciprocal space and
+ * the Ewald self term) of the dipoles u [n*3] at every site, into field
+ * [n*3]: the T of (1/alpha - T) u = E, one column block per call, so a test
+ * can build the dense operator of a small system. */
+int orc_dipole_field(const amg_params* P, const double* xyz, const double box[6], const double* u, double* field) {
+    if (!P || !xyz || !u || !field || P->n <= 0) return AMG_ERR_BAD_ARG;
+    Work w;
+    const int rc = setup_work(P, xyz, box, nullptr, w);
+    if (rc != AMG_OK) return rc;
+    std::vector<Mp> M(w.s.n);
+    for (int i = 0; i < w.s.n; i++) M[i] = dipole_only(V3{u[3 * i], u[3 * i + 1], u[3 * i + 2]});
+    std::vector<V3> F;
+    total_field(w, M, 2, F, 1);
+    for (int i = 0; i < w.s.n; i++) { field[3 * i] = F[i].x; field[3 * i + 1] = F[i].y; field[3 * i + 2] = F[i].z; }
+    return AMG_OK;
 }
 
 /* Number of real-space pairs within the cutoff (minimum image). */

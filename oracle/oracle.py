@@ -44,6 +44,9 @@ def lib():
                                   C.c_int32, C.POINTER(orc_options), C.POINTER(abi.amg_results)]
         L.orc_forward.restype = C.c_int
         L.orc_pair_count.argtypes = [C.POINTER(C.c_double), C.c_int32, C.POINTER(C.c_double), C.c_int32, C.c_double]
+        L.orc_dipole_field.argtypes = [C.POINTER(abi.amg_params), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                       C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.orc_dipole_field.restype = C.c_int
         L.orc_pair_count.restype = C.c_int64
         _lib = L
     return _lib
@@ -69,3 +72,16 @@ def pair_count(system, cutoff):
     x = np.ascontiguousarray(system.xyz, np.float64).reshape(-1)
     box = np.ascontiguousarray(system.box, np.float64)
     return int(lib().orc_pair_count(abi.dptr(x), system.n, abi.dptr(box), int(system.use_bounds), cutoff))
+
+
+def dipole_field(system, settings: Settings, u, params=None):
+    """Field [n,3] of the dipoles u [n,3] (the T of (1/alpha - T) u = E)."""
+    P = params or Params(system, settings)
+    x = np.ascontiguousarray(system.xyz, np.float64).reshape(-1)
+    box = np.ascontiguousarray(system.box, np.float64)
+    uu = np.ascontiguousarray(u, np.float64).reshape(-1)
+    out = np.zeros(3 * system.n)
+    rc = lib().orc_dipole_field(C.byref(P.struct), abi.dptr(x), abi.dptr(box), abi.dptr(uu), abi.dptr(out))
+    if rc != abi.AMG_OK:
+        raise RuntimeError(f"oracle failed: {abi.STATUS.get(rc, rc)}")
+    return out.reshape(system.n, 3)

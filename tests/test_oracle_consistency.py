@@ -279,3 +279,48 @@ def test_periodic_ewald_virial_shear_components(box27, poltyp):
             q = oracle.forward(t, st, flags=abi.DO_ENERGY)
             e.append(q.em + q.ep)
         assert abs(W[a, b] - (e[0] - e[1]) / (2 * h)) < 1e-8 * np.abs(W).max()
+
+
+def test_pcg_dipoles_equal_a_dense_solve(box27):
+    """The PCG solution of (1/alpha - T) u = E against Gaussian elimination on
+    the explicit 3N x 3N operator (columns from the field of unit dipoles),
+    for both right-hand sides, with Ewald."""
+    from polmdqc_b200.engine import Params
+    st = Settings(aewald=0.7, nfft=(24, 24, 24), cutoff=4.6)
+    P = Params(box27, st)
+    n3 = 3 * box27.n
+    T = np.zeros((n3, n3))
+    for j in range(n3):
+        e = np.zeros(n3)
+        e[j] = 1.0
+        T[:, j] = oracle.dipole_field(box27, st, e.reshape(-1, 3), params=P).reshape(-1)
+    assert np.abs(T - T.T).max() < 1e-10 * np.abs(T).max()       # symmetric operator
+    alpha = np.repeat(box27.polarity, 3)
+    direct = oracle.forward(box27, dataclasses.replace(st, poltyp=abi.POL_DIRECT))
+    mutual = oracle.forward(box27, dataclasses.replace(st, poleps=1e-12))
+    A = np.diag(1.0 / alpha) - T
+    for u_direct, u_pcg in ((direct.uind, mutual.uind), (direct.uinp, mutual.uinp)):
+        E = u_direct.reshape(-1) / alpha                             # direct dipoles are alpha E
+        u = np.linalg.solve(A, E)
+        assert np.abs(u - u_pcg.reshape(-1)).max() < 1e-10
+
+
+def test_ewald_dimer_approaches_the_isolated_reference():
+    """The reference's water dimer (test/amoeba.h, isolated, its em golden)
+    in growing periodic cubes with Ewald: the difference is the periodic
+    images' dipolar energy, shrinking as 1/V (tinfoil boundary)."""
+    from conftest import golden, ref_dump, ref_fixture
+    d = ref_dump(ref_fixture("amoeba", "water09.xyz"))
+    s = systems.from_dump(d)
+    em_isolated = golden("ref_tests.json")["amoeba1"]["em"]
+    diffs = []
+    for L, K in ((40.0, 48), (60.0, 64), (90.0, 96)):
+        t = copy.deepcopy(s)
+        t.use_bounds = True
+        t.box = np.array([L, L, L, 90.0, 90.0, 90.0])
+        t.xyz = t.xyz - t.xyz.mean(0) + L / 2
+        st = Settings(aewald=0.25, nfft=(K,) * 3, cutoff=min(25.0, L / 2 - 1), poltyp=abi.POL_NONE)
+        diffs.append((L, oracle.forward(t, st, flags=abi.DO_ENERGY).em - em_isolated))
+    vol_scaled = [dv * L ** 3 for L, dv in diffs]
+    assert abs(diffs[-1][1]) < 3e-4
+    assert max(vol_scaled) - min(vol_scaled) < 0.1 * abs(vol_scaled[0])

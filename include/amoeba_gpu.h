@@ -138,10 +138,11 @@ typedef struct amg_params {
                                         0 = diagonal (alpha) */
     double usolvcut;                 /* limits.h usolvcut (Angstrom), at most cutoff */
     /* Appended in ABI version 3 (zero keeps the version-2 behaviour): */
-    int32_t cell_shape;              /* AMG_CELL_*; a cell other than orthogonal
-                                        is supported without Ewald (the reference's
-                                        multipole mode) and returns UNSUPPORTED
-                                        with it */
+    int32_t cell_shape;              /* AMG_CELL_*: every cell works without Ewald
+                                        (the reference's multipole mode); with Ewald
+                                        the prism cells (orthogonal, monoclinic,
+                                        triclinic) work and the octahedron and
+                                        dodecahedron return UNSUPPORTED */
     double opt_coef[AMG_MAX_OPT + 1]; /* polopt.h copt: with AMG_POL_OPT the dipoles
                                         are sum_k (sum_{j>=k} copt_j) u^(k), u^(0) =
                                         alpha E, u^(k) = alpha T u^(k-1); the order is
@@ -196,7 +197,7 @@ int amg_create(const amg_params* params, amg_ctx** out);
  * alpha,beta,gamma (degrees) as boxes.h xbox,ybox,zbox,alphaA,betaA,gammaA.
  * With use_bounds, the minimum image of the cell shape (params cell_shape and
  * the angles) is the reference's image() (src/md/image.cpp:37-124).  Ewald
- * needs an orthogonal box (else UNSUPPORTED). */
+ * needs a prism cell: orthogonal, monoclinic or triclinic (else UNSUPPORTED). */
 int amg_set_coords(amg_ctx* ctx, const double* xyz, const double box[6]);
 
 /* Evaluates em and ep (and their gradients, analysis data, dipoles) for the

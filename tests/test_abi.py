@@ -57,3 +57,34 @@ def test_create_without_gpu_fails_cleanly():
     s = systems.water_box(8, 12.0, seed=0)
     p = Params(s, Settings(nfft=(12, 12, 12), cutoff=5.0))
     assert lib.amg_create(ctypes.byref(p.struct), ctypes.byref(ctx)) == 6   # NO_DEVICE
+
+
+def test_parameter_validation_before_any_device_call():
+    """amg_create checks its parameters before it touches a device, so the
+    statuses of bad inputs hold on any host: unknown polarization model
+    (UNSUPPORTED), OPT without coefficients, unknown cell shape, the sparse
+    preconditioner without usolvcut (BAD_ARG); valid OPT and cell-shape
+    parameters get as far as the device (NO_DEVICE here)."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from polmdqc_b200 import systems
+    from polmdqc_b200.engine import Params, Settings
+    BAD_ARG, UNSUPPORTED, NO_DEVICE = 1, 2, 6
+    lib = abi.load_library()
+    ctx = ctypes.c_void_p()
+    s = systems.water_box(8, 12.0, seed=0)
+
+    def status(**changes):
+        p = Params(s, Settings(nfft=(12, 12, 12), cutoff=5.0))
+        for k, v in changes.items():
+            setattr(p.struct, k, v)
+        return lib.amg_create(ctypes.byref(p.struct), ctypes.byref(ctx))
+
+    assert status(poltyp=7) == UNSUPPORTED
+    assert status(poltyp=abi.POL_OPT) == BAD_ARG          # all opt_coef zero
+    assert status(cell_shape=5) == BAD_ARG
+    assert status(pcg_prec=1, usolvcut=0.0) == BAD_ARG
+    p = Params(s, Settings(nfft=(12, 12, 12), cutoff=5.0, poltyp=abi.POL_OPT, opt_order=4))
+    assert lib.amg_create(ctypes.byref(p.struct), ctypes.byref(ctx)) == NO_DEVICE
+    assert status(cell_shape=abi.CELL_OCTAHEDRON) == NO_DEVICE

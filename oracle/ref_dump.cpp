@@ -38,6 +38,7 @@
 #include "pme.h"
 #include "polar.h"
 #include "polgrp.h"
+#include "polopt.h"
 #include "polpcg.h"
 #include "polpot.h"
 #include "potent.h"
@@ -138,6 +139,9 @@ int main(int argc, char** argv)
         ilists("ip12", n, [](int i) { return np12[i]; }, [](int i, int j) { return ip12[i][j]; });
         ilists("ip13", n, [](int i) { return np13[i]; }, [](int i, int j) { return ip13[i][j]; });
         ilists("ip14", n, [](int i) { return np14[i]; }, [](int i, int j) { return ip14[i][j]; });
+        key("poltyp");
+        fprintf(fo, "\"%s\"", poltyp.c_str());
+        if (poltyp == "OPT") darr("copt", maxopt + 1, [](int i) { return copt[i]; });
     }
     ilists("i12", n, [](int i) { return n12[i]; }, [](int i, int j) { return i12[i][j]; });
     ilists("i13", n, [](int i) { return n13[i]; }, [](int i, int j) { return i13[i][j]; });

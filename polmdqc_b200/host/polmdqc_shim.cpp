@@ -151,8 +151,12 @@ void ensure_context(bool want_polar)
         p.polarity = dev.polar_.data(); p.thole = dev.thole_.data(); p.pdamp = dev.pdamp_.data();
         p.ip11 = dev.g11.view(); p.ip12 = dev.g12.view(); p.ip13 = dev.g13.view(); p.ip14 = dev.g14.view();
         p.poltyp = poltyp == "DIRECT" ? AMG_POL_DIRECT : poltyp == "OPT" ? AMG_POL_OPT : AMG_POL_MUTUAL;
+        // kpolar zeroes copt below index maxopt only (src/md/kpolar.cpp:110-113),
+        // so the last entry may hold a leftover value for orders below 6: a
+        // coefficient that small is no order of the model
         if (poltyp == "OPT")
-            for (int k = 0; k <= maxopt && k <= AMG_MAX_OPT; k++) p.opt_coef[k] = copt[k];
+            for (int k = 0; k <= maxopt && k <= AMG_MAX_OPT; k++)
+                p.opt_coef[k] = std::fabs(copt[k]) > 1e-100 ? copt[k] : 0.0;
     } else {
         p.poltyp = AMG_POL_NONE;
     }

@@ -93,3 +93,26 @@ def test_parameter_assignment_matches_reference(name):
                    ("u_scale", "uscale")):
         assert getattr(s, k) == p[ref], k
     assert p["aeewald"] == 0.5446 and p["nefft"] == [24, 24, 24] and p["bseorder"] == 5
+
+
+@pytest.mark.parametrize("model,order", [("OPT1", 1), ("OPT2", 2), ("OPT3", 3), ("OPT", 4), ("OPT4", 4),
+                                         ("OPT5", 5), ("OPT6", 6)])
+def test_opt_coefficients_match_the_reference(tmp_path, model, order):
+    """The OPT coefficients of polmdqc_b200.engine.OPT_COEF are the reference's
+    own (kpolar, src/md/kpolar.cpp:108-153; plain "OPT" is OPT4), read from
+    its copt after mechanic() with the keyword 'polarization <model>'."""
+    import os
+    from conftest import REF_BUILD
+    from polmdqc_b200.engine import OPT_COEF
+    s = systems.water_box(27, 9.32, seed=1)
+    xyz, key = str(tmp_path / "w.xyz"), str(tmp_path / "w.key")
+    prm = os.path.join(REF_BUILD, "params", "water03.prm")
+    if not os.path.exists(prm):
+        pytest.skip("reference build (oracle/_ref) not present")
+    systems.write_tinker(s, xyz, key, prm, [f"polarization {model}"])
+    d = ref_dump(xyz, key)
+    assert d["poltyp"] == "OPT"
+    want = list(OPT_COEF[order]) + [0.0] * (7 - len(OPT_COEF[order]))
+    # the reference zeroes copt below index maxopt only (kpolar.cpp:110-113),
+    # so its last entry can hold a leftover denormal for orders below 6
+    np.testing.assert_allclose(d["copt"], want, rtol=0, atol=1e-300)

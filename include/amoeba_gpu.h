@@ -242,26 +242,28 @@ int amg_last_virial(amg_ctx* ctx, double vir_em[9], double vir_ep[9]);
  * CUDA graph, and the lanes per site of the pair kernels. */
 int amg_last_stats(amg_ctx* ctx, int64_t* launches, int32_t* graphed, int32_t* lanes_per_site);
 
-/* Allocation-free evaluation of the reference's own electrostatics mode
- * (no counterpart in the reference; it mirrors the empole_a loop of
- * src/md/empole.cpp:96-357): non-Ewald multipole energy and gradient over all
- * pairs within `cutoff`, minimum image in an orthogonal box (box[a] <= 0: no
- * wrapping on that axis), 1-2..1-5 scaling by m_scale.
+/* Allocation-free entry point.  It has no counterpart in the reference: it is
+ * an addition of this library for callers that cannot let a library allocate
+ * device memory -- codes that take all device memory from one arena at
+ * start-up and forbid later allocation, and codes that must not call
+ * cudaMalloc/cudaFree between steps because those calls synchronize the
+ * whole device.  It computes the non-Ewald multipole energy and gradient over
+ * all pairs within `cutoff`, minimum image in an orthogonal box (box NULL, or
+ * box[a] <= 0: no wrapping on that axis), 1-2..1-5 scaling by m_scale.
  *
- * For callers that cannot let a library allocate device memory -- codes that
- * take all device memory from one arena at start-up, or that must not call
- * cudaMalloc/cudaFree between steps because those synchronize the device.
- * It allocates nothing: every pointer argument except m_scale and box is
- * device memory supplied by the caller (xyz [3n], pole [13n], the frame
- * arrays [n], bonded[4] = the 1-2..1-5 lists as device CSR, *em [1],
- * dem [3n], ADDED to); its scratch is one fixed device array of about 1.7 MB
- * that every GPU loading the library holds until exit.  n above
- * AMG_NOALLOC_MAX_ATOMS returns AMG_ERR_OUT_OF_RANGE.  The first call on a
- * device looks up the array's device address; make that call before any
- * stream capture.  All calls share the array: calls that overlap on the GPU
- * (different streams or threads) race and must be serialized by the caller.
- * Runs on `stream` (NULL: the legacy default stream) and returns after it
- * completes.  f = electric / dielec. */
+ * It calls no cudaMalloc, cudaFree or allocating library routine.  Every
+ * pointer argument except m_scale and box is device memory supplied by the
+ * caller: xyz [3n], pole [13n], the frame arrays [n], bonded[4] = the
+ * 1-2..1-5 lists as device CSR.  *em [1] is overwritten with the energy;
+ * dem [3n] is ADDED to.  The kernels' scratch is one fixed device array of
+ * about 1.7 MB that every GPU loading the library holds until exit.
+ * n above AMG_NOALLOC_MAX_ATOMS returns AMG_ERR_OUT_OF_RANGE.  The first call
+ * on a device loads the library's device code there and looks up the
+ * array's device address; make that first call before any stream capture.
+ * All calls share the array, which keeps the last call's contents: calls
+ * that overlap on the GPU (different streams or threads) race and must be
+ * serialized by the caller.  Runs on `stream` (NULL: the legacy default
+ * stream) and returns after it completes.  f = electric / dielec. */
 #define AMG_NOALLOC_MAX_ATOMS 16384
 int amg_empole_direct_noalloc(int32_t n, const double* xyz, const double* pole, const int32_t* zaxis,
                               const int32_t* xaxis, const int32_t* yaxis, const int32_t* polaxe,

@@ -18,7 +18,6 @@
 #include <algorithm>
 #include <climits>
 #include <initializer_list>
-#include <mutex>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -2201,12 +2200,11 @@ void amg_destroy(amg_ctx* ctx) {
 // all device memory out of one arena at start-up and forbid later allocation,
 // and codes that must not allocate between steps because cudaMalloc and
 // cudaFree synchronize the whole device.  amg_empole_direct_noalloc serves
-// them: it evaluates the reference's own electrostatics mode -- non-Ewald
-// multipoles, pairs within a cutoff, 1-n exclusion scaling (the empole_a loop
-// of src/md/empole.cpp:96-357) -- with every buffer supplied by the caller and
-// the kernels' scratch (rotated multipoles, site torques, per-block energy
-// partials) in one fixed device array declared below.  It calls no
-// cudaMalloc/cudaFree and no allocating library routine.
+// them (it has no counterpart in the reference): non-Ewald multipoles, pairs
+// within a cutoff, 1-n exclusion scaling, with every buffer supplied by the
+// caller and the kernels' scratch (rotated multipoles, site torques,
+// per-block energy partials) in one fixed device array declared below.  It
+// calls no cudaMalloc/cudaFree and no allocating library routine.
 // ===========================================================================
 
 namespace {
@@ -2220,12 +2218,9 @@ constexpr int kNoAllocBlocks = kNoAllocMaxAtoms * kNoAllocLanes / kNoAllocThread
 constexpr size_t kNoAllocScratch = (size_t)kNoAllocMaxAtoms * 13 + kNoAllocBlocks;
 
 // Every GPU that loads the library holds this array (about 1.7 MB) until exit.
+// In host code its name is only a stand-in, not a device address: the kernels
+// get the address that cudaGetSymbolAddress returns for the current device.
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratch];
-
-// host-side device address of the scratch array, per device (the symbol's
-// name is only a host-side stand-in, not a device address)
-std::mutex g_noalloc_mutex;
-double* g_noalloc_ptr[64] = {};
 
 // rotate the multipoles (as the main path's frame code) into scratch
 __global__ void k_noalloc_rotate(int n, const double* __restrict__ xyz, const double* __restrict__ pole13,
@@ -2332,21 +2327,24 @@ extern "C" int amg_empole_direct_noalloc(int32_t n, const double* xyz, const dou
         return AMG_ERR_BAD_ARG;
     if (n > kNoAllocMaxAtoms) return AMG_ERR_OUT_OF_RANGE;  // scratch holds AMG_NOALLOC_MAX_ATOMS sites
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return AMG_ERR_NO_DEVICE;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return AMG_ERR_NO_DEVICE;
+    }
+    // The scratch array's device address on the current device, looked up on
+    // every call rather than cached: after a cudaDeviceReset, or under another
+    // context on the same device, the module is loaded again and the array
+    // can move.  The first call on a device also loads the library's device
+    // code there (lazy module loading), which is why that first call belongs
+    // before any stream capture.
     double* scratch = nullptr;
     {
-        // once per device, with that device current: the scratch array's
-        // device address (the first call on a device does this set-up)
-        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-        if (!g_noalloc_ptr[dev]) {
-            void* p = nullptr;
-            if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
-                cudaGetLastError();
-                return AMG_ERR_CUDA;
-            }
-            g_noalloc_ptr[dev] = (double*)p;
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
+            cudaGetLastError();
+            return AMG_ERR_CUDA;
         }
-        scratch = g_noalloc_ptr[dev];
+        scratch = (double*)p;
     }
     if (box)
         for (int a = 0; a < 3; a++)

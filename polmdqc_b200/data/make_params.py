@@ -35,4 +35,6 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python -m polmdqc_b200.data.make_params <reference-root>")
+    main(sys.argv[1])

@@ -252,20 +252,38 @@ def orient_waters(O, box_len, rng, fixed=(), min_contact=1.7, tries=200):
     cell = 3.5
     nc = max(1, int(box_len // cell))
     size = box_len / nc
-    bins = {}
+    # placed atoms binned on a periodic grid of cells >= 3.5 A: positions
+    # [nc, nc, nc, cap, 3] and counts per cell; a candidate is tested against
+    # the 27 cells around its own
+    cap = 16
+    pos = np.zeros((nc, nc, nc, cap, 3))
+    cnt = np.zeros((nc, nc, nc), np.int64)
+    offs = np.array([(dx, dy, dz) for dx in (-1, 0, 1) for dy in (-1, 0, 1) for dz in (-1, 0, 1)])
+    thr = min_contact * min_contact
 
     def key(p):
-        return tuple((np.floor((p % box_len) / size).astype(int)) % nc)
-
-    def near(p):
-        k = key(p)
-        for dx in (-1, 0, 1):
-            for dy in (-1, 0, 1):
-                for dz in (-1, 0, 1):
-                    yield from bins.get(((k[0] + dx) % nc, (k[1] + dy) % nc, (k[2] + dz) % nc), ())
+        return (np.floor((p % box_len) / size).astype(int)) % nc
 
     def add(p):
-        bins.setdefault(key(p), []).append(p)
+        nonlocal pos, cap
+        k = tuple(key(p))
+        if cnt[k] == cap:
+            grown = np.zeros((nc, nc, nc, 2 * cap, 3))
+            grown[:, :, :, :cap] = pos
+            pos, cap = grown, 2 * cap
+        pos[k + (cnt[k],)] = p
+        cnt[k] += 1
+
+    def clash(atoms):
+        for atom in atoms:
+            nb = (key(atom) + offs) % nc
+            c = cnt[nb[:, 0], nb[:, 1], nb[:, 2]]
+            q = pos[nb[:, 0], nb[:, 1], nb[:, 2]][np.arange(cap)[None, :] < c[:, None]]
+            d = atom - q
+            d -= box_len * np.round(d / box_len)
+            if np.any(d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1] + d[:, 2] * d[:, 2] < thr):
+                return True
+        return False
 
     for p in fixed:
         add(p)
@@ -273,16 +291,7 @@ def orient_waters(O, box_len, rng, fixed=(), min_contact=1.7, tries=200):
         for t in range(tries):
             R = random_rotations(rng, 1)
             h = water_geometry(O[w:w + 1], R)[0]
-            ok = True
-            for atom in (h[0], h[1], O[w]):
-                for q in near(atom):
-                    d = atom - q
-                    d -= box_len * np.round(d / box_len)
-                    if d @ d < min_contact * min_contact:
-                        ok = False
-                        break
-                if not ok:
-                    break
+            ok = not clash((h[0], h[1], O[w]))
             if ok or t == tries - 1:
                 break
         H[w] = h

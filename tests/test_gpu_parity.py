@@ -348,25 +348,6 @@ def test_config_4096_waters_vs_oracle(w4096):
     assert frms(gm, o) < 1e-4
 
 
-def test_config_32768_waters_properties():
-    """98,304 atoms, 108^3 grid: mixed vs FP64 on the GPU at the target error,
-    and invariance under a shift by whole grid spacings.  (The net force is
-    not checked: smooth PME does not conserve momentum exactly.)"""
-    s = systems.water_box(32768, 99.3, seed=0)
-    g64 = run(s, Settings(nfft=(108, 108, 108), precision=FP64))
-    gm = run(s, Settings(nfft=(108, 108, 108), precision=MIXED))
-    assert gm.pcg_eps <= 1e-6 and g64.pcg_eps <= 1e-6
-    assert rel(gm.em, g64.em) < 1e-6 and rel(gm.ep, g64.ep) < 1e-6
-    assert frms(gm, g64) < 1e-4
-    # a shift by whole PME grid spacings changes no B-spline weight and no
-    # pair distance: the energy is unchanged to round-off (an arbitrary shift
-    # changes the PME interpolation error, ~1e-5 relative at this grid)
-    shifted = systems.water_box(32768, 99.3, seed=0)
-    shifted.xyz = shifted.xyz + np.array([3.0, -2.0, 5.0]) * (99.3 / 108)
-    gs = run(shifted, Settings(nfft=(108, 108, 108), precision=FP64))
-    assert rel(gs.em, g64.em) < 1e-10 and rel(gs.ep, g64.ep) < 1e-8
-
-
 # ---------------------------------------------------------------- status codes
 def test_status_codes():
     s = systems.water_box(64, 12.4, seed=5)

@@ -81,9 +81,11 @@ $(OUT)/ref_dump: oracle/ref_dump.cpp $(OUT)/libpolmdqc.a
 $(OUT)/data.stamp: $(wildcard $(REF)/params/*.prm)
 	@mkdir -p $(OUT)/params $(OUT)/testFiles
 	cp $(REF)/params/water03.prm $(REF)/params/amoebabio09.prm $(REF)/params/amoebabio18.prm \
-	   $(REF)/params/amoebaplus.prm $(OUT)/params/
+	   $(REF)/params/amoebaplus.prm $(REF)/params/hippoS101.prm $(REF)/params/hippo19.prm \
+	   $(REF)/params/water21.prm $(OUT)/params/
 	cp -r $(REF)/test/testFiles/amoeba $(REF)/test/testFiles/bounds $(REF)/test/testFiles/rotpole \
-	   $(REF)/test/testFiles/amoebap $(OUT)/testFiles/
+	   $(REF)/test/testFiles/amoebap $(REF)/test/testFiles/chkpole $(REF)/test/testFiles/amoebaMisc \
+	   $(REF)/test/testFiles/hippo $(OUT)/testFiles/
 	touch $@
 
 .PHONY: all shim

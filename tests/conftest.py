@@ -34,6 +34,39 @@ def ref_fixture(*parts):
     return p
 
 
+def last_structure(xyz, key, tmpdir):
+    """The last structure of a concatenated Tinker .xyz (the reference's
+    analyze processes every structure; its goldens hold the last one),
+    written to tmpdir with a copy of the keyfile whose parameter path is
+    made absolute.  Returns (xyz, key) paths."""
+    def is_box_line(line):
+        f = line.split()
+        try:
+            return len(f) == 6 and all(float(v) == float(v) for v in f)
+        except ValueError:
+            return False
+
+    lines = open(xyz).read().splitlines()
+    frames, i = [], 0
+    while i < len(lines) and lines[i].strip():
+        n = int(lines[i].split()[0])
+        end = i + 1 + n + (1 if i + 1 < len(lines) and is_box_line(lines[i + 1]) else 0)
+        frames.append((i, end))
+        i = end
+    s, end = frames[-1]
+    out_xyz = os.path.join(tmpdir, "last.xyz")
+    with open(out_xyz, "w") as f:
+        f.write("\n".join(lines[s:end]) + "\n")
+    out_key = os.path.join(tmpdir, "last.key")
+    with open(out_key, "w") as f:
+        for line in open(key):
+            w = line.split()
+            if w and w[0].lower() == "parameters":
+                line = f"parameters {os.path.normpath(os.path.join(os.path.dirname(key), w[1]))}\n"
+            f.write(line)
+    return out_xyz, out_key
+
+
 def ref_dump(xyz, key=None):
     """Runs the compiled reference on a Tinker .xyz (+ .key) and returns its
     globals (oracle/ref_dump.cpp)."""

@@ -1,13 +1,14 @@
 """Generates the committed golden fixtures of tests/golden/ from the reference.
 
-    python tests/golden/make_golden.py [reference-root]
+    python tests/golden/make_golden.py <reference-root>
 
 Needs the compiled reference (oracle/_ref, built by `make -f oracle/ref.mk`)
-and the reference source tree (default /root/reference).  Writes:
+and the reference source tree.  Writes:
 
   ref_tests.json        the expected values the reference's own Catch2 tests
-                        hold (test/amoeba.h, test/bounds.h), parsed from the
-                        headers, with the input files they apply to;
+                        hold (test/amoeba.h, bounds.h, chkpole.h,
+                        amoebaMisc.h, rotpole.h), parsed from the headers,
+                        with the input files they apply to;
   ref_water216.json     the reference run (oracle/_ref/ref_dump) on the
                         seeded 216-water box in its only electrostatics mode
                         (non-Ewald multipoles, 7 A cutoff): em, nem, dem, vir,
@@ -49,6 +50,9 @@ def parse_header(path):
             d[mm.group(1)] = float(mm.group(2))
         for mm in re.finditer(r"std::vector<real>\s+(\w+)\s*=\s*\{(.*?)\};", body, re.S):
             d[mm.group(1)] = [float(v) for v in mm.group(2).replace("\n", " ").split(",") if v.strip()]
+        for mm in re.finditer(r"std::vector<std::vector<real>>\s+(\w+)\s*=\s*\{(.*?)\};", body, re.S):
+            rows = re.findall(r"\{([^{}]*)\}", mm.group(2))
+            d[mm.group(1)] = [[float(v) for v in r.replace("\n", " ").split(",") if v.strip()] for r in rows]
         out[name] = d
     return out
 
@@ -60,15 +64,34 @@ def run_dump(xyz, key, cwd):
     return json.load(open(out))
 
 
-def main(ref_root="/root/reference"):
+def main(ref_root):
     # ---- golden values of the reference's own tests
-    amoeba = parse_header(os.path.join(ref_root, "test", "amoeba.h"))
-    bounds = parse_header(os.path.join(ref_root, "test", "bounds.h"))
+    hdr = {h: parse_header(os.path.join(ref_root, "test", h + ".h"))
+           for h in ("amoeba", "bounds", "chkpole", "amoebaMisc", "rotpole")}
+    amoeba, bounds = hdr["amoeba"], hdr["bounds"]
     tests = {
-        "source": "test/amoeba.h, test/bounds.h of momokchung/polmdqc",
+        "source": "test/amoeba.h, bounds.h, chkpole.h, amoebaMisc.h, rotpole.h of momokchung/polmdqc",
         "amoeba1": {"inputs": "test/testFiles/amoeba/water09.xyz (+ water09.key)", **amoeba["amoeba1"]},
         "amoeba2": {"inputs": "test/testFiles/amoeba/water09.xyz (+ water09.key)", **amoeba["amoeba2"]},
     }
+    # chiral Z-then-X sites (alanine tetrapeptide, amoebabio09, multipoles only)
+    for k in ("chkpole1", "chkpole2"):
+        tests[k] = {"inputs": "test/testFiles/chkpole/alatet.xyz (+ alatet.key)", **hdr["chkpole"][k]}
+    # reader cases: a versioned file name (water09 -> water09.xyz_2), a
+    # concatenated file (the goldens hold its last structure, the water
+    # dimer) and non-sequential atom numbers
+    misc_inputs = {"amoebaMisc1": "test/testFiles/amoebaMisc/water09 (the reader opens water09.xyz_2)",
+                   "amoebaMisc2": "test/testFiles/amoebaMisc/alatet_water09.xyz (last structure)",
+                   "amoebaMisc3": "test/testFiles/amoebaMisc/alatet_water09.xyz (last structure)",
+                   "amoebaMisc5": "test/testFiles/amoebaMisc/water09NSeq.xyz"}
+    for k, inp in misc_inputs.items():
+        tests[k] = {"inputs": inp, **hdr["amoebaMisc"][k]}
+    # frames: Z-Only (rotpole2) and Z-Bisect + 3-Fold (rotpole3) in HIPPO
+    # inputs; only the rotated multipoles are used here (the energies include
+    # charge penetration)
+    for k, inp in (("rotpole2", "test/testFiles/rotpole/benzene_ethyne_water.xyz"),
+                   ("rotpole3", "test/testFiles/rotpole/ammonia.xyz")):
+        tests[k] = {"inputs": inp, **hdr["rotpole"][k]}
     shapes = {"bounds1": "orthogonal", "bounds2": "monoclinic", "bounds3": "triclinic", "bounds4": "octahedron",
               "bounds5": "dodecahedron"}
     for k, shape in shapes.items():
@@ -118,4 +141,6 @@ def main(ref_root="/root/reference"):
 
 
 if __name__ == "__main__":
-    main(*(sys.argv[1:2]))
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <reference-root>")
+    main(sys.argv[1])

@@ -90,3 +90,37 @@ def test_dropin_ewald_polarization_matches_oracle():
     np.testing.assert_allclose(d["dem"], o.dem.reshape(-1), atol=1e-7)
     np.testing.assert_allclose(d["dep"], o.dep.reshape(-1), atol=1e-5)
     np.testing.assert_allclose(d["uind"], o.uind.reshape(-1), atol=1e-7)
+
+
+def test_dropin_chiral_sites_golden():
+    """chkpole-1/-2 (alanine tetrapeptide, chiral Z-then-X sites) through the
+    reference's own set-up and energy() with the shim."""
+    g = golden("ref_tests.json")
+    d = dump_gpu(ref_fixture("chkpole", "alatet.xyz"))
+    c1, c2 = g["chkpole1"], g["chkpole2"]
+    assert d["nem"] == c1["nem"]
+    assert abs(d["em"] - c1["em"]) < c1["eps"]
+    np.testing.assert_allclose(d["aem"], c1["aem"], atol=c1["eps"], rtol=0)
+    np.testing.assert_allclose(d["dem"], c2["dem"], atol=c2["eps1"], rtol=0)
+
+
+def test_dropin_analyze_program_reads_every_structure():
+    """amoebaMisc-2: the reference's own analyze program, linked with the
+    shim, on a concatenated file (alanine tetrapeptide, then the water
+    dimer).  The shim rebuilds its device context when the system changes;
+    the last structure's line ' Atomic Multipoles  <em> <nem>' (8 decimals,
+    the keyfile's 'digits 8') matches the golden."""
+    exe = os.path.join(REF_BUILD, "analyze_gpu")
+    if not os.path.exists(exe):
+        pytest.skip("shim-linked reference build not present")
+    g = golden("ref_tests.json")["amoebaMisc2"]
+    xyz = ref_fixture("amoebaMisc", "alatet_water09.xyz")
+    env = dict(os.environ, AMG_PRECISION="fp64")
+    out = subprocess.run([exe, xyz, "e"], cwd=os.path.dirname(xyz), env=env, capture_output=True, text=True,
+                         check=True).stdout
+    rows = [line.split() for line in out.splitlines() if line.startswith(" Atomic Multipoles")]
+    assert len(rows) == 2, out[-2000:]
+    em, nem = float(rows[-1][2]), int(rows[-1][3])
+    assert nem == g["nem"]
+    assert abs(em - g["em"]) < 1e-8
+    assert abs(float(rows[0][2]) - g["em"]) > 1.0     # the first structure is the peptide

@@ -116,3 +116,77 @@ def test_opt_coefficients_match_the_reference(tmp_path, model, order):
     # the reference zeroes copt below index maxopt only (kpolar.cpp:110-113),
     # so its last entry can hold a leftover denormal for orders below 6
     np.testing.assert_allclose(d["copt"], want, rtol=0, atol=1e-300)
+
+
+def _analysis(d):
+    s = systems.from_dump(d)
+    return s, oracle.forward(s, nonewald(d["mpolecut"]), flags=abi.DO_ENERGY | abi.DO_GRADIENT | abi.DO_ANALYSIS)
+
+
+def flip_chiral_sites(s):
+    """The other chirality at every chiral Z-then-X site: yaxis and the
+    y-components of the local multipoles (dipole y, quadrupole xy/yx/yz/zy)
+    change sign, which is what the reference's chkpole undoes when the
+    site's chirality disagrees with the sign of yaxis
+    (src/md/chkpole.cpp:44-89).  Returns the number of sites flipped."""
+    sites = [i for i in range(s.n) if s.polaxe[i] == abi.FRAME_ZTHENX and s.yaxis[i] != 0]
+    for i in sites:
+        s.yaxis[i] = -s.yaxis[i]
+        for c in (2, 5, 7, 9, 11):
+            s.pole[i, c] = -s.pole[i, c]
+    return len(sites)
+
+
+def test_chiral_sites_golden():
+    """test/chkpole.cpp chkpole-1/-2: alanine tetrapeptide (amoebabio09),
+    chiral Z-then-X sites: em, nem, einter, aem and dem at 1e-10; the same
+    values when every chiral site is given the opposite chirality first."""
+    g = golden("ref_tests.json")
+    d = ref_dump(ref_fixture("chkpole", "alatet.xyz"))
+    s, r = _analysis(d)
+    c1, c2 = g["chkpole1"], g["chkpole2"]
+    assert r.nem == c1["nem"]
+    assert abs(r.em - c1["em"]) < c1["eps"] and abs(r.einter - c1["einter"]) < c1["eps"]
+    np.testing.assert_allclose(r.aem, c1["aem"], atol=c1["eps"], rtol=0)
+    np.testing.assert_allclose(r.dem.reshape(-1), c2["dem"], atol=c2["eps1"], rtol=0)
+    assert flip_chiral_sites(s) == 3
+    f = oracle.forward(s, nonewald(d["mpolecut"]), flags=abi.DO_ENERGY | abi.DO_GRADIENT)
+    assert abs(f.em - c1["em"]) < c1["eps"]
+    np.testing.assert_allclose(f.dem.reshape(-1), c2["dem"], atol=c2["eps1"], rtol=0)
+
+
+@pytest.mark.parametrize("case,parts", [("amoebaMisc1", ("amoebaMisc", "water09")),
+                                        ("amoebaMisc2", ("amoebaMisc", "alatet_water09.xyz")),
+                                        ("amoebaMisc5", ("amoebaMisc", "water09NSeq.xyz"))])
+def test_reader_cases_golden(tmp_path, case, parts):
+    """test/amoebaMisc.cpp amoebaMisc-1/-2/-3/-5: a versioned file name, the
+    last structure of a concatenated file, non-sequential atom numbers."""
+    import os
+    g = golden("ref_tests.json")[case]
+    xyz = ref_fixture(*parts) if parts[1] != "water09" else os.path.join(
+        os.path.dirname(ref_fixture("amoebaMisc", "water09.xyz")), "water09")
+    if case == "amoebaMisc2":
+        from conftest import last_structure
+        xyz, key = last_structure(xyz, ref_fixture("amoebaMisc", "alatet_water09.key"), str(tmp_path))
+        d = ref_dump(xyz, key)
+    else:
+        d = ref_dump(xyz)
+    _, r = _analysis(d)
+    assert r.nem == g["nem"]
+    assert abs(r.em - g["em"]) < g["eps"] and abs(r.einter - g["einter"]) < g["eps"]
+    np.testing.assert_allclose(r.aem, g["aem"], atol=g["eps"], rtol=0)
+    if case == "amoebaMisc2":
+        g3 = golden("ref_tests.json")["amoebaMisc3"]
+        np.testing.assert_allclose(r.dem.reshape(-1), g3["dem"], atol=g3["eps1"], rtol=0)
+
+
+@pytest.mark.parametrize("case,name", [("rotpole2", "benzene_ethyne_water.xyz"), ("rotpole3", "ammonia.xyz")])
+def test_frames_golden_rotated_multipoles(case, name):
+    """test/rotpole.cpp rotpole-2 (Z-Only) and rotpole-3 (Z-Bisect, 3-Fold):
+    the rotated multipoles at 1e-14 (the reference holds them at 1e-16 against
+    its own Eigen rotation; the restatement here rounds differently)."""
+    g = golden("ref_tests.json")[case]
+    d = ref_dump(ref_fixture("rotpole", name))
+    s = systems.from_dump(d)
+    r = oracle.forward(s, nonewald(d["mpolecut"]), flags=abi.DO_ENERGY)
+    np.testing.assert_allclose(r.rpole, np.array(g["rpole"]), atol=1e-14, rtol=0)

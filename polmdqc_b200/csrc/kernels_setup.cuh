@@ -234,7 +234,7 @@ __global__ void k_neighbors(int n, const double4* __restrict__ spos, const unsig
 // order, each in sorted order), so the rows are identical too.  Staging is
 // chunked (kNbrChunk candidates, kNbrHome home atoms at a time), so any cell
 // occupancy works.
-constexpr int kNbrChunk = 1536;
+constexpr int kNbrChunk = 1280;
 constexpr int kNbrHome = 128;
 constexpr int kNbrThreads = 256;
 
@@ -247,6 +247,11 @@ __global__ void __launch_bounds__(kNbrThreads) k_neighbors_cells(
     __shared__ int csrt[kNbrChunk];  // sorted index
     __shared__ int cid[kNbrChunk];   // site index
     __shared__ int hcnt[kNbrHome];
+    // home sites of the current chunk: position relative to the cell corner,
+    // site index, scaled-partner range (CSR offsets) and index range
+    __shared__ float4 hpos[kNbrHome];
+    __shared__ int hid[kNbrHome], hx0[kNbrHome], hx1[kNbrHome];
+    __shared__ int2 hxr[kNbrHome];
     __shared__ int rstart[27], rpre[28];
     __shared__ double rshift[27][3];
     __shared__ int nst;
@@ -258,36 +263,49 @@ __global__ void __launch_bounds__(kNbrThreads) k_neighbors_cells(
     double corner[3];
 #pragma unroll
     for (int a = 0; a < 3; a++) corner[a] = cg.origin[a] + cc[a] * cg.size[a];
-    if (threadIdx.x == 0) {
-        int k = 0, pre = 0;
-        for (int dx = cg.off_lo[0]; dx <= cg.off_hi[0]; dx++)
-            for (int dy = cg.off_lo[1]; dy <= cg.off_hi[1]; dy++)
-                for (int dz = cg.off_lo[2]; dz <= cg.off_hi[2]; dz++) {
-                    const int d[3] = {dx, dy, dz};
-                    int q[3];
-                    double sh[3];
-                    bool skip = false;
-                    for (int a = 0; a < 3; a++) {
-                        q[a] = cc[a] + d[a];
-                        sh[a] = 0.0;
-                        if (cg.periodic) {
-                            if (q[a] < 0) { q[a] += cg.nc[a]; sh[a] = -bx.L[a]; }
-                            else if (q[a] >= cg.nc[a]) { q[a] -= cg.nc[a]; sh[a] = bx.L[a]; }
-                        } else if (q[a] < 0 || q[a] >= cg.nc[a]) {
-                            skip = true;
-                        }
-                    }
-                    if (skip) continue;
-                    const int qc = (q[0] * cg.nc[1] + q[1]) * cg.nc[2] + q[2];
-                    const int len = cend[qc] - cstart[qc];
-                    rstart[k] = cstart[qc];
-                    rpre[k] = pre;
-                    for (int a = 0; a < 3; a++) rshift[k][a] = sh[a];
-                    pre += len > 0 ? len : 0;
-                    k++;
+    if (threadIdx.x < 32) {
+        // stencil cell k = lane (all of a warp's loads of cstart/cend in
+        // flight at once), lengths summed by a warp scan; cells outside an
+        // open system's grid count as empty
+        const int na0 = cg.off_hi[0] - cg.off_lo[0] + 1, na1 = cg.off_hi[1] - cg.off_lo[1] + 1;
+        const int na2 = cg.off_hi[2] - cg.off_lo[2] + 1;
+        const int k = threadIdx.x, total = na0 * na1 * na2;
+        int len = 0;
+        if (k < total) {
+            const int d[3] = {cg.off_lo[0] + k / (na1 * na2), cg.off_lo[1] + (k / na2) % na1, cg.off_lo[2] + k % na2};
+            int q[3];
+            double sh[3];
+            bool skip = false;
+            for (int a = 0; a < 3; a++) {
+                q[a] = cc[a] + d[a];
+                sh[a] = 0.0;
+                if (cg.periodic) {
+                    if (q[a] < 0) { q[a] += cg.nc[a]; sh[a] = -bx.L[a]; }
+                    else if (q[a] >= cg.nc[a]) { q[a] -= cg.nc[a]; sh[a] = bx.L[a]; }
+                } else if (q[a] < 0 || q[a] >= cg.nc[a]) {
+                    skip = true;
                 }
-        rpre[k] = pre;
-        nst = k;
+            }
+            rstart[k] = 0;
+            if (!skip) {
+                const int qc = (q[0] * cg.nc[1] + q[1]) * cg.nc[2] + q[2];
+                const int s0 = cstart[qc];
+                len = max(cend[qc] - s0, 0);
+                rstart[k] = s0;
+            }
+            for (int a = 0; a < 3; a++) rshift[k][a] = sh[a];
+        }
+        int incl = len;  // inclusive scan over the warp
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (k >= o) incl += v;
+        }
+        if (k < total) rpre[k] = incl - len;
+        if (k == total - 1) {
+            rpre[total] = incl;
+            nst = total;
+        }
     }
     __syncthreads();
     const int M = rpre[nst];
@@ -301,7 +319,18 @@ __global__ void __launch_bounds__(kNbrThreads) k_neighbors_cells(
     const unsigned below = (1u << lane) - 1u;
     for (int h0 = hs; h0 < he; h0 += kNbrHome) {
         const int hn = min(kNbrHome, he - h0);
-        for (int t = threadIdx.x; t < hn; t += blockDim.x) hcnt[t] = 0;
+        for (int t = threadIdx.x; t < hn; t += blockDim.x) {
+            // every thread loads one home site: the warps below then start
+            // their scans without a chain of dependent global loads
+            hcnt[t] = 0;
+            const int i = sids[h0 + t];
+            const double4 xi = spos[h0 + t];
+            hpos[t] = make_float4((float)rel(xi.x, 0), (float)rel(xi.y, 1), (float)rel(xi.z, 2), 0.f);
+            hid[t] = i;
+            hx0[t] = xoff[i];
+            hx1[t] = xoff[i + 1];
+            hxr[t] = xrange[i];
+        }
         for (int m0 = 0; m0 < M; m0 += kNbrChunk) {
             const int mn = min(kNbrChunk, M - m0);
             __syncthreads();  // the previous chunk is consumed and hcnt is initialised
@@ -321,11 +350,11 @@ __global__ void __launch_bounds__(kNbrThreads) k_neighbors_cells(
             __syncthreads();
             for (int hh = warp; hh < hn; hh += nwarp) {
                 const int ph = h0 + hh;
-                const int i = sids[ph];
-                const double4 xi = spos[ph];
-                const float hx = (float)rel(xi.x, 0), hy = (float)rel(xi.y, 1), hz = (float)rel(xi.z, 2);
-                const int x0 = xoff[i], x1 = xoff[i + 1];
-                const int2 xr = xrange[i];  // index range of i's scaled partners
+                const int i = hid[hh];
+                const float4 hp = hpos[hh];
+                const float hx = hp.x, hy = hp.y, hz = hp.z;
+                const int x0 = hx0[hh], x1 = hx1[hh];
+                const int2 xr = hxr[hh];  // index range of i's scaled partners
                 const int limit = cap - (x1 - x0);  // the row's tail holds the scaled partners
                 // the first kExcl scaled partners in registers, the rest read when needed
                 constexpr int kExcl = 8;
@@ -346,6 +375,7 @@ __global__ void __launch_bounds__(kNbrThreads) k_neighbors_cells(
                             j = cid[t];
                             hit = j != i;
                             if (hit && r2 > lo2) {  // near the cutoff: the FP64 test
+                                const double4 xi = spos[ph];
                                 const double4 pj = spos[csrt[t]];
                                 const double rx = wrap1<double>(pj.x - xi.x, bx.L[0], bx.iL[0]);
                                 const double ry = wrap1<double>(pj.y - xi.y, bx.L[1], bx.iL[1]);

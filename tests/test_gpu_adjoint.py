@@ -146,3 +146,94 @@ def test_dipole_cotangents_need_the_adjoint_solve(box):
         b.xyz[atom, ax] -= h
         num = (L(a) - L(b)) / (2 * h)
         assert abs(num - g["d_xyz"][atom, ax]) < 1e-5 * max(1.0, abs(num))
+
+
+# ---------------------------------------------------------------- torch.autograd
+class _Selected:
+    """A few scalar parameters of the box, as one vector theta: a charge, a
+    dipole component, a polarizability (pdamp follows as alpha^(1/6)), a
+    Thole factor and a coordinate."""
+    SLOTS = (("pole", (0, 0)), ("pole", (1, 3)), ("polarity", (0,)), ("thole", (1,)), ("xyz", (2, 1)),
+             ("polarity", (4,)))
+
+    def __init__(self, box):
+        self.box = box
+
+    def values(self):
+        return np.array([getattr(self.box, name)[idx] for name, idx in self.SLOTS])
+
+    def system(self, theta):
+        s = copy.deepcopy(self.box)
+        for (name, idx), v in zip(self.SLOTS, theta):
+            getattr(s, name)[idx] = v
+        s.pdamp = s.polarity ** (1 / 6)
+        return s
+
+    @staticmethod
+    def pick(g):
+        full = {"pole": g["d_pole"], "polarity": g["d_polarity"], "thole": g["d_thole"], "xyz": g["d_xyz"]}
+        return np.array([full[name][idx] for name, idx in _Selected.SLOTS])
+
+
+def make_amoeba_function(sel, gd, gp):
+    """torch.autograd.Function over the C ABI: forward = amg_forward (FP64),
+    outputs E = em + ep and L = <gd, uind> + <gp, uinp>; backward =
+    amg_backward with d_energy = dE and the dipole cotangents dL gd, dL gp
+    (the adjoint PCG solve).  Test harness only: the library itself has no
+    torch dependency."""
+    import torch
+
+    class AmoebaEnergy(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, theta):
+            eng = Engine(sel.system(theta.detach().cpu().numpy()), ST)
+            r = eng.forward(abi.DO_ENERGY | abi.DO_GRADIENT | abi.DO_DIPOLES)
+            ctx.eng = eng
+            E = r.em + r.ep
+            L = gd @ r.uind.reshape(-1) + gp @ r.uinp.reshape(-1)
+            return theta.new_tensor(E), theta.new_tensor(L)
+
+        @staticmethod
+        def backward(ctx, dE, dL):
+            # the context stays open for repeated backward calls on one
+            # forward (gradcheck makes one per output); Engine closes it when
+            # the autograd node is released
+            cE = 0.0 if dE is None else float(dE)
+            cL = 0.0 if dL is None else float(dL)
+            g = ctx.eng.backward(d_energy=cE, d_uind=cL * gd, d_uinp=cL * gp)
+            return torch.tensor(_Selected.pick(g), dtype=torch.float64)
+
+    return AmoebaEnergy
+
+
+def test_autograd_function_gradcheck(box):
+    """torch.autograd.gradcheck of the wrapped forward/backward against
+    central differences (step 1e-4) of the GPU's own FP64 forward, for both
+    outputs (energy, and a dipole functional that needs the adjoint solve)."""
+    import torch
+    rng = np.random.default_rng(5)
+    gd, gp = rng.standard_normal(3 * box.n), rng.standard_normal(3 * box.n)
+    sel = _Selected(box)
+    fn = make_amoeba_function(sel, gd, gp)
+    theta = torch.tensor(sel.values(), dtype=torch.float64, requires_grad=True)
+    assert torch.autograd.gradcheck(fn.apply, (theta,), eps=1e-4, atol=1e-4, rtol=1e-5, nondet_tol=1e-7)
+
+
+def test_adjoint_matches_oracle_finite_differences(box, grads):
+    """Parameter gradients of amg_backward against central differences of the
+    FP64 CPU oracle's energies (not the GPU's): a charge, a dipole component,
+    a polarizability, a Thole factor and a coordinate, 1e-5 relative."""
+    from oracle import oracle
+    _, g = grads
+    sel = _Selected(box)
+    theta0 = sel.values()
+    an = _Selected.pick(g)
+    h = 1e-5
+    for k in range(len(theta0)):
+        tp, tm = theta0.copy(), theta0.copy()
+        tp[k] += h
+        tm[k] -= h
+        ep = oracle.forward(sel.system(tp), ST, tol=1e-12, flags=abi.DO_ENERGY)
+        em = oracle.forward(sel.system(tm), ST, tol=1e-12, flags=abi.DO_ENERGY)
+        num = ((ep.em + ep.ep) - (em.em + em.ep)) / (2 * h)
+        assert abs(num - an[k]) < 1e-5 * max(1.0, abs(num)), (k, num, an[k])

@@ -99,10 +99,8 @@ struct Atoms {
     R4<R>* u4 = nullptr;  // [n][2] dipoles
     R4<R>* p4 = nullptr;  // [n][2] PCG directions
     R4<R>* s4 = nullptr;  // [n][2] alpha r, input of the sparse preconditioner
-    R4<R>* c0 = nullptr;  // [n][cap] stored T coefficients (r, B1)
-    R* c1 = nullptr;      // [n][cap] B2
-    R4<R>* cu0 = nullptr; // [n][cap] sparse preconditioner coefficients (r, B1), rows nbru
-    R* cu1 = nullptr;     // [n][cap] B2
+    R4<R>* c0 = nullptr;  // [n][cap] stored T coefficients (pack_tensor)
+    R4<R>* cu0 = nullptr; // [n][cap] sparse preconditioner coefficients (pack_tensor), rows nbru
     int cap = 0;
 };
 
@@ -205,6 +203,7 @@ struct amg_ctx {
     double4* adj_vec = nullptr;  // [n][5]
     double* adj_phi = nullptr;   // [3][2][n][20]
     double* adj_dpole = nullptr; // [n][13]
+    double* adj_opt = nullptr;   // OPT: cotangent orders [K+1][2][3n], then P1, P2 [3n] each
     std::string graph_note;
     double timing[5] = {0, 0, 0, 0, 0};
     // last forward state for the adjoint
@@ -584,10 +583,8 @@ void ensure_coeff_buffers(amg_ctx* ctx, Atoms<R>& A) {
     }
     if (A.cap == ctx->cap && A.c0) return;
     dalloc(ctx, A.c0, (size_t)ctx->cap * ctx->n);
-    dalloc(ctx, A.c1, (size_t)ctx->cap * ctx->n);
     if (ctx->sparse_prec) {
         dalloc(ctx, A.cu0, (size_t)ctx->cap * ctx->n);
-        dalloc(ctx, A.cu1, (size_t)ctx->cap * ctx->n);
         if (!A.s4) dalloc(ctx, A.s4, 2 * (size_t)ctx->n);
     }
     A.cap = ctx->cap;
@@ -734,7 +731,8 @@ template <class R>
 void spread_dipoles(amg_ctx* ctx, cudaStream_t s, const double* vd, const double* vp) {
     Pme<R>& pm = pme_of<R>(ctx);
     int3 K = make_int3(ctx->K[0], ctx->K[1], ctx->K[2]);
-    k_spread_dipoles<R, kOrder><<<ctx->n, 128, 0, s>>>(ctx->n, ctx->sids, vd, vp, pm.theta, pm.k0, K, ctx->frac,
+    k_spread_dipoles<R, kOrder><<<nblk(ctx->n, kLineSites), 128, 0, s>>>(ctx->n, ctx->sids, vd, vp, pm.theta, pm.k0,
+                                                                          K, ctx->frac,
                                                         pm.zg);
     KCHECK();
 }
@@ -830,8 +828,8 @@ void build_scaled_coeffs(amg_ctx* ctx, cudaStream_t s) {
     const bool sp = ctx->sparse_prec;
     k_scaled_coeffs<R><<<nblk(ctx->nsp), kThreads, 0, s>>>(
         ctx->nsp, ctx->sp, ctx->xyz, ctx->pdamp, ctx->thole, ctx->bx, ctx->cut * ctx->cut, ewald_alpha(ctx), ctx->nnb,
-        ctx->cap, ctx->nbr, A.c0, A.c1, ctx->usolvcut * ctx->usolvcut, sp ? ctx->nnbu : nullptr,
-        sp ? ctx->nbru : nullptr, sp ? A.cu0 : nullptr, sp ? A.cu1 : nullptr);
+        ctx->cap, ctx->nbr, A.c0, ctx->usolvcut * ctx->usolvcut, sp ? ctx->nnbu : nullptr,
+        sp ? ctx->nbru : nullptr, sp ? A.cu0 : nullptr);
     KCHECK();
 }
 
@@ -846,20 +844,19 @@ void build_tu_coeffs(amg_ctx* ctx, cudaStream_t s) {
     int* nbru = sp ? ctx->nbru : nullptr;
     int* nnbu = sp ? ctx->nnbu : nullptr;
     R4<R>* cu0 = sp ? A.cu0 : nullptr;
-    R* cu1 = sp ? A.cu1 : nullptr;
     LPA_DISPATCH(ctx->lpa, {
         if (ewald_cells(ctx))
             k_tu_coeffs<R, true, 8, true><<<nblk((size_t)n * 8), kThreads, 0, s>>>(n, ctx->sids, A.at, ctx->bx, (R)ctx->aewald,
-                                                                                   ctx->nbr, ctx->cap, ctx->nnb, A.c0, A.c1,
-                                                                                   (R)u2, nbru, cu0, cu1, nnbu);
+                                                                                   ctx->nbr, ctx->cap, ctx->nnb, A.c0,
+                                                                                   (R)u2, nbru, cu0, nnbu);
         else if (ctx->ewald)
             k_tu_coeffs<R, true, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(n, ctx->sids, A.at, ctx->bx, (R)ctx->aewald, ctx->nbr,
-                                                                             ctx->cap, ctx->nnb, A.c0, A.c1, (R)u2, nbru,
-                                                                             cu0, cu1, nnbu);
+                                                                             ctx->cap, ctx->nnb, A.c0, (R)u2, nbru,
+                                                                             cu0, nnbu);
         else
             k_tu_coeffs<R, false, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(n, ctx->sids, A.at, ctx->bx, (R)0, ctx->nbr, ctx->cap,
-                                                                              ctx->nnb, A.c0, A.c1, (R)u2, nbru, cu0,
-                                                                              cu1, nnbu);
+                                                                              ctx->nnb, A.c0, (R)u2, nbru, cu0,
+                                                                              nnbu);
     });
     KCHECK();
     build_scaled_coeffs<R>(ctx, s);
@@ -875,7 +872,7 @@ void matvec_stored(amg_ctx* ctx, cudaStream_t s, const R4<R>* v4, const double* 
     // real space on the side stream, PME on s
     cudaStream_t r = ctx->ewald ? fork_side(ctx, s) : s;
     LPA_DISPATCH(ctx->lpa, {
-        k_tu_stored<R, L><<<nblk((size_t)n * L), kThreads, 0, r>>>(n, ctx->sids, ctx->nbr, A.c0, A.c1, ctx->cap, ctx->nnb, ctx->xoff,
+        k_tu_stored<R, L><<<nblk((size_t)n * L), kThreads, 0, r>>>(n, ctx->sids, ctx->nbr, A.c0, ctx->cap, ctx->nnb, ctx->xoff,
                                                                     v4, ctx->Fd, ctx->Fp);
     });
     KCHECK();
@@ -920,12 +917,12 @@ void precondition(amg_ctx* ctx, cudaStream_t s, bool first, double* rz_out, cuda
     const double thr = pcg_threshold(ctx);
     if (first)
         k_precond<R, L, true><<<blocks, kThreads, 0, s>>>(
-            n, ctx->sids, ctx->nbru, A.cu0, A.cu1, ctx->cap, ctx->nnbu, ctx->xoff, A.s4, ctx->pol, kPrecDiag, ctx->rd,
+            n, ctx->sids, ctx->nbru, A.cu0, ctx->cap, ctx->nnbu, ctx->xoff, A.s4, ctx->pol, kPrecDiag, ctx->rd,
             ctx->rp, ctx->zd, ctx->zp, ctx->pd, ctx->pp, A.p4, rz_out, ctx->dir_done, ctx->iter, thr, ctx->politer, h,
             use_handle, ctx->cont);
     else
         k_precond<R, L, false><<<blocks, kThreads, 0, s>>>(
-            n, ctx->sids, ctx->nbru, A.cu0, A.cu1, ctx->cap, ctx->nnbu, ctx->xoff, A.s4, ctx->pol, kPrecDiag, ctx->rd,
+            n, ctx->sids, ctx->nbru, A.cu0, ctx->cap, ctx->nnbu, ctx->xoff, A.s4, ctx->pol, kPrecDiag, ctx->rd,
             ctx->rp, ctx->zd, ctx->zp, ctx->pd, ctx->pp, A.p4, rz_out, ctx->dir_done, ctx->iter, thr, ctx->politer, h,
             use_handle, ctx->cont);
     KCHECK();
@@ -940,7 +937,7 @@ void direction(amg_ctx* ctx, cudaStream_t s) {
     if (ctx->ewald) {
         Pme<R>& pm = pme_of<R>(ctx);
         const int3 K = make_int3(ctx->K[0], ctx->K[1], ctx->K[2]);
-        k_pcg_dir_spread<R, kOrder><<<n, 128, 0, s>>>(n, ctx->zd, ctx->zp, ctx->pd, ctx->pp, ctx->scal, A.p4, pm.theta,
+        k_pcg_dir_spread<R, kOrder><<<nblk(n, kLineSites), 128, 0, s>>>(n, ctx->zd, ctx->zp, ctx->pd, ctx->pp, ctx->scal, A.p4, pm.theta,
                                                        pm.k0, K, ctx->frac, pm.zg);
     } else {
         k_pcg_dir<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->zd, ctx->zp, ctx->pd, ctx->pp, ctx->scal, A.p4);
@@ -1063,8 +1060,8 @@ void enqueue_front(amg_ctx* ctx, cudaStream_t s) {
         const R u2 = (R)(ctx->usolvcut * ctx->usolvcut);
         auto launch = [&](auto kern, unsigned nb) {
             kern<<<nb, kThreads, 0, r>>>(n, ctx->sids, A.at, ctx->bx, aew, ctx->nbr, ctx->cap, ctx->nnb, ctx->Ed, ctx->Ep,
-                                         coef ? A.c0 : nullptr, coef ? A.c1 : nullptr, u2, sp ? ctx->nbru : nullptr,
-                                         sp ? A.cu0 : nullptr, sp ? A.cu1 : nullptr, sp ? ctx->nnbu : nullptr);
+                                         coef ? A.c0 : nullptr, u2, sp ? ctx->nbru : nullptr,
+                                         sp ? A.cu0 : nullptr, sp ? ctx->nnbu : nullptr);
         };
         LPA_DISPATCH(ctx->lpa, {
             const unsigned nb = nblk((size_t)n * L);
@@ -1544,9 +1541,9 @@ void release(amg_ctx* ctx) {
     if (ctx->cubtmp) cudaFree(ctx->cubtmp);
     ctx->cubtmp = nullptr;
     dfree(ctx->af.at); dfree(ctx->af.u4); dfree(ctx->ad.at); dfree(ctx->ad.u4);
-    dfree(ctx->af.p4); dfree(ctx->ad.p4); dfree(ctx->af.c0); dfree(ctx->af.c1); dfree(ctx->ad.c0); dfree(ctx->ad.c1);
-    dfree(ctx->af.s4); dfree(ctx->ad.s4); dfree(ctx->af.cu0); dfree(ctx->af.cu1); dfree(ctx->ad.cu0);
-    dfree(ctx->ad.cu1); dfree(ctx->nbru); dfree(ctx->nnbu);
+    dfree(ctx->af.p4); dfree(ctx->ad.p4); dfree(ctx->af.c0); dfree(ctx->ad.c0);
+    dfree(ctx->af.s4); dfree(ctx->ad.s4); dfree(ctx->af.cu0); dfree(ctx->ad.cu0);
+    dfree(ctx->nbru); dfree(ctx->nnbu);
     pme_destroy(ctx->pmf);
     pme_destroy(ctx->pmd);
     for (auto& e : ctx->ev)
@@ -1563,6 +1560,7 @@ void release(amg_ctx* ctx) {
     dfree(ctx->flushbuf);
     dfree(ctx->adj); dfree(ctx->adj_pot); dfree(ctx->adj_n); dfree(ctx->adj_vec); dfree(ctx->adj_phi);
     dfree(ctx->adj_dpole);
+    dfree(ctx->adj_opt);
     if (ctx->st) { cudaStreamDestroy(ctx->st); ctx->st = nullptr; }
     if (ctx->st2) { cudaStreamDestroy(ctx->st2); ctx->st2 = nullptr; }
 }
@@ -1789,6 +1787,9 @@ int backward_impl(amg_ctx* ctx, const amg_cotangents* cot, amg_param_grads* gr) 
     double *dpd = ctx->adj_n, *dth = dpd + n, *dpol = dth + n;
     const bool have_g = cot->d_uind || cot->d_uinp;
     const bool iter = iterative(ctx);
+    const bool opt = ctx->poltyp == AMG_POL_OPT && ctx->npolar > 0;
+    const int K = ctx->optorder;
+    if (opt && !ctx->adj_opt) dalloc(ctx, ctx->adj_opt, (size_t)(2 * K + 4) * n3);
     // FP64 copies of the sites, stencils and T coefficients
     rotate_and_pack<double>(ctx, s);
     if (ctx->ewald) {
@@ -1813,6 +1814,24 @@ int backward_impl(amg_ctx* ctx, const amg_cotangents* cot, amg_param_grads* gr) 
             k_scale3<<<nblk(n), kThreads, 0, s>>>(n, ctx->pol, gd, wd);
             KCHECK();
             k_scale3<<<nblk(n), kThreads, 0, s>>>(n, ctx->pol, gp, wp);
+            KCHECK();
+        } else if (opt) {
+            // orders w^(k) = (alpha T)^k alpha g of both cotangents, and
+            // w = S g = sum_k c_k w^(k) (no solve: S is the OPT polynomial)
+            double* wo = ctx->adj_opt;
+            k_scale3<<<nblk(n), kThreads, 0, s>>>(n, ctx->pol, gd, wo);
+            KCHECK();
+            k_scale3<<<nblk(n), kThreads, 0, s>>>(n, ctx->pol, gp, wo + n3);
+            KCHECK();
+            for (int k = 1; k <= K; k++) {
+                const double* vd = wo + (size_t)(2 * k - 2) * n3;
+                matvec<double>(ctx, s, vd, vd + n3, ctx->Apd, ctx->App);
+                k_opt_step<<<nblk(n3), kThreads, 0, s>>>((int)n3, ctx->pol, vd, vd + n3, ctx->Apd, ctx->App, 0.0,
+                                                         wo + (size_t)(2 * k) * n3, wo + (size_t)(2 * k + 1) * n3,
+                                                         zeros, zeros);
+                KCHECK();
+            }
+            k_opt_combine<<<nblk(n3), kThreads, 0, s>>>((int)n3, K, ctx->copm, wo, wd, wp);
             KCHECK();
         } else if (iter) {
             ensure_coeff_buffers<double>(ctx, atoms_of<double>(ctx));
@@ -1846,6 +1865,14 @@ int backward_impl(amg_ctx* ctx, const amg_cotangents* cot, amg_param_grads* gr) 
     k_adj_vectors<<<nblk(n), kThreads, 0, s>>>(n, cf, ctx->has_pol ? ctx->ud : zeros, ctx->has_pol ? ctx->up : zeros,
                                                wd, wp, bd, bp, vbar, mwp, ctx->pol, dpol);
     KCHECK();
+    if (opt) {
+        if (!(have_g && ctx->has_pol)) {  // no dipole cotangents: all orders w^(k) vanish
+            k_zero<double><<<nblk((size_t)2 * (K + 1) * n3, 256), 256, 0, s>>>(ctx->adj_opt, (size_t)2 * (K + 1) * n3);
+            KCHECK();
+        }
+        k_opt_adj_diag<<<nblk(n), kThreads, 0, s>>>(n, K, ctx->copm, cf, ctx->pol, ctx->adj_opt, ctx->uopt, dpol);
+        KCHECK();
+    }
     k_adj_pack<<<nblk(n), kThreads, 0, s>>>(n, vbar, bd, ctx->ud, mwp, ctx->up, ctx->adj_vec);
     KCHECK();
     k_zero<double><<<nblk(2 * n3, 256), 256, 0, s>>>(grad, 2 * n3);
@@ -1890,6 +1917,49 @@ int backward_impl(amg_ctx* ctx, const amg_cotangents* cot, amg_param_grads* gr) 
         CK(cudaMemcpyAsync(r10.data(), ctx->rp10, sizeof(double) * 10 * n, cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
         for (int i = 0; i < n; i++) qtot += r10[10 * (size_t)i];
+    }
+    if (opt) {
+        // OPT dipole-dipole terms: the pairs (-V1_b, u_d^(b)) and (-V2_b,
+        // u_p^(b)) of U_u for b = 0..K-1, through the same adjoint kernels
+        // with the multipole channels off (cm = 0, vbar = 0)
+        double* P1 = ctx->adj_opt + (size_t)(2 * K + 2) * n3;
+        double* P2 = P1 + n3;
+        for (int b = 0; b < K; b++) {
+            const double* Q1 = ctx->uopt + (size_t)(2 * b) * n3;
+            const double* Q2 = Q1 + n3;
+            k_opt_adj_cross<<<nblk(n3), kThreads, 0, s>>>((int)n3, K, b, ctx->copm, cf, ctx->adj_opt, ctx->uopt, P1, P2);
+            KCHECK();
+            k_adj_pack<<<nblk(n), kThreads, 0, s>>>(n, zeros, P1, Q1, P2, Q2, ctx->adj_vec);
+            KCHECK();
+            LPA_DISPATCH(ctx->lpa, {
+                if (ctx->ewald)
+                    k_adjoint_pair<true, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(
+                        n, ctx->sids, ctx->ad.at, ctx->adj_vec, ctx->bx, ctx->aewald, ctx->nbr, ctx->cap, ctx->nnb, 1,
+                        0.0, grad, trq, ctx->adj_pot, dpd, dth);
+                else
+                    k_adjoint_pair<false, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(
+                        n, ctx->sids, ctx->ad.at, ctx->adj_vec, ctx->bx, 0.0, ctx->nbr, ctx->cap, ctx->nnb, 1, 0.0,
+                        grad, trq, ctx->adj_pot, dpd, dth);
+            });
+            KCHECK();
+            if (ctx->nsp) {
+                k_adjoint_scaled<<<nblk(ctx->nsp), kThreads, 0, s>>>(
+                    ctx->nsp, ctx->sp, ctx->xyz, ctx->rp10, ctx->pdamp, ctx->thole, ctx->bx, ctx->cut * ctx->cut,
+                    ewald_alpha(ctx), zeros, zeros, P1, Q1, P2, Q2, 1, 0.0, grad, trq, ctx->adj_pot, dpd, dth);
+                KCHECK();
+            }
+            if (ctx->ewald) {
+                double* ph = ctx->adj_phi;
+                const size_t blk = 2 * 20 * (size_t)n, one = 20 * (size_t)n;
+                pme_dipoles<double, 20>(ctx, s, zeros, P1, ph);
+                pme_dipoles<double, 20>(ctx, s, Q1, Q2, ph + blk);
+                pme_dipoles<double, 20>(ctx, s, P2, zeros, ph + 2 * blk);
+                k_adjoint_recip<<<nblk(n), kThreads, 0, s>>>(n, ctx->rp10, ctx->phiM, ph, ph + one, ph + blk,
+                                                             ph + 2 * blk, ph + blk + one, zeros, P1, Q1, P2, Q2, 1,
+                                                             self_coef(ctx), ctx->aewald, 0.0, grad, trq, ctx->adj_pot);
+                KCHECK();
+            }
+        }
     }
     k_torque<<<nblk(n), kThreads, 0, s>>>(n, ctx->xyz, ctx->zax, ctx->xax, ctx->yax, ctx->axe, trq, grad, nullptr);
     KCHECK();
@@ -2019,10 +2089,6 @@ int amg_backward(amg_ctx* ctx, const amg_cotangents* cot, amg_param_grads* grads
         ctx->err = "amg_backward needs an amg_forward at the current coordinates";
         return AMG_ERR_BAD_ARG;
     }
-    if (ctx->poltyp == AMG_POL_OPT) {
-        ctx->err = "the adjoint covers the mutual and direct models";
-        return AMG_ERR_UNSUPPORTED;
-    }
     try {
         CK(cudaSetDevice(ctx->device));
         return backward_impl(ctx, cot, grads);
@@ -2129,11 +2195,11 @@ int amg_time_tu_kernel(amg_ctx* ctx, int32_t reps, int64_t flush_bytes, double* 
             LPA_DISPATCH(ctx->lpa, {
                 if (mixed)
                     k_tu_stored<float, L><<<nblk((size_t)n * L), kThreads, 0, ctx->st>>>(
-                        n, ctx->sids, ctx->nbr, ctx->af.c0, ctx->af.c1, ctx->cap, ctx->nnb, ctx->xoff, ctx->af.p4,
+                        n, ctx->sids, ctx->nbr, ctx->af.c0, ctx->cap, ctx->nnb, ctx->xoff, ctx->af.p4,
                         ctx->Fd, ctx->Fp);
                 else
                     k_tu_stored<double, L><<<nblk((size_t)n * L), kThreads, 0, ctx->st>>>(
-                        n, ctx->sids, ctx->nbr, ctx->ad.c0, ctx->ad.c1, ctx->cap, ctx->nnb, ctx->xoff, ctx->ad.p4,
+                        n, ctx->sids, ctx->nbr, ctx->ad.c0, ctx->cap, ctx->nnb, ctx->xoff, ctx->ad.p4,
                         ctx->Fd, ctx->Fp);
             });
             KCHECK();
@@ -2147,7 +2213,7 @@ int amg_time_tu_kernel(amg_ctx* ctx, int32_t reps, int64_t flush_bytes, double* 
         cudaEventDestroy(b);
         *ms_avg = tot / reps;
         if (bytes_per_launch)
-            *bytes_per_launch = (double)pairs * (4.0 + 5.0 * rs) + (double)n * (2 * 4 * rs + 2 * 3 * 8.0 + 8.0);
+            *bytes_per_launch = (double)pairs * (4.0 + 4.0 * rs) + (double)n * (2 * 4 * rs + 2 * 3 * 8.0 + 8.0);
         if (directed_pairs) *directed_pairs = pairs;
     } catch (Fail& f) {
         return f.code;

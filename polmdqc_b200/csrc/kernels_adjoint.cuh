@@ -13,6 +13,7 @@
 #pragma once
 #include "kernels.cuh"
 #include "kernels_pair.cuh"
+#include "kernels_misc.cuh"
 
 namespace amg {
 
@@ -341,6 +342,72 @@ __global__ void k_adjoint_recip(int n, const double* __restrict__ rp10, const do
     pot[10 * (size_t)i + 1] -= selfc * vb.x;
     pot[10 * (size_t)i + 2] -= selfc * vb.y;
     pot[10 * (size_t)i + 3] -= selfc * vb.z;
+}
+
+// ---------------------------------------------------------------- OPT
+// Adjoint of the OPT dipoles u = S E, S = sum_k c_k (alpha T)^k alpha
+// (c_k the mixed coefficients copm_k; S is symmetric).  With w^(a) =
+// (alpha T)^a alpha g and u^(b) = (alpha T)^b alpha E the orders of the
+// cotangents and of the fields (u^(b) kept by the forward), the part of
+// dL/dtheta through S is
+//   X1^T dS E_d + X2^T dS E_p,  X1 = g_d - c f/2 E_p, X2 = g_p,
+// whose orders are X1~_a = w_d^(a) - c f/2 u_p^(a), X2~_a = w_p^(a).  From
+// d[(alpha T)^k alpha] = sum_{a+b=k-1} (alpha T)^a alpha dT (alpha T)^b alpha
+// + sum_{a+b=k} (alpha T)^a d(alpha) (T alpha)^b it splits into
+//   dipole-dipole terms  sum_b V_b^T dT u^(b),
+//     V_b = sum_a c_{a+b+1} X~_a   (the pairs (-V_b, u^(b)) of U_u),
+//   diagonal terms       dL/dalpha_i += sum_k c_k sum_{a+b=k} X~_a,i . u^(b)_i / alpha_i^2.
+// Orders are stored [K+1][2][3n] (d set, then p set, per order).
+
+// w = sum_k c_k w^(k) for both sets
+__global__ void k_opt_combine(int n3, int K, OptCoef c, const double* __restrict__ orders, double* __restrict__ wd,
+                              double* __restrict__ wp) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n3) return;
+    double d = 0, p = 0;
+    for (int k = 0; k <= K; k++) {
+        d += c.c[k] * orders[(size_t)(2 * k) * n3 + t];
+        p += c.c[k] * orders[(size_t)(2 * k + 1) * n3 + t];
+    }
+    wd[t] = d;
+    wp[t] = p;
+}
+
+// the dipole-dipole partners of u_d^(b) and u_p^(b): P1 = -V1_b, P2 = -V2_b
+__global__ void k_opt_adj_cross(int n3, int K, int b, OptCoef c, double cf, const double* __restrict__ w,
+                                const double* __restrict__ u, double* __restrict__ P1, double* __restrict__ P2) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n3) return;
+    double v1 = 0, v2 = 0;
+    for (int a = 0; a + b + 1 <= K; a++) {
+        const double ck = c.c[a + b + 1];
+        v1 += ck * (w[(size_t)(2 * a) * n3 + t] - 0.5 * cf * u[(size_t)(2 * a + 1) * n3 + t]);
+        v2 += ck * w[(size_t)(2 * a + 1) * n3 + t];
+    }
+    P1[t] = -v1;
+    P2[t] = -v2;
+}
+
+// the diagonal terms of dL/dalpha (they replace the mutual model's)
+__global__ void k_opt_adj_diag(int n, int K, OptCoef c, double cf, const double* __restrict__ pol,
+                               const double* __restrict__ w, const double* __restrict__ u, double* __restrict__ dpol) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const size_t n3 = 3 * (size_t)n;
+    double s = 0;
+    for (int k = 0; k <= K; k++) {
+        double sk = 0;
+        for (int a = 0; a <= k; a++) {
+            const int b = k - a;
+            for (int q = 3 * i; q < 3 * i + 3; q++) {
+                const double x1 = w[(2 * a) * n3 + q] - 0.5 * cf * u[(2 * a + 1) * n3 + q];
+                const double x2 = w[(2 * a + 1) * n3 + q];
+                sk += x1 * u[(2 * b) * n3 + q] + x2 * u[(2 * b + 1) * n3 + q];
+            }
+        }
+        s += c.c[k] * sk;
+    }
+    dpol[i] = pol[i] > 0 ? s / (pol[i] * pol[i]) : 0.0;
 }
 
 // dL/d(local pole): chain the global-frame potentials through the rotation

@@ -187,11 +187,12 @@ __global__ void k_pcg_dir(int n, const double* __restrict__ zd, const double* __
     p4[2 * i + 1] = make_r4<R>((R)b[0], (R)b[1], (R)b[2], R(0));
 }
 
-// The direction update fused with the spreading of the new direction for
-// the next matvec: one block of 128 threads per site; threads 0..5 form
-// p = z + beta p (and its R4 copy), then thread t < P^3 adds stencil point t
-// of both sets to the complex grid zg (one vector atomic add; zg holds the
-// cleared grid left by the previous transform).
+// p = z + beta p (after the control decision) fused with the spreading of
+// p into the complex grid zg for the next matvec: a block of 128 threads takes
+// kLineSites sites; threads 0..6 kLineSites - 1 form p (and its R4 copy), then
+// each thread t < kLineSites P^2 adds one z-line of one site (as
+// k_spread_dipoles; zg holds the cleared grid left by the previous
+// transform).
 template <class R, int P>
 __global__ void __launch_bounds__(128) k_pcg_dir_spread(int n, const double* __restrict__ zd,
                                                         const double* __restrict__ zp, double* __restrict__ pd,
@@ -199,36 +200,28 @@ __global__ void __launch_bounds__(128) k_pcg_dir_spread(int n, const double* __r
                                                         R4<R>* __restrict__ p4, const R* __restrict__ theta,
                                                         const int* __restrict__ k0, int3 K, Frac F,
                                                         typename Cplx<R>::type* __restrict__ zg) {
-    __shared__ double pv[6];
-    const int i = blockIdx.x, t = threadIdx.x;
-    if (t < 6) {
-        double bd, bp;
-        pcg_beta(scal, bd, bp);
-        const int c = t % 3;
-        const int q = 3 * i + c;
-        const double v = t < 3 ? zd[q] + bd * pd[q] : zp[q] + bp * pp[q];
-        (t < 3 ? pd : pp)[q] = v;
-        pv[t] = v;
+    __shared__ double pv[kLineSites][6];
+    const int t = threadIdx.x, i0 = blockIdx.x * kLineSites;
+    if (t < 6 * kLineSites) {
+        const int s = t / 6, k = t % 6, i = i0 + s;
+        if (i < n) {
+            double bd, bp;
+            pcg_beta(scal, bd, bp);
+            const int q = 3 * i + k % 3;
+            const double v = k < 3 ? zd[q] + bd * pd[q] : zp[q] + bp * pp[q];
+            (k < 3 ? pd : pp)[q] = v;
+            pv[s][k] = v;
+        }
     }
     __syncthreads();
-    if (t == 0) {
-        p4[2 * i] = make_r4<R>((R)pv[0], (R)pv[1], (R)pv[2], R(0));
-        p4[2 * i + 1] = make_r4<R>((R)pv[3], (R)pv[4], (R)pv[5], R(0));
+    if (t < kLineSites && i0 + t < n) {
+        const double* v = pv[t];
+        p4[2 * (i0 + t)] = make_r4<R>((R)v[0], (R)v[1], (R)v[2], R(0));
+        p4[2 * (i0 + t) + 1] = make_r4<R>((R)v[3], (R)v[4], (R)v[5], R(0));
     }
-    if (t >= P * P * P) return;
-    const int a = t / (P * P), b = (t / P) % P, c = t % P;
-    const R* th = theta + (size_t)i * 3 * 4 * P;
-    const R t0 = th[a], t1 = th[P + a];
-    const R u0 = th[4 * P + b], u1 = th[5 * P + b];
-    const R v0 = th[8 * P + c], v1 = th[9 * P + c];
-    const R w100 = t1 * u0 * v0, w010 = t0 * u1 * v0, w001 = t0 * u0 * v1;
-    R d0, d1, d2, q0, q1, q2;
-    frac_dipole<R>(F, pv[0], pv[1], pv[2], d0, d1, d2);
-    frac_dipole<R>(F, pv[3], pv[4], pv[5], q0, q1, q2);
-    int ga = k0[3 * i] + a; if (ga >= K.x) ga -= K.x;
-    int gb = k0[3 * i + 1] + b; if (gb >= K.y) gb -= K.y;
-    int gc = k0[3 * i + 2] + c; if (gc >= K.z) gc -= K.z;
-    add_cplx<R>(zg + gidx(ga, gb, gc, K), d0 * w100 + d1 * w010 + d2 * w001, q0 * w100 + q1 * w010 + q2 * w001);
+    const int s = t / (P * P), i = i0 + s;
+    if (t >= kLineSites * P * P || i >= n) return;
+    spread_site_line<R, P>(i, t % (P * P), pv[s], pv[s] + 3, theta, k0, K, F, zg);
 }
 
 // One preconditioned correction step u += alpha r with the FP64 residual

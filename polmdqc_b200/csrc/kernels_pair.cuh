@@ -15,17 +15,16 @@ namespace amg {
 // Permanent field at every site from all neighbours' multipoles, bulk
 // (scale 1, Thole damped, Ewald or bare).  Writes Ed = Ep (the d/p
 // differences come only from the scaled pairs).  With COEF the same radial
-// factors also fill the PCG's stored coefficient rows (see k_tu_coeffs:
-// c0 = (x_i - x_j, B1), c1 = B2) and the sparse preconditioner's rows (pairs
-// within usolvcut, compacted in row order, when cu0 is given), so the
-// solve's set-up recomputes nothing.
+// factors also fill the PCG's stored coefficient rows (see k_tu_coeffs: c0 =
+// pack_tensor(x_i - x_j, B1, B2)) and the sparse preconditioner's rows (pairs
+// within usolvcut, compacted in row order, when cu0 is given), so the solve's
+// set-up recomputes nothing.
 template <class R, bool EWALD, int LPA, bool COEF, bool CELLS = false>
 __global__ void __launch_bounds__(128) k_perm_field(int n, const int* __restrict__ order, const AtomR<R>* __restrict__ at, Box bx, R aewald,
                                                     const int* __restrict__ nbr, int cap,
                                                     const int* __restrict__ nnb, double* __restrict__ Ed,
                                                     double* __restrict__ Ep, R4<R>* __restrict__ c0,
-                                                    R* __restrict__ c1, R usolv2, int* __restrict__ nbru,
-                                                    R4<R>* __restrict__ cu0, R* __restrict__ cu1,
+                                                    R usolv2, int* __restrict__ nbru, R4<R>* __restrict__ cu0,
                                                     int* __restrict__ nnbu) {
     const int g = (blockIdx.x * blockDim.x + threadIdx.x) / LPA, lane = threadIdx.x % LPA;
     const int i = order[min(g, n - 1)];
@@ -54,8 +53,7 @@ __global__ void __launch_bounds__(128) k_perm_field(int n, const int* __restrict
             R B[6];
             if (COEF) {
                 bulk_radial_prec<R, EWALD>(r2, aewald, pdi * Aj.e.y, pair_thole<R>(thi, Aj.e.z), B, P1, P2);
-                c0[base + s] = make_r4<R>(r.x, r.y, r.z, B[1]);
-                c1[base + s] = B[2];
+                c0[base + s] = pack_tensor<R>(r.x, r.y, r.z, B[1], B[2]);
             } else {
                 bulk_radial<R, EWALD, true>(r2, aewald, pdi * Aj.e.y, pair_thole<R>(thi, Aj.e.z), B);
             }
@@ -68,8 +66,7 @@ __global__ void __launch_bounds__(128) k_perm_field(int n, const int* __restrict
             if (take) {
                 const size_t q = base + nu + __popc(b & below);
                 nbru[q] = j;
-                cu0[q] = make_r4<R>(r.x, r.y, r.z, P1);
-                cu1[q] = P2;
+                cu0[q] = pack_tensor<R>(r.x, r.y, r.z, P1, P2);
             }
             nu += __popc(b);
         }
@@ -258,16 +255,15 @@ __global__ void __launch_bounds__(128) k_polar_pair(int n, const int* __restrict
 // ------------------------------------------------------------ stored T
 // The dipole interaction tensor does not change during the PCG solve, so its
 // pair coefficients are computed once per evaluation and streamed by every
-// matvec: per slot (r = x_i - x_j, B1) as R4 and B2 as R; the neighbour
-// index is the list entry itself.  Rows hold the bulk neighbours followed by
+// matvec: per slot one packed R4 (pack_tensor of r = x_i - x_j, B1, B2); the
+// neighbour index is the list entry itself.  Rows hold the bulk neighbours followed by
 // the scaled partners (filled by k_scaled_coeffs), so one kernel applies the
 // whole real-space T.
 template <class R, bool EWALD, int LPA, bool CELLS = false>
 __global__ void __launch_bounds__(128) k_tu_coeffs(int n, const int* __restrict__ order, const AtomR<R>* __restrict__ at, Box bx, R aewald,
                                                    const int* __restrict__ nbr, int cap, const int* __restrict__ nnb,
-                                                   R4<R>* __restrict__ c0, R* __restrict__ c1, R usolv2,
-                                                   int* __restrict__ nbru, R4<R>* __restrict__ cu0,
-                                                   R* __restrict__ cu1, int* __restrict__ nnbu) {
+                                                   R4<R>* __restrict__ c0, R usolv2, int* __restrict__ nbru,
+                                                   R4<R>* __restrict__ cu0, int* __restrict__ nnbu) {
     const int g = (blockIdx.x * blockDim.x + threadIdx.x) / LPA, lane = threadIdx.x % LPA;
     if (g >= n) return;  // whole lane groups leave together
     const int i = order[g];
@@ -310,8 +306,7 @@ __global__ void __launch_bounds__(128) k_tu_coeffs(int n, const int* __restrict_
                 P1 -= e * b1;
                 P2 -= (R(1) + x) * e * b2;
             }
-            c0[base + s] = make_r4<R>(r.x, r.y, r.z, B1);
-            c1[base + s] = B2;
+            c0[base + s] = pack_tensor<R>(r.x, r.y, r.z, B1, B2);
         }
         if (cu0) {  // sparse preconditioner: bare Thole-damped T within usolvcut, compacted in order
             const bool take = ok && r2 <= usolv2;
@@ -319,8 +314,7 @@ __global__ void __launch_bounds__(128) k_tu_coeffs(int n, const int* __restrict_
             if (take) {
                 const size_t q = base + nu + __popc(b & below);
                 nbru[q] = j;
-                cu0[q] = make_r4<R>(r.x, r.y, r.z, P1);
-                cu1[q] = P2;
+                cu0[q] = pack_tensor<R>(r.x, r.y, r.z, P1, P2);
             }
             nu += __popc(b);
         }
@@ -332,7 +326,7 @@ __global__ void __launch_bounds__(128) k_tu_coeffs(int n, const int* __restrict_
 // slots plus the site's scaled partners.  u4: [n][2] R4.
 template <class R, int LPA>
 __global__ void __launch_bounds__(128) k_tu_stored(int n, const int* __restrict__ order, const int* __restrict__ nbr,
-                                                   const R4<R>* __restrict__ c0, const R* __restrict__ c1, int cap,
+                                                   const R4<R>* __restrict__ c0, int cap,
                                                    const int* __restrict__ nnb, const int* __restrict__ xoff,
                                                    const R4<R>* __restrict__ u4, double* __restrict__ Fd,
                                                    double* __restrict__ Fp) {
@@ -347,14 +341,12 @@ __global__ void __launch_bounds__(128) k_tu_stored(int n, const int* __restrict_
     for (int s0 = lane; s0 < cnt; s0 += U * LPA) {
         int j[U];
         R4<R> c[U];
-        R B2[U];
 #pragma unroll
         for (int q = 0; q < U; q++) {
             const int s = s0 + q * LPA;
             const bool ok = s < cnt;
             j[q] = ok ? nbr[base + s] : i;
             c[q] = ok ? c0[base + s] : make_r4<R>(0, 0, 0, 0);
-            B2[q] = ok ? c1[base + s] : R(0);
         }
         R4<R> ud[U], up[U];
 #pragma unroll
@@ -364,12 +356,8 @@ __global__ void __launch_bounds__(128) k_tu_stored(int n, const int* __restrict_
         }
 #pragma unroll
         for (int q = 0; q < U; q++) {
-            R ad = (ud[q].x * c[q].x + ud[q].y * c[q].y + ud[q].z * c[q].z) * B2[q];
-            R ap = (up[q].x * c[q].x + up[q].y * c[q].y + up[q].z * c[q].z) * B2[q];
-            ax += ad * c[q].x - c[q].w * ud[q].x; ay += ad * c[q].y - c[q].w * ud[q].y;
-            az += ad * c[q].z - c[q].w * ud[q].z;
-            bx_ += ap * c[q].x - c[q].w * up[q].x; by += ap * c[q].y - c[q].w * up[q].y;
-            bz += ap * c[q].z - c[q].w * up[q].z;
+            apply_tensor<R>(c[q], ud[q], ax, ay, az);
+            apply_tensor<R>(c[q], up[q], bx_, by, bz);
         }
     }
     double sx = group_sum<LPA>((double)ax), sy = group_sum<LPA>((double)ay), sz = group_sum<LPA>((double)az);
@@ -489,9 +477,8 @@ template <class R>
 __global__ void k_scaled_coeffs(int np, const ScaledPair* __restrict__ sp, const double* __restrict__ xyz,
                                 const double* __restrict__ pdamp, const double* __restrict__ thole, Box bx,
                                 double cut2, double aewald, const int* __restrict__ nnb, int cap,
-                                int* __restrict__ nbr, R4<R>* __restrict__ c0, R* __restrict__ c1, double usolv2,
-                                const int* __restrict__ nnbu, int* __restrict__ nbru, R4<R>* __restrict__ cu0,
-                                R* __restrict__ cu1) {
+                                int* __restrict__ nbr, R4<R>* __restrict__ c0, double usolv2,
+                                const int* __restrict__ nnbu, int* __restrict__ nbru, R4<R>* __restrict__ cu0) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= np) return;
     ScaledPair P = sp[t];
@@ -503,10 +490,8 @@ __global__ void k_scaled_coeffs(int np, const ScaledPair* __restrict__ sp, const
     size_t sk = (size_t)P.k * cap + nnb[P.k] + P.sk;
     nbr[si] = P.k;
     nbr[sk] = P.i;
-    c0[si] = make_r4<R>((R)(-r.x), (R)(-r.y), (R)(-r.z), (R)B[1]);   // x_i - x_k
-    c0[sk] = make_r4<R>((R)r.x, (R)r.y, (R)r.z, (R)B[1]);
-    c1[si] = (R)B[2];
-    c1[sk] = (R)B[2];
+    c0[si] = pack_tensor<R>((R)(-r.x), (R)(-r.y), (R)(-r.z), (R)B[1], (R)B[2]);   // x_i - x_k
+    c0[sk] = pack_tensor<R>((R)r.x, (R)r.y, (R)r.z, (R)B[1], (R)B[2]);
     if (cu0) {  // preconditioner slots after the row's compacted bulk entries; zero beyond usolvcut
         double U[6] = {0, 0, 0, 0, 0, 0};
         const bool in = G.inside && dot(G.r, G.r) <= usolv2;
@@ -515,10 +500,8 @@ __global__ void k_scaled_coeffs(int np, const ScaledPair* __restrict__ sp, const
         size_t uk = (size_t)P.k * cap + nnbu[P.k] + P.sk;
         nbru[ui] = P.k;
         nbru[uk] = P.i;
-        cu0[ui] = make_r4<R>((R)(-r.x), (R)(-r.y), (R)(-r.z), (R)U[1]);
-        cu0[uk] = make_r4<R>((R)r.x, (R)r.y, (R)r.z, (R)U[1]);
-        cu1[ui] = (R)U[2];
-        cu1[uk] = (R)U[2];
+        cu0[ui] = pack_tensor<R>((R)(-r.x), (R)(-r.y), (R)(-r.z), (R)U[1], (R)U[2]);
+        cu0[uk] = pack_tensor<R>((R)r.x, (R)r.y, (R)r.z, (R)U[1], (R)U[2]);
     }
 }
 
@@ -532,7 +515,7 @@ __global__ void k_scaled_coeffs(int np, const ScaledPair* __restrict__ sp, const
 // decision (rz_out points into the scalar block at RZ_D (FIRST) or RZN_D).
 template <class R, int LPA, bool FIRST>
 __global__ void __launch_bounds__(128) k_precond(int n, const int* __restrict__ order, const int* __restrict__ nbru, const R4<R>* __restrict__ cu0,
-                                                 const R* __restrict__ cu1, int cap, const int* __restrict__ nnbu,
+                                                 int cap, const int* __restrict__ nnbu,
                                                  const int* __restrict__ xoff, const R4<R>* __restrict__ s4,
                                                  const double* __restrict__ pol, double wdiag,
                                                  const double* __restrict__ rd, const double* __restrict__ rp,
@@ -554,14 +537,12 @@ __global__ void __launch_bounds__(128) k_precond(int n, const int* __restrict__ 
         for (int s0 = lane; s0 < cnt; s0 += U * LPA) {
             int j[U];
             R4<R> c[U];
-            R B2[U];
 #pragma unroll
             for (int q = 0; q < U; q++) {
                 const int s = s0 + q * LPA;
                 const bool ok = s < cnt;
                 j[q] = ok ? nbru[base + s] : i;
                 c[q] = ok ? cu0[base + s] : make_r4<R>(0, 0, 0, 0);
-                B2[q] = ok ? cu1[base + s] : R(0);
             }
             R4<R> vd[U], vp[U];
 #pragma unroll
@@ -571,12 +552,8 @@ __global__ void __launch_bounds__(128) k_precond(int n, const int* __restrict__ 
             }
 #pragma unroll
             for (int q = 0; q < U; q++) {
-                R ad = (vd[q].x * c[q].x + vd[q].y * c[q].y + vd[q].z * c[q].z) * B2[q];
-                R ap = (vp[q].x * c[q].x + vp[q].y * c[q].y + vp[q].z * c[q].z) * B2[q];
-                ax += ad * c[q].x - c[q].w * vd[q].x; ay += ad * c[q].y - c[q].w * vd[q].y;
-                az += ad * c[q].z - c[q].w * vd[q].z;
-                bx_ += ap * c[q].x - c[q].w * vp[q].x; by += ap * c[q].y - c[q].w * vp[q].y;
-                bz += ap * c[q].z - c[q].w * vp[q].z;
+                apply_tensor<R>(c[q], vd[q], ax, ay, az);
+                apply_tensor<R>(c[q], vp[q], bx_, by, bz);
             }
         }
         double S[6];

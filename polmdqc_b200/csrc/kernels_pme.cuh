@@ -124,12 +124,16 @@ __global__ void k_spread_mpole(int n, const double* __restrict__ rp10, const R* 
     }
 }
 
-// Point-parallel spreading of two dipole sets (FP64 [3n] each) into the
-// complex grid zg = Q_d + i Q_p: one block of 128 threads per site (sites
-// taken in the order `order`, cell-sorted, so consecutive blocks touch
-// nearby grid points), thread t < P^3 owns stencil point
-// (a,b,c) = (t / P^2, t / P % P, t % P) and adds (d, p) with one atomic
-// vector add (FP32) or two atomic adds (FP64).  zg must start at zero.
+// Line-parallel spreading of two dipole sets (FP64 [3n] each) into the
+// complex grid zg = Q_d + i Q_p.  A block of 128 threads takes
+// kLineSites = 5 sites (sites in the order `order`); thread t < 5 P^2 owns the
+// z-line (a, b) = (l / P, l % P), l = t % P^2, of site t / P^2: the P grid
+// points (a, b, c0 .. c0 + P - 1) that are consecutive in memory.  In FP32
+// with an even K3 the line is added as aligned pairs of complex points (one
+// 16-byte vector atomic each: 3 atomics for P = 5 instead of 5); otherwise
+// point by point.  zg must start at zero.
+constexpr int kLineSites = 5;
+
 template <class R>
 __device__ __forceinline__ void add_cplx(typename Cplx<R>::type* p, R x, R y);
 template <>
@@ -142,6 +146,71 @@ __device__ __forceinline__ void add_cplx<double>(double2* p, double x, double y)
     atomicAdd(&p->y, y);
 }
 
+// add the P values (vx + i vy) of one z-line starting at c0 (wrapping at K3)
+template <class R, int P>
+__device__ __forceinline__ void add_line(typename Cplx<R>::type* line, int c0, int K3, const R (&vx)[P],
+                                         const R (&vy)[P]) {
+    if constexpr (sizeof(R) == 4) {
+        if ((K3 & 1) == 0) {
+            // with K3 even a pair starting at an even index never straddles
+            // the wrap, and the line start (a multiple of K3 points of 8 B)
+            // keeps even indices 16-byte aligned
+            auto pair = [&](int cc) {  // points cc, cc + 1 (cc a compile-time index after unrolling)
+                int gc = c0 + cc;
+                if (gc >= K3) gc -= K3;
+                atomicAdd(reinterpret_cast<float4*>(line + gc), make_float4(vx[cc], vy[cc], vx[cc + 1], vy[cc + 1]));
+            };
+            if (c0 & 1) {  // odd start: a single point, then pairs
+                add_cplx<R>(line + c0, vx[0], vy[0]);
+#pragma unroll
+                for (int q = 0; q < (P - 1) / 2; q++) pair(1 + 2 * q);
+            } else {       // even start: pairs, then a single point
+#pragma unroll
+                for (int q = 0; q < (P - 1) / 2; q++) pair(2 * q);
+                int gc = c0 + P - 1;
+                if (gc >= K3) gc -= K3;
+                add_cplx<R>(line + gc, vx[P - 1], vy[P - 1]);
+            }
+            return;
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < P; c++) {
+        int gc = c0 + c;
+        if (gc >= K3) gc -= K3;
+        add_cplx<R>(line + gc, vx[c], vy[c]);
+    }
+}
+
+// spread the line (a, b) of site i with Cartesian dipoles pd (d set) and pq
+// (p set), converted to fractional dipoles here
+template <class R, int P>
+__device__ __forceinline__ void spread_site_line(int i, int l, const double* pd, const double* pq,
+                                                 const R* __restrict__ theta, const int* __restrict__ k0, int3 K,
+                                                 const Frac& F, typename Cplx<R>::type* __restrict__ zg) {
+    static_assert(P % 2 == 1, "the pairing of line points assumes an odd order");
+    const int a = l / P, b = l % P;
+    const R* th = theta + (size_t)i * 3 * 4 * P;
+    const R t0 = th[a], t1 = th[P + a];
+    const R u0 = th[4 * P + b], u1 = th[5 * P + b];
+    R d0, d1, d2, p0, p1, p2;
+    frac_dipole<R>(F, pd[0], pd[1], pd[2], d0, d1, d2);
+    frac_dipole<R>(F, pq[0], pq[1], pq[2], p0, p1, p2);
+    // value at z weight (v0, v1): (d0 t1 u0 + d1 t0 u1) v0 + d2 t0 u0 v1
+    const R ad = d0 * t1 * u0 + d1 * t0 * u1, bd = d2 * t0 * u0;
+    const R ap = p0 * t1 * u0 + p1 * t0 * u1, bp = p2 * t0 * u0;
+    R vx[P], vy[P];
+#pragma unroll
+    for (int c = 0; c < P; c++) {
+        const R v0 = th[8 * P + c], v1 = th[9 * P + c];
+        vx[c] = ad * v0 + bd * v1;
+        vy[c] = ap * v0 + bp * v1;
+    }
+    int ga = k0[3 * i] + a; if (ga >= K.x) ga -= K.x;
+    int gb = k0[3 * i + 1] + b; if (gb >= K.y) gb -= K.y;
+    add_line<R, P>(zg + ((size_t)ga * K.y + gb) * K.z, k0[3 * i + 2], K.z, vx, vy);
+}
+
 template <class R, int P>
 __global__ void __launch_bounds__(128) k_spread_dipoles(int n, const int* __restrict__ order,
                                                         const double* __restrict__ ud,
@@ -149,22 +218,12 @@ __global__ void __launch_bounds__(128) k_spread_dipoles(int n, const int* __rest
                                                         const R* __restrict__ theta, const int* __restrict__ k0,
                                                         int3 K, Frac F,
                                                         typename Cplx<R>::type* __restrict__ zg) {
+    static_assert(kLineSites * P * P <= 128, "lines of a block");
     const int t = threadIdx.x;
-    if (t >= P * P * P) return;
-    const int i = order[blockIdx.x];
-    const int a = t / (P * P), b = (t / P) % P, c = t % P;
-    const R* th = theta + (size_t)i * 3 * 4 * P;
-    const R t0 = th[a], t1 = th[P + a];
-    const R u0 = th[4 * P + b], u1 = th[5 * P + b];
-    const R v0 = th[8 * P + c], v1 = th[9 * P + c];
-    R d0, d1, d2, p0, p1, p2;
-    frac_dipole<R>(F, ud[3 * i], ud[3 * i + 1], ud[3 * i + 2], d0, d1, d2);
-    frac_dipole<R>(F, up[3 * i], up[3 * i + 1], up[3 * i + 2], p0, p1, p2);
-    const R w100 = t1 * u0 * v0, w010 = t0 * u1 * v0, w001 = t0 * u0 * v1;
-    int ga = k0[3 * i] + a; if (ga >= K.x) ga -= K.x;
-    int gb = k0[3 * i + 1] + b; if (gb >= K.y) gb -= K.y;
-    int gc = k0[3 * i + 2] + c; if (gc >= K.z) gc -= K.z;
-    add_cplx<R>(zg + gidx(ga, gb, gc, K), d0 * w100 + d1 * w010 + d2 * w001, p0 * w100 + p1 * w010 + p2 * w001);
+    const int g = blockIdx.x * kLineSites + t / (P * P);
+    if (t >= kLineSites * P * P || g >= n) return;
+    const int i = order[g];
+    spread_site_line<R, P>(i, t % (P * P), ud + 3 * i, up + 3 * i, theta, k0, K, F, zg);
 }
 
 // Gather of the field of two dipole potential grids (interleaved as the

@@ -237,3 +237,45 @@ def test_adjoint_matches_oracle_finite_differences(box, grads):
         em = oracle.forward(sel.system(tm), ST, tol=1e-12, flags=abi.DO_ENERGY)
         num = ((ep.em + ep.ep) - (em.em + em.ep)) / (2 * h)
         assert abs(num - an[k]) < 1e-5 * max(1.0, abs(num)), (k, num, an[k])
+
+
+# ---------------------------------------------------------------- OPT
+@pytest.mark.parametrize("order", [2, 4])
+def test_opt_adjoint_matches_fd(box, order):
+    """The adjoint of the OPT dipoles (extrapolated perturbation theory, no
+    solve: the cotangents pass through the same polynomial in alpha T),
+    against central differences of the GPU's FP64 forward: coordinates equal
+    the forces; a charge, a dipole component, a polarizability and a Thole
+    factor; and a dipole functional L = <gd, uind> + <gp, uinp>."""
+    st = Settings(nfft=(24, 24, 24), precision=FP64, poltyp=abi.POL_OPT, opt_order=order)
+    rng = np.random.default_rng(7)
+    gd, gp = rng.standard_normal(3 * box.n), rng.standard_normal(3 * box.n)
+    e = Engine(box, st)
+    try:
+        r = e.forward(abi.DO_ENERGY | abi.DO_GRADIENT | abi.DO_DIPOLES)
+        g = e.backward(d_energy=1.0)
+        gl = e.backward(d_energy=0.0, d_uind=gd, d_uinp=gp)
+    finally:
+        e.close()
+    np.testing.assert_allclose(g["d_xyz"], r.dem + r.dep, atol=1e-8, rtol=0)
+
+    def eval_(s):
+        eng = Engine(s, st)
+        try:
+            q = eng.forward(abi.DO_ENERGY | abi.DO_DIPOLES)
+        finally:
+            eng.close()
+        return q.em + q.ep, gd @ q.uind.reshape(-1) + gp @ q.uinp.reshape(-1)
+
+    sel = _Selected(box)
+    theta0 = sel.values()
+    an_e, an_l = _Selected.pick(g), _Selected.pick(gl)
+    h = 1e-5
+    for k in range(len(theta0)):
+        tp, tm = theta0.copy(), theta0.copy()
+        tp[k] += h
+        tm[k] -= h
+        (ep_, lp), (em_, lm) = eval_(sel.system(tp)), eval_(sel.system(tm))
+        ne, nl = (ep_ - em_) / (2 * h), (lp - lm) / (2 * h)
+        assert abs(ne - an_e[k]) < 1e-5 * max(1.0, abs(ne)), (k, ne, an_e[k])
+        assert abs(nl - an_l[k]) < 1e-5 * max(1.0, abs(nl)), (k, nl, an_l[k])

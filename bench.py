@@ -339,6 +339,9 @@ def main():
                                "what": "amg_backward after one forward (d/d coordinates, local multipoles, "
                                        "polarizabilities, Thole factors), synchronous, host wall clock"}}
         line["config_4096_waters"] = small
+        from polmdqc_b200.engine import fma_peak
+        line["fma_peak_gflops"] = {"fp32": fma_peak(local, False), "fp64": fma_peak(local, True),
+                                   "what": "amg_fma_peak: independent FMA chains on every SM, 2 flops per FMA"}
         if ions:
             line["ion_solution"] = ions
         if world == 1 and not args.no_cpu_baseline:

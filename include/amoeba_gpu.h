@@ -232,6 +232,12 @@ int amg_bench(amg_ctx* ctx, int32_t flags, int32_t steps, int64_t flush_bytes, d
 int amg_time_tu_kernel(amg_ctx* ctx, int32_t reps, int64_t flush_bytes, double* ms_avg, double* bytes_per_launch,
                        int64_t* directed_pairs);
 
+/* Benchmark support (no counterpart in the reference): the measured FMA
+ * throughput of `device` in GFLOP/s (2 flops per fused multiply-add), FP32
+ * (fp64 = 0) or FP64 (fp64 = 1), from a kernel of independent FMA chains on
+ * every SM -- the roofline denominator of the compute-bound pair kernels. */
+int amg_fma_peak(int32_t device, int32_t fp64, double* gflops);
+
 /* The two parts of the last amg_forward's virial (AMG_DO_VIRIAL), as added
  * to amg_results.vir: the em terms and the ep terms (the reference keeps one
  * vir array and adds each term's share from its own routine, empole / epolar,

@@ -120,13 +120,15 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.amg_time_tu_kernel.argtypes = [C.c_void_p, C.c_int32, C.c_int64, _dp, _dp, C.POINTER(C.c_int64)]
     lib.amg_last_stats.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
     lib.amg_last_virial.argtypes = [C.c_void_p, _dp, _dp]
+    lib.amg_fma_peak.argtypes = [C.c_int32, C.c_int32, _dp]
     lib.amg_last_error.argtypes = [C.c_void_p]
     lib.amg_last_error.restype = C.c_char_p
     lib.amg_abi_version.argtypes = []
     lib.amg_destroy.argtypes = [C.c_void_p]
     lib.amg_destroy.restype = None
     for name in ("amg_create", "amg_set_coords", "amg_forward", "amg_backward", "amg_last_timing",
-                 "amg_abi_version", "amg_bench", "amg_last_stats", "amg_time_tu_kernel", "amg_last_virial"):
+                 "amg_abi_version", "amg_bench", "amg_last_stats", "amg_time_tu_kernel", "amg_last_virial",
+                 "amg_fma_peak"):
         getattr(lib, name).restype = C.c_int
     _lib = lib
     return lib

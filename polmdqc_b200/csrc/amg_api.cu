@@ -2221,6 +2221,81 @@ int amg_time_tu_kernel(amg_ctx* ctx, int32_t reps, int64_t flush_bytes, double* 
     return AMG_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// FMA throughput kernel: kFmaChains independent multiply-add chains per
+// thread (enough to cover the pipeline latency), kFmaIters rounds each; the
+// result is stored only in an impossible case, so nothing is optimized away
+constexpr int kFmaChains = 8;
+constexpr int kFmaIters = 4096;
+
+template <class T>
+__global__ void __launch_bounds__(256) k_fma_peak(T a, T b, int* __restrict__ sink) {
+    T x[kFmaChains];
+#pragma unroll
+    for (int c = 0; c < kFmaChains; c++) x[c] = (T)(threadIdx.x + c);
+    for (int it = 0; it < kFmaIters; it++) {
+#pragma unroll
+        for (int c = 0; c < kFmaChains; c++) x[c] = fma(x[c], a, b);
+    }
+    T s = 0;
+#pragma unroll
+    for (int c = 0; c < kFmaChains; c++) s += x[c];
+    if (s == (T)-12345.678) sink[0] = 1;
+}
+
+}  // namespace
+
+extern "C" {
+
+int amg_fma_peak(int32_t device, int32_t fp64, double* gflops) {
+    if (!gflops) return AMG_ERR_BAD_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        cudaGetLastError();
+        return AMG_ERR_NO_DEVICE;
+    }
+    if (cudaSetDevice(device) != cudaSuccess) return AMG_ERR_CUDA;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return AMG_ERR_CUDA;
+    const int blocks = prop.multiProcessorCount * 8, threads = 256;
+    int* sink = nullptr;
+    cudaEvent_t a = nullptr, b = nullptr;
+    int rc = AMG_OK;
+    if (cudaMalloc((void**)&sink, sizeof(int)) != cudaSuccess || cudaEventCreate(&a) != cudaSuccess ||
+        cudaEventCreate(&b) != cudaSuccess) {
+        rc = AMG_ERR_CUDA;
+    } else {
+        float best = 1e30f;
+        for (int rep = 0; rep < 6; rep++) {  // the first run warms up; the best of the rest counts
+            cudaEventRecord(a);
+            if (fp64)
+                k_fma_peak<double><<<blocks, threads>>>(0.999999, 1e-7, sink);
+            else
+                k_fma_peak<float><<<blocks, threads>>>(0.9999f, 1e-4f, sink);
+            cudaEventRecord(b);
+            if (cudaEventSynchronize(b) != cudaSuccess) {
+                rc = AMG_ERR_CUDA;
+                break;
+            }
+            float ms = 0;
+            cudaEventElapsedTime(&ms, a, b);
+            if (rep > 0) best = std::min(best, ms);
+        }
+        if (rc == AMG_OK) {
+            const double flops = 2.0 * kFmaChains * kFmaIters * (double)blocks * threads;
+            *gflops = flops / (best * 1e-3) / 1e9;
+        }
+    }
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    if (sink) cudaFree(sink);
+    cudaGetLastError();
+    return rc;
+}
+
 int amg_last_stats(amg_ctx* ctx, int64_t* launches, int32_t* graphed, int32_t* lanes_per_site) {
     if (!ctx) return AMG_ERR_BAD_ARG;
     if (launches) *launches = ctx->klast;

@@ -145,6 +145,16 @@ class AmgError(RuntimeError):
     pass
 
 
+def fma_peak(device=0, fp64=False):
+    """Measured FMA throughput of the device in GFLOP/s (amg_fma_peak)."""
+    lib = abi.load_library()
+    out = C.c_double(0)
+    rc = lib.amg_fma_peak(device, int(fp64), C.byref(out))
+    if rc != abi.AMG_OK:
+        raise AmgError(f"amg_fma_peak: {abi.STATUS.get(rc, rc)}")
+    return out.value
+
+
 class Engine:
     """One device context (amg_create .. amg_destroy)."""
 

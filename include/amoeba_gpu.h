@@ -46,7 +46,7 @@
 extern "C" {
 #endif
 
-#define AMG_ABI_VERSION 3
+#define AMG_ABI_VERSION 4
 
 /* status codes */
 #define AMG_OK               0
@@ -85,6 +85,12 @@ extern "C" {
 #define AMG_POL_DIRECT  2
 #define AMG_POL_OPT     3  /* extrapolated perturbation theory, coefficients opt_coef */
 #define AMG_MAX_OPT     6  /* highest OPT order (polopt.h maxopt) */
+
+/* charge penetration of the multipoles (mplpot.h pentype; AMOEBA+ and
+ * HIPPO, include/md/damping.h): none, Gordon f1, Gordon f2 */
+#define AMG_PEN_NONE     0
+#define AMG_PEN_GORDON1  1
+#define AMG_PEN_GORDON2  2
 
 /* CalcMode flags for amg_forward (reference calcMode.h:18-45) */
 #define AMG_DO_ENERGY    1
@@ -148,6 +154,25 @@ typedef struct amg_params {
                                         alpha E, u^(k) = alpha T u^(k-1); the order is
                                         the last nonzero entry (src/md/kpolar.cpp:
                                         108-153, 228-236) */
+    /* Appended in ABI version 4 (zero keeps the version-3 behaviour): charge
+     * penetration and charge flux of the multipoles (AMOEBA+, HIPPO), in the
+     * reference's non-Ewald multipole mode only (src/md/empole.cpp:64-82):
+     * with Ewald or polarization they return UNSUPPORTED. */
+    int32_t pentype;                 /* AMG_PEN_*: core/valence split of each monopole,
+                                        valence damped (include/md/pairMpole.h:186-389) */
+    const double* pcore;             /* [n] core charge (chgpen.h pcore); valence = q - core */
+    const double* palpha;            /* [n] damping exponent (chgpen.h palpha) */
+    int32_t cflux;                   /* potent.h use_chgflx: the monopoles follow the
+                                        geometry, q = pole[i][0] + dq (src/md/alterchg.cpp);
+                                        pole[i][0] is then the unaltered monopole (mpole.h mono0) */
+    int32_t nbond;                   /* bonds of the charge flux (bndstr.h nbond) */
+    const int32_t* bond_atoms;       /* [nbond*2] 0-based atoms (bndstr.h ibnd) */
+    const double* bond_flux;         /* [nbond*2] ideal length bl, flux bflx (cflux.h) */
+    int32_t nangle;                  /* angles of the charge flux (angbnd.h nangle) */
+    const int32_t* angle_atoms;      /* [nangle*3] 0-based a, b (vertex), c (angbnd.h iang) */
+    const double* angle_flux;        /* [nangle*7] ideal angle anat (degrees), ideal
+                                        lengths of bonds a-b and c-b (bl via atmlst.h
+                                        balist), aflx[2], abflx[2] (cflux.h) */
 } amg_params;
 
 typedef struct amg_results {

@@ -30,7 +30,19 @@
 //       preconditioner M = w alpha + alpha T_u alpha over pairs within
 //       usolvcut (Thole-damped bare tensor, u-scaled), w = 2;
 //   * scale-factor semantics: src/md/empole.cpp:224-235 for m-scales; the
-//     p/d/u meanings documented in include/md/polpot.h:18-45.
+//     p/d/u meanings documented in include/md/polpot.h:18-45;
+//   * charge penetration (AMOEBA+ / HIPPO multipoles, the reference's
+//     pairMpoleCP, include/md/pairMpole.h:186-389): each monopole split
+//     into a point core and a valence charge smeared as a Slater density
+//     (Rackers et al., J. Chem. Theory Comput. 13, 2427 (2017), "Gordon"
+//     f1 / f2); the damped radial hierarchy is generated here from the
+//     potential of that density by B_{n+1} = -(1/r) dB_n/dr, which is
+//     what the reference's closed forms (include/md/damping.h:32-196)
+//     tabulate;
+//   * charge flux (Liu, Piquemal & Ren, J. Phys. Chem. Lett. 11, 419
+//     (2020)): monopoles following bond lengths and angles as the
+//     reference's alterchg (src/md/alterchg.cpp:36-170), and the gradient
+//     through the sites' potentials as its dcflux (src/md/dcflux.cpp:32-230).
 //
 // Parity status: the non-Ewald multipole path and the frames are pinned to the
 // reference (its golden tests and the compiled reference run here).  Ewald,
@@ -121,6 +133,17 @@ struct System {
     bool guess = true;
     bool prec = false;      // sparse preconditioner within usolvcut
     double usolvcut = 0;
+    // charge penetration: core charge and valence damping exponent per site
+    int pentype = AMG_PEN_NONE;
+    std::vector<double> pcore, palpha;
+    // charge flux: monopole increments of the current geometry, and the
+    // bond / angle terms that produce them
+    bool cflux = false;
+    std::vector<double> dq;
+    struct Bond { int a, b; double r0, k; };
+    struct Angle { int a, b, c; double th0, rab0, rcb0, pa1, pa2, pb1, pb2; };
+    std::vector<Bond> bonds;
+    std::vector<Angle> angles;
 };
 
 inline uint64_t pkey(int i, int k) {
@@ -249,6 +272,7 @@ void rotate_multipoles(System& s, const amg_params* P) {
     for (int i = 0; i < s.n; i++) {
         double sp[13];
         for (int j = 0; j < 13; j++) sp[j] = P->pole[13 * i + j];
+        if (s.cflux) sp[0] += s.dq[i];  // charge flux: q = mono0 + dq (src/md/alterchg.cpp:51-53)
         if (chiral_flip(s, P, i)) {
             sp[2] = -sp[2]; sp[5] = -sp[5]; sp[7] = -sp[7]; sp[9] = -sp[9]; sp[11] = -sp[11];
         }
@@ -438,6 +462,70 @@ Radial channel(const System& s, double r, double scale, const double lam[6]) {
         for (int n = 0; n < 6; n++) R.B[n] = scale * lam[n] * bare[n];
     }
     return R;
+}
+
+// ---------------------------------------------------------------- charge penetration
+// A valence charge smeared as a Slater density of exponent a has the potential
+// (1 - Q_0(x) e^{-x}) / r with x = a r and Q_0 a polynomial fixed by the
+// density.  Its radial hierarchy is B_n = bare_n (1 - Q_n(x) e^{-x}), and
+// B_{n+1} = -(1/r) dB_n/dr gives Q_{n+1} = Q_n + x (Q_n - Q_n') / (2n + 1).
+// Bases: the core-valence potentials of Gordon f1 (1 + x/2) and f2 (1), and
+// the valence-valence potential of two equal f1 densities
+// (1 + 11x/16 + 3x^2/16 + x^3/48); two unequal densities combine the
+// single-density families with the weights of their partial fractions.
+struct Qpoly { double c[12] = {}; };
+
+void damp_family(const std::vector<double>& q0, Qpoly out[6]) {
+    out[0] = Qpoly{};
+    for (size_t j = 0; j < q0.size(); j++) out[0].c[j] = q0[j];
+    for (int n = 0; n < 5; n++) {
+        const Qpoly& q = out[n];
+        Qpoly nx = q;
+        for (int j = 0; j < 11; j++) {
+            const double diff = q.c[j] - (j + 1 < 12 ? (j + 1) * q.c[j + 1] : 0.0);  // (Q - Q')_j
+            nx.c[j + 1] += diff / (2 * n + 1);
+        }
+        out[n + 1] = nx;
+    }
+}
+
+inline double qeval(const Qpoly& q, double x) {
+    double v = 0;
+    for (int j = 11; j >= 0; j--) v = v * x + q.c[j];
+    return v;
+}
+
+struct DampFamilies {
+    Qpoly f1[6], f2[6], e1[6];
+    DampFamilies() {
+        damp_family({1.0, 0.5}, f1);
+        damp_family({1.0}, f2);
+        damp_family({1.0, 11.0 / 16, 3.0 / 16, 1.0 / 48}, e1);
+    }
+};
+
+// Damping factors of the bare B_n (n = 0..5) for the pair (i, k): fi for the
+// valence of i seen by the core of k, fk the reverse, fik valence-valence.
+// Exponents closer than 1e-3 take the equal-exponent form, the threshold of
+// the reference (include/md/damping.h:42-43).
+void cp_factors(int pentype, double r, double ai, double ak, double fi[6], double fk[6], double fik[6]) {
+    static const DampFamilies F;
+    const Qpoly* core = pentype == AMG_PEN_GORDON1 ? F.f1 : F.f2;
+    const double xi = ai * r, xk = ak * r, ei = std::exp(-xi), ek = std::exp(-xk);
+    const bool equal = std::fabs(ai - ak) < 1e-3;
+    const double ti = equal ? 0.0 : ak * ak / (ak * ak - ai * ai), tk = equal ? 0.0 : ai * ai / (ai * ai - ak * ak);
+    for (int n = 0; n < 6; n++) {
+        fi[n] = 1.0 - qeval(core[n], xi) * ei;
+        fk[n] = 1.0 - qeval(core[n], xk) * ek;
+        if (pentype == AMG_PEN_GORDON1) {
+            fik[n] = equal ? 1.0 - qeval(F.e1[n], xi) * ei
+                           : 1.0 - ti * ti * (qeval(F.f1[n], xi) + 2 * tk * qeval(F.f2[n], xi)) * ei -
+                                 tk * tk * (qeval(F.f1[n], xk) + 2 * ti * qeval(F.f2[n], xk)) * ek;
+        } else {
+            fik[n] = equal ? 1.0 - qeval(F.f1[n], xi) * ei
+                           : 1.0 - ti * qeval(F.f2[n], xi) * ei - tk * qeval(F.f2[n], xk) * ek;
+        }
+    }
 }
 
 // Cartesian derivative tensor T_tuv = d^(t+u+v) psi / dx^t dy^u dz^v of a
@@ -1137,6 +1225,71 @@ int solve_dipoles(Work& w, Result& R, double tol_override, int maxit_override) {
 }
 
 
+// ---------------------------------------------------------------- charge flux
+// Monopole increments of the current geometry: a bond a-b moves
+// k (r_ab - r0) of charge from a to b; an angle a-b-c gives a the increment
+// pb1 (r_cb - r0_cb) + pa1 (theta - theta0), c the increment
+// pb2 (r_ab - r0_ab) + pa2 (theta - theta0), and b minus their sum
+// (src/md/alterchg.cpp:62-167; plain coordinate differences, no images).
+void charge_flux_charges(System& s) {
+    s.dq.assign(s.n, 0.0);
+    for (const System::Bond& b : s.bonds) {
+        const double r = norm(s.x[b.a] - s.x[b.b]);
+        const double d = b.k * (r - b.r0);
+        s.dq[b.a] -= d;
+        s.dq[b.b] += d;
+    }
+    for (const System::Angle& a : s.angles) {
+        const V3 u = s.x[a.a] - s.x[a.b], v = s.x[a.c] - s.x[a.b];
+        const double ru = norm(u), rv = norm(v);
+        if (!(ru > 0 && rv > 0)) continue;
+        const double c = std::max(-1.0, std::min(1.0, dot(u, v) / (ru * rv)));
+        const double dth = std::acos(c) - a.th0 * kPi / 180.0;
+        const double q1 = a.pb1 * (rv - a.rcb0) + a.pa1 * dth;
+        const double q2 = a.pb2 * (ru - a.rab0) + a.pa2 * dth;
+        s.dq[a.a] += q1;
+        s.dq[a.b] -= q1 + q2;
+        s.dq[a.c] += q2;
+    }
+}
+
+// dE/dx through the increments: sum over sites of pot_i d(dq_i)/dx with pot
+// the sites' potentials (dE/dq), added to grad; vir (strain derivative) when
+// given, as the pair terms: each term's gradients times its atoms' offsets
+// from the bond / angle vertex (src/md/dcflux.cpp:32-230 restated)
+void charge_flux_gradient(const System& s, const std::vector<double>& pot, std::vector<V3>& grad,
+                          double (*vir)[3]) {
+    for (const System::Bond& b : s.bonds) {
+        const V3 u = s.x[b.a] - s.x[b.b];
+        const double r = norm(u);
+        const V3 g = ((pot[b.b] - pot[b.a]) * b.k / r) * u;   // on a; -g on b
+        grad[b.a] = grad[b.a] + g;
+        grad[b.b] = grad[b.b] - g;
+        if (vir) add_outer(vir, g, u);
+    }
+    for (const System::Angle& a : s.angles) {
+        const V3 u = s.x[a.a] - s.x[a.b], v = s.x[a.c] - s.x[a.b];
+        const double ru = norm(u), rv = norm(v);
+        if (!(ru > 0 && rv > 0)) continue;
+        const double c = dot(u, v) / (ru * rv);
+        const double sn = std::sqrt(std::max(0.0, 1.0 - c * c));
+        const double pa = pot[a.a] - pot[a.b], pc = pot[a.c] - pot[a.b];
+        // d theta / dx_a = -(1/sin) (v/(ru rv) - c u/ru^2), likewise for c
+        const V3 dca = (1.0 / (ru * rv)) * v - (c / (ru * ru)) * u;
+        const V3 dcc = (1.0 / (ru * rv)) * u - (c / (rv * rv)) * v;
+        const double wt = -(pa * a.pa1 + pc * a.pa2) / sn;
+        const V3 ga = (pc * a.pb2 / ru) * u + wt * dca;   // dq2 holds r_ab, both hold theta
+        const V3 gc = (pa * a.pb1 / rv) * v + wt * dcc;
+        grad[a.a] = grad[a.a] + ga;
+        grad[a.c] = grad[a.c] + gc;
+        grad[a.b] = grad[a.b] - ga - gc;
+        if (vir) {
+            add_outer(vir, ga, u);
+            add_outer(vir, gc, v);
+        }
+    }
+}
+
 struct Flags { bool grad, analysis, virial; };
 
 void evaluate(Work& w, Flags fl, Result& R, double tol_override, int maxit_override, int& status) {
@@ -1148,6 +1301,10 @@ void evaluate(Work& w, Flags fl, Result& R, double tol_override, int maxit_overr
     R.aem.assign(s.n, 0.0);
     R.aep.assign(s.n, 0.0);
     const std::vector<Mp>& M = s.gm;
+    // charge penetration or charge flux: the pair loop below takes the
+    // core/valence form and collects each site's potential dE/dq (cfpot)
+    const bool cpath = s.pentype != AMG_PEN_NONE || s.cflux;
+    std::vector<double> cfpot(cpath ? s.n : 0, 0.0);
     // ---- permanent multipoles, real space (the reference's empole_a pair
     //      loop, src/md/empole.cpp:199-345, with Ewald damping when enabled)
     {
@@ -1156,27 +1313,78 @@ void evaluate(Work& w, Flags fl, Result& R, double tol_override, int maxit_overr
 #pragma omp parallel
         {
             std::vector<V3> gl(s.n, V3{0, 0, 0}), tl(s.n, V3{0, 0, 0});
-            std::vector<double> al(s.n, 0.0);
+            std::vector<double> al(s.n, 0.0), pl(cpath ? s.n : 0, 0.0);
             double el = 0, eil = 0, wl[3][3] = {};
             long nl = 0;
 #pragma omp for schedule(dynamic, 256)
             for (size_t pi = 0; pi < w.pairs.size(); pi++) {
                 const Pair& P = w.pairs[pi];
                 Scales sc = pair_scales(s, P.i, P.k);
-                double lam1[6] = {1, 1, 1, 1, 1, 1};
-                Radial rad = channel(s, P.rr, sc.m, lam1);
-                Tensor T;
-                build_tensor(P.r, rad, 5, T);
-                double ph[20];
-                source_potential(T, M[P.i], 3, ph);  // potential of i at k
-                double e = site_energy(M[P.k], ph);
-                V3 gk = site_gradient(M[P.k], ph);
-                V3 tk = site_torque(M[P.k], ph);
-                Tensor Tm;
-                build_tensor(-1.0 * P.r, rad, 4, Tm);
-                double pi_[20];
-                source_potential(Tm, M[P.k], 2, pi_);  // potential of k at i
-                V3 ti = site_torque(M[P.i], pi_);
+                double e;
+                V3 gk, tk, ti;
+                if (cpath) {
+                    // core/valence form (include/md/pairMpole.h:186-389): the
+                    // cores are point charges; each valence multipole is seen
+                    // by the other core through its own damping (fi, fk) and
+                    // by the other valence multipole through the overlap
+                    // damping (fik); every channel carries the m-scale
+                    const int i = P.i, k = P.k;
+                    const bool cp = s.pentype != AMG_PEN_NONE;
+                    double bare[6], fi[6] = {1, 1, 1, 1, 1, 1}, fk[6] = {1, 1, 1, 1, 1, 1}, fik[6] = {1, 1, 1, 1, 1, 1};
+                    bare_terms(P.rr, bare);
+                    if (cp) cp_factors(s.pentype, P.rr, s.palpha[i], s.palpha[k], fi, fk, fik);
+                    auto radial = [&](const double* fac) {
+                        Radial R;
+                        for (int q = 0; q < 6; q++) R.B[q] = sc.m * fac[q] * bare[q];
+                        return R;
+                    };
+                    const double one[6] = {1, 1, 1, 1, 1, 1};
+                    const Radial Rb = radial(one), Ri = radial(fi), Rk = radial(fk), Rik = radial(fik);
+                    Mp ci{}, ck{}, vi = M[i], vk = M[k];
+                    ci.c[0] = cp ? s.pcore[i] : 0.0;
+                    ck.c[0] = cp ? s.pcore[k] : 0.0;
+                    vi.c[0] -= ci.c[0];
+                    vk.c[0] -= ck.c[0];
+                    Tensor Tb, Ti, Tk, Tik;
+                    build_tensor(P.r, Rb, 5, Tb);
+                    build_tensor(P.r, Ri, 5, Ti);
+                    build_tensor(P.r, Rk, 5, Tk);
+                    build_tensor(P.r, Rik, 5, Tik);
+                    double pc[20], pv[20], t1[20], t2[20];
+                    source_potential(Tb, ci, 3, pc);   // at the core of k
+                    source_potential(Ti, vi, 3, t1);
+                    source_potential(Tk, ci, 3, pv);   // at the valence multipole of k
+                    source_potential(Tik, vi, 3, t2);
+                    for (int q = 0; q < 20; q++) { pc[q] += t1[q]; pv[q] += t2[q]; }
+                    e = site_energy(ck, pc) + site_energy(vk, pv);
+                    gk = site_gradient(ck, pc) + site_gradient(vk, pv);
+                    tk = site_torque(vk, pv);
+                    Tensor Ri_m, Rik_m;
+                    build_tensor(-1.0 * P.r, Ri, 4, Ri_m);
+                    build_tensor(-1.0 * P.r, Rik, 4, Rik_m);
+                    double qv[20];
+                    source_potential(Ri_m, ck, 2, qv);   // at the valence multipole of i
+                    source_potential(Rik_m, vk, 2, t1);
+                    for (int q = 0; q < 20; q++) qv[q] += t1[q];
+                    ti = site_torque(vi, qv);
+                    pl[k] += pv[0];   // dE/d(valence charge): the charge flux potentials
+                    pl[i] += qv[0];
+                } else {
+                    double lam1[6] = {1, 1, 1, 1, 1, 1};
+                    Radial rad = channel(s, P.rr, sc.m, lam1);
+                    Tensor T;
+                    build_tensor(P.r, rad, 5, T);
+                    double ph[20];
+                    source_potential(T, M[P.i], 3, ph);  // potential of i at k
+                    e = site_energy(M[P.k], ph);
+                    gk = site_gradient(M[P.k], ph);
+                    tk = site_torque(M[P.k], ph);
+                    Tensor Tm;
+                    build_tensor(-1.0 * P.r, rad, 4, Tm);
+                    double pi_[20];
+                    source_potential(Tm, M[P.k], 2, pi_);  // potential of k at i
+                    ti = site_torque(M[P.i], pi_);
+                }
                 el += e;
                 if (e != 0.0) nl++;
                 al[P.i] += 0.5 * e;
@@ -1199,6 +1407,7 @@ void evaluate(Work& w, Flags fl, Result& R, double tol_override, int maxit_overr
                     R.dem[i] = R.dem[i] + gl[i];
                     tm[i] = tm[i] + tl[i];
                     R.aem[i] += al[i];
+                    if (cpath) cfpot[i] += pl[i];
                 }
             }
         }
@@ -1244,6 +1453,10 @@ void evaluate(Work& w, Flags fl, Result& R, double tol_override, int maxit_overr
     for (int i = 0; i < s.n; i++) { R.dem[i] = s.f * R.dem[i]; tm[i] = s.f * tm[i]; R.aem[i] *= s.f; }
     for (auto& row : R.vir) for (double& v : row) v *= s.f;
     if (fl.grad) torque_to_gradient(s, w.P, tm, R.dem, fl.virial ? R.vir : nullptr);
+    if (fl.grad && s.cflux) {
+        for (double& v : cfpot) v *= s.f;
+        charge_flux_gradient(s, cfpot, R.dem, fl.virial ? R.vir : nullptr);
+    }
 
     // ---- polarization
     if (s.poltyp == AMG_POL_NONE) return;
@@ -1536,6 +1749,30 @@ static int setup_work(const amg_params* P, const double* xyz, const double box[6
     s.usolvcut = std::min(P->usolvcut, P->cutoff);
     if (s.prec && !(s.usolvcut > 0)) return AMG_ERR_BAD_ARG;
     if (opt) w.opt.kmax = opt->kmax;
+    s.pentype = P->pentype;
+    s.cflux = P->cflux != 0;
+    if (s.pentype != AMG_PEN_NONE || s.cflux) {
+        // the reference has charge penetration and charge flux only in its
+        // non-Ewald multipole mode (src/md/empole.cpp:64-82)
+        if (s.ewald || s.poltyp != AMG_POL_NONE) return AMG_ERR_UNSUPPORTED;
+        if (s.pentype != AMG_PEN_NONE) {
+            if (s.pentype != AMG_PEN_GORDON1 && s.pentype != AMG_PEN_GORDON2) return AMG_ERR_BAD_ARG;
+            if (!P->pcore || !P->palpha) return AMG_ERR_BAD_ARG;
+            s.pcore.assign(P->pcore, P->pcore + s.n);
+            s.palpha.assign(P->palpha, P->palpha + s.n);
+        }
+        if (s.cflux) {
+            for (int b = 0; b < P->nbond; b++)
+                s.bonds.push_back({P->bond_atoms[2 * b], P->bond_atoms[2 * b + 1], P->bond_flux[2 * b],
+                                   P->bond_flux[2 * b + 1]});
+            for (int a = 0; a < P->nangle; a++) {
+                const double* f = P->angle_flux + 7 * a;
+                s.angles.push_back({P->angle_atoms[3 * a], P->angle_atoms[3 * a + 1], P->angle_atoms[3 * a + 2], f[0],
+                                    f[1], f[2], f[3], f[4], f[5], f[6]});
+            }
+            charge_flux_charges(s);
+        }
+    }
     build_scales(s, P);
     rotate_multipoles(s, P);
     w.pairs = build_pairs(s);

@@ -14,6 +14,11 @@
 
 #include "action.h"
 #include "analyz.h"
+#include "angbnd.h"
+#include "atmlst.h"
+#include "bndstr.h"
+#include "cflux.h"
+#include "chgpen.h"
 #include "atoms.h"
 #include "bound.h"
 #include "boxes.h"
@@ -189,6 +194,28 @@ int main(int argc, char** argv)
         darr("uinp", 3 * n, [](int i) { return uinp[i / 3][i % 3]; });
     }
     darr("vir", 9, [](int i) { return vir[i / 3][i % 3]; });
+    // charge penetration and charge flux (AMOEBA+ / HIPPO multipoles)
+    inum("pentype", pentype == PenTyp::Gordon1 ? 1 : pentype == PenTyp::Gordon2 ? 2 : 0);
+    inum("use_chgflx", use_chgflx);
+    if (pentype != PenTyp::None) {
+        darr("pcore", n, [](int i) { return pcore[i]; });
+        darr("pval0", n, [](int i) { return pval0[i]; });
+        darr("palpha", n, [](int i) { return palpha[i]; });
+    }
+    if (use_chgflx) {
+        darr("mono0", n, [](int i) { return mono0[i]; });
+        inum("nbond", nbond);
+        iarr("ibnd", 2 * nbond, [](int i) { return ibnd[i / 2][i % 2]; });
+        darr("bl", nbond, [](int i) { return bl[i]; });
+        darr("bflx", nbond, [](int i) { return bflx[i]; });
+        inum("nangle", nangle);
+        iarr("iang", 3 * nangle, [](int i) { return iang[i / 3][i % 3]; });
+        darr("anat", nangle, [](int i) { return anat[i]; });
+        darr("rab0", nangle, [](int i) { return bl[balist[i][0]]; });
+        darr("rcb0", nangle, [](int i) { return bl[balist[i][1]]; });
+        darr("aflx", 2 * nangle, [](int i) { return aflx[i / 2][i % 2]; });
+        darr("abflx", 2 * nangle, [](int i) { return abflx[i / 2][i % 2]; });
+    }
     fputs("\n}\n", fo);
     if (fo != stdout) fclose(fo);
     return 0;

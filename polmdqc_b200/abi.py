@@ -27,6 +27,7 @@ PREC_FP64, PREC_MIXED = 0, 1
 POL_NONE, POL_MUTUAL, POL_DIRECT, POL_OPT = 0, 1, 2, 3
 CELL_FROM_ANGLES, CELL_OCTAHEDRON, CELL_DODECAHEDRON = 0, 1, 2
 DO_ENERGY, DO_ANALYSIS, DO_GRADIENT, DO_VIRIAL, DO_DIPOLES = 1, 2, 4, 8, 16
+PEN_NONE, PEN_GORDON1, PEN_GORDON2 = 0, 1, 2
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -56,6 +57,10 @@ class amg_params(C.Structure):
         ("pcg_prec", C.c_int32), ("usolvcut", C.c_double),
         ("cell_shape", C.c_int32),
         ("opt_coef", C.c_double * 7),
+        ("pentype", C.c_int32), ("pcore", _dp), ("palpha", _dp),
+        ("cflux", C.c_int32),
+        ("nbond", C.c_int32), ("bond_atoms", _ip), ("bond_flux", _dp),
+        ("nangle", C.c_int32), ("angle_atoms", _ip), ("angle_flux", _dp),
     ]
 
 

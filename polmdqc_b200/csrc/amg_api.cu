@@ -11,6 +11,7 @@
 #include "kernels_pair.cuh"
 #include "kernels_misc.cuh"
 #include "kernels_adjoint.cuh"
+#include "kernels_cp.cuh"
 
 #include <cub/device/device_radix_sort.cuh>
 #include <cufft.h>
@@ -208,6 +209,18 @@ struct amg_ctx {
     double timing[5] = {0, 0, 0, 0, 0};
     // last forward state for the adjoint
     bool have_forward = false;
+    // charge penetration / charge flux of the multipoles (non-Ewald, no
+    // polarization): damping tables, per-site core charges and exponents,
+    // the bond and angle terms of the flux, the increments dq and the sites'
+    // potentials cfpot of the current evaluation
+    bool cp_mode = false, cflux = false;
+    CpTables cpt{};
+    double *pcore = nullptr, *palpha = nullptr, *dq = nullptr, *cfpot = nullptr;
+    int nbond = 0, nangle = 0;
+    int2* bonds = nullptr;
+    double2* bflux = nullptr;
+    int* angles = nullptr;
+    double* aflux = nullptr;
 };
 
 namespace {
@@ -448,7 +461,8 @@ void rotate_and_pack(amg_ctx* ctx, cudaStream_t s) {
     k_rotate<R><<<nblk(ctx->n), kThreads, 0, s>>>(ctx->n, ctx->xyz, ctx->pole13, ctx->zax, ctx->xax, ctx->yax,
                                                   ctx->axe, ctx->has_pol ? ctx->pdamp : nullptr,
                                                   ctx->has_pol ? ctx->thole : nullptr,
-                                                  ctx->has_pol ? ctx->pol : nullptr, ctx->rp10, A.at);
+                                                  ctx->has_pol ? ctx->pol : nullptr, ctx->cflux ? ctx->dq : nullptr,
+                                                  ctx->rp10, A.at);
     KCHECK();
 }
 
@@ -1028,6 +1042,13 @@ void enqueue_front(amg_ctx* ctx, cudaStream_t s) {
     const int n = ctx->n;
     const bool mixed = ctx->prec == AMG_PREC_MIXED;
     CK(cudaEventRecord(ctx->ev[0], s));
+    if (ctx->cflux) {  // monopole increments of this geometry, before the rotation uses them
+        k_zero<double><<<nblk(n, 256), 256, 0, s>>>(ctx->dq, (size_t)n);
+        KCHECK();
+        k_cflux_charges<<<nblk((size_t)ctx->nbond + ctx->nangle), kThreads, 0, s>>>(
+            ctx->nbond, ctx->bonds, ctx->bflux, ctx->nangle, ctx->angles, ctx->aflux, ctx->xyz, ctx->dq);
+        KCHECK();
+    }
     rotate_and_pack<R>(ctx, s);
     if (mixed && iterative(ctx)) rotate_and_pack<double>(ctx, s);
     k_zero<double><<<1, 32, 0, s>>>(ctx->eacc, kEacc);
@@ -1200,6 +1221,29 @@ void enqueue_back(amg_ctx* ctx, cudaStream_t s, int flags) {
     double* virp = ctx->want_vir ? ctx->eacc + kVirP : nullptr;  // ep terms
     // Analysis and Virial outputs come from the EXTRA pair kernels
     const bool extra = analysis || vir;
+    if (ctx->cp_mode) {
+        // charge penetration / charge flux: the core/valence pairs in FP64
+        if (ctx->cflux) {
+            k_zero<double><<<nblk(n, 256), 256, 0, r>>>(ctx->cfpot, (size_t)n);
+            KCHECK();
+        }
+        auto launch = [&](auto kern) {
+            kern<<<nblk((size_t)n * 8), kThreads, 0, r>>>(
+                n, ctx->sids, ctx->xyz, ctx->rp10, ctx->pcore, ctx->palpha, ctx->cpt, ctx->bx, ctx->nbr, ctx->cap,
+                ctx->nnb, ctx->f, ctx->grad_m, ctx->trq_m, ctx->cflux ? ctx->cfpot : nullptr, ctx->eacc,
+                analysis ? ctx->aem : nullptr, analysis ? mol : nullptr, analysis ? ctx->cnt : nullptr, vir);
+        };
+        if (extra) launch(k_cp_pair<8, true>);
+        else launch(k_cp_pair<8, false>);
+        KCHECK();
+        if (ctx->nsp) {
+            k_cp_scaled<<<nblk(ctx->nsp), kThreads, 0, r>>>(
+                ctx->nsp, ctx->sp, ctx->xyz, ctx->rp10, ctx->pcore, ctx->palpha, ctx->cpt, ctx->bx, cut2, ctx->f,
+                ctx->grad_m, ctx->trq_m, ctx->cflux ? ctx->cfpot : nullptr, ctx->eacc, analysis ? ctx->aem : nullptr,
+                analysis ? mol : nullptr, analysis ? ctx->cnt : nullptr, vir);
+            KCHECK();
+        }
+    } else {
     LPA_DISPATCH(ctx->lpa, {
         const size_t nb = nblk((size_t)n * L);
         auto launch_n = [&](auto kern, size_t blocks) {
@@ -1227,6 +1271,7 @@ void enqueue_back(amg_ctx* ctx, cudaStream_t s, int flags) {
                                                           analysis ? ctx->aem : nullptr, analysis ? mol : nullptr,
                                                           analysis ? ctx->cnt : nullptr, vir);
         KCHECK();
+    }
     }
     if (polgrad) {
         auto launch = [&](auto kern, int lanes) {
@@ -1281,6 +1326,12 @@ void enqueue_back(amg_ctx* ctx, cudaStream_t s, int flags) {
         k_torque<<<nblk(n), kThreads, 0, s>>>(n, ctx->xyz, ctx->zax, ctx->xax, ctx->yax, ctx->axe, ctx->trq_m,
                                               ctx->grad_m, vir);
         KCHECK();
+        if (ctx->cflux) {  // the gradient through the geometry-dependent monopoles
+            k_cflux_grad<<<nblk((size_t)ctx->nbond + ctx->nangle), kThreads, 0, s>>>(
+                ctx->nbond, ctx->bonds, ctx->bflux, ctx->nangle, ctx->angles, ctx->aflux, ctx->xyz, ctx->cfpot,
+                ctx->grad_m, vir);
+            KCHECK();
+        }
     }
     CK(cudaEventRecord(ctx->ev[4], s));
 }
@@ -1561,8 +1612,36 @@ void release(amg_ctx* ctx) {
     dfree(ctx->adj); dfree(ctx->adj_pot); dfree(ctx->adj_n); dfree(ctx->adj_vec); dfree(ctx->adj_phi);
     dfree(ctx->adj_dpole);
     dfree(ctx->adj_opt);
+    dfree(ctx->pcore); dfree(ctx->palpha); dfree(ctx->dq); dfree(ctx->cfpot);
+    dfree(ctx->bonds); dfree(ctx->bflux); dfree(ctx->angles); dfree(ctx->aflux);
     if (ctx->st) { cudaStreamDestroy(ctx->st); ctx->st = nullptr; }
     if (ctx->st2) { cudaStreamDestroy(ctx->st2); ctx->st2 = nullptr; }
+}
+
+// Damping polynomials of the charge-penetration densities: Q_0 the base of
+// each family, Q_{n+1} = Q_n + x (Q_n - Q_n') / (2n + 1), the relation that
+// makes B_n = bare_n (1 - Q_n(x) e^{-x}) the radial hierarchy of the base
+// potential (see kernels_cp.cuh)
+CpTables cp_tables(int pentype) {
+    CpTables T{};
+    T.pentype = pentype;
+    auto family = [](std::initializer_list<double> base, double (&out)[6][kCpTerms]) {
+        for (auto& row : out)
+            for (double& c : row) c = 0.0;
+        int j = 0;
+        for (double c : base) out[0][j++] = c;
+        for (int n = 0; n < 5; n++) {
+            for (int q = 0; q < kCpTerms; q++) out[n + 1][q] = out[n][q];
+            for (int q = 0; q + 1 < kCpTerms; q++) {
+                const double qmd = out[n][q] - (q + 1) * out[n][q + 1];  // (Q - Q') at x^q
+                out[n + 1][q + 1] += qmd / (2 * n + 1);
+            }
+        }
+    };
+    family({1.0, 0.5}, T.f1);
+    family({1.0}, T.f2);
+    family({1.0, 11.0 / 16, 3.0 / 16, 1.0 / 48}, T.e1);
+    return T;
 }
 
 int create_impl(amg_ctx* ctx, const amg_params* P) {
@@ -1681,6 +1760,31 @@ int create_impl(amg_ctx* ctx, const amg_params* P) {
         dalloc(ctx, *p, 3 * (size_t)n);
         CK(cudaMemset(*p, 0, sizeof(double) * 3 * n));
     }
+    if (P->pentype != AMG_PEN_NONE || P->cflux) {
+        ctx->cp_mode = true;
+        ctx->cpt = cp_tables(P->pentype);
+        if (P->pentype != AMG_PEN_NONE) {
+            upload(ctx, ctx->pcore, P->pcore, n);
+            upload(ctx, ctx->palpha, P->palpha, n);
+        }
+        if (P->cflux) {
+            ctx->cflux = true;
+            ctx->nbond = P->nbond;
+            ctx->nangle = P->nangle;
+            std::vector<int2> b(std::max(1, P->nbond));
+            std::vector<double2> bf(std::max(1, P->nbond));
+            for (int q = 0; q < P->nbond; q++) {
+                b[q] = make_int2(P->bond_atoms[2 * q], P->bond_atoms[2 * q + 1]);
+                bf[q] = make_double2(P->bond_flux[2 * q], P->bond_flux[2 * q + 1]);
+            }
+            upload(ctx, ctx->bonds, b.data(), b.size());
+            upload(ctx, ctx->bflux, bf.data(), bf.size());
+            upload(ctx, ctx->angles, P->nangle ? P->angle_atoms : nullptr, 3 * (size_t)std::max(1, P->nangle));
+            upload(ctx, ctx->aflux, P->nangle ? P->angle_flux : nullptr, 7 * (size_t)std::max(1, P->nangle));
+            dalloc(ctx, ctx->dq, n);
+            dalloc(ctx, ctx->cfpot, n);
+        }
+    }
     dalloc(ctx, ctx->aem, n);
     dalloc(ctx, ctx->aep, n);
     dalloc(ctx, ctx->scal, 16);
@@ -1739,6 +1843,32 @@ int validate(const amg_params* P, std::string& why) {
     if (P->cell_shape < AMG_CELL_FROM_ANGLES || P->cell_shape > AMG_CELL_DODECAHEDRON) {
         why = "unknown cell shape";
         return AMG_ERR_BAD_ARG;
+    }
+    if (P->pentype != AMG_PEN_NONE || P->cflux) {
+        // the reference has both only in its non-Ewald multipole mode
+        if (P->use_ewald || (P->polarity && P->poltyp != AMG_POL_NONE)) {
+            why = "charge penetration and charge flux need the non-Ewald multipole mode without polarization";
+            return AMG_ERR_UNSUPPORTED;
+        }
+        if (P->pentype < AMG_PEN_NONE || P->pentype > AMG_PEN_GORDON2) {
+            why = "unknown charge penetration type";
+            return AMG_ERR_BAD_ARG;
+        }
+        if (P->pentype != AMG_PEN_NONE && (!P->pcore || !P->palpha)) {
+            why = "charge penetration needs pcore and palpha";
+            return AMG_ERR_BAD_ARG;
+        }
+        if (P->cflux) {
+            if (P->nbond < 0 || P->nangle < 0 || (P->nbond && (!P->bond_atoms || !P->bond_flux)) ||
+                (P->nangle && (!P->angle_atoms || !P->angle_flux))) {
+                why = "charge flux needs its bond and angle arrays";
+                return AMG_ERR_BAD_ARG;
+            }
+            for (int q = 0; q < 2 * P->nbond; q++)
+                if (P->bond_atoms[q] < 0 || P->bond_atoms[q] >= P->n) { why = "bond atom out of range"; return AMG_ERR_BAD_ARG; }
+            for (int q = 0; q < 3 * P->nangle; q++)
+                if (P->angle_atoms[q] < 0 || P->angle_atoms[q] >= P->n) { why = "angle atom out of range"; return AMG_ERR_BAD_ARG; }
+        }
     }
     for (int i = 0; i < P->n; i++) {
         int ft = P->polaxe[i];

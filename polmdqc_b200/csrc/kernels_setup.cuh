@@ -99,11 +99,12 @@ __global__ void k_rotate(int n, const double* __restrict__ xyz, const double* __
                          const int* __restrict__ zax, const int* __restrict__ xax, const int* __restrict__ yax,
                          const int* __restrict__ axe, const double* __restrict__ pdamp,
                          const double* __restrict__ thole, const double* __restrict__ pol,
-                         double* __restrict__ rp10, AtomR<R>* __restrict__ atoms) {
+                         const double* __restrict__ dq, double* __restrict__ rp10, AtomR<R>* __restrict__ atoms) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double m[10];
     frame_and_rotate(i, xyz, pole13, zax, xax, yax, axe, m);
+    if (dq) m[0] += dq[i];  // charge flux: the monopole of the current geometry
     for (int j = 0; j < 10; j++) rp10[10 * i + j] = m[j];
     AtomR<R> A;
     A.a = make_r4<R>((R)xyz[3 * i], (R)xyz[3 * i + 1], (R)xyz[3 * i + 2], (R)m[0]);

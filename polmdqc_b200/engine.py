@@ -101,6 +101,20 @@ class Params:
         if st.poltyp == abi.POL_OPT:
             for k, c in enumerate(OPT_COEF[st.opt_order]):
                 p.opt_coef[k] = c
+        if getattr(s, "pentype", 0):
+            pc = np.ascontiguousarray(s.pcore, np.float64)
+            pa = np.ascontiguousarray(s.palpha, np.float64)
+            self.keep += [pc, pa]
+            p.pentype, p.pcore, p.palpha = int(s.pentype), abi.dptr(pc), abi.dptr(pa)
+        if getattr(s, "cflux", False):
+            ba = np.ascontiguousarray(s.bond_atoms, np.int32).reshape(-1)
+            bf = np.ascontiguousarray(s.bond_flux, np.float64).reshape(-1)
+            aa = np.ascontiguousarray(s.angle_atoms, np.int32).reshape(-1)
+            af = np.ascontiguousarray(s.angle_flux, np.float64).reshape(-1)
+            self.keep += [ba, bf, aa, af]
+            p.cflux = 1
+            p.nbond, p.bond_atoms, p.bond_flux = len(s.bond_atoms), abi.iptr(ba), abi.dptr(bf)
+            p.nangle, p.angle_atoms, p.angle_flux = len(s.angle_atoms), abi.iptr(aa), abi.dptr(af)
         self.struct = p
         self.n = s.n
 

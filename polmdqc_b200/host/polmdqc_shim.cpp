@@ -22,10 +22,15 @@
 // which is where the library's status codes meet the reference's convention.
 #include "action.h"
 #include "analyz.h"
+#include "angbnd.h"
+#include "atmlst.h"
 #include "atoms.h"
 #include "bound.h"
+#include "bndstr.h"
 #include "boxes.h"
 #include "calcMode.h"
+#include "cflux.h"
+#include "chgpen.h"
 #include "chgpot.h"
 #include "couple.h"
 #include "deriv.h"
@@ -86,13 +91,21 @@ struct Device {
     std::vector<double> pole13, polar_, thole_, pdamp_;
     std::vector<int32_t> zax, xax, yax, axe, mol;
     Csr l12, l13, l14, l15, g11, g12, g13, g14;
+    // charge penetration and charge flux (chgpen.h, cflux.h, bndstr.h, angbnd.h)
+    std::vector<double> pcore_, palpha_, bflux_, aflux_;
+    std::vector<int32_t> batoms_, aatoms_;
 } dev;
+
+// the monopole the context starts from: with charge flux the reference's
+// energy() rewrites pole[i][0] every call (alterchg, src/md/energy.cpp:241),
+// so the unaltered mono0 is the parameter
+double monopole(int i) { return use_chgflx ? mono0[i] : pole[i][0]; }
 
 // a cheap signature of the parameters that would force a new context
 double signature()
 {
     double s = n + 7 * aeewald + 3 * ewaldcut + 5 * mpolecut + nefft1 + 3 * nefft2 + 5 * nefft3 + (use_ewald ? 11 : 0);
-    for (int i = 0; i < n; i++) s += (i % 13 + 1) * pole[i][0];
+    for (int i = 0; i < n; i++) s += (i % 13 + 1) * monopole(i);
     return s;
 }
 
@@ -118,6 +131,7 @@ void ensure_context(bool want_polar)
     dev.zax.resize(n); dev.xax.resize(n); dev.yax.resize(n); dev.axe.resize(n); dev.mol.resize(n);
     for (int i = 0; i < n; i++) {
         for (int j = 0; j < 13; j++) dev.pole13[13 * i + j] = pole[i][j];
+        dev.pole13[13 * i] = monopole(i);
         dev.zax[i] = zaxis[i]; dev.xax[i] = xaxis[i]; dev.yax[i] = yaxis[i];
         dev.axe[i] = (int32_t)polaxe[i];
         dev.mol[i] = molcule[i];
@@ -178,6 +192,44 @@ void ensure_context(bool want_polar)
     p.pcg_prec = pcgprec;
     p.usolvcut = usolvcut;
     p.cell_shape = octahedron ? AMG_CELL_OCTAHEDRON : dodecadron ? AMG_CELL_DODECAHEDRON : AMG_CELL_FROM_ANGLES;
+    // charge penetration (pairMpoleCP) and charge flux (alterchg / dcflux):
+    // the library takes them in the non-Ewald multipole mode and returns
+    // UNSUPPORTED otherwise, which stops the program below
+    p.pentype = pentype == PenTyp::Gordon1 ? AMG_PEN_GORDON1 : pentype == PenTyp::Gordon2 ? AMG_PEN_GORDON2 : AMG_PEN_NONE;
+    if (p.pentype != AMG_PEN_NONE) {
+        dev.pcore_.assign(pcore.ptr(), pcore.ptr() + n);
+        dev.palpha_.assign(palpha.ptr(), palpha.ptr() + n);
+        p.pcore = dev.pcore_.data();
+        p.palpha = dev.palpha_.data();
+    }
+    if (use_chgflx) {
+        p.cflux = 1;
+        dev.batoms_.assign(2 * (size_t)nbond + 1, 0);
+        dev.bflux_.assign(2 * (size_t)nbond + 1, 0.0);
+        for (int b = 0; b < nbond; b++) {
+            dev.batoms_[2 * b] = ibnd[b][0];
+            dev.batoms_[2 * b + 1] = ibnd[b][1];
+            dev.bflux_[2 * b] = bl[b];
+            dev.bflux_[2 * b + 1] = bflx[b];
+        }
+        dev.aatoms_.assign(3 * (size_t)nangle + 1, 0);
+        dev.aflux_.assign(7 * (size_t)nangle + 1, 0.0);
+        for (int a = 0; a < nangle; a++) {
+            for (int j = 0; j < 3; j++) dev.aatoms_[3 * a + j] = iang[a][j];
+            double* f = &dev.aflux_[7 * (size_t)a];
+            f[0] = anat[a];
+            f[1] = bl[balist[a][0]];
+            f[2] = bl[balist[a][1]];
+            f[3] = aflx[a][0]; f[4] = aflx[a][1];
+            f[5] = abflx[a][0]; f[6] = abflx[a][1];
+        }
+        p.nbond = nbond;
+        p.bond_atoms = dev.batoms_.data();
+        p.bond_flux = dev.bflux_.data();
+        p.nangle = nangle;
+        p.angle_atoms = dev.aatoms_.data();
+        p.angle_flux = dev.aflux_.data();
+    }
     int rc = amg_create(&p, &dev.ctx);
     if (rc != AMG_OK) {
         printf("\n AMOEBA GPU  --  amg_create failed (status %d)\n", rc);
@@ -189,14 +241,6 @@ template <CalcMode M>
 void evaluate(bool fill_mpole, bool fill_polar)
 {
     constexpr CalcFlag flags = getCalculationFlags<M>();
-    // charge penetration (pairMpoleCP, include/md/pairMpole.h:186-389) and
-    // charge flux (dcflux) are not on the GPU: stop, as the reference's
-    // fatal() does, rather than return plain multipole energies
-    if (pentype != PenTyp::None || use_chgflx) {
-        printf("\n AMOEBA GPU  --  charge penetration / charge flux are not supported (status %d)\n",
-               AMG_ERR_UNSUPPORTED);
-        fatal();
-    }
     const bool want_polar = use_polar && polarity.size() >= n;
     ensure_context(want_polar);
     std::vector<double> xyz(3 * (size_t)n);

@@ -57,6 +57,15 @@ class System:
     use_bounds: bool
     prm_name: str = ""
     cell_shape: int = 0        # abi.CELL_*: octahedron / dodecahedron, else from the angles
+    # charge penetration (chgpen.h) and charge flux (cflux.h, bndstr.h, angbnd.h)
+    pentype: int = 0           # abi.PEN_*
+    pcore: np.ndarray = None   # [n] core charges
+    palpha: np.ndarray = None  # [n] valence damping exponents
+    cflux: bool = False        # monopoles follow the geometry; pole[:, 0] is then mono0
+    bond_atoms: np.ndarray = None   # [nbond, 2] 0-based
+    bond_flux: np.ndarray = None    # [nbond, 2] ideal length, flux
+    angle_atoms: np.ndarray = None  # [nangle, 3] 0-based a, b (vertex), c
+    angle_flux: np.ndarray = None   # [nangle, 7] theta0 (deg), r0_ab, r0_cb, pa1, pa2, pb1, pb2
 
     def csr(self, name):
         lists = self.lists[name]
@@ -366,8 +375,21 @@ def from_dump(d: dict, prm_name: str = "") -> System:
     for k in ("ip11", "ip12", "ip13", "ip14"):
         lists[k] = d.get(k, [[] for _ in range(n)])
     box = np.array(d["box"], np.float64)
+    pole = np.array(d["pole"]).reshape(n, 13)
+    cp = {}
+    if d.get("pentype", 0):
+        cp.update(pentype=int(d["pentype"]), pcore=np.array(d["pcore"]), palpha=np.array(d["palpha"]))
+    if d.get("use_chgflx", 0):
+        pole[:, 0] = d["mono0"]          # the dump's pole holds the monopoles altered for its geometry
+        nb, na = d["nbond"], d["nangle"]
+        cp.update(cflux=True, bond_atoms=np.array(d["ibnd"], np.int32).reshape(nb, 2),
+                  bond_flux=np.stack([d["bl"], d["bflx"]], 1).reshape(nb, 2),
+                  angle_atoms=np.array(d["iang"], np.int32).reshape(na, 3),
+                  angle_flux=np.concatenate([np.array(d["anat"]).reshape(na, 1), np.array(d["rab0"]).reshape(na, 1),
+                                             np.array(d["rcb0"]).reshape(na, 1), np.array(d["aflx"]).reshape(na, 2),
+                                             np.array(d["abflx"]).reshape(na, 2)], 1))
     return System(n=n, xyz=xyz, types=np.array(d["type"], np.int32), names=[""] * n, bonds=bonds,
-                  pole=np.array(d["pole"]).reshape(n, 13), zaxis=np.array(d["zaxis"], np.int32),
+                  pole=pole, zaxis=np.array(d["zaxis"], np.int32),
                   xaxis=np.array(d["xaxis"], np.int32), yaxis=np.array(d["yaxis"], np.int32),
                   polaxe=np.array(d["polaxe"], np.int32), molcule=np.array(d["molcule"], np.int32),
                   polarity=np.array(d["polarity"]) if has_pol else np.zeros(n),
@@ -377,7 +399,7 @@ def from_dump(d: dict, prm_name: str = "") -> System:
                   d_scale=d["dscale"], u_scale=d["uscale"], box=box,
                   use_bounds=bool(d["use_bounds"]), prm_name=prm_name,
                   cell_shape=(abi.CELL_OCTAHEDRON if d.get("octahedron") else
-                              abi.CELL_DODECAHEDRON if d.get("dodecadron") else abi.CELL_FROM_ANGLES))
+                              abi.CELL_DODECAHEDRON if d.get("dodecadron") else abi.CELL_FROM_ANGLES), **cp)
 
 
 def write_tinker(sys_: System, xyz_path: str, key_path: str, prm_path: str, keys: list):

@@ -67,10 +67,10 @@ def run_dump(xyz, key, cwd):
 def main(ref_root):
     # ---- golden values of the reference's own tests
     hdr = {h: parse_header(os.path.join(ref_root, "test", h + ".h"))
-           for h in ("amoeba", "bounds", "chkpole", "amoebaMisc", "rotpole")}
+           for h in ("amoeba", "bounds", "chkpole", "amoebaMisc", "rotpole", "amoebap", "hippo")}
     amoeba, bounds = hdr["amoeba"], hdr["bounds"]
     tests = {
-        "source": "test/amoeba.h, bounds.h, chkpole.h, amoebaMisc.h, rotpole.h of momokchung/polmdqc",
+        "source": "test/amoeba.h, bounds.h, chkpole.h, amoebaMisc.h, rotpole.h, amoebap.h, hippo.h of momokchung/polmdqc",
         "amoeba1": {"inputs": "test/testFiles/amoeba/water09.xyz (+ water09.key)", **amoeba["amoeba1"]},
         "amoeba2": {"inputs": "test/testFiles/amoeba/water09.xyz (+ water09.key)", **amoeba["amoeba2"]},
     }
@@ -86,12 +86,18 @@ def main(ref_root):
                    "amoebaMisc5": "test/testFiles/amoebaMisc/water09NSeq.xyz"}
     for k, inp in misc_inputs.items():
         tests[k] = {"inputs": inp, **hdr["amoebaMisc"][k]}
-    # frames: Z-Only (rotpole2) and Z-Bisect + 3-Fold (rotpole3) in HIPPO
-    # inputs; only the rotated multipoles are used here (the energies include
-    # charge penetration)
+    # frames: Z-Only (rotpole2/5) and Z-Bisect + 3-Fold (rotpole3/6) in HIPPO
+    # inputs (charge penetration, Gordon f1, no charge flux)
     for k, inp in (("rotpole2", "test/testFiles/rotpole/benzene_ethyne_water.xyz"),
-                   ("rotpole3", "test/testFiles/rotpole/ammonia.xyz")):
+                   ("rotpole3", "test/testFiles/rotpole/ammonia.xyz"),
+                   ("rotpole5", "test/testFiles/rotpole/benzene_ethyne_water.xyz"),
+                   ("rotpole6", "test/testFiles/rotpole/ammonia.xyz")):
         tests[k] = {"inputs": inp, **hdr["rotpole"][k]}
+    # charge penetration with charge flux: the AMOEBA+ water dimer (Gordon
+    # f2, amoebaplus.prm) and the HIPPO water dimer (Gordon f1, water21.prm)
+    for name, inp in (("amoebap", "test/testFiles/amoebap/waterap.xyz"), ("hippo", "test/testFiles/hippo/water21.xyz")):
+        for k in (name + "1", name + "2"):
+            tests[k] = {"inputs": inp, **hdr[name][k]}
     shapes = {"bounds1": "orthogonal", "bounds2": "monoclinic", "bounds3": "triclinic", "bounds4": "octahedron",
               "bounds5": "dodecahedron"}
     for k, shape in shapes.items():

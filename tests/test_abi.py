@@ -18,7 +18,7 @@ def test_library_exports_header_symbols():
     assert {"amg_create", "amg_set_coords", "amg_forward", "amg_backward", "amg_destroy"} <= set(declared)
     for name in declared:
         assert hasattr(lib, name), name
-    assert lib.amg_abi_version() == 3
+    assert lib.amg_abi_version() == 4
 
 
 def test_struct_layout_matches_header():
@@ -27,9 +27,10 @@ def test_struct_layout_matches_header():
     #include <cstddef>
     #include "amoeba_gpu.h"
     int main() {
-      printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(amg_params), sizeof(amg_results), sizeof(amg_cotangents),
+      printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(amg_params), sizeof(amg_results), sizeof(amg_cotangents),
              sizeof(amg_param_grads), offsetof(amg_params, precision), offsetof(amg_results, pcg_eps),
-             offsetof(amg_params, u_scale), offsetof(amg_results, rpole), offsetof(amg_params, cell_shape));
+             offsetof(amg_params, u_scale), offsetof(amg_results, rpole), offsetof(amg_params, cell_shape),
+             offsetof(amg_params, pentype), offsetof(amg_params, angle_flux));
     }"""
     with tempfile.TemporaryDirectory() as t:
         c = os.path.join(t, "s.cpp")
@@ -40,7 +41,7 @@ def test_struct_layout_matches_header():
     P, R = abi.amg_params, abi.amg_results
     assert vals == [ctypes.sizeof(P), ctypes.sizeof(R), ctypes.sizeof(abi.amg_cotangents),
                     ctypes.sizeof(abi.amg_param_grads), P.precision.offset, R.pcg_eps.offset,
-                    P.u_scale.offset, R.rpole.offset, P.cell_shape.offset]
+                    P.u_scale.offset, R.rpole.offset, P.cell_shape.offset, P.pentype.offset, P.angle_flux.offset]
 
 
 def test_create_without_gpu_fails_cleanly():

@@ -124,3 +124,20 @@ def test_dropin_analyze_program_reads_every_structure():
     assert nem == g["nem"]
     assert abs(em - g["em"]) < 1e-8
     assert abs(float(rows[0][2]) - g["em"]) > 1.0     # the first structure is the peptide
+
+
+@pytest.mark.parametrize("analysis,gradient,name", [("amoebap1", "amoebap2", ("amoebap", "waterap.xyz")),
+                                                    ("hippo1", "hippo2", ("hippo", "water21.xyz"))])
+def test_dropin_charge_penetration_and_flux_golden(analysis, gradient, name):
+    """amoebap-1/-2 and hippo-1/-2 through the reference's own set-up and
+    energy() with the shim: its alterchg rewrites the monopoles each call, the
+    shim hands the library the unaltered ones and the bond / angle flux terms,
+    and the library's charge penetration and charge flux reproduce the
+    goldens."""
+    g = golden("ref_tests.json")
+    d = dump_gpu(ref_fixture(*name))
+    ga, gg = g[analysis], g[gradient]
+    assert d["nem"] == ga["nem"]
+    assert abs(d["em"] - ga["em"]) < ga["eps"]
+    np.testing.assert_allclose(d["aem"], ga["aem"], atol=ga["eps"], rtol=0)
+    np.testing.assert_allclose(d["dem"], gg["dem"], atol=gg["eps1"], rtol=0)

@@ -125,3 +125,24 @@ def test_frames_rotated_multipoles_and_torques(case, name):
                 assert abs((p - m) / (2 * h) - r.dem[i, a]) < 1e-6, (i, a)
     finally:
         e.close()
+
+
+CP_CASES = [("amoebap1", "amoebap2", ("amoebap", "waterap.xyz")),      # Gordon f2 + charge flux (AMOEBA+)
+            ("hippo1", "hippo2", ("hippo", "water21.xyz")),            # Gordon f1 + charge flux (HIPPO)
+            ("rotpole3", "rotpole6", ("rotpole", "ammonia.xyz")),      # Gordon f1, Z-Bisect and 3-Fold frames
+            ("rotpole2", "rotpole5", ("rotpole", "benzene_ethyne_water.xyz"))]  # Gordon f1, Z-Only frames
+
+
+@pytest.mark.parametrize("prec", [FP64, MIXED])
+@pytest.mark.parametrize("analysis,gradient,parts", CP_CASES)
+def test_charge_penetration_goldens(analysis, gradient, parts, prec):
+    """amoebap-1/-2, hippo-1/-2 and rotpole-2/-3/-5/-6 through the C ABI:
+    charge penetration of the multipoles (the FP64 core/valence pair kernels
+    in both precisions) and, for the two water dimers, charge flux: em, nem,
+    einter, aem at the reference's eps and dem at eps1 (1e-10)."""
+    g = golden("ref_tests.json")
+    ga, gg = g[analysis], g[gradient]
+    d = ref_dump(ref_fixture(*parts))
+    r = run(systems.from_dump(d), d["mpolecut"], prec)
+    check_analysis(r, ga, FP64)
+    np.testing.assert_allclose(r.dem.reshape(-1), gg["dem"], atol=gg["eps1"], rtol=0)

@@ -190,3 +190,48 @@ def test_frames_golden_rotated_multipoles(case, name):
     s = systems.from_dump(d)
     r = oracle.forward(s, nonewald(d["mpolecut"]), flags=abi.DO_ENERGY)
     np.testing.assert_allclose(r.rpole, np.array(g["rpole"]), atol=1e-14, rtol=0)
+
+
+CP_CASES = [("amoebap1", "amoebap2", ("amoebap", "waterap.xyz")),      # Gordon f2 + charge flux (AMOEBA+)
+            ("hippo1", "hippo2", ("hippo", "water21.xyz")),            # Gordon f1 + charge flux (HIPPO)
+            ("rotpole3", "rotpole6", ("rotpole", "ammonia.xyz")),      # Gordon f1, Z-Bisect and 3-Fold frames
+            ("rotpole2", "rotpole5", ("rotpole", "benzene_ethyne_water.xyz"))]  # Gordon f1, Z-Only frames
+
+
+@pytest.mark.parametrize("analysis,gradient,parts", CP_CASES)
+def test_charge_penetration_goldens(analysis, gradient, parts):
+    """test/amoebap.cpp, test/hippo.cpp and test/rotpole.cpp: charge
+    penetration of the multipoles (include/md/pairMpole.h:186-389), with charge
+    flux for the AMOEBA+ and HIPPO water dimers (src/md/alterchg.cpp,
+    src/md/dcflux.cpp): em, nem, einter, aem at eps and the analytic dem at
+    eps1 (1e-10)."""
+    g = golden("ref_tests.json")
+    ga, gg = g[analysis], g[gradient]
+    d = ref_dump(ref_fixture(*parts))
+    assert d["pentype"] in (1, 2)
+    _, r = _analysis(d)
+    assert r.nem == ga["nem"]
+    assert abs(r.em - ga["em"]) < ga["eps"] and abs(r.einter - ga["einter"]) < ga["eps"]
+    np.testing.assert_allclose(r.aem, ga["aem"], atol=ga["eps"], rtol=0)
+    np.testing.assert_allclose(r.dem.reshape(-1), gg["dem"], atol=gg["eps1"], rtol=0)
+
+
+def test_charge_flux_gradient_matches_finite_differences():
+    """The charge-flux chain rule of the oracle (dE/dq times dq/dx for bonds
+    and angles) against central differences of its energies, on the HIPPO
+    water dimer with its bonds and angles bent away from their ideal values."""
+    d = ref_dump(ref_fixture("hippo", "water21.xyz"))
+    s = systems.from_dump(d)
+    rng = np.random.default_rng(2)
+    s.xyz = s.xyz + 0.05 * rng.standard_normal(s.xyz.shape)
+    st = nonewald(d["mpolecut"])
+    r = oracle.forward(s, st, flags=abi.DO_ENERGY | abi.DO_GRADIENT)
+    h = 1e-5
+    for i in range(s.n):
+        for a in range(3):
+            x = s.xyz.copy()
+            x[i, a] += h
+            p = oracle.forward(s, st, xyz=x, flags=abi.DO_ENERGY).em
+            x[i, a] -= 2 * h
+            m = oracle.forward(s, st, xyz=x, flags=abi.DO_ENERGY).em
+            assert abs((p - m) / (2 * h) - r.dem[i, a]) < 1e-7, (i, a)

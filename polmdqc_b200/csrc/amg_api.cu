@@ -138,6 +138,8 @@ struct amg_ctx {
     size_t cubtmp_bytes = 0;
     int* nbr = nullptr;
     int* nnb = nullptr;
+    int* rank = nullptr;  // position of each site in cell order (inverse of sids)
+    int* cnb = nullptr;   // [n][cap] cell-order positions of the PCG coefficient rows' neighbours
     int cap = 0, lpa = 16, num_sms = 148;
     int* overflow = nullptr;
     // sparse PCG preconditioner (pcgprec): rows of the pairs within usolvcut,
@@ -622,6 +624,7 @@ void ensure_list_buffers(amg_ctx* ctx) {
         dalloc(ctx, ctx->nnb, n);
         dalloc(ctx, ctx->overflow, 1);
         dalloc(ctx, ctx->spos, n);
+        dalloc(ctx, ctx->rank, n);
         size_t bytes = 0;
         cub::DeviceRadixSort::SortPairs(nullptr, bytes, ctx->keys, ctx->skeys, ctx->ids, ctx->sids, n);
         dalloc(ctx, ctx->cubtmp, bytes);
@@ -639,6 +642,7 @@ void ensure_list_buffers(amg_ctx* ctx) {
         int cap = (int)std::min<double>(n - 1 + nx, std::ceil(1.4 * est) + 64 + nx);
         ctx->cap = std::max(cap, 1);
         dalloc(ctx, ctx->nbr, (size_t)ctx->cap * n);
+        dalloc(ctx, ctx->cnb, (size_t)ctx->cap * n);
         ctx->graph_dirty = true;
     }
 }
@@ -660,7 +664,8 @@ void enqueue_lists(amg_ctx* ctx, cudaStream_t s) {
     KCHECK();
     size_t bytes = ctx->cubtmp_bytes;
     CK(cub::DeviceRadixSort::SortPairs(ctx->cubtmp, bytes, ctx->keys, ctx->skeys, ctx->ids, ctx->sids, n, 0, nbits, s));
-    k_cell_bounds<<<nblk(n), kThreads, 0, s>>>(n, ctx->skeys, ctx->sids, ctx->xyz, ctx->cstart, ctx->cend, ctx->spos);
+    k_cell_bounds<<<nblk(n), kThreads, 0, s>>>(n, ctx->skeys, ctx->sids, ctx->xyz, ctx->cstart, ctx->cend, ctx->spos,
+                                               ctx->rank);
     KCHECK();
     const double cut2 = ctx->cut * ctx->cut;
     if (!cg.periodic || (cg.nc[0] >= 3 && cg.nc[1] >= 3 && cg.nc[2] >= 3)) {
@@ -745,7 +750,7 @@ template <class R>
 void spread_dipoles(amg_ctx* ctx, cudaStream_t s, const double* vd, const double* vp) {
     Pme<R>& pm = pme_of<R>(ctx);
     int3 K = make_int3(ctx->K[0], ctx->K[1], ctx->K[2]);
-    k_spread_dipoles<R, kOrder><<<nblk(ctx->n, kLineSites), 128, 0, s>>>(ctx->n, ctx->sids, vd, vp, pm.theta, pm.k0,
+    k_spread_dipoles<R, kOrder><<<spread_blocks<R>(ctx->n), 128, 0, s>>>(ctx->n, ctx->sids, vd, vp, pm.theta, pm.k0,
                                                                           K, ctx->frac,
                                                         pm.zg);
     KCHECK();
@@ -842,7 +847,7 @@ void build_scaled_coeffs(amg_ctx* ctx, cudaStream_t s) {
     const bool sp = ctx->sparse_prec;
     k_scaled_coeffs<R><<<nblk(ctx->nsp), kThreads, 0, s>>>(
         ctx->nsp, ctx->sp, ctx->xyz, ctx->pdamp, ctx->thole, ctx->bx, ctx->cut * ctx->cut, ewald_alpha(ctx), ctx->nnb,
-        ctx->cap, ctx->nbr, A.c0, ctx->usolvcut * ctx->usolvcut, sp ? ctx->nnbu : nullptr,
+        ctx->cap, ctx->rank, ctx->cnb, A.c0, ctx->usolvcut * ctx->usolvcut, sp ? ctx->nnbu : nullptr,
         sp ? ctx->nbru : nullptr, sp ? A.cu0 : nullptr);
     KCHECK();
 }
@@ -861,15 +866,15 @@ void build_tu_coeffs(amg_ctx* ctx, cudaStream_t s) {
     LPA_DISPATCH(ctx->lpa, {
         if (ewald_cells(ctx))
             k_tu_coeffs<R, true, 8, true><<<nblk((size_t)n * 8), kThreads, 0, s>>>(n, ctx->sids, A.at, ctx->bx, (R)ctx->aewald,
-                                                                                   ctx->nbr, ctx->cap, ctx->nnb, A.c0,
+                                                                                   ctx->nbr, ctx->cap, ctx->nnb, A.c0, ctx->rank, ctx->cnb,
                                                                                    (R)u2, nbru, cu0, nnbu);
         else if (ctx->ewald)
             k_tu_coeffs<R, true, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(n, ctx->sids, A.at, ctx->bx, (R)ctx->aewald, ctx->nbr,
-                                                                             ctx->cap, ctx->nnb, A.c0, (R)u2, nbru,
+                                                                             ctx->cap, ctx->nnb, A.c0, ctx->rank, ctx->cnb, (R)u2, nbru,
                                                                              cu0, nnbu);
         else
             k_tu_coeffs<R, false, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(n, ctx->sids, A.at, ctx->bx, (R)0, ctx->nbr, ctx->cap,
-                                                                              ctx->nnb, A.c0, (R)u2, nbru, cu0,
+                                                                              ctx->nnb, A.c0, ctx->rank, ctx->cnb, (R)u2, nbru, cu0,
                                                                               nnbu);
     });
     KCHECK();
@@ -886,7 +891,7 @@ void matvec_stored(amg_ctx* ctx, cudaStream_t s, const R4<R>* v4, const double* 
     // real space on the side stream, PME on s
     cudaStream_t r = ctx->ewald ? fork_side(ctx, s) : s;
     LPA_DISPATCH(ctx->lpa, {
-        k_tu_stored<R, L><<<nblk((size_t)n * L), kThreads, 0, r>>>(n, ctx->sids, ctx->nbr, A.c0, ctx->cap, ctx->nnb, ctx->xoff,
+        k_tu_stored<R, L><<<nblk((size_t)n * L), kThreads, 0, r>>>(n, ctx->sids, ctx->cnb, A.c0, ctx->cap, ctx->nnb, ctx->xoff,
                                                                     v4, ctx->Fd, ctx->Fp);
     });
     KCHECK();
@@ -951,10 +956,10 @@ void direction(amg_ctx* ctx, cudaStream_t s) {
     if (ctx->ewald) {
         Pme<R>& pm = pme_of<R>(ctx);
         const int3 K = make_int3(ctx->K[0], ctx->K[1], ctx->K[2]);
-        k_pcg_dir_spread<R, kOrder><<<nblk(n, kLineSites), 128, 0, s>>>(n, ctx->zd, ctx->zp, ctx->pd, ctx->pp, ctx->scal, A.p4, pm.theta,
-                                                       pm.k0, K, ctx->frac, pm.zg);
+        k_pcg_dir_spread<R, kOrder><<<spread_blocks<R>(n), 128, 0, s>>>(n, ctx->zd, ctx->zp, ctx->pd, ctx->pp, ctx->scal, A.p4, pm.theta,
+                                                       pm.k0, K, ctx->frac, pm.zg, ctx->rank);
     } else {
-        k_pcg_dir<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->zd, ctx->zp, ctx->pd, ctx->pp, ctx->scal, A.p4);
+        k_pcg_dir<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->zd, ctx->zp, ctx->pd, ctx->pp, ctx->scal, A.p4, ctx->rank);
     }
     KCHECK();
 }
@@ -975,17 +980,17 @@ void enqueue_pcg_init(amg_ctx* ctx, cudaStream_t s, cudaGraphConditionalHandle h
     k_zero<double><<<1, 32, 0, s>>>(ctx->scal, NSCAL);
     KCHECK();
     if (!coeffs_built) build_tu_coeffs<R>(ctx, s);
-    k_pack_u<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->ud, ctx->up, A.u4);
+    k_pack_u<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->ud, ctx->up, A.u4, ctx->rank);  // cell order
     KCHECK();
     matvec_stored<R>(ctx, s, A.u4, ctx->ud, ctx->up, ctx->Apd, ctx->App);
     k_pcg_init<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->Ed, ctx->Ep, ctx->Apd, ctx->App, ctx->pol, ctx->rd, ctx->rp,
                                                ctx->zd, ctx->zp, ctx->pd, ctx->pp, ctx->scal,
-                                               ctx->sparse_prec ? A.s4 : nullptr);
+                                               ctx->sparse_prec ? A.s4 : nullptr, ctx->rank);
     KCHECK();
     if (ctx->sparse_prec) {
         precondition<R>(ctx, s, true, ctx->scal + RZ_D, h, use_handle);  // with the first control decision
     } else {
-        k_pack_u<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->pd, ctx->pp, A.p4);
+        k_pack_u<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->pd, ctx->pp, A.p4, ctx->rank);
         KCHECK();
         k_pcg_control<<<1, 1, 0, s>>>(ctx->scal, ctx->iter, pcg_threshold(ctx), ctx->politer, 1, h, use_handle,
                                       ctx->cont);
@@ -1012,7 +1017,7 @@ void enqueue_pcg_iter(amg_ctx* ctx, cudaStream_t s, cudaGraphConditionalHandle h
     }
     k_pcg_update<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->pol, ctx->pd, ctx->pp, ctx->Apd, ctx->App, ctx->ud, ctx->up,
                                                  ctx->rd, ctx->rp, ctx->zd, ctx->zp, ctx->scal,
-                                                 ctx->sparse_prec ? A.s4 : nullptr);
+                                                 ctx->sparse_prec ? A.s4 : nullptr, ctx->rank);
     KCHECK();
     if (ctx->sparse_prec) {
         precondition<R>(ctx, s, false, ctx->scal + RZN_D, h, use_handle);  // with the control decision
@@ -1081,7 +1086,7 @@ void enqueue_front(amg_ctx* ctx, cudaStream_t s) {
         const R u2 = (R)(ctx->usolvcut * ctx->usolvcut);
         auto launch = [&](auto kern, unsigned nb) {
             kern<<<nb, kThreads, 0, r>>>(n, ctx->sids, A.at, ctx->bx, aew, ctx->nbr, ctx->cap, ctx->nnb, ctx->Ed, ctx->Ep,
-                                         coef ? A.c0 : nullptr, u2, sp ? ctx->nbru : nullptr,
+                                         coef ? A.c0 : nullptr, ctx->rank, ctx->cnb, u2, sp ? ctx->nbru : nullptr,
                                          sp ? A.cu0 : nullptr, sp ? ctx->nnbu : nullptr);
         };
         LPA_DISPATCH(ctx->lpa, {
@@ -1483,6 +1488,7 @@ int forward_impl(amg_ctx* ctx, int flags, amg_results* res) {
         }
         ctx->cap = ((over * 5 / 4) + 31) / 32 * 32;
         dalloc(ctx, ctx->nbr, (size_t)ctx->cap * n);
+        dalloc(ctx, ctx->cnb, (size_t)ctx->cap * n);
         ctx->graph_dirty = true;
     }
     ctx->graphed_last = ctx->use_graphs && ctx->bounds && ctx->gexec != nullptr;
@@ -1586,6 +1592,8 @@ void release(amg_ctx* ctx) {
     for (int** p : ints) dfree(*p);
     dfree(ctx->keys);
     dfree(ctx->skeys);
+    dfree(ctx->rank);
+    dfree(ctx->cnb);
     dfree(ctx->spos);
     dfree(ctx->cnt);
     dfree(ctx->sp);
@@ -2325,11 +2333,11 @@ int amg_time_tu_kernel(amg_ctx* ctx, int32_t reps, int64_t flush_bytes, double* 
             LPA_DISPATCH(ctx->lpa, {
                 if (mixed)
                     k_tu_stored<float, L><<<nblk((size_t)n * L), kThreads, 0, ctx->st>>>(
-                        n, ctx->sids, ctx->nbr, ctx->af.c0, ctx->cap, ctx->nnb, ctx->xoff, ctx->af.p4,
+                        n, ctx->sids, ctx->cnb, ctx->af.c0, ctx->cap, ctx->nnb, ctx->xoff, ctx->af.p4,
                         ctx->Fd, ctx->Fp);
                 else
                     k_tu_stored<double, L><<<nblk((size_t)n * L), kThreads, 0, ctx->st>>>(
-                        n, ctx->sids, ctx->nbr, ctx->ad.c0, ctx->cap, ctx->nnb, ctx->xoff, ctx->ad.p4,
+                        n, ctx->sids, ctx->cnb, ctx->ad.c0, ctx->cap, ctx->nnb, ctx->xoff, ctx->ad.p4,
                         ctx->Fd, ctx->Fp);
             });
             KCHECK();

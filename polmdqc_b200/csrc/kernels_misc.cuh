@@ -23,13 +23,17 @@ __global__ void k_field_finish(int n, const double* __restrict__ phiM, int ewald
     }
 }
 
-// FP64 dipole vectors -> R4 copies for the pair kernels ([n][2], d then p)
+// FP64 dipole vectors -> R4 copies for the pair kernels ([n][2], d then p),
+// at site i or, with rank, at the site's position in cell order (the PCG's
+// stored-coefficient matvec)
 template <class R>
-__global__ void k_pack_u(int n, const double* __restrict__ ud, const double* __restrict__ up, R4<R>* __restrict__ u4) {
+__global__ void k_pack_u(int n, const double* __restrict__ ud, const double* __restrict__ up, R4<R>* __restrict__ u4,
+                         const int* __restrict__ rank = nullptr) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    u4[2 * i] = make_r4<R>((R)ud[3 * i], (R)ud[3 * i + 1], (R)ud[3 * i + 2], R(0));
-    u4[2 * i + 1] = make_r4<R>((R)up[3 * i], (R)up[3 * i + 1], (R)up[3 * i + 2], R(0));
+    const int o = rank ? rank[i] : i;
+    u4[2 * o] = make_r4<R>((R)ud[3 * i], (R)ud[3 * i + 1], (R)ud[3 * i + 2], R(0));
+    u4[2 * o + 1] = make_r4<R>((R)up[3 * i], (R)up[3 * i + 1], (R)up[3 * i + 2], R(0));
 }
 
 // A v = v/alpha - (real + recip + self) field of v, both sets; pol = 0 sites
@@ -75,7 +79,8 @@ __global__ void k_pcg_init(int n, const double* __restrict__ Ed, const double* _
                            const double* __restrict__ Aud, const double* __restrict__ Aup,
                            const double* __restrict__ pol, double* __restrict__ rd, double* __restrict__ rp,
                            double* __restrict__ zd, double* __restrict__ zp, double* __restrict__ pd,
-                           double* __restrict__ pp, double* __restrict__ scal, R4<R>* __restrict__ s4) {
+                           double* __restrict__ pp, double* __restrict__ scal, R4<R>* __restrict__ s4,
+                           const int* __restrict__ rank) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double rzd = 0, rzp = 0, rrd = 0, rrp = 0;
     if (i < n) {
@@ -95,8 +100,8 @@ __global__ void k_pcg_init(int n, const double* __restrict__ Ed, const double* _
             rrd += r1 * r1; rrp += r2 * r2;
         }
         if (s4) {
-            s4[2 * i] = make_r4<R>((R)sv[0], (R)sv[1], (R)sv[2], R(0));
-            s4[2 * i + 1] = make_r4<R>((R)sv[3], (R)sv[4], (R)sv[5], R(0));
+            s4[2 * rank[i]] = make_r4<R>((R)sv[0], (R)sv[1], (R)sv[2], R(0));
+            s4[2 * rank[i] + 1] = make_r4<R>((R)sv[3], (R)sv[4], (R)sv[5], R(0));
         }
     }
     if (!s4) {
@@ -125,7 +130,8 @@ __global__ void k_pcg_update(int n, const double* __restrict__ pol, const double
                              const double* __restrict__ pp, const double* __restrict__ Apd,
                              const double* __restrict__ App, double* __restrict__ ud, double* __restrict__ up,
                              double* __restrict__ rd, double* __restrict__ rp, double* __restrict__ zd,
-                             double* __restrict__ zp, double* __restrict__ scal, R4<R>* __restrict__ s4) {
+                             double* __restrict__ zp, double* __restrict__ scal, R4<R>* __restrict__ s4,
+                             const int* __restrict__ rank) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double ad = scal[PAP_D] != 0 ? scal[RZ_D] / scal[PAP_D] : 0.0;
     double ap = scal[PAP_P] != 0 ? scal[RZ_P] / scal[PAP_P] : 0.0;
@@ -148,8 +154,8 @@ __global__ void k_pcg_update(int n, const double* __restrict__ pol, const double
             rrd += r1 * r1; rrp += r2 * r2;
         }
         if (s4) {
-            s4[2 * i] = make_r4<R>((R)sv[0], (R)sv[1], (R)sv[2], R(0));
-            s4[2 * i + 1] = make_r4<R>((R)sv[3], (R)sv[4], (R)sv[5], R(0));
+            s4[2 * rank[i]] = make_r4<R>((R)sv[0], (R)sv[1], (R)sv[2], R(0));
+            s4[2 * rank[i] + 1] = make_r4<R>((R)sv[3], (R)sv[4], (R)sv[5], R(0));
         }
     }
     if (!s4) {
@@ -170,7 +176,7 @@ __device__ __forceinline__ void pcg_beta(const double* __restrict__ scal, double
 template <class R>
 __global__ void k_pcg_dir(int n, const double* __restrict__ zd, const double* __restrict__ zp,
                           double* __restrict__ pd, double* __restrict__ pp, const double* __restrict__ scal,
-                          R4<R>* __restrict__ p4) {
+                          R4<R>* __restrict__ p4, const int* __restrict__ rank) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double bd, bp;
@@ -183,26 +189,28 @@ __global__ void k_pcg_dir(int n, const double* __restrict__ zd, const double* __
         pd[q] = a[c];
         pp[q] = b[c];
     }
-    p4[2 * i] = make_r4<R>((R)a[0], (R)a[1], (R)a[2], R(0));
-    p4[2 * i + 1] = make_r4<R>((R)b[0], (R)b[1], (R)b[2], R(0));
+    p4[2 * rank[i]] = make_r4<R>((R)a[0], (R)a[1], (R)a[2], R(0));
+    p4[2 * rank[i] + 1] = make_r4<R>((R)b[0], (R)b[1], (R)b[2], R(0));
 }
 
 // p = z + beta p (after the control decision) fused with the spreading of
-// p into the complex grid zg for the next matvec: a block of 128 threads takes
-// kLineSites sites; threads 0..6 kLineSites - 1 form p (and its R4 copy), then
-// each thread t < kLineSites P^2 adds one z-line of one site (as
-// k_spread_dipoles; zg holds the cleared grid left by the previous
-// transform).
+// p into the complex grid zg for the next matvec (zg holds the cleared grid
+// left by the previous transform), in the layout of k_spread_dipoles: FP32,
+// kLineSites sites per block of 128 threads and one z-line per thread; FP64,
+// one site per block and one stencil point per thread.  The first 6 threads
+// per site form p (and its R4 copy).
 template <class R, int P>
 __global__ void __launch_bounds__(128) k_pcg_dir_spread(int n, const double* __restrict__ zd,
                                                         const double* __restrict__ zp, double* __restrict__ pd,
                                                         double* __restrict__ pp, const double* __restrict__ scal,
                                                         R4<R>* __restrict__ p4, const R* __restrict__ theta,
                                                         const int* __restrict__ k0, int3 K, Frac F,
-                                                        typename Cplx<R>::type* __restrict__ zg) {
-    __shared__ double pv[kLineSites][6];
-    const int t = threadIdx.x, i0 = blockIdx.x * kLineSites;
-    if (t < 6 * kLineSites) {
+                                                        typename Cplx<R>::type* __restrict__ zg,
+                                                        const int* __restrict__ rank) {
+    constexpr int SPB = sizeof(R) == 8 ? 1 : kLineSites;  // sites per block
+    __shared__ double pv[SPB][6];
+    const int t = threadIdx.x, i0 = blockIdx.x * SPB;
+    if (t < 6 * SPB) {
         const int s = t / 6, k = t % 6, i = i0 + s;
         if (i < n) {
             double bd, bp;
@@ -214,14 +222,20 @@ __global__ void __launch_bounds__(128) k_pcg_dir_spread(int n, const double* __r
         }
     }
     __syncthreads();
-    if (t < kLineSites && i0 + t < n) {
+    if (t < SPB && i0 + t < n) {
         const double* v = pv[t];
-        p4[2 * (i0 + t)] = make_r4<R>((R)v[0], (R)v[1], (R)v[2], R(0));
-        p4[2 * (i0 + t) + 1] = make_r4<R>((R)v[3], (R)v[4], (R)v[5], R(0));
+        const int o = rank[i0 + t];  // p4 in cell order
+        p4[2 * o] = make_r4<R>((R)v[0], (R)v[1], (R)v[2], R(0));
+        p4[2 * o + 1] = make_r4<R>((R)v[3], (R)v[4], (R)v[5], R(0));
     }
-    const int s = t / (P * P), i = i0 + s;
-    if (t >= kLineSites * P * P || i >= n) return;
-    spread_site_line<R, P>(i, t % (P * P), pv[s], pv[s] + 3, theta, k0, K, F, zg);
+    if constexpr (SPB == 1) {
+        if (t >= P * P * P || i0 >= n) return;
+        spread_site_point<R, P>(i0, t, pv[0], pv[0] + 3, theta, k0, K, F, zg);
+    } else {
+        const int s = t / (P * P), i = i0 + s;
+        if (t >= SPB * P * P || i >= n) return;
+        spread_site_line<R, P>(i, t % (P * P), pv[s], pv[s] + 3, theta, k0, K, F, zg);
+    }
 }
 
 // One preconditioned correction step u += alpha r with the FP64 residual

@@ -24,6 +24,7 @@ __global__ void __launch_bounds__(128) k_perm_field(int n, const int* __restrict
                                                     const int* __restrict__ nbr, int cap,
                                                     const int* __restrict__ nnb, double* __restrict__ Ed,
                                                     double* __restrict__ Ep, R4<R>* __restrict__ c0,
+                                                    const int* __restrict__ rank, int* __restrict__ cnb,
                                                     R usolv2, int* __restrict__ nbru, R4<R>* __restrict__ cu0,
                                                     int* __restrict__ nnbu) {
     const int g = (blockIdx.x * blockDim.x + threadIdx.x) / LPA, lane = threadIdx.x % LPA;
@@ -54,6 +55,7 @@ __global__ void __launch_bounds__(128) k_perm_field(int n, const int* __restrict
             if (COEF) {
                 bulk_radial_prec<R, EWALD>(r2, aewald, pdi * Aj.e.y, pair_thole<R>(thi, Aj.e.z), B, P1, P2);
                 c0[base + s] = pack_tensor<R>(r.x, r.y, r.z, B[1], B[2]);
+                cnb[base + s] = rank[j];
             } else {
                 bulk_radial<R, EWALD, true>(r2, aewald, pdi * Aj.e.y, pair_thole<R>(thi, Aj.e.z), B);
             }
@@ -65,7 +67,7 @@ __global__ void __launch_bounds__(128) k_perm_field(int n, const int* __restrict
             const unsigned b = __ballot_sync(gmask, take) & gmask;
             if (take) {
                 const size_t q = base + nu + __popc(b & below);
-                nbru[q] = j;
+                nbru[q] = rank[j];
                 cu0[q] = pack_tensor<R>(r.x, r.y, r.z, P1, P2);
             }
             nu += __popc(b);
@@ -255,14 +257,18 @@ __global__ void __launch_bounds__(128) k_polar_pair(int n, const int* __restrict
 // ------------------------------------------------------------ stored T
 // The dipole interaction tensor does not change during the PCG solve, so its
 // pair coefficients are computed once per evaluation and streamed by every
-// matvec: per slot one packed R4 (pack_tensor of r = x_i - x_j, B1, B2); the
-// neighbour index is the list entry itself.  Rows hold the bulk neighbours followed by
-// the scaled partners (filled by k_scaled_coeffs), so one kernel applies the
-// whole real-space T.
+// matvec: per slot one packed R4 (pack_tensor of r = x_i - x_j, B1, B2) and
+// the neighbour's position in cell order (cnb, rank[j]).  Rows hold the bulk
+// neighbours followed by the scaled partners (filled by k_scaled_coeffs), so
+// one kernel applies the whole real-space T.  The PCG's R4 vectors (u4 of the
+// first matvec, p4, s4) are stored in cell order too: the neighbours of the
+// sites a warp handles then lie in a few contiguous runs of those vectors,
+// which the gathers read as whole cache lines, mostly from L1.
 template <class R, bool EWALD, int LPA, bool CELLS = false>
 __global__ void __launch_bounds__(128) k_tu_coeffs(int n, const int* __restrict__ order, const AtomR<R>* __restrict__ at, Box bx, R aewald,
                                                    const int* __restrict__ nbr, int cap, const int* __restrict__ nnb,
-                                                   R4<R>* __restrict__ c0, R usolv2, int* __restrict__ nbru,
+                                                   R4<R>* __restrict__ c0, const int* __restrict__ rank,
+                                                   int* __restrict__ cnb, R usolv2, int* __restrict__ nbru,
                                                    R4<R>* __restrict__ cu0, int* __restrict__ nnbu) {
     const int g = (blockIdx.x * blockDim.x + threadIdx.x) / LPA, lane = threadIdx.x % LPA;
     if (g >= n) return;  // whole lane groups leave together
@@ -307,13 +313,14 @@ __global__ void __launch_bounds__(128) k_tu_coeffs(int n, const int* __restrict_
                 P2 -= (R(1) + x) * e * b2;
             }
             c0[base + s] = pack_tensor<R>(r.x, r.y, r.z, B1, B2);
+            cnb[base + s] = rank[j];
         }
         if (cu0) {  // sparse preconditioner: bare Thole-damped T within usolvcut, compacted in order
             const bool take = ok && r2 <= usolv2;
             const unsigned b = __ballot_sync(gmask, take) & gmask;
             if (take) {
                 const size_t q = base + nu + __popc(b & below);
-                nbru[q] = j;
+                nbru[q] = rank[j];
                 cu0[q] = pack_tensor<R>(r.x, r.y, r.z, P1, P2);
             }
             nu += __popc(b);
@@ -323,15 +330,15 @@ __global__ void __launch_bounds__(128) k_tu_coeffs(int n, const int* __restrict_
 }
 
 // T v with the stored coefficients (both dipole sets): rows of nnb[i] bulk
-// slots plus the site's scaled partners.  u4: [n][2] R4.
+// slots plus the site's scaled partners.  u4: [n][2] R4 in cell order.
 template <class R, int LPA>
-__global__ void __launch_bounds__(128) k_tu_stored(int n, const int* __restrict__ order, const int* __restrict__ nbr,
+__global__ void __launch_bounds__(128) k_tu_stored(int n, const int* __restrict__ order, const int* __restrict__ cnb,
                                                    const R4<R>* __restrict__ c0, int cap,
                                                    const int* __restrict__ nnb, const int* __restrict__ xoff,
                                                    const R4<R>* __restrict__ u4, double* __restrict__ Fd,
                                                    double* __restrict__ Fp) {
     const int g = (blockIdx.x * blockDim.x + threadIdx.x) / LPA, lane = threadIdx.x % LPA;
-    const int i = order[min(g, n - 1)];
+    const int gs = min(g, n - 1), i = order[gs];  // gs: the site's position in cell order
     const int cnt = g < n ? nnb[i] + (xoff[i + 1] - xoff[i]) : 0;
     const size_t base = (size_t)i * cap;
     R ax = 0, ay = 0, az = 0, bx_ = 0, by = 0, bz = 0;
@@ -345,7 +352,7 @@ __global__ void __launch_bounds__(128) k_tu_stored(int n, const int* __restrict_
         for (int q = 0; q < U; q++) {
             const int s = s0 + q * LPA;
             const bool ok = s < cnt;
-            j[q] = ok ? nbr[base + s] : i;
+            j[q] = ok ? cnb[base + s] : gs;
             c[q] = ok ? c0[base + s] : make_r4<R>(0, 0, 0, 0);
         }
         R4<R> ud[U], up[U];
@@ -477,7 +484,8 @@ template <class R>
 __global__ void k_scaled_coeffs(int np, const ScaledPair* __restrict__ sp, const double* __restrict__ xyz,
                                 const double* __restrict__ pdamp, const double* __restrict__ thole, Box bx,
                                 double cut2, double aewald, const int* __restrict__ nnb, int cap,
-                                int* __restrict__ nbr, R4<R>* __restrict__ c0, double usolv2,
+                                const int* __restrict__ rank, int* __restrict__ cnb, R4<R>* __restrict__ c0,
+                                double usolv2,
                                 const int* __restrict__ nnbu, int* __restrict__ nbru, R4<R>* __restrict__ cu0) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= np) return;
@@ -488,8 +496,8 @@ __global__ void k_scaled_coeffs(int np, const ScaledPair* __restrict__ sp, const
     V3<double> r = G.inside ? G.r : v3<double>(0, 0, 0);
     size_t si = (size_t)P.i * cap + nnb[P.i] + P.si;
     size_t sk = (size_t)P.k * cap + nnb[P.k] + P.sk;
-    nbr[si] = P.k;
-    nbr[sk] = P.i;
+    cnb[si] = rank[P.k];
+    cnb[sk] = rank[P.i];
     c0[si] = pack_tensor<R>((R)(-r.x), (R)(-r.y), (R)(-r.z), (R)B[1], (R)B[2]);   // x_i - x_k
     c0[sk] = pack_tensor<R>((R)r.x, (R)r.y, (R)r.z, (R)B[1], (R)B[2]);
     if (cu0) {  // preconditioner slots after the row's compacted bulk entries; zero beyond usolvcut
@@ -498,17 +506,18 @@ __global__ void k_scaled_coeffs(int np, const ScaledPair* __restrict__ sp, const
         if (in) scaled_radial(G, P.u, true, false, U);
         size_t ui = (size_t)P.i * cap + nnbu[P.i] + P.si;
         size_t uk = (size_t)P.k * cap + nnbu[P.k] + P.sk;
-        nbru[ui] = P.k;
-        nbru[uk] = P.i;
+        nbru[ui] = rank[P.k];
+        nbru[uk] = rank[P.i];
         cu0[ui] = pack_tensor<R>((R)(-r.x), (R)(-r.y), (R)(-r.z), (R)U[1], (R)U[2]);
         cu0[uk] = pack_tensor<R>((R)r.x, (R)r.y, (R)r.z, (R)U[1], (R)U[2]);
     }
 }
 
 // Sparse preconditioner z = M r for both residuals:
-//   z_i = alpha_i (w r_i + sum_j T_ij s_j),  s = alpha r  (packed in s4),
-// T over the rows built by k_tu_coeffs / k_scaled_coeffs (bulk pairs within
-// usolvcut, then the scaled partners).  Adds r.z of both sets to
+//   z_i = alpha_i (w r_i + sum_j T_ij s_j),  s = alpha r  (packed in s4,
+// cell order), T over the rows built by k_tu_coeffs / k_scaled_coeffs (bulk
+// pairs within usolvcut, then the scaled partners; nbru holds the partners'
+// positions in cell order).  Adds r.z of both sets to
 // rz_out[0], rz_out[1]; FIRST also starts the directions p = z.  Blocks
 // stride over the sites (a grid of a few blocks per SM), so each block adds
 // its r.z once; with `done`, the last block then takes the PCG control
@@ -529,7 +538,7 @@ __global__ void __launch_bounds__(128) k_precond(int n, const int* __restrict__ 
     double rzd = 0, rzp = 0;
     for (int g0 = blockIdx.x * per_block; g0 < n; g0 += gridDim.x * per_block) {
         const int g = g0 + threadIdx.x / LPA;
-        const int i = order[min(g, n - 1)];
+        const int gs = min(g, n - 1), i = order[gs];  // gs: the site's position in cell order
         const int cnt = g < n ? nnbu[i] + (xoff[i + 1] - xoff[i]) : 0;
         const size_t base = (size_t)i * cap;
         R ax = 0, ay = 0, az = 0, bx_ = 0, by = 0, bz = 0;
@@ -541,7 +550,7 @@ __global__ void __launch_bounds__(128) k_precond(int n, const int* __restrict__ 
             for (int q = 0; q < U; q++) {
                 const int s = s0 + q * LPA;
                 const bool ok = s < cnt;
-                j[q] = ok ? nbru[base + s] : i;
+                j[q] = ok ? nbru[base + s] : gs;
                 c[q] = ok ? cu0[base + s] : make_r4<R>(0, 0, 0, 0);
             }
             R4<R> vd[U], vp[U];
@@ -584,8 +593,8 @@ __global__ void __launch_bounds__(128) k_precond(int n, const int* __restrict__ 
                     const double rv = k < 3 ? rd[3 * i + k] : rp[3 * i + k - 3];
                     z[k] = a > 0 ? a * (wdiag * rv + S[k]) : 0.0;
                 }
-                p4[2 * i] = make_r4<R>((R)z[0], (R)z[1], (R)z[2], R(0));
-                p4[2 * i + 1] = make_r4<R>((R)z[3], (R)z[4], (R)z[5], R(0));
+                p4[2 * gs] = make_r4<R>((R)z[0], (R)z[1], (R)z[2], R(0));
+                p4[2 * gs + 1] = make_r4<R>((R)z[3], (R)z[4], (R)z[5], R(0));
             }
         }
     }

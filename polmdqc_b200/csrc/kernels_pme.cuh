@@ -182,6 +182,28 @@ __device__ __forceinline__ void add_line(typename Cplx<R>::type* line, int c0, i
     }
 }
 
+// spread stencil point t = (a, b, c) = (t / P^2, t / P % P, t % P) of site i
+// (FP64, where one point per thread measured faster than whole lines: without
+// vector atomics a line is P dependent pairs of atomics in one thread)
+template <class R, int P>
+__device__ __forceinline__ void spread_site_point(int i, int t, const double* pd, const double* pq,
+                                                  const R* __restrict__ theta, const int* __restrict__ k0, int3 K,
+                                                  const Frac& F, typename Cplx<R>::type* __restrict__ zg) {
+    const int a = t / (P * P), b = (t / P) % P, c = t % P;
+    const R* th = theta + (size_t)i * 3 * 4 * P;
+    const R t0 = th[a], t1 = th[P + a];
+    const R u0 = th[4 * P + b], u1 = th[5 * P + b];
+    const R v0 = th[8 * P + c], v1 = th[9 * P + c];
+    R d0, d1, d2, p0, p1, p2;
+    frac_dipole<R>(F, pd[0], pd[1], pd[2], d0, d1, d2);
+    frac_dipole<R>(F, pq[0], pq[1], pq[2], p0, p1, p2);
+    const R w100 = t1 * u0 * v0, w010 = t0 * u1 * v0, w001 = t0 * u0 * v1;
+    int ga = k0[3 * i] + a; if (ga >= K.x) ga -= K.x;
+    int gb = k0[3 * i + 1] + b; if (gb >= K.y) gb -= K.y;
+    int gc = k0[3 * i + 2] + c; if (gc >= K.z) gc -= K.z;
+    add_cplx<R>(zg + gidx(ga, gb, gc, K), d0 * w100 + d1 * w010 + d2 * w001, p0 * w100 + p1 * w010 + p2 * w001);
+}
+
 // spread the line (a, b) of site i with Cartesian dipoles pd (d set) and pq
 // (p set), converted to fractional dipoles here
 template <class R, int P>
@@ -220,10 +242,22 @@ __global__ void __launch_bounds__(128) k_spread_dipoles(int n, const int* __rest
                                                         typename Cplx<R>::type* __restrict__ zg) {
     static_assert(kLineSites * P * P <= 128, "lines of a block");
     const int t = threadIdx.x;
-    const int g = blockIdx.x * kLineSites + t / (P * P);
-    if (t >= kLineSites * P * P || g >= n) return;
-    const int i = order[g];
-    spread_site_line<R, P>(i, t % (P * P), ud + 3 * i, up + 3 * i, theta, k0, K, F, zg);
+    if constexpr (sizeof(R) == 8) {  // FP64: one site per block, one stencil point per thread
+        if (t >= P * P * P) return;
+        const int i = order[blockIdx.x];
+        spread_site_point<R, P>(i, t, ud + 3 * i, up + 3 * i, theta, k0, K, F, zg);
+    } else {
+        const int g = blockIdx.x * kLineSites + t / (P * P);
+        if (t >= kLineSites * P * P || g >= n) return;
+        const int i = order[g];
+        spread_site_line<R, P>(i, t % (P * P), ud + 3 * i, up + 3 * i, theta, k0, K, F, zg);
+    }
+}
+
+// blocks of k_spread_dipoles / k_pcg_dir_spread for n sites
+template <class R>
+inline unsigned spread_blocks(int n) {
+    return sizeof(R) == 8 ? (unsigned)n : (unsigned)((n + kLineSites - 1) / kLineSites);
 }
 
 // Gather of the field of two dipole potential grids (interleaved as the

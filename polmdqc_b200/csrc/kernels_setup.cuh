@@ -143,10 +143,11 @@ __global__ void k_cell_index(int n, const double* __restrict__ xyz, CellGrid cg,
     ids[i] = i;
 }
 
-// cell start/end of the sorted keys, and the coordinates in cell order
+// cell start/end of the sorted keys, the coordinates in cell order and each
+// site's position in that order (rank, the inverse of sids)
 __global__ void k_cell_bounds(int n, const unsigned* __restrict__ skeys, const int* __restrict__ sids,
                               const double* __restrict__ xyz, int* __restrict__ start, int* __restrict__ end,
-                              double4* __restrict__ spos) {
+                              double4* __restrict__ spos, int* __restrict__ rank) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     unsigned k = skeys[i];
@@ -154,6 +155,7 @@ __global__ void k_cell_bounds(int n, const unsigned* __restrict__ skeys, const i
     if (i == n - 1 || skeys[i + 1] != k) end[k] = i + 1;
     int a = sids[i];
     spos[i] = make_double4(xyz[3 * a], xyz[3 * a + 1], xyz[3 * a + 2], 0.0);
+    rank[a] = i;
 }
 
 // Exact neighbour list: all j != i with minimum-image |r| <= cutoff, decided

@@ -92,17 +92,23 @@ def test_water_dimer_testgrad_golden():
     np.testing.assert_allclose(r.dem.reshape(-1), g["amoeba2"]["dem"], atol=g["amoeba2"]["eps1"], rtol=0)
 
 
-@pytest.mark.parametrize("case,name", [("rotpole2", "benzene_ethyne_water.xyz"), ("rotpole3", "ammonia.xyz")])
-def test_frames_rotated_multipoles_and_torques(case, name):
+@pytest.mark.parametrize("case,name,fd_tol", [("rotpole2", "benzene_ethyne_water.xyz", 1e-6),
+                                              ("rotpole3", "ammonia.xyz", 1e-4)])
+def test_frames_rotated_multipoles_and_torques(case, name, fd_tol):
     """rotpole-2 (Z-Only) and rotpole-3 (Z-Bisect, 3-Fold): the GPU's rotated
-    multipoles against the reference's golden at 1e-14.  These HIPPO inputs'
-    energies include charge penetration, which this library does not model,
-    so the torques of these frames are checked without it: dem against the
-    oracle at 1e-9 and against central differences (step 1e-5 A) of the GPU's
-    own FP64 energies at 1e-6, for every atom."""
+    multipoles against the reference's golden at 1e-14; then, with the charge
+    penetration of these HIPPO inputs switched off so that only the frames and
+    torques are under test, dem against the oracle at 1e-9 and against central
+    differences (step 1e-5 A) of the GPU's own FP64 energies for every atom.
+    The reference's torque for Z-Bisect and 3-Fold sites is not the exact
+    derivative of its energy (the oracle, which restates it, differs from its
+    own finite differences by 4e-5 on ammonia, and the reference's testgrad
+    run of ammonia, rotpole-6, allows 1e-4); those frames are held to that
+    tolerance, Z-Only to 1e-6."""
+    import dataclasses
     g = golden("ref_tests.json")[case]
     d = ref_dump(ref_fixture("rotpole", name))
-    s = systems.from_dump(d)
+    s = dataclasses.replace(systems.from_dump(d), pentype=0)
     cut = d["mpolecut"]
     st = Settings(use_ewald=False, cutoff=cut, poltyp=abi.POL_NONE, precision=FP64)
     e = Engine(s, st)
@@ -122,7 +128,7 @@ def test_frames_rotated_multipoles_and_torques(case, name):
                 x[i, a] -= 2 * h
                 e.set_coords(x)
                 m = e.forward(abi.DO_ENERGY).em
-                assert abs((p - m) / (2 * h) - r.dem[i, a]) < 1e-6, (i, a)
+                assert abs((p - m) / (2 * h) - r.dem[i, a]) < fd_tol, (i, a)
     finally:
         e.close()
 

@@ -140,6 +140,7 @@ struct amg_ctx {
     int* nnb = nullptr;
     int* rank = nullptr;  // position of each site in cell order (inverse of sids)
     int* cnb = nullptr;   // [n][cap] cell-order positions of the PCG coefficient rows' neighbours
+    double2* sdt = nullptr;  // (pdamp, thole) in cell order, for the FP64 sweep
     int cap = 0, lpa = 16, num_sms = 148;
     int* overflow = nullptr;
     // sparse PCG preconditioner (pcgprec): rows of the pairs within usolvcut,
@@ -625,6 +626,7 @@ void ensure_list_buffers(amg_ctx* ctx) {
         dalloc(ctx, ctx->overflow, 1);
         dalloc(ctx, ctx->spos, n);
         dalloc(ctx, ctx->rank, n);
+        dalloc(ctx, ctx->sdt, n);
         size_t bytes = 0;
         cub::DeviceRadixSort::SortPairs(nullptr, bytes, ctx->keys, ctx->skeys, ctx->ids, ctx->sids, n);
         dalloc(ctx, ctx->cubtmp, bytes);
@@ -665,7 +667,8 @@ void enqueue_lists(amg_ctx* ctx, cudaStream_t s) {
     size_t bytes = ctx->cubtmp_bytes;
     CK(cub::DeviceRadixSort::SortPairs(ctx->cubtmp, bytes, ctx->keys, ctx->skeys, ctx->ids, ctx->sids, n, 0, nbits, s));
     k_cell_bounds<<<nblk(n), kThreads, 0, s>>>(n, ctx->skeys, ctx->sids, ctx->xyz, ctx->cstart, ctx->cend, ctx->spos,
-                                               ctx->rank);
+                                               ctx->rank, ctx->pdamp, ctx->thole,
+                                               ctx->has_pol ? ctx->sdt : nullptr);
     KCHECK();
     const double cut2 = ctx->cut * ctx->cut;
     if (!cg.periodic || (cg.nc[0] >= 3 && cg.nc[1] >= 3 && cg.nc[2] >= 3)) {
@@ -803,16 +806,37 @@ double self_coef(const amg_ctx* ctx) {
 bool ewald_cells(const amg_ctx* ctx) { return ctx->ewald && ctx->bx.shape != 0; }
 
 // A v for both dipole sets (v/alpha - field of v), pair tensors computed on
-// the fly (FP64 correction sweep)
+// the fly (FP64 correction sweep, OPT orders).  `cells` (the sweep, which
+// follows a solve and so has the cell-order partner rows cnb): the FP64
+// real-space part gathers from cell-order copies (k_Tu_cells).
 template <class R>
-void matvec(amg_ctx* ctx, cudaStream_t s, const double* vd, const double* vp, double* Ad, double* Ap) {
+void matvec(amg_ctx* ctx, cudaStream_t s, const double* vd, const double* vp, double* Ad, double* Ap,
+            bool cells = false) {
     const int n = ctx->n;
     Atoms<R>& A = atoms_of<R>(ctx);
-    k_pack_u<R><<<nblk(n), kThreads, 0, s>>>(n, vd, vp, A.u4);
+    k_pack_u<R><<<nblk(n), kThreads, 0, s>>>(n, vd, vp, A.u4, cells ? ctx->rank : nullptr);
     KCHECK();
     // real space on the side stream, PME on s
     cudaStream_t r = ctx->ewald ? fork_side(ctx, s) : s;
-    LPA_DISPATCH(ctx->lpa, {
+    if constexpr (sizeof(R) == 8) {
+        if (cells) {
+            LPA_DISPATCH(ctx->lpa, {
+                if (ewald_cells(ctx))
+                    k_Tu_cells<true, 8, true><<<nblk((size_t)n * 8), kThreads, 0, r>>>(
+                        n, ctx->sids, ctx->spos, ctx->sdt, A.u4, ctx->bx, ctx->aewald, ctx->cnb, ctx->cap, ctx->nnb,
+                        ctx->Fd, ctx->Fp);
+                else if (ctx->ewald)
+                    k_Tu_cells<true, L><<<nblk((size_t)n * L), kThreads, 0, r>>>(
+                        n, ctx->sids, ctx->spos, ctx->sdt, A.u4, ctx->bx, ctx->aewald, ctx->cnb, ctx->cap, ctx->nnb,
+                        ctx->Fd, ctx->Fp);
+                else
+                    k_Tu_cells<false, L><<<nblk((size_t)n * L), kThreads, 0, r>>>(
+                        n, ctx->sids, ctx->spos, ctx->sdt, A.u4, ctx->bx, 0.0, ctx->cnb, ctx->cap, ctx->nnb, ctx->Fd,
+                        ctx->Fp);
+            });
+        }
+    }
+    if (!(cells && sizeof(R) == 8)) LPA_DISPATCH(ctx->lpa, {
         if (ewald_cells(ctx))
             k_Tu<R, true, 8, true><<<nblk((size_t)n * 8), kThreads, 0, r>>>(n, ctx->sids, A.at, A.u4, ctx->bx, (R)ctx->aewald,
                                                                             ctx->nbr, ctx->cap, ctx->nnb, ctx->Fd, ctx->Fp);
@@ -1032,7 +1056,7 @@ void enqueue_pcg_iter(amg_ctx* ctx, cudaStream_t s, cudaGraphConditionalHandle h
 // FP64 correction sweep: the true residual with every term in FP64, one
 // diagonal-preconditioned step u += alpha r, and the residual norms
 void enqueue_sweep(amg_ctx* ctx, cudaStream_t s) {
-    matvec<double>(ctx, s, ctx->ud, ctx->up, ctx->Apd, ctx->App);
+    matvec<double>(ctx, s, ctx->ud, ctx->up, ctx->Apd, ctx->App, true);
     k_zero<double><<<1, 32, 0, s>>>(ctx->scal + PAP_D, 6);
     KCHECK();
     k_correct<<<nblk(ctx->n), kThreads, 0, s>>>(ctx->n, ctx->Ed, ctx->Ep, ctx->Apd, ctx->App, ctx->pol, ctx->ud, ctx->up,
@@ -1594,6 +1618,7 @@ void release(amg_ctx* ctx) {
     dfree(ctx->skeys);
     dfree(ctx->rank);
     dfree(ctx->cnb);
+    dfree(ctx->sdt);
     dfree(ctx->spos);
     dfree(ctx->cnt);
     dfree(ctx->sp);

@@ -137,6 +137,60 @@ __global__ void __launch_bounds__(128) k_Tu(int n, const int* __restrict__ order
     }
 }
 
+// The same T u in FP64 with every gathered array in cell order (the FP64
+// correction sweep): positions spos (x, y, z), damping sdt (pdamp, thole), the
+// dipoles u4 [2n] and the rows' partners cnb (positions in cell order, bulk
+// slots only), so the gathers of a warp's sites read contiguous runs.
+template <bool EWALD, int LPA, bool CELLS = false>
+__global__ void __launch_bounds__(128) k_Tu_cells(int n, const int* __restrict__ order,
+                                                  const double4* __restrict__ spos, const double2* __restrict__ sdt,
+                                                  const double4* __restrict__ u4, Box bx, double aewald,
+                                                  const int* __restrict__ cnb, int cap, const int* __restrict__ nnb,
+                                                  double* __restrict__ Fd, double* __restrict__ Fp) {
+    const int g = (blockIdx.x * blockDim.x + threadIdx.x) / LPA, lane = threadIdx.x % LPA;
+    const int gs = min(g, n - 1), i = order[gs];
+    const int cnt = g < n ? nnb[i] : 0;
+    const double4 pi = spos[gs];
+    const double2 di = sdt[gs];
+    const V3<double> xi = v3<double>(pi.x, pi.y, pi.z);
+    double ax = 0, ay = 0, az = 0, bx_ = 0, by = 0, bz = 0;
+    const int* row = cnb + (size_t)i * cap;
+    for (int s = lane; s < cnt; s += LPA) {
+        const int j = row[s];
+        const double4 pj = spos[j];
+        const double2 dj = sdt[j];
+        const V3<double> r = min_image<double, !EWALD || CELLS>(xi - v3<double>(pj.x, pj.y, pj.z), bx);
+        const double r2 = dot(r, r), rinv = rsqrt(r2), rr = r2 * rinv, rinv2 = rinv * rinv;
+        const double b1 = rinv * rinv2, b2 = 3 * b1 * rinv2;
+        double B1 = b1, B2 = b2;
+        if (EWALD) {
+            double eb[3];
+            ewald_terms<double, 3>(rr, rinv2, aewald, eb);
+            B1 = eb[1];
+            B2 = eb[2];
+        }
+        const double damp = di.x * dj.x;
+        if (damp != 0.0) {
+            const double t = rr / damp;
+            const double x = pair_thole<double>(di.y, dj.y) * t * t * t;
+            const double e = exp(-x);
+            B1 -= e * b1;                 // (1 - lambda3) = e
+            B2 -= (1.0 + x) * e * b2;     // (1 - lambda5) = (1 + x) e
+        }
+        const double4 ud = u4[2 * j], up = u4[2 * j + 1];
+        const double ad = (ud.x * r.x + ud.y * r.y + ud.z * r.z) * B2;
+        const double ap = (up.x * r.x + up.y * r.y + up.z * r.z) * B2;
+        ax += ad * r.x - B1 * ud.x; ay += ad * r.y - B1 * ud.y; az += ad * r.z - B1 * ud.z;
+        bx_ += ap * r.x - B1 * up.x; by += ap * r.y - B1 * up.y; bz += ap * r.z - B1 * up.z;
+    }
+    ax = group_sum<LPA>(ax); ay = group_sum<LPA>(ay); az = group_sum<LPA>(az);
+    bx_ = group_sum<LPA>(bx_); by = group_sum<LPA>(by); bz = group_sum<LPA>(bz);
+    if (lane == 0 && g < n) {
+        Fd[3 * i] = ax; Fd[3 * i + 1] = ay; Fd[3 * i + 2] = az;
+        Fp[3 * i] = bx_; Fp[3 * i + 1] = by; Fp[3 * i + 2] = bz;
+    }
+}
+
 // Multipole energy (half of each directed pair), gradient and torque of site
 // i from all its neighbours (bulk, m-scale 1).  f = electric/dielec.
 // EXTRA: the outputs of the Analysis and Virial modes, each written when its

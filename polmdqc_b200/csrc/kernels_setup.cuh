@@ -144,10 +144,13 @@ __global__ void k_cell_index(int n, const double* __restrict__ xyz, CellGrid cg,
 }
 
 // cell start/end of the sorted keys, the coordinates in cell order and each
-// site's position in that order (rank, the inverse of sids)
+// site's position in that order (rank, the inverse of sids); with sdt, the
+// sites' (pdamp, thole) in cell order as well
 __global__ void k_cell_bounds(int n, const unsigned* __restrict__ skeys, const int* __restrict__ sids,
                               const double* __restrict__ xyz, int* __restrict__ start, int* __restrict__ end,
-                              double4* __restrict__ spos, int* __restrict__ rank) {
+                              double4* __restrict__ spos, int* __restrict__ rank,
+                              const double* __restrict__ pdamp, const double* __restrict__ thole,
+                              double2* __restrict__ sdt) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     unsigned k = skeys[i];
@@ -156,6 +159,7 @@ __global__ void k_cell_bounds(int n, const unsigned* __restrict__ skeys, const i
     int a = sids[i];
     spos[i] = make_double4(xyz[3 * a], xyz[3 * a + 1], xyz[3 * a + 2], 0.0);
     rank[a] = i;
+    if (sdt) sdt[i] = make_double2(pdamp[a], thole[a]);  // damping parameters in cell order
 }
 
 // Exact neighbour list: all j != i with minimum-image |r| <= cutoff, decided
@@ -164,12 +168,14 @@ __global__ void k_cell_bounds(int n, const unsigned* __restrict__ skeys, const i
 // the FP64 scaled-pair kernels evaluate.  One warp per site (sites taken in
 // cell order); the lanes scan a stencil cell together and compact the hits
 // with a ballot, so each list is in cell order, then index order.  Stored
-// site-major: nbr[i * cap + s].
+// site-major: nbr[i * cap + s] holds the partner, cnb[i * cap + s] its
+// position in cell order (the index the pair kernels gather with).
 __global__ void k_neighbors(int n, const double4* __restrict__ spos, const unsigned* __restrict__ skeys,
                             const int* __restrict__ sids, const int* __restrict__ cstart,
                             const int* __restrict__ cend, CellGrid cg, Box bx, double cut2, int cap,
                             const int* __restrict__ xoff, const int* __restrict__ xidx, const int2* __restrict__ xrange,
-                            int* __restrict__ nbr, int* __restrict__ nnb, int* __restrict__ overflow) {
+                            int* __restrict__ nbr, int* __restrict__ cnb, int* __restrict__ nnb,
+                            int* __restrict__ overflow) {
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (w >= n) return;  // whole warps exit together
     const int i = sids[w];
@@ -212,7 +218,10 @@ __global__ void k_neighbors(int n, const double4* __restrict__ spos, const unsig
                     unsigned m = __ballot_sync(0xffffffffu, hit);
                     if (hit) {
                         int pos = cnt + __popc(m & ((1u << lane) - 1u));
-                        if (pos < limit) row[pos] = j;
+                        if (pos < limit) {
+                            row[pos] = j;
+                            cnb[(size_t)i * cap + pos] = p;  // the partner's position in cell order
+                        }
                     }
                     cnt += __popc(m);
                 }
@@ -244,7 +253,8 @@ constexpr int kNbrThreads = 256;
 __global__ void __launch_bounds__(kNbrThreads) k_neighbors_cells(
     const double4* __restrict__ spos, const int* __restrict__ sids, const int* __restrict__ cstart,
     const int* __restrict__ cend, CellGrid cg, Box bx, double cut2, double margin, int cap,
-    const int* __restrict__ xoff, const int* __restrict__ xidx, const int2* __restrict__ xrange, int* __restrict__ nbr, int* __restrict__ nnb,
+    const int* __restrict__ xoff, const int* __restrict__ xidx, const int2* __restrict__ xrange, int* __restrict__ nbr,
+    int* __restrict__ cnb, int* __restrict__ nnb,
     int* __restrict__ overflow) {
     __shared__ float4 cpos[kNbrChunk];
     __shared__ int csrt[kNbrChunk];  // sorted index
@@ -395,7 +405,10 @@ __global__ void __launch_bounds__(kNbrThreads) k_neighbors_cells(
                     const unsigned m = __ballot_sync(0xffffffffu, hit);
                     if (hit) {
                         const int pos = cnt + __popc(m & below);
-                        if (pos < limit) row[pos] = j;
+                        if (pos < limit) {
+                            row[pos] = j;
+                            cnb[(size_t)i * cap + pos] = csrt[t];  // the partner's position in cell order
+                        }
                     }
                     cnt += __popc(m);
                 }

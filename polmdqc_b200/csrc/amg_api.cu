@@ -97,6 +97,7 @@ struct Pme {
 template <class R>
 struct Atoms {
     AtomR<R>* at = nullptr;
+    AtomR<R>* atS = nullptr;  // the same sites in cell order (gathered each evaluation after the sort)
     R4<R>* u4 = nullptr;  // [n][2] dipoles
     R4<R>* p4 = nullptr;  // [n][2] PCG directions
     R4<R>* s4 = nullptr;  // [n][2] alpha r, input of the sparse preconditioner
@@ -676,11 +677,11 @@ void enqueue_lists(amg_ctx* ctx, cudaStream_t s) {
         // FP64 decision within 1e-3 cut^2 of the cutoff
         k_neighbors_cells<<<(unsigned)ncell, kNbrThreads, 0, s>>>(ctx->spos, ctx->sids, ctx->cstart, ctx->cend, cg,
                                                                   ctx->bx, cut2, 1e-3 * cut2, ctx->cap, ctx->xoff,
-                                                                  ctx->xidx, ctx->xrange, ctx->nbr, ctx->nnb, ctx->overflow);
+                                                                  ctx->xidx, ctx->xrange, ctx->nbr, ctx->cnb, ctx->nnb, ctx->overflow);
     } else {
         k_neighbors<<<nblk((size_t)n * 32), kThreads, 0, s>>>(n, ctx->spos, ctx->skeys, ctx->sids, ctx->cstart,
                                                               ctx->cend, cg, ctx->bx, cut2, ctx->cap, ctx->xoff,
-                                                              ctx->xidx, ctx->xrange, ctx->nbr, ctx->nnb, ctx->overflow);
+                                                              ctx->xidx, ctx->xrange, ctx->nbr, ctx->cnb, ctx->nnb, ctx->overflow);
     }
     KCHECK();
 }
@@ -889,16 +890,16 @@ void build_tu_coeffs(amg_ctx* ctx, cudaStream_t s) {
     R4<R>* cu0 = sp ? A.cu0 : nullptr;
     LPA_DISPATCH(ctx->lpa, {
         if (ewald_cells(ctx))
-            k_tu_coeffs<R, true, 8, true><<<nblk((size_t)n * 8), kThreads, 0, s>>>(n, ctx->sids, A.at, ctx->bx, (R)ctx->aewald,
-                                                                                   ctx->nbr, ctx->cap, ctx->nnb, A.c0, ctx->rank, ctx->cnb,
+            k_tu_coeffs<R, true, 8, true><<<nblk((size_t)n * 8), kThreads, 0, s>>>(n, ctx->sids, A.atS, ctx->bx, (R)ctx->aewald,
+                                                                                   ctx->cnb, ctx->cap, ctx->nnb, A.c0,
                                                                                    (R)u2, nbru, cu0, nnbu);
         else if (ctx->ewald)
-            k_tu_coeffs<R, true, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(n, ctx->sids, A.at, ctx->bx, (R)ctx->aewald, ctx->nbr,
-                                                                             ctx->cap, ctx->nnb, A.c0, ctx->rank, ctx->cnb, (R)u2, nbru,
+            k_tu_coeffs<R, true, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(n, ctx->sids, A.atS, ctx->bx, (R)ctx->aewald, ctx->cnb,
+                                                                             ctx->cap, ctx->nnb, A.c0, (R)u2, nbru,
                                                                              cu0, nnbu);
         else
-            k_tu_coeffs<R, false, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(n, ctx->sids, A.at, ctx->bx, (R)0, ctx->nbr, ctx->cap,
-                                                                              ctx->nnb, A.c0, ctx->rank, ctx->cnb, (R)u2, nbru, cu0,
+            k_tu_coeffs<R, false, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(n, ctx->sids, A.atS, ctx->bx, (R)0, ctx->cnb, ctx->cap,
+                                                                              ctx->nnb, A.c0, (R)u2, nbru, cu0,
                                                                               nnbu);
     });
     KCHECK();
@@ -1088,6 +1089,8 @@ void enqueue_front(amg_ctx* ctx, cudaStream_t s) {
     // stencils and the reciprocal permanent potential on s
     cudaStream_t r = fork_side(ctx, s);
     enqueue_lists(ctx, r);
+    k_gather_atoms<R><<<nblk(n), kThreads, 0, r>>>(n, ctx->sids, atoms_of<R>(ctx).at, atoms_of<R>(ctx).atS);
+    KCHECK();
     if (ctx->ewald) {
         pme_stencils<R>(ctx, s);
         Pme<R>& pm = pme_of<R>(ctx);
@@ -1109,8 +1112,8 @@ void enqueue_front(amg_ctx* ctx, cudaStream_t s) {
         const bool sp = coef && ctx->sparse_prec;
         const R u2 = (R)(ctx->usolvcut * ctx->usolvcut);
         auto launch = [&](auto kern, unsigned nb) {
-            kern<<<nb, kThreads, 0, r>>>(n, ctx->sids, A.at, ctx->bx, aew, ctx->nbr, ctx->cap, ctx->nnb, ctx->Ed, ctx->Ep,
-                                         coef ? A.c0 : nullptr, ctx->rank, ctx->cnb, u2, sp ? ctx->nbru : nullptr,
+            kern<<<nb, kThreads, 0, r>>>(n, ctx->sids, A.atS, ctx->bx, aew, ctx->cnb, ctx->cap, ctx->nnb, ctx->Ed, ctx->Ep,
+                                         coef ? A.c0 : nullptr, u2, sp ? ctx->nbru : nullptr,
                                          sp ? A.cu0 : nullptr, sp ? ctx->nnbu : nullptr);
         };
         LPA_DISPATCH(ctx->lpa, {
@@ -1181,10 +1184,10 @@ void enqueue_opt_cross(amg_ctx* ctx, cudaStream_t s, double* virp) {
         const double* Y = uo + b * blk;  // ud^(b)
         k_opt_cross<<<nblk(n3), kThreads, 0, s>>>(n3, ctx->optorder, b, ctx->copm, uo, V);
         KCHECK();
-        k_pack_u<R><<<nblk(n), kThreads, 0, s>>>(n, Y, V, A.u4);
+        k_pack_u<R><<<nblk(n), kThreads, 0, s>>>(n, Y, V, A.u4, ctx->rank);  // cell order
         KCHECK();
         auto launch = [&](auto kern) {
-            kern<<<nblk((size_t)n * 8), kThreads, 0, s>>>(n, ctx->sids, A.at, A.u4, ctx->bx, aew, ctx->nbr, ctx->cap,
+            kern<<<nblk((size_t)n * 8), kThreads, 0, s>>>(n, ctx->sids, A.atS, A.u4, ctx->bx, aew, ctx->cnb, ctx->cap,
                                                           ctx->nnb, 1, ctx->f, ctx->grad_p, ctx->trq_p, virp);
         };
         if (ewald_cells(ctx)) {
@@ -1237,7 +1240,7 @@ void enqueue_back(amg_ctx* ctx, cudaStream_t s, int flags) {
         KCHECK();
         k_zero<double><<<nblk(3 * n, 256), 256, 0, s>>>(ctx->trq_p, 3 * (size_t)n);
         KCHECK();
-        k_pack_u<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->ud, ctx->up, A.u4);
+        k_pack_u<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->ud, ctx->up, A.u4, ctx->rank);  // cell order
         KCHECK();
     }
     // Real-space pair kernels (atomic accumulation) on the side stream; the
@@ -1276,7 +1279,7 @@ void enqueue_back(amg_ctx* ctx, cudaStream_t s, int flags) {
     LPA_DISPATCH(ctx->lpa, {
         const size_t nb = nblk((size_t)n * L);
         auto launch_n = [&](auto kern, size_t blocks) {
-            kern<<<blocks, kThreads, 0, r>>>(n, ctx->sids, A.at, ctx->bx, aew, ctx->nbr, ctx->cap, ctx->nnb, ctx->f,
+            kern<<<blocks, kThreads, 0, r>>>(n, ctx->sids, A.atS, ctx->bx, aew, ctx->cnb, ctx->cap, ctx->nnb, ctx->f,
                                              ctx->grad_m, ctx->trq_m, ctx->eacc, analysis ? ctx->aem : nullptr,
                                              analysis ? mol : nullptr, analysis ? ctx->cnt : nullptr, vir);
         };
@@ -1304,7 +1307,7 @@ void enqueue_back(amg_ctx* ctx, cudaStream_t s, int flags) {
     }
     if (polgrad) {
         auto launch = [&](auto kern, int lanes) {
-            kern<<<nblk((size_t)n * lanes), kThreads, 0, r>>>(n, ctx->sids, A.at, A.u4, ctx->bx, aew, ctx->nbr, ctx->cap,
+            kern<<<nblk((size_t)n * lanes), kThreads, 0, r>>>(n, ctx->sids, A.atS, A.u4, ctx->bx, aew, ctx->cnb, ctx->cap,
                                                               ctx->nnb, mutual, ctx->f, ctx->grad_p, ctx->trq_p, virp);
         };
         if (ewald_cells(ctx)) {  // one lane count for the cell variants
@@ -1625,6 +1628,7 @@ void release(amg_ctx* ctx) {
     if (ctx->cubtmp) cudaFree(ctx->cubtmp);
     ctx->cubtmp = nullptr;
     dfree(ctx->af.at); dfree(ctx->af.u4); dfree(ctx->ad.at); dfree(ctx->ad.u4);
+    dfree(ctx->af.atS); dfree(ctx->ad.atS);
     dfree(ctx->af.p4); dfree(ctx->ad.p4); dfree(ctx->af.c0); dfree(ctx->ad.c0);
     dfree(ctx->af.s4); dfree(ctx->ad.s4); dfree(ctx->af.cu0); dfree(ctx->ad.cu0);
     dfree(ctx->nbru); dfree(ctx->nnbu);
@@ -1779,10 +1783,12 @@ int create_impl(amg_ctx* ctx, const amg_params* P) {
     dalloc(ctx, ctx->xyz, 3 * (size_t)n);
     dalloc(ctx, ctx->rp10, 10 * (size_t)n);
     dalloc(ctx, ctx->ad.at, n);
+    dalloc(ctx, ctx->ad.atS, n);
     dalloc(ctx, ctx->ad.u4, 2 * (size_t)n);
     dalloc(ctx, ctx->ad.p4, 2 * (size_t)n);
     if (ctx->prec == AMG_PREC_MIXED) {
         dalloc(ctx, ctx->af.at, n);
+        dalloc(ctx, ctx->af.atS, n);
         dalloc(ctx, ctx->af.u4, 2 * (size_t)n);
         dalloc(ctx, ctx->af.p4, 2 * (size_t)n);
     }
@@ -1953,8 +1959,10 @@ int backward_impl(amg_ctx* ctx, const amg_cotangents* cot, amg_param_grads* gr) 
     const bool opt = ctx->poltyp == AMG_POL_OPT && ctx->npolar > 0;
     const int K = ctx->optorder;
     if (opt && !ctx->adj_opt) dalloc(ctx, ctx->adj_opt, (size_t)(2 * K + 4) * n3);
-    // FP64 copies of the sites, stencils and T coefficients
+    // FP64 copies of the sites (also in cell order), stencils and T coefficients
     rotate_and_pack<double>(ctx, s);
+    k_gather_atoms<double><<<nblk(n), kThreads, 0, s>>>(n, ctx->sids, ctx->ad.at, ctx->ad.atS);
+    KCHECK();
     if (ctx->ewald) {
         pme_prepare<double>(ctx, pme_of<double>(ctx));
         pme_stencils<double>(ctx, s);

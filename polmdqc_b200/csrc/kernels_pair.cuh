@@ -7,10 +7,13 @@
 namespace amg {
 
 // All bulk pair kernels below give each site a group of LPA consecutive
-// lanes (LPA = 4, 8, 16 or 32); the lanes stride through the site's
-// neighbour slots nbr[i * cap + s] and the partial sums are combined with
-// warp shuffles (group_sum).  Sites past n run with an empty list so every
-// lane takes part in the shuffles.
+// lanes (LPA = 4, 8, 16 or 32); sites are taken in cell order (order = sids,
+// g the position in that order, i = order[g] the site).  The lanes stride
+// through the site's neighbour slots nbr[i * cap + s] -- here the partners'
+// positions in cell order (the lists' cnb) -- and gather the packed sites
+// `at` and dipoles u4 stored in cell order; results go to site i.  Partial
+// sums are combined with warp shuffles (group_sum).  Sites past n run with an
+// empty list so every lane takes part in the shuffles.
 
 // Permanent field at every site from all neighbours' multipoles, bulk
 // (scale 1, Thole damped, Ewald or bare).  Writes Ed = Ep (the d/p
@@ -24,13 +27,12 @@ __global__ void __launch_bounds__(128) k_perm_field(int n, const int* __restrict
                                                     const int* __restrict__ nbr, int cap,
                                                     const int* __restrict__ nnb, double* __restrict__ Ed,
                                                     double* __restrict__ Ep, R4<R>* __restrict__ c0,
-                                                    const int* __restrict__ rank, int* __restrict__ cnb,
                                                     R usolv2, int* __restrict__ nbru, R4<R>* __restrict__ cu0,
                                                     int* __restrict__ nnbu) {
     const int g = (blockIdx.x * blockDim.x + threadIdx.x) / LPA, lane = threadIdx.x % LPA;
-    const int i = order[min(g, n - 1)];
+    const int gs = min(g, n - 1), i = order[gs];
     const int cnt = g < n ? nnb[i] : 0;
-    AtomR<R> Ai = at[i];
+    AtomR<R> Ai = at[gs];
     V3<R> xi = v3<R>(Ai.a.x, Ai.a.y, Ai.a.z);
     R pdi = Ai.e.y, thi = Ai.e.z;
     double fx = 0, fy = 0, fz = 0;
@@ -55,7 +57,6 @@ __global__ void __launch_bounds__(128) k_perm_field(int n, const int* __restrict
             if (COEF) {
                 bulk_radial_prec<R, EWALD>(r2, aewald, pdi * Aj.e.y, pair_thole<R>(thi, Aj.e.z), B, P1, P2);
                 c0[base + s] = pack_tensor<R>(r.x, r.y, r.z, B[1], B[2]);
-                cnb[base + s] = rank[j];
             } else {
                 bulk_radial<R, EWALD, true>(r2, aewald, pdi * Aj.e.y, pair_thole<R>(thi, Aj.e.z), B);
             }
@@ -67,7 +68,7 @@ __global__ void __launch_bounds__(128) k_perm_field(int n, const int* __restrict
             const unsigned b = __ballot_sync(gmask, take) & gmask;
             if (take) {
                 const size_t q = base + nu + __popc(b & below);
-                nbru[q] = rank[j];
+                nbru[q] = j;
                 cu0[q] = pack_tensor<R>(r.x, r.y, r.z, P1, P2);
             }
             nu += __popc(b);
@@ -205,11 +206,11 @@ __global__ void __launch_bounds__(128) k_mpole_pair(int n, const int* __restrict
                                                     double* __restrict__ aem, const int* __restrict__ mol,
                                                     unsigned long long* __restrict__ npair, double* __restrict__ vir) {
     const int gi_ = (blockIdx.x * blockDim.x + threadIdx.x) / LPA, lane = threadIdx.x % LPA;
-    const int i = order[min(gi_, n - 1)];
+    const int gs = min(gi_, n - 1), i = order[gs];
     const int cnt = gi_ < n ? nnb[i] : 0;
     double e_i = 0, einter = 0, w[6] = {0, 0, 0, 0, 0, 0};
     long long cntnz = 0;
-    AtomR<R> Ai = at[i];
+    AtomR<R> Ai = at[gs];
     Mpole<R> Mi = load_mpole(Ai);
     V3<R> xi = v3<R>(Ai.a.x, Ai.a.y, Ai.a.z);
     V3<R> g = v3<R>(0, 0, 0), t = v3<R>(0, 0, 0);
@@ -229,7 +230,7 @@ __global__ void __launch_bounds__(128) k_mpole_pair(int n, const int* __restrict
         t = t + ti;
         if (EXTRA) {
             if (E != R(0)) cntnz++;
-            if (mol && mol[j] != mi) einter += 0.5 * (double)E;
+            if (mol && mol[order[j]] != mi) einter += 0.5 * (double)E;
             vir_outer(w, gi.x, gi.y, gi.z, r.x, r.y, r.z, -0.5 * f);
         }
     }
@@ -264,12 +265,12 @@ __global__ void __launch_bounds__(128) k_polar_pair(int n, const int* __restrict
                                                     double* __restrict__ grad, double* __restrict__ trq,
                                                     double* __restrict__ vir) {
     const int gi_ = (blockIdx.x * blockDim.x + threadIdx.x) / LPA, lane = threadIdx.x % LPA;
-    const int i = order[min(gi_, n - 1)];
+    const int gs = min(gi_, n - 1), i = order[gs];
     const int cnt = gi_ < n ? nnb[i] : 0;
-    AtomR<R> Ai = at[i];
+    AtomR<R> Ai = at[gs];
     Mpole<R> Mi = load_mpole(Ai);
     V3<R> xi = v3<R>(Ai.a.x, Ai.a.y, Ai.a.z);
-    R4<R> udi4 = u4[2 * i], upi4 = u4[2 * i + 1];
+    R4<R> udi4 = u4[2 * gs], upi4 = u4[2 * gs + 1];
     V3<R> udi = v3<R>(udi4.x, udi4.y, udi4.z), upi = v3<R>(upi4.x, upi4.y, upi4.z);
     V3<R> ubi = R(0.5) * (udi + upi);
     V3<R> g = v3<R>(0, 0, 0), t = v3<R>(0, 0, 0);
@@ -321,14 +322,13 @@ __global__ void __launch_bounds__(128) k_polar_pair(int n, const int* __restrict
 template <class R, bool EWALD, int LPA, bool CELLS = false>
 __global__ void __launch_bounds__(128) k_tu_coeffs(int n, const int* __restrict__ order, const AtomR<R>* __restrict__ at, Box bx, R aewald,
                                                    const int* __restrict__ nbr, int cap, const int* __restrict__ nnb,
-                                                   R4<R>* __restrict__ c0, const int* __restrict__ rank,
-                                                   int* __restrict__ cnb, R usolv2, int* __restrict__ nbru,
+                                                   R4<R>* __restrict__ c0, R usolv2, int* __restrict__ nbru,
                                                    R4<R>* __restrict__ cu0, int* __restrict__ nnbu) {
     const int g = (blockIdx.x * blockDim.x + threadIdx.x) / LPA, lane = threadIdx.x % LPA;
     if (g >= n) return;  // whole lane groups leave together
     const int i = order[g];
     const int cnt = nnb[i];
-    R4<R> pi = at[i].a, ei = at[i].e;
+    R4<R> pi = at[g].a, ei = at[g].e;
     V3<R> xi = v3<R>(pi.x, pi.y, pi.z);
     const size_t base = (size_t)i * cap;
     // lanes of this group within the warp, and the lanes below this one
@@ -367,14 +367,13 @@ __global__ void __launch_bounds__(128) k_tu_coeffs(int n, const int* __restrict_
                 P2 -= (R(1) + x) * e * b2;
             }
             c0[base + s] = pack_tensor<R>(r.x, r.y, r.z, B1, B2);
-            cnb[base + s] = rank[j];
         }
         if (cu0) {  // sparse preconditioner: bare Thole-damped T within usolvcut, compacted in order
             const bool take = ok && r2 <= usolv2;
             const unsigned b = __ballot_sync(gmask, take) & gmask;
             if (take) {
                 const size_t q = base + nu + __popc(b & below);
-                nbru[q] = rank[j];
+                nbru[q] = j;
                 cu0[q] = pack_tensor<R>(r.x, r.y, r.z, P1, P2);
             }
             nu += __popc(b);

@@ -162,6 +162,16 @@ __global__ void k_cell_bounds(int n, const unsigned* __restrict__ skeys, const i
     if (sdt) sdt[i] = make_double2(pdamp[a], thole[a]);  // damping parameters in cell order
 }
 
+// The packed sites in cell order (atS[g] = at[sids[g]]), which the bulk pair
+// kernels gather with the cell-order partner indices of the lists: a warp's
+// sites share most of their partners, which then sit in a few contiguous runs.
+template <class R>
+__global__ void k_gather_atoms(int n, const int* __restrict__ sids, const AtomR<R>* __restrict__ at,
+                               AtomR<R>* __restrict__ atS) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < n) atS[g] = at[sids[g]];
+}
+
 // Exact neighbour list: all j != i with minimum-image |r| <= cutoff, decided
 // in FP64 so the pair set is the same in both precisions, leaving out the
 // scaled (1-n / polarization-group) partners of i (xoff/xidx, CSR), which

@@ -907,30 +907,37 @@ void build_tu_coeffs(amg_ctx* ctx, cudaStream_t s) {
 }
 
 // A v with the stored coefficients; v4 is the R4 copy of (vd, vp).  With
-// vAv (Ewald only) the dot products v.Av are added to vAv[0..1].
+// vAv (Ewald only) the dot products v.Av are added to vAv[0..1].  `apart`
+// (Ewald, with vAv) keeps the real-space field out of Ad, Ap: the gather then
+// runs beside the real-space kernel instead of after it, each adds its share
+// of v.Av, and the caller takes A v = Ad - Fd (k_pcg_update).
 template <class R>
 void matvec_stored(amg_ctx* ctx, cudaStream_t s, const R4<R>* v4, const double* vd, const double* vp, double* Ad,
-                   double* Ap, double* vAv = nullptr, bool spread = true) {
+                   double* Ap, double* vAv = nullptr, bool spread = true, bool apart = false) {
     const int n = ctx->n;
     Atoms<R>& A = atoms_of<R>(ctx);
+    apart = apart && ctx->ewald && vAv;
     // real space on the side stream, PME on s
     cudaStream_t r = ctx->ewald ? fork_side(ctx, s) : s;
     LPA_DISPATCH(ctx->lpa, {
         k_tu_stored<R, L><<<nblk((size_t)n * L), kThreads, 0, r>>>(n, ctx->sids, ctx->cnb, A.c0, ctx->cap, ctx->nnb, ctx->xoff,
-                                                                    v4, ctx->Fd, ctx->Fp);
+                                                                    v4, ctx->Fd, ctx->Fp, apart ? vd : nullptr,
+                                                                    apart ? vp : nullptr, apart ? vAv : nullptr);
     });
     KCHECK();
     if (ctx->ewald) {
         Pme<R>& pm = pme_of<R>(ctx);
         pme_dipole_grids<R>(ctx, s, vd, vp, spread);
-        join_side(ctx, s);
+        if (!apart) join_side(ctx, s);
         int3 K = make_int3(ctx->K[0], ctx->K[1], ctx->K[2]);
         constexpr int G = 8;  // lanes per site
         const unsigned blocks = (unsigned)std::min<size_t>(nblk((size_t)n * G), (size_t)ctx->num_sms * 8);
         k_gather_field<R, kOrder, G><<<blocks, kThreads, 0, s>>>(n, pm.zq, pm.theta, pm.k0, K, ctx->frac, vd,
-                                                                 vp, ctx->Fd, ctx->Fp, self_coef(ctx), ctx->pol, Ad,
-                                                                 Ap, vAv);
+                                                                 vp, apart ? nullptr : ctx->Fd,
+                                                                 apart ? nullptr : ctx->Fp, self_coef(ctx), ctx->pol,
+                                                                 Ad, Ap, vAv);
         KCHECK();
+        if (apart) join_side(ctx, s);
     } else {
         k_matvec_finish<<<nblk(n), kThreads, 0, s>>>(n, vd, vp, ctx->Fd, ctx->Fp, ctx->phiU4, 0, 0.0, ctx->pol, Ad, Ap);
         KCHECK();
@@ -1033,8 +1040,9 @@ void enqueue_pcg_iter(amg_ctx* ctx, cudaStream_t s, cudaGraphConditionalHandle h
     const int n = ctx->n, n3 = 3 * n;
     Atoms<R>& A = atoms_of<R>(ctx);
     // p.Ap: fused into the PME gather with Ewald, a separate pass without
+    const bool apart = ctx->ewald;  // real-space field kept apart: the gather overlaps k_tu_stored
     matvec_stored<R>(ctx, s, A.p4, ctx->pd, ctx->pp, ctx->Apd, ctx->App, ctx->ewald ? ctx->scal + PAP_D : nullptr,
-                     false);
+                     false, apart);
     if (!ctx->ewald) {
         k_dot2<<<nblk(n3, 256), 256, 0, s>>>(n3, ctx->pd, ctx->Apd, ctx->pp, ctx->App, ctx->scal + PAP_D,
                                               ctx->scal + PAP_P);
@@ -1042,7 +1050,8 @@ void enqueue_pcg_iter(amg_ctx* ctx, cudaStream_t s, cudaGraphConditionalHandle h
     }
     k_pcg_update<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->pol, ctx->pd, ctx->pp, ctx->Apd, ctx->App, ctx->ud, ctx->up,
                                                  ctx->rd, ctx->rp, ctx->zd, ctx->zp, ctx->scal,
-                                                 ctx->sparse_prec ? A.s4 : nullptr, ctx->rank);
+                                                 ctx->sparse_prec ? A.s4 : nullptr, ctx->rank,
+                                                 apart ? ctx->Fd : nullptr, apart ? ctx->Fp : nullptr);
     KCHECK();
     if (ctx->sparse_prec) {
         precondition<R>(ctx, s, false, ctx->scal + RZN_D, h, use_handle);  // with the control decision

@@ -188,6 +188,65 @@ __device__ __forceinline__ void apply_tensor(const R4<R>& c, const R4<R>& v, R& 
     fz += a * c.z - c.w * v.z;
 }
 
+// streaming (evict-first) load of one packed coefficient: the rows are read
+// once per launch and would otherwise push the gathered vectors out of L2
+template <class R>
+__device__ __forceinline__ R4<R> load_stream(const R4<R>* p) {
+    if constexpr (sizeof(R) == 4) {
+        return __ldcs(reinterpret_cast<const float4*>(p));
+    } else {
+        const double2 a = __ldcs(reinterpret_cast<const double2*>(p));
+        const double2 b = __ldcs(reinterpret_cast<const double2*>(p) + 1);
+        return make_r4<R>(a.x, a.y, b.x, b.y);
+    }
+}
+
+// Sum of T v over one stored row (cnt slots from `base`; partner indices and
+// packed coefficients side by side) for two vector sets v4[2j], v4[2j+1],
+// the row's LPA lanes taking every LPA-th slot.  Software-pipelined: the next
+// batch of U indices and coefficients is requested before the current batch's
+// partner vectors are consumed, so a lane keeps two memory round trips in
+// flight (the kernels using it are bound by memory latency).  Empty slots
+// point at `self` with a zero coefficient.
+template <class R, int LPA, int U>
+__device__ __forceinline__ void row_apply(const int* __restrict__ idx, const R4<R>* __restrict__ coef, size_t base,
+                                          int cnt, int lane, int self, const R4<R>* __restrict__ v4, R& ax, R& ay,
+                                          R& az, R& bx, R& by, R& bz) {
+    int jn[U];
+    R4<R> cn[U];
+    auto fetch = [&](int s0) {
+#pragma unroll
+        for (int q = 0; q < U; q++) {
+            const int s = s0 + q * LPA;
+            const bool ok = s < cnt;
+            jn[q] = ok ? __ldcs(idx + base + s) : self;
+            cn[q] = ok ? load_stream<R>(coef + base + s) : make_r4<R>(0, 0, 0, 0);
+        }
+    };
+    fetch(lane);
+    for (int s0 = lane; s0 < cnt; s0 += U * LPA) {
+        int j[U];
+        R4<R> c[U];
+#pragma unroll
+        for (int q = 0; q < U; q++) {
+            j[q] = jn[q];
+            c[q] = cn[q];
+        }
+        R4<R> vd[U], vp[U];
+#pragma unroll
+        for (int q = 0; q < U; q++) {
+            vd[q] = v4[2 * j[q]];
+            vp[q] = v4[2 * j[q] + 1];
+        }
+        fetch(s0 + U * LPA);
+#pragma unroll
+        for (int q = 0; q < U; q++) {
+            apply_tensor<R>(c[q], vd[q], ax, ay, az);
+            apply_tensor<R>(c[q], vp[q], bx, by, bz);
+        }
+    }
+}
+
 // PCG scalars: rz (current), p.Ap, rz of the next iteration, r.r, and the
 // previous rz for the direction update
 enum Scal { RZ_D = 0, RZ_P, PAP_D, PAP_P, RZN_D, RZN_P, RR_D, RR_P, RZO_D, RZO_P, NSCAL };

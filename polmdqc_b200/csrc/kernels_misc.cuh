@@ -124,14 +124,16 @@ __global__ void k_dot2(int n3, const double* __restrict__ a1, const double* __re
 
 // u += a p; r -= a Ap; rr  (a = rz / pAp per set).  Diagonal
 // preconditioner (s4 null): z = alpha r and rz_new; sparse preconditioner:
-// s = alpha r packed into s4 for k_precond.
+// s = alpha r packed into s4 for k_precond.  With Fd, Fp the stored Apd, App
+// lack the real-space part, and A p = Apd - Fd (see k_gather_field).
 template <class R>
 __global__ void k_pcg_update(int n, const double* __restrict__ pol, const double* __restrict__ pd,
                              const double* __restrict__ pp, const double* __restrict__ Apd,
                              const double* __restrict__ App, double* __restrict__ ud, double* __restrict__ up,
                              double* __restrict__ rd, double* __restrict__ rp, double* __restrict__ zd,
                              double* __restrict__ zp, double* __restrict__ scal, R4<R>* __restrict__ s4,
-                             const int* __restrict__ rank) {
+                             const int* __restrict__ rank, const double* __restrict__ Fd = nullptr,
+                             const double* __restrict__ Fp = nullptr) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double ad = scal[PAP_D] != 0 ? scal[RZ_D] / scal[PAP_D] : 0.0;
     double ap = scal[PAP_P] != 0 ? scal[RZ_P] / scal[PAP_P] : 0.0;
@@ -143,7 +145,8 @@ __global__ void k_pcg_update(int n, const double* __restrict__ pol, const double
             int q = 3 * i + c;
             ud[q] += ad * pd[q];
             up[q] += ap * pp[q];
-            double r1 = rd[q] - ad * Apd[q], r2 = rp[q] - ap * App[q];
+            const double Aq1 = Fd ? Apd[q] - Fd[q] : Apd[q], Aq2 = Fp ? App[q] - Fp[q] : App[q];
+            double r1 = rd[q] - ad * Aq1, r2 = rp[q] - ap * Aq2;
             rd[q] = r1; rp[q] = r2;
             double z1 = a * r1, z2 = a * r2;
             sv[c] = z1; sv[3 + c] = z2;

@@ -384,47 +384,36 @@ __global__ void __launch_bounds__(128) k_tu_coeffs(int n, const int* __restrict_
 
 // T v with the stored coefficients (both dipole sets): rows of nnb[i] bulk
 // slots plus the site's scaled partners.  u4: [n][2] R4 in cell order.
+// With vAv, also adds -v.F of both sets to vAv[0..1] (the real-space share
+// of v.Av when the rest of Av is assembled apart, see k_gather_field).
 template <class R, int LPA>
 __global__ void __launch_bounds__(128) k_tu_stored(int n, const int* __restrict__ order, const int* __restrict__ cnb,
                                                    const R4<R>* __restrict__ c0, int cap,
                                                    const int* __restrict__ nnb, const int* __restrict__ xoff,
                                                    const R4<R>* __restrict__ u4, double* __restrict__ Fd,
-                                                   double* __restrict__ Fp) {
+                                                   double* __restrict__ Fp, const double* __restrict__ vd = nullptr,
+                                                   const double* __restrict__ vp = nullptr,
+                                                   double* __restrict__ vAv = nullptr) {
     const int g = (blockIdx.x * blockDim.x + threadIdx.x) / LPA, lane = threadIdx.x % LPA;
     const int gs = min(g, n - 1), i = order[gs];  // gs: the site's position in cell order
     const int cnt = g < n ? nnb[i] + (xoff[i + 1] - xoff[i]) : 0;
     const size_t base = (size_t)i * cap;
     R ax = 0, ay = 0, az = 0, bx_ = 0, by = 0, bz = 0;
-    // U slots per lane in flight: all loads of a batch are issued before any
-    // is consumed (the kernel is bound by memory latency, not bandwidth)
-    constexpr int U = 4;
-    for (int s0 = lane; s0 < cnt; s0 += U * LPA) {
-        int j[U];
-        R4<R> c[U];
-#pragma unroll
-        for (int q = 0; q < U; q++) {
-            const int s = s0 + q * LPA;
-            const bool ok = s < cnt;
-            j[q] = ok ? cnb[base + s] : gs;
-            c[q] = ok ? c0[base + s] : make_r4<R>(0, 0, 0, 0);
-        }
-        R4<R> ud[U], up[U];
-#pragma unroll
-        for (int q = 0; q < U; q++) {
-            ud[q] = u4[2 * j[q]];
-            up[q] = u4[2 * j[q] + 1];
-        }
-#pragma unroll
-        for (int q = 0; q < U; q++) {
-            apply_tensor<R>(c[q], ud[q], ax, ay, az);
-            apply_tensor<R>(c[q], up[q], bx_, by, bz);
-        }
-    }
+    row_apply<R, LPA, sizeof(R) == 4 ? 4 : 2>(cnb, c0, base, cnt, lane, gs, u4, ax, ay, az, bx_, by, bz);
     double sx = group_sum<LPA>((double)ax), sy = group_sum<LPA>((double)ay), sz = group_sum<LPA>((double)az);
     double tx = group_sum<LPA>((double)bx_), ty = group_sum<LPA>((double)by), tz = group_sum<LPA>((double)bz);
+    double dd = 0, dp = 0;
     if (lane == 0 && g < n) {
         Fd[3 * i] = sx; Fd[3 * i + 1] = sy; Fd[3 * i + 2] = sz;
         Fp[3 * i] = tx; Fp[3 * i + 1] = ty; Fp[3 * i + 2] = tz;
+        if (vAv) {  // this part's share of v.Av (Av holds -F)
+            dd = -(vd[3 * i] * sx + vd[3 * i + 1] * sy + vd[3 * i + 2] * sz);
+            dp = -(vp[3 * i] * tx + vp[3 * i + 1] * ty + vp[3 * i + 2] * tz);
+        }
+    }
+    if (vAv) {
+        block_sum_add(dd, vAv);
+        block_sum_add(dp, vAv + 1);
     }
 }
 
@@ -595,29 +584,7 @@ __global__ void __launch_bounds__(128) k_precond(int n, const int* __restrict__ 
         const int cnt = g < n ? nnbu[i] + (xoff[i + 1] - xoff[i]) : 0;
         const size_t base = (size_t)i * cap;
         R ax = 0, ay = 0, az = 0, bx_ = 0, by = 0, bz = 0;
-        constexpr int U = 4;
-        for (int s0 = lane; s0 < cnt; s0 += U * LPA) {
-            int j[U];
-            R4<R> c[U];
-#pragma unroll
-            for (int q = 0; q < U; q++) {
-                const int s = s0 + q * LPA;
-                const bool ok = s < cnt;
-                j[q] = ok ? nbru[base + s] : gs;
-                c[q] = ok ? cu0[base + s] : make_r4<R>(0, 0, 0, 0);
-            }
-            R4<R> vd[U], vp[U];
-#pragma unroll
-            for (int q = 0; q < U; q++) {
-                vd[q] = s4[2 * j[q]];
-                vp[q] = s4[2 * j[q] + 1];
-            }
-#pragma unroll
-            for (int q = 0; q < U; q++) {
-                apply_tensor<R>(c[q], vd[q], ax, ay, az);
-                apply_tensor<R>(c[q], vp[q], bx_, by, bz);
-            }
-        }
+        row_apply<R, LPA, sizeof(R) == 4 ? 4 : 2>(nbru, cu0, base, cnt, lane, gs, s4, ax, ay, az, bx_, by, bz);
         double S[6];
         S[0] = group_sum<LPA>((double)ax); S[1] = group_sum<LPA>((double)ay); S[2] = group_sum<LPA>((double)az);
         S[3] = group_sum<LPA>((double)bx_); S[4] = group_sum<LPA>((double)by); S[5] = group_sum<LPA>((double)bz);

@@ -269,6 +269,9 @@ inline unsigned spread_blocks(int n) {
 // z-lines (a, b) of the P^3 stencil (P grid values per line), the per-lane
 // sums are combined with shuffles and lanes 0..5 write the six components.
 // Blocks stride over the sites, so each block adds its dot products once.
+// With Fd, Fp null the real-space field is left out (A v without -F_real,
+// and its dot products): the real-space kernel then runs beside this one and
+// adds its own share (k_tu_stored with vAv), and k_pcg_update subtracts F.
 template <class R, int P, int G>
 __global__ void __launch_bounds__(128) k_gather_field(int n, const typename Cplx<R>::type* __restrict__ zg,
                                                       const R* __restrict__ theta, const int* __restrict__ k0,
@@ -328,7 +331,7 @@ __global__ void __launch_bounds__(128) k_gather_field(int n, const typename Cplx
             const double* FF = dset ? Fd : Fp;
             double* AA = dset ? Ad : Ap;
             const double alpha = pol[i];
-            const double field = FF[3 * i + c] - dphi + selfc * vv[3 * i + c];
+            const double field = (FF ? FF[3 * i + c] : 0.0) - dphi + selfc * vv[3 * i + c];
             const double av = alpha > 0 ? vv[3 * i + c] / alpha - field : 0.0;
             AA[3 * i + c] = av;
             if (dset) dotd += vv[3 * i + c] * av;

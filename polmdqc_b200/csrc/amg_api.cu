@@ -176,7 +176,7 @@ struct amg_ctx {
     double cell_volume = 1.0;
     int npolar = 0;
     int *iter = nullptr, *cont = nullptr;
-    int* dir_done = nullptr;  // block counter of k_pcg_dir (back to 0 after every launch)
+    int* blk_done = nullptr;  // last-block counter of k_precond and k_pcg_update (back to 0 after every launch)
     // OPT: order, copm_k = sum_{j>=k} copt_j, and the perturbation orders
     // u^(k) [K+1][2][3n] followed by one [3n] scratch vector
     int optorder = 0;
@@ -956,30 +956,20 @@ double pcg_threshold(const amg_ctx* ctx) {
 constexpr double kPrecDiag = 2.0;
 
 // z = M r for both residual sets from the packed s = alpha r (A.s4); adds
-// r.z to rz_out[0..1]; `first` also starts the directions p = z
-// (and, its last block, the PCG control decision)
+// r.z to the scalars and (its last block) rolls them for the direction update
 template <class R>
-void precondition(amg_ctx* ctx, cudaStream_t s, bool first, double* rz_out, cudaGraphConditionalHandle h,
-                  int use_handle) {
+void precondition(amg_ctx* ctx, cudaStream_t s) {
     const int n = ctx->n;
     Atoms<R>& A = atoms_of<R>(ctx);
     constexpr int L = 4;  // lanes per site: the rows are short
     const unsigned blocks = (unsigned)std::min<size_t>(nblk((size_t)n * L), (size_t)ctx->num_sms * 8);
-    const double thr = pcg_threshold(ctx);
-    if (first)
-        k_precond<R, L, true><<<blocks, kThreads, 0, s>>>(
-            n, ctx->sids, ctx->nbru, A.cu0, ctx->cap, ctx->nnbu, ctx->xoff, A.s4, ctx->pol, kPrecDiag, ctx->rd,
-            ctx->rp, ctx->zd, ctx->zp, ctx->pd, ctx->pp, A.p4, rz_out, ctx->dir_done, ctx->iter, thr, ctx->politer, h,
-            use_handle, ctx->cont);
-    else
-        k_precond<R, L, false><<<blocks, kThreads, 0, s>>>(
-            n, ctx->sids, ctx->nbru, A.cu0, ctx->cap, ctx->nnbu, ctx->xoff, A.s4, ctx->pol, kPrecDiag, ctx->rd,
-            ctx->rp, ctx->zd, ctx->zp, ctx->pd, ctx->pp, A.p4, rz_out, ctx->dir_done, ctx->iter, thr, ctx->politer, h,
-            use_handle, ctx->cont);
+    k_precond<R, L><<<blocks, kThreads, 0, s>>>(n, ctx->sids, ctx->nbru, A.cu0, ctx->cap, ctx->nnbu, ctx->xoff, A.s4,
+                                                ctx->pol, kPrecDiag, ctx->rd, ctx->rp, ctx->zd, ctx->zp, ctx->scal,
+                                                ctx->blk_done);
     KCHECK();
 }
 
-// p = z + beta p after the control decision; with Ewald fused with the
+// p = z + beta p after the rz scalars were rolled; with Ewald fused with the
 // spreading of p for the next matvec
 template <class R>
 void direction(amg_ctx* ctx, cudaStream_t s) {
@@ -996,8 +986,9 @@ void direction(amg_ctx* ctx, cudaStream_t s) {
     KCHECK();
 }
 
-// set-up of the solve: r = E - A u0, z = p = alpha r, and the first control
-// decision (continue while rr > threshold and iterations < politer)
+// set-up of the solve: r = E - A u0 (with the diagonal preconditioner also
+// z = alpha r and r.z) and the first control decision (continue while
+// rr > threshold and iterations < politer)
 template <class R>
 void enqueue_pcg_init(amg_ctx* ctx, cudaStream_t s, cudaGraphConditionalHandle h, int use_handle,
                       bool coeffs_built) {
@@ -1014,31 +1005,27 @@ void enqueue_pcg_init(amg_ctx* ctx, cudaStream_t s, cudaGraphConditionalHandle h
     if (!coeffs_built) build_tu_coeffs<R>(ctx, s);
     k_pack_u<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->ud, ctx->up, A.u4, ctx->rank);  // cell order
     KCHECK();
+    // leaves the dipole grid clear for the direction updates' spreading
     matvec_stored<R>(ctx, s, A.u4, ctx->ud, ctx->up, ctx->Apd, ctx->App);
     k_pcg_init<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->Ed, ctx->Ep, ctx->Apd, ctx->App, ctx->pol, ctx->rd, ctx->rp,
-                                               ctx->zd, ctx->zp, ctx->pd, ctx->pp, ctx->scal,
-                                               ctx->sparse_prec ? A.s4 : nullptr, ctx->rank);
+                                               ctx->zd, ctx->zp, ctx->scal, ctx->sparse_prec ? A.s4 : nullptr,
+                                               ctx->rank);
     KCHECK();
-    if (ctx->sparse_prec) {
-        precondition<R>(ctx, s, true, ctx->scal + RZ_D, h, use_handle);  // with the first control decision
-    } else {
-        k_pack_u<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->pd, ctx->pp, A.p4, ctx->rank);
-        KCHECK();
-        k_pcg_control<<<1, 1, 0, s>>>(ctx->scal, ctx->iter, pcg_threshold(ctx), ctx->politer, 1, h, use_handle,
-                                      ctx->cont);
-        KCHECK();
-    }
-    // the iterations' matvecs find p already spread (the direction update
-    // spreads the next one); the grid is clear after the first matvec
-    if (ctx->ewald) spread_dipoles<R>(ctx, s, ctx->pd, ctx->pp);
+    k_pcg_control<<<1, 1, 0, s>>>(ctx->scal, ctx->iter, pcg_threshold(ctx), ctx->politer, 1, 0, h, use_handle,
+                                  ctx->cont);
+    KCHECK();
 }
 
-// one PCG iteration (both right-hand sides): matvec, update, preconditioner
-// and control decision, direction update
+// one PCG iteration (both right-hand sides): preconditioner (sparse), the
+// direction update (spreading p with Ewald), matvec, and the residual update
+// whose last block takes the control decision.  Ending with the decision, the iteration that meets the
+// threshold leaves no preconditioner or direction work behind it.
 template <class R>
 void enqueue_pcg_iter(amg_ctx* ctx, cudaStream_t s, cudaGraphConditionalHandle h, int use_handle) {
     const int n = ctx->n, n3 = 3 * n;
     Atoms<R>& A = atoms_of<R>(ctx);
+    if (ctx->sparse_prec) precondition<R>(ctx, s);
+    direction<R>(ctx, s);
     // p.Ap: fused into the PME gather with Ewald, a separate pass without
     const bool apart = ctx->ewald;  // real-space field kept apart: the gather overlaps k_tu_stored
     matvec_stored<R>(ctx, s, A.p4, ctx->pd, ctx->pp, ctx->Apd, ctx->App, ctx->ewald ? ctx->scal + PAP_D : nullptr,
@@ -1051,16 +1038,10 @@ void enqueue_pcg_iter(amg_ctx* ctx, cudaStream_t s, cudaGraphConditionalHandle h
     k_pcg_update<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->pol, ctx->pd, ctx->pp, ctx->Apd, ctx->App, ctx->ud, ctx->up,
                                                  ctx->rd, ctx->rp, ctx->zd, ctx->zp, ctx->scal,
                                                  ctx->sparse_prec ? A.s4 : nullptr, ctx->rank,
-                                                 apart ? ctx->Fd : nullptr, apart ? ctx->Fp : nullptr);
+                                                 apart ? ctx->Fd : nullptr, apart ? ctx->Fp : nullptr,
+                                                 ctx->blk_done, ctx->iter, pcg_threshold(ctx), ctx->politer,
+                                                 ctx->sparse_prec ? 0 : 1, h, use_handle, ctx->cont);
     KCHECK();
-    if (ctx->sparse_prec) {
-        precondition<R>(ctx, s, false, ctx->scal + RZN_D, h, use_handle);  // with the control decision
-    } else {
-        k_pcg_control<<<1, 1, 0, s>>>(ctx->scal, ctx->iter, pcg_threshold(ctx), ctx->politer, 0, h, use_handle,
-                                      ctx->cont);
-        KCHECK();
-    }
-    direction<R>(ctx, s);
 }
 
 // FP64 correction sweep: the true residual with every term in FP64, one
@@ -1653,7 +1634,7 @@ void release(amg_ctx* ctx) {
     if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
     dfree(ctx->iter);
     dfree(ctx->cont);
-    dfree(ctx->dir_done);
+    dfree(ctx->blk_done);
     dfree(ctx->flushbuf);
     dfree(ctx->adj); dfree(ctx->adj_pot); dfree(ctx->adj_n); dfree(ctx->adj_vec); dfree(ctx->adj_phi);
     dfree(ctx->adj_dpole);
@@ -1740,8 +1721,8 @@ int create_impl(amg_ctx* ctx, const amg_params* P) {
     if (ctx->lpa != 8 && ctx->lpa != 16 && ctx->lpa != 32) ctx->lpa = 16;
     dalloc(ctx, ctx->iter, 1);
     dalloc(ctx, ctx->cont, 1);
-    dalloc(ctx, ctx->dir_done, 1);
-    CK(cudaMemset(ctx->dir_done, 0, sizeof(int)));
+    dalloc(ctx, ctx->blk_done, 1);
+    CK(cudaMemset(ctx->blk_done, 0, sizeof(int)));
     CK(cudaMemset(ctx->iter, 0, sizeof(int)));
     if (ctx->has_pol)
         for (int i = 0; i < n; i++) ctx->npolar += P->polarity[i] > 0;

@@ -251,27 +251,36 @@ __device__ __forceinline__ void row_apply(const int* __restrict__ idx, const R4<
 // previous rz for the direction update
 enum Scal { RZ_D = 0, RZ_P, PAP_D, PAP_P, RZN_D, RZN_P, RR_D, RR_P, RZO_D, RZO_P, NSCAL };
 
-// PCG control (one thread): counts the iteration, decides whether to
-// continue (residual above threshold and fewer than politer iterations) and,
-// inside a captured graph, sets the WHILE node's condition.  `first` marks the
-// decision taken right after the initial residual.
+// rz_old <- rz, rz <- rz_new (cleared): the scalars of the direction update
+// p = z + (rz / rz_old) p that follows (rz_old = 0 on the first iteration
+// gives p = z)
+__device__ __forceinline__ void pcg_roll(double* __restrict__ scal) {
+    scal[RZO_D] = scal[RZ_D];
+    scal[RZO_P] = scal[RZ_P];
+    scal[RZ_D] = scal[RZN_D];
+    scal[RZ_P] = scal[RZN_P];
+    scal[RZN_D] = scal[RZN_P] = 0;
+}
+
+// PCG control (one thread), after the residual update: counts the iteration,
+// decides whether to continue (residual above threshold and fewer than
+// politer iterations) and, inside a captured graph, sets the WHILE node's
+// condition.  `first` marks the decision taken right after the initial
+// residual; `roll` rolls the rz scalars here (diagonal preconditioner, whose
+// z comes with the update; the sparse preconditioner rolls them itself).
+// The loop body starts with the preconditioner and the direction update, so
+// an iteration that meets the threshold ends the loop without them.
 __device__ __forceinline__ void pcg_decide(double* __restrict__ scal, int* __restrict__ iter, double thr2, int maxit,
-                                           int first, cudaGraphConditionalHandle h, int use_handle,
+                                           int first, int roll, cudaGraphConditionalHandle h, int use_handle,
                                            int* __restrict__ cont_out) {
     int it = first ? 0 : *iter + 1;
     *iter = it;
-    if (!first) {  // rz_old <- rz, rz <- rz_new: the direction update follows
-        scal[RZO_D] = scal[RZ_D];
-        scal[RZO_P] = scal[RZ_P];
-        scal[RZ_D] = scal[RZN_D];
-        scal[RZ_P] = scal[RZN_P];
-    }
+    if (!first && roll) pcg_roll(scal);
     double e2 = fmax(scal[RR_D], scal[RR_P]);
     int cont = (e2 > thr2) && (it < maxit);
     *cont_out = cont;
     if (cont) {  // accumulators of the next iteration
         scal[PAP_D] = scal[PAP_P] = 0;
-        scal[RZN_D] = scal[RZN_P] = 0;
         scal[RR_D] = scal[RR_P] = 0;
     }
     if (use_handle) cudaGraphSetConditional(h, cont ? 1u : 0u);

@@ -67,20 +67,19 @@ __global__ void k_zero(T* __restrict__ p, size_t n) {
 
 
 __global__ void k_pcg_control(double* __restrict__ scal, int* __restrict__ iter, double thr2, int maxit, int first,
-                              cudaGraphConditionalHandle h, int use_handle, int* __restrict__ cont_out) {
-    pcg_decide(scal, iter, thr2, maxit, first, h, use_handle, cont_out);
+                              int roll, cudaGraphConditionalHandle h, int use_handle, int* __restrict__ cont_out) {
+    pcg_decide(scal, iter, thr2, maxit, first, roll, h, use_handle, cont_out);
 }
 
-// r = E - A u and rr.  Diagonal preconditioner (s4 null): z = alpha r,
-// p = z and rz.  Sparse preconditioner: s = alpha r packed into s4 for
-// k_precond, which forms z, p and rz.
+// r = E - A u and rr.  Diagonal preconditioner (s4 null): z = alpha r and
+// rz.  Sparse preconditioner: s = alpha r packed into s4 for k_precond, which
+// forms z and rz.
 template <class R>
 __global__ void k_pcg_init(int n, const double* __restrict__ Ed, const double* __restrict__ Ep,
                            const double* __restrict__ Aud, const double* __restrict__ Aup,
                            const double* __restrict__ pol, double* __restrict__ rd, double* __restrict__ rp,
-                           double* __restrict__ zd, double* __restrict__ zp, double* __restrict__ pd,
-                           double* __restrict__ pp, double* __restrict__ scal, R4<R>* __restrict__ s4,
-                           const int* __restrict__ rank) {
+                           double* __restrict__ zd, double* __restrict__ zp, double* __restrict__ scal,
+                           R4<R>* __restrict__ s4, const int* __restrict__ rank) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double rzd = 0, rzp = 0, rrd = 0, rrp = 0;
     if (i < n) {
@@ -94,7 +93,6 @@ __global__ void k_pcg_init(int n, const double* __restrict__ Ed, const double* _
             sv[c] = z1; sv[3 + c] = z2;
             if (!s4) {
                 zd[q] = z1; zp[q] = z2;
-                pd[q] = z1; pp[q] = z2;
                 rzd += r1 * z1; rzp += r2 * z2;
             }
             rrd += r1 * r1; rrp += r2 * r2;
@@ -125,15 +123,18 @@ __global__ void k_dot2(int n3, const double* __restrict__ a1, const double* __re
 // u += a p; r -= a Ap; rr  (a = rz / pAp per set).  Diagonal
 // preconditioner (s4 null): z = alpha r and rz_new; sparse preconditioner:
 // s = alpha r packed into s4 for k_precond.  With Fd, Fp the stored Apd, App
-// lack the real-space part, and A p = Apd - Fd (see k_gather_field).
+// lack the real-space part, and A p = Apd - Fd (see k_gather_field).  The
+// last block takes the PCG control decision (pcg_decide).
 template <class R>
 __global__ void k_pcg_update(int n, const double* __restrict__ pol, const double* __restrict__ pd,
                              const double* __restrict__ pp, const double* __restrict__ Apd,
                              const double* __restrict__ App, double* __restrict__ ud, double* __restrict__ up,
                              double* __restrict__ rd, double* __restrict__ rp, double* __restrict__ zd,
                              double* __restrict__ zp, double* __restrict__ scal, R4<R>* __restrict__ s4,
-                             const int* __restrict__ rank, const double* __restrict__ Fd = nullptr,
-                             const double* __restrict__ Fp = nullptr) {
+                             const int* __restrict__ rank, const double* __restrict__ Fd,
+                             const double* __restrict__ Fp, int* __restrict__ done, int* __restrict__ iter,
+                             double thr2, int maxit, int roll, cudaGraphConditionalHandle h, int use_handle,
+                             int* __restrict__ cont_out) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double ad = scal[PAP_D] != 0 ? scal[RZ_D] / scal[PAP_D] : 0.0;
     double ap = scal[PAP_P] != 0 ? scal[RZ_P] / scal[PAP_P] : 0.0;
@@ -167,15 +168,31 @@ __global__ void k_pcg_update(int n, const double* __restrict__ pol, const double
     }
     block_sum_add(rrd, scal + RR_D);
     block_sum_add(rrp, scal + RR_P);
+    // the last block to finish (counted in *done, which it resets) takes the
+    // control decision: every block has added its r.r by then
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(done, 1) == (int)gridDim.x - 1) {
+            __threadfence();
+            *done = 0;
+            pcg_decide(scal, iter, thr2, maxit, 0, roll, h, use_handle, cont_out);
+        }
+    }
 }
 
-// beta = rz / rz_old after the control decision has rolled the scalars
+// beta = rz / rz_old after the scalars were rolled (0 on the first iteration)
 __device__ __forceinline__ void pcg_beta(const double* __restrict__ scal, double& bd, double& bp) {
     bd = scal[RZO_D] != 0 ? scal[RZ_D] / scal[RZO_D] : 0.0;
     bp = scal[RZO_P] != 0 ? scal[RZ_P] / scal[RZO_P] : 0.0;
 }
 
-// p = z + beta p and its R4 copy (runs after the control decision)
+// p = z + beta p; p = z when beta = 0 (the first direction, whose old p is
+// not defined)
+__device__ __forceinline__ double pcg_dir_value(double z, double beta, double p) {
+    return beta != 0 ? z + beta * p : z;
+}
+
+// p = z + beta p and its R4 copy (after the rz scalars were rolled)
 template <class R>
 __global__ void k_pcg_dir(int n, const double* __restrict__ zd, const double* __restrict__ zp,
                           double* __restrict__ pd, double* __restrict__ pp, const double* __restrict__ scal,
@@ -187,8 +204,8 @@ __global__ void k_pcg_dir(int n, const double* __restrict__ zd, const double* __
     double a[3], b[3];
     for (int c = 0; c < 3; c++) {
         int q = 3 * i + c;
-        a[c] = zd[q] + bd * pd[q];
-        b[c] = zp[q] + bp * pp[q];
+        a[c] = pcg_dir_value(zd[q], bd, pd[q]);
+        b[c] = pcg_dir_value(zp[q], bp, pp[q]);
         pd[q] = a[c];
         pp[q] = b[c];
     }
@@ -196,7 +213,7 @@ __global__ void k_pcg_dir(int n, const double* __restrict__ zd, const double* __
     p4[2 * rank[i] + 1] = make_r4<R>((R)b[0], (R)b[1], (R)b[2], R(0));
 }
 
-// p = z + beta p (after the control decision) fused with the spreading of
+// p = z + beta p (after the rz scalars were rolled) fused with the spreading of
 // p into the complex grid zg for the next matvec (zg holds the cleared grid
 // left by the previous transform), in the layout of k_spread_dipoles: FP32,
 // kLineSites sites per block of 128 threads and one z-line per thread; FP64,
@@ -219,7 +236,7 @@ __global__ void __launch_bounds__(128) k_pcg_dir_spread(int n, const double* __r
             double bd, bp;
             pcg_beta(scal, bd, bp);
             const int q = 3 * i + k % 3;
-            const double v = k < 3 ? zd[q] + bd * pd[q] : zp[q] + bp * pp[q];
+            const double v = k < 3 ? pcg_dir_value(zd[q], bd, pd[q]) : pcg_dir_value(zp[q], bp, pp[q]);
             (k < 3 ? pd : pp)[q] = v;
             pv[s][k] = v;
         }

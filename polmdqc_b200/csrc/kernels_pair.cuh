@@ -559,23 +559,19 @@ __global__ void k_scaled_coeffs(int np, const ScaledPair* __restrict__ sp, const
 //   z_i = alpha_i (w r_i + sum_j T_ij s_j),  s = alpha r  (packed in s4,
 // cell order), T over the rows built by k_tu_coeffs / k_scaled_coeffs (bulk
 // pairs within usolvcut, then the scaled partners; nbru holds the partners'
-// positions in cell order).  Adds r.z of both sets to
-// rz_out[0], rz_out[1]; FIRST also starts the directions p = z.  Blocks
-// stride over the sites (a grid of a few blocks per SM), so each block adds
-// its r.z once; with `done`, the last block then takes the PCG control
-// decision (rz_out points into the scalar block at RZ_D (FIRST) or RZN_D).
-template <class R, int LPA, bool FIRST>
+// positions in cell order).  Adds r.z of both sets to scal[RZN_D..RZN_P].
+// Blocks stride over the sites (a grid of a few blocks per SM), so each block
+// adds its r.z once; the last block to finish (counted in *done, which it
+// resets) then rolls the PCG scalars (rz_old <- rz <- r.z) for the direction
+// update that follows.
+template <class R, int LPA>
 __global__ void __launch_bounds__(128) k_precond(int n, const int* __restrict__ order, const int* __restrict__ nbru, const R4<R>* __restrict__ cu0,
                                                  int cap, const int* __restrict__ nnbu,
                                                  const int* __restrict__ xoff, const R4<R>* __restrict__ s4,
                                                  const double* __restrict__ pol, double wdiag,
                                                  const double* __restrict__ rd, const double* __restrict__ rp,
                                                  double* __restrict__ zd, double* __restrict__ zp,
-                                                 double* __restrict__ pd, double* __restrict__ pp,
-                                                 R4<R>* __restrict__ p4, double* __restrict__ rz_out,
-                                                 int* __restrict__ done, int* __restrict__ iter, double thr2,
-                                                 int maxit, cudaGraphConditionalHandle h, int use_handle,
-                                                 int* __restrict__ cont_out) {
+                                                 double* __restrict__ scal, int* __restrict__ done) {
     const int lane = threadIdx.x % LPA, per_block = blockDim.x / LPA;
     double rzd = 0, rzp = 0;
     for (int g0 = blockIdx.x * per_block; g0 < n; g0 += gridDim.x * per_block) {
@@ -600,34 +596,17 @@ __global__ void __launch_bounds__(128) k_precond(int n, const int* __restrict__ 
                 const double z = a > 0 ? a * (wdiag * rv + Sv) : 0.0;
                 (dset ? zd : zp)[q] = z;
                 if (dset) rzd += rv * z; else rzp += rv * z;
-                if (FIRST) (dset ? pd : pp)[q] = z;
-            }
-        }
-        if (FIRST) {
-            // the R4 copy of p = z for the first matvec (lane 0 of the group)
-            if (g < n && lane == 0) {
-                const double a = pol[i];
-                double z[6];
-#pragma unroll
-                for (int k = 0; k < 6; k++) {
-                    const double rv = k < 3 ? rd[3 * i + k] : rp[3 * i + k - 3];
-                    z[k] = a > 0 ? a * (wdiag * rv + S[k]) : 0.0;
-                }
-                p4[2 * gs] = make_r4<R>((R)z[0], (R)z[1], (R)z[2], R(0));
-                p4[2 * gs + 1] = make_r4<R>((R)z[3], (R)z[4], (R)z[5], R(0));
             }
         }
     }
-    block_sum_add(rzd, rz_out);
-    block_sum_add(rzp, rz_out + 1);
-    // the last block to finish (counted in *done, which it resets) takes the
-    // PCG control decision: every block has added its r.z by then
-    if (done && threadIdx.x == 0) {
+    block_sum_add(rzd, scal + RZN_D);
+    block_sum_add(rzp, scal + RZN_P);
+    if (threadIdx.x == 0) {
         __threadfence();
         if (atomicAdd(done, 1) == (int)gridDim.x - 1) {
             __threadfence();
             *done = 0;
-            pcg_decide(rz_out - (FIRST ? (int)RZ_D : (int)RZN_D), iter, thr2, maxit, FIRST ? 1 : 0, h, use_handle, cont_out);
+            pcg_roll(scal);
         }
     }
 }

@@ -3,7 +3,9 @@
     python -m polmdqc_b200.profile --waters 4096 --evals 3 [--fp64]
 
 Box sizes and PME grids are those of the benchmark configurations (216, 4,096
-and 32,768 waters).  Set AMG_NO_GRAPH=1 to run the eager path, whose kernels
+and 32,768 waters), plus a 19,683-water box (27^3 lattice, the same density and
+grid spacing) whose stored pair rows (~170 MB) exceed L2 while the whole
+context stays near 1 GB: the size for multi-pass ncu captures.  Set AMG_NO_GRAPH=1 to run the eager path, whose kernels
 ncu can profile (it cannot see kernels inside graphs with conditional nodes).
 """
 import argparse
@@ -11,7 +13,7 @@ import argparse
 from . import abi, systems
 from .engine import Engine, Settings
 
-BOXES = {216: (18.643, 24), 4096: (49.7, 54), 32768: (99.3, 108)}
+BOXES = {216: (18.643, 24), 4096: (49.7, 54), 19683: (83.8, 90), 32768: (99.3, 108)}
 
 
 def main():

@@ -15,6 +15,7 @@ value = evaluations of all ranks / max-over-ranks device time.
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import os
 import statistics
@@ -120,6 +121,52 @@ def cpu_baseline_oracle(seed=0, system=None):
     return {"value": 1.0 / dt, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
             "sample": f"1 full E+F evaluation of the {WATERS}-water box, FP64, PCG to 1e-6 D ({o.pcg_iters} "
                       f"iterations), OpenMP on {os.cpu_count()} threads ({dt:.2f} s)"}
+
+
+def reference_own_mode(s, device, reps):
+    """The reference's own CPU code on the same box, in the one electrostatics
+    mode it computes: non-Ewald permanent multipoles within a 7 A cutoff
+    (empole_a, src/md/empole.cpp:96-357) through energy<CalcMode::Gradient>()
+    (src/md/energy.cpp:31), run by oracle/_ref/ref_time (the reference built
+    from its sources) on every host core.  This library runs the same mode on
+    the same coordinates (the Tinker file's 6 decimals), FP64 and mixed,
+    device-resident with L2 flushed; em is compared with the reference's."""
+    from polmdqc_b200 import abi, systems
+    from polmdqc_b200.engine import Engine, Settings
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_time")
+    prm = os.path.join(ROOT, "oracle", "_ref", "params", "water03.prm")
+    if not (os.path.exists(exe) and os.path.exists(prm)):
+        return {"unavailable": "oracle/_ref (the reference built from its sources) is not present"}
+    with tempfile.TemporaryDirectory() as d:
+        xyz, key = os.path.join(d, "box.xyz"), os.path.join(d, "box.key")
+        systems.write_tinker(s, xyz, key, prm, ["multipoleterm only", "mpole-cutoff 7.0"])
+        p = subprocess.run([exe, "--reps", "1", xyz, "-k", key], capture_output=True, text=True, timeout=900, cwd=d)
+        if p.returncode != 0:
+            return {"unavailable": f"ref_time exited {p.returncode}: {p.stderr.strip()[-200:]}"}
+        ref = json.loads(p.stdout.strip().splitlines()[-1])
+    s6 = dataclasses.replace(s, xyz=np.round(s.xyz, 6))
+    flags = abi.DO_ENERGY | abi.DO_GRADIENT
+    cpu_s = min(ref["call_s"])
+    out = {"what": "the reference's only electrostatics mode (non-Ewald permanent multipoles, cutoff 7 A, "
+                   "energy<Gradient>) on the same box: the reference's own code (oracle/_ref/ref_time) on the "
+                   "host cores beside this library in the same mode on the GPU",
+           "reference_cpu": {"seconds_per_call": cpu_s, "evals_per_s": 1.0 / cpu_s, "threads": ref["nthread"],
+                             "em": ref["em"], "kind": "reference"}}
+    for name, prec in (("fp64", abi.PREC_FP64), ("mixed", abi.PREC_MIXED)):
+        e = Engine(s6, Settings(use_ewald=False, poltyp=abi.POL_NONE, cutoff=7.0, precision=prec, device=device))
+        try:
+            g = e.forward(flags)
+            e.bench(3, flags, FLUSH_BYTES)
+            ms, _ = e.bench(reps, flags, FLUSH_BYTES)
+        finally:
+            e.close()
+        t = float(np.median(ms))
+        out["gpu_" + name] = {"ms_per_eval": t, "evals_per_s": 1000.0 / t, "em": g.em,
+                              "em_rel_diff_vs_reference": abs(g.em - ref["em"]) / abs(ref["em"]),
+                              "dem_abs_sum_rel_diff": abs(float(np.abs(g.dem).sum()) - ref["dem_abs_sum"])
+                              / ref["dem_abs_sum"],
+                              "speedup_vs_reference_cpu": cpu_s * 1000.0 / t}
+    return out
 
 
 def error_vs_oracle(s, g):
@@ -347,6 +394,7 @@ def main():
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_oracle(seed=0, system=s)
             line["mixed_error_vs_oracle"] = error_vs_oracle(s, rmx)
+            line["reference_own_mode"] = reference_own_mode(s, local, max(3, args.steps // 2))
         print(json.dumps(line), flush=True)
     eng.close()
     if dist:

@@ -29,7 +29,7 @@ CORE_OBJS = $(filter-out $(OUT)/obj/md_empole.o,$(OBJS))
 GPULIB    = polmdqc_b200/_lib/libamoeba_gpu.so
 SHIM      = polmdqc_b200/host/polmdqc_shim.cpp
 
-all: $(OUT)/libpolmdqc.a $(OUT)/libpolmdqc_noempole.a $(OUT)/ref_dump $(OUT)/data.stamp
+all: $(OUT)/libpolmdqc.a $(OUT)/libpolmdqc_noempole.a $(OUT)/ref_dump $(OUT)/ref_time $(OUT)/data.stamp
 
 # The reference's own programs with the shim in place of empole.o: the
 # drop-in demonstration (analyze_gpu, testgrad_gpu) and ref_dump_gpu, the
@@ -74,6 +74,11 @@ $(OUT)/testgrad_gpu: $(REF)/src/md/testgradExe.cpp $(SHIM) $(OUT)/libpolmdqc_noe
 # ref_dump: our own driver (oracle/ref_dump.cpp) around the reference library;
 # runs initial/getcart/mechanic/energy and prints the globals as JSON.
 $(OUT)/ref_dump: oracle/ref_dump.cpp $(OUT)/libpolmdqc.a
+	$(REFCXX) $(FLAGS) $(INC) $< $(OUT)/libpolmdqc.a -o $@
+
+# ref_time: our own timing driver (oracle/ref_time.cpp): the reference's
+# energy<Gradient>() in its only electrostatics mode, for the benchmark's CPU leg.
+$(OUT)/ref_time: oracle/ref_time.cpp $(OUT)/libpolmdqc.a
 	$(REFCXX) $(FLAGS) $(INC) $< $(OUT)/libpolmdqc.a -o $@
 
 # Parameter files and test fixtures the reference's own tests read, copied next

@@ -1,6 +1,6 @@
 """Profiling driver: a few evaluations of a seeded water box, for ncu.
 
-    python -m polmdqc_b200.profile --waters 4096 --evals 3 [--fp64]
+    python -m polmdqc_b200.profile --waters 4096 --evals 3 [--fp64] [--backward 2]
 
 Box sizes and PME grids are those of the benchmark configurations (216, 4,096
 and 32,768 waters), plus a 19,683-water box (27^3 lattice, the same density and
@@ -22,6 +22,7 @@ def main():
     ap.add_argument("--evals", type=int, default=3)
     ap.add_argument("--fp64", action="store_true")
     ap.add_argument("--bench", type=int, default=0, help="also time this many device-resident evaluations")
+    ap.add_argument("--backward", type=int, default=0, help="then this many amg_backward calls (host wall time)")
     a = ap.parse_args()
     box, grid = BOXES[a.waters]
     s = systems.water_box(a.waters, box, seed=0)
@@ -35,6 +36,13 @@ def main():
         ms, launches = e.bench(a.bench, flush_bytes=256 << 20)
         print(f"device ms per evaluation: median {sorted(ms)[len(ms) // 2]:.3f} min {ms.min():.3f} "
               f"launches {launches}")
+    if a.backward:
+        import time
+        e.backward(1.0)
+        t0 = time.perf_counter()
+        for _ in range(a.backward):
+            e.backward(1.0)
+        print(f"backward ms (host wall, synchronous): {1000.0 * (time.perf_counter() - t0) / a.backward:.3f}")
     e.close()
 
 

@@ -330,6 +330,98 @@ def _assemble_waters(O, H, ions, box_len, prm):
     return assign(np.array(xyz), np.array(types), names, bonds, mol, ff, box, True, prm)
 
 
+def prism_edges(cell_shape: int, L: float) -> np.ndarray:
+    """Edges of the orthogonal prism that encloses two cells of a truncated
+    octahedron (a cube of edge L) or a rhombic dodecahedron (L x L x sqrt(2) L:
+    the reference's image wraps z by sqrt(2) times the box length,
+    src/md/image.cpp:109-121)."""
+    return np.array([L, L, L * (math.sqrt(2.0) if cell_shape == abi.CELL_DODECAHEDRON else 1.0)])
+
+
+def cell_image(d: np.ndarray, cell_shape: int, L: float) -> np.ndarray:
+    """Minimum image of difference vectors d [m, 3] in a truncated octahedron
+    or rhombic dodecahedron of box length L, the reference's image()
+    (src/md/image.cpp:92-121) in vector form."""
+    d = np.array(d, np.float64, copy=True)
+    if cell_shape == abi.CELL_OCTAHEDRON:
+        d -= L * np.rint(d / L)
+        far = np.abs(d).sum(axis=1) > 0.75 * L
+        d[far] -= np.copysign(0.5 * L, d[far])
+        return d
+    r2 = math.sqrt(2.0)
+    d[:, :2] -= L * np.rint(d[:, :2] / L)
+    d[:, 2] -= r2 * L * np.rint(d[:, 2] / (r2 * L))
+    corr = 0.5 * L * np.floor(np.abs(d[:, 0] / L) + np.abs(d[:, 1] / L) + np.abs(r2 * d[:, 2] / L))
+    d[:, 0] -= np.copysign(corr, d[:, 0])
+    d[:, 1] -= np.copysign(corr, d[:, 1])
+    d[:, 2] -= np.copysign(corr, d[:, 2]) * r2
+    return d
+
+
+def water_cell(cell_shape: int, L: float = 24.8, seed: int = 0, jitter: float = 0.25, prm: str = "water03",
+               min_contact: float = 1.7, tries: int = 200) -> System:
+    """Rigid AMOEBA waters filling a truncated octahedron or a rhombic
+    dodecahedron of box length L.  O sit on a jittered lattice of the
+    enclosing prism (8 sites per L along x and y; 8 along z for the
+    octahedron, 12 along the dodecahedron's sqrt(2) L), one of each pair of
+    sites that the cell's centring translation (half of every prism edge)
+    exchanges, so the periodic images complete the lattice; orientations are
+    uniform random, redrawn while an atom comes within `min_contact` of
+    another molecule's atom under the cell's minimum image."""
+    edges = prism_edges(cell_shape, L)
+    nz = 12 if cell_shape == abi.CELL_DODECAHEDRON else 8
+    steps = edges / np.array([8, 8, nz])
+    grid = np.stack(np.meshgrid(np.arange(4), np.arange(8), np.arange(nz), indexing="ij"), -1).reshape(-1, 3)
+    rng = np.random.default_rng(seed)
+    O = (grid + 0.5) * steps - 0.5 * edges + rng.uniform(-jitter, jitter, (len(grid), 3))
+    orng = np.random.default_rng(seed + 1)
+    placed = np.zeros((0, 3))
+    H = np.zeros((len(O), 2, 3))
+    for w in range(len(O)):
+        for t in range(tries):
+            h = water_geometry(O[w:w + 1], random_rotations(orng, 1))[0]
+            atoms = np.vstack([O[w:w + 1], h])
+            if len(placed) == 0 or t == tries - 1:
+                break
+            d = cell_image((atoms[:, None, :] - placed[None, :, :]).reshape(-1, 3), cell_shape, L)
+            if np.min(np.einsum("ij,ij->i", d, d)) >= min_contact * min_contact:
+                break
+        H[w] = h
+        placed = np.vstack([placed, atoms])
+    s = _assemble_waters(O, H, [], L, prm)
+    s.cell_shape = cell_shape
+    return s
+
+
+def doubled_prism(s: System) -> System:
+    """The same periodic system written as an orthogonal prism holding two
+    copies of the cell (the atoms and their images under the centring
+    translation): a truncated octahedron's lattice is the cube's plus the
+    body centre, a rhombic dodecahedron's the L x L x sqrt(2) L prism's plus
+    its centre.  Every pair sum over the cell's lattice is half the prism's,
+    so the prism gives twice the cell's energies and, on each copy, the
+    cell's forces and dipoles."""
+    L = float(s.box[0])
+    edges = prism_edges(s.cell_shape, L)
+    n = s.n
+    shift = 0.5 * edges
+    xyz = np.vstack([s.xyz, s.xyz + shift])
+
+    def ax(a):
+        a = np.asarray(a)
+        return np.concatenate([a, np.where(a > 0, a + n, 0)]).astype(a.dtype)
+
+    lists = {k: [list(v) for v in vals] + [[j + n for j in v] for v in vals] for k, vals in s.lists.items()}
+    mol = np.concatenate([s.molcule, s.molcule + int(s.molcule.max()) + 1])
+    return dataclasses.replace(
+        s, n=2 * n, xyz=xyz, types=np.concatenate([s.types, s.types]), names=list(s.names) * 2,
+        bonds=[list(b) for b in s.bonds] + [[j + n for j in b] for b in s.bonds], pole=np.vstack([s.pole, s.pole]),
+        zaxis=ax(s.zaxis), xaxis=ax(s.xaxis), yaxis=ax(s.yaxis), polaxe=np.concatenate([s.polaxe, s.polaxe]),
+        molcule=mol, polarity=np.concatenate([s.polarity, s.polarity]), thole=np.concatenate([s.thole, s.thole]),
+        pdamp=np.concatenate([s.pdamp, s.pdamp]), lists=lists,
+        box=np.array([*edges, 90.0, 90.0, 90.0]), cell_shape=abi.CELL_FROM_ANGLES)
+
+
 def ion_solution(n_waters=8000, n_pairs=22, box_len=62.1, seed=0, jitter=0.3) -> System:
     """Waters plus Na+/Cl- pairs (amoebabio18 types 349/350/352/363) on a
     cubic lattice: ion sites are random lattice sites; their face neighbours

@@ -144,11 +144,12 @@ typedef struct amg_params {
                                         0 = diagonal (alpha) */
     double usolvcut;                 /* limits.h usolvcut (Angstrom), at most cutoff */
     /* Appended in ABI version 3 (zero keeps the version-2 behaviour): */
-    int32_t cell_shape;              /* AMG_CELL_*: every cell works without Ewald
-                                        (the reference's multipole mode); with Ewald
-                                        the prism cells (orthogonal, monoclinic,
-                                        triclinic) work and the octahedron and
-                                        dodecahedron return UNSUPPORTED */
+    int32_t cell_shape;              /* AMG_CELL_*: every cell works without
+                                        Ewald; with Ewald the prism cells, the
+                                        octahedron and the dodecahedron with c = a
+                                        (else UNSUPPORTED); their PME grid (nfft)
+                                        spans the enclosing prism: a^3, or
+                                        a x a x sqrt(2) a */
     double opt_coef[AMG_MAX_OPT + 1]; /* polopt.h copt: with AMG_POL_OPT the dipoles
                                         are sum_k (sum_{j>=k} copt_j) u^(k), u^(0) =
                                         alpha E, u^(k) = alpha T u^(k-1); the order is
@@ -221,8 +222,10 @@ int amg_create(const amg_params* params, amg_ctx** out);
 /* Sets coordinates [n*3] (Angstrom) and the box: a,b,c (Angstrom) and
  * alpha,beta,gamma (degrees) as boxes.h xbox,ybox,zbox,alphaA,betaA,gammaA.
  * With use_bounds, the minimum image of the cell shape (params cell_shape and
- * the angles) is the reference's image() (src/md/image.cpp:37-124).  Ewald
- * needs a prism cell: orthogonal, monoclinic or triclinic (else UNSUPPORTED). */
+ * the angles) is the reference's image() (src/md/image.cpp:37-124).  With Ewald
+ * in a truncated octahedron or rhombic dodecahedron the cell volume is half the
+ * enclosing prism's (a^3 / 2 and a^3 / sqrt(2)); the dodecahedron needs c = a,
+ * for which its image is a lattice (UNSUPPORTED otherwise). */
 int amg_set_coords(amg_ctx* ctx, const double* xyz, const double box[6]);
 
 /* Evaluates em and ep (and their gradients, analysis data, dipoles) for the
@@ -268,6 +271,27 @@ int amg_fma_peak(int32_t device, int32_t fp64, double* gflops);
  * vir array and adds each term's share from its own routine, empole / epolar,
  * virial.h).  Either pointer may be NULL. */
 int amg_last_virial(amg_ctx* ctx, double vir_em[9], double vir_ep[9]);
+
+/* Induced-dipole predictor, the reference's uprior module (include/md/uprior.h:
+ * use_pred, polpred, udalt/upalt; the reference declares it and leaves it off,
+ * src/md/initprm.cpp:396).  With a predictor set, every mutual-polarization
+ * amg_forward keeps its converged dipoles (both sets) in a history of the
+ * last AMG_PRED_STEPS evaluations on the device; once the history is full,
+ * the PCG starts from the extrapolation sum_j b_j u(n-j), j = 1..6, instead
+ * of the direct dipoles:
+ *   AMG_PRED_GEAR: b_j = (-1)^(j+1) C(6, j), the binomial (polynomial) predictor;
+ *   AMG_PRED_ASPC: b_j = (-1)^(j+1) j C(2k+4, k+2-j) / C(2k+2, k+1), k = 4, the
+ *   always stable predictor-corrector coefficients (Kolafa, J. Comput. Chem.
+ *   25, 335 (2004)).
+ * The converged dipoles do not depend on the start beyond poleps; the
+ * predictor saves PCG iterations when consecutive calls are consecutive
+ * steps of one trajectory.  Setting a predictor (or AMG_PRED_NONE) clears
+ * the history. */
+#define AMG_PRED_NONE 0
+#define AMG_PRED_GEAR 1
+#define AMG_PRED_ASPC 2
+#define AMG_PRED_STEPS 6
+int amg_set_predictor(amg_ctx* ctx, int32_t kind);
 
 /* Kernel launches of the last amg_forward, whether it ran as one captured
  * CUDA graph, and the lanes per site of the pair kernels. */

@@ -26,6 +26,7 @@ FRAME_NONE, FRAME_ZTHENX, FRAME_ZONLY, FRAME_BISECTOR, FRAME_ZBISECT, FRAME_THRE
 PREC_FP64, PREC_MIXED = 0, 1
 POL_NONE, POL_MUTUAL, POL_DIRECT, POL_OPT = 0, 1, 2, 3
 CELL_FROM_ANGLES, CELL_OCTAHEDRON, CELL_DODECAHEDRON = 0, 1, 2
+PRED_NONE, PRED_GEAR, PRED_ASPC = 0, 1, 2
 DO_ENERGY, DO_ANALYSIS, DO_GRADIENT, DO_VIRIAL, DO_DIPOLES = 1, 2, 4, 8, 16
 PEN_NONE, PEN_GORDON1, PEN_GORDON2 = 0, 1, 2
 
@@ -126,6 +127,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.amg_last_stats.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
     lib.amg_last_virial.argtypes = [C.c_void_p, _dp, _dp]
     lib.amg_fma_peak.argtypes = [C.c_int32, C.c_int32, _dp]
+    lib.amg_set_predictor.argtypes = [C.c_void_p, C.c_int32]
     lib.amg_last_error.argtypes = [C.c_void_p]
     lib.amg_last_error.restype = C.c_char_p
     lib.amg_abi_version.argtypes = []
@@ -133,7 +135,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.amg_destroy.restype = None
     for name in ("amg_create", "amg_set_coords", "amg_forward", "amg_backward", "amg_last_timing",
                  "amg_abi_version", "amg_bench", "amg_last_stats", "amg_time_tu_kernel", "amg_last_virial",
-                 "amg_fma_peak"):
+                 "amg_fma_peak", "amg_set_predictor"):
         getattr(lib, name).restype = C.c_int
     _lib = lib
     return lib

@@ -209,6 +209,14 @@ struct amg_ctx {
     double* adj_phi = nullptr;   // [3][2][n][20]
     double* adj_dpole = nullptr; // [n][13]
     double* adj_opt = nullptr;   // OPT: cotangent orders [K+1][2][3n], then P1, P2 [3n] each
+    double* adj_host = nullptr;  // pinned staging [n][25]: cotangents in (6), gradients out (19)
+    double qtot = 0;             // net charge of the last forward (Ewald)
+    // induced-dipole predictor (amg_set_predictor): history [kPredSteps][2][3n]
+    // and its device state (next slot, filled slots)
+    int pred = AMG_PRED_NONE;
+    PredCoef pred_coef{};
+    double* pred_hist = nullptr;
+    int* pred_state = nullptr;
     std::string graph_note;
     double timing[5] = {0, 0, 0, 0, 0};
     // last forward state for the adjoint
@@ -418,6 +426,11 @@ void pme_prepare(amg_ctx* ctx, Pme<R>& pm) {
                     if (!F.general) { hx = ma / ctx->box[0]; hy = mb / ctx->box[1]; hz = mc / ctx->box[2]; }
                     double h2 = hx * hx + hy * hy + hz * hz;
                     h[id] = (R)(pref * exp(-kPi * kPi * h2 / a2) / h2 / (b1[a] * b2[b] * b3[c]));
+                    // octahedron and dodecahedron: the cell's lattice is the
+                    // prism's plus its body-centring translation (half of every
+                    // edge), so its reciprocal vectors are the prism's with an
+                    // even index sum; the others cancel between the two halves
+                    if (ctx->bx.shape >= 3 && ((ma + mb + mc) & 1)) h[id] = 0;
                 }
         CK(cudaMemcpy(pm.infl, h.data(), sizeof(R) * pm.Gc, cudaMemcpyHostToDevice));
         // the same function on the full grid (even: G(m) = G(-m))
@@ -529,6 +542,11 @@ void set_frac(amg_ctx* ctx) {
     A[2][0] = ctx->box[2] * b.bcos;
     A[2][1] = ctx->box[2] * b.bterm;
     A[2][2] = ctx->box[2] * b.gterm;
+    // truncated octahedron and rhombic dodecahedron: the PME grid spans the
+    // enclosing prism (a cube; L x L x sqrt(2) L for the dodecahedron, whose
+    // image wraps z by sqrt(2) L, src/md/image.cpp:109-121) and the cell is
+    // half of it
+    if (b.shape == 4) A[2][2] *= kSqrt2;
     R[0][0] = 1 / A[0][0];
     R[1][1] = 1 / A[1][1];
     R[2][2] = 1 / A[2][2];
@@ -551,7 +569,7 @@ void cell_grid(amg_ctx* ctx, const double* hxyz) {
     if (ctx->bounds && ctx->bx.shape != 0) {
         const Box& b = ctx->bx;
         double vol = ctx->box[0] * ctx->box[1] * ctx->box[2];
-        vol *= b.shape == 1 ? b.bsin : b.shape == 2 ? b.gsin * b.gterm : 0.5;
+        vol *= b.shape == 1 ? b.bsin : b.shape == 2 ? b.gsin * b.gterm : b.shape == 3 ? 0.5 : 0.5 * kSqrt2;
         for (int a = 0; a < 3; a++) {
             cg.nc[a] = 1;
             cg.size[a] = ctx->box[a];
@@ -1208,6 +1226,23 @@ void enqueue_opt_cross(amg_ctx* ctx, cudaStream_t s, double* virp) {
 }
 
 // everything after the solve: energies, gradients, torques
+// predictor: the starting dipoles from the history (before the PCG set-up)
+// and the converged dipoles into it (after the correction sweep)
+void enqueue_predict(amg_ctx* ctx, cudaStream_t s) {
+    if (!ctx->pred) return;
+    const int n3 = 3 * ctx->n;
+    k_predict<<<nblk(n3), kThreads, 0, s>>>(n3, ctx->pred_hist, ctx->pred_state, ctx->pred_coef, ctx->ud, ctx->up);
+    KCHECK();
+}
+void enqueue_pred_store(amg_ctx* ctx, cudaStream_t s) {
+    if (!ctx->pred) return;
+    const int n3 = 3 * ctx->n;
+    k_pred_store<<<nblk(n3), kThreads, 0, s>>>(n3, ctx->pred_hist, ctx->pred_state, ctx->ud, ctx->up);
+    KCHECK();
+    k_pred_advance<<<1, 1, 0, s>>>(ctx->pred_state);
+    KCHECK();
+}
+
 template <class R>
 void enqueue_back(amg_ctx* ctx, cudaStream_t s, int flags) {
     const int n = ctx->n;
@@ -1392,6 +1427,7 @@ bool capture_graph(amg_ctx* ctx, int flags) {
             cudaGraphConditionalHandle h;
             e = cudaGraphConditionalHandleCreate(&h, graph, 0, 0);
             if (e != cudaSuccess) return fail("conditional handle", e);
+            enqueue_predict(ctx, s);
             enqueue_pcg_init<R>(ctx, s, h, 1, true);
             e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &graph, &deps, &ndeps);
             if (e != cudaSuccess) return fail("capture info", e);
@@ -1414,6 +1450,7 @@ bool capture_graph(amg_ctx* ctx, int flags) {
             e = cudaStreamEndCapture(ctx->st2, &body);
             if (e != cudaSuccess) return fail("end body capture", e);
             enqueue_sweep(ctx, s);
+            enqueue_pred_store(ctx, s);
         }
         enqueue_back<R>(ctx, s, flags);
     } catch (Fail&) {
@@ -1443,6 +1480,7 @@ void enqueue_eager(amg_ctx* ctx, int flags) {
     enqueue_front<R>(ctx, s);
     if (ctx->poltyp == AMG_POL_OPT && ctx->npolar > 0) enqueue_opt<R>(ctx, s);
     if (iterative(ctx)) {
+        enqueue_predict(ctx, s);
         enqueue_pcg_init<R>(ctx, s, 0, 0, true);
         int cont = 1;
         while (true) {
@@ -1452,6 +1490,7 @@ void enqueue_eager(amg_ctx* ctx, int flags) {
             enqueue_pcg_iter<R>(ctx, s, 0, 0);
         }
         enqueue_sweep(ctx, s);
+        enqueue_pred_store(ctx, s);
     }
     enqueue_back<R>(ctx, s, flags);
 }
@@ -1507,6 +1546,9 @@ int forward_impl(amg_ctx* ctx, int flags, amg_results* res) {
         dalloc(ctx, ctx->nbr, (size_t)ctx->cap * n);
         dalloc(ctx, ctx->cnb, (size_t)ctx->cap * n);
         ctx->graph_dirty = true;
+        // the overflowed evaluation's dipoles went into the predictor's
+        // history: start the history again
+        if (ctx->pred_state) CK(cudaMemsetAsync(ctx->pred_state, 0, 2 * sizeof(int), st));
     }
     ctx->graphed_last = ctx->use_graphs && ctx->bounds && ctx->gexec != nullptr;
     // ---- results
@@ -1531,6 +1573,7 @@ int forward_impl(amg_ctx* ctx, int flags, amg_results* res) {
     if (ctx->ewald) {
         double V = ctx->vol;
         double qt = e[3];
+        ctx->qtot = qt;
         echg = -ctx->f * kPi * qt * qt / (2 * V * ctx->aewald * ctx->aewald);
         em += echg;
     }
@@ -1597,6 +1640,7 @@ int forward_impl(amg_ctx* ctx, int flags, amg_results* res) {
 void release(amg_ctx* ctx) {
     if (ctx->rb) { cudaFreeHost(ctx->rb); ctx->rb = nullptr; }
     if (ctx->rb_grad) { cudaFreeHost(ctx->rb_grad); ctx->rb_grad = nullptr; }
+    if (ctx->adj_host) { cudaFreeHost(ctx->adj_host); ctx->adj_host = nullptr; }
     double** dbl[] = {&ctx->pole13, &ctx->pol, &ctx->thole, &ctx->pdamp, &ctx->xyz, &ctx->rp10, &ctx->Ed, &ctx->Ep,
                       &ctx->ud, &ctx->up, &ctx->rd, &ctx->rp, &ctx->zd, &ctx->zp, &ctx->pd, &ctx->pp, &ctx->Apd,
                       &ctx->App, &ctx->Fd, &ctx->Fp, &ctx->resd, &ctx->scal, &ctx->eacc, &ctx->grad_m, &ctx->grad_p,
@@ -1639,6 +1683,7 @@ void release(amg_ctx* ctx) {
     dfree(ctx->adj); dfree(ctx->adj_pot); dfree(ctx->adj_n); dfree(ctx->adj_vec); dfree(ctx->adj_phi);
     dfree(ctx->adj_dpole);
     dfree(ctx->adj_opt);
+    dfree(ctx->pred_hist); dfree(ctx->pred_state);
     dfree(ctx->pcore); dfree(ctx->palpha); dfree(ctx->dq); dfree(ctx->cfpot);
     dfree(ctx->bonds); dfree(ctx->bflux); dfree(ctx->angles); dfree(ctx->aflux);
     if (ctx->st) { cudaStreamDestroy(ctx->st); ctx->st = nullptr; }
@@ -1928,7 +1973,26 @@ __global__ void k_scale3(int n, const double* __restrict__ pol, const double* __
     for (int c = 0; c < 3; c++) w[3 * i + c] = pol[i] * g[3 * i + c];
 }
 
-// amg_backward: FP64 throughout (see kernels_adjoint.cuh for the algebra)
+// the adjoint solve A w = g for both right-hand sides, as the forward solves
+// A u = E: PCG in the context's precision on the forward's stored coefficient
+// rows and grids (same coordinates), then the FP64 correction sweep.  The
+// caller has pointed the context's field and dipole vectors at g and w, with
+// w = alpha g as the starting guess.
+template <class R>
+void adjoint_solve(amg_ctx* ctx, cudaStream_t s) {
+    enqueue_pcg_init<R>(ctx, s, 0, 0, true);
+    int cont = 1;
+    while (true) {
+        CK(cudaMemcpyAsync(&cont, ctx->cont, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (!cont) break;
+        enqueue_pcg_iter<R>(ctx, s, 0, 0);
+    }
+    enqueue_sweep(ctx, s);
+}
+
+// amg_backward: the adjoint solve in the context's precision (above), every
+// other term in FP64 (see kernels_adjoint.cuh for the algebra)
 int backward_impl(amg_ctx* ctx, const amg_cotangents* cot, amg_param_grads* gr) {
     const int n = ctx->n;
     cudaStream_t s = ctx->st;
@@ -1940,6 +2004,7 @@ int backward_impl(amg_ctx* ctx, const amg_cotangents* cot, amg_param_grads* gr) 
         dalloc(ctx, ctx->adj_vec, 5 * (size_t)n);
         dalloc(ctx, ctx->adj_phi, 3 * 2 * 20 * (size_t)n);
         dalloc(ctx, ctx->adj_dpole, 13 * (size_t)n);
+        CK(cudaMallocHost((void**)&ctx->adj_host, sizeof(double) * 25 * (size_t)n));
     }
     double *gd = ctx->adj, *gp = gd + n3, *wd = gp + n3, *wp = wd + n3, *bd = wp + n3, *bp = bd + n3,
            *vbar = bp + n3, *mwp = vbar + n3, *grad = mwp + n3, *trq = grad + n3, *zeros = trq + n3;
@@ -1963,14 +2028,12 @@ int backward_impl(amg_ctx* ctx, const amg_cotangents* cot, amg_param_grads* gr) 
     KCHECK();
     if (have_g && ctx->has_pol) {
         // adjoint solve A w = g for both right-hand sides (the forward's PCG)
-        std::vector<double> h(n3, 0.0);
-        if (cot->d_uind) std::memcpy(h.data(), cot->d_uind, sizeof(double) * n3);
-        CK(cudaMemcpyAsync(gd, h.data(), sizeof(double) * n3, cudaMemcpyHostToDevice, s));
-        CK(cudaStreamSynchronize(s));
-        std::fill(h.begin(), h.end(), 0.0);
-        if (cot->d_uinp) std::memcpy(h.data(), cot->d_uinp, sizeof(double) * n3);
-        CK(cudaMemcpyAsync(gp, h.data(), sizeof(double) * n3, cudaMemcpyHostToDevice, s));
-        CK(cudaStreamSynchronize(s));
+        double* hg = ctx->adj_host;  // both cotangents through the pinned staging buffer
+        if (cot->d_uind) std::memcpy(hg, cot->d_uind, sizeof(double) * n3);
+        else std::fill(hg, hg + n3, 0.0);
+        if (cot->d_uinp) std::memcpy(hg + n3, cot->d_uinp, sizeof(double) * n3);
+        else std::fill(hg + n3, hg + 2 * n3, 0.0);
+        CK(cudaMemcpyAsync(gd, hg, sizeof(double) * 2 * n3, cudaMemcpyHostToDevice, s));  // gp follows gd
         if (ctx->poltyp == AMG_POL_DIRECT) {
             k_scale3<<<nblk(n), kThreads, 0, s>>>(n, ctx->pol, gd, wd);
             KCHECK();
@@ -1995,7 +2058,6 @@ int backward_impl(amg_ctx* ctx, const amg_cotangents* cot, amg_param_grads* gr) 
             k_opt_combine<<<nblk(n3), kThreads, 0, s>>>((int)n3, K, ctx->copm, wo, wd, wp);
             KCHECK();
         } else if (iter) {
-            ensure_coeff_buffers<double>(ctx, atoms_of<double>(ctx));
             double *Ed = ctx->Ed, *Ep = ctx->Ep, *ud = ctx->ud, *up = ctx->up;
             ctx->Ed = gd; ctx->Ep = gp; ctx->ud = wd; ctx->up = wp;
             int guess = ctx->guess;
@@ -2006,14 +2068,10 @@ int backward_impl(amg_ctx* ctx, const amg_cotangents* cot, amg_param_grads* gr) 
             KCHECK();
             bool ok = true;
             try {
-                enqueue_pcg_init<double>(ctx, s, 0, 0, false);
-                int cont = 1;
-                while (true) {
-                    CK(cudaMemcpyAsync(&cont, ctx->cont, sizeof(int), cudaMemcpyDeviceToHost, s));
-                    CK(cudaStreamSynchronize(s));
-                    if (!cont) break;
-                    enqueue_pcg_iter<double>(ctx, s, 0, 0);
-                }
+                if (ctx->prec == AMG_PREC_MIXED)
+                    adjoint_solve<float>(ctx, s);
+                else
+                    adjoint_solve<double>(ctx, s);
             } catch (Fail&) {
                 ok = false;
             }
@@ -2074,10 +2132,7 @@ int backward_impl(amg_ctx* ctx, const amg_cotangents* cot, amg_param_grads* gr) 
                                                      ph + blk + one, vbar, bd, ctx->ud, mwp, ctx->up, mutual,
                                                      self_coef(ctx), ctx->aewald, cf, grad, trq, ctx->adj_pot);
         KCHECK();
-        std::vector<double> r10(10 * (size_t)n);
-        CK(cudaMemcpyAsync(r10.data(), ctx->rp10, sizeof(double) * 10 * n, cudaMemcpyDeviceToHost, s));
-        CK(cudaStreamSynchronize(s));
-        for (int i = 0; i < n; i++) qtot += r10[10 * (size_t)i];
+        qtot = ctx->qtot;  // the forward's net charge (monopoles do not rotate)
     }
     if (opt) {
         // OPT dipole-dipole terms: the pairs (-V1_b, u_d^(b)) and (-V2_b,
@@ -2127,30 +2182,28 @@ int backward_impl(amg_ctx* ctx, const amg_cotangents* cot, amg_param_grads* gr) 
     k_pole_grad_local<<<nblk(n), kThreads, 0, s>>>(n, ctx->xyz, ctx->pole13, ctx->zax, ctx->xax, ctx->yax, ctx->axe,
                                                    ctx->adj_pot, ctx->adj_dpole);
     KCHECK();
-    std::vector<double> hx(n3), hpole(13 * (size_t)n), hn(3 * (size_t)n), hpol(n), hpd(n);
-    CK(cudaMemcpyAsync(hx.data(), grad, sizeof(double) * n3, cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(hpole.data(), ctx->adj_dpole, sizeof(double) * 13 * n, cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(hn.data(), dpd, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(hpol.data(), ctx->pol, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(hpd.data(), ctx->pdamp, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
     // net-charge term of the Ewald energy, -f pi Q^2 / (2 V alpha^2): dq_i
     double dq = 0;
     if (ctx->ewald) {
         double V = ctx->vol;
         dq = -cf * kPi * qtot / (V * ctx->aewald * ctx->aewald);
     }
-    if (gr->d_xyz) std::memcpy(gr->d_xyz, hx.data(), sizeof(double) * n3);
-    if (gr->d_pole)
-        for (int i = 0; i < n; i++)
-            for (int k = 0; k < 13; k++) gr->d_pole[13 * (size_t)i + k] = hpole[13 * (size_t)i + k] + (k == 0 ? dq : 0.0);
-    for (int i = 0; i < n; i++) {
-        double dpd_i = hn[i], dth_i = hn[n + i], dpol_i = hn[2 * n + i];
-        // pdamp = alpha^(1/6): dpdamp/dalpha = pdamp / (6 alpha)
-        double chain = hpol[i] > 0 ? hpd[i] / (6.0 * hpol[i]) : 0.0;
-        if (gr->d_polarity) gr->d_polarity[i] = ctx->has_pol ? dpol_i + dpd_i * chain : 0.0;
-        if (gr->d_thole) gr->d_thole[i] = ctx->has_pol ? dth_i : 0.0;
-    }
+    k_adj_finish<<<nblk(n), kThreads, 0, s>>>(n, dq, ctx->has_pol ? 1 : 0, ctx->pol, ctx->pdamp, dpd, dth, dpol,
+                                              ctx->adj_dpole);
+    KCHECK();
+    // outputs through the pinned staging buffer: d_xyz [3n], d_pole [13n],
+    // d_thole [n], d_polarity [n]
+    double* h = ctx->adj_host;
+    double *hx = h, *hpole = h + n3, *hth = hpole + 13 * (size_t)n, *hpol = hth + n;
+    if (gr->d_xyz) CK(cudaMemcpyAsync(hx, grad, sizeof(double) * n3, cudaMemcpyDeviceToHost, s));
+    if (gr->d_pole) CK(cudaMemcpyAsync(hpole, ctx->adj_dpole, sizeof(double) * 13 * n, cudaMemcpyDeviceToHost, s));
+    if (gr->d_thole) CK(cudaMemcpyAsync(hth, dth, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+    if (gr->d_polarity) CK(cudaMemcpyAsync(hpol, dpol, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (gr->d_xyz) std::memcpy(gr->d_xyz, hx, sizeof(double) * n3);
+    if (gr->d_pole) std::memcpy(gr->d_pole, hpole, sizeof(double) * 13 * n);
+    if (gr->d_thole) std::memcpy(gr->d_thole, hth, sizeof(double) * n);
+    if (gr->d_polarity) std::memcpy(gr->d_polarity, hpol, sizeof(double) * n);
     return AMG_OK;
 }
 
@@ -2192,8 +2245,15 @@ int amg_set_coords(amg_ctx* ctx, const double* xyz, const double box[6]) {
             }
             Box nb = ctx->bx;
             if (!set_lattice(ctx, box, nb)) return AMG_ERR_BAD_ARG;
-            if (ctx->ewald && nb.shape > 2) {
-                ctx->err = "Ewald needs a prism cell (orthogonal, monoclinic or triclinic)";
+            // The dodecahedron's image (src/md/image.cpp:111-121) wraps z by
+            // sqrt(2) c and moves corners by (a/2, a/2, c/sqrt(2)): a lattice
+            // (the face-centred one whose cell is the rhombic dodecahedron)
+            // only when c = a.  The reference's unitcell() sets c = sqrt(2) a
+            // (src/md/unitcell.cpp:148), for which these translations form no
+            // lattice and no Ewald sum exists; without Ewald the image is used
+            // as it stands.
+            if (ctx->ewald && nb.shape == 4 && std::fabs(box[2] - box[0]) > 1e-9 * box[0]) {
+                ctx->err = "Ewald in a rhombic dodecahedron needs c = a (its minimum image is a lattice only then)";
                 return AMG_ERR_UNSUPPORTED;
             }
             if (nb.shape != ctx->bx.shape) ctx->graph_dirty = true;
@@ -2481,6 +2541,42 @@ int amg_last_virial(amg_ctx* ctx, double vir_em[9], double vir_ep[9]) {
 int amg_last_timing(amg_ctx* ctx, double ms[5]) {
     if (!ctx || !ms) return AMG_ERR_BAD_ARG;
     for (int k = 0; k < 5; k++) ms[k] = ctx->timing[k];
+    return AMG_OK;
+}
+
+int amg_set_predictor(amg_ctx* ctx, int32_t kind) {
+    if (!ctx) return AMG_ERR_BAD_ARG;
+    if (kind != AMG_PRED_NONE && kind != AMG_PRED_GEAR && kind != AMG_PRED_ASPC) {
+        ctx->err = "unknown predictor";
+        return AMG_ERR_BAD_ARG;
+    }
+    static_assert(kPredSteps == AMG_PRED_STEPS, "predictor history length");
+    try {
+        CK(cudaSetDevice(ctx->device));
+        // b_j, j = 1..6: Gear's binomial extrapolation (-1)^(j+1) C(6, j); ASPC
+        // (Kolafa 2004) (-1)^(j+1) j C(2k+4, k+2-j) / C(2k+2, k+1), k = 4
+        auto binom = [](int a, int b) {
+            double r = 1;
+            for (int i = 1; i <= b; i++) r = r * (a - b + i) / i;
+            return r;
+        };
+        const int k = kPredSteps - 2;
+        for (int j = 1; j <= kPredSteps; j++) {
+            const double sgn = (j % 2) ? 1.0 : -1.0;
+            ctx->pred_coef.b[j - 1] = kind == AMG_PRED_GEAR ? sgn * binom(kPredSteps, j)
+                                                            : sgn * j * binom(2 * k + 4, k + 2 - j) / binom(2 * k + 2, k + 1);
+        }
+        if (kind != AMG_PRED_NONE && !ctx->pred_hist) {
+            dalloc(ctx, ctx->pred_hist, (size_t)kPredSteps * 2 * 3 * ctx->n);
+            dalloc(ctx, ctx->pred_state, 2);
+        }
+        if (ctx->pred_state) CK(cudaMemsetAsync(ctx->pred_state, 0, 2 * sizeof(int), ctx->st));
+        ctx->pred = kind;
+        ctx->graph_dirty = true;
+        CK(cudaStreamSynchronize(ctx->st));
+    } catch (Fail& f) {
+        return f.code;
+    }
     return AMG_OK;
 }
 

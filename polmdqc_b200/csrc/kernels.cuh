@@ -13,6 +13,7 @@
 namespace amg {
 
 constexpr double kPi = 3.141592653589793238462643383279502884;
+constexpr double kSqrt2 = 1.414213562373095048801688724209698079;
 constexpr double kSqrtPi = 1.772453850905516027298167483341145183;
 
 template <class R>

@@ -455,4 +455,22 @@ __global__ void k_pole_grad_local(int n, const double* __restrict__ xyz, const d
     for (int k = 0; k < 13; k++) dpole[13 * (size_t)i + k] = out[k];
 }
 
+// the net-charge term's share of each monopole gradient and the chain
+// through pdamp = alpha^(1/6) (dpdamp/dalpha = pdamp / (6 alpha)), in place:
+// dpole[13 i] += dq, dpol[i] <- dpol + dpd * chain (0 without polarization)
+__global__ void k_adj_finish(int n, double dq, int has_pol, const double* __restrict__ pol,
+                             const double* __restrict__ pdamp, const double* __restrict__ dpd, double* __restrict__ dth,
+                             double* __restrict__ dpol, double* __restrict__ dpole) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    dpole[13 * (size_t)i] += dq;
+    if (!has_pol) {
+        dpol[i] = 0;
+        dth[i] = 0;
+        return;
+    }
+    const double chain = pol[i] > 0 ? pdamp[i] / (6.0 * pol[i]) : 0.0;
+    dpol[i] += dpd[i] * chain;
+}
+
 }  // namespace amg

@@ -598,4 +598,46 @@ __device__ __forceinline__ void torque_site(int i, const double* __restrict__ xy
     }
 }
 
+// ------------------------------------------------------------ predictor
+// History of converged dipoles: slots [kPredSteps][2][3n] (u_d then u_p),
+// state[0] = the slot the next evaluation writes, state[1] = filled slots.
+constexpr int kPredSteps = 6;
+struct PredCoef {
+    double b[kPredSteps];  // b[j-1] multiplies the dipoles of evaluation n-j
+};
+
+// starting dipoles sum_j b_j u(n-j) once the history is full (else the
+// direct dipoles already in ud/up stay)
+__global__ void k_predict(int n3, const double* __restrict__ hist, const int* __restrict__ state, PredCoef c,
+                          double* __restrict__ ud, double* __restrict__ up) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n3 || state[1] < kPredSteps) return;
+    const int next = state[0];
+    double vd = 0, vp = 0;
+#pragma unroll
+    for (int j = 1; j <= kPredSteps; j++) {
+        const int slot = (next - j + kPredSteps) % kPredSteps;
+        const double* h = hist + (size_t)slot * 2 * n3;
+        vd += c.b[j - 1] * h[t];
+        vp += c.b[j - 1] * h[n3 + t];
+    }
+    ud[t] = vd;
+    up[t] = vp;
+}
+
+// the converged dipoles into the next slot
+__global__ void k_pred_store(int n3, double* __restrict__ hist, const int* __restrict__ state,
+                             const double* __restrict__ ud, const double* __restrict__ up) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n3) return;
+    double* h = hist + (size_t)state[0] * 2 * n3;
+    h[t] = ud[t];
+    h[n3 + t] = up[t];
+}
+
+__global__ void k_pred_advance(int* __restrict__ state) {
+    state[0] = (state[0] + 1) % kPredSteps;
+    state[1] = min(state[1] + 1, kPredSteps);
+}
+
 }  // namespace amg

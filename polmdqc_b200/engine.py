@@ -217,6 +217,10 @@ class Engine:
         out["d_xyz"] = out["d_xyz"].reshape(self.n, 3)
         return out
 
+    def set_predictor(self, kind):
+        """Induced-dipole predictor (abi.PRED_*); clears the dipole history."""
+        self._check(self.lib.amg_set_predictor(self.ctx, kind), "amg_set_predictor")
+
     def bench(self, steps, flags=abi.DO_ENERGY | abi.DO_GRADIENT, flush_bytes=0):
         """Device-resident evaluations: per-step ms (CUDA events) and the
         number of this library's kernel launches."""

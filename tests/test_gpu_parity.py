@@ -99,13 +99,32 @@ def test_waterbox30_cell_shapes_golden(case, shape, prec):
         assert abs(r.einter - g["einter"]) < 1e-4 * scale
 
 
-def test_ewald_needs_a_prism_cell():
-    """Ewald runs in orthogonal, monoclinic and triclinic cells; the truncated
-    octahedron and rhombic dodecahedron return UNSUPPORTED."""
+def test_ewald_in_the_reference_octahedron():
+    """The reference's bounds-4 input (its waterbox30 coordinates read as a
+    truncated octahedron of box length 30) with Ewald, cutoff 9: em and its
+    gradient are half those of the same system written as the enclosing cube
+    with two copies of the cell, which the oracle evaluates with its
+    orthogonal Ewald and PME on the same 32^3 grid."""
     d = ref_dump(ref_fixture("bounds", "waterbox30.xyz"), ref_fixture("bounds", "octahedron.key"))
     s = systems.from_dump(d)
+    st = Settings(nfft=(32, 32, 32), cutoff=9.0, poltyp=abi.POL_NONE, precision=FP64)
+    g = run(s, st, abi.DO_ENERGY | abi.DO_GRADIENT)
+    o = oracle.forward(systems.doubled_prism(s), st, flags=abi.DO_ENERGY | abi.DO_GRADIENT)
+    assert abs(g.em - o.em / 2) < 1e-10 * abs(o.em / 2), (g.em, o.em / 2)
+    # the cube's coordinates read as an octahedron bring image atoms nearly on
+    # top of each other (gradients up to 2e6 kcal/mol/A): relative bound
+    od = o.dem.reshape(-1, 3)[:s.n]
+    np.testing.assert_allclose(g.dem, od, atol=1e-10 * np.abs(od).max(), rtol=0)
+
+
+def test_ewald_in_the_reference_dodecahedron_is_refused():
+    """The reference's bounds-5 dodecahedron has c = sqrt(2) a (its unitcell()),
+    for which its minimum image is no lattice: Ewald returns UNSUPPORTED
+    (the non-Ewald bounds-5 golden above uses the image as it stands)."""
+    d = ref_dump(ref_fixture("bounds", "waterbox30.xyz"), ref_fixture("bounds", "dodecahedron.key"))
+    s = systems.from_dump(d)
     with pytest.raises(AmgError, match="UNSUPPORTED"):
-        run(s, Settings(nfft=(32, 32, 32), cutoff=9.0, poltyp=abi.POL_NONE))
+        run(s, Settings(nfft=(32, 32, 48), cutoff=9.0, poltyp=abi.POL_NONE))
 
 
 @pytest.mark.parametrize("prec", [FP64, MIXED])

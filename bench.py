@@ -84,16 +84,17 @@ class Clocks:
                 "samples": len(rows)}
 
 
-def ncu_traffic(kernel):
+def ncu_traffic(kernel, pairs):
     """DRAM bytes (read + write) per launch of `kernel` on this workload from
-    the committed ncu capture summary, or None."""
+    the committed ncu capture summary, or None.  The capture is of a smaller
+    box (the headline box is too large for a multi-pass capture); its traffic
+    is scaled to this launch by the directed pairs each processes, the unit
+    the kernel's bytes grow with."""
     try:
         with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
             d = json.load(f)[kernel]
-        if d.get("waters") != WATERS:      # a capture of another box does not apply
-            return None
-        return d["dram_bytes_read"] + d["dram_bytes_write"]
-    except (OSError, KeyError):
+        return (d["dram_bytes_read"] + d["dram_bytes_write"]) * pairs / d["directed_pairs"]
+    except (OSError, KeyError, ZeroDivisionError):
         return None
 
 
@@ -371,7 +372,7 @@ def main():
         achieved = tu_bytes / (tu_ms * 1e-3) / 1e9
         roofline = {"kernel": "k_tu_stored (PCG real-space T.u, stored pair coefficients)", "bound": "hbm",
                     "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                    "frac": achieved / peaks["hbm_gbs"], "traffic": ncu_traffic("k_tu_stored"),
+                    "frac": achieved / peaks["hbm_gbs"], "traffic": ncu_traffic("k_tu_stored", tu_pairs),
                     "bytes_per_launch": tu_bytes, "directed_pairs": tu_pairs, "avg_launch_ms": tu_ms,
                     "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({src}); L2 flushed before each timed launch"}
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

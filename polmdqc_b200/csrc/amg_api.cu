@@ -1957,14 +1957,42 @@ int validate(const amg_params* P, std::string& why) {
     return AMG_OK;
 }
 
-__global__ void k_adj_pack(int n, const double* __restrict__ vbar, const double* __restrict__ p1,
-                           const double* __restrict__ q1, const double* __restrict__ p2,
-                           const double* __restrict__ q2, double4* __restrict__ vec) {
+// the adjoint pair kernel's five vectors of site i, in precision R, at the
+// site's cell-order position rank[i]
+template <class R>
+__global__ void k_adj_pack(int n, const int* __restrict__ rank, const double* __restrict__ vbar,
+                           const double* __restrict__ p1, const double* __restrict__ q1, const double* __restrict__ p2,
+                           const double* __restrict__ q2, R4<R>* __restrict__ vec) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double* src[5] = {vbar, p1, q1, p2, q2};
+    const size_t o = 5 * (size_t)rank[i];
     for (int k = 0; k < 5; k++)
-        vec[5 * (size_t)i + k] = make_double4(src[k][3 * i], src[k][3 * i + 1], src[k][3 * i + 2], 0.0);
+        vec[o + k] = make_r4<R>((R)src[k][3 * i], (R)src[k][3 * i + 1], (R)src[k][3 * i + 2], R(0));
+}
+
+// bulk real-space adjoint pairs in precision R (the forward's pair
+// precision): the vectors packed in cell order, then the pair kernel
+template <class R>
+void adjoint_pairs(amg_ctx* ctx, cudaStream_t s, const double* vbar, const double* p1, const double* q1,
+                   const double* p2, const double* q2, int mutual, double cm, double* grad, double* trq,
+                   double* dpd, double* dth) {
+    const int n = ctx->n;
+    Atoms<R>& A = atoms_of<R>(ctx);
+    R4<R>* vec = reinterpret_cast<R4<R>*>(ctx->adj_vec);  // [n][5] double4 of room
+    k_adj_pack<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->rank, vbar, p1, q1, p2, q2, vec);
+    KCHECK();
+    LPA_DISPATCH(ctx->lpa, {
+        if (ctx->ewald)
+            k_adjoint_pair<R, true, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(
+                n, ctx->sids, A.atS, vec, ctx->bx, (R)ctx->aewald, ctx->cnb, ctx->cap, ctx->nnb, mutual, cm, grad, trq,
+                ctx->adj_pot, dpd, dth);
+        else
+            k_adjoint_pair<R, false, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(
+                n, ctx->sids, A.atS, vec, ctx->bx, R(0), ctx->cnb, ctx->cap, ctx->nnb, mutual, cm, grad, trq,
+                ctx->adj_pot, dpd, dth);
+    });
+    KCHECK();
 }
 
 __global__ void k_scale3(int n, const double* __restrict__ pol, const double* __restrict__ g, double* __restrict__ w) {
@@ -2092,8 +2120,6 @@ int backward_impl(amg_ctx* ctx, const amg_cotangents* cot, amg_param_grads* gr) 
         k_opt_adj_diag<<<nblk(n), kThreads, 0, s>>>(n, K, ctx->copm, cf, ctx->pol, ctx->adj_opt, ctx->uopt, dpol);
         KCHECK();
     }
-    k_adj_pack<<<nblk(n), kThreads, 0, s>>>(n, vbar, bd, ctx->ud, mwp, ctx->up, ctx->adj_vec);
-    KCHECK();
     k_zero<double><<<nblk(2 * n3, 256), 256, 0, s>>>(grad, 2 * n3);
     KCHECK();
     k_zero<double><<<nblk(10 * (size_t)n, 256), 256, 0, s>>>(ctx->adj_pot, 10 * (size_t)n);
@@ -2101,17 +2127,16 @@ int backward_impl(amg_ctx* ctx, const amg_cotangents* cot, amg_param_grads* gr) 
     k_zero<double><<<nblk(2 * (size_t)n, 256), 256, 0, s>>>(dpd, 2 * (size_t)n);
     KCHECK();
     const int mutual = ctx->poltyp == AMG_POL_MUTUAL;
-    LPA_DISPATCH(ctx->lpa, {
-        if (ctx->ewald)
-            k_adjoint_pair<true, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(
-                n, ctx->sids, ctx->ad.at, ctx->adj_vec, ctx->bx, ctx->aewald, ctx->nbr, ctx->cap, ctx->nnb, mutual, cf, grad, trq,
-                ctx->adj_pot, dpd, dth);
-        else
-            k_adjoint_pair<false, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(
-                n, ctx->sids, ctx->ad.at, ctx->adj_vec, ctx->bx, 0.0, ctx->nbr, ctx->cap, ctx->nnb, mutual, cf, grad, trq,
-                ctx->adj_pot, dpd, dth);
-    });
-    KCHECK();
+    const bool mixed = ctx->prec == AMG_PREC_MIXED;
+    // potentials (and derivatives, 20) of two dipole sets from the PME grid
+    auto adj_pme = [&](const double* a, const double* b, double* ph) {
+        if (mixed) pme_dipoles<float, 20>(ctx, s, a, b, ph);
+        else pme_dipoles<double, 20>(ctx, s, a, b, ph);
+    };
+    if (mixed)
+        adjoint_pairs<float>(ctx, s, vbar, bd, ctx->ud, mwp, ctx->up, mutual, cf, grad, trq, dpd, dth);
+    else
+        adjoint_pairs<double>(ctx, s, vbar, bd, ctx->ud, mwp, ctx->up, mutual, cf, grad, trq, dpd, dth);
     if (ctx->nsp) {
         k_adjoint_scaled<<<nblk(ctx->nsp), kThreads, 0, s>>>(ctx->nsp, ctx->sp, ctx->xyz, ctx->rp10, ctx->pdamp,
                                                             ctx->thole, ctx->bx, ctx->cut * ctx->cut, ewald_alpha(ctx),
@@ -2121,12 +2146,15 @@ int backward_impl(amg_ctx* ctx, const amg_cotangents* cot, amg_param_grads* gr) 
     }
     double qtot = 0;
     if (ctx->ewald) {
-        pme_mpole<double>(ctx, s);  // FP64 permanent potentials (overwrites the forward's phiM)
+        // permanent potentials (overwrite the forward's phiM), in the forward's
+        // grid precision like the dipole potentials below
+        if (mixed) pme_mpole<float>(ctx, s);
+        else pme_mpole<double>(ctx, s);
         double* ph = ctx->adj_phi;
         const size_t blk = 2 * 20 * (size_t)n;
-        pme_dipoles<double, 20>(ctx, s, vbar, bd, ph);              // phi of vbar, P1
-        pme_dipoles<double, 20>(ctx, s, ctx->ud, ctx->up, ph + blk);  // phi of Q1, Q2
-        pme_dipoles<double, 20>(ctx, s, mwp, zeros, ph + 2 * blk);    // phi of P2
+        adj_pme(vbar, bd, ph);              // phi of vbar, P1
+        adj_pme(ctx->ud, ctx->up, ph + blk);  // phi of Q1, Q2
+        adj_pme(mwp, zeros, ph + 2 * blk);    // phi of P2
         const size_t one = 20 * (size_t)n;
         k_adjoint_recip<<<nblk(n), kThreads, 0, s>>>(n, ctx->rp10, ctx->phiM, ph, ph + one, ph + blk, ph + 2 * blk,
                                                      ph + blk + one, vbar, bd, ctx->ud, mwp, ctx->up, mutual,
@@ -2145,19 +2173,10 @@ int backward_impl(amg_ctx* ctx, const amg_cotangents* cot, amg_param_grads* gr) 
             const double* Q2 = Q1 + n3;
             k_opt_adj_cross<<<nblk(n3), kThreads, 0, s>>>((int)n3, K, b, ctx->copm, cf, ctx->adj_opt, ctx->uopt, P1, P2);
             KCHECK();
-            k_adj_pack<<<nblk(n), kThreads, 0, s>>>(n, zeros, P1, Q1, P2, Q2, ctx->adj_vec);
-            KCHECK();
-            LPA_DISPATCH(ctx->lpa, {
-                if (ctx->ewald)
-                    k_adjoint_pair<true, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(
-                        n, ctx->sids, ctx->ad.at, ctx->adj_vec, ctx->bx, ctx->aewald, ctx->nbr, ctx->cap, ctx->nnb, 1,
-                        0.0, grad, trq, ctx->adj_pot, dpd, dth);
-                else
-                    k_adjoint_pair<false, L><<<nblk((size_t)n * L), kThreads, 0, s>>>(
-                        n, ctx->sids, ctx->ad.at, ctx->adj_vec, ctx->bx, 0.0, ctx->nbr, ctx->cap, ctx->nnb, 1, 0.0,
-                        grad, trq, ctx->adj_pot, dpd, dth);
-            });
-            KCHECK();
+            if (mixed)
+                adjoint_pairs<float>(ctx, s, zeros, P1, Q1, P2, Q2, 1, 0.0, grad, trq, dpd, dth);
+            else
+                adjoint_pairs<double>(ctx, s, zeros, P1, Q1, P2, Q2, 1, 0.0, grad, trq, dpd, dth);
             if (ctx->nsp) {
                 k_adjoint_scaled<<<nblk(ctx->nsp), kThreads, 0, s>>>(
                     ctx->nsp, ctx->sp, ctx->xyz, ctx->rp10, ctx->pdamp, ctx->thole, ctx->bx, ctx->cut * ctx->cut,
@@ -2167,9 +2186,9 @@ int backward_impl(amg_ctx* ctx, const amg_cotangents* cot, amg_param_grads* gr) 
             if (ctx->ewald) {
                 double* ph = ctx->adj_phi;
                 const size_t blk = 2 * 20 * (size_t)n, one = 20 * (size_t)n;
-                pme_dipoles<double, 20>(ctx, s, zeros, P1, ph);
-                pme_dipoles<double, 20>(ctx, s, Q1, Q2, ph + blk);
-                pme_dipoles<double, 20>(ctx, s, P2, zeros, ph + 2 * blk);
+                adj_pme(zeros, P1, ph);
+                adj_pme(Q1, Q2, ph + blk);
+                adj_pme(P2, zeros, ph + 2 * blk);
                 k_adjoint_recip<<<nblk(n), kThreads, 0, s>>>(n, ctx->rp10, ctx->phiM, ph, ph + one, ph + blk,
                                                              ph + 2 * blk, ph + blk + one, zeros, P1, Q1, P2, Q2, 1,
                                                              self_coef(ctx), ctx->aewald, 0.0, grad, trq, ctx->adj_pot);

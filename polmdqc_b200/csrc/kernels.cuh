@@ -202,6 +202,41 @@ __device__ __forceinline__ R4<R> load_stream(const R4<R>* p) {
     }
 }
 
+// The two vectors v4[2j], v4[2j+1] of partner j (adjacent, 32-byte aligned:
+// the arrays come from cudaMalloc) with 256-bit loads: one request for both
+// FP32 vectors, two for the FP64 ones, instead of one per 16 bytes.  Read
+// through the non-coherent path: the kernels using it never write v4.
+__device__ __forceinline__ void load_pair(const float4* __restrict__ v4, int j, float4& d, float4& p) {
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(d.x), "=f"(d.y), "=f"(d.z), "=f"(d.w), "=f"(p.x), "=f"(p.y), "=f"(p.z), "=f"(p.w)
+        : "l"(v4 + 2 * (size_t)j));
+}
+__device__ __forceinline__ void load_pair(const double4* __restrict__ v4, int j, double4& d, double4& p) {
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+        : "=d"(d.x), "=d"(d.y), "=d"(d.z), "=d"(d.w)
+        : "l"(v4 + 2 * (size_t)j));
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+        : "=d"(p.x), "=d"(p.y), "=d"(p.z), "=d"(p.w)
+        : "l"(v4 + 2 * (size_t)j + 1));
+}
+
+// One site's packed data (64 bytes in FP32, 128 in FP64; 32-byte aligned)
+// with 256-bit loads, for the pair kernels' partner gathers (read-only there).
+__device__ __forceinline__ AtomR<float> ld_atom(const AtomR<float>* __restrict__ at, int j) {
+    AtomR<float> A;
+    const float4* p = reinterpret_cast<const float4*>(at + j);
+    load_pair(p, 0, A.a, A.b);
+    load_pair(p, 1, A.c, A.e);
+    return A;
+}
+__device__ __forceinline__ AtomR<double> ld_atom(const AtomR<double>* __restrict__ at, int j) {
+    AtomR<double> A;
+    const double4* p = reinterpret_cast<const double4*>(at + j);
+    load_pair(p, 0, A.a, A.b);
+    load_pair(p, 1, A.c, A.e);
+    return A;
+}
+
 // Sum of T v over one stored row (cnt slots from `base`; partner indices and
 // packed coefficients side by side) for two vector sets v4[2j], v4[2j+1],
 // the row's LPA lanes taking every LPA-th slot.  Software-pipelined: the next
@@ -235,10 +270,7 @@ __device__ __forceinline__ void row_apply(const int* __restrict__ idx, const R4<
         }
         R4<R> vd[U], vp[U];
 #pragma unroll
-        for (int q = 0; q < U; q++) {
-            vd[q] = v4[2 * j[q]];
-            vp[q] = v4[2 * j[q] + 1];
-        }
+        for (int q = 0; q < U; q++) load_pair(v4, j[q], vd[q], vp[q]);
         fetch(s0 + U * LPA);
 #pragma unroll
         for (int q = 0; q < U; q++) {

@@ -18,62 +18,65 @@
 namespace amg {
 
 // d(lambda_n)/dx of the Thole factors (n = 1..4 <-> lambda_3,5,7,9)
-__device__ __forceinline__ void thole_dlambda_dx(double x, double e, double (&d)[5]) {
+template <class R>
+__device__ __forceinline__ void thole_dlambda_dx(R x, R e, R (&d)[5]) {
     d[0] = 0;
     d[1] = e;
     d[2] = x * e;
-    d[3] = (0.6 * x * x - 0.2 * x) * e;
-    d[4] = ((9.0 / 35.0) * x * x * x - (9.0 / 35.0) * x * x - (1.0 / 35.0) * x) * e;
+    d[3] = (R(0.6) * x * x - R(0.2) * x) * e;
+    d[4] = (R(9.0 / 35.0) * x * x * x - R(9.0 / 35.0) * x * x - R(1.0 / 35.0) * x) * e;
 }
 
 // radial derivatives of a Thole channel: dB_n/d(damp) and dB_n/d(a)
 // (B_n = ... + scale lambda_n bare_n), n = 1..4; zero without damping
-__device__ __forceinline__ void thole_radial_derivs(double r, double damp, double a, double scale,
-                                                    const double (&bare)[6], double (&dBd)[6], double (&dBa)[6]) {
+template <class R>
+__device__ __forceinline__ void thole_radial_derivs(R r, R damp, R a, R scale, const R (&bare)[6], R (&dBd)[6],
+                                                    R (&dBa)[6]) {
     for (int k = 0; k < 6; k++) dBd[k] = dBa[k] = 0;
-    if (damp == 0.0) return;
-    double t = r / damp;
-    double x = a * t * t * t;
-    double e = exp(-x);
-    double dl[5];
-    thole_dlambda_dx(x, e, dl);
+    if (damp == R(0)) return;
+    R t = r / damp;
+    R x = a * t * t * t;
+    R e = exp(-x);
+    R dl[5];
+    thole_dlambda_dx<R>(x, e, dl);
     for (int n = 1; n <= 4; n++) {
-        dBd[n] = scale * bare[n] * dl[n] * (-3.0 * x / damp);
-        dBa[n] = a != 0.0 ? scale * bare[n] * dl[n] * (x / a) : 0.0;
+        dBd[n] = scale * bare[n] * dl[n] * (R(-3) * x / damp);
+        dBa[n] = a != R(0) ? scale * bare[n] * dl[n] * (x / a) : R(0);
     }
 }
 
 // pair energies (for the parameter derivatives) -------------------------------
-__device__ __forceinline__ double md_energy(const Mpole<double>& Mi, const SiteInv<double>& si, V3<double> v,
-                                            V3<double> r, const double (&B)[6]) {
-    double av = dot(v, r);
+template <class R>
+__device__ __forceinline__ R md_energy(const Mpole<R>& Mi, const SiteInv<R>& si, V3<R> v, V3<R> r, const R (&B)[6]) {
+    R av = dot(v, r);
     return (-Mi.q * av + dot(Mi.d, v)) * B[1] + (-si.a * av + 2 * dot(v, si.Qr)) * B[2] - av * si.b * B[3];
 }
-__device__ __forceinline__ double dm_energy(V3<double> w, const Mpole<double>& Mk, const SiteInv<double>& sk,
-                                            V3<double> r, const double (&B)[6]) {
-    double aw = dot(w, r);
+template <class R>
+__device__ __forceinline__ R dm_energy(V3<R> w, const Mpole<R>& Mk, const SiteInv<R>& sk, V3<R> r, const R (&B)[6]) {
+    R aw = dot(w, r);
     return (Mk.q * aw + dot(w, Mk.d)) * B[1] + (-aw * sk.a - 2 * dot(w, sk.Qr)) * B[2] + aw * sk.b * B[3];
 }
-__device__ __forceinline__ double dd_energy(V3<double> a, V3<double> b, V3<double> r, const double (&B)[6]) {
+template <class R>
+__device__ __forceinline__ R dd_energy(V3<R> a, V3<R> b, V3<R> r, const R (&B)[6]) {
     return dot(a, b) * B[1] - dot(a, r) * dot(b, r) * B[2];
 }
 
 // potential derivatives (phi, grad phi, grad grad phi: 10) at the target of
 // a multipole at the source, r = x_target - x_source, order xx yy zz xy xz yz
-__device__ __forceinline__ void mpole_potential10(const Mpole<double>& M, V3<double> r, const double (&B)[6],
-                                                  double (&p)[10]) {
-    SiteInv<double> s = invariants(M, r);
-    double rr[3] = {r.x, r.y, r.z}, d[3] = {M.d.x, M.d.y, M.d.z}, qr[3] = {s.Qr.x, s.Qr.y, s.Qr.z};
-    double Q[3][3] = {{M.Q.xx, M.Q.xy, M.Q.xz}, {M.Q.xy, M.Q.yy, M.Q.yz}, {M.Q.xz, M.Q.yz, M.Q.zz}};
+template <class R>
+__device__ __forceinline__ void mpole_potential10(const Mpole<R>& M, V3<R> r, const R (&B)[6], R (&p)[10]) {
+    SiteInv<R> s = invariants(M, r);
+    R rr[3] = {r.x, r.y, r.z}, d[3] = {M.d.x, M.d.y, M.d.z}, qr[3] = {s.Qr.x, s.Qr.y, s.Qr.z};
+    R Q[3][3] = {{M.Q.xx, M.Q.xy, M.Q.xz}, {M.Q.xy, M.Q.yy, M.Q.yz}, {M.Q.xz, M.Q.yz, M.Q.zz}};
     p[0] = M.q * B[0] + s.a * B[1] + s.b * B[2];
     for (int a = 0; a < 3; a++)
         p[1 + a] = -M.q * rr[a] * B[1] + d[a] * B[1] - s.a * rr[a] * B[2] + 2 * qr[a] * B[2] - s.b * rr[a] * B[3];
     const int ia[6] = {0, 1, 2, 0, 0, 1}, ib[6] = {0, 1, 2, 1, 2, 2};
-    double c2 = M.q * B[2] + s.a * B[3] + s.b * B[4], c1 = M.q * B[1] + s.a * B[2] + s.b * B[3];
+    R c2 = M.q * B[2] + s.a * B[3] + s.b * B[4], c1 = M.q * B[1] + s.a * B[2] + s.b * B[3];
     for (int k = 0; k < 6; k++) {
         int a = ia[k], b = ib[k];
-        double v = rr[a] * rr[b] * c2 - (d[a] * rr[b] + d[b] * rr[a]) * B[2] + 2 * Q[a][b] * B[2] -
-                   2 * (qr[a] * rr[b] + qr[b] * rr[a]) * B[3];
+        R v = rr[a] * rr[b] * c2 - (d[a] * rr[b] + d[b] * rr[a]) * B[2] + 2 * Q[a][b] * B[2] -
+              2 * (qr[a] * rr[b] + qr[b] * rr[a]) * B[3];
         if (a == b) v -= c1;
         p[4 + k] = v;
     }
@@ -105,99 +108,101 @@ __global__ void k_adj_vectors(int n, double cf, const double* __restrict__ ud, c
 
 // Bulk real-space part of the adjoint, site i over its neighbour list:
 // gradient dG_L/dx_i, torque on M_i, the per-site potentials dG_L/dM_i (10),
-// and dG_L/d(pdamp_i), dG_L/d(thole_i).  Vectors as R4 [n][5]:
-// vbar, P1, Q1, P2, Q2.  mscale channel for M-M uses the cm factor (= c f).
-template <bool EWALD, int LPA>
-__global__ void __launch_bounds__(128) k_adjoint_pair(int n, const int* __restrict__ order, const AtomR<double>* __restrict__ at,
-                                                      const double4* __restrict__ vec, Box bx, double aewald,
+// and dG_L/d(pdamp_i), dG_L/d(thole_i).  Sites, vectors and partner rows in
+// cell order (at = cell-order copy of the sites, nbr = cell-order partner
+// positions, vec = R4 [n][5] in cell order: vbar, P1, Q1, P2, Q2); the
+// results go to site i = order[g] in the original order.  Pair arithmetic in
+// R (FP32 for a mixed-precision context, as its forward's pair kernels),
+// every sum in FP64.  The mscale channel for M-M uses the cm factor (= c f).
+template <class R, bool EWALD, int LPA>
+__global__ void __launch_bounds__(128) k_adjoint_pair(int n, const int* __restrict__ order, const AtomR<R>* __restrict__ at,
+                                                      const R4<R>* __restrict__ vec, Box bx, R aewald,
                                                       const int* __restrict__ nbr, int cap,
                                                       const int* __restrict__ nnb, int mutual, double cm,
                                                       double* __restrict__ grad, double* __restrict__ trq,
                                                       double* __restrict__ pot, double* __restrict__ dpd,
                                                       double* __restrict__ dth) {
     const int g = (blockIdx.x * blockDim.x + threadIdx.x) / LPA, lane = threadIdx.x % LPA;
-    const int i = order[min(g, n - 1)];
+    const int gs = min(g, n - 1), i = order[gs];
     const int cnt = g < n ? nnb[i] : 0;
-    const AtomR<double> Ai = at[i];
-    const Mpole<double> Mi = load_mpole(Ai);
-    const V3<double> xi = v3<double>(Ai.a.x, Ai.a.y, Ai.a.z);
-    auto V = [&](int j, int k) { double4 t = vec[5 * (size_t)j + k]; return v3<double>(t.x, t.y, t.z); };
-    const V3<double> vb_i = V(i, 0), p1_i = V(i, 1), q1_i = V(i, 2), p2_i = V(i, 3), q2_i = V(i, 4);
-    V3<double> gacc = v3<double>(0, 0, 0), tacc = v3<double>(0, 0, 0);
-    double pacc[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-    double dpd_acc = 0, dth_acc = 0;
+    const AtomR<R> Ai = at[gs];
+    const Mpole<R> Mi = load_mpole(Ai);
+    const V3<R> xi = v3<R>(Ai.a.x, Ai.a.y, Ai.a.z);
+    auto V = [&](int j, int k) { R4<R> t = vec[5 * (size_t)j + k]; return v3<R>(t.x, t.y, t.z); };
+    const V3<R> vb_i = V(gs, 0), p1_i = V(gs, 1), q1_i = V(gs, 2), p2_i = V(gs, 3), q2_i = V(gs, 4);
+    const R cmr = (R)cm;
+    double acc[18] = {0};  // gradient 3, torque 3, dpdamp, dthole, potentials 10
     const int* row = nbr + (size_t)i * cap;
     for (int s = lane; s < cnt; s += LPA) {
         const int j = row[s];
-        const AtomR<double> Aj = at[j];
-        const Mpole<double> Mk = load_mpole(Aj);
-        const V3<double> r = min_image<double>(v3<double>(Aj.a.x, Aj.a.y, Aj.a.z) - xi, bx);  // x_k - x_i
-        const double r2 = dot(r, r), rr = sqrt(r2);
+        const AtomR<R> Aj = ld_atom(at, j);
+        const Mpole<R> Mk = load_mpole(Aj);
+        const V3<R> r = min_image<R>(v3<R>(Aj.a.x, Aj.a.y, Aj.a.z) - xi, bx);  // x_k - x_i
+        const R r2 = dot(r, r), rr = sqrt(r2);
         // multipole-multipole (em), no Thole, scale 1
-        double Bm[6];
-        bulk_radial<double, EWALD, false>(r2, aewald, 0.0, 0.0, Bm);
-        double E;
-        V3<double> gi, ti;
-        mm_pair_i<double>(Mi, Mk, r, Bm, E, gi, ti);
-        gacc = gacc + cm * gi;
-        tacc = tacc + cm * ti;
-        double pm[10];
-        mpole_potential10(Mk, (-1.0) * r, Bm, pm);  // potential of M_k at i
-        for (int k = 0; k < 10; k++) pacc[k] += cm * pm[k];
+        R Bm[6];
+        bulk_radial<R, EWALD, false>(r2, aewald, R(0), R(0), Bm);
+        R E;
+        V3<R> gi, ti;
+        mm_pair_i<R>(Mi, Mk, r, Bm, E, gi, ti);
+        V3<R> gsum = cmr * gi, tsum = cmr * ti;
+        R pm[10];
+        mpole_potential10<R>(Mk, R(-1) * r, Bm, pm);  // potential of M_k at i
         // polarization channels (Thole, scale 1)
-        const double damp = Ai.e.y * Aj.e.y, a = pair_thole<double>(Ai.e.z, Aj.e.z);
-        double B[6];
-        bulk_radial<double, EWALD, true>(r2, aewald, damp, a, B);
-        const V3<double> vb_k = V(j, 0), p1_k = V(j, 1), q1_k = V(j, 2), p2_k = V(j, 3), q2_k = V(j, 4);
-        const SiteInv<double> si = invariants(Mi, r), sk = invariants(Mk, r);
-        V3<double> d1, t1;
-        md_pair<double>(Mi, si, vb_k, r, B, d1, t1);
-        V3<double> dEdr = d1 + dm_pair<double>(vb_i, Mk, sk, r, B);
+        const R damp = Ai.e.y * Aj.e.y, a = pair_thole<R>(Ai.e.z, Aj.e.z);
+        R B[6];
+        bulk_radial<R, EWALD, true>(r2, aewald, damp, a, B);
+        const V3<R> vb_k = V(j, 0), p1_k = V(j, 1), q1_k = V(j, 2), p2_k = V(j, 3), q2_k = V(j, 4);
+        const SiteInv<R> si = invariants(Mi, r), sk = invariants(Mk, r);
+        V3<R> d1, t1;
+        md_pair<R>(Mi, si, vb_k, r, B, d1, t1);
+        V3<R> dEdr = d1 + dm_pair<R>(vb_i, Mk, sk, r, B);
         if (mutual)
-            dEdr = dEdr + dd_pair<double>(p1_i, q1_k, r, B) + dd_pair<double>(q1_i, p1_k, r, B) +
-                   dd_pair<double>(p2_i, q2_k, r, B) + dd_pair<double>(q2_i, p2_k, r, B);
-        gacc = gacc - dEdr;
-        tacc = tacc + t1;
+            dEdr = dEdr + dd_pair<R>(p1_i, q1_k, r, B) + dd_pair<R>(q1_i, p1_k, r, B) + dd_pair<R>(p2_i, q2_k, r, B) +
+                   dd_pair<R>(q2_i, p2_k, r, B);
+        gsum = gsum - dEdr;
+        tsum = tsum + t1;
         // potential of the dipoles vbar_k at i (d/p channels coincide here)
-        Mpole<double> Dk;
+        Mpole<R> Dk;
         Dk.q = 0;
         Dk.d = vb_k;
-        Dk.Q = Sym<double>{0, 0, 0, 0, 0, 0};
-        double pd_[10];
-        mpole_potential10(Dk, (-1.0) * r, B, pd_);
-        for (int k = 0; k < 10; k++) pacc[k] += pd_[k];
+        Dk.Q = Sym<R>{0, 0, 0, 0, 0, 0};
+        R pd_[10];
+        mpole_potential10<R>(Dk, R(-1) * r, B, pd_);
         // damping derivatives: the same pair energies with dB
-        double bare[6], dBd[6], dBa[6];
-        double rinv = 1.0 / rr;
-        bare_terms<double, 6>(rinv, rinv * rinv, bare);
-        thole_radial_derivs(rr, damp, a, 1.0, bare, dBd, dBa);
-        auto Gwith = [&](const double (&D)[6]) {
-            double e = md_energy(Mi, si, vb_k, r, D) + dm_energy(vb_i, Mk, sk, r, D);
+        R bare[6], dBd[6], dBa[6];
+        const R rinv = R(1) / rr;
+        bare_terms<R, 6>(rinv, rinv * rinv, bare);
+        thole_radial_derivs<R>(rr, damp, a, R(1), bare, dBd, dBa);
+        auto Gwith = [&](const R (&D)[6]) {
+            R e = md_energy<R>(Mi, si, vb_k, r, D) + dm_energy<R>(vb_i, Mk, sk, r, D);
             if (mutual)
-                e += dd_energy(p1_i, q1_k, r, D) + dd_energy(q1_i, p1_k, r, D) + dd_energy(p2_i, q2_k, r, D) +
-                     dd_energy(q2_i, p2_k, r, D);
+                e += dd_energy<R>(p1_i, q1_k, r, D) + dd_energy<R>(q1_i, p1_k, r, D) + dd_energy<R>(p2_i, q2_k, r, D) +
+                     dd_energy<R>(q2_i, p2_k, r, D);
             return e;
         };
-        dpd_acc += Gwith(dBd) * Aj.e.y;  // d damp / d pdamp_i = pdamp_k
-        double ga = Gwith(dBa);
-        double ti_ = Ai.e.z, tk_ = Aj.e.z;
-        double lo = fmin(ti_, tk_);
-        double own = (lo == 0.0) ? (ti_ > tk_ ? 1.0 : ti_ == tk_ ? 0.5 : 0.0)
-                                 : (ti_ < tk_ ? 1.0 : ti_ == tk_ ? 0.5 : 0.0);
-        dth_acc += own * ga;
+        const R gd = Gwith(dBd) * Aj.e.y;  // d damp / d pdamp_i = pdamp_k
+        const R ga = Gwith(dBa);
+        const R ti_ = Ai.e.z, tk_ = Aj.e.z;
+        const R lo = fmin(ti_, tk_);
+        const R own = (lo == R(0)) ? (ti_ > tk_ ? R(1) : ti_ == tk_ ? R(0.5) : R(0))
+                                   : (ti_ < tk_ ? R(1) : ti_ == tk_ ? R(0.5) : R(0));
+        acc[0] += gsum.x; acc[1] += gsum.y; acc[2] += gsum.z;
+        acc[3] += tsum.x; acc[4] += tsum.y; acc[5] += tsum.z;
+        acc[6] += gd;
+        acc[7] += own * ga;
+        for (int k = 0; k < 10; k++) acc[8 + k] += cmr * pm[k] + pd_[k];
     }
-    double out[18] = {gacc.x, gacc.y, gacc.z, tacc.x, tacc.y, tacc.z, dpd_acc, dth_acc};
-    for (int k = 0; k < 10; k++) out[8 + k] = pacc[k];
 #pragma unroll
-    for (int k = 0; k < 18; k++) out[k] = group_sum<LPA>(out[k]);
+    for (int k = 0; k < 18; k++) acc[k] = group_sum<LPA>(acc[k]);
     if (lane == 0 && g < n) {
         for (int c = 0; c < 3; c++) {
-            grad[3 * i + c] += out[c];
-            trq[3 * i + c] += out[3 + c];
+            grad[3 * i + c] += acc[c];
+            trq[3 * i + c] += acc[3 + c];
         }
-        dpd[i] += out[6];
-        dth[i] += out[7];
-        for (int k = 0; k < 10; k++) pot[10 * (size_t)i + k] += out[8 + k];
+        dpd[i] += acc[6];
+        dth[i] += acc[7];
+        for (int k = 0; k < 10; k++) pot[10 * (size_t)i + k] += acc[8 + k];
     }
 }
 

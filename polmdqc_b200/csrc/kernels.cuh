@@ -220,6 +220,13 @@ __device__ __forceinline__ void load_pair(const double4* __restrict__ v4, int j,
         : "l"(v4 + 2 * (size_t)j + 1));
 }
 
+// one 32-byte aligned FP64 vector with a single 256-bit load (read-only data)
+__device__ __forceinline__ double4 ld256(const double4* __restrict__ p) {
+    double4 v;
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(v.x), "=d"(v.y), "=d"(v.z), "=d"(v.w) : "l"(p));
+    return v;
+}
+
 // One site's packed data (64 bytes in FP32, 128 in FP64; 32-byte aligned)
 // with 256-bit loads, for the pair kernels' partner gathers (read-only there).
 __device__ __forceinline__ AtomR<float> ld_atom(const AtomR<float>* __restrict__ at, int j) {

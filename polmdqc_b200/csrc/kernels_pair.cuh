@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(128) k_Tu_cells(int n, const int* __restrict__
     const int* row = cnb + (size_t)i * cap;
     for (int s = lane; s < cnt; s += LPA) {
         const int j = row[s];
-        const double4 pj = spos[j];
+        const double4 pj = ld256(spos + j);
         const double2 dj = sdt[j];
         const V3<double> r = min_image<double, !EWALD || CELLS>(xi - v3<double>(pj.x, pj.y, pj.z), bx);
         const double r2 = dot(r, r), rinv = rsqrt(r2), rr = r2 * rinv, rinv2 = rinv * rinv;
@@ -178,7 +178,8 @@ __global__ void __launch_bounds__(128) k_Tu_cells(int n, const int* __restrict__
             B1 -= e * b1;                 // (1 - lambda3) = e
             B2 -= (1.0 + x) * e * b2;     // (1 - lambda5) = (1 + x) e
         }
-        const double4 ud = u4[2 * j], up = u4[2 * j + 1];
+        double4 ud, up;
+        load_pair(u4, j, ud, up);
         const double ad = (ud.x * r.x + ud.y * r.y + ud.z * r.z) * B2;
         const double ap = (up.x * r.x + up.y * r.y + up.z * r.z) * B2;
         ax += ad * r.x - B1 * ud.x; ay += ad * r.y - B1 * ud.y; az += ad * r.z - B1 * ud.z;

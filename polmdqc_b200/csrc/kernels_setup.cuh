@@ -121,13 +121,35 @@ struct CellGrid {
     double size[3];     // cell edge
     int periodic;
     int off_lo[3], off_hi[3];  // distinct stencil offsets per axis
+    // monoclinic / triclinic cell: cells are the lattice's parallelepipeds,
+    // indexed by fractional coordinates s_a = sum_j x_j R[j][a]; A rows are the
+    // lattice vectors (x = sum_a s_a A[a])
+    int general;
+    double R[3][3], A[3][3];
 };
+
+// fractional coordinates of x in [0, 1) along each lattice vector
+__device__ __forceinline__ void frac_wrapped(const CellGrid& cg, double x, double y, double z, double (&f)[3]) {
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        f[a] = x * cg.R[0][a] + y * cg.R[1][a] + z * cg.R[2][a];
+        f[a] -= floor(f[a]);
+    }
+}
 
 __global__ void k_cell_index(int n, const double* __restrict__ xyz, CellGrid cg, Box bx, unsigned* __restrict__ keys,
                              int* __restrict__ ids) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int c[3];
+    if (cg.general) {
+        double f[3];
+        frac_wrapped(cg, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], f);
+        for (int a = 0; a < 3; a++) c[a] = min(cg.nc[a] - 1, (int)(f[a] * cg.nc[a]));
+        keys[i] = (unsigned)((c[0] * cg.nc[1] + c[1]) * cg.nc[2] + c[2]);
+        ids[i] = i;
+        return;
+    }
     for (int a = 0; a < 3; a++) {
         double x = xyz[3 * i + a];
         double f;
@@ -245,7 +267,9 @@ __global__ void k_neighbors(int n, const double4* __restrict__ spos, const unsig
 }
 
 // The same exact neighbour list, one block per home cell, for boxes with at
-// least 3 cells on every periodic axis.  The atoms of the (up to) 27 stencil
+// least 3 cells on every periodic axis (orthogonal cells; or the lattice's
+// parallelepipeds of a monoclinic or triclinic cell, whose stencil images are
+// lattice translations).  The atoms of the (up to) 27 stencil
 // cells are staged in shared memory as FP32 positions relative to the home
 // cell's corner (periodic coordinates first wrapped into the box, as the
 // cell index does), each moved by its stencil cell's periodic image, so
@@ -260,6 +284,7 @@ constexpr int kNbrChunk = 1280;
 constexpr int kNbrHome = 128;
 constexpr int kNbrThreads = 256;
 
+template <bool GENERAL>
 __global__ void __launch_bounds__(kNbrThreads) k_neighbors_cells(
     const double4* __restrict__ spos, const int* __restrict__ sids, const int* __restrict__ cstart,
     const int* __restrict__ cend, CellGrid cg, Box bx, double cut2, double margin, int cap,
@@ -286,6 +311,10 @@ __global__ void __launch_bounds__(kNbrThreads) k_neighbors_cells(
     double corner[3];
 #pragma unroll
     for (int a = 0; a < 3; a++) corner[a] = cg.origin[a] + cc[a] * cg.size[a];
+    if (GENERAL)  // the cell's lowest lattice point
+        for (int a = 0; a < 3; a++)
+            corner[a] = (double)cc[0] / cg.nc[0] * cg.A[0][a] + (double)cc[1] / cg.nc[1] * cg.A[1][a] +
+                        (double)cc[2] / cg.nc[2] * cg.A[2][a];
     if (threadIdx.x < 32) {
         // stencil cell k = lane (all of a warp's loads of cstart/cend in
         // flight at once), lengths summed by a warp scan; cells outside an
@@ -299,16 +328,20 @@ __global__ void __launch_bounds__(kNbrThreads) k_neighbors_cells(
             int q[3];
             double sh[3];
             bool skip = false;
+            int wrap[3] = {0, 0, 0};
             for (int a = 0; a < 3; a++) {
                 q[a] = cc[a] + d[a];
                 sh[a] = 0.0;
                 if (cg.periodic) {
-                    if (q[a] < 0) { q[a] += cg.nc[a]; sh[a] = -bx.L[a]; }
-                    else if (q[a] >= cg.nc[a]) { q[a] -= cg.nc[a]; sh[a] = bx.L[a]; }
+                    if (q[a] < 0) { q[a] += cg.nc[a]; sh[a] = -bx.L[a]; wrap[a] = -1; }
+                    else if (q[a] >= cg.nc[a]) { q[a] -= cg.nc[a]; sh[a] = bx.L[a]; wrap[a] = 1; }
                 } else if (q[a] < 0 || q[a] >= cg.nc[a]) {
                     skip = true;
                 }
             }
+            if (GENERAL)  // the periodic image is a lattice translation
+                for (int a = 0; a < 3; a++)
+                    sh[a] = wrap[0] * cg.A[0][a] + wrap[1] * cg.A[1][a] + wrap[2] * cg.A[2][a];
             rstart[k] = 0;
             if (!skip) {
                 const int qc = (q[0] * cg.nc[1] + q[1]) * cg.nc[2] + q[2];
@@ -332,10 +365,21 @@ __global__ void __launch_bounds__(kNbrThreads) k_neighbors_cells(
     }
     __syncthreads();
     const int M = rpre[nst];
-    // position in the box (periodic) relative to the home cell's corner
-    auto rel = [&](double x, int a) {
-        if (cg.periodic) x -= bx.L[a] * floor(x * bx.iL[a]);
-        return x - corner[a];
+    // position in the box (periodic) relative to the home cell's corner;
+    // a general cell wraps the fractional coordinates
+    auto rel3 = [&](const double4& x, double (&o)[3]) {
+        if (GENERAL) {
+            double f[3];
+            frac_wrapped(cg, x.x, x.y, x.z, f);
+            for (int a = 0; a < 3; a++) o[a] = f[0] * cg.A[0][a] + f[1] * cg.A[1][a] + f[2] * cg.A[2][a] - corner[a];
+            return;
+        }
+        const double xs[3] = {x.x, x.y, x.z};
+        for (int a = 0; a < 3; a++) {
+            double v = xs[a];
+            if (cg.periodic) v -= bx.L[a] * floor(v * bx.iL[a]);
+            o[a] = v - corner[a];
+        }
     };
     const float lo2 = (float)(cut2 - margin), hi2 = (float)(cut2 + margin);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
@@ -347,8 +391,9 @@ __global__ void __launch_bounds__(kNbrThreads) k_neighbors_cells(
             // their scans without a chain of dependent global loads
             hcnt[t] = 0;
             const int i = sids[h0 + t];
-            const double4 xi = spos[h0 + t];
-            hpos[t] = make_float4((float)rel(xi.x, 0), (float)rel(xi.y, 1), (float)rel(xi.z, 2), 0.f);
+            double h3[3];
+            rel3(spos[h0 + t], h3);
+            hpos[t] = make_float4((float)h3[0], (float)h3[1], (float)h3[2], 0.f);
             hid[t] = i;
             hx0[t] = xoff[i];
             hx1[t] = xoff[i + 1];
@@ -362,10 +407,11 @@ __global__ void __launch_bounds__(kNbrThreads) k_neighbors_cells(
                 const int f0 = max(rpre[k], m0), f1 = min(rpre[k + 1], m0 + mn);
                 for (int f = f0 + threadIdx.x; f < f1; f += blockDim.x) {
                     const int p = rstart[k] + (f - rpre[k]);
-                    const double4 x = spos[p];
+                    double c3[3];
+                    rel3(spos[p], c3);
                     const int t = f - m0;
-                    cpos[t] = make_float4((float)(rel(x.x, 0) + rshift[k][0]), (float)(rel(x.y, 1) + rshift[k][1]),
-                                          (float)(rel(x.z, 2) + rshift[k][2]), 0.f);
+                    cpos[t] = make_float4((float)(c3[0] + rshift[k][0]), (float)(c3[1] + rshift[k][1]),
+                                          (float)(c3[2] + rshift[k][2]), 0.f);
                     csrt[t] = p;
                     cid[t] = sids[p];
                 }
@@ -397,13 +443,15 @@ __global__ void __launch_bounds__(kNbrThreads) k_neighbors_cells(
                         if (r2 <= hi2) {
                             j = cid[t];
                             hit = j != i;
-                            if (hit && r2 > lo2) {  // near the cutoff: the FP64 test
+                            // near the cutoff the FP64 minimum image decides; in a
+                            // general cell it decides every pair, so the pair set
+                            // is that of the cell's image(), as in k_neighbors
+                            if (hit && (r2 > lo2 || GENERAL)) {
                                 const double4 xi = spos[ph];
                                 const double4 pj = spos[csrt[t]];
-                                const double rx = wrap1<double>(pj.x - xi.x, bx.L[0], bx.iL[0]);
-                                const double ry = wrap1<double>(pj.y - xi.y, bx.L[1], bx.iL[1]);
-                                const double rz = wrap1<double>(pj.z - xi.z, bx.L[2], bx.iL[2]);
-                                hit = rx * rx + ry * ry + rz * rz <= cut2;
+                                const V3<double> r =
+                                    min_image<double, GENERAL>(v3<double>(pj.x - xi.x, pj.y - xi.y, pj.z - xi.z), bx);
+                                hit = dot(r, r) <= cut2;
                             }
                             if (hit && j >= xr.x && j <= xr.y) {  // only then can j be a scaled partner
 #pragma unroll

@@ -150,6 +150,30 @@ def test_ewald_in_prism_cells_matches_oracle(w216, box, prec):
         assert np.abs(g.vir - o.vir).max() < 1e-5 * np.abs(o.vir).max()
 
 
+@pytest.mark.parametrize("prec", [FP64, MIXED])
+@pytest.mark.parametrize("box", [(28.3, 28.7, 29.0, 90.0, 97.0, 90.0), (28.3, 28.7, 29.0, 84.0, 97.0, 93.0)])
+def test_prism_cell_lists_at_size(box, prec):
+    """729 waters in a monoclinic and a triclinic cell wide enough for 3
+    lattice cells per axis at a 7 A cutoff: the neighbour lists come from the
+    cell grid of the lattice's parallelepipeds (every pair decided by the
+    cell's FP64 image) instead of the all-pairs search; energies, gradients
+    and virial against the oracle, with Ewald and mutual polarization."""
+    s = systems.water_box(729, 28.3, seed=4)
+    s.box = np.array(box)
+    flags = ALL | abi.DO_VIRIAL | abi.DO_ANALYSIS
+    st = Settings(nfft=(30, 30, 30), precision=FP64)
+    o = oracle.forward(s, st, tol=1e-11, flags=flags)
+    g = run(s, Settings(nfft=(30, 30, 30), precision=prec, poleps=1e-8 if prec == FP64 else 1e-6), flags)
+    assert g.nem == o.nem
+    if prec == FP64:
+        assert rel(g.em, o.em) < 1e-10 and rel(g.ep, o.ep) < 1e-8
+        assert np.abs(g.dem - o.dem).max() < 1e-8 and np.abs(g.dep - o.dep).max() < 1e-5
+        assert np.abs(g.vir - o.vir).max() < 1e-7 * np.abs(o.vir).max()
+    else:
+        assert rel(g.em, o.em) < 1e-6 and rel(g.ep, o.ep) < 1e-6
+        assert frms(g, o) < 1e-4
+
+
 def test_synthetic_box_matches_reference_run():
     """Seeded 216-water box: the compiled reference's em/nem/dem (non-Ewald, 7 A)."""
     d = golden("ref_water216.json")

@@ -1634,10 +1634,18 @@ int forward_impl(amg_ctx* ctx, int flags, amg_results* res) {
     res->pcg_iters = iters;
     res->pcg_eps = eps;
     if (grad) {  // the gradients were read back with the scalars; added to the caller's arrays
-        if (res->dem)
-            for (size_t k = 0; k < 3 * (size_t)n; k++) res->dem[k] += ctx->rb_grad[k];
-        if (res->dep && ctx->has_pol)
-            for (size_t k = 0; k < 3 * (size_t)n; k++) res->dep[k] += ctx->rb_grad[3 * (size_t)n + k];
+        // (host threads share the adds: one thread moves ~10 GB/s, which at
+        // 10^5 atoms is most of a millisecond)
+        double* dem = res->dem;
+        const long long n3 = 3 * (long long)n;
+        const double* gm = ctx->rb_grad;
+        const double* gp = ctx->rb_grad + n3;
+        double* outp = ctx->has_pol ? res->dep : nullptr;
+#pragma omp parallel for schedule(static) if (n3 > 65536)
+        for (long long k = 0; k < n3; k++) {
+            if (dem) dem[k] += gm[k];
+            if (outp) outp[k] += gp[k];
+        }
     }
     if (analysis) {
         fetch(res->aem, ctx->aem, n);
@@ -2038,6 +2046,20 @@ __global__ void k_scale3(int n, const double* __restrict__ pol, const double* __
     for (int c = 0; c < 3; c++) w[3 * i + c] = pol[i] * g[3 * i + c];
 }
 
+// dst[0, cnt) = src[0, cnt) on the host threads (the adjoint's outputs are
+// ~18 doubles per site: one thread would take most of a millisecond at 10^5
+// sites); nothing for a null dst
+void host_copy(double* dst, const double* src, size_t cnt) {
+    if (!dst) return;
+    constexpr long long kChunk = 1 << 15;
+    const long long nchunk = ((long long)cnt + kChunk - 1) / kChunk;
+#pragma omp parallel for schedule(static) if (nchunk > 2)
+    for (long long c = 0; c < nchunk; c++) {
+        const size_t a = (size_t)c * kChunk, b = std::min(cnt, a + (size_t)kChunk);
+        std::memcpy(dst + a, src + a, sizeof(double) * (b - a));
+    }
+}
+
 // the adjoint solve A w = g for both right-hand sides, as the forward solves
 // A u = E: PCG in the context's precision on the forward's stored coefficient
 // rows and grids (same coordinates), then the FP64 correction sweep.  The
@@ -2256,10 +2278,10 @@ int backward_impl(amg_ctx* ctx, const amg_cotangents* cot, amg_param_grads* gr) 
     if (gr->d_thole) CK(cudaMemcpyAsync(hth, dth, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
     if (gr->d_polarity) CK(cudaMemcpyAsync(hpol, dpol, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
-    if (gr->d_xyz) std::memcpy(gr->d_xyz, hx, sizeof(double) * n3);
-    if (gr->d_pole) std::memcpy(gr->d_pole, hpole, sizeof(double) * 13 * n);
-    if (gr->d_thole) std::memcpy(gr->d_thole, hth, sizeof(double) * n);
-    if (gr->d_polarity) std::memcpy(gr->d_polarity, hpol, sizeof(double) * n);
+    host_copy(gr->d_xyz, hx, n3);
+    host_copy(gr->d_pole, hpole, 13 * (size_t)n);
+    host_copy(gr->d_thole, hth, n);
+    host_copy(gr->d_polarity, hpol, n);
     return AMG_OK;
 }
 

@@ -33,9 +33,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(ROOT, "include", "amoeba_gpu.h")]
     if not force and not _stale(LIB, deps):
         return LIB
-    cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fopenmp",
-           "-shared", "-Xptxas", "-v", "-I", os.path.join(ROOT, "include"),
-           *[os.path.join(CSRC, s) for s in SOURCES], "-o", LIB, "-lcufft", "-lgomp"]
+    cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared", "-Xptxas", "-v", "-I", os.path.join(ROOT, "include"),
+           *[os.path.join(CSRC, s) for s in SOURCES], "-o", LIB, "-lcufft"]
     proc = subprocess.run(cmd, capture_output=True, text=True)
     with open(os.path.join(OUT_DIR, "ptxas.log"), "w") as f:
         f.write(proc.stdout + proc.stderr)

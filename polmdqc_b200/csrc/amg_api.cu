@@ -33,6 +33,7 @@ namespace {
 constexpr int kOrder = 5;        // B-spline order compiled in (pme.h bseorder default)
 constexpr int kGatherLanes = 8;  // lanes per site in the PME derivative gathers
 constexpr int kThreads = 128;
+constexpr int kRbChunks = 8;  // pieces of the gradient read-back
 // FP64 accumulators (eacc): em real 0, einter 1, em reciprocal 2, net charge
 // 3, ep 4; the virial's six sums (xx yy zz xy xz yz) of em from kVir and of
 // ep from kVirP
@@ -201,6 +202,7 @@ struct amg_ctx {
     };
     Readback* rb = nullptr;
     double* rb_grad = nullptr;  // [2][3n]
+    cudaEvent_t rbev[1 + kRbChunks] = {};  // scalars read back, then each gradient piece
     size_t flush_bytes = 0;
     // adjoint buffers (allocated on the first amg_backward)
     double *adj = nullptr;       // [3n] x 11 vectors: gd gp wd wp bd bp vbar mwp grad trq zero
@@ -655,7 +657,10 @@ void ensure_coeff_buffers(amg_ctx* ctx, Atoms<R>& A) {
     dalloc(ctx, A.c0, (size_t)ctx->cap * ctx->n);
     if (ctx->sparse_prec) {
         dalloc(ctx, A.cu0, (size_t)ctx->cap * ctx->n);
-        if (!A.s4) dalloc(ctx, A.s4, 2 * (size_t)ctx->n);
+        if (!A.s4) {
+            dalloc(ctx, A.s4, 2 * (size_t)ctx->n);
+            CK(cudaMemset(A.s4, 0, sizeof(R4<R>) * 2 * (size_t)ctx->n));  // the w words stay zero
+        }
     }
     A.cap = ctx->cap;
     ctx->graph_dirty = true;
@@ -761,10 +766,26 @@ void join_side(amg_ctx* ctx, cudaStream_t s) {
 
 // B-spline stencils of every site
 template <class R>
-void pme_stencils(amg_ctx* ctx, cudaStream_t s) {
-    Pme<R>& pm = pme_of<R>(ctx);
-    k_bspline<R, kOrder><<<nblk(ctx->n), kThreads, 0, s>>>(ctx->n, ctx->xyz, ctx->bx, ctx->frac,
-                                                           make_int3(ctx->K[0], ctx->K[1], ctx->K[2]), pm.theta, pm.k0);
+void pme_stencils(amg_ctx* ctx, cudaStream_t s, bool with_fp64 = false) {
+    // the FP64 stencils, the FP32 ones, or (a mixed-precision solve with its
+    // FP64 correction sweep) both from one pass
+    constexpr int BS = 64;
+    const unsigned blocks = (unsigned)((ctx->n + BS - 1) / BS);
+    const int3 K = make_int3(ctx->K[0], ctx->K[1], ctx->K[2]);
+    if constexpr (sizeof(R) == 8) {
+        Pme<double>& pd = pme_of<double>(ctx);
+        k_bspline_rows<kOrder, BS, true, false><<<blocks, BS, 0, s>>>(ctx->n, ctx->xyz, ctx->bx, ctx->frac, K, pd.theta,
+                                                                      pd.k0, nullptr, nullptr);
+    } else if (with_fp64) {
+        Pme<double>& pd = pme_of<double>(ctx);
+        Pme<float>& pf = pme_of<float>(ctx);
+        k_bspline_rows<kOrder, BS, true, true><<<blocks, BS, 0, s>>>(ctx->n, ctx->xyz, ctx->bx, ctx->frac, K, pd.theta,
+                                                                     pd.k0, pf.theta, pf.k0);
+    } else {
+        Pme<float>& pf = pme_of<float>(ctx);
+        k_bspline_rows<kOrder, BS, false, true><<<blocks, BS, 0, s>>>(ctx->n, ctx->xyz, ctx->bx, ctx->frac, K, nullptr,
+                                                                      nullptr, pf.theta, pf.k0);
+    }
     KCHECK();
 }
 
@@ -1090,7 +1111,7 @@ void enqueue_pcg_iter(amg_ctx* ctx, cudaStream_t s, cudaGraphConditionalHandle h
                                               ctx->scal + PAP_P);
         KCHECK();
     }
-    k_pcg_update<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->pol, ctx->pd, ctx->pp, ctx->Apd, ctx->App, ctx->ud, ctx->up,
+    k_pcg_update<R><<<nblk(3 * (size_t)n, 256), 256, 0, s>>>(n, ctx->pol, ctx->pd, ctx->pp, ctx->Apd, ctx->App, ctx->ud, ctx->up,
                                                  ctx->rd, ctx->rp, ctx->zd, ctx->zp, ctx->scal,
                                                  ctx->sparse_prec ? A.s4 : nullptr, ctx->rank,
                                                  apart ? ctx->Fd : nullptr, apart ? ctx->Fp : nullptr,
@@ -1137,12 +1158,11 @@ void enqueue_front(amg_ctx* ctx, cudaStream_t s) {
     k_gather_atoms<R><<<nblk(n), kThreads, 0, r>>>(n, ctx->sids, atoms_of<R>(ctx).at, atoms_of<R>(ctx).atS);
     KCHECK();
     if (ctx->ewald) {
-        pme_stencils<R>(ctx, s);
+        pme_stencils<R>(ctx, s, mixed && iterative(ctx));  // FP64 ones too for the sweep
         Pme<R>& pm = pme_of<R>(ctx);
         k_zero<R><<<nblk(2 * pm.G, 256), 256, 0, s>>>(pm.grid, 2 * pm.G);
         KCHECK();
         if (mixed && iterative(ctx)) {
-            pme_stencils<double>(ctx, s);
             Pme<double>& pd = pme_of<double>(ctx);
             k_zero<double><<<nblk(2 * pd.G, 256), 256, 0, s>>>(pd.grid, 2 * pd.G);
             KCHECK();
@@ -1542,6 +1562,7 @@ int forward_impl(amg_ctx* ctx, int flags, amg_results* res) {
     if (!ctx->rb) {
         CK(cudaMallocHost((void**)&ctx->rb, sizeof(amg_ctx::Readback)));
         CK(cudaMallocHost((void**)&ctx->rb_grad, sizeof(double) * 6 * (size_t)n));
+        for (auto& e : ctx->rbev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
     for (int attempt = 0; attempt < 2; attempt++) {
         ensure_list_buffers(ctx);
@@ -1568,13 +1589,23 @@ int forward_impl(amg_ctx* ctx, int flags, amg_results* res) {
         CK(cudaMemcpyAsync(rb->c, ctx->cnt, sizeof(rb->c), cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(rb->hs, ctx->scal, sizeof(double) * NSCAL, cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(&rb->iters, ctx->iter, sizeof(int), cudaMemcpyDeviceToHost, st));
-        if (grad && res->dem) CK(cudaMemcpyAsync(ctx->rb_grad, ctx->grad_m, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, st));
-        if (grad && res->dep && ctx->has_pol)
-            CK(cudaMemcpyAsync(ctx->rb_grad + 3 * (size_t)n, ctx->grad_p, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost,
-                               st));
-        CK(cudaStreamSynchronize(st));
+        CK(cudaEventRecord(ctx->rbev[0], st));
+        // the gradients in kRbChunks pieces, each with its event: the host adds
+        // a piece to the caller's arrays while the next one is in flight
+        const size_t n3 = 3 * (size_t)n, piece = (n3 + kRbChunks - 1) / kRbChunks;
+        for (int k = 0; k < kRbChunks; k++) {
+            const size_t a = std::min(n3, k * piece), b = std::min(n3, a + piece);
+            if (b > a && grad && res->dem)
+                CK(cudaMemcpyAsync(ctx->rb_grad + a, ctx->grad_m + a, sizeof(double) * (b - a), cudaMemcpyDeviceToHost, st));
+            if (b > a && grad && res->dep && ctx->has_pol)
+                CK(cudaMemcpyAsync(ctx->rb_grad + n3 + a, ctx->grad_p + a, sizeof(double) * (b - a),
+                                   cudaMemcpyDeviceToHost, st));
+            CK(cudaEventRecord(ctx->rbev[1 + k], st));
+        }
+        CK(cudaEventSynchronize(ctx->rbev[0]));
         const int over = rb->over;
         if (over <= ctx->cap) break;
+        CK(cudaStreamSynchronize(st));
         if (attempt == 1) {
             ctx->err = "neighbour list overflow";
             return AMG_ERR_CUDA;
@@ -1633,18 +1664,19 @@ int forward_impl(amg_ctx* ctx, int flags, amg_results* res) {
     res->nep = (int64_t)c[1];
     res->pcg_iters = iters;
     res->pcg_eps = eps;
-    if (grad) {  // the gradients were read back with the scalars; added to the caller's arrays
-        // (host threads share the adds: one thread moves ~10 GB/s, which at
-        // 10^5 atoms is most of a millisecond)
+    if (grad) {  // added to the caller's arrays piece by piece as the copies land
         double* dem = res->dem;
-        const long long n3 = 3 * (long long)n;
+        double* dep = ctx->has_pol ? res->dep : nullptr;
+        const size_t n3 = 3 * (size_t)n, piece = (n3 + kRbChunks - 1) / kRbChunks;
         const double* gm = ctx->rb_grad;
         const double* gp = ctx->rb_grad + n3;
-        double* outp = ctx->has_pol ? res->dep : nullptr;
-#pragma omp parallel for schedule(static) if (n3 > 65536)
-        for (long long k = 0; k < n3; k++) {
-            if (dem) dem[k] += gm[k];
-            if (outp) outp[k] += gp[k];
+        for (int k = 0; k < kRbChunks; k++) {
+            const size_t a = std::min(n3, k * piece), b = std::min(n3, a + piece);
+            CK(cudaEventSynchronize(ctx->rbev[1 + k]));
+            if (dem)
+                for (size_t q = a; q < b; q++) dem[q] += gm[q];
+            if (dep)
+                for (size_t q = a; q < b; q++) dep[q] += gp[q];
         }
     }
     if (analysis) {
@@ -1685,6 +1717,8 @@ int forward_impl(amg_ctx* ctx, int flags, amg_results* res) {
 void release(amg_ctx* ctx) {
     if (ctx->rb) { cudaFreeHost(ctx->rb); ctx->rb = nullptr; }
     if (ctx->rb_grad) { cudaFreeHost(ctx->rb_grad); ctx->rb_grad = nullptr; }
+    for (auto& e : ctx->rbev)
+        if (e) { cudaEventDestroy(e); e = nullptr; }
     if (ctx->adj_host) { cudaFreeHost(ctx->adj_host); ctx->adj_host = nullptr; }
     double** dbl[] = {&ctx->pole13, &ctx->pol, &ctx->thole, &ctx->pdamp, &ctx->xyz, &ctx->rp10, &ctx->Ed, &ctx->Ep,
                       &ctx->ud, &ctx->up, &ctx->rd, &ctx->rp, &ctx->zd, &ctx->zp, &ctx->pd, &ctx->pp, &ctx->Apd,
@@ -2046,18 +2080,9 @@ __global__ void k_scale3(int n, const double* __restrict__ pol, const double* __
     for (int c = 0; c < 3; c++) w[3 * i + c] = pol[i] * g[3 * i + c];
 }
 
-// dst[0, cnt) = src[0, cnt) on the host threads (the adjoint's outputs are
-// ~18 doubles per site: one thread would take most of a millisecond at 10^5
-// sites); nothing for a null dst
+// dst[0, cnt) = src[0, cnt); nothing for a null dst
 void host_copy(double* dst, const double* src, size_t cnt) {
-    if (!dst) return;
-    constexpr long long kChunk = 1 << 15;
-    const long long nchunk = ((long long)cnt + kChunk - 1) / kChunk;
-#pragma omp parallel for schedule(static) if (nchunk > 2)
-    for (long long c = 0; c < nchunk; c++) {
-        const size_t a = (size_t)c * kChunk, b = std::min(cnt, a + (size_t)kChunk);
-        std::memcpy(dst + a, src + a, sizeof(double) * (b - a));
-    }
+    if (dst) std::memcpy(dst, src, sizeof(double) * cnt);
 }
 
 // the adjoint solve A w = g for both right-hand sides, as the forward solves

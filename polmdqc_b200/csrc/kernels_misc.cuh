@@ -135,32 +135,30 @@ __global__ void k_pcg_update(int n, const double* __restrict__ pol, const double
                              const double* __restrict__ Fp, int* __restrict__ done, int* __restrict__ iter,
                              double thr2, int maxit, int roll, cudaGraphConditionalHandle h, int use_handle,
                              int* __restrict__ cont_out) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    // one thread per vector component q = 3i + c: the site loop had too few
+    // threads in flight for its chains of dependent loads
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
     double ad = scal[PAP_D] != 0 ? scal[RZ_D] / scal[PAP_D] : 0.0;
     double ap = scal[PAP_P] != 0 ? scal[RZ_P] / scal[PAP_P] : 0.0;
     double rzd = 0, rzp = 0, rrd = 0, rrp = 0;
-    if (i < n) {
-        double a = pol[i];
-        double sv[6];
-        for (int c = 0; c < 3; c++) {
-            int q = 3 * i + c;
-            ud[q] += ad * pd[q];
-            up[q] += ap * pp[q];
-            const double Aq1 = Fd ? Apd[q] - Fd[q] : Apd[q], Aq2 = Fp ? App[q] - Fp[q] : App[q];
-            double r1 = rd[q] - ad * Aq1, r2 = rp[q] - ap * Aq2;
-            rd[q] = r1; rp[q] = r2;
-            double z1 = a * r1, z2 = a * r2;
-            sv[c] = z1; sv[3 + c] = z2;
-            if (!s4) {
-                zd[q] = z1; zp[q] = z2;
-                rzd += r1 * z1; rzp += r2 * z2;
-            }
-            rrd += r1 * r1; rrp += r2 * r2;
+    if (q < 3 * n) {
+        const int i = q / 3, c = q - 3 * (q / 3);
+        const double a = pol[i];
+        ud[q] += ad * pd[q];
+        up[q] += ap * pp[q];
+        const double Aq1 = Fd ? Apd[q] - Fd[q] : Apd[q], Aq2 = Fp ? App[q] - Fp[q] : App[q];
+        const double r1 = rd[q] - ad * Aq1, r2 = rp[q] - ap * Aq2;
+        rd[q] = r1; rp[q] = r2;
+        const double z1 = a * r1, z2 = a * r2;
+        if (s4) {  // the scaled residual in cell order, both sets (x, y, z of each R4)
+            R* sv = reinterpret_cast<R*>(s4 + 2 * (size_t)rank[i]);
+            sv[c] = (R)z1;
+            sv[4 + c] = (R)z2;
+        } else {
+            zd[q] = z1; zp[q] = z2;
+            rzd += r1 * z1; rzp += r2 * z2;
         }
-        if (s4) {
-            s4[2 * rank[i]] = make_r4<R>((R)sv[0], (R)sv[1], (R)sv[2], R(0));
-            s4[2 * rank[i] + 1] = make_r4<R>((R)sv[3], (R)sv[4], (R)sv[5], R(0));
-        }
+        rrd += r1 * r1; rrp += r2 * r2;
     }
     if (!s4) {
         block_sum_add(rzd, scal + RZN_D);

@@ -260,6 +260,60 @@ inline unsigned spread_blocks(int n) {
     return sizeof(R) == 8 ? (unsigned)n : (unsigned)((n + kLineSites - 1) / kLineSites);
 }
 
+// The P grid values z = c0 .. c0+P-1 (periodic in Kz) of one z-line of the
+// complex dipole grid.  With the line's z-range inside the grid and Kz even,
+// from three aligned loads of two values each (16 bytes in FP32, 32 in FP64)
+// and a select by the parity of c0, instead of one load per value: 6 values
+// cover any 5 consecutive ones; else value by value.  (Two 256-bit FP32
+// loads of 8 values were slower: 64 bytes through L1 for 40 used.)  The grid
+// is read-only in the gathers.
+template <int P>
+__device__ __forceinline__ void load_line(const float2* __restrict__ line, int c0, int Kz, float2 (&q)[P]) {
+    static_assert(P <= 5, "a line of at most 5 values fits 6 loaded ones");
+    const int zb = c0 & ~1, o = c0 & 1;
+    if ((Kz & 1) == 0 && zb + 6 <= Kz) {
+        float4 w[3];
+#pragma unroll
+        for (int h = 0; h < 3; h++) w[h] = __ldg(reinterpret_cast<const float4*>(line + zb) + h);
+        const float2 v[6] = {make_float2(w[0].x, w[0].y), make_float2(w[0].z, w[0].w), make_float2(w[1].x, w[1].y),
+                             make_float2(w[1].z, w[1].w), make_float2(w[2].x, w[2].y), make_float2(w[2].z, w[2].w)};
+#pragma unroll
+        for (int c = 0; c < P; c++) q[c] = o ? v[c + 1] : v[c];
+        return;
+    }
+#pragma unroll
+    for (int c = 0; c < P; c++) {
+        int gc = c0 + c;
+        if (gc >= Kz) gc -= Kz;
+        q[c] = line[gc];
+    }
+}
+template <int P>
+__device__ __forceinline__ void load_line(const double2* __restrict__ line, int c0, int Kz, double2 (&q)[P]) {
+    static_assert(P <= 5, "a line of at most 5 values fits 6 loaded ones");
+    const int zb = c0 & ~1, o = c0 & 1;
+    if ((Kz & 1) == 0 && zb + 6 <= Kz) {
+        double w[12];
+#pragma unroll
+        for (int h = 0; h < 3; h++)
+            asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+                : "=d"(w[4 * h]), "=d"(w[4 * h + 1]), "=d"(w[4 * h + 2]), "=d"(w[4 * h + 3])
+                : "l"(line + zb + 2 * h));
+#pragma unroll
+        for (int c = 0; c < P; c++) {
+            q[c].x = o ? w[2 * c + 2] : w[2 * c];
+            q[c].y = o ? w[2 * c + 3] : w[2 * c + 1];
+        }
+        return;
+    }
+#pragma unroll
+    for (int c = 0; c < P; c++) {
+        int gc = c0 + c;
+        if (gc >= Kz) gc -= Kz;
+        q[c] = line[gc];
+    }
+}
+
 // Gather of the field of two dipole potential grids (interleaved as the
 // real and imaginary parts of zg; first derivatives only) fused with the
 // matvec assembly:
@@ -289,14 +343,10 @@ __global__ void __launch_bounds__(128) k_gather_field(int n, const typename Cplx
         const R* th = theta + (size_t)i * 3 * 4 * P;
         const int a0 = k0[3 * i], b0 = k0[3 * i + 1], c0 = k0[3 * i + 2];
         R v0[P], v1[P];
-        int zc[P];
 #pragma unroll
         for (int c = 0; c < P; c++) {
             v0[c] = th[8 * P + c];
             v1[c] = th[9 * P + c];
-            int gc = c0 + c;
-            if (gc >= K.z) gc -= K.z;
-            zc[c] = gc;
         }
         R f[6] = {0, 0, 0, 0, 0, 0};
         for (int l = lane; l < P * P; l += G) {
@@ -304,11 +354,12 @@ __global__ void __launch_bounds__(128) k_gather_field(int n, const typename Cplx
             int ga = a0 + a; if (ga >= K.x) ga -= K.x;
             int gb = b0 + b; if (gb >= K.y) gb -= K.y;
             const typename Cplx<R>::type* line = zg + ((size_t)ga * K.y + gb) * K.z;
+            typename Cplx<R>::type qv[P];
+            load_line<P>(line, c0, K.z, qv);
             R sd0 = 0, sd1 = 0, sp0 = 0, sp1 = 0;
 #pragma unroll
             for (int c = 0; c < P; c++) {
-                const typename Cplx<R>::type q = line[zc[c]];
-                const R qd = q.x, qp = q.y;
+                const R qd = qv[c].x, qp = qv[c].y;
                 sd0 += v0[c] * qd; sd1 += v1[c] * qd;
                 sp0 += v0[c] * qp; sp1 += v1[c] * qp;
             }
@@ -550,13 +601,14 @@ __global__ void __launch_bounds__(128) k_gather(int n, const void* __restrict__ 
 #pragma unroll
             for (int s = 0; s < NS; s++) z[s][d] = 0;
         }
+        C qv[P];
+        if constexpr (NS == 2) load_line<P>(static_cast<const C*>(gridv) + line, c0, K.z, qv);
 #pragma unroll
         for (int c = 0; c < P; c++) {
             R q[NS];
             if constexpr (NS == 2) {
-                const C v = static_cast<const C*>(gridv)[line + zc[c]];
-                q[0] = v.x;
-                q[NS - 1] = v.y;
+                q[0] = qv[c].x;
+                q[NS - 1] = qv[c].y;
             } else {
                 q[0] = static_cast<const R*>(gridv)[line + zc[c]];
             }

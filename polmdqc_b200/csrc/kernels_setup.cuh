@@ -511,28 +511,46 @@ __device__ __forceinline__ void bspline_weights(double w, R (&th)[4][P]) {
     }
 }
 
-template <class R, int P>
-__global__ void k_bspline(int n, const double* __restrict__ xyz, Box bx, Frac F, int3 K, R* __restrict__ theta,
-                          int* __restrict__ k0) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    int Ks[3] = {K.x, K.y, K.z};
-    const double x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2];
-    for (int a = 0; a < 3; a++) {
-        // fractional coordinate (grid units / K) along cell axis a
-        double f = F.general ? (x * F.m[0][a] + y * F.m[1][a] + z * F.m[2][a]) / Ks[a]
-                             : (a == 0 ? x : a == 1 ? y : z) * bx.iL[a];
-        f -= floor(f);
-        double u = f * Ks[a];
-        double fl = floor(u);
-        R th[4][P];
-        bspline_weights<R, P>(u - fl, th);
-        int start = (int)fl - P + 1;
-        if (start < 0) start += Ks[a];
-        k0[3 * i + a] = start;
-        R* o = theta + ((size_t)i * 3 + a) * 4 * P;
-        for (int d = 0; d < 4; d++)
-            for (int s = 0; s < P; s++) o[d * P + s] = th[d][s];
+// B-spline stencils (weights and three derivatives per axis, start indices)
+// of a block of BS sites, computed once in FP64 and
+// written through shared memory, so the block's rows (3 axes x 4 orders x P
+// values per site, consecutive sites adjacent) leave as contiguous runs
+// instead of 60 scattered words per thread; with WD the FP64 stencils, with
+// WF the FP32 copy (the FP32 path rounds the same FP64 values), each with
+// its start indices.
+template <int P, int BS, bool WD, bool WF>
+__global__ void __launch_bounds__(BS) k_bspline_rows(int n, const double* __restrict__ xyz, Box bx, Frac F, int3 K,
+                                                    double* __restrict__ thd, int* __restrict__ k0d,
+                                                    float* __restrict__ thf, int* __restrict__ k0f) {
+    constexpr int W = 3 * 4 * P;
+    __shared__ double sd[BS * W];
+    const int i0 = blockIdx.x * BS, i = i0 + threadIdx.x;
+    if (i < n) {
+        const int Ks[3] = {K.x, K.y, K.z};
+        const double x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2];
+        for (int a = 0; a < 3; a++) {
+            double f = F.general ? (x * F.m[0][a] + y * F.m[1][a] + z * F.m[2][a]) / Ks[a]
+                                 : (a == 0 ? x : a == 1 ? y : z) * bx.iL[a];
+            f -= floor(f);
+            const double u = f * Ks[a];
+            const double fl = floor(u);
+            double th[4][P];
+            bspline_weights<double, P>(u - fl, th);
+            int start = (int)fl - P + 1;
+            if (start < 0) start += Ks[a];
+            if (WD) k0d[3 * i + a] = start;
+            if (WF) k0f[3 * i + a] = start;
+            double* o = sd + threadIdx.x * W + a * 4 * P;
+            for (int d = 0; d < 4; d++)
+                for (int s = 0; s < P; s++) o[d * P + s] = th[d][s];
+        }
+    }
+    __syncthreads();
+    const int cnt = min(BS, n - i0) * W;
+    for (int t = threadIdx.x; t < cnt; t += BS) {
+        const double v = sd[t];
+        if (WD) thd[(size_t)i0 * W + t] = v;
+        if (WF) thf[(size_t)i0 * W + t] = (float)v;
     }
 }
 

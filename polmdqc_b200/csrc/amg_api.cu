@@ -170,9 +170,12 @@ struct amg_ctx {
     cudaStream_t st = nullptr, st2 = nullptr;
     // side streams: real-space pair kernels run there while the PME chain
     // runs on the main stream; side[0] pairs with st, side[1] with st2 (the
-    // PCG loop body is captured on st2 into its own graph)
-    cudaStream_t side[2] = {nullptr, nullptr};
-    cudaEvent_t efork[2] = {}, ejoin[2] = {};
+    // PCG loop body is captured on st2 into its own graph); side[kMpoleSide]
+    // carries the permanent-multipole forces from the end of the front to
+    // the end of the back, beside the dipole solve
+    cudaStream_t side[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t efork[3] = {}, ejoin[3] = {};
+    cudaEvent_t erot = nullptr;  // rotated multipoles ready (the list build starts before them)
     cudaEvent_t ev[6] = {};
     CellGrid cg{};
     double cell_volume = 1.0;
@@ -195,7 +198,7 @@ struct amg_ctx {
     // pinned host staging of one evaluation's read-back (status, scalars,
     // gradients), filled by asynchronous copies behind one synchronisation
     struct Readback {
-        int over, iters;
+        int over, iters, over_m;
         double e[kEacc];
         unsigned long long c[4];
         double hs[NSCAL];
@@ -203,6 +206,12 @@ struct amg_ctx {
     Readback* rb = nullptr;
     double* rb_grad = nullptr;  // [2][3n]
     cudaEvent_t rbev[1 + kRbChunks] = {};  // scalars read back, then each gradient piece
+    // the permanent-multipole gradient, read back on its own stream while the
+    // solve still runs: gm_ready is recorded when the force stream is done
+    // (an external event node in the captured graph), rbevm per piece
+    cudaStream_t rbst = nullptr;
+    cudaEvent_t gm_ready = nullptr;
+    cudaEvent_t rbevm[kRbChunks] = {};
     size_t flush_bytes = 0;
     // adjoint buffers (allocated on the first amg_backward)
     double *adj = nullptr;       // [3n] x 11 vectors: gd gp wd wp bd bp vbar mwp grad trq zero
@@ -764,6 +773,18 @@ void join_side(amg_ctx* ctx, cudaStream_t s) {
     CK(cudaStreamWaitEvent(s, ctx->ejoin[k], 0));
 }
 
+// the permanent-multipole force stream, forked from and joined to st
+constexpr int kMpoleSide = 2;
+cudaStream_t fork_mpole(amg_ctx* ctx, cudaStream_t s) {
+    CK(cudaEventRecord(ctx->efork[kMpoleSide], s));
+    CK(cudaStreamWaitEvent(ctx->side[kMpoleSide], ctx->efork[kMpoleSide], 0));
+    return ctx->side[kMpoleSide];
+}
+void join_mpole(amg_ctx* ctx, cudaStream_t s) {
+    CK(cudaEventRecord(ctx->ejoin[kMpoleSide], ctx->side[kMpoleSide]));
+    CK(cudaStreamWaitEvent(s, ctx->ejoin[kMpoleSide], 0));
+}
+
 // B-spline stencils of every site
 template <class R>
 void pme_stencils(amg_ctx* ctx, cudaStream_t s, bool with_fp64 = false) {
@@ -840,10 +861,10 @@ void spread_dipoles(amg_ctx* ctx, cudaStream_t s, const double* vd, const double
 // transform and the permanent one saved by pme_mpole
 template <class R>
 void pme_dipole_grids(amg_ctx* ctx, cudaStream_t s, const double* vd, const double* vp, bool spread = true,
-                      double* vir = nullptr, bool mterms = true) {
+                      double* vir = nullptr, bool mterms = true, bool clear = true) {
     Pme<R>& pm = pme_of<R>(ctx);
     if (spread) {
-        CK(cudaMemsetAsync(pm.zg, 0, sizeof(typename Cplx<R>::type) * pm.G, s));
+        if (clear) CK(cudaMemsetAsync(pm.zg, 0, sizeof(typename Cplx<R>::type) * pm.G, s));
         spread_dipoles<R>(ctx, s, vd, vp);
     }
     CKFFT(cufftSetStream(pm.zplan, s));
@@ -989,7 +1010,7 @@ void build_tu_coeffs(amg_ctx* ctx, cudaStream_t s) {
 // of v.Av, and the caller takes A v = Ad - Fd (k_pcg_update).
 template <class R>
 void matvec_stored(amg_ctx* ctx, cudaStream_t s, const R4<R>* v4, const double* vd, const double* vp, double* Ad,
-                   double* Ap, double* vAv = nullptr, bool spread = true, bool apart = false) {
+                   double* Ap, double* vAv = nullptr, bool spread = true, bool apart = false, bool clear = true) {
     const int n = ctx->n;
     Atoms<R>& A = atoms_of<R>(ctx);
     apart = apart && ctx->ewald && vAv;
@@ -1003,7 +1024,7 @@ void matvec_stored(amg_ctx* ctx, cudaStream_t s, const R4<R>* v4, const double* 
     KCHECK();
     if (ctx->ewald) {
         Pme<R>& pm = pme_of<R>(ctx);
-        pme_dipole_grids<R>(ctx, s, vd, vp, spread);
+        pme_dipole_grids<R>(ctx, s, vd, vp, spread, nullptr, true, clear);
         if (!apart) join_side(ctx, s);
         int3 K = make_int3(ctx->K[0], ctx->K[1], ctx->K[2]);
         constexpr int G = 8;  // lanes per site
@@ -1045,13 +1066,20 @@ void precondition(amg_ctx* ctx, cudaStream_t s) {
     KCHECK();
 }
 
-// p = z + beta p after the rz scalars were rolled; with Ewald fused with the
-// spreading of p for the next matvec
+// Up to this many sites the PCG direction update and the spreading of p are
+// separate kernels, and the spreading runs beside k_tu_stored (4,096 waters:
+// 3.5% faster per evaluation); above it the fused k_pcg_dir_spread is as fast
+// (32,768 waters) with fewer launches.
+constexpr int kSplitSpreadSites = 65536;
+bool split_spread(const amg_ctx* ctx) { return ctx->ewald && ctx->n <= kSplitSpreadSites; }
+
+// p = z + beta p after the rz scalars were rolled; with Ewald (and above
+// kSplitSpreadSites) fused with the spreading of p for the next matvec
 template <class R>
 void direction(amg_ctx* ctx, cudaStream_t s) {
     const int n = ctx->n;
     Atoms<R>& A = atoms_of<R>(ctx);
-    if (ctx->ewald) {
+    if (ctx->ewald && !split_spread(ctx)) {
         Pme<R>& pm = pme_of<R>(ctx);
         const int3 K = make_int3(ctx->K[0], ctx->K[1], ctx->K[2]);
         k_pcg_dir_spread<R, kOrder><<<spread_blocks<R>(n), 128, 0, s>>>(n, ctx->zd, ctx->zp, ctx->pd, ctx->pp, ctx->scal, A.p4, pm.theta,
@@ -1104,8 +1132,10 @@ void enqueue_pcg_iter(amg_ctx* ctx, cudaStream_t s, cudaGraphConditionalHandle h
     direction<R>(ctx, s);
     // p.Ap: fused into the PME gather with Ewald, a separate pass without
     const bool apart = ctx->ewald;  // real-space field kept apart: the gather overlaps k_tu_stored
+    // split: the direction kernel only updates p; p is spread here, beside
+    // k_tu_stored, into the grid the previous transform left cleared
     matvec_stored<R>(ctx, s, A.p4, ctx->pd, ctx->pp, ctx->Apd, ctx->App, ctx->ewald ? ctx->scal + PAP_D : nullptr,
-                     false, apart);
+                     split_spread(ctx), apart, false);
     if (!ctx->ewald) {
         k_dot2<<<nblk(n3, 256), 256, 0, s>>>(n3, ctx->pd, ctx->Apd, ctx->pp, ctx->App, ctx->scal + PAP_D,
                                               ctx->scal + PAP_P);
@@ -1145,16 +1175,19 @@ void enqueue_front(amg_ctx* ctx, cudaStream_t s) {
             ctx->nbond, ctx->bonds, ctx->bflux, ctx->nangle, ctx->angles, ctx->aflux, ctx->xyz, ctx->dq);
         KCHECK();
     }
+    // neighbour list and real-space permanent field on the side stream (the
+    // list build needs only the positions, so it starts beside the frame
+    // rotations); PME stencils and the reciprocal permanent potential on s
+    cudaStream_t r = fork_side(ctx, s);
+    enqueue_lists(ctx, r);
     rotate_and_pack<R>(ctx, s);
     if (mixed && iterative(ctx)) rotate_and_pack<double>(ctx, s);
     k_zero<double><<<1, 32, 0, s>>>(ctx->eacc, kEacc);
     KCHECK();
     k_zero<unsigned long long><<<1, 32, 0, s>>>(ctx->cnt, 4);
     KCHECK();
-    // neighbour list and real-space permanent field on the side stream; PME
-    // stencils and the reciprocal permanent potential on s
-    cudaStream_t r = fork_side(ctx, s);
-    enqueue_lists(ctx, r);
+    CK(cudaEventRecord(ctx->erot, s));  // the packed sites for the cell-order copy
+    CK(cudaStreamWaitEvent(r, ctx->erot, 0));
     k_gather_atoms<R><<<nblk(n), kThreads, 0, r>>>(n, ctx->sids, atoms_of<R>(ctx).at, atoms_of<R>(ctx).atS);
     KCHECK();
     if (ctx->ewald) {
@@ -1300,39 +1333,29 @@ void enqueue_pred_store(amg_ctx* ctx, cudaStream_t s) {
     KCHECK();
 }
 
+// Permanent-multipole energy and forces: the real-space pair kernels (atomic
+// accumulation), then the reciprocal part and the frame torques, which add to
+// the same arrays without atomics.  They need only what the front computed
+// (lists, rotated multipoles, the permanent PME potentials) and touch none of
+// the solve's arrays, so they run on their own stream m beside the dipole
+// solve; enqueue_back joins m at its end.
 template <class R>
-void enqueue_back(amg_ctx* ctx, cudaStream_t s, int flags) {
+void enqueue_mpole_forces(amg_ctx* ctx, cudaStream_t m, int flags) {
     const int n = ctx->n;
     const bool grad = flags & AMG_DO_GRADIENT;
     const bool analysis = flags & AMG_DO_ANALYSIS;
-    const bool polgrad = grad && ctx->has_pol;
     const double cut2 = ctx->cut * ctx->cut;
     Atoms<R>& A = atoms_of<R>(ctx);
     const R aew = (R)ctx->aewald;
-    const int mutual = ctx->poltyp == AMG_POL_MUTUAL;
-    CK(cudaEventRecord(ctx->ev[3], s));
-    k_zero<double><<<nblk(3 * n, 256), 256, 0, s>>>(ctx->grad_m, 3 * (size_t)n);
+    k_zero<double><<<nblk(3 * n, 256), 256, 0, m>>>(ctx->grad_m, 3 * (size_t)n);
     KCHECK();
-    k_zero<double><<<nblk(3 * n, 256), 256, 0, s>>>(ctx->trq_m, 3 * (size_t)n);
+    k_zero<double><<<nblk(3 * n, 256), 256, 0, m>>>(ctx->trq_m, 3 * (size_t)n);
     KCHECK();
-    k_zero<double><<<nblk(n, 256), 256, 0, s>>>(ctx->aem, (size_t)n);
+    k_zero<double><<<nblk(n, 256), 256, 0, m>>>(ctx->aem, (size_t)n);
     KCHECK();
-    if (polgrad) {
-        k_zero<double><<<nblk(3 * n, 256), 256, 0, s>>>(ctx->grad_p, 3 * (size_t)n);
-        KCHECK();
-        k_zero<double><<<nblk(3 * n, 256), 256, 0, s>>>(ctx->trq_p, 3 * (size_t)n);
-        KCHECK();
-        k_pack_u<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->ud, ctx->up, A.u4, ctx->rank);  // cell order
-        KCHECK();
-    }
-    // Real-space pair kernels (atomic accumulation) on the side stream; the
-    // PME dipole potentials and the polarization energy on s.  The
-    // reciprocal-space force kernels add to the same arrays without atomics,
-    // so they run after the join.
-    cudaStream_t r = fork_side(ctx, s);
+    const cudaStream_t r = m;
     const int* mol = ctx->mol;
-    double* vir = ctx->want_vir ? ctx->eacc + kVir : nullptr;    // em terms
-    double* virp = ctx->want_vir ? ctx->eacc + kVirP : nullptr;  // ep terms
+    double* vir = ctx->want_vir ? ctx->eacc + kVir : nullptr;  // em terms
     // Analysis and Virial outputs come from the EXTRA pair kernels
     const bool extra = analysis || vir;
     if (ctx->cp_mode) {
@@ -1387,15 +1410,66 @@ void enqueue_back(amg_ctx* ctx, cudaStream_t s, int flags) {
         KCHECK();
     }
     }
+    if (ctx->ewald) {
+        k_recip_mpole<<<nblk(n), kThreads, 0, m>>>(n, ctx->rp10, ctx->phiM, ctx->f, ctx->aewald, ctx->grad_m, ctx->trq_m,
+                                                   ctx->eacc + 2, analysis ? ctx->aem : nullptr, ctx->eacc + 3, vir);
+        KCHECK();
+    }
+    if (grad) {
+        k_torque<<<nblk(n), kThreads, 0, m>>>(n, ctx->xyz, ctx->zax, ctx->xax, ctx->yax, ctx->axe, ctx->trq_m,
+                                              ctx->grad_m, vir);
+        KCHECK();
+        if (ctx->cflux) {  // the gradient through the geometry-dependent monopoles
+            k_cflux_grad<<<nblk((size_t)ctx->nbond + ctx->nangle), kThreads, 0, m>>>(
+                ctx->nbond, ctx->bonds, ctx->bflux, ctx->nangle, ctx->angles, ctx->aflux, ctx->xyz, ctx->cfpot,
+                ctx->grad_m, vir);
+            KCHECK();
+        }
+    }
+    // grad_m is final: the read-back stream may copy it while the solve runs
+    // (inside a capture, an event node that work outside the graph can wait on)
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(m, &cs));
+    if (cs == cudaStreamCaptureStatusActive) CK(cudaEventRecordWithFlags(ctx->gm_ready, m, cudaEventRecordExternal));
+    else CK(cudaEventRecord(ctx->gm_ready, m));
+}
+
+// Polarization energy and forces after the solve; the permanent-multipole
+// forces, forked onto their own stream after the front, join here.
+template <class R>
+void enqueue_back(amg_ctx* ctx, cudaStream_t s, int flags) {
+    const int n = ctx->n;
+    const bool grad = flags & AMG_DO_GRADIENT;
+    const bool analysis = flags & AMG_DO_ANALYSIS;
+    const bool polgrad = grad && ctx->has_pol;
+    const double cut2 = ctx->cut * ctx->cut;
+    Atoms<R>& A = atoms_of<R>(ctx);
+    const R aew = (R)ctx->aewald;
+    const int mutual = ctx->poltyp == AMG_POL_MUTUAL;
+    CK(cudaEventRecord(ctx->ev[3], s));
+    if (polgrad) {
+        k_zero<double><<<nblk(3 * n, 256), 256, 0, s>>>(ctx->grad_p, 3 * (size_t)n);
+        KCHECK();
+        k_zero<double><<<nblk(3 * n, 256), 256, 0, s>>>(ctx->trq_p, 3 * (size_t)n);
+        KCHECK();
+        k_pack_u<R><<<nblk(n), kThreads, 0, s>>>(n, ctx->ud, ctx->up, A.u4, ctx->rank);  // cell order
+        KCHECK();
+    }
+    // Real-space polarization pair kernels (atomic accumulation) on the side
+    // stream; the PME dipole potentials and the polarization energy on s.
+    // The reciprocal-space force kernels add to the same arrays without
+    // atomics, so they run after the join.
+    cudaStream_t r = fork_side(ctx, s);
+    double* virp = ctx->want_vir ? ctx->eacc + kVirP : nullptr;  // ep terms
     if (polgrad) {
         auto launch = [&](auto kern, int lanes) {
             kern<<<nblk((size_t)n * lanes), kThreads, 0, r>>>(n, ctx->sids, A.atS, A.u4, ctx->bx, aew, ctx->cnb, ctx->cap,
                                                               ctx->nnb, mutual, ctx->f, ctx->grad_p, ctx->trq_p, virp);
         };
         if (ewald_cells(ctx)) {  // one lane count for the cell variants
-            if (vir) launch(k_polar_pair<R, true, 8, true, false, true>, 8);
+            if (virp) launch(k_polar_pair<R, true, 8, true, false, true>, 8);
             else launch(k_polar_pair<R, true, 8, false, false, true>, 8);
-        } else if (vir) {  // one lane count for the virial variants
+        } else if (virp) {  // one lane count for the virial variants
             if (ctx->ewald) launch(k_polar_pair<R, true, 8, true>, 8);
             else launch(k_polar_pair<R, false, 8, true>, 8);
         } else {
@@ -1419,11 +1493,6 @@ void enqueue_back(amg_ctx* ctx, cudaStream_t s, int flags) {
     }
     if (polgrad && ctx->ewald) pme_dipoles<R, 20>(ctx, s, ctx->ud, ctx->up, ctx->phiU, virp);
     join_side(ctx, s);
-    if (ctx->ewald) {
-        k_recip_mpole<<<nblk(n), kThreads, 0, s>>>(n, ctx->rp10, ctx->phiM, ctx->f, ctx->aewald, ctx->grad_m, ctx->trq_m,
-                                                   ctx->eacc + 2, analysis ? ctx->aem : nullptr, ctx->eacc + 3, vir);
-        KCHECK();
-    }
     if (polgrad) {
         if (ctx->ewald) {
             k_recip_polar<<<nblk(n), kThreads, 0, s>>>(n, ctx->rp10, ctx->phiM, ctx->phiU, ctx->phiU + 20 * (size_t)n,
@@ -1436,17 +1505,7 @@ void enqueue_back(amg_ctx* ctx, cudaStream_t s, int flags) {
                                               ctx->grad_p, virp);
         KCHECK();
     }
-    if (grad) {
-        k_torque<<<nblk(n), kThreads, 0, s>>>(n, ctx->xyz, ctx->zax, ctx->xax, ctx->yax, ctx->axe, ctx->trq_m,
-                                              ctx->grad_m, vir);
-        KCHECK();
-        if (ctx->cflux) {  // the gradient through the geometry-dependent monopoles
-            k_cflux_grad<<<nblk((size_t)ctx->nbond + ctx->nangle), kThreads, 0, s>>>(
-                ctx->nbond, ctx->bonds, ctx->bflux, ctx->nangle, ctx->angles, ctx->aflux, ctx->xyz, ctx->cfpot,
-                ctx->grad_m, vir);
-            KCHECK();
-        }
-    }
+    join_mpole(ctx, s);
     CK(cudaEventRecord(ctx->ev[4], s));
 }
 
@@ -1474,6 +1533,7 @@ bool capture_graph(amg_ctx* ctx, int flags) {
     long long kb = 0;
     try {
         enqueue_front<R>(ctx, s);
+        enqueue_mpole_forces<R>(ctx, fork_mpole(ctx, s), flags);
         if (ctx->poltyp == AMG_POL_OPT && ctx->npolar > 0) enqueue_opt<R>(ctx, s);
         if (iterative(ctx)) {
             const cudaGraphNode_t* deps = nullptr;
@@ -1517,7 +1577,7 @@ bool capture_graph(amg_ctx* ctx, int flags) {
     if (e != cudaSuccess) return fail("end capture", e);
     if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
     ctx->gexec = nullptr;
-    e = cudaGraphInstantiate(&ctx->gexec, graph, 0);
+    e = cudaGraphInstantiate(&ctx->gexec, graph, cudaGraphInstantiateFlagUseNodePriority);
     cudaGraphDestroy(graph);
     if (e != cudaSuccess) {
         ctx->gexec = nullptr;
@@ -1535,6 +1595,7 @@ template <class R>
 void enqueue_eager(amg_ctx* ctx, int flags) {
     cudaStream_t s = ctx->st;
     enqueue_front<R>(ctx, s);
+    enqueue_mpole_forces<R>(ctx, fork_mpole(ctx, s), flags);
     if (ctx->poltyp == AMG_POL_OPT && ctx->npolar > 0) enqueue_opt<R>(ctx, s);
     if (iterative(ctx)) {
         enqueue_predict(ctx, s);
@@ -1563,7 +1624,9 @@ int forward_impl(amg_ctx* ctx, int flags, amg_results* res) {
         CK(cudaMallocHost((void**)&ctx->rb, sizeof(amg_ctx::Readback)));
         CK(cudaMallocHost((void**)&ctx->rb_grad, sizeof(double) * 6 * (size_t)n));
         for (auto& e : ctx->rbev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        for (auto& e : ctx->rbevm) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
+    bool dem_added = false;  // the permanent-multipole gradient is in res->dem
     for (int attempt = 0; attempt < 2; attempt++) {
         ensure_list_buffers(ctx);
         if (iterative(ctx)) ensure_coeff_buffers<R>(ctx, atoms_of<R>(ctx));
@@ -1591,16 +1654,40 @@ int forward_impl(amg_ctx* ctx, int flags, amg_results* res) {
         CK(cudaMemcpyAsync(&rb->iters, ctx->iter, sizeof(int), cudaMemcpyDeviceToHost, st));
         CK(cudaEventRecord(ctx->rbev[0], st));
         // the gradients in kRbChunks pieces, each with its event: the host adds
-        // a piece to the caller's arrays while the next one is in flight
+        // a piece to the caller's arrays while the next one is in flight.  The
+        // permanent-multipole gradient is final once its force stream is done
+        // (gm_ready), so its pieces are copied, and added, beside the solve;
+        // the list-overflow flag, final by then too, is read with them.
         const size_t n3 = 3 * (size_t)n, piece = (n3 + kRbChunks - 1) / kRbChunks;
+        const bool early_m = grad && res->dem;
+        if (early_m) {
+            CK(cudaStreamWaitEvent(ctx->rbst, ctx->gm_ready, 0));
+            CK(cudaMemcpyAsync(&rb->over_m, ctx->overflow, sizeof(int), cudaMemcpyDeviceToHost, ctx->rbst));
+            for (int k = 0; k < kRbChunks; k++) {
+                const size_t a = std::min(n3, k * piece), b = std::min(n3, a + piece);
+                if (b > a)
+                    CK(cudaMemcpyAsync(ctx->rb_grad + a, ctx->grad_m + a, sizeof(double) * (b - a),
+                                       cudaMemcpyDeviceToHost, ctx->rbst));
+                CK(cudaEventRecord(ctx->rbevm[k], ctx->rbst));
+            }
+        }
         for (int k = 0; k < kRbChunks; k++) {
             const size_t a = std::min(n3, k * piece), b = std::min(n3, a + piece);
-            if (b > a && grad && res->dem)
-                CK(cudaMemcpyAsync(ctx->rb_grad + a, ctx->grad_m + a, sizeof(double) * (b - a), cudaMemcpyDeviceToHost, st));
             if (b > a && grad && res->dep && ctx->has_pol)
                 CK(cudaMemcpyAsync(ctx->rb_grad + n3 + a, ctx->grad_p + a, sizeof(double) * (b - a),
                                    cudaMemcpyDeviceToHost, st));
             CK(cudaEventRecord(ctx->rbev[1 + k], st));
+        }
+        if (early_m) {
+            CK(cudaEventSynchronize(ctx->rbevm[0]));  // over_m landed before the first piece
+            if (rb->over_m <= ctx->cap) {
+                dem_added = true;
+                for (int k = 0; k < kRbChunks; k++) {
+                    const size_t a = std::min(n3, k * piece), b = std::min(n3, a + piece);
+                    CK(cudaEventSynchronize(ctx->rbevm[k]));
+                    for (size_t q = a; q < b; q++) res->dem[q] += ctx->rb_grad[q];
+                }
+            }
         }
         CK(cudaEventSynchronize(ctx->rbev[0]));
         const int over = rb->over;
@@ -1665,7 +1752,7 @@ int forward_impl(amg_ctx* ctx, int flags, amg_results* res) {
     res->pcg_iters = iters;
     res->pcg_eps = eps;
     if (grad) {  // added to the caller's arrays piece by piece as the copies land
-        double* dem = res->dem;
+        double* dem = dem_added ? nullptr : res->dem;
         double* dep = ctx->has_pol ? res->dep : nullptr;
         const size_t n3 = 3 * (size_t)n, piece = (n3 + kRbChunks - 1) / kRbChunks;
         const double* gm = ctx->rb_grad;
@@ -1719,6 +1806,10 @@ void release(amg_ctx* ctx) {
     if (ctx->rb_grad) { cudaFreeHost(ctx->rb_grad); ctx->rb_grad = nullptr; }
     for (auto& e : ctx->rbev)
         if (e) { cudaEventDestroy(e); e = nullptr; }
+    for (auto& e : ctx->rbevm)
+        if (e) { cudaEventDestroy(e); e = nullptr; }
+    if (ctx->gm_ready) { cudaEventDestroy(ctx->gm_ready); ctx->gm_ready = nullptr; }
+    if (ctx->rbst) { cudaStreamDestroy(ctx->rbst); ctx->rbst = nullptr; }
     if (ctx->adj_host) { cudaFreeHost(ctx->adj_host); ctx->adj_host = nullptr; }
     double** dbl[] = {&ctx->pole13, &ctx->pol, &ctx->thole, &ctx->pdamp, &ctx->xyz, &ctx->rp10, &ctx->Ed, &ctx->Ep,
                       &ctx->ud, &ctx->up, &ctx->rd, &ctx->rp, &ctx->zd, &ctx->zp, &ctx->pd, &ctx->pp, &ctx->Apd,
@@ -1749,7 +1840,7 @@ void release(amg_ctx* ctx) {
     pme_destroy(ctx->pmd);
     for (auto& e : ctx->ev)
         if (e) { cudaEventDestroy(e); e = nullptr; }
-    for (int k = 0; k < 2; k++) {
+    for (int k = 0; k < 3; k++) {
         if (ctx->efork[k]) { cudaEventDestroy(ctx->efork[k]); ctx->efork[k] = nullptr; }
         if (ctx->ejoin[k]) { cudaEventDestroy(ctx->ejoin[k]); ctx->ejoin[k] = nullptr; }
         if (ctx->side[k]) { cudaStreamDestroy(ctx->side[k]); ctx->side[k] = nullptr; }
@@ -1765,6 +1856,7 @@ void release(amg_ctx* ctx) {
     dfree(ctx->pred_hist); dfree(ctx->pred_state);
     dfree(ctx->pcore); dfree(ctx->palpha); dfree(ctx->dq); dfree(ctx->cfpot);
     dfree(ctx->bonds); dfree(ctx->bflux); dfree(ctx->angles); dfree(ctx->aflux);
+    if (ctx->erot) { cudaEventDestroy(ctx->erot); ctx->erot = nullptr; }
     if (ctx->st) { cudaStreamDestroy(ctx->st); ctx->st = nullptr; }
     if (ctx->st2) { cudaStreamDestroy(ctx->st2); ctx->st2 = nullptr; }
 }
@@ -1832,10 +1924,15 @@ int create_impl(amg_ctx* ctx, const amg_params* P) {
     ctx->usolvcut = std::min(P->usolvcut, P->cutoff);
     ctx->cell_shape = P->cell_shape;
     for (int a = 0; a < 3; a++) ctx->K[a] = P->nfft[a];
-    CK(cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking));
-    CK(cudaStreamCreateWithFlags(&ctx->st2, cudaStreamNonBlocking));
-    for (int k = 0; k < 2; k++) {
-        CK(cudaStreamCreateWithFlags(&ctx->side[k], cudaStreamNonBlocking));
+    // the solve's streams at the highest priority, the permanent-multipole
+    // force stream at the lowest: its blocks fill what the solve leaves idle
+    int plo = 0, phi = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&plo, &phi));
+    const int pmain = phi;
+    CK(cudaStreamCreateWithPriority(&ctx->st, cudaStreamNonBlocking, pmain));
+    CK(cudaStreamCreateWithPriority(&ctx->st2, cudaStreamNonBlocking, pmain));
+    for (int k = 0; k < 3; k++) {
+        CK(cudaStreamCreateWithPriority(&ctx->side[k], cudaStreamNonBlocking, k == kMpoleSide ? plo : pmain));
         CK(cudaEventCreateWithFlags(&ctx->efork[k], cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&ctx->ejoin[k], cudaEventDisableTiming));
     }
@@ -1858,6 +1955,9 @@ int create_impl(amg_ctx* ctx, const amg_params* P) {
         dalloc(ctx, ctx->uopt, (size_t)(ctx->optorder + 1) * 6 * n + 3 * (size_t)n);
     }
     for (auto& e : ctx->ev) CK(cudaEventCreate(&e));
+    CK(cudaEventCreateWithFlags(&ctx->erot, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&ctx->gm_ready, cudaEventDisableTiming));
+    CK(cudaStreamCreateWithFlags(&ctx->rbst, cudaStreamNonBlocking));
     upload(ctx, ctx->pole13, P->pole, 13 * (size_t)n);
     upload(ctx, ctx->zax, P->zaxis, n);
     upload(ctx, ctx->xax, P->xaxis, n);

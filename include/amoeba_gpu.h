@@ -225,7 +225,9 @@ int amg_create(const amg_params* params, amg_ctx** out);
  * the angles) is the reference's image() (src/md/image.cpp:37-124).  With Ewald
  * in a truncated octahedron or rhombic dodecahedron the cell volume is half the
  * enclosing prism's (a^3 / 2 and a^3 / sqrt(2)); the dodecahedron needs c = a,
- * for which its image is a lattice (UNSUPPORTED otherwise). */
+ * for which its image is a lattice (UNSUPPORTED otherwise).  A non-finite
+ * coordinate returns AMG_ERR_NAN and leaves the context without coordinates
+ * until the next successful call. */
 int amg_set_coords(amg_ctx* ctx, const double* xyz, const double box[6]);
 
 /* Evaluates em and ep (and their gradients, analysis data, dipoles) for the

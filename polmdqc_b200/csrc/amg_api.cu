@@ -2437,6 +2437,18 @@ int amg_create(const amg_params* params, amg_ctx** out) {
     return AMG_OK;
 }
 
+// true when no value is an infinity or a NaN (exponent bits not all set);
+// branch-free, so the compiler vectorises it
+static bool all_finite(const double* x, size_t count) {
+    uint64_t bad = 0;
+    for (size_t i = 0; i < count; i++) {
+        uint64_t b;
+        std::memcpy(&b, x + i, sizeof b);
+        bad |= (uint64_t)((b & 0x7ff0000000000000ull) == 0x7ff0000000000000ull);
+    }
+    return bad == 0;
+}
+
 int amg_set_coords(amg_ctx* ctx, const double* xyz, const double box[6]) {
     if (!ctx || !xyz) return AMG_ERR_BAD_ARG;
     try {
@@ -2476,13 +2488,15 @@ int amg_set_coords(amg_ctx* ctx, const double* xyz, const double box[6]) {
         } else {
             for (int a = 0; a < 3; a++) { ctx->bx.L[a] = 0; ctx->bx.iL[a] = 0; }
         }
-        for (int i = 0; i < 3 * ctx->n; i++)
-            if (!std::isfinite(xyz[i])) {
-                ctx->err = "non-finite coordinate";
-                return AMG_ERR_NAN;
-            }
-        cell_grid(ctx, xyz);
+        // the copy is under way while the host checks the values (a non-finite
+        // coordinate leaves the context without coordinates)
+        ctx->have_coords = false;
         CK(cudaMemcpyAsync(ctx->xyz, xyz, sizeof(double) * 3 * ctx->n, cudaMemcpyHostToDevice, ctx->st));
+        if (!all_finite(xyz, 3 * (size_t)ctx->n)) {
+            ctx->err = "non-finite coordinate";
+            return AMG_ERR_NAN;
+        }
+        cell_grid(ctx, xyz);
         ctx->have_coords = true;
         ctx->have_forward = false;
     } catch (Fail& f) {

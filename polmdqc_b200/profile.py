@@ -23,6 +23,8 @@ def main():
     ap.add_argument("--fp64", action="store_true")
     ap.add_argument("--bench", type=int, default=0, help="also time this many device-resident evaluations")
     ap.add_argument("--backward", type=int, default=0, help="then this many amg_backward calls (host wall time)")
+    ap.add_argument("--e2e", type=int, default=0,
+                    help="also time this many calls of set_coords + forward from pinned host buffers (host wall time)")
     a = ap.parse_args()
     box, grid = BOXES[a.waters]
     s = systems.water_box(a.waters, box, seed=0)
@@ -36,6 +38,22 @@ def main():
         ms, launches = e.bench(a.bench, flush_bytes=256 << 20)
         print(f"device ms per evaluation: median {sorted(ms)[len(ms) // 2]:.3f} min {ms.min():.3f} "
               f"launches {launches}")
+    if a.e2e:
+        import time
+        import torch  # pinned host buffers
+        n = s.n
+        xyz = torch.from_numpy(s.xyz.reshape(-1).copy()).pin_memory().numpy()
+        dem = torch.zeros(3 * n, dtype=torch.float64).pin_memory().numpy()
+        dep = torch.zeros(3 * n, dtype=torch.float64).pin_memory().numpy()
+        flags = abi.DO_ENERGY | abi.DO_GRADIENT
+        for _ in range(3):
+            e.set_coords(xyz)
+            e.forward_into(flags, dem, dep)
+        t0 = time.perf_counter()
+        for _ in range(a.e2e):
+            e.set_coords(xyz)
+            e.forward_into(flags, dem, dep)
+        print(f"end-to-end ms per evaluation (host wall): {1000.0 * (time.perf_counter() - t0) / a.e2e:.3f}")
     if a.backward:
         import time
         e.backward(1.0)

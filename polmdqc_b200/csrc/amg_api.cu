@@ -190,6 +190,10 @@ struct amg_ctx {
     // captured evaluation (periodic systems)
     bool use_graphs = true, graph_dirty = true, graphed_last = false;
     cudaGraphExec_t gexec = nullptr;
+    // the adjoint solve captured the same way (set-up, conditional WHILE
+    // node, sweep); recaptured after every capture of the forward (fwd_gen)
+    cudaGraphExec_t adj_gexec = nullptr;
+    long long fwd_gen = 0, adj_gen = -1;
     int gflags = -1;
     // kernel launches of this library: counter, and per captured graph the
     // launches outside the PCG loop and per loop iteration
@@ -1141,7 +1145,8 @@ void enqueue_pcg_iter(amg_ctx* ctx, cudaStream_t s, cudaGraphConditionalHandle h
                                               ctx->scal + PAP_P);
         KCHECK();
     }
-    k_pcg_update<R><<<nblk(3 * (size_t)n, 256), 256, 0, s>>>(n, ctx->pol, ctx->pd, ctx->pp, ctx->Apd, ctx->App, ctx->ud, ctx->up,
+    const unsigned ublocks = (unsigned)std::min<size_t>(nblk(3 * (size_t)n, 256), (size_t)ctx->num_sms * 4);
+    k_pcg_update<R><<<ublocks, 256, 0, s>>>(n, ctx->pol, ctx->pd, ctx->pp, ctx->Apd, ctx->App, ctx->ud, ctx->up,
                                                  ctx->rd, ctx->rp, ctx->zd, ctx->zp, ctx->scal,
                                                  ctx->sparse_prec ? A.s4 : nullptr, ctx->rank,
                                                  apart ? ctx->Fd : nullptr, apart ? ctx->Fp : nullptr,
@@ -1585,6 +1590,7 @@ bool capture_graph(amg_ctx* ctx, int flags) {
     }
     ctx->gflags = flags;
     ctx->graph_dirty = false;
+    ctx->fwd_gen++;
     ctx->kbody = kb;
     ctx->kmain = ctx->kcount - k0 - kb;
     ctx->kcount = k0;
@@ -1846,6 +1852,7 @@ void release(amg_ctx* ctx) {
         if (ctx->side[k]) { cudaStreamDestroy(ctx->side[k]); ctx->side[k] = nullptr; }
     }
     if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
+    if (ctx->adj_gexec) { cudaGraphExecDestroy(ctx->adj_gexec); ctx->adj_gexec = nullptr; }
     dfree(ctx->iter);
     dfree(ctx->cont);
     dfree(ctx->blk_done);
@@ -2191,7 +2198,83 @@ void host_copy(double* dst, const double* src, size_t cnt) {
 // caller has pointed the context's field and dipole vectors at g and w, with
 // w = alpha g as the starting guess.
 template <class R>
+bool capture_adjoint(amg_ctx* ctx) {
+    cudaStream_t s = ctx->st;
+    cudaGraph_t graph = nullptr;
+    const long long k0 = ctx->kcount;
+    auto fail = [&](cudaError_t) {
+        cudaStreamCaptureStatus st;
+        if (cudaStreamIsCapturing(s, &st) == cudaSuccess && st != cudaStreamCaptureStatusNone) {
+            cudaGraph_t g2 = nullptr;
+            cudaStreamEndCapture(s, &g2);
+            if (g2) cudaGraphDestroy(g2);
+        }
+        cudaGetLastError();
+        ctx->kcount = k0;
+        return false;
+    };
+    cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return fail(e);
+    try {
+        const cudaGraphNode_t* deps = nullptr;
+        size_t ndeps = 0;
+        cudaStreamCaptureStatus cs;
+        e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &graph, &deps, &ndeps);
+        if (e != cudaSuccess) return fail(e);
+        cudaGraphConditionalHandle h;
+        e = cudaGraphConditionalHandleCreate(&h, graph, 0, 0);
+        if (e != cudaSuccess) return fail(e);
+        enqueue_pcg_init<R>(ctx, s, h, 1, true);
+        e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &graph, &deps, &ndeps);
+        if (e != cudaSuccess) return fail(e);
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t cnode;
+        e = cudaGraphAddNode(&cnode, graph, deps, ndeps, &cp);
+        if (e != cudaSuccess) return fail(e);
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        e = cudaStreamUpdateCaptureDependencies(s, &cnode, 1, cudaStreamSetCaptureDependencies);
+        if (e != cudaSuccess) return fail(e);
+        e = cudaStreamBeginCaptureToGraph(ctx->st2, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return fail(e);
+        enqueue_pcg_iter<R>(ctx, ctx->st2, h, 1);
+        e = cudaStreamEndCapture(ctx->st2, &body);
+        if (e != cudaSuccess) return fail(e);
+        enqueue_sweep(ctx, s);
+    } catch (Fail&) {
+        return fail(cudaGetLastError());
+    }
+    e = cudaStreamEndCapture(s, &graph);
+    if (e != cudaSuccess) return fail(e);
+    if (ctx->adj_gexec) cudaGraphExecDestroy(ctx->adj_gexec);
+    ctx->adj_gexec = nullptr;
+    e = cudaGraphInstantiate(&ctx->adj_gexec, graph, cudaGraphInstantiateFlagUseNodePriority);
+    cudaGraphDestroy(graph);
+    ctx->kcount = k0;
+    if (e != cudaSuccess) {
+        ctx->adj_gexec = nullptr;
+        cudaGetLastError();
+        return false;
+    }
+    ctx->adj_gen = ctx->fwd_gen;
+    return true;
+}
+
+template <class R>
 void adjoint_solve(amg_ctx* ctx, cudaStream_t s) {
+    // periodic systems: one graph launch, the loop's control on the device
+    // (captured with the vectors the caller set; they are the same buffers on
+    // every call)
+    if (ctx->use_graphs && ctx->bounds && ctx->gexec) {
+        if (!ctx->adj_gexec || ctx->adj_gen != ctx->fwd_gen) capture_adjoint<R>(ctx);
+        if (ctx->adj_gexec) {
+            CK(cudaGraphLaunch(ctx->adj_gexec, s));
+            return;
+        }
+    }
     enqueue_pcg_init<R>(ctx, s, 0, 0, true);
     int cont = 1;
     while (true) {

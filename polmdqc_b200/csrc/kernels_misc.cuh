@@ -135,13 +135,13 @@ __global__ void k_pcg_update(int n, const double* __restrict__ pol, const double
                              const double* __restrict__ Fp, int* __restrict__ done, int* __restrict__ iter,
                              double thr2, int maxit, int roll, cudaGraphConditionalHandle h, int use_handle,
                              int* __restrict__ cont_out) {
-    // one thread per vector component q = 3i + c: the site loop had too few
-    // threads in flight for its chains of dependent loads
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    // one thread per vector component q = 3i + c (the site loop had too few
+    // threads in flight for its chains of dependent loads), blocks striding
+    // over the components so that few blocks add to the scalars
     double ad = scal[PAP_D] != 0 ? scal[RZ_D] / scal[PAP_D] : 0.0;
     double ap = scal[PAP_P] != 0 ? scal[RZ_P] / scal[PAP_P] : 0.0;
     double rzd = 0, rzp = 0, rrd = 0, rrp = 0;
-    if (q < 3 * n) {
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < 3 * n; q += gridDim.x * blockDim.x) {
         const int i = q / 3, c = q - 3 * (q / 3);
         const double a = pol[i];
         ud[q] += ad * pd[q];

@@ -624,6 +624,28 @@ void cell_grid(amg_ctx* ctx, const double* hxyz) {
                 }
             }
         }
+        if (b.shape >= 3) {
+            // truncated octahedron / rhombic dodecahedron (equal box lengths):
+            // the lattice is the enclosing prism's (L, L, L; or L, L, sqrt(2) L)
+            // plus half of every edge, so the cells of the prism with an even
+            // count of at least 6 per axis, and the stencil around the home
+            // cell plus the one half a prism away, hold every atom within the
+            // cutoff (k_neighbors_cells<false, true>)
+            const double L = ctx->box[0];
+            const bool equal = std::fabs(ctx->box[1] - L) <= 1e-12 * L && std::fabs(ctx->box[2] - L) <= 1e-12 * L;
+            const double P[3] = {L, L, b.shape == 4 ? kSqrt2 * L : L};
+            int nc[3];
+            for (int a = 0; a < 3; a++) nc[a] = std::min(256, (int)std::floor(P[a] / ctx->cut)) & ~1;
+            if (equal && nc[0] >= 6 && nc[1] >= 6 && nc[2] >= 6) {
+                cg.centred = 1;
+                for (int a = 0; a < 3; a++) {
+                    cg.nc[a] = nc[a];
+                    cg.size[a] = P[a] / nc[a];
+                    cg.off_lo[a] = -1;
+                    cg.off_hi[a] = 1;
+                }
+            }
+        }
         return;
     }
     double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
@@ -747,7 +769,8 @@ void enqueue_lists(amg_ctx* ctx, cudaStream_t s) {
         // FP64 decision within 1e-3 cut^2 of the cutoff
         // (monoclinic and triclinic cells: parallelepiped cells, every pair
         // decided by the FP64 image of the cell)
-        auto kern = cg.general ? k_neighbors_cells<true> : k_neighbors_cells<false>;
+        auto kern = cg.general ? k_neighbors_cells<true> : cg.centred ? k_neighbors_cells<false, true>
+                                                                      : k_neighbors_cells<false>;
         kern<<<(unsigned)ncell, kNbrThreads, 0, s>>>(ctx->spos, ctx->sids, ctx->cstart, ctx->cend, cg, ctx->bx, cut2,
                                                      1e-3 * cut2, ctx->cap, ctx->xoff, ctx->xidx, ctx->xrange, ctx->nbr,
                                                      ctx->cnb, ctx->nnb, ctx->overflow);

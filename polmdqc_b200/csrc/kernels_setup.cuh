@@ -126,6 +126,10 @@ struct CellGrid {
     // lattice vectors (x = sum_a s_a A[a])
     int general;
     double R[3][3], A[3][3];
+    // truncated octahedron / rhombic dodecahedron: cells of the enclosing
+    // prism (edges size * nc, an even count per axis), whose lattice plus the
+    // centring translation (half of every edge) is the cell's lattice
+    int centred;
 };
 
 // fractional coordinates of x in [0, 1) along each lattice vector
@@ -153,7 +157,11 @@ __global__ void k_cell_index(int n, const double* __restrict__ xyz, CellGrid cg,
     for (int a = 0; a < 3; a++) {
         double x = xyz[3 * i + a];
         double f;
-        if (cg.periodic) {
+        if (cg.centred) {  // wrapped into the enclosing prism
+            f = x / (cg.size[a] * cg.nc[a]);
+            f -= floor(f);
+            c[a] = min(cg.nc[a] - 1, (int)(f * cg.nc[a]));
+        } else if (cg.periodic) {
             f = x * bx.iL[a];
             f -= floor(f);
             c[a] = min(cg.nc[a] - 1, (int)(f * cg.nc[a]));
@@ -284,7 +292,13 @@ constexpr int kNbrChunk = 1280;
 constexpr int kNbrHome = 128;
 constexpr int kNbrThreads = 256;
 
-template <bool GENERAL>
+// CENTRED (truncated octahedron, rhombic dodecahedron): the stencil is the 27
+// cells around the home cell plus the 27 around the cell half a prism away,
+// whose sites reach the home cell by the centring translation; with an even
+// count of at least 6 cells per axis the two stencils are disjoint, so each
+// site is a candidate at most once, and every candidate within reach is
+// decided by the cell's FP64 image().
+template <bool GENERAL, bool CENTRED = false>
 __global__ void __launch_bounds__(kNbrThreads) k_neighbors_cells(
     const double4* __restrict__ spos, const int* __restrict__ sids, const int* __restrict__ cstart,
     const int* __restrict__ cend, CellGrid cg, Box bx, double cut2, double margin, int cap,
@@ -300,8 +314,8 @@ __global__ void __launch_bounds__(kNbrThreads) k_neighbors_cells(
     __shared__ float4 hpos[kNbrHome];
     __shared__ int hid[kNbrHome], hx0[kNbrHome], hx1[kNbrHome];
     __shared__ int2 hxr[kNbrHome];
-    __shared__ int rstart[27], rpre[28];
-    __shared__ double rshift[27][3];
+    __shared__ int rstart[54], rpre[55];
+    __shared__ double rshift[54][3];
     __shared__ int nst;
     const int cell = blockIdx.x;
     const int hs = cstart[cell], he = cend[cell];
@@ -316,51 +330,61 @@ __global__ void __launch_bounds__(kNbrThreads) k_neighbors_cells(
             corner[a] = (double)cc[0] / cg.nc[0] * cg.A[0][a] + (double)cc[1] / cg.nc[1] * cg.A[1][a] +
                         (double)cc[2] / cg.nc[2] * cg.A[2][a];
     if (threadIdx.x < 32) {
-        // stencil cell k = lane (all of a warp's loads of cstart/cend in
-        // flight at once), lengths summed by a warp scan; cells outside an
-        // open system's grid count as empty
+        // stencil cell k = lane (+ 32 in a second round: all of a warp's loads
+        // of cstart/cend in flight at once), lengths summed by a warp scan;
+        // cells outside an open system's grid count as empty
         const int na0 = cg.off_hi[0] - cg.off_lo[0] + 1, na1 = cg.off_hi[1] - cg.off_lo[1] + 1;
         const int na2 = cg.off_hi[2] - cg.off_lo[2] + 1;
-        const int k = threadIdx.x, total = na0 * na1 * na2;
-        int len = 0;
-        if (k < total) {
-            const int d[3] = {cg.off_lo[0] + k / (na1 * na2), cg.off_lo[1] + (k / na2) % na1, cg.off_lo[2] + k % na2};
-            int q[3];
-            double sh[3];
-            bool skip = false;
-            int wrap[3] = {0, 0, 0};
-            for (int a = 0; a < 3; a++) {
-                q[a] = cc[a] + d[a];
-                sh[a] = 0.0;
-                if (cg.periodic) {
-                    if (q[a] < 0) { q[a] += cg.nc[a]; sh[a] = -bx.L[a]; wrap[a] = -1; }
-                    else if (q[a] >= cg.nc[a]) { q[a] -= cg.nc[a]; sh[a] = bx.L[a]; wrap[a] = 1; }
-                } else if (q[a] < 0 || q[a] >= cg.nc[a]) {
-                    skip = true;
+        const int n27 = na0 * na1 * na2, total = CENTRED ? 2 * n27 : n27;
+        int carry = 0;
+        for (int k0 = 0; k0 < total; k0 += 32) {
+            const int k = k0 + (int)threadIdx.x;
+            int len = 0;
+            if (k < total) {
+                const int kk = k < n27 ? k : k - n27;  // the second 27: around the centred cell
+                const int d[3] = {cg.off_lo[0] + kk / (na1 * na2), cg.off_lo[1] + (kk / na2) % na1,
+                                  cg.off_lo[2] + kk % na2};
+                int q[3];
+                double sh[3];
+                bool skip = false;
+                int wrap[3] = {0, 0, 0};
+                for (int a = 0; a < 3; a++) {
+                    // prism edge: the centred grids' own, else the box's
+                    const double La = CENTRED ? cg.size[a] * cg.nc[a] : bx.L[a];
+                    const int half = (CENTRED && k >= n27) ? cg.nc[a] / 2 : 0;
+                    q[a] = cc[a] + half + d[a];
+                    sh[a] = half ? -0.5 * La : 0.0;  // the centring translation
+                    if (cg.periodic) {
+                        if (q[a] < 0) { q[a] += cg.nc[a]; sh[a] -= La; wrap[a] = -1; }
+                        else if (q[a] >= cg.nc[a]) { q[a] -= cg.nc[a]; sh[a] += La; wrap[a] = 1; }
+                    } else if (q[a] < 0 || q[a] >= cg.nc[a]) {
+                        skip = true;
+                    }
                 }
+                if (GENERAL)  // the periodic image is a lattice translation
+                    for (int a = 0; a < 3; a++)
+                        sh[a] = wrap[0] * cg.A[0][a] + wrap[1] * cg.A[1][a] + wrap[2] * cg.A[2][a];
+                rstart[k] = 0;
+                if (!skip) {
+                    const int qc = (q[0] * cg.nc[1] + q[1]) * cg.nc[2] + q[2];
+                    const int s0 = cstart[qc];
+                    len = max(cend[qc] - s0, 0);
+                    rstart[k] = s0;
+                }
+                for (int a = 0; a < 3; a++) rshift[k][a] = sh[a];
             }
-            if (GENERAL)  // the periodic image is a lattice translation
-                for (int a = 0; a < 3; a++)
-                    sh[a] = wrap[0] * cg.A[0][a] + wrap[1] * cg.A[1][a] + wrap[2] * cg.A[2][a];
-            rstart[k] = 0;
-            if (!skip) {
-                const int qc = (q[0] * cg.nc[1] + q[1]) * cg.nc[2] + q[2];
-                const int s0 = cstart[qc];
-                len = max(cend[qc] - s0, 0);
-                rstart[k] = s0;
-            }
-            for (int a = 0; a < 3; a++) rshift[k][a] = sh[a];
-        }
-        int incl = len;  // inclusive scan over the warp
+            int incl = len;  // inclusive scan over the warp
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int v = __shfl_up_sync(0xffffffffu, incl, o);
-            if (k >= o) incl += v;
-        }
-        if (k < total) rpre[k] = incl - len;
-        if (k == total - 1) {
-            rpre[total] = incl;
-            nst = total;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                if ((int)threadIdx.x >= o) incl += v;
+            }
+            if (k < total) rpre[k] = carry + incl - len;
+            if (k == total - 1) {
+                rpre[total] = carry + incl;
+                nst = total;
+            }
+            carry += __shfl_sync(0xffffffffu, incl, 31);
         }
     }
     __syncthreads();
@@ -377,7 +401,12 @@ __global__ void __launch_bounds__(kNbrThreads) k_neighbors_cells(
         const double xs[3] = {x.x, x.y, x.z};
         for (int a = 0; a < 3; a++) {
             double v = xs[a];
-            if (cg.periodic) v -= bx.L[a] * floor(v * bx.iL[a]);
+            if (CENTRED) {
+                const double La = cg.size[a] * cg.nc[a];
+                v -= La * floor(v / La);
+            } else if (cg.periodic) {
+                v -= bx.L[a] * floor(v * bx.iL[a]);
+            }
             o[a] = v - corner[a];
         }
     };
@@ -446,11 +475,11 @@ __global__ void __launch_bounds__(kNbrThreads) k_neighbors_cells(
                             // near the cutoff the FP64 minimum image decides; in a
                             // general cell it decides every pair, so the pair set
                             // is that of the cell's image(), as in k_neighbors
-                            if (hit && (r2 > lo2 || GENERAL)) {
+                            if (hit && (r2 > lo2 || GENERAL || CENTRED)) {
                                 const double4 xi = spos[ph];
                                 const double4 pj = spos[csrt[t]];
-                                const V3<double> r =
-                                    min_image<double, GENERAL>(v3<double>(pj.x - xi.x, pj.y - xi.y, pj.z - xi.z), bx);
+                                const V3<double> r = min_image<double, GENERAL || CENTRED>(
+                                    v3<double>(pj.x - xi.x, pj.y - xi.y, pj.z - xi.z), bx);
                                 hit = dot(r, r) <= cut2;
                             }
                             if (hit && j >= xr.x && j <= xr.y) {  // only then can j be a scaled partner

@@ -359,19 +359,21 @@ def cell_image(d: np.ndarray, cell_shape: int, L: float) -> np.ndarray:
 
 
 def water_cell(cell_shape: int, L: float = 24.8, seed: int = 0, jitter: float = 0.25, prm: str = "water03",
-               min_contact: float = 1.7, tries: int = 200) -> System:
+               min_contact: float = 1.7, tries: int = 200, per_edge: int = 8) -> System:
     """Rigid AMOEBA waters filling a truncated octahedron or a rhombic
     dodecahedron of box length L.  O sit on a jittered lattice of the
-    enclosing prism (8 sites per L along x and y; 8 along z for the
-    octahedron, 12 along the dodecahedron's sqrt(2) L), one of each pair of
+    enclosing prism (`per_edge` sites per L along x and y, an even number; as
+    many along z for the octahedron, 1.5 times as many along the
+    dodecahedron's sqrt(2) L), one of each pair of
     sites that the cell's centring translation (half of every prism edge)
     exchanges, so the periodic images complete the lattice; orientations are
     uniform random, redrawn while an atom comes within `min_contact` of
     another molecule's atom under the cell's minimum image."""
     edges = prism_edges(cell_shape, L)
-    nz = 12 if cell_shape == abi.CELL_DODECAHEDRON else 8
-    steps = edges / np.array([8, 8, nz])
-    grid = np.stack(np.meshgrid(np.arange(4), np.arange(8), np.arange(nz), indexing="ij"), -1).reshape(-1, 3)
+    m = per_edge
+    nz = 3 * m // 2 if cell_shape == abi.CELL_DODECAHEDRON else m
+    steps = edges / np.array([m, m, nz])
+    grid = np.stack(np.meshgrid(np.arange(m // 2), np.arange(m), np.arange(nz), indexing="ij"), -1).reshape(-1, 3)
     rng = np.random.default_rng(seed)
     O = (grid + 0.5) * steps - 0.5 * edges + rng.uniform(-jitter, jitter, (len(grid), 3))
     orng = np.random.default_rng(seed + 1)

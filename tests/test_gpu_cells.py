@@ -81,3 +81,41 @@ def test_mixed_cell_meets_the_target(case):
     frms = float(np.sqrt(np.mean((g.dem + g.dep - first(o.dem, n) - first(o.dep, n)) ** 2)))
     assert frms < 1e-4, (name, frms)
     assert dipole_rms(g, o, n) < 1e-5, name
+
+
+LARGE = {"octahedron": (abi.CELL_OCTAHEDRON, (48, 48, 48)),
+         "dodecahedron": (abi.CELL_DODECAHEDRON, (48, 48, 64))}
+
+
+@pytest.mark.parametrize("name", list(LARGE))
+def test_centred_cell_lists_at_size(name):
+    """A 43 A box of liquid density (1,372 and 2,058 waters): the neighbour
+    lists come from the cell grid of the enclosing prism (6 cells per axis, 8
+    along the dodecahedron's sqrt(2) L), searching
+    the 27 cells around each cell and the 27 around the cell half a prism away
+    (the centring translation), instead of the all-pairs search.  Without
+    Ewald the oracle runs the cell itself (the reference's image(), every
+    pair): the pair count is exact, FP64 energies and gradients agree.  With
+    Ewald the oracle runs the doubled prism, as above."""
+    shape, grid = LARGE[name]
+    s = systems.water_cell(shape, L=43.0, seed=4, per_edge=14)
+    flags = ALL | abi.DO_ANALYSIS
+    st = Settings(use_ewald=False, precision=FP64, poleps=1e-8)
+    o = oracle.forward(s, st, tol=1e-11, flags=flags)
+    g = run(s, st, flags)
+    assert g.nem == o.nem and o.nem > 0, (name, g.nem, o.nem)
+    assert abs(g.em - o.em) < 1e-10 * abs(o.em) and abs(g.ep - o.ep) < 1e-8 * abs(o.ep), name
+    np.testing.assert_allclose(g.dem, o.dem, atol=1e-8, rtol=0)
+    np.testing.assert_allclose(g.dep, o.dep, atol=1e-5, rtol=0)  # dipoles converged to 1e-8 D
+
+    n = s.n
+    o2 = oracle.forward(systems.doubled_prism(s), Settings(nfft=grid, precision=FP64), tol=1e-10, flags=ALL)
+    g64 = run(s, Settings(nfft=grid, precision=FP64, poleps=1e-8))
+    assert abs(g64.em - o2.em / 2) < 1e-10 * abs(o2.em / 2), (name, g64.em, o2.em / 2)
+    assert abs(g64.ep - o2.ep / 2) < 1e-8 * abs(o2.ep / 2), (name, g64.ep, o2.ep / 2)
+    assert dipole_rms(g64, o2, n) < 1e-7, name
+    np.testing.assert_allclose(g64.dem, first(o2.dem, n), atol=1e-6, rtol=0)
+    gm = run(s, Settings(nfft=grid, precision=MIXED))
+    assert abs(gm.em - o2.em / 2) < 1e-6 * abs(o2.em / 2) and abs(gm.ep - o2.ep / 2) < 1e-6 * abs(o2.ep / 2), name
+    frms = float(np.sqrt(np.mean((gm.dem + gm.dep - first(o2.dem, n) - first(o2.dep, n)) ** 2)))
+    assert frms < 1e-4, (name, frms)

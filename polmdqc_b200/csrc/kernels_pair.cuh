@@ -268,7 +268,7 @@ __global__ void __launch_bounds__(128) k_mpole_pair(int n, const int* __restrict
 // dipole-dipole term 1/2 [E(up_i, ud_k) + E(ud_i, up_k)] (the OPT cross
 // terms between perturbation orders; no torques).
 template <class R, bool EWALD, int LPA, bool VIR, bool DDONLY = false, bool CELLS = false>
-__global__ void __launch_bounds__(128) k_polar_pair(int n, const int* __restrict__ order, const AtomR<R>* __restrict__ at,
+__global__ void __launch_bounds__(128, (sizeof(R) == 4 && !VIR && !DDONLY) ? 6 : 1) k_polar_pair(int n, const int* __restrict__ order, const AtomR<R>* __restrict__ at,
                                                     const R4<R>* __restrict__ u4, Box bx, R aewald,
                                                     const int* __restrict__ nbr, int cap,
                                                     const int* __restrict__ nnb, int mutual, double f,

@@ -2595,8 +2595,10 @@ int amg_set_coords(amg_ctx* ctx, const double* xyz, const double box[6]) {
             for (int a = 0; a < 3; a++) { ctx->bx.L[a] = 0; ctx->bx.iL[a] = 0; }
         }
         // the copy is under way while the host checks the values (a non-finite
-        // coordinate leaves the context without coordinates)
+        // coordinate leaves the context without coordinates, and without the
+        // forward evaluation a backward needs)
         ctx->have_coords = false;
+        ctx->have_forward = false;
         CK(cudaMemcpyAsync(ctx->xyz, xyz, sizeof(double) * 3 * ctx->n, cudaMemcpyHostToDevice, ctx->st));
         if (!all_finite(xyz, 3 * (size_t)ctx->n)) {
             ctx->err = "non-finite coordinate";
@@ -2604,7 +2606,6 @@ int amg_set_coords(amg_ctx* ctx, const double* xyz, const double box[6]) {
         }
         cell_grid(ctx, xyz);
         ctx->have_coords = true;
-        ctx->have_forward = false;
     } catch (Fail& f) {
         return f.code;
     }
